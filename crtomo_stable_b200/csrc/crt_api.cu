@@ -1,0 +1,1095 @@
+// crt_api.cu -- the C ABI (include/crt_b200.h): context, uploads, the
+// forward / Jacobian / update drivers and the Gauss-Newton step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/crt_b200.h"
+#include "crt_band.h"
+#include "crt_cg.h"
+#include "crt_common.cuh"
+#include "crt_sens.h"
+#include "crt_setup.h"
+#include "crt_volt.h"
+
+template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>&, T*, cudaStream_t);
+
+struct crt_ctx {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[8] = {};
+    double timings[7] = {0, 0, 0, 0, 0, 0, 0};
+    int64_t launches = 0;
+    std::string err;
+
+    // sizes
+    int n = 0, mb = 0, W = 0, E = 0, R = 0, ntot = 0, maxnodes = 0, nmn = 0;
+    int L = 0, N = 0, K = 0, swrtr = 1;
+    int lbeta = 0, lrandb = 0, lrandb2 = 0, lsink = 0, nsink = 0;
+    int nkmax = 0;
+    double pi = 0.0;
+
+    // host copies
+    std::vector<double> kwnwi_h, kwn_h;
+    std::vector<int> strnr_h, vnr_h;
+
+    // device mesh / survey
+    int *d_nrel0 = nullptr, *d_snr0 = nullptr, *d_etyp = nullptr, *d_enk = nullptr;
+    int *d_enr0 = nullptr, *d_mixed_rel = nullptr, *d_strnr = nullptr, *d_vnr = nullptr;
+    int4* d_elec = nullptr;
+    double *d_sx = nullptr, *d_sy = nullptr, *d_kwn = nullptr, *d_kwnwi = nullptr;
+    double *d_elbg = nullptr, *d_relbg = nullptr, *d_kg = nullptr;
+    int *d_row_ptr = nullptr, *d_ent_d = nullptr, *d_ent_ptr = nullptr, *d_con_code = nullptr,
+        *d_con_sig = nullptr;
+    unsigned char* d_dflag = nullptr;
+    cd* d_dval = nullptr;
+    int* d_status = nullptr;    // [max(K*L, K) + 8] per-system errnr; [last] global
+    int nstatus = 0;
+
+    // forward state
+    cd *d_sigma = nullptr, *d_kpot = nullptr, *d_kpt = nullptr, *d_volt = nullptr,
+       *d_sigmaa = nullptr, *d_hel = nullptr;
+    int last_ldc = 0, have_forward = 0;
+    // band workspaces (chunked)
+    void* d_Lws = nullptr;
+    void* d_yws = nullptr;
+    double* d_fakws = nullptr;
+    void* d_scratch = nullptr;
+    size_t lws_slot_bytes = 0;
+    int chunk = 0;
+
+    // Jacobian / inversion state
+    void* d_sens = nullptr;
+    int sens_real = 0, have_sens = 0;
+    cd* d_part_sens = nullptr;
+    double* d_strom = nullptr;
+    int ltri = -1, nx = 0, nnb = 0;
+    double* d_smatm = nullptr;
+    int* d_nachbar = nullptr;
+    cd* d_dat = nullptr;
+    double* d_wd = nullptr;
+    double *d_cgfac = nullptr, *d_cgres = nullptr, *d_bdpar = nullptr;
+    cd *d_rhs = nullptr, *d_p = nullptr, *d_r = nullptr, *d_bvec = nullptr, *d_dpar = nullptr,
+       *d_ap = nullptr, *d_cgpart = nullptr, *d_par = nullptr;
+    CGState* d_cgst = nullptr;
+    int cg_nsplit = 1, cg_ncgmax_alloc = 0;
+};
+
+namespace {
+
+bool ck(crt_ctx* c, cudaError_t e, const char* what)
+{
+    if (e == cudaSuccess) return true;
+    c->err = std::string(what) + ": " + cudaGetErrorString(e);
+    return false;
+}
+
+#define CK(call)                                   \
+    do {                                           \
+        if (!ck(ctx, (call), #call)) return CRT_ERR_CUDA; \
+    } while (0)
+
+template <typename T>
+bool dalloc(crt_ctx* ctx, T** p, size_t count)
+{
+    if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void**)p, count * sizeof(T));
+    if (e != cudaSuccess) {
+        ctx->err = std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) + " bytes: " +
+                   cudaGetErrorString(e);
+        *p = nullptr;
+        return false;
+    }
+    return true;
+}
+
+template <typename T>
+bool upload(crt_ctx* ctx, T** p, const T* h, size_t count)
+{
+    if (!dalloc(ctx, p, count)) return false;
+    if (count && h) return ck(ctx, cudaMemcpyAsync(*p, h, count * sizeof(T), cudaMemcpyHostToDevice, ctx->st), "upload");
+    return true;
+}
+
+int set_err(crt_ctx* ctx, int code, const std::string& msg)
+{
+    if (ctx) ctx->err = msg;
+    return code;
+}
+
+// First non-zero per-system status (the reference stops at the first error).
+int collect_status(crt_ctx* ctx, int count)
+{
+    std::vector<int> h(count);
+    if (!ck(ctx, cudaMemcpyAsync(h.data(), ctx->d_status, sizeof(int) * count, cudaMemcpyDeviceToHost, ctx->st),
+            "status copy"))
+        return CRT_ERR_CUDA;
+    if (!ck(ctx, cudaStreamSynchronize(ctx->st), "stream sync")) return CRT_ERR_CUDA;
+    for (int i = 0; i < count; ++i)
+        if (h[i]) {
+            char buf[160];
+            std::snprintf(buf, sizeof buf, "device status %d in system %d", h[i], i);
+            ctx->err = buf;
+            return h[i];
+        }
+    return CRT_OK;
+}
+
+int kernel_check(crt_ctx* ctx, const char* what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_err(ctx, CRT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return CRT_OK;
+}
+
+// Workspace chunk: how many band systems are factored per launch.
+int plan_chunk(crt_ctx* ctx, int nsys, size_t tsize)
+{
+    const size_t slot = (size_t)ctx->n * ctx->W * tsize;
+    size_t budget = (size_t)16 << 30;
+    if (const char* env = std::getenv("CRT_B200_WORKSPACE_GB")) budget = (size_t)(std::atof(env) * (1u << 30));
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 2);
+    int c = (int)std::max<size_t>(1, budget / std::max<size_t>(slot + (size_t)ctx->n * (tsize + 8), 1));
+    return std::min(c, nsys);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+extern "C" int32_t crt_abi_version(void) { return CRT_B200_ABI_VERSION; }
+
+extern "C" const char* crt_last_error(const crt_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+extern "C" int64_t crt_launch_count(const crt_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int32_t crt_last_timings(const crt_ctx* ctx, double* ms7)
+{
+    if (!ctx || !ms7) return CRT_ERR_ARG;
+    for (int i = 0; i < 7; ++i) ms7[i] = ctx->timings[i];
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_rwaven(const crt_mesh* mesh, int32_t eanz, const int32_t* enr, int32_t nanz,
+                              const int32_t* strnr, const int32_t* vnr, int32_t* kwnanz, double* kwn,
+                              double* kwnwi)
+{
+    (void)eanz;
+    if (!mesh || !enr || !strnr || !vnr || !kwnanz || !kwn || !kwnwi) return CRT_ERR_ARG;
+    return crt_rwaven_host(nanz, strnr, vnr, enr, mesh->snr, mesh->sx, mesh->sy, kwnanz, kwn, kwnwi, nullptr,
+                           nullptr);
+}
+
+extern "C" void crt_destroy(crt_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    void* ptrs[] = {ctx->d_nrel0, ctx->d_snr0, ctx->d_etyp, ctx->d_enk, ctx->d_enr0, ctx->d_mixed_rel,
+                    ctx->d_strnr, ctx->d_vnr, ctx->d_elec, ctx->d_sx, ctx->d_sy, ctx->d_kwn, ctx->d_kwnwi,
+                    ctx->d_elbg, ctx->d_relbg, ctx->d_kg, ctx->d_row_ptr, ctx->d_ent_d, ctx->d_ent_ptr,
+                    ctx->d_con_code, ctx->d_con_sig, ctx->d_dflag, ctx->d_dval, ctx->d_status, ctx->d_sigma,
+                    ctx->d_kpot, ctx->d_kpt, ctx->d_volt, ctx->d_sigmaa, ctx->d_hel, ctx->d_Lws, ctx->d_yws,
+                    ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
+                    ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
+                    ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
+                    ctx->d_par, ctx->d_cgst};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->st) cudaStreamDestroy(ctx->st);
+    delete ctx;
+}
+
+extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_survey* sv, int32_t precision,
+                               int32_t* errnr)
+{
+    auto fail = [&](crt_ctx* c, int code) -> crt_ctx* {
+        if (errnr) *errnr = code;
+        if (c && !c->err.empty()) std::fprintf(stderr, "crt_create: %s\n", c->err.c_str());
+        crt_destroy(c);
+        return nullptr;
+    };
+    if (errnr) *errnr = CRT_OK;
+    if (!mesh || !sv) return fail(nullptr, CRT_ERR_ARG);
+    if (precision != CRT_PREC_FP64) return fail(nullptr, CRT_ERR_UNSUPPORTED);
+    crt_ctx* ctx = new crt_ctx();
+    ctx->device = device;
+    ctx->pi = std::acos(-1.0);
+    if (!ck(ctx, cudaSetDevice(device), "cudaSetDevice")) return fail(ctx, CRT_ERR_CUDA);
+    if (!ck(ctx, cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking), "stream")) return fail(ctx, CRT_ERR_CUDA);
+    for (auto& e : ctx->ev)
+        if (!ck(ctx, cudaEventCreate(&e), "event")) return fail(ctx, CRT_ERR_CUDA);
+
+    // ---- mesh
+    MeshHost m{};
+    m.sanz = mesh->sanz;
+    m.mb = mesh->mb;
+    m.typanz = mesh->typanz;
+    m.typ = mesh->typ;
+    m.nelanz = mesh->nelanz;
+    m.selanz = mesh->selanz;
+    m.nrel = mesh->nrel;
+    m.rnr = mesh->rnr;
+    m.snr = mesh->snr;
+    m.sx = mesh->sx;
+    m.sy = mesh->sy;
+    m.elanz = m.relanz = m.maxnodes = 0;
+    for (int t = 0; t < m.typanz; ++t) {
+        if (m.typ[t] > 10) m.relanz += m.nelanz[t];
+        else m.elanz += m.nelanz[t];
+        m.maxnodes = std::max(m.maxnodes, (int)m.selanz[t]);
+    }
+    m.ntot = m.elanz + m.relanz;
+    ctx->n = m.sanz;
+    ctx->mb = m.mb;
+    ctx->W = m.mb + 1;
+    ctx->E = m.elanz;
+    ctx->R = m.relanz;
+    ctx->ntot = m.ntot;
+    ctx->maxnodes = m.maxnodes;
+    ctx->nmn = m.maxnodes * (m.maxnodes + 1) / 2;
+    ctx->L = sv->eanz;
+    ctx->N = sv->nanz;
+    ctx->K = sv->kwnanz;
+    ctx->swrtr = sv->swrtr;
+    ctx->lsink = sv->lsink;
+    ctx->nsink = sv->nsink;
+    if (ctx->n <= 0 || ctx->E <= 0 || ctx->L <= 0 || ctx->K <= 0 || m.maxnodes > 4)
+        return fail(ctx, set_err(ctx, CRT_ERR_ARG, "empty mesh / survey or element with > 4 nodes"));
+    if (band_factor_smem<cd>(ctx->W) > 227 * 1024)
+        return fail(ctx, set_err(ctx, CRT_ERR_UNSUPPORTED, "half bandwidth too large for the FP64 window"));
+
+    // element table: 0-based nodes, types, node counts, boundary flags
+    std::vector<int> nrel0((size_t)m.ntot * m.maxnodes, 0);
+    {
+        // area elements must precede the boundary segments (the reference's
+        // sigma(iel) and nrel(elanz + rel, .) indexing relies on it)
+        bool seen_boundary = false;
+        for (int t = 0; t < m.typanz; ++t) {
+            if (m.typ[t] > 10) seen_boundary = true;
+            else if (seen_boundary)
+                return fail(ctx, set_err(ctx, CRT_ERR_ARG, "area element types listed after boundary types"));
+        }
+    }
+    std::vector<int> et(m.elanz), enk(m.elanz), mixed_rel;
+    std::vector<unsigned char> dflag(ctx->n, 0);
+    std::vector<cd> dval(ctx->n, cd{0.0, 0.0});
+    {
+        int row = 0;
+        for (int t = 0; t < m.typanz; ++t)
+            for (int j = 0; j < m.nelanz[t]; ++j, ++row) {
+                for (int q = 0; q < m.selanz[t]; ++q) {
+                    int node = m.nrel[(size_t)q * m.ntot + row];
+                    if (node < 1 || node > m.sanz)
+                        return fail(ctx, set_err(ctx, CRT_ERR_ARG, "node number out of range in nrel"));
+                    nrel0[(size_t)row * m.maxnodes + q] = node - 1;
+                }
+                if (m.typ[t] <= 10) {
+                    et[row] = m.typ[t];
+                    enk[row] = m.selanz[t];
+                    ctx->nkmax = std::max(ctx->nkmax, (int)m.selanz[t]);
+                } else if (m.typ[t] == 11) {
+                    ctx->lbeta = 1;
+                    const int rel = row - m.elanz;
+                    if (m.rnr[rel] < 1 || m.rnr[rel] > m.elanz)
+                        return fail(ctx, set_err(ctx, 111, "border to element context is wrong (errnr 111)"));
+                    mixed_rel.push_back(rel);
+                } else if (m.typ[t] == 13) {
+                    ctx->lrandb = 1;
+                    for (int q = 0; q < m.selanz[t]; ++q) dflag[m.nrel[(size_t)q * m.ntot + row] - 1] = 1;
+                }
+            }
+    }
+    if (ctx->lbeta && ctx->lrandb)
+        return fail(ctx, set_err(ctx, 101, "mixed boundary and Dirichlet elements together (errnr 101)"));
+    if (sv->rwdanz > 0) {
+        ctx->lrandb2 = 1;
+        for (int i = 0; i < sv->rwdanz; ++i) {
+            int node = sv->rwdnr[i] - 1;
+            dflag[node] = 2;
+            dval[node] = cd{sv->rwd[2 * i], sv->rwd[2 * i + 1]};
+        }
+        // boundary.dat couplings moved to the RHS are not streamed yet
+        bool nonzero = false;
+        for (int i = 0; i < sv->rwdanz; ++i) nonzero |= (sv->rwd[2 * i] != 0.0 || sv->rwd[2 * i + 1] != 0.0);
+        if (nonzero)
+            return fail(ctx, set_err(ctx, CRT_ERR_UNSUPPORTED, "non-zero boundary.dat values are not supported yet"));
+    }
+    AssemblyLists lists;
+    int e = build_assembly_lists(m, lists);
+    if (e) return fail(ctx, set_err(ctx, e, "band width violated in kompab (errnr 19)"));
+
+    std::vector<int> snr0(ctx->n), enr0(ctx->L);
+    for (int i = 0; i < ctx->n; ++i) snr0[i] = mesh->snr[i] - 1;
+    for (int i = 0; i < ctx->L; ++i) {
+        enr0[i] = sv->enr[i] - 1;
+        if (enr0[i] < 0 || enr0[i] >= ctx->n) return fail(ctx, set_err(ctx, 29, "electrode node > sanz (errnr 29)"));
+    }
+    std::vector<int4> elec(ctx->N);
+    for (int i = 0; i < ctx->N; ++i) {
+        int s = sv->strnr[i], v = sv->vnr[i];
+        int e1 = s % 10000, e2 = s / 10000, e3 = v % 10000, e4 = v / 10000;
+        if (std::min({e1, e2, e3, e4}) < 0 || std::max({e1, e2, e3, e4}) > ctx->L)
+            return fail(ctx, set_err(ctx, 46, "electrode number out of range (errnr 46)"));
+        elec[i] = make_int4(e1 - 1, e2 - 1, e3 - 1, e4 - 1);
+    }
+    ctx->strnr_h.assign(sv->strnr, sv->strnr + ctx->N);
+    ctx->vnr_h.assign(sv->vnr, sv->vnr + ctx->N);
+    ctx->kwn_h.assign(sv->kwn, sv->kwn + ctx->K);
+    ctx->kwnwi_h.assign(sv->kwnwi, sv->kwnwi + ctx->K);
+
+    bool ok = upload(ctx, &ctx->d_nrel0, nrel0.data(), nrel0.size()) &&
+              upload(ctx, &ctx->d_snr0, snr0.data(), snr0.size()) &&
+              upload(ctx, &ctx->d_etyp, et.data(), et.size()) && upload(ctx, &ctx->d_enk, enk.data(), enk.size()) &&
+              upload(ctx, &ctx->d_enr0, enr0.data(), enr0.size()) &&
+              upload(ctx, &ctx->d_mixed_rel, mixed_rel.data(), mixed_rel.size()) &&
+              upload(ctx, &ctx->d_strnr, sv->strnr, (size_t)ctx->N) && upload(ctx, &ctx->d_vnr, sv->vnr, (size_t)ctx->N) &&
+              upload(ctx, &ctx->d_elec, elec.data(), elec.size()) && upload(ctx, &ctx->d_sx, mesh->sx, (size_t)ctx->n) &&
+              upload(ctx, &ctx->d_sy, mesh->sy, (size_t)ctx->n) && upload(ctx, &ctx->d_kwn, sv->kwn, (size_t)ctx->K) &&
+              upload(ctx, &ctx->d_kwnwi, sv->kwnwi, (size_t)ctx->K) &&
+              upload(ctx, &ctx->d_row_ptr, lists.row_ptr.data(), lists.row_ptr.size()) &&
+              upload(ctx, &ctx->d_ent_d, lists.ent_d.data(), lists.ent_d.size()) &&
+              upload(ctx, &ctx->d_ent_ptr, lists.ent_ptr.data(), lists.ent_ptr.size()) &&
+              upload(ctx, &ctx->d_con_code, lists.con_code.data(), lists.con_code.size()) &&
+              upload(ctx, &ctx->d_con_sig, lists.con_sig.data(), lists.con_sig.size()) &&
+              upload(ctx, &ctx->d_dflag, dflag.data(), dflag.size()) &&
+              upload(ctx, &ctx->d_dval, dval.data(), dval.size());
+    if (!ok) return fail(ctx, CRT_ERR_ALLOC);
+    ctx->nstatus = std::max(ctx->K * ctx->L, ctx->K) + 8;
+    if (!dalloc(ctx, &ctx->d_status, (size_t)ctx->nstatus)) return fail(ctx, CRT_ERR_ALLOC);
+    if (!ck(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int) * ctx->nstatus, ctx->st), "memset")) return fail(ctx, CRT_ERR_CUDA);
+
+    // ---- precal: elbg [K][E][nmn], relbg [R][3], kg [K][L][R]
+    const size_t n_elbg = (size_t)ctx->K * ctx->E * ctx->nmn;
+    const size_t n_kg = (size_t)ctx->K * ctx->L * std::max(ctx->R, 1);
+    if (!dalloc(ctx, &ctx->d_elbg, n_elbg) || !dalloc(ctx, &ctx->d_relbg, (size_t)std::max(ctx->R, 1) * 3) ||
+        !dalloc(ctx, &ctx->d_kg, n_kg))
+        return fail(ctx, CRT_ERR_ALLOC);
+    cudaMemsetAsync(ctx->d_relbg, 0, sizeof(double) * std::max(ctx->R, 1) * 3, ctx->st);
+    cudaMemsetAsync(ctx->d_kg, 0, sizeof(double) * n_kg, ctx->st);
+    if (sv->elbg) {
+        // Fortran elbg(elanz, nmn, kwnanz) -> [K][E][nmn]
+        std::vector<double> h(n_elbg);
+        for (int k = 0; k < ctx->K; ++k)
+            for (int q = 0; q < ctx->nmn; ++q)
+                for (int el = 0; el < ctx->E; ++el)
+                    h[((size_t)k * ctx->E + el) * ctx->nmn + q] = sv->elbg[((size_t)k * ctx->nmn + q) * ctx->E + el];
+        if (!ck(ctx, cudaMemcpyAsync(ctx->d_elbg, h.data(), sizeof(double) * n_elbg, cudaMemcpyHostToDevice, ctx->st), "elbg"))
+            return fail(ctx, CRT_ERR_CUDA);
+        if (ctx->R > 0 && sv->relbg && sv->kg) {
+            std::vector<double> hr((size_t)ctx->R * 3), hk(n_kg);
+            for (int q = 0; q < 3; ++q)
+                for (int r = 0; r < ctx->R; ++r) hr[(size_t)r * 3 + q] = sv->relbg[(size_t)q * ctx->R + r];
+            std::memcpy(hk.data(), sv->kg, sizeof(double) * n_kg);   // kg(R, L, K) is already [K][L][R]
+            if (!ck(ctx, cudaMemcpyAsync(ctx->d_relbg, hr.data(), sizeof(double) * hr.size(), cudaMemcpyHostToDevice, ctx->st), "relbg") ||
+                !ck(ctx, cudaMemcpyAsync(ctx->d_kg, hk.data(), sizeof(double) * n_kg, cudaMemcpyHostToDevice, ctx->st), "kg"))
+                return fail(ctx, CRT_ERR_CUDA);
+        }
+        if (!ck(ctx, cudaStreamSynchronize(ctx->st), "sync")) return fail(ctx, CRT_ERR_CUDA);
+    } else {
+        SetupArgs A{};
+        A.E = ctx->E;
+        A.R = std::max(ctx->R, 1);
+        A.K = ctx->K;
+        A.L = ctx->L;
+        A.maxnodes = ctx->maxnodes;
+        A.nmn = ctx->nmn;
+        A.nmixed = (int)mixed_rel.size();
+        A.nrel0 = ctx->d_nrel0;
+        A.snr0 = ctx->d_snr0;
+        A.etyp = ctx->d_etyp;
+        A.enk = ctx->d_enk;
+        A.enr0 = ctx->d_enr0;
+        A.mixed_rel = ctx->d_mixed_rel;
+        A.sx = ctx->d_sx;
+        A.sy = ctx->d_sy;
+        A.kwn = ctx->d_kwn;
+        A.sytop = sv->lsytop ? crt_sytop_host(m) : 0.0;
+        A.elbg = ctx->d_elbg;
+        A.relbg = ctx->d_relbg;
+        A.kg = ctx->d_kg;
+        A.status = ctx->d_status + ctx->nstatus - 1;
+        int64_t t1 = (int64_t)ctx->E * ctx->K;
+        k_elem_matrices<<<(unsigned)((t1 + 255) / 256), 256, 0, ctx->st>>>(A);
+        ctx->launches++;
+        if (A.nmixed > 0) {
+            int64_t t2 = (int64_t)A.nmixed * ctx->L * ctx->K;
+            k_beta<<<(unsigned)((t2 + 255) / 256), 256, 0, ctx->st>>>(A);
+            ctx->launches++;
+        }
+        if (kernel_check(ctx, "precal kernels")) return fail(ctx, CRT_ERR_CUDA);
+        int st = collect_status(ctx, ctx->nstatus);
+        if (st) return fail(ctx, st);
+    }
+    return ctx;
+}
+
+extern "C" int32_t crt_precal(crt_ctx* ctx, double* elbg, double* relbg, double* kg, int32_t* lbeta, int32_t* lrandb)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    const size_t n_elbg = (size_t)ctx->K * ctx->E * ctx->nmn;
+    if (elbg) {
+        std::vector<double> h(n_elbg);
+        CK(cudaMemcpyAsync(h.data(), ctx->d_elbg, sizeof(double) * n_elbg, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (int k = 0; k < ctx->K; ++k)
+            for (int q = 0; q < ctx->nmn; ++q)
+                for (int el = 0; el < ctx->E; ++el)
+                    elbg[((size_t)k * ctx->nmn + q) * ctx->E + el] = h[((size_t)k * ctx->E + el) * ctx->nmn + q];
+    }
+    if (relbg && ctx->R > 0) {
+        std::vector<double> h((size_t)ctx->R * 3);
+        CK(cudaMemcpyAsync(h.data(), ctx->d_relbg, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        // relbg(relanz, nmn): only the first three columns are used by 2-node segments
+        for (int q = 0; q < ctx->nmn; ++q)
+            for (int r = 0; r < ctx->R; ++r) relbg[(size_t)q * ctx->R + r] = q < 3 ? h[(size_t)r * 3 + q] : 0.0;
+    }
+    if (kg && ctx->R > 0) {
+        CK(cudaMemcpyAsync(kg, ctx->d_kg, sizeof(double) * (size_t)ctx->K * ctx->L * ctx->R, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    if (lbeta) *lbeta = ctx->lbeta;
+    if (lrandb) *lrandb = ctx->lrandb;
+    return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Forward.
+namespace {
+
+template <typename T>
+int run_forward(crt_ctx* ctx)
+{
+    const int n = ctx->n, W = ctx->W, L = ctx->L, K = ctx->K;
+    const bool mixed = ctx->lbeta != 0;
+    const int nfac = mixed ? K * L : K;
+    const size_t slot_bytes = (size_t)n * W * sizeof(T);
+    int chunk = plan_chunk(ctx, nfac, sizeof(T));
+    // factor workspace
+    if (ctx->lws_slot_bytes != slot_bytes || ctx->chunk < chunk || !ctx->d_Lws) {
+        if (ctx->d_Lws) cudaFree(ctx->d_Lws);
+        if (ctx->d_yws) cudaFree(ctx->d_yws);
+        if (ctx->d_fakws) cudaFree(ctx->d_fakws);
+        if (ctx->d_scratch) cudaFree(ctx->d_scratch);
+        ctx->d_Lws = ctx->d_yws = ctx->d_scratch = nullptr;
+        ctx->d_fakws = nullptr;
+        CK(cudaMalloc(&ctx->d_Lws, slot_bytes * chunk));
+        CK(cudaMalloc(&ctx->d_yws, (size_t)n * sizeof(cd) * chunk));
+        CK(cudaMalloc((void**)&ctx->d_fakws, (size_t)n * sizeof(double) * chunk));
+        if (!mixed) CK(cudaMalloc(&ctx->d_scratch, (size_t)n * sizeof(cd) * chunk * L));
+        ctx->lws_slot_bytes = slot_bytes;
+        ctx->chunk = chunk;
+    }
+    chunk = ctx->chunk;
+    float ms_f = 0, ms_s = 0;
+    for (int s0 = 0; s0 < nfac; s0 += chunk) {
+        const int ns = std::min(chunk, nfac - s0);
+        BandArgs<T> A{};
+        A.n = n;
+        A.mb = ctx->mb;
+        A.W = W;
+        A.sys0 = s0;
+        A.nsys = ns;
+        A.L = L;
+        A.K = K;
+        A.mixed = mixed;
+        A.fuse_rhs = 1;
+        A.E = ctx->E;
+        A.R = std::max(ctx->R, 1);
+        A.nmn = ctx->nmn;
+        A.row_ptr = ctx->d_row_ptr;
+        A.ent_d = ctx->d_ent_d;
+        A.ent_ptr = ctx->d_ent_ptr;
+        A.con_code = ctx->d_con_code;
+        A.con_sig = ctx->d_con_sig;
+        A.elbg = ctx->d_elbg;
+        A.relbg = ctx->d_relbg;
+        A.kg = ctx->d_kg;
+        A.sigma = ctx->d_sigma;
+        A.dflag = ctx->d_dflag;
+        A.dval = ctx->d_dval;
+        A.bdir = nullptr;
+        A.enr0 = ctx->d_enr0;
+        A.lsink = ctx->lsink;
+        A.nsink0 = ctx->nsink - 1;
+        A.Lws = static_cast<T*>(ctx->d_Lws);
+        A.lstride = (size_t)n * W;
+        A.yws = static_cast<T*>(ctx->d_yws);
+        A.fakws = ctx->d_fakws;
+        A.status = ctx->d_status;
+        CK(cudaEventRecord(ctx->ev[0], ctx->st));
+        launch_band_factor<T>(A, ctx->st);
+        ctx->launches++;
+        if (int e = kernel_check(ctx, "band factor")) return e;
+        CK(cudaEventRecord(ctx->ev[1], ctx->st));
+        SolveArgs<T> S{};
+        S.n = n;
+        S.mb = ctx->mb;
+        S.W = W;
+        S.L = L;
+        S.mixed = mixed;
+        S.lsink = ctx->lsink;
+        S.nsink0 = ctx->nsink - 1;
+        S.enr0 = ctx->d_enr0;
+        S.Lws = A.Lws;
+        S.lstride = A.lstride;
+        S.fakws = ctx->d_fakws;
+        S.yws = A.yws;
+        S.kpot = ctx->d_kpot;
+        S.status = ctx->d_status;
+        if (mixed) {
+            S.sys0 = s0;
+            S.nsys = ns;
+            S.factor_of_sys_div = 1;
+            launch_band_solve_with_scratch<T>(S, static_cast<T*>(ctx->d_yws), ctx->st);
+        } else {
+            S.sys0 = s0 * L;
+            S.nsys = ns * L;
+            S.factor_of_sys_div = L;
+            launch_band_solve_with_scratch<T>(S, static_cast<T*>(ctx->d_scratch), ctx->st);
+        }
+        ctx->launches++;
+        if (int e = kernel_check(ctx, "band solve")) return e;
+        CK(cudaEventRecord(ctx->ev[2], ctx->st));
+        CK(cudaEventSynchronize(ctx->ev[2]));
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+        ms_f += a;
+        ms_s += b;
+    }
+    ctx->timings[0] = ms_f;
+    ctx->timings[1] = ms_s;
+    return collect_status(ctx, nfac);
+}
+
+int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
+{
+    const size_t nk = (size_t)ctx->n * ctx->L * ctx->K;
+    if (!ctx->d_kpot) {
+        if (!dalloc(ctx, &ctx->d_kpot, nk)) return CRT_ERR_ALLOC;
+        if (!dalloc(ctx, &ctx->d_volt, (size_t)ctx->N) || !dalloc(ctx, &ctx->d_sigmaa, (size_t)ctx->N) ||
+            !dalloc(ctx, &ctx->d_hel, (size_t)ctx->L * ctx->L))
+            return CRT_ERR_ALLOC;
+    }
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int) * ctx->nstatus, ctx->st));
+    int e = ldc ? run_forward<double>(ctx) : run_forward<cd>(ctx);
+    if (e) return e;
+    double* d_kfak = nullptr;
+    if (kfak_h && mode == 1) {
+        CK(cudaMalloc((void**)&d_kfak, sizeof(double) * ctx->N));
+        CK(cudaMemcpyAsync(d_kfak, kfak_h, sizeof(double) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
+    }
+    VoltArgs V{};
+    V.n = ctx->n;
+    V.L = ctx->L;
+    V.K = ctx->K;
+    V.N = ctx->N;
+    V.swrtr = ctx->swrtr;
+    V.ldc = ldc;
+    V.mode = mode;
+    V.pi = ctx->pi;
+    V.kpot = ctx->d_kpot;
+    V.kwnwi = ctx->d_kwnwi;
+    V.enr0 = ctx->d_enr0;
+    V.strnr = ctx->d_strnr;
+    V.vnr = ctx->d_vnr;
+    V.kfak = d_kfak;
+    V.hel = ctx->d_hel;
+    V.volt = ctx->d_volt;
+    V.sigmaa = ctx->d_sigmaa;
+    V.status = ctx->d_status + ctx->nstatus - 1;
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    launch_voltages(V, ctx->st);
+    ctx->launches += 2;
+    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    if (int k = kernel_check(ctx, "voltages")) return k;
+    CK(cudaEventSynchronize(ctx->ev[4]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[3], ctx->ev[4]);
+    ctx->timings[2] = ms;
+    if (d_kfak) cudaFree(d_kfak);
+    int st = collect_status(ctx, ctx->nstatus);
+    if (st) return st;
+    ctx->last_ldc = ldc;
+    ctx->have_forward = 1;
+    ctx->have_sens = 0;
+    return CRT_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t crt_forward(crt_ctx* ctx, const double* sigma, int32_t ldc, int32_t mode, const double* kfak,
+                               double* volt, double* sigmaa, double* kpot)
+{
+    if (!ctx || !sigma) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->d_sigma && !dalloc(ctx, &ctx->d_sigma, (size_t)ctx->E)) return CRT_ERR_ALLOC;
+    CK(cudaMemcpyAsync(ctx->d_sigma, sigma, sizeof(cd) * ctx->E, cudaMemcpyHostToDevice, ctx->st));
+    int e = forward_common(ctx, ldc, mode, kfak);
+    if (e) return e;
+    if (volt) CK(cudaMemcpyAsync(volt, ctx->d_volt, sizeof(cd) * ctx->N, cudaMemcpyDeviceToHost, ctx->st));
+    if (sigmaa) CK(cudaMemcpyAsync(sigmaa, ctx->d_sigmaa, sizeof(cd) * ctx->N, cudaMemcpyDeviceToHost, ctx->st));
+    if (kpot)
+        CK(cudaMemcpyAsync(kpot, ctx->d_kpot, sizeof(cd) * (size_t)ctx->n * ctx->L * ctx->K, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_potentials(crt_ctx* ctx, double* hpot)
+{
+    if (!ctx || !hpot) return CRT_ERR_ARG;
+    if (!ctx->have_forward) return set_err(ctx, CRT_ERR_ARG, "crt_potentials before crt_forward");
+    CK(cudaSetDevice(ctx->device));
+    cd* d_h = nullptr;
+    CK(cudaMalloc((void**)&d_h, sizeof(cd) * (size_t)ctx->n * ctx->L));
+    VoltArgs V{};
+    V.n = ctx->n;
+    V.L = ctx->L;
+    V.K = ctx->K;
+    V.swrtr = ctx->swrtr;
+    V.pi = ctx->pi;
+    V.kpot = ctx->d_kpot;
+    V.kwnwi = ctx->d_kwnwi;
+    launch_hpot_full(V, d_h, ctx->st);
+    ctx->launches++;
+    if (int e = kernel_check(ctx, "hpot")) {
+        cudaFree(d_h);
+        return e;
+    }
+    CK(cudaMemcpyAsync(hpot, d_h, sizeof(cd) * (size_t)ctx->n * ctx->L, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    cudaFree(d_h);
+    return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Jacobian.
+namespace {
+int jacobian_device(crt_ctx* ctx, int mode, const double* strom_h)
+{
+    const bool real = (mode == 1);
+    const size_t ne = (size_t)ctx->E * ctx->N;
+    if (!ctx->d_kpt && !dalloc(ctx, &ctx->d_kpt, (size_t)ctx->n * ctx->L * ctx->K)) return CRT_ERR_ALLOC;
+    if (!ctx->d_sens || ctx->sens_real != (int)real) {
+        if (ctx->d_sens) cudaFree(ctx->d_sens);
+        ctx->d_sens = nullptr;
+        CK(cudaMalloc(&ctx->d_sens, ne * (real ? sizeof(double) : sizeof(cd))));
+        ctx->sens_real = real;
+    }
+    if (strom_h && mode == 2) {
+        if (!upload(ctx, &ctx->d_strom, strom_h, (size_t)ctx->N)) return CRT_ERR_ALLOC;
+    }
+    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    launch_transpose_kpot(ctx->d_kpot, ctx->d_kpt, ctx->n, ctx->L, ctx->K, ctx->st);
+    ctx->launches++;
+    int kc = 0;
+    size_t smem = sens_smem(ctx->L, ctx->K, ctx->nkmax, ctx->nmn, &kc, 200 * 1024, real);
+    SensArgs S{};
+    S.n = ctx->n;
+    S.E = ctx->E;
+    S.L = ctx->L;
+    S.K = ctx->K;
+    S.N = ctx->N;
+    S.nmn = ctx->nmn;
+    S.maxnodes = ctx->maxnodes;
+    S.swrtr = ctx->swrtr;
+    S.mode = mode;
+    S.kchunk = kc;
+    S.pi = ctx->pi;
+    S.kpt = ctx->d_kpt;
+    S.elbg = ctx->d_elbg;
+    S.kwnwi = ctx->d_kwnwi;
+    S.nrel0 = ctx->d_nrel0;
+    S.enk = ctx->d_enk;
+    S.elec = ctx->d_elec;
+    S.sigma = ctx->d_sigma;
+    S.volt = ctx->d_volt;
+    S.strom = (mode == 2 && strom_h) ? ctx->d_strom : nullptr;
+    S.sens = ctx->d_sens;
+    if (kc < ctx->K) {
+        if (!ctx->d_part_sens && !dalloc(ctx, &ctx->d_part_sens, ne)) return CRT_ERR_ALLOC;
+    }
+    S.part = ctx->d_part_sens;
+    launch_sens(S, smem, real, ctx->st);
+    ctx->launches++;
+    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    if (int e = kernel_check(ctx, "sensitivities")) return e;
+    CK(cudaEventSynchronize(ctx->ev[6]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[5], ctx->ev[6]);
+    ctx->timings[3] = ms;
+    ctx->have_sens = 1;
+    return CRT_OK;
+}
+}  // namespace
+
+extern "C" int32_t crt_jacobian(crt_ctx* ctx, int32_t mode, const double* strom, double* sens)
+{
+    if (!ctx || mode < 0 || mode > 2) return CRT_ERR_ARG;
+    if (!ctx->have_forward) return set_err(ctx, CRT_ERR_ARG, "crt_jacobian before crt_forward");
+    CK(cudaSetDevice(ctx->device));
+    int e = jacobian_device(ctx, mode, strom);
+    if (e) return e;
+    if (sens) {
+        const size_t bytes = (size_t)ctx->E * ctx->N * (mode == 1 ? sizeof(double) : sizeof(cd));
+        CK(cudaMemcpyAsync(sens, ctx->d_sens, bytes, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_set_jacobian(crt_ctx* ctx, int32_t real, const double* sens)
+{
+    if (!ctx || !sens) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    const size_t ne = (size_t)ctx->E * ctx->N;
+    const size_t bytes = ne * (real ? sizeof(double) : sizeof(cd));
+    if (!ctx->d_sens || ctx->sens_real != (real != 0)) {
+        if (ctx->d_sens) cudaFree(ctx->d_sens);
+        ctx->d_sens = nullptr;
+        CK(cudaMalloc(&ctx->d_sens, bytes));
+        ctx->sens_real = real != 0;
+    }
+    CK(cudaMemcpyAsync(ctx->d_sens, sens, bytes, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->have_sens = 1;
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_set_configs(crt_ctx* ctx, const int32_t* strnr, const int32_t* vnr)
+{
+    if (!ctx || !strnr || !vnr) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<int4> elec(ctx->N);
+    for (int i = 0; i < ctx->N; ++i) {
+        int s = strnr[i], v = vnr[i];
+        int e1 = s % 10000, e2 = s / 10000, e3 = v % 10000, e4 = v / 10000;
+        if (std::min({e1, e2, e3, e4}) < 0 || std::max({e1, e2, e3, e4}) > ctx->L)
+            return set_err(ctx, 46, "electrode number out of range (errnr 46)");
+        elec[i] = make_int4(e1 - 1, e2 - 1, e3 - 1, e4 - 1);
+    }
+    CK(cudaMemcpyAsync(ctx->d_strnr, strnr, sizeof(int) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_vnr, vnr, sizeof(int) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_elec, elec.data(), sizeof(int4) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->strnr_h.assign(strnr, strnr + ctx->N);
+    ctx->vnr_h.assign(vnr, vnr + ctx->N);
+    return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Inversion pieces.
+extern "C" int32_t crt_set_regularizer(crt_ctx* ctx, int32_t ltri, int32_t nx, int32_t nnb, const double* smatm,
+                                       const int32_t* nachbar)
+{
+    if (!ctx || !smatm) return CRT_ERR_ARG;
+    if (!(ltri == 0 || ltri == 1 || ltri == 2))
+        return set_err(ctx, CRT_ERR_UNSUPPORTED, "only the smoothness regularisers ltri 0/1/2 are implemented");
+    CK(cudaSetDevice(ctx->device));
+    const int M = ctx->E;
+    ctx->ltri = ltri;
+    ctx->nx = nx;
+    ctx->nnb = nnb;
+    if (ltri == 0) {
+        if (nx < 1 || M % nx != 0) return set_err(ctx, 89, "five-point regulariser needs manz = nx * nz (errnr 89)");
+        if (!upload(ctx, &ctx->d_smatm, smatm, (size_t)M * 3)) return CRT_ERR_ALLOC;
+    } else {
+        if (!nachbar || nnb < 1) return CRT_ERR_ARG;
+        for (size_t q = 0; q < (size_t)M * nnb; ++q)
+            if (nachbar[q] < 0 || nachbar[q] > M) return set_err(ctx, CRT_ERR_ARG, "nachbar entry out of range");
+        if (!upload(ctx, &ctx->d_smatm, smatm, (size_t)M * (nnb + 1)) ||
+            !upload(ctx, &ctx->d_nachbar, nachbar, (size_t)M * (nnb + 1)))
+            return CRT_ERR_ALLOC;
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_set_data(crt_ctx* ctx, const double* dat, const double* wmatd, const int32_t* wdfak)
+{
+    if (!ctx || !dat || !wmatd) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    std::vector<double> wd(ctx->N);
+    for (int i = 0; i < ctx->N; ++i) wd[i] = wmatd[i] * (double)(wdfak ? wdfak[i] : 1);
+    if (!upload(ctx, &ctx->d_dat, reinterpret_cast<const cd*>(dat), (size_t)ctx->N) ||
+        !upload(ctx, &ctx->d_wd, wd.data(), wd.size()))
+        return CRT_ERR_ALLOC;
+    CK(cudaStreamSynchronize(ctx->st));
+    return CRT_OK;
+}
+
+namespace {
+
+int ensure_cg_buffers(crt_ctx* ctx, int ncgmax)
+{
+    const int M = ctx->E, N = ctx->N;
+    if (!ctx->d_cgfac) {
+        int nsplit = std::max(1, std::min(64, (148 * 4) / std::max(1, (N + 255) / 256)));
+        ctx->cg_nsplit = nsplit;
+        bool ok = dalloc(ctx, &ctx->d_cgfac, (size_t)M) && dalloc(ctx, &ctx->d_rhs, (size_t)M) &&
+                  dalloc(ctx, &ctx->d_p, (size_t)M) && dalloc(ctx, &ctx->d_r, (size_t)M) &&
+                  dalloc(ctx, &ctx->d_bvec, (size_t)M) && dalloc(ctx, &ctx->d_dpar, (size_t)M) &&
+                  dalloc(ctx, &ctx->d_ap, (size_t)N) && dalloc(ctx, &ctx->d_cgpart, (size_t)nsplit * N) &&
+                  dalloc(ctx, &ctx->d_cgst, (size_t)1) && dalloc(ctx, &ctx->d_bdpar, (size_t)1) &&
+                  dalloc(ctx, &ctx->d_par, (size_t)M);
+        if (!ok) return CRT_ERR_ALLOC;
+    }
+    if (ctx->cg_ncgmax_alloc < ncgmax + 2) {
+        if (!dalloc(ctx, &ctx->d_cgres, (size_t)ncgmax + 2)) return CRT_ERR_ALLOC;
+        ctx->cg_ncgmax_alloc = ncgmax + 2;
+    }
+    return CRT_OK;
+}
+
+CGArgs make_cg_args(crt_ctx* ctx, const crt_cg_params* prm)
+{
+    CGArgs a{};
+    a.M = ctx->E;
+    a.N = ctx->N;
+    a.jmode = prm->ldc ? 1 : (prm->lfpi ? 2 : 0);
+    a.ltri = ctx->ltri;
+    a.nx = ctx->nx;
+    a.nnb = ctx->nnb;
+    a.ncgmax = prm->ncgmax;
+    a.lam = prm->lam;
+    a.eps = prm->eps;
+    a.J = ctx->d_sens;
+    a.wd = ctx->d_wd;
+    a.smatm = ctx->d_smatm;
+    a.nachbar = ctx->d_nachbar;
+    a.cgfac = ctx->d_cgfac;
+    a.rhs = ctx->d_rhs;
+    a.p = ctx->d_p;
+    a.r = ctx->d_r;
+    a.bvec = ctx->d_bvec;
+    a.dpar = ctx->d_dpar;
+    a.ap = ctx->d_ap;
+    a.part = ctx->d_cgpart;
+    a.nsplit = ctx->cg_nsplit;
+    a.cgres = ctx->d_cgres;
+    a.st = ctx->d_cgst;
+    return a;
+}
+
+// update.f90 on device-resident J, data, response and model (d_par).
+int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, int* ncg_out)
+{
+    if (ctx->ltri < 0) return set_err(ctx, CRT_ERR_ARG, "regulariser not set (crt_set_regularizer)");
+    if (!ctx->d_dat) return set_err(ctx, CRT_ERR_ARG, "data not set (crt_set_data)");
+    if (!ctx->have_sens) return set_err(ctx, CRT_ERR_ARG, "no Jacobian (crt_jacobian / crt_set_jacobian)");
+    if (prm->ldc != ctx->sens_real) return set_err(ctx, CRT_ERR_ARG, "ldc does not match the Jacobian type");
+    if (int e = ensure_cg_buffers(ctx, prm->ncgmax)) return e;
+    CGArgs a = make_cg_args(ctx, prm);
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    launch_cg_setup(a, ctx->d_dat, d_sigmaa, ctx->d_par, ctx->st);
+    launch_cg_init(a, ctx->st);
+    ctx->launches += 2;
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    if (int e = kernel_check(ctx, "cg setup")) return e;
+    // iterate in batches; the device-side stop flag makes surplus launches no-ops
+    CGState hs{};
+    int done_iters = 0;
+    const int batch = 16;
+    while (done_iters < prm->ncgmax) {
+        int it = std::min(batch, prm->ncgmax - done_iters);
+        launch_cg_iterations(a, it, ctx->st);
+        ctx->launches += 5 * it;
+        done_iters += it;
+        CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (hs.done) break;
+    }
+    if (int e = kernel_check(ctx, "cg iterations")) return e;
+    launch_cg_finish(a, prm->lfpi, prm->step, ctx->d_par, ctx->d_bdpar, ctx->st);
+    ctx->launches++;
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[2]));
+    float a1 = 0, a2 = 0;
+    cudaEventElapsedTime(&a1, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&a2, ctx->ev[1], ctx->ev[2]);
+    ctx->timings[4] = a1;
+    ctx->timings[5] = a2;
+    CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (ncg_out) *ncg_out = hs.ncg;
+    return CRT_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t crt_set_model(crt_ctx* ctx, const double* par)
+{
+    if (!ctx || !par) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->d_par && !dalloc(ctx, &ctx->d_par, (size_t)ctx->E)) return CRT_ERR_ALLOC;
+    CK(cudaMemcpyAsync(ctx->d_par, par, sizeof(cd) * ctx->E, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_get_model(crt_ctx* ctx, double* par)
+{
+    if (!ctx || !par || !ctx->d_par) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(par, ctx->d_par, sizeof(cd) * ctx->E, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_update(crt_ctx* ctx, const crt_cg_params* prm, const double* sigmaa, double* par, double* dpar,
+                              double* cgfac, double* cgres, int32_t* ncg, double* bdpar)
+{
+    if (!ctx || !prm || !par) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (int e = ensure_cg_buffers(ctx, prm->ncgmax)) return e;
+    CK(cudaMemcpyAsync(ctx->d_par, par, sizeof(cd) * ctx->E, cudaMemcpyHostToDevice, ctx->st));
+    const cd* d_sa = ctx->d_sigmaa;
+    cd* tmp = nullptr;
+    if (sigmaa) {
+        CK(cudaMalloc((void**)&tmp, sizeof(cd) * ctx->N));
+        CK(cudaMemcpyAsync(tmp, sigmaa, sizeof(cd) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
+        d_sa = tmp;
+    } else if (!ctx->have_forward) {
+        return set_err(ctx, CRT_ERR_ARG, "no forward response for crt_update");
+    }
+    int n_cg = 0;
+    int e = update_device(ctx, prm, d_sa, &n_cg);
+    if (tmp) cudaFree(tmp);
+    if (e) return e;
+    CK(cudaMemcpyAsync(par, ctx->d_par, sizeof(cd) * ctx->E, cudaMemcpyDeviceToHost, ctx->st));
+    if (dpar) CK(cudaMemcpyAsync(dpar, ctx->d_dpar, sizeof(cd) * ctx->E, cudaMemcpyDeviceToHost, ctx->st));
+    if (cgfac) CK(cudaMemcpyAsync(cgfac, ctx->d_cgfac, sizeof(double) * ctx->E, cudaMemcpyDeviceToHost, ctx->st));
+    if (cgres) CK(cudaMemcpyAsync(cgres, ctx->d_cgres, sizeof(double) * (n_cg + 1), cudaMemcpyDeviceToHost, ctx->st));
+    if (bdpar) CK(cudaMemcpyAsync(bdpar, ctx->d_bdpar, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (ncg) *ncg = n_cg;
+    return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Gauss-Newton step.
+namespace {
+__global__ void k_exp_model(const cd* par, cd* sigma, int M)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    // sigma = cdexp(par) (src/bsigma.f90)
+    const cd p = par[i];
+    const double r = exp(p.x);
+    double s, c;
+    sincos(p.y, &s, &c);
+    sigma[i] = cd{r * c, r * s};
+}
+
+int gn_step_device(crt_ctx* ctx, const crt_cg_params* prm, int* ncg)
+{
+    if (!ctx->d_par) return set_err(ctx, CRT_ERR_ARG, "no model (crt_set_model)");
+    if (!ctx->d_sigma && !dalloc(ctx, &ctx->d_sigma, (size_t)ctx->E)) return CRT_ERR_ALLOC;
+    cudaEvent_t t0 = ctx->ev[7];
+    CK(cudaEventRecord(t0, ctx->st));
+    k_exp_model<<<(ctx->E + 255) / 256, 256, 0, ctx->st>>>(ctx->d_par, ctx->d_sigma, ctx->E);
+    ctx->launches++;
+    double tm[7] = {0};
+    int e = forward_common(ctx, prm->ldc, 0, nullptr);
+    if (e) return e;
+    for (int i = 0; i < 3; ++i) tm[i] = ctx->timings[i];
+    e = jacobian_device(ctx, prm->ldc ? 1 : 0, nullptr);
+    if (e) return e;
+    tm[3] = ctx->timings[3];
+    e = update_device(ctx, prm, ctx->d_sigmaa, ncg);
+    if (e) return e;
+    tm[4] = ctx->timings[4];
+    tm[5] = ctx->timings[5];
+    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[3]));
+    float tot = 0;
+    cudaEventElapsedTime(&tot, t0, ctx->ev[3]);
+    tm[6] = tot;
+    for (int i = 0; i < 7; ++i) ctx->timings[i] = tm[i];
+    return CRT_OK;
+}
+}  // namespace
+
+extern "C" int32_t crt_gn_step_device(crt_ctx* ctx, const crt_cg_params* prm, int32_t* ncg)
+{
+    if (!ctx || !prm) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    int n = 0;
+    int e = gn_step_device(ctx, prm, &n);
+    if (ncg) *ncg = n;
+    return e;
+}
+
+extern "C" int32_t crt_gn_step(crt_ctx* ctx, const crt_cg_params* prm, double* par, double* sigmaa, double* cgres,
+                               int32_t* ncg, double* bdpar)
+{
+    if (!ctx || !prm || !par) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (int e = ensure_cg_buffers(ctx, prm->ncgmax)) return e;
+    CK(cudaMemcpyAsync(ctx->d_par, par, sizeof(cd) * ctx->E, cudaMemcpyHostToDevice, ctx->st));
+    int n = 0;
+    int e = gn_step_device(ctx, prm, &n);
+    if (e) return e;
+    CK(cudaMemcpyAsync(par, ctx->d_par, sizeof(cd) * ctx->E, cudaMemcpyDeviceToHost, ctx->st));
+    if (sigmaa) CK(cudaMemcpyAsync(sigmaa, ctx->d_sigmaa, sizeof(cd) * ctx->N, cudaMemcpyDeviceToHost, ctx->st));
+    if (cgres) CK(cudaMemcpyAsync(cgres, ctx->d_cgres, sizeof(double) * (n + 1), cudaMemcpyDeviceToHost, ctx->st));
+    if (bdpar) CK(cudaMemcpyAsync(bdpar, ctx->d_bdpar, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (ncg) *ncg = n;
+    return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Data misfit (src/dmisft.f90:73-137 with chkpo2, lrobust = ldiff = .false.).
+extern "C" double crt_dmisft(int32_t nanz, const double* dat, const double* sigmaa, const double* wmatd,
+                             const double* wmatdr, const double* wmatdp, int32_t lfpi, int32_t lpol, double* betrms,
+                             double* pharms, int32_t* npol)
+{
+    const double pi = std::acos(-1.0);
+    double nrm = 0.0, br = 0.0, ph = 0.0;
+    int ok = 0;
+    for (int i = 0; i < nanz; ++i) {
+        int wdlok = 1;
+        double rd = dat[2 * i], id = dat[2 * i + 1], rs = sigmaa[2 * i], is = sigmaa[2 * i + 1];
+        int idat = id > pi / 2 ? -1 : (id <= -pi / 2 ? 1 : 0);
+        int isig = is > pi / 2 ? -1 : (is <= -pi / 2 ? 1 : 0);
+        if (idat == 0 && isig != 0) {
+            is += (double)isig * pi;
+            if (!lpol) id = id - std::copysign(pi, id);
+            wdlok = 0;
+        } else if (idat != 0 && isig == 0) {
+            if (lpol) id = id + (double)idat * pi;
+            wdlok = 0;
+        } else if (idat != 0 && isig != 0) {
+            is += (double)isig * pi;
+            id += (double)idat * pi;
+        }
+        const double cr = rd - rs, ci = id - is;
+        const double psi = lfpi ? std::sqrt(wmatd[i]) * std::fabs(ci) : std::sqrt(wmatd[i]) * std::hypot(cr, ci);
+        ok += wdlok;
+        nrm += psi * psi * (double)wdlok;
+        if (wmatdr) br += wmatdr[i] * (double)wdlok * cr * cr;
+        if (wmatdp) ph += wmatdp[i] * (double)wdlok * ci * ci;
+    }
+    if (npol) *npol = nanz - ok;
+    if (ok == 0) return -1.0;
+    if (betrms) *betrms = std::sqrt(br / ok);
+    if (pharms) *pharms = std::sqrt(ph / ok);
+    return std::sqrt(nrm / ok);
+}

@@ -1,0 +1,393 @@
+// crt_band.cu -- batched band Cholesky path of the forward model.
+//
+// One CTA owns one band system (one wavenumber k and, with mixed boundaries,
+// one source electrode l).  The system is never materialised in HBM:
+//
+//   * rows of the FE matrix are formed when they enter an (mb+1)-row window
+//     from the gather lists (kompab / kompadc, src/kompab.f90:80-128), with
+//     the Dirichlet edits of randb / randb2 and the diagonal scaling of
+//     scalab / scaldc (src/scalab.f90:52-76) applied on the way in;
+//   * the window is factored right-looking, column by column (the same
+//     L L^T, unconjugated for complex systems, as src/chol.f90:44-78), and the
+//     system's own right-hand side is forward-substituted in the same pass
+//     (the first half of src/vre.f90:45-56);
+//   * each finished column of L leaves the window for a column-packed HBM
+//     workspace; the back substitution (src/vre.f90:58-69) streams it back.
+//
+// The window is addressed in "slot space": row r lives in slot r mod W,
+// W = mb + 1, and the symmetric entry of rows (r1, r2) sits at the packed
+// index of the unordered slot pair, so a slot freed by the outgoing column
+// is exactly the storage the incoming row needs.
+#include "crt_band.h"
+
+namespace {
+
+__device__ __forceinline__ int pair_index(int x, int y)
+{
+    return x >= y ? x * (x + 1) / 2 + y : y * (y + 1) / 2 + x;
+}
+
+template <typename T>
+__device__ __forceinline__ T assemble_entry(const BandArgs<T>& A, int e, int k, int l)
+{
+    T v = Sc<T>::zero();
+    const int c1 = A.ent_ptr[e + 1];
+    const double* elbg_k = A.elbg + (size_t)k * A.E * A.nmn;
+    for (int c = A.ent_ptr[e]; c < c1; ++c) {
+        const int code = A.con_code[c];
+        double coef;
+        if (code >= 0) {
+            coef = elbg_k[code];
+        } else {
+            const int q = -code - 1;
+            coef = A.relbg[q] * A.kg[((size_t)k * A.L + l) * A.R + q / 3];
+        }
+        v += scale(Sc<T>::from(A.sigma[A.con_sig[c]]), coef);
+    }
+    return v;
+}
+
+// Source vector entry of row r before scaling: kompab sets b(enr(l)) = -1
+// and b(nsink) = +1, randb zeroes type-13 nodes, randb2 prescribes -value
+// at boundary.dat nodes and moves their couplings (bdir) to the free rows.
+template <typename T>
+__device__ __forceinline__ T rhs_entry(int r, int src, int lsink, int nsink0,
+                                       const unsigned char* dflag, const cd* dval, const cd* bdir)
+{
+    T b = Sc<T>::zero();
+    if (r == src) b = -Sc<T>::one();
+    if (lsink && r == nsink0) b = Sc<T>::one();
+    const unsigned char f = dflag[r];
+    if (f == 1) b = Sc<T>::zero();
+    else if (f == 2) b = -Sc<T>::from(dval[r]);
+    else if (bdir) b += Sc<T>::from(bdir[r]);
+    return b;
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_band_factor(BandArgs<T> A)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int W = A.W, n = A.n, mb = A.mb;
+    const int P = W * (W + 1) / 2;
+    T* win = reinterpret_cast<T*>(smem_raw);
+    T* col = win + P;
+    T* bsl = col + W;
+    T* rowbuf = bsl + W;
+    double* fakw = reinterpret_cast<double*>(rowbuf + W);
+    __shared__ T s_piv;
+    __shared__ double s_fak;
+    __shared__ int s_err;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+    const int b = blockIdx.x, sys = A.sys0 + b;
+    int k, l;
+    if (A.mixed) {
+        k = sys / A.L;
+        l = sys % A.L;
+    } else {
+        k = sys;
+        l = 0;
+    }
+    T* Lc = A.Lws + (size_t)b * A.lstride;
+    double* fk = A.fakws + (size_t)b * n;
+    const bool fuse = A.fuse_rhs != 0;
+    T* yv = fuse ? A.yws + (size_t)b * n : nullptr;
+    const cd* bdir = (fuse && A.bdir) ? A.bdir + (size_t)b * n : nullptr;
+    const int src = A.enr0[l];
+
+    for (int i = tid; i < P; i += NT) win[i] = Sc<T>::zero();
+    for (int i = tid; i < W; i += NT) {
+        col[i] = Sc<T>::zero();
+        bsl[i] = Sc<T>::zero();
+        rowbuf[i] = Sc<T>::zero();
+        fakw[i] = 0.0;
+    }
+    if (tid == 0) s_err = 0;
+    __syncthreads();
+
+    // Raw (unscaled) entries of row r into rowbuf[d].
+    auto assemble_row = [&](int r) {
+        const int e1 = A.row_ptr[r + 1];
+        for (int e = A.row_ptr[r] + tid; e < e1; e += NT) rowbuf[A.ent_d[e]] = assemble_entry(A, e, k, l);
+    };
+    // Scaling factor of row r from its raw diagonal (thread 0).
+    auto row_fak = [&](int r) {
+        T raw = A.dflag[r] ? Sc<T>::one() : rowbuf[0];
+        double d = Sc<T>::absval(raw);
+        double f = 1.0;
+        if (!(d > 0.0)) {
+            s_err = CRT_ERR_ZERO_DIAG;
+        } else {
+            f = 1.0 / sqrt(d);
+        }
+        s_fak = f;
+        fk[r] = f;
+    };
+    // Scaled row r into slot sr; clears rowbuf.
+    auto scatter_row = [&](int r, int sr, double fr) {
+        const bool dr = A.dflag[r] != 0;
+        for (int d = tid; d <= mb; d += NT) {
+            const int c = r - d;
+            if (c < 0) continue;
+            const int sc_ = c % W;
+            T v;
+            if (d == 0) {
+                T raw = dr ? Sc<T>::one() : rowbuf[0];
+                v = Sc<T>::normalise(raw, Sc<T>::absval(raw));
+            } else {
+                v = (dr || A.dflag[c]) ? Sc<T>::zero() : scale(rowbuf[d], fr * fakw[sc_]);
+            }
+            win[pair_index(sr, sc_)] = v;
+            rowbuf[d] = Sc<T>::zero();
+        }
+        if (tid == 0) {
+            fakw[sr] = fr;
+            if (fuse) bsl[sr] = scale(rhs_entry<T>(r, src, A.lsink, A.nsink0, A.dflag, A.dval, bdir), fr);
+        }
+    };
+
+    // Initial window: rows 0 .. W-1.
+    const int r0n = min(W, n);
+    for (int r = 0; r < r0n; ++r) {
+        assemble_row(r);
+        __syncthreads();
+        if (tid == 0) row_fak(r);
+        __syncthreads();
+        scatter_row(r, r % W, s_fak);
+        __syncthreads();
+    }
+
+    for (int i = 0; i < n; ++i) {
+        const int s = i % W;
+        const int rnew = i + W;
+        // Phase A: pivot of column i, raw assembly of the incoming row.
+        if (tid == 0) {
+            T p = win[pair_index(s, s)];
+            if (Sc<T>::bad_pivot(p)) s_err = CRT_ERR_PIVOT;
+            T lii = Sc<T>::sqrt_(p);
+            s_piv = lii;
+            Lc[(size_t)i * W] = lii;
+            if (fuse) {
+                T yi = Sc<T>::div(bsl[s], lii);
+                bsl[s] = yi;
+                yv[i] = yi;
+            }
+        }
+        if (rnew < n) assemble_row(rnew);
+        __syncthreads();
+        if (s_err) break;
+        // Phase B: column i of L, forward substitution, scaling of the new row.
+        {
+            const T lii = s_piv;
+            const T yi = fuse ? bsl[s] : Sc<T>::zero();
+            for (int x = tid; x < W; x += NT) {
+                if (x == s) continue;
+                const int d = (x - s + W) % W;
+                T v = Sc<T>::zero();
+                if (i + d < n) v = Sc<T>::div(win[pair_index(x, s)], lii);
+                col[x] = v;
+                Lc[(size_t)i * W + d] = v;
+                if (fuse) bsl[x] -= Sc<T>::mul(v, yi);
+            }
+            if (tid == 0) {
+                col[s] = Sc<T>::zero();
+                if (rnew < n) row_fak(rnew);
+            }
+        }
+        __syncthreads();
+        // Phase C: rank-1 update of the trailing window (slot s excluded),
+        // and the new row into the freed slot s.
+        for (int x = warp; x < W; x += NW) {
+            if (x == s) continue;
+            const int dx = (x - s + W) % W;
+            if (i + dx >= n) continue;
+            const T cx = col[x];
+            T* wrow = win + x * (x + 1) / 2;
+            for (int y = lane; y <= x; y += 32) {
+                if (y == s) continue;
+                wrow[y] -= Sc<T>::mul(cx, col[y]);
+            }
+        }
+        if (rnew < n) scatter_row(rnew, s, s_fak);
+        __syncthreads();
+    }
+    if (tid == 0) A.status[sys] = s_err;
+}
+
+// Back substitution (and, for systems without a fused forward pass, the
+// forward substitution of the kompb right-hand side, src/kompb.f90:39-66).
+// Both sweeps are blocked by BB columns: the off-block part of every column
+// is a coalesced dot/axpy over the column-packed factor, the in-block
+// triangle is solved by one warp.
+template <typename T, int NT, int BB>
+__global__ void __launch_bounds__(NT) k_band_solve(SolveArgs<T> A, T* scratch)
+{
+    __shared__ T tri[BB][BB];
+    __shared__ T part[BB];
+    __shared__ T zb[BB];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int NW = NT / 32;
+    const int n = A.n, W = A.W, mb = A.mb;
+    const int b = blockIdx.x, sys = A.sys0 + b;
+    const int slot = b / A.factor_of_sys_div;
+    // solve systems are always (k, l) pairs, sys = k * L + l
+    const int k = sys / A.L, l = sys % A.L;
+    const T* Lc = A.Lws + (size_t)slot * A.lstride;
+    const double* fk = A.fakws + (size_t)slot * n;
+    T* z = scratch + (size_t)b * n;
+
+    // The fused forward pass belongs to the system's own right-hand side:
+    // every (k, l) system with mixed boundaries, only electrode 1 otherwise
+    // (the reference refactors for l == 1 and calls kompb for l > 1).
+    const bool use_fused = A.yws && (A.mixed || l == 0);
+    if (use_fused) {
+        const T* y = A.yws + (size_t)slot * n;
+        for (int i = tid; i < n; i += NT) z[i] = y[i];
+    } else {
+        // kompb right-hand side: b(enr(l)) = -fak, b(nsink) = +fak.
+        for (int i = tid; i < n; i += NT) z[i] = Sc<T>::zero();
+        __syncthreads();
+        if (tid == 0) {
+            const int src = A.enr0[l];
+            z[src] = scale(-Sc<T>::one(), fk[src]);
+            if (A.lsink) z[A.nsink0] = scale(Sc<T>::one(), fk[A.nsink0]);
+        }
+        __syncthreads();
+        // Forward substitution L y = b, right-looking by blocks.
+        for (int c0 = 0; c0 < n; c0 += BB) {
+            const int c1 = min(n, c0 + BB);
+            // in-block triangle, column-major: tri[c-c0][d]
+            for (int t = tid; t < BB * BB; t += NT) {
+                int cc = t / BB, d = t % BB;
+                int c = c0 + cc;
+                tri[cc][d] = (c < c1 && d <= mb && c + d < c1) ? Lc[(size_t)c * W + d] : Sc<T>::zero();
+            }
+            if (tid < BB) zb[tid] = (c0 + tid < c1) ? z[c0 + tid] : Sc<T>::zero();
+            __syncthreads();
+            if (warp == 0) {
+                for (int cc = 0; cc < c1 - c0; ++cc) {
+                    T yc = zb[cc];
+                    if (lane == 0) {
+                        yc = Sc<T>::div(yc, tri[cc][0]);
+                        zb[cc] = yc;
+                    }
+                    __syncwarp();
+                    yc = zb[cc];
+                    int d = lane;
+                    if (d >= 1 && cc + d < c1 - c0) zb[cc + d] -= Sc<T>::mul(tri[cc][d], yc);
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            if (tid < BB && c0 + tid < c1) z[c0 + tid] = zb[tid];
+            // rows beyond the block: b_r -= sum_c L(r, c) y_c
+            for (int r = c1 + tid; r < min(n, c1 + mb); r += NT) {
+                T acc = Sc<T>::zero();
+                for (int cc = max(0, r - mb - c0); cc < c1 - c0; ++cc)
+                    acc += Sc<T>::mul(Lc[(size_t)(c0 + cc) * W + (r - c0 - cc)], zb[cc]);
+                z[r] -= acc;
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    // Back substitution L^T x = y, blocked from the end.
+    for (int c1 = n; c1 > 0; c1 -= BB) {
+        const int c0 = max(0, c1 - BB), nb = c1 - c0;
+        // off-block part of every column in the block (one warp per column)
+        for (int cc = warp; cc < nb; cc += NW) {
+            const int c = c0 + cc;
+            T acc = Sc<T>::zero();
+            for (int d = c1 - c + lane; d <= mb && c + d < n; d += 32)
+                acc += Sc<T>::mul(Lc[(size_t)c * W + d], z[c + d]);
+            // warp reduction
+            for (int off = 16; off > 0; off >>= 1) {
+                T o;
+                if constexpr (sizeof(T) == sizeof(double)) {
+                    o = __shfl_down_sync(0xffffffffu, acc, off);
+                } else {
+                    cd a = Sc<T>::to_cd(acc);
+                    cd r;
+                    r.x = __shfl_down_sync(0xffffffffu, a.x, off);
+                    r.y = __shfl_down_sync(0xffffffffu, a.y, off);
+                    o = *reinterpret_cast<T*>(&r);
+                }
+                acc += o;
+            }
+            if (lane == 0) part[cc] = acc;
+        }
+        for (int t = tid; t < BB * BB; t += NT) {
+            int cc = t / BB, d = t % BB;
+            int c = c0 + cc;
+            tri[cc][d] = (cc < nb && d <= mb && c + d < c1) ? Lc[(size_t)c * W + d] : Sc<T>::zero();
+        }
+        if (tid < BB) zb[tid] = (tid < nb) ? z[c0 + tid] : Sc<T>::zero();
+        __syncthreads();
+        if (warp == 0) {
+            for (int cc = nb - 1; cc >= 0; --cc) {
+                T acc = Sc<T>::zero();
+                int d = lane;
+                if (d >= 1 && cc + d < nb) acc = Sc<T>::mul(tri[cc][d], zb[cc + d]);
+                for (int off = 16; off > 0; off >>= 1) {
+                    T o;
+                    if constexpr (sizeof(T) == sizeof(double)) {
+                        o = __shfl_down_sync(0xffffffffu, acc, off);
+                    } else {
+                        cd a = Sc<T>::to_cd(acc);
+                        cd r;
+                        r.x = __shfl_down_sync(0xffffffffu, a.x, off);
+                        r.y = __shfl_down_sync(0xffffffffu, a.y, off);
+                        o = *reinterpret_cast<T*>(&r);
+                    }
+                    acc += o;
+                }
+                if (lane == 0) zb[cc] = Sc<T>::div(zb[cc] - part[cc] - acc, tri[cc][0]);
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        if (tid < nb) z[c0 + tid] = zb[tid];
+        __syncthreads();
+    }
+    // kpot(j, l, k) = pot(j) * fak(j) with pot = -z.
+    cd* out = A.kpot + ((size_t)k * A.L + l) * n;
+    for (int j = tid; j < n; j += NT) out[j] = Sc<T>::to_cd(scale(-z[j], fk[j]));
+    (void)A.status;
+}
+
+}  // namespace
+
+template <typename T>
+size_t band_factor_smem(int W)
+{
+    size_t P = (size_t)W * (W + 1) / 2;
+    return P * sizeof(T) + 3 * (size_t)W * sizeof(T) + (size_t)W * sizeof(double) + 64;
+}
+
+template <typename T>
+void launch_band_factor(const BandArgs<T>& a, cudaStream_t st)
+{
+    constexpr int NT = 256;
+    size_t smem = band_factor_smem<T>(a.W);
+    cudaFuncSetAttribute(k_band_factor<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_band_factor<T, NT><<<a.nsys, NT, smem, st>>>(a);
+}
+
+// The solve kernel needs one n-vector of scratch per system; it is carved
+// from the caller's y workspace when the forward pass was fused, otherwise
+// from a dedicated buffer passed through SolveArgs::yws == NULL.
+template <typename T>
+void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st)
+{
+    constexpr int NT = 256, BB = 32;
+    k_band_solve<T, NT, BB><<<a.nsys, NT, 0, st>>>(a, scratch);
+}
+
+template size_t band_factor_smem<double>(int);
+template size_t band_factor_smem<cd>(int);
+template void launch_band_factor<double>(const BandArgs<double>&, cudaStream_t);
+template void launch_band_factor<cd>(const BandArgs<cd>&, cudaStream_t);
+template void launch_band_solve_with_scratch<double>(const SolveArgs<double>&, double*, cudaStream_t);
+template void launch_band_solve_with_scratch<cd>(const SolveArgs<cd>&, cd*, cudaStream_t);

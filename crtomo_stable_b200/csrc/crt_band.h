@@ -1,0 +1,50 @@
+// crt_band.h -- batched band factorisation and solves (kompab/kompadc +
+// randb + scalab/scaldc + chol/choldc + vre/vredc in one streamed pass).
+#pragma once
+
+#include "crt_common.cuh"
+
+template <typename T>
+struct BandArgs {
+    int n, mb, W;            // W = mb + 1 window slots
+    int sys0, nsys;          // systems of this launch: sys0 .. sys0+nsys-1
+    int L, K;                // electrodes, wavenumbers
+    int mixed;               // 1: system s is (k = s / L, l = s % L) with its own matrix
+    int fuse_rhs;            // 1: forward-substitute the system's own RHS in the factor pass
+    int E, R, nmn;
+    // gather lists (AssemblyLists, device copies)
+    const int *row_ptr, *ent_d, *ent_ptr, *con_code, *con_sig;
+    const double *elbg, *relbg, *kg;   // [K][E][nmn], [R][3], [K][L][R]
+    const cd* sigma;                   // [E]
+    const unsigned char* dflag;        // [n] 0 free, 1 type-13 node, 2 boundary.dat node
+    const cd* dval;                    // [n] boundary.dat values (for dflag == 2)
+    const cd* bdir;                    // [nsys][n] RHS moves of boundary.dat values, or NULL
+    const int* enr0;                   // [L] 0-based electrode nodes
+    int lsink, nsink0;
+    // workspaces, indexed by b = blockIdx.x (system sys0 + b)
+    T* Lws;                  // column-packed factor: column c at Lws[b*lstride + c*W + d], d = row - c
+    size_t lstride;
+    T* yws;                  // [b][n] forward-substitution result
+    double* fakws;           // [b][n] scaling factors
+    int* status;             // [total systems] errnr per system
+};
+
+template <typename T>
+struct SolveArgs {
+    int n, mb, W;
+    int sys0, nsys, L, mixed;
+    int lsink, nsink0;
+    const int* enr0;
+    const T* Lws;            // factor per workspace slot
+    size_t lstride;
+    const double* fakws;     // [slot][n]
+    const T* yws;            // [slot][n] for fused systems (else NULL)
+    int factor_of_sys_div;   // workspace slot of system s: (s - sys0) / factor_of_sys_div
+    cd* kpot;                // kpot(sanz, eanz, kwnanz) Fortran order
+    int* status;
+};
+
+template <typename T> void launch_band_factor(const BandArgs<T>& a, cudaStream_t st);
+// scratch: one n-vector per launched system (may alias the fused y workspace).
+template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st);
+template <typename T> size_t band_factor_smem(int W);

@@ -1,0 +1,311 @@
+// crt_cg.cu -- preconditioned CG on the Gauss-Newton normal equations.
+//
+// Restates cjggra (src/cg_mod.f90:426-518) and cjggdc (:106-199) with the
+// operator pieces bap (J p, :520-545), bp / bptri (R p, :547-613) and bb
+// (J^H W J p + lam R p, :699-726), and the set-up of src/update.f90:63-231
+// (Jacobi factors cgfac and the scaled right-hand side).
+//
+// J is the sens(nanz, manz) array kept on the device as produced by the
+// Jacobian kernel (column e contiguous in the readings i).  The two HBM
+// passes per iteration are:
+//   k_cg_jv  : ap_i = sum_e p_e J_ie cgfac_e     (threads over i, coalesced,
+//              columns split into nsplit ranges, deterministic reduction)
+//   k_cg_jhv : b_e  = (sum_i conj(J_ie) w_i ap_i + lam (R (cgfac o p))_e) cgfac_e
+//              (one warp per column)
+// The O(M) vector work and the FP64 dot products run in one CTA each; the
+// stop rule is evaluated on the device, so a batch of iterations can be
+// queued without host round trips.  Real systems (DC, final phase
+// improvement) use the same kernels with zero imaginary parts, which keeps
+// the real arithmetic of cjggdc exact.
+#include "crt_cg.h"
+
+namespace {
+
+constexpr int VEC_NT = 1024;
+
+__device__ __forceinline__ cd jval(const CGArgs& A, int e, int i)
+{
+    const size_t o = (size_t)e * A.N + i;
+    if (A.jmode == 1) return cd{static_cast<const double*>(A.J)[o], 0.0};
+    cd v = static_cast<const cd*>(A.J)[o];
+    if (A.jmode == 2) v.y = 0.0;
+    return v;
+}
+
+// bp / bptri: (R (cgfac o p))_i
+__device__ cd reg_apply_cg(const CGArgs& A, const cd* p, int i)
+{
+    const int M = A.M;
+    const double* c = A.cgfac;
+    if (A.ltri == 0) {
+        const int nx = A.nx;
+        const double *s1 = A.smatm, *s2 = s1 + M, *s3 = s2 + M;
+        cd acc{0.0, 0.0};
+        if (i > 0) acc = p[i - 1] * (s2[i - 1] * c[i - 1]);
+        if (i < M - 1) acc = acc + p[i + 1] * (s2[i] * c[i + 1]);
+        if (i >= nx) acc = acc + p[i - nx] * (s3[i - nx] * c[i - nx]);
+        if (i < M - nx) acc = acc + p[i + nx] * (s3[i] * c[i + nx]);
+        return acc + p[i] * (s1[i] * c[i]);
+    }
+    cd acc{0.0, 0.0};
+    for (int j = 0; j < A.nnb; ++j) {
+        const int id = A.nachbar[(size_t)j * M + i];
+        if (id != 0) acc = acc + (p[id - 1] * A.smatm[(size_t)j * M + i]) * c[id - 1];
+    }
+    return acc + (p[i] * A.smatm[(size_t)A.nnb * M + i]) * c[i];
+}
+
+// update.f90:63-106: (R par)_i
+__device__ cd reg_apply_par(const CGArgs& A, const cd* par, int i)
+{
+    const int M = A.M;
+    if (A.ltri == 0) {
+        const int nx = A.nx;
+        const double *s1 = A.smatm, *s2 = s1 + M, *s3 = s2 + M;
+        cd acc{0.0, 0.0};
+        if (i > 0) acc = s2[i - 1] * par[i - 1];
+        if (i < M - 1) acc = acc + s2[i] * par[i + 1];
+        if (i >= nx) acc = acc + s3[i - nx] * par[i - nx];
+        if (i < M - nx) acc = acc + s3[i] * par[i + nx];
+        return acc + s1[i] * par[i];
+    }
+    cd acc{0.0, 0.0};
+    for (int j = 0; j < A.nnb; ++j) {
+        const int id = A.nachbar[(size_t)j * M + i];
+        if (id != 0) acc = acc + A.smatm[(size_t)j * M + i] * par[id - 1];
+    }
+    return acc + A.smatm[(size_t)A.nnb * M + i] * par[i];
+}
+
+__device__ __forceinline__ double reg_diag(const CGArgs& A, int i)
+{
+    return A.ltri == 0 ? A.smatm[i] : A.smatm[(size_t)A.nnb * A.M + i];
+}
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum (all threads receive the total).
+template <int NT>
+__device__ double block_sum(double v, double* red)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = warp_sum(v);
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        double t = lane < NT / 32 ? red[lane] : 0.0;
+        t = warp_sum(t);
+        if (lane == 0) red[32] = t;
+    }
+    __syncthreads();
+    double r = red[32];
+    __syncthreads();
+    return r;
+}
+
+// cgfac and scaled RHS, one warp per model cell.
+__global__ void k_cg_setup(CGArgs A, const cd* dat, const cd* sigmaa, const cd* par)
+{
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= A.M) return;
+    const int e = warp;
+    double an = 0.0, arx = 0.0, ary = 0.0;
+    for (int i = lane; i < A.N; i += 32) {
+        const cd j = jval(A, e, i);
+        const double w = A.wd[i];
+        const cd rd = dat[i] - sigmaa[i];
+        an += (j.x * j.x + j.y * j.y) * w;
+        const cd t = conj(j) * w * rd;
+        arx += t.x;
+        ary += t.y;
+    }
+    an = warp_sum(an);
+    arx = warp_sum(arx);
+    ary = warp_sum(ary);
+    if (lane == 0) {
+        const double dum = an + A.lam * reg_diag(A, e);
+        const double cg = 1.0 / sqrt(dum);
+        A.cgfac[e] = cg;
+        const cd rg = reg_apply_par(A, par, e);
+        const cd b = cd{arx, ary} - rg * A.lam;
+        A.rhs[e] = b * cg;
+    }
+}
+
+__global__ void __launch_bounds__(VEC_NT) k_cg_init(CGArgs A)
+{
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
+        A.dpar[e] = cd{0.0, 0.0};
+        A.r[e] = A.rhs[e];
+        A.p[e] = cd{0.0, 0.0};
+    }
+    if (threadIdx.x == 0) {
+        CGState s{};
+        s.k = 1;
+        s.done = A.ncgmax < 1;
+        s.ncg = 0;
+        *A.st = s;
+    }
+}
+
+// Iteration head: dr = |r|^2, stop rule, beta, p = r + beta p.
+__global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A)
+{
+    __shared__ double red[33];
+    __shared__ int s_stop;
+    CGState* st = A.st;
+    if (st->done) return;
+    double v = 0.0;
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) v += cabs2(A.r[e]);
+    const double dr = block_sum<VEC_NT>(v, red);
+    const int k = st->k;
+    double beta = 0.0;
+    if (threadIdx.x == 0) {
+        s_stop = 0;
+        if (k == 1) {
+            st->dr0 = dr * A.eps;
+            // the real solver (cjggdc) tests the stop rule at k = 1 as well
+            if (A.jmode != 0 && dr <= st->dr0) s_stop = 1;
+        } else {
+            if (dr <= st->dr0) s_stop = 1;
+            st->beta = dr / st->dr1;
+        }
+        if (s_stop) {
+            st->done = 1;
+            st->ncg = k - 1;
+        }
+        st->dr = dr;
+    }
+    __syncthreads();
+    if (s_stop) return;
+    beta = (k == 1) ? 0.0 : st->beta;
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) A.p[e] = A.r[e] + A.p[e] * beta;
+}
+
+// ap partial sums over a column range: thread per reading.
+__global__ void k_cg_jv(CGArgs A)
+{
+    if (A.st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.N) return;
+    const int split = blockIdx.y;
+    const int per = (A.M + A.nsplit - 1) / A.nsplit;
+    const int e0 = split * per, e1 = min(A.M, e0 + per);
+    cd acc{0.0, 0.0};
+    for (int e = e0; e < e1; ++e) acc += (A.p[e] * jval(A, e, i)) * A.cgfac[e];
+    A.part[(size_t)split * A.N + i] = acc;
+}
+
+__global__ void k_cg_jv_reduce(CGArgs A)
+{
+    if (A.st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.N) return;
+    cd acc{0.0, 0.0};
+    for (int s = 0; s < A.nsplit; ++s) acc += A.part[(size_t)s * A.N + i];
+    A.ap[i] = acc;
+}
+
+// b_e = (sum_i conj(J_ie) w_i ap_i + lam (R (cgfac o p))_e) * cgfac_e
+__global__ void k_cg_jhv(CGArgs A)
+{
+    if (A.st->done) return;
+    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (e >= A.M) return;
+    double ax = 0.0, ay = 0.0;
+    for (int i = lane; i < A.N; i += 32) {
+        const cd t = (conj(jval(A, e, i)) * A.wd[i]) * A.ap[i];
+        ax += t.x;
+        ay += t.y;
+    }
+    ax = warp_sum(ax);
+    ay = warp_sum(ay);
+    if (lane == 0) {
+        const cd rp = reg_apply_cg(A, A.p, e);
+        const cd b = cd{ax, ay} + rp * A.lam;
+        A.bvec[e] = b * A.cgfac[e];
+    }
+}
+
+// Iteration tail: alpha = dr / Re(p^H b), dpar += alpha p, r -= alpha b.
+__global__ void __launch_bounds__(VEC_NT) k_cg_end(CGArgs A)
+{
+    __shared__ double red[33];
+    CGState* st = A.st;
+    if (st->done) return;
+    double v = 0.0;
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
+        const cd pp = A.p[e], bb = A.bvec[e];
+        v += pp.x * bb.x + pp.y * bb.y;
+    }
+    const double dr1 = block_sum<VEC_NT>(v, red);
+    const double alpha = st->dr / dr1;
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
+        A.dpar[e] = A.dpar[e] + A.p[e] * alpha;
+        A.r[e] = A.r[e] - A.bvec[e] * alpha;
+    }
+    if (threadIdx.x == 0) {
+        const int k = st->k;
+        st->alpha = alpha;
+        st->dr1 = st->dr;
+        A.cgres[k] = (double)(float)(A.eps * st->dr / st->dr0);
+        st->k = k + 1;
+        if (k + 1 > A.ncgmax) {
+            st->done = 1;
+            st->ncg = A.ncgmax;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(VEC_NT) k_cg_finish(CGArgs A, int lfpi, double step, cd* par,
+                                                      double* bdpar)
+{
+    __shared__ double red[33];
+    double v = 0.0;
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
+        cd d = A.dpar[e];
+        if (lfpi) d = cd{0.0, d.x};
+        d = d * A.cgfac[e];
+        A.dpar[e] = d;
+        par[e] = par[e] + d * step;
+        v += d.x * d.x + d.y * d.y;
+    }
+    const double s = block_sum<VEC_NT>(v, red);
+    if (threadIdx.x == 0) {
+        *bdpar = s * step;
+        A.cgres[0] = (double)(float)A.st->ncg;
+    }
+}
+
+}  // namespace
+
+void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s)
+{
+    const int threads = 256, warps = threads / 32;
+    k_cg_setup<<<(a.M + warps - 1) / warps, threads, 0, s>>>(a, dat, sigmaa, par);
+}
+
+void launch_cg_init(const CGArgs& a, cudaStream_t s) { k_cg_init<<<1, VEC_NT, 0, s>>>(a); }
+
+void launch_cg_iterations(const CGArgs& a, int iters, cudaStream_t s)
+{
+    const int nt = 256;
+    dim3 gjv((a.N + nt - 1) / nt, a.nsplit);
+    const int warps = nt / 32;
+    for (int it = 0; it < iters; ++it) {
+        k_cg_begin<<<1, VEC_NT, 0, s>>>(a);
+        k_cg_jv<<<gjv, nt, 0, s>>>(a);
+        k_cg_jv_reduce<<<(a.N + nt - 1) / nt, nt, 0, s>>>(a);
+        k_cg_jhv<<<(a.M + warps - 1) / warps, nt, 0, s>>>(a);
+        k_cg_end<<<1, VEC_NT, 0, s>>>(a);
+    }
+}
+
+void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* bdpar, cudaStream_t s)
+{
+    k_cg_finish<<<1, VEC_NT, 0, s>>>(a, lfpi, step, par, bdpar);
+}

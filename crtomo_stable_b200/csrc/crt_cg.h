@@ -1,0 +1,42 @@
+// crt_cg.h -- Gauss-Newton normal-equation CG (src/cg_mod.f90, src/update.f90).
+#pragma once
+
+#include "crt_common.cuh"
+
+// Device-resident CG control block (cjgmod scalars).
+struct CGState {
+    double dr, dr0, dr1, alpha, beta;
+    int k;        // next iteration number (1-based)
+    int done;     // 1 once the stop rule fired or ncgmax was reached
+    int ncg;      // completed iterations
+    int pad;
+};
+
+struct CGArgs {
+    int M, N;             // manz, nanz
+    int jmode;            // 0 complex J (cjggra), 1 real sensdc (ldc), 2 real part of complex J (lfpi)
+    int ltri, nx, nnb;    // regulariser: 0 five-point (smatm(M,3)), else neighbour list (smatm(M,nnb+1))
+    int ncgmax;
+    double lam, eps;
+    const void* J;        // [M][N]: cd (jmode 0/2) or double (jmode 1)
+    const double* wd;     // [N] wmatd * wdfak
+    const double* smatm;  // Fortran smatm(M, ncol)
+    const int* nachbar;   // Fortran nachbar(M, nnb+1), 1-based, 0 = none
+    double* cgfac;        // [M]
+    cd* rhs;              // [M] scaled right-hand side (bvec on entry to cjg)
+    cd *p, *r, *bvec, *dpar, *ap;   // [M],[M],[M],[M],[N]
+    cd* part;             // [nsplit][N] partial J*p sums
+    int nsplit;
+    double* cgres;        // [ncgmax + 2]
+    CGState* st;
+};
+
+// update.f90:63-231: cgfac and the scaled RHS from J, the data residual
+// dat - sigmaa and the regularisation gradient lam * R * par.
+void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s);
+// cjggra / cjggdc: resets the state, then runs up to `iters` iterations.
+void launch_cg_init(const CGArgs& a, cudaStream_t s);
+void launch_cg_iterations(const CGArgs& a, int iters, cudaStream_t s);
+// update.f90:300-351: dpar *= cgfac (lfpi: (0, Re dpar) first), par += step
+// dpar, bdpar = step * sum |dpar|^2.
+void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* bdpar, cudaStream_t s);

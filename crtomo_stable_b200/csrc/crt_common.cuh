@@ -1,0 +1,101 @@
+// crt_common.cuh -- shared device helpers for the CRTomo B200 path.
+//
+// Complex numbers are stored as two adjacent doubles (the layout of Fortran
+// COMPLEX(KIND(0D0)) and C99 double _Complex).  Division follows Smith's
+// algorithm (1962) and the square root is the principal branch, which are
+// the rules gfortran applies to the reference's complex arithmetic.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define CRT_HD __host__ __device__ __forceinline__
+
+struct __align__(16) cd {
+    double x, y;
+};
+
+CRT_HD cd mk(double x, double y) { return cd{x, y}; }
+CRT_HD cd operator+(cd a, cd b) { return cd{a.x + b.x, a.y + b.y}; }
+CRT_HD cd operator-(cd a, cd b) { return cd{a.x - b.x, a.y - b.y}; }
+CRT_HD cd operator-(cd a) { return cd{-a.x, -a.y}; }
+CRT_HD cd operator*(cd a, cd b) { return cd{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+CRT_HD cd operator*(cd a, double s) { return cd{a.x * s, a.y * s}; }
+CRT_HD cd operator*(double s, cd a) { return cd{a.x * s, a.y * s}; }
+CRT_HD cd& operator+=(cd& a, cd b) { a.x += b.x; a.y += b.y; return a; }
+CRT_HD cd& operator-=(cd& a, cd b) { a.x -= b.x; a.y -= b.y; return a; }
+CRT_HD cd conj(cd a) { return cd{a.x, -a.y}; }
+CRT_HD double cabs2(cd a) { return a.x * a.x + a.y * a.y; }
+
+// Smith's complex division a / b.
+CRT_HD cd cdiv(cd a, cd b)
+{
+    if (fabs(b.x) >= fabs(b.y)) {
+        double r = b.y / b.x, den = b.x + b.y * r;
+        return cd{(a.x + a.y * r) / den, (a.y - a.x * r) / den};
+    }
+    double r = b.x / b.y, den = b.x * r + b.y;
+    return cd{(a.x * r + a.y) / den, (a.y * r - a.x) / den};
+}
+CRT_HD cd operator/(cd a, cd b) { return cdiv(a, b); }
+CRT_HD cd operator/(cd a, double s) { return cd{a.x / s, a.y / s}; }
+
+// Principal square root: with r = |z|, t = sqrt((r + |Re z|)/2); the root
+// is (t, Im z/(2t)) for Re z >= 0, else (|Im z|/(2t), copysign(t, Im z)).
+CRT_HD cd csqrt_p(cd z)
+{
+    double r = hypot(z.x, z.y);
+    if (r == 0.0) return cd{0.0, 0.0};
+    double t = sqrt(0.5 * (r + fabs(z.x)));
+    if (z.x >= 0.0) return cd{t, z.y / (2.0 * t)};
+    return cd{fabs(z.y) / (2.0 * t), copysign(t, z.y)};
+}
+CRT_HD double cabs_(cd a) { return hypot(a.x, a.y); }
+
+// Scalar traits so kernels can be written once for the complex (kompab /
+// chol / vre) and the real (kompadc / choldc / vredc) systems.
+template <typename T> struct Sc;
+template <> struct Sc<double> {
+    static CRT_HD double zero() { return 0.0; }
+    static CRT_HD double one() { return 1.0; }
+    static CRT_HD double from(cd s) { return s.x; }            // DBLE(sigma)
+    static CRT_HD double absval(double a) { return a; }       // scaldc tests a <= 0
+    static CRT_HD double normalise(double a, double) { return 1.0; }
+    static CRT_HD double sqrt_(double a) { return sqrt(a); }
+    static CRT_HD bool bad_pivot(double s) { return !(s > 0.0); }
+    static CRT_HD double mul(double a, double b) { return a * b; }
+    static CRT_HD double div(double a, double b) { return a / b; }
+    static CRT_HD cd to_cd(double a) { return cd{a, 0.0}; }
+};
+template <> struct Sc<cd> {
+    static CRT_HD cd zero() { return cd{0.0, 0.0}; }
+    static CRT_HD cd one() { return cd{1.0, 0.0}; }
+    static CRT_HD cd from(cd s) { return s; }
+    static CRT_HD double absval(cd a) { return cabs_(a); }
+    static CRT_HD cd normalise(cd a, double d) { return cd{a.x / d, a.y / d}; }
+    static CRT_HD cd sqrt_(cd a) { return csqrt_p(a); }
+    static CRT_HD bool bad_pivot(cd s) { return !(cabs_(s) > 0.0); }
+    static CRT_HD cd mul(cd a, cd b) { return a * b; }
+    static CRT_HD cd div(cd a, cd b) { return cdiv(a, b); }
+    static CRT_HD cd to_cd(cd a) { return a; }
+};
+
+CRT_HD double scale(double a, double s) { return a * s; }
+CRT_HD cd scale(cd a, double s) { return cd{a.x * s, a.y * s}; }
+
+// Reference error numbers (src/error.txt) returned through the C ABI.
+enum crt_errnr : int32_t {
+    CRT_OK = 0,
+    CRT_ERR_BAND = 19,        // kompab: |i-j| > mb
+    CRT_ERR_ORIENT = 26,      // elem3/elem8: bad element orientation
+    CRT_ERR_ZERO_DIAG = 27,   // scalab/scaldc: zero diagonal
+    CRT_ERR_PIVOT = 28,       // chol/choldc: non-positive pivot
+    CRT_ERR_BETA = 35,        // beta: degenerate boundary geometry
+    CRT_ERR_TOPO = 73,        // rwaven: duplicate electrodes
+    CRT_ERR_ZERO_VOLT = 82,   // bvolti: zero voltage
+    CRT_ERR_KFAK = 93,        // bkfak: zero geometric factor
+    CRT_ERR_ALLOC = 97,       // allocation problem
+    CRT_ERR_ARG = 3,          // inconsistent input
+    CRT_ERR_CUDA = 200,       // CUDA runtime failure (no reference counterpart)
+    CRT_ERR_UNSUPPORTED = 201 // option outside the implemented path
+};

@@ -1,0 +1,26 @@
+// crt_sens.h -- reciprocity Jacobian (bsensi / bsendc / bsens).
+#pragma once
+
+#include "crt_common.cuh"
+
+struct SensArgs {
+    int n, E, L, K, N, nmn, maxnodes, swrtr;
+    int mode;              // 0 bsensi (complex, sigma/V), 1 bsendc (real), 2 bsens (CRMod, -strom)
+    int kchunk;            // wavenumbers staged per pass
+    double pi;
+    const cd* kpt;         // [K][n][L]
+    const double* elbg;    // [K][E][nmn]
+    const double* kwnwi;   // [K]
+    const int* nrel0;      // [ntot][maxnodes]
+    const int* enk;        // [E]
+    const int4* elec;      // [N] 0-based C1, C2, P1, P2 (-1 absent)
+    const cd* sigma;       // [E]
+    const cd* volt;        // [N]
+    const double* strom;   // [N] or NULL
+    void* sens;            // [E][N]: cd for modes 0/2, double for mode 1
+    cd* part;              // [E][N] partial sums when K is split (kchunk < K)
+};
+
+void launch_transpose_kpot(const cd* kpot, cd* kpt, int n, int L, int K, cudaStream_t st);
+size_t sens_smem(int L, int K, int nkmax, int nmn, int* kchunk, size_t limit, bool real);
+void launch_sens(const SensArgs& a, size_t smem, bool real, cudaStream_t st);

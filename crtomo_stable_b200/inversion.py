@@ -1,0 +1,371 @@
+"""Host driver of the CRTomo inversion around the device path.
+
+Mirrors the set-up of src/rall.f90 (crtomo.cfg), src/rdati.f90 (data and
+error model), src/bsigm0.f90 (starting model) and the first pass of the
+Gauss-Newton loop of src/inv.f90:332-956 (forward, dmisft, bsensi/bsendc,
+bsmatm, blam0 presets, bpar, update, bsigma, brough), calling the C ABI for
+every hot-path step.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+from typing import Optional
+
+import numpy as np
+
+from . import io, regularization
+from .lib import Context, dmisft
+
+
+@dataclasses.dataclass
+class CRTomoConfig:
+    """crtomo.cfg (src/rall.f90:234-472)."""
+
+    mswitch: int
+    elem: str
+    elec: str
+    volt: str
+    ramd: str
+    ldiff: bool
+    nx: int
+    nz: int
+    alfx: float
+    alfz: float
+    itmax: int
+    ldc: bool
+    lrobust: bool
+    lfphai: bool
+    stabw0: float
+    stabm0: float
+    stabpA1: float
+    stabpB: float
+    stabpA2: float
+    stabp0: float
+    lrho0: bool
+    bet0: float
+    pha0: float
+    lagain: bool
+    swrtr: int
+    lsink: bool
+    nsink: int
+    lrandb2: bool
+    randb: str
+    ltri: int = 0
+    lamfix: float = 0.0
+    llamf: int = 0
+    iseedpri: int = 0
+    modl_stdn: float = 0.0
+
+
+def _lines_no_comments(path):
+    with open(path) as fh:
+        raw = fh.read().splitlines()
+    return raw
+
+
+def read_crtomo_cfg(path: str) -> CRTomoConfig:
+    lines = _lines_no_comments(path)
+    pos = 0
+
+    def nxt():
+        # read_comments (src/get_unit.f90): skip lines whose first non-blank
+        # character is '#', then return the next record
+        nonlocal pos
+        while pos < len(lines) and lines[pos].strip().startswith("#"):
+            pos += 1
+        if pos >= len(lines):
+            raise EOFError(path)
+        ln = lines[pos]
+        pos += 1
+        return ln
+
+    def val(ln):
+        return ln.split("!")[0].strip()
+
+    def first_tok(ln):
+        t = val(ln).split()
+        return t[0] if t else ""
+
+    ln = nxt()
+    try:
+        mswitch = int(first_tok(ln))
+    except ValueError:
+        mswitch = 0
+    elem = val(nxt())
+    elec = val(nxt())
+    volt = val(nxt())
+    ramd = val(nxt())
+    ldiff = io._fortran_bool(first_tok(nxt()))
+    nxt(); nxt(); nxt()          # dd0, dm0, dfm0
+    iseedpri, modl_stdn = 0, 0.0
+    save = pos
+    ln = nxt()
+    toks = val(ln).split()
+    try:
+        iseedpri, modl_stdn = int(toks[0]), float(toks[1])
+    except (ValueError, IndexError):
+        pass  # a non-numeric line is consumed (err= branch of rall)
+    del save
+    nx = int(first_tok(nxt()))
+    nz = int(first_tok(nxt()))
+    alfx = float(first_tok(nxt()))
+    alfz = float(first_tok(nxt()))
+    itmax = int(first_tok(nxt()))
+    ldc = io._fortran_bool(first_tok(nxt()))
+    lrobust = io._fortran_bool(first_tok(nxt()))
+    lfphai = io._fortran_bool(first_tok(nxt()))
+    stabw0 = io._ffloat(first_tok(nxt()))
+    stabm0 = io._ffloat(first_tok(nxt()))
+    stabpA1 = io._ffloat(first_tok(nxt()))
+    stabpB = io._ffloat(first_tok(nxt()))
+    stabpA2 = io._ffloat(first_tok(nxt()))
+    stabp0 = io._ffloat(first_tok(nxt()))
+    lrho0 = io._fortran_bool(first_tok(nxt()))
+    bet0 = io._ffloat(first_tok(nxt()))
+    pha0 = io._ffloat(first_tok(nxt()))
+    lagain = io._fortran_bool(first_tok(nxt()))
+    swrtr = int(first_tok(nxt()))
+    lsink = io._fortran_bool(first_tok(nxt()))
+    nsink = int(first_tok(nxt()))
+    lrandb2 = io._fortran_bool(first_tok(nxt()))
+    randb = val(nxt())
+    ltri = 0
+    lamfix = 0.0
+    llamf = 0
+    try:
+        ln = nxt()
+        s = ln[:2].strip()   # READ '(I2)'
+        ltri = int(s) if s else 0
+        if ltri & (1 << 5):
+            llamf = 1
+            try:
+                lamfix = float(first_tok(nxt()))
+            except (ValueError, EOFError):
+                lamfix = 1.0
+            ltri -= 1 << 5
+            if ltri & (1 << 6):
+                llamf += 2
+                ltri -= 1 << 6
+    except (ValueError, EOFError):
+        ltri = 0
+    if (nx <= 0 or nz <= 0) and ltri == 0:
+        ltri = 1
+    return CRTomoConfig(mswitch, elem, elec, volt, ramd, ldiff, nx, nz, alfx, alfz, itmax, ldc, lrobust,
+                        lfphai, stabw0, stabm0, stabpA1, stabpB, stabpA2, stabp0, lrho0, bet0, pha0, lagain,
+                        swrtr, lsink, nsink, lrandb2, randb, ltri, lamfix, llamf, iseedpri, modl_stdn)
+
+
+@dataclasses.dataclass
+class DataSet:
+    """datmod / invmod arrays after rdati."""
+
+    strnr: np.ndarray
+    vnr: np.ndarray
+    dat: np.ndarray        # complex (-ln|R|, -phase/1000)
+    wmatdr: np.ndarray
+    wmatdp: np.ndarray
+    wmatd_cri: np.ndarray
+    wmatd: np.ndarray
+    wdfak: np.ndarray
+
+
+def error_model(d: io.Data, cfg: CRTomoConfig) -> DataSet:
+    """src/rdati.f90:133-231 without synthetic noise (lnse = .false.), and
+    the wmatd choice of src/rall.f90:802-817."""
+    stabp0 = abs(cfg.stabp0)      # lffhom: negative A3 flags a phase restart
+    bet = np.asarray(d.bet, np.float64)
+    pha = np.asarray(d.pha, np.float64)
+    if d.stabw is not None:
+        stabw = d.stabw / bet
+        stabwp = 1e-3 * d.stabwp if not cfg.ldc else np.zeros_like(bet)
+    else:
+        stabw = 1e-2 * cfg.stabw0 + cfg.stabm0 / bet
+        if cfg.ldc:
+            stabwp = np.zeros_like(bet)
+        else:
+            stabwp = (cfg.stabpA1 * bet ** cfg.stabpB + 1e-2 * cfg.stabpA2 * np.abs(pha) + stabp0) * 1e-3
+    if np.any(bet <= 0):
+        raise ValueError("non-positive resistance (errnr 94)")
+    if cfg.ldc:
+        pha = np.zeros_like(pha)
+    dat = -np.log(bet) - 1j * pha / 1e3
+    wmatdr = 1.0 / stabw ** 2
+    with np.errstate(divide="ignore"):
+        wmatdp = np.where(stabwp > 0, 1.0 / stabwp ** 2, 0.0) if not cfg.ldc else np.zeros_like(bet)
+    wmatd_cri = 1.0 / (stabw ** 2 + stabwp ** 2) if not cfg.ldc else np.zeros_like(bet)
+    lelerr = (not cfg.lfphai and not cfg.ldc) or bool(cfg.mswitch & (1 << 5))
+    if cfg.ldc:
+        wmatd = wmatdr
+    elif lelerr:
+        wmatd = wmatd_cri
+    else:
+        wmatd = wmatdr
+    return DataSet(d.strnr, d.vnr, dat, wmatdr, wmatdp, wmatd_cri, wmatd.copy(), np.ones(len(bet), np.int32))
+
+
+def lam0_preset(cfg: CRTomoConfig, manz: int, nanz: int, lamnull_file: Optional[str] = None) -> Optional[float]:
+    """blam0 presets (src/blam0.f90:45-77 with src/rall.f90:763-800).
+    Returns None when lam0 has to be computed from the Jacobian."""
+    lamnull_cri = 0.0
+    if lamnull_file and os.path.exists(lamnull_file):
+        with open(lamnull_file) as fh:
+            try:
+                lamnull_cri = float(fh.read().split()[0])
+            except (ValueError, IndexError):
+                lamnull_cri = 0.0
+    elif cfg.llamf & 1:
+        lamnull_cri = cfg.lamfix
+    elif cfg.nz == -1:
+        lamnull_cri = float(max(manz, nanz))
+    elif cfg.nz < 0:
+        lamnull_cri = float(abs(cfg.nz))
+    if (cfg.llamf & 1) or lamnull_cri > np.finfo(float).eps:
+        if cfg.nz == -1:
+            return float(np.float32(max(manz, nanz)))
+        return lamnull_cri
+    return None
+
+
+class Inversion:
+    """Device-backed CRTomo state for one tomodir-like problem."""
+
+    def __init__(self, mesh: io.Mesh, enr, data: DataSet, cfg: CRTomoConfig, device: int = 0,
+                 lam0: Optional[float] = None):
+        self.mesh = mesh
+        self.cfg = cfg
+        self.data = data
+        self.ctx = Context(mesh, enr, data.strnr, data.vnr, swrtr=cfg.swrtr, lsink=cfg.lsink,
+                           nsink=cfg.nsink, device=device)
+        self.manz = mesh.elanz
+        self.nanz = len(data.dat)
+        if cfg.ltri == 0:
+            self.smatm = regularization.smatm_reg(mesh, cfg.nx, cfg.nz, cfg.alfx, cfg.alfz)
+            self.ctx.set_regularizer(0, self.smatm, nx=cfg.nx)
+            self.nachbar = None
+        elif cfg.ltri in (1, 2):
+            self.nachbar = regularization.nachbar(mesh)
+            self.smatm = regularization.smatm_tri(mesh, self.nachbar, cfg.alfx, cfg.alfz)
+            self.ctx.set_regularizer(1, self.smatm, nachbar=self.nachbar)
+        else:
+            raise NotImplementedError(f"regulariser ltri={cfg.ltri} is outside the implemented path")
+        self.ctx.set_data(data.dat, data.wmatd, data.wdfak)
+        self.lam0 = lam0 if lam0 is not None else lam0_preset(cfg, self.manz, self.nanz)
+        self.ncgmax = self.manz // 10 if cfg.ltri < 5 else self.manz
+
+    def start_model(self) -> np.ndarray:
+        """bsigm0 with a homogeneous background (src/bsigm0.f90:55-61)."""
+        c = self.cfg
+        if not c.lrho0:
+            raise NotImplementedError("only the homogeneous starting model is implemented")
+        s = complex(math.cos(c.pha0 / 1e3) / c.bet0, -math.sin(c.pha0 / 1e3) / c.bet0)
+        return np.full(self.manz, s, np.complex128)
+
+    def misfit(self, sigmaa):
+        d = self.data
+        return dmisft(d.dat, sigmaa, d.wmatd, d.wmatdr, d.wmatdp)
+
+    def roughness(self, par) -> float:
+        """src/brough_mod.f90 (lprior = lfpi = .false.)."""
+        if self.cfg.ltri == 0:
+            sm = self.smatm
+            M, nx = self.manz, self.cfg.nx
+            rp = sm[:, 0] * par
+            rp[1:] += sm[:-1, 1] * par[:-1]
+            rp[:-1] += sm[:-1, 1] * par[1:]
+            rp[nx:] += sm[:-nx, 2] * par[:-nx]
+            rp[:-nx] += sm[:-nx, 2] * par[nx:]
+            _ = M
+        else:
+            n = self.nachbar.shape[1] - 1
+            rp = np.zeros_like(par)
+            for j in range(n):
+                nb = self.nachbar[:, j]
+                has = nb > 0
+                rp[has] += self.smatm[has, j] * par[nb[has] - 1]
+            rp += self.smatm[:, n] * par
+        return float(np.sum((rp * np.conj(par)).real))
+
+    def first_step(self, eps: float = 1e-4, ncgmax: Optional[int] = None, step: float = 1.0):
+        """IT 0 and the first UP row of inv.ctr: forward at the starting
+        model, misfit, Jacobian, lam0, update, forward at the new model."""
+        if self.lam0 is None:
+            raise NotImplementedError("lam0 from blam0's Jacobian estimate is not wired up yet")
+        sig0 = self.start_model()
+        ldc = self.cfg.ldc
+        volt, sa0 = self.ctx.forward(sig0, ldc=ldc, mode=0)
+        # set-up polarity check (inv.f90:510-519): corrected data / response,
+        # swapped potential electrodes and excluded readings
+        d = self.data
+        dat, sa0, vnr, wdfak = chkpol(d.dat, sa0, d.vnr, lsetup=True)
+        self.data = dataclasses.replace(d, dat=dat, vnr=vnr, wdfak=wdfak)
+        self.ctx.set_data(dat, d.wmatd, wdfak)
+        nrmsd0 = self.misfit(sa0)[0]
+        # J / V is unchanged by the simultaneous swap of P1/P2 and sign of V,
+        # so the Jacobian of this forward pass is used as is
+        self.ctx.jacobian(mode=1 if ldc else 0, copy=False)
+        if np.any(vnr != d.vnr):
+            self.ctx.set_configs(d.strnr, vnr)
+        prm = Context.params(self.lam0, eps=eps, ncgmax=ncgmax or self.ncgmax, ldc=ldc, step=step)
+        par = np.log(sig0)
+        up = self.ctx.update(prm, par, sigmaa=sa0)
+        par1 = up["par"]
+        rough = self.roughness(par1)
+        sig1 = np.exp(par1)
+        _, sa1 = self.ctx.forward(sig1, ldc=ldc, mode=0)
+        nrmsd1 = self.misfit(sa1)[0]
+        return dict(nrmsd0=nrmsd0, nrmsd1=nrmsd1, bdpar=up["bdpar"], rough=rough, ncg=up["ncg"],
+                    cgres=up["cgres"], lam=self.lam0, par=par1, sigmaa0=sa0, sigmaa1=sa1)
+
+    def close(self):
+        self.ctx.close()
+
+
+def load_tomodir_inversion(exe_dir: str, device: int = 0) -> Inversion:
+    """Set up an Inversion from a tomodir's exe/ directory (crtomo.cfg)."""
+    cfg = read_crtomo_cfg(os.path.join(exe_dir, "crtomo.cfg"))
+    mesh = io.read_elem(io.resolve(exe_dir, cfg.elem))
+    enr = io.read_elec(io.resolve(exe_dir, cfg.elec))
+    data = error_model(io.read_volt(io.resolve(exe_dir, cfg.volt)), cfg)
+    return Inversion(mesh, enr, data, cfg, device=device)
+
+
+def chkpol(dat: np.ndarray, sigmaa: np.ndarray, vnr: np.ndarray, lsetup: bool, lpol: bool = False):
+    """Polarity check of src/chkpol.f90:43-128.  Returns corrected copies
+    (dat, sigmaa, vnr, wdfak): readings whose model response and datum sit on
+    opposite sides of +-pi/2 in phase get their potential electrodes swapped
+    and, unless lpol, are excluded (wdfak = 0)."""
+    pi = math.acos(-1.0)
+    dat = np.array(dat, np.complex128)
+    sigmaa = np.array(sigmaa, np.complex128)
+    vnr = np.array(vnr, np.int32)
+    wdfak = np.ones(len(dat), np.int32)
+    for i in range(len(dat)):
+        e3 = int(vnr[i]) % 10000
+        e4 = (int(vnr[i]) - e3) // 10000
+        redat, imdat = dat[i].real, dat[i].imag
+        resig, imsig = sigmaa[i].real, sigmaa[i].imag
+        idat = -1 if imdat > pi / 2 else (1 if imdat <= -pi / 2 else 0)
+        isig = -1 if imsig > pi / 2 else (1 if imsig <= -pi / 2 else 0)
+        if idat == 0 and isig != 0:
+            vnr[i] = e3 * 10000 + e4
+            sigmaa[i] = complex(resig, imsig + isig * pi)
+            if lpol:
+                if not lsetup:
+                    wdfak[i] = 0
+            else:
+                dat[i] = complex(redat, imdat - math.copysign(pi, imdat))
+                wdfak[i] = 0
+        elif idat != 0 and isig == 0:
+            if lpol:
+                dat[i] = complex(redat, imdat + idat * pi)
+                if not lsetup:
+                    wdfak[i] = 0
+            else:
+                wdfak[i] = 0
+        elif idat != 0 and isig != 0:
+            vnr[i] = e3 * 10000 + e4
+            sigmaa[i] = complex(resig, imsig + isig * pi)
+            dat[i] = complex(redat, imdat + idat * pi)
+    return dat, sigmaa, vnr, wdfak

@@ -1,0 +1,184 @@
+/*
+ * crt_b200.h -- C ABI of the B200-native CRTomo forward / sensitivity /
+ * Gauss-Newton inner-solve path (libcrt_b200.so).
+ *
+ * The ABI replaces the Fortran call sites of geophysics-ubonn/crtomo_stable
+ * listed beside each entry point.  Conventions:
+ *   - every entry point returns the reference's integer error number
+ *     (src/error.txt: 0 ok, 19 band width, 26 element orientation, 27 zero
+ *     diagonal, 28 non-positive pivot, 35 boundary geometry, 73 duplicate
+ *     electrodes, 82 zero voltage, 93 zero geometric factor, 97 allocation),
+ *     plus 200 for a CUDA runtime failure and 201 for an option outside the
+ *     implemented path; crt_last_error() gives the message (fetxt);
+ *   - arrays use the Fortran module layouts (column-major) and the
+ *     reference's 1-based node / element / electrode numbers;
+ *   - complex arrays are interleaved (re, im) doubles, the layout of
+ *     COMPLEX(KIND(0D0)) / C99 double _Complex;
+ *   - host arrays are borrowed for the duration of a call only; kpot, the
+ *     Jacobian and the CG vectors stay in device memory inside the context
+ *     between crt_forward -> crt_jacobian -> crt_update;
+ *   - a context is bound to one device and one host thread; calls are
+ *     synchronous.
+ */
+#ifndef CRT_B200_H
+#define CRT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRT_B200_ABI_VERSION 1
+
+typedef struct crt_ctx crt_ctx;
+
+/* Mesh: the elemmod arrays read by src/relem.f90 (elem.dat). */
+typedef struct {
+    int32_t sanz, typanz, mb;
+    const int32_t *typ, *nelanz, *selanz; /* [typanz] */
+    const int32_t *snr;                   /* [sanz] coordinate row of each node */
+    const double *sx, *sy;                /* [sanz] */
+    const int32_t *nrel;                  /* nrel(elanz+relanz, max(selanz)) */
+    const int32_t *rnr;                   /* rnr(relanz) */
+} crt_mesh;
+
+/* Electrodes, measurements, wavenumbers and boundary options
+ * (electrmod, datmod, wavenmod, femmod, randbmod). */
+typedef struct {
+    int32_t eanz;
+    const int32_t *enr;                   /* [eanz] node numbers */
+    int32_t nanz;
+    const int32_t *strnr, *vnr;           /* [nanz] C1 + 10000*C2, P1 + 10000*P2 */
+    int32_t kwnanz, swrtr;                /* swrtr 0: 2D (kwnanz 1), 1: 2.5D */
+    const double *kwn, *kwnwi;            /* [kwnanz] from rwaven (crt_rwaven) */
+    /* precal results in Fortran layout, or NULL to compute them on the
+     * device (src/precal.f90): elbg(elanz, nmn, kwnanz), relbg(relanz, nmn),
+     * kg(relanz, eanz, kwnanz), nmn = m(m+1)/2, m = max(selanz). */
+    const double *elbg, *relbg, *kg;
+    int32_t lsink, nsink;                 /* fictitious sink node */
+    int32_t rwdanz;                       /* boundary.dat (lrandb2) */
+    const int32_t *rwdnr;                 /* [rwdanz] node numbers */
+    const double *rwd;                    /* [rwdanz] complex values */
+    int32_t lsytop;                       /* mswitch bit 8: mirror about sytop */
+} crt_survey;
+
+/* Inner-solve controls (konvmod / cjgmod / invmod). */
+typedef struct {
+    double lam;        /* regularisation parameter */
+    double eps;        /* stop when |r|^2 <= eps |r0|^2 (reference default 1e-4) */
+    int32_t ncgmax;    /* iteration cap (reference: manz/10 for ltri < 5) */
+    int32_t ldc;       /* DC inversion: real Jacobian (bsendc), cjggdc */
+    int32_t lfpi;      /* final phase improvement: real part of J, imaginary RHS */
+    double step;       /* model step length applied by crt_update */
+} crt_cg_params;
+
+/* Precision of the band factorisations and solves. */
+#define CRT_PREC_FP64 0
+
+/* Creates a context on `device`: uploads the mesh, builds the gather lists
+ * of the streamed assembly, and evaluates precal on the device unless the
+ * survey provides elbg/relbg/kg.  Replaces the set-up part of
+ * src/inv.f90:179-248 / src/fem.f90:308-326 (precal + ALLOCATEs). */
+crt_ctx *crt_create(int32_t device, const crt_mesh *mesh, const crt_survey *survey,
+                    int32_t precision, int32_t *errnr);
+void crt_destroy(crt_ctx *ctx);
+const char *crt_last_error(const crt_ctx *ctx);
+int32_t crt_abi_version(void);
+
+/* Wavenumbers and weights: src/rwaven.f90:22-171 (FP64, host).  kwn and
+ * kwnwi need room for 30 values. */
+int32_t crt_rwaven(const crt_mesh *mesh, int32_t eanz, const int32_t *enr, int32_t nanz,
+                   const int32_t *strnr, const int32_t *vnr, int32_t *kwnanz, double *kwn,
+                   double *kwnwi);
+
+/* Copies the device precal results to the host in Fortran layout
+ * (src/precal.f90 outputs elbg, relbg, kg) and reports lbeta / lrandb. */
+int32_t crt_precal(crt_ctx *ctx, double *elbg, double *relbg, double *kg, int32_t *lbeta,
+                   int32_t *lrandb);
+
+/* Forward model for conductivities sigma(elanz) (complex):
+ * the wavenumber x electrode loop of src/inv.f90:343-484 / src/fem.f90:
+ * 328-397 (kompab/kompadc, randb/randb2, scalab/scaldc, chol/choldc,
+ * kompb, vre/vredc), then rtrafo (src/rtrafo.f90) at the electrode nodes
+ * and bvolti (mode 0, src/bvolti.f90: sigmaa = -ln V) or bvolt (mode 1,
+ * src/bvolt.f90: sigmaa = kfak V, kfak NULL = 1).
+ * ldc != 0 solves the real systems with Re(sigma).
+ * volt / sigmaa: complex [nanz]; kpot: complex kpot(sanz, eanz, kwnanz) or
+ * NULL (kept on the device for crt_jacobian / crt_potentials). */
+int32_t crt_forward(crt_ctx *ctx, const double *sigma, int32_t ldc, int32_t mode,
+                    const double *kfak, double *volt, double *sigmaa, double *kpot);
+
+/* Potentials of the last forward call at all nodes, hpot(sanz, eanz)
+ * (rtrafo, src/rtrafo.f90:46-90, used by bpot/wpot). */
+int32_t crt_potentials(crt_ctx *ctx, double *hpot);
+
+/* Jacobian of the last forward call: mode 0 bsensi (src/bsensi.f90),
+ * 1 bsendc (src/bsendc.f90, real), 2 bsens (src/bsens.f90, CRMod).
+ * strom: [nanz] currents for mode 2 (NULL = 1).  sens: sens(nanz, elanz),
+ * complex (modes 0, 2) or real (mode 1), or NULL to keep it on the device. */
+int32_t crt_jacobian(crt_ctx *ctx, int32_t mode, const double *strom, double *sens);
+
+/* Uploads a Jacobian computed elsewhere (complex sens(nanz, manz), or real
+ * sensdc when real != 0), replacing the device-resident one. */
+int32_t crt_set_jacobian(crt_ctx *ctx, int32_t real, const double *sens);
+
+/* Replaces the measurement configurations (same nanz), e.g. after the
+ * polarity check of src/chkpol.f90 swapped potential electrodes. */
+int32_t crt_set_configs(crt_ctx *ctx, const int32_t *strnr, const int32_t *vnr);
+
+/* Regularisation operator R (src/bsmatm_mod.f90): ltri 0 five-point
+ * smatm(manz, 3) with nx cells per row; ltri 1/2 neighbour form
+ * smatm(manz, nnb+1) with nachbar(manz, nnb+1). */
+int32_t crt_set_regularizer(crt_ctx *ctx, int32_t ltri, int32_t nx, int32_t nnb,
+                            const double *smatm, const int32_t *nachbar);
+
+/* Data and weights (datmod / invmod): dat complex [nanz] (-ln|R|, -phase),
+ * wmatd [nanz], wdfak [nanz] (NULL = 1). */
+int32_t crt_set_data(crt_ctx *ctx, const double *dat, const double *wmatd, const int32_t *wdfak);
+
+/* src/update.f90:27-353 (lprior = ldiff = lw_ref = .false.): regularisation
+ * gradient, Jacobi factors cgfac, scaled RHS, the CG of src/cg_mod.f90
+ * (cjggra, or cjggdc for ldc / lfpi) on the device-resident Jacobian and
+ * the model step par += step * dpar.  sigmaa: complex [nanz] forward
+ * response (NULL = from the last crt_forward); par: complex [manz] in/out.
+ * Optional outputs (NULL to skip): dpar [manz] complex, cgfac [manz],
+ * cgres [ncgmax+1] (cgres[0] = ncg, cgres[k] = eps |r_k|^2/|r_0|^2 as
+ * float), ncg, bdpar. */
+int32_t crt_update(crt_ctx *ctx, const crt_cg_params *prm, const double *sigmaa, double *par,
+                   double *dpar, double *cgfac, double *cgres, int32_t *ncg, double *bdpar);
+
+/* One Gauss-Newton step of the reference loop (src/inv.f90:426-495,
+ * :739-743, :924-933): sigma = exp(par); forward + bvolti; bsensi (or
+ * bsendc); update.  par is updated in place.  Outputs as crt_update plus
+ * sigmaa (complex [nanz], the response of the model the step started
+ * from; NULL to skip). */
+int32_t crt_gn_step(crt_ctx *ctx, const crt_cg_params *prm, double *par, double *sigmaa,
+                    double *cgres, int32_t *ncg, double *bdpar);
+
+/* Device-resident variant used for throughput measurement: the same step
+ * on a model already in device memory (crt_set_model) without host
+ * copies.  Returns after the work is enqueued and completed. */
+int32_t crt_set_model(crt_ctx *ctx, const double *par);
+int32_t crt_gn_step_device(crt_ctx *ctx, const crt_cg_params *prm, int32_t *ncg);
+int32_t crt_get_model(crt_ctx *ctx, double *par);
+
+/* Timings of the phases of the last crt_gn_step / crt_gn_step_device
+ * (milliseconds, CUDA events on the context stream): [0] forward factor,
+ * [1] forward solves, [2] voltages, [3] Jacobian, [4] CG set-up, [5] CG
+ * iterations, [6] total. */
+int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
+
+/* Kernel launches enqueued by the context since creation. */
+int64_t crt_launch_count(const crt_ctx *ctx);
+
+/* Data misfit: src/dmisft.f90:73-137 with chkpo2 (FP64, host).
+ * Returns nrmsd; betrms / pharms / npol optional. */
+double crt_dmisft(int32_t nanz, const double *dat, const double *sigmaa, const double *wmatd,
+                  const double *wmatdr, const double *wmatdp, int32_t lfpi, int32_t lpol,
+                  double *betrms, double *pharms, int32_t *npol);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CRT_B200_H */

@@ -1,0 +1,265 @@
+"""Parity of the device path (through the C ABI) with the FP64 oracle and the
+reference's recorded outputs.  Tolerances are relative and stated per test:
+the device path computes in FP64 with a different summation order
+(right-looking factorisation, tree reductions), so results agree with the
+oracle to ~1e-12 and with the float32 text goldens to their print precision.
+"""
+import numpy as np
+import pytest
+
+from fixtures import FORWARD_CASES, load_forward_case, read_eps_ctr_first_block, read_inv_ctr_rows, wdatm_phase
+
+pytestmark = pytest.mark.gpu
+
+RTOL_FP64 = 1e-10      # device FP64 vs oracle FP64 (potentials, voltages)
+RTOL_SENS = 1e-9       # Jacobian entries relative to the column's largest entry
+
+
+def _ctx(case):
+    from crtomo_stable_b200.lib import Context
+    c = case
+    return Context(c["mesh"], c["enr"], c["volt"].strnr, c["volt"].vnr, swrtr=c["cfg"].swrtr,
+                   lsink=c["cfg"].lsink, nsink=c["cfg"].nsink)
+
+
+def _oracle(case):
+    from oracle.oracle import OracleProblem
+    c = case
+    return OracleProblem(c["mesh"], c["enr"], c["volt"].strnr, c["volt"].vnr, swrtr=c["cfg"].swrtr,
+                         lsink=c["cfg"].lsink, nsink=c["cfg"].nsink)
+
+
+def test_library_loads_on_device():
+    from crtomo_stable_b200 import lib
+    L = lib.load()
+    assert L.crt_abi_version() == 1
+
+
+@pytest.mark.parametrize("name", ["minimal", "TestModInv", "grid_decoupling"])
+def test_precal_matches_oracle(name):
+    case = load_forward_case(name)
+    ctx = _ctx(case)
+    op = _oracle(case)
+    elbg, relbg, kg, lbeta, lrandb = ctx.precal()
+    m = case["mesh"]
+    nmn = m.maxnodes * (m.maxnodes + 1) // 2
+    ref_elbg = op.elbg.reshape((m.elanz, nmn, len(op.kwn)), order="F")
+    np.testing.assert_allclose(elbg, ref_elbg, rtol=1e-13, atol=1e-13 * np.abs(ref_elbg).max())
+    assert lbeta == op.p.lbeta and lrandb == op.p.lrandb
+    if op.p.lbeta:
+        R = m.relanz
+        ref_kg = op.kg.reshape((R, len(op.enr), len(op.kwn)), order="F")
+        ref_relbg = op.relbg.reshape((R, nmn), order="F")
+        mixed = np.repeat(m.typ, m.nelanz)[m.elanz:] == 11
+        np.testing.assert_allclose(kg[mixed], ref_kg[mixed], rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(relbg[mixed, :3], ref_relbg[mixed, :3], rtol=1e-14)
+    ctx.close()
+
+
+@pytest.mark.parametrize("name", sorted(FORWARD_CASES))
+def test_forward_matches_oracle_and_golden(name):
+    case = load_forward_case(name)
+    ctx = _ctx(case)
+    op = _oracle(case)
+    volt_g, sa_g, kpot_g = ctx.forward(case["sigma"], mode=1, want_kpot=True)
+    kpot_o = op.forward(case["sigma"], nthreads=4)
+    scale = np.abs(kpot_o).max()
+    assert np.abs(kpot_g - kpot_o).max() <= RTOL_FP64 * scale
+    hp = op.rtrafo(kpot_o)
+    volt_o, _ = op.bvolt(hp)
+    np.testing.assert_allclose(volt_g, volt_o, rtol=RTOL_FP64, atol=RTOL_FP64 * np.abs(volt_o).max())
+    mag, pha = wdatm_phase(sa_g)
+    d = case["volt"]
+    assert np.abs(mag / d.bet - 1).max() <= FORWARD_CASES[name]
+    assert np.abs(pha - d.pha).max() <= 1e-3
+    ctx.close()
+
+
+def test_forward_dc_path_matches_oracle():
+    """kompadc / scaldc / choldc / vredc with Re(sigma) (ldc)."""
+    case = load_forward_case("TestModInv")
+    ctx = _ctx(case)
+    op = _oracle(case)
+    _, _, kp_g = ctx.forward(case["sigma"], ldc=True, want_kpot=True)
+    kp_o = op.forward(case["sigma"], ldc=True, nthreads=4)
+    assert np.abs(kp_g.imag).max() == 0.0
+    assert np.abs(kp_g - kp_o).max() <= RTOL_FP64 * np.abs(kp_o).max()
+    ctx.close()
+
+
+def test_potentials_match_oracle_rtrafo():
+    case = load_forward_case("minimal")
+    ctx = _ctx(case)
+    op = _oracle(case)
+    ctx.forward(case["sigma"])
+    hp_g = ctx.potentials()
+    hp_o = op.rtrafo(op.forward(case["sigma"]))
+    assert np.abs(hp_g - hp_o).max() <= RTOL_FP64 * np.abs(hp_o).max()
+    ctx.close()
+
+
+@pytest.mark.parametrize("name,mode", [("minimal", 0), ("TestModInv", 0), ("TestModInv", 1),
+                                       ("mixed_surf", 2), ("grid_decoupling", 0)])
+def test_jacobian_matches_oracle(name, mode):
+    case = load_forward_case(name)
+    ctx = _ctx(case)
+    op = _oracle(case)
+    sig = case["sigma"]
+    ldc = mode == 1
+    volt_g, _ = ctx.forward(sig, ldc=ldc)
+    J_g = ctx.jacobian(mode=mode)
+    kp = op.forward(sig, ldc=ldc, nthreads=4)
+    volt_o, _ = op.bvolti(op.rtrafo(kp)) if mode != 2 else op.bvolt(op.rtrafo(kp))
+    if mode == 0:
+        J_o = op.bsensi(kp, sig, volt_o, nthreads=4)
+    elif mode == 1:
+        J_o = op.bsendc(kp, sig, volt_o, nthreads=4)
+    else:
+        J_o = op.bsens(kp, nthreads=4)
+    colmax = np.abs(J_o).max(axis=0, keepdims=True) + 1e-300
+    assert (np.abs(J_g - J_o) / colmax).max() <= RTOL_SENS
+    ctx.close()
+
+
+def _setup_cg_case(name="minimal"):
+    from crtomo_stable_b200 import regularization
+    from crtomo_stable_b200.lib import Context
+    case = load_forward_case(name)
+    ctx = _ctx(case)
+    op = _oracle(case)
+    m = case["mesh"]
+    d = case["volt"]
+    dat = -np.log(d.bet) - 1j * d.pha / 1e3
+    wmatd = 1.0 / (1e-2 + 1e-3 / d.bet) ** 2
+    sig = np.full(m.elanz, 0.01 + 0j)
+    ctx.forward(sig)
+    ctx.jacobian(mode=0, copy=False)
+    kp = op.forward(sig, nthreads=4)
+    volt_o, sa_o = op.bvolti(op.rtrafo(kp))
+    J_o = op.bsensi(kp, sig, volt_o, nthreads=4)
+    nb = regularization.nachbar(m)
+    sm = regularization.smatm_tri(m, nb, 10.0, 1.0)
+    ctx.set_regularizer(1, sm, nachbar=nb)
+    ctx.set_data(dat, wmatd)
+    return ctx, op, case, dat, wmatd, sig, sa_o, J_o, nb, sm, Context
+
+
+def test_update_cg_matches_oracle():
+    from oracle.oracle import OracleCG
+    ctx, op, case, dat, wmatd, sig, sa_o, J_o, nb, sm, Context = _setup_cg_case()
+    E = case["mesh"].elanz
+    lam, eps, ncgmax = 300.0, 1e-4, E // 10
+    cg = OracleCG(E, len(dat), 1, sm, nachbar=nb, nnb=case["mesh"].maxnodes, wmatd=wmatd, lam=lam, eps=eps,
+                  ncgmax=ncgmax)
+    par = np.log(sig)
+    ref = cg.update(J_o, dat, sa_o, par, 1.0)
+    got = ctx.update(Context.params(lam, eps=eps, ncgmax=ncgmax), par)
+    assert got["ncg"] == ref["ncg"]
+    np.testing.assert_allclose(got["cgfac"], ref["cgfac"], rtol=1e-11)
+    np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-7, atol=1e-7 * np.abs(ref["dpar"]).max())
+    np.testing.assert_allclose(got["bdpar"], ref["bdpar"], rtol=1e-8)
+    # the CG residual history is the float32 record cgres(k+1) = eps |r|^2/|r0|^2
+    np.testing.assert_allclose(got["cgres"][1:], ref["cgres"][1:], rtol=1e-5)
+    ctx.close()
+
+
+def test_cg_tight_tolerance_converges_and_matches():
+    """rel-res 1e-6 (|r|^2 <= 1e-12 |r0|^2): the iteration the metric uses."""
+    from oracle.oracle import OracleCG
+    ctx, op, case, dat, wmatd, sig, sa_o, J_o, nb, sm, Context = _setup_cg_case()
+    E = case["mesh"].elanz
+    cg = OracleCG(E, len(dat), 1, sm, nachbar=nb, nnb=case["mesh"].maxnodes, wmatd=wmatd, lam=300.0, eps=1e-12,
+                  ncgmax=2000)
+    par = np.log(sig)
+    ref = cg.update(J_o, dat, sa_o, par, 1.0)
+    got = ctx.update(Context.params(300.0, eps=1e-12, ncgmax=2000), par)
+    assert got["ncg"] < 2000 and ref["ncg"] < 2000
+    assert abs(got["ncg"] - ref["ncg"]) <= 2
+    np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-6, atol=1e-6 * np.abs(ref["dpar"]).max())
+    ctx.close()
+
+
+def test_gn_first_step_minimal_golden():
+    """IT 0 / UP 1 of tests/minimal/Reference/inv/inv.ctr and the IT 0 model
+    response of eps.ctr / volt00.dat."""
+    import os
+    from crtomo_stable_b200 import inversion, io
+    base = os.path.join(os.path.dirname(__file__), "golden", "minimal")
+    cfg = inversion.read_crtomo_cfg(os.path.join(base, "exe", "crtomo.cfg"))
+    assert cfg.ltri == 1 and cfg.nz == -1
+    mesh = io.read_elem(os.path.join(base, "grid", "elem.dat"))
+    enr = io.read_elec(os.path.join(base, "grid", "elec.dat"))
+    data = inversion.error_model(io.read_volt(os.path.join(base, "mod", "volt.dat")), cfg)
+    inv = inversion.Inversion(mesh, enr, data, cfg)
+    res = inv.first_step()
+    rows = read_inv_ctr_rows(os.path.join(base, "inv", "inv.ctr"))
+    it0 = [r for r in rows if r["kind"] == "IT"][0]
+    up1 = [r for r in rows if r["kind"] == "UP"][0]
+    assert abs(res["nrmsd0"] / it0["rms"] - 1) < 5e-4
+    assert abs(res["nrmsd1"] / up1["rms"] - 1) < 5e-4
+    assert abs(res["bdpar"] / up1["step"] - 1) < 5e-3
+    assert abs(res["rough"] / up1["rough"] - 1) < 5e-4
+    assert res["lam"] == up1["lam"]
+    assert res["ncg"] == up1["ncg"]
+    f0 = read_eps_ctr_first_block(os.path.join(base, "inv", "eps.ctr"))
+    np.testing.assert_allclose(res["sigmaa0"].real, f0.real, rtol=2e-6)
+    v00 = io.read_volt(os.path.join(base, "inv", "volt00.dat"))
+    np.testing.assert_allclose(np.exp(-res["sigmaa0"].real), v00.bet, rtol=1e-7)
+    inv.close()
+
+
+def test_gn_first_step_triangles_golden():
+    """DC_Problem/Complex (type-3 triangles, mixed boundaries): UP 1 stops on
+    the eps rule after 37 CG steps."""
+    import os
+    from crtomo_stable_b200 import inversion, io
+    base = os.path.join(os.path.dirname(__file__), "golden", "dc_problem_complex")
+    cfg = inversion.read_crtomo_cfg(os.path.join(base, "exe", "crtomo.cfg"))
+    mesh = io.read_elem(os.path.join(base, "grid", "elem.dat"))
+    enr = io.read_elec(os.path.join(base, "grid", "elec.dat"))
+    data = inversion.error_model(io.read_volt(os.path.join(base, "mod", "volt.dat")), cfg)
+    inv = inversion.Inversion(mesh, enr, data, cfg)
+    res = inv.first_step()
+    rows = read_inv_ctr_rows(os.path.join(base, "inv", "inv.ctr"))
+    it0 = [r for r in rows if r["kind"] == "IT"][0]
+    up1 = [r for r in rows if r["kind"] == "UP"][0]
+    assert abs(res["nrmsd0"] / it0["rms"] - 1) < 5e-4
+    assert res["ncg"] == up1["ncg"]
+    assert abs(res["nrmsd1"] / up1["rms"] - 1) < 5e-4
+    assert abs(res["bdpar"] / up1["step"] - 1) < 5e-3
+    assert abs(res["rough"] / up1["rough"] - 1) < 5e-4
+    inv.close()
+
+
+def test_dc_forward_triangles_golden():
+    """DC_Problem/DC: real path on triangles, IT 0 response of eps.ctr."""
+    import os
+    from crtomo_stable_b200 import inversion, io
+    base = os.path.join(os.path.dirname(__file__), "golden", "dc_problem")
+    cfg = inversion.read_crtomo_cfg(os.path.join(base, "exe", "crtomo.cfg"))
+    assert cfg.ldc
+    mesh = io.read_elem(os.path.join(base, "grid", "elem.dat"))
+    enr = io.read_elec(os.path.join(base, "grid", "elec.dat"))
+    data = inversion.error_model(io.read_volt(os.path.join(base, "mod", "volt.dat")), cfg)
+    inv = inversion.Inversion(mesh, enr, data, cfg)
+    _, sa = inv.ctx.forward(inv.start_model(), ldc=True)
+    f0 = read_eps_ctr_first_block(os.path.join(base, "inv", "eps.ctr"))
+    np.testing.assert_allclose(sa.real, f0.real, rtol=2e-6, atol=1e-6)
+    rows = read_inv_ctr_rows(os.path.join(base, "inv", "inv.ctr"))
+    it0 = [r for r in rows if r["kind"] == "IT"][0]
+    assert abs(inv.misfit(sa)[0] / it0["rms"] - 1) < 5e-4
+    inv.close()
+
+
+def test_pivot_error_code():
+    """A negative conductivity makes the system indefinite: the device
+    status word reports errnr 28 or 27 instead of producing numbers."""
+    from crtomo_stable_b200.lib import CRTError
+    case = load_forward_case("minimal")
+    ctx = _ctx(case)
+    sig = case["sigma"].copy()
+    sig[:] = -1.0
+    with pytest.raises(CRTError) as ei:
+        ctx.forward(sig, ldc=True)
+    assert ei.value.errnr in (27, 28)
+    ctx.close()
