@@ -1,0 +1,348 @@
+"""Gauss-Newton step benchmark (forward + Jacobian + inner CG to relative
+residual 1e-6) on the seeded synthetic 60k-triangle / 128-electrode
+configuration, through the C ABI of libcrt_b200.so.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line on rank 0.  `value` is the GN-step wall time with all
+inputs resident in device memory (CUDA events on the library's stream, max
+over ranks); `e2e` is the same step through crt_gn_step with host buffers
+(model upload, model / response / CG-history download inside the timed
+region).  Multi-GPU runs are independent replicas (the reference's hot path
+has no exchange step), so the per-step time is reported as the max over
+ranks with "scaling": "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GN-step wall time, learned-PCG/FP32-refined vs plain CG on B200 at rel-res 1e-6"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="C5")
+    ap.add_argument("--eps", type=float, default=1e-12, help="|r|^2 <= eps |r0|^2 (1e-12 = rel-res 1e-6)")
+    ap.add_argument("--ncgmax", type=int, default=20000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-s", type=float, default=20.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(pg, local, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def make_problem(config: str):
+    """Synthetic survey, its 'observed' data (the true model's response with
+    3 % + 0.1 mrad seeded Gaussian noise, computed on the device once) and
+    the homogeneous starting model."""
+    from crtomo_stable_b200 import regularization, synth
+    s = synth.CONFIGS[config]()
+    return s
+
+
+def setup_context(s, device: int):
+    from crtomo_stable_b200 import regularization
+    from crtomo_stable_b200.lib import Context
+    ctx = Context(s.mesh, s.enr, s.strnr, s.vnr, device=device)
+    # observed data: forward of the true model + seeded noise
+    _, sa_true = ctx.forward(s.sigma)
+    rng = np.random.default_rng(20261203)
+    mag = np.exp(-sa_true.real)
+    pha = -sa_true.imag
+    mag = mag * (1.0 + 0.03 * rng.standard_normal(len(mag)))
+    pha = pha + 1e-4 * rng.standard_normal(len(pha))
+    dat = -np.log(np.abs(mag)) - 1j * pha
+    stabw = 0.03 + 1e-4 / np.abs(mag)
+    wmatd = 1.0 / stabw ** 2
+    nb = regularization.nachbar(s.mesh)
+    sm = regularization.smatm_tri(s.mesh, nb, 1.0, 1.0)
+    ctx.set_regularizer(1, sm, nachbar=nb)
+    ctx.set_data(dat, wmatd)
+    rho0 = float(np.exp(np.mean(np.log(np.abs(1.0 / s.sigma)))))
+    par0 = np.full(s.mesh.elanz, np.log(1.0 / rho0) + 0j)
+    lam = float(max(s.mesh.elanz, len(s.strnr)))
+    return ctx, dat, wmatd, par0, lam, nb, sm
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def cpu_sample(s, ncg: int, budget_s: float, nthreads: int):
+    """The FP64 oracle (restatement of the Fortran path, OpenMP as the
+    reference) on a bounded sample of the same GN step, scaled to one step:
+      forward  : all wavenumbers x `le` source electrodes (of eanz) with the
+                 reference's OpenMP over wavenumbers, scaled by eanz / le;
+      Jacobian : `ni` readings (of nanz) on one thread, scaled by
+                 nanz / ni / threads (bsensi is OpenMP over readings);
+      CG       : two serial cjggra iterations on `nc` model cells (of manz),
+                 scaled by manz / nc and by the device's CG iteration count."""
+    from oracle.oracle import OracleCG, OracleProblem
+    from crtomo_stable_b200.lib import rwaven
+    m = s.mesh
+    L, N, E = len(s.enr), len(s.strnr), m.elanz
+    kwn, kwnwi = rwaven(m, s.enr, s.strnr, s.vnr)
+    K = len(kwn)
+    one = np.array([1], np.int32)
+    zero = np.array([0], np.int32)
+    le = 1
+    op_f = OracleProblem(m, s.enr[:le], one, zero, kwn=kwn, kwnwi=kwnwi)
+    t = time.perf_counter()
+    op_f.forward(s.sigma, nthreads=min(K, nthreads))
+    t_fwd = (time.perf_counter() - t) * (L / le)
+    ni = 4
+    op_j = OracleProblem(m, s.enr, s.strnr[:ni], s.vnr[:ni], kwn=kwn, kwnwi=kwnwi)
+    kp = np.zeros((m.sanz, L, K), np.complex128, order="F")
+    t = time.perf_counter()
+    op_j.bsensi(kp, s.sigma, np.ones(ni, np.complex128), nthreads=1)
+    t_sens = (time.perf_counter() - t) * N / ni / nthreads
+    nc = min(E, 2048)
+    J = np.full((N, nc), 1e-3 + 0j, order="F")
+    sm = np.zeros((nc, 4), order="F")
+    sm[:, 3] = 1.0
+    nb = np.zeros((nc, 4), np.int32, order="F")
+    cg = OracleCG(nc, N, 1, sm, nachbar=nb, nnb=3, wmatd=np.ones(N), lam=1.0, eps=0.0, ncgmax=2)
+    t = time.perf_counter()
+    cg.cjggra(J, np.ones(nc), np.ones(nc, np.complex128))
+    t_cg = (time.perf_counter() - t) / 2.0 * (E / nc) * ncg
+    total = t_fwd + t_sens + t_cg
+    sample = (f"oracle (FP64 C restatement, OpenMP like the reference): forward of all {K} wavenumbers x "
+              f"{le} of {L} source electrodes on {min(K, nthreads)} threads (x{L // le}); bsensi on {ni} of "
+              f"{N} readings on 1 thread (/{nthreads} threads); 2 serial cjggra iterations on {nc} of {E} "
+              f"cells (x{E / nc:.1f} cells, x{ncg} iterations)")
+    return total, dict(forward_s=t_fwd, jacobian_s=t_sens, cg_s=t_cg, sample=sample)
+
+
+def run_reference(args, ws, rank, pg):
+    """--impl reference: the oracle (FP64 restatement of the Fortran/OpenMP
+    path; the Fortran reference cannot be built here) on the host cores."""
+    if rank != 0:
+        return
+    s = make_problem(args.config)
+    nthreads = os.cpu_count() or 1
+    ncg_guess = int(os.environ.get("CRT_REF_NCG", "200"))
+    times = []
+    info = {}
+    for it in range(args.warmup + args.steps):
+        t, info = cpu_sample(s, ncg_guess, args.cpu_sample_s, nthreads)
+        if it >= args.warmup:
+            times.append(t)
+    v = float(np.median(times))
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
+            "config": {"workload": f"{args.config}: one GN step (forward+Jacobian+CG rel-res 1e-6)",
+                       "parallelism": "host cores"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "s", "cores": nthreads, "kind": "port",
+                             "sample": info.get("sample", "")},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    ws, rank, local, pg = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank, pg)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    from crtomo_stable_b200.lib import Context
+    s = make_problem(args.config)
+    ctx, dat, wmatd, par0, lam, nb, sm = setup_context(s, local)
+    prm = Context.params(lam, eps=args.eps, ncgmax=args.ncgmax)
+    ctx.set_model(par0)
+    ctx.model_backup(restore=False)
+    # warm-up (identical steps from the same starting model)
+    ncg = 0
+    for _ in range(args.warmup):
+        ctx.model_backup(restore=True)
+        ncg = ctx.gn_step_device(prm)
+    barrier(pg)
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = ctx.launch_count()
+    phase = np.zeros(7)
+    step_ms = []
+    for _ in range(args.steps):
+        ctx.model_backup(restore=True)
+        ncg = ctx.gn_step_device(prm)
+        t = ctx.timings()
+        step_ms.append(t["total"])
+        phase += np.array([t[k] for k in ("factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total")])
+    launches = ctx.launch_count() - launches0
+    barrier(pg)
+    clocks = sampler.stop()
+    t_step = max_over_ranks(pg, local, float(np.mean(step_ms)) / 1e3)
+    phase /= max(args.steps, 1)
+    # end to end through crt_gn_step with host buffers
+    import ctypes as C
+    e2e_ms = []
+    for _ in range(args.steps):
+        p = par0.copy()
+        t0 = time.perf_counter()
+        ctx.gn_step(prm, p)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    t_e2e = max_over_ranks(pg, local, float(np.mean(e2e_ms)) / 1e3)
+    E, N = s.mesh.elanz, len(s.strnr)
+    h2d = E * 16
+    d2h = E * 16 + N * 16 + (ncg + 1) * 8 + 8
+    # roofline of the dominant phase
+    peak_gbs, peak_kind = load_peaks()
+    names = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter"]
+    dom = names[int(np.argmax(phase[:6]))]
+    n, mb, L, K = s.mesh.sanz, s.mesh.mb, len(s.enr), ctx.kwn.size
+    roof = None
+    if dom == "cg_iter" and ncg > 0:
+        bytes_it = 2.0 * N * E * 16 + 6.0 * E * 16 + 3.0 * N * 16
+        ach = bytes_it * ncg / (phase[5] / 1e3) / 1e9
+        roof = {"kernel": "k_cg_jv + k_cg_jhv (J p, J^H W J p)", "bound": "hbm", "achieved": ach,
+                "peak": peak_gbs, "unit": "GB/s", "frac": ach / peak_gbs, "traffic": None,
+                "peak_source": peak_kind}
+    else:
+        # the band factorisation: FP64 FMA pipe, report its HBM side and flops
+        nsys = K * L
+        flops = nsys * 4.0 * n * mb * mb
+        bytes_f = nsys * (n * (mb + 1) * 16.0 * 2)
+        ach_gbs = bytes_f / (phase[0] / 1e3) / 1e9 if phase[0] > 0 else 0.0
+        roof = {"kernel": f"phase {dom}", "bound": "hbm", "achieved": ach_gbs, "peak": peak_gbs, "unit": "GB/s",
+                "frac": ach_gbs / peak_gbs, "traffic": None, "peak_source": peak_kind,
+                "fp64_tflops": flops / (phase[0] / 1e3) / 1e12 if phase[0] > 0 else None}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            v, info = cpu_sample(s, ncg, args.cpu_sample_s, os.cpu_count() or 1)
+            cpu = {"value": v, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port", "sample": info["sample"],
+                   "phases_s": {k: info[k] for k in ("forward_s", "jacobian_s", "cg_s")}}
+        except Exception as exc:  # the baseline must not hide the GPU number
+            cpu = {"value": None, "unit": "s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": t_step, "unit": "s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
+                "config": {"workload": f"{args.config}: {E} triangles, n={n}, mb={mb}, {L} electrodes, "
+                                       f"{N} readings, K={K}; one GN step from a homogeneous model "
+                                       f"(forward {K * L} band systems + Jacobian + CG to rel-res 1e-6)",
+                           "form": "plain FP64 (complex128) factorisation + diagonal-PCG",
+                           "cg_iterations": ncg, "lam": lam,
+                           "l2": "inputs larger than L2 (J alone is %.1f GB)" % (N * E * 16 / 1e9),
+                           "parallelism": f"replicas x{ws}"},
+                "phases_ms": dict(zip(names + ["total"], [float(x) for x in phase])),
+                "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(launches / args.steps)}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -77,7 +77,7 @@ struct crt_ctx {
     double* d_wd = nullptr;
     double *d_cgfac = nullptr, *d_cgres = nullptr, *d_bdpar = nullptr;
     cd *d_rhs = nullptr, *d_p = nullptr, *d_r = nullptr, *d_bvec = nullptr, *d_dpar = nullptr,
-       *d_ap = nullptr, *d_cgpart = nullptr, *d_par = nullptr;
+       *d_ap = nullptr, *d_cgpart = nullptr, *d_par = nullptr, *d_par_backup = nullptr;
     CGState* d_cgst = nullptr;
     int cg_nsplit = 1, cg_ncgmax_alloc = 0;
 };
@@ -162,6 +162,11 @@ int plan_chunk(crt_ctx* ctx, int nsys, size_t tsize)
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 2);
     int c = (int)std::max<size_t>(1, budget / std::max<size_t>(slot + (size_t)ctx->n * (tsize + 8), 1));
+    // one factor CTA per SM (the window fills the shared memory): round the
+    // chunk down to whole waves so no wave runs part-empty
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    if (c >= nsm && c < nsys) c = (c / nsm) * nsm;
     return std::min(c, nsys);
 }
 
@@ -204,7 +209,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_cgst};
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& e : ctx->ev)
@@ -948,6 +953,22 @@ extern "C" int32_t crt_get_model(crt_ctx* ctx, double* par)
     if (!ctx || !par || !ctx->d_par) return CRT_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
     CK(cudaMemcpyAsync(par, ctx->d_par, sizeof(cd) * ctx->E, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_model_backup(crt_ctx* ctx, int32_t restore)
+{
+    if (!ctx || !ctx->d_par) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->d_par_backup) {
+        if (restore) return set_err(ctx, CRT_ERR_ARG, "no model backup");
+        if (!dalloc(ctx, &ctx->d_par_backup, (size_t)ctx->E)) return CRT_ERR_ALLOC;
+    }
+    if (restore)
+        CK(cudaMemcpyAsync(ctx->d_par, ctx->d_par_backup, sizeof(cd) * ctx->E, cudaMemcpyDeviceToDevice, ctx->st));
+    else
+        CK(cudaMemcpyAsync(ctx->d_par_backup, ctx->d_par, sizeof(cd) * ctx->E, cudaMemcpyDeviceToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     return CRT_OK;
 }

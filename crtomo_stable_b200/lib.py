@@ -64,7 +64,7 @@ EXPORTS = [
     "crt_abi_version", "crt_create", "crt_destroy", "crt_last_error", "crt_rwaven", "crt_precal",
     "crt_forward", "crt_potentials", "crt_jacobian", "crt_set_jacobian", "crt_set_regularizer",
     "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
-    "crt_get_model", "crt_last_timings", "crt_launch_count", "crt_dmisft",
+    "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
 ]
 
 _LIB = None
@@ -114,6 +114,8 @@ def load(path: str = LIB_PATH):
     L.crt_set_model.restype = C.c_int32
     L.crt_get_model.argtypes = [vp, vp]
     L.crt_get_model.restype = C.c_int32
+    L.crt_model_backup.argtypes = [vp, C.c_int32]
+    L.crt_model_backup.restype = C.c_int32
     L.crt_gn_step_device.argtypes = [vp, P(crt_cg_params), i32p]
     L.crt_gn_step_device.restype = C.c_int32
     L.crt_last_timings.argtypes = [vp, f64p]
@@ -340,6 +342,9 @@ class Context:
         p = np.zeros(self.elanz, np.complex128)
         self._check(self.L.crt_get_model(self.h, _vp(p)), "crt_get_model")
         return p
+
+    def model_backup(self, restore=False):
+        self._check(self.L.crt_model_backup(self.h, int(bool(restore))), "crt_model_backup")
 
     def gn_step_device(self, prm):
         ncg = C.c_int32()

@@ -162,6 +162,10 @@ int32_t crt_gn_step(crt_ctx *ctx, const crt_cg_params *prm, double *par, double 
 int32_t crt_set_model(crt_ctx *ctx, const double *par);
 int32_t crt_gn_step_device(crt_ctx *ctx, const crt_cg_params *prm, int32_t *ncg);
 int32_t crt_get_model(crt_ctx *ctx, double *par);
+/* Device-side copy of the current model: save (0) to or restore (1) from a
+ * backup buffer, so repeated steps can restart from one model without host
+ * traffic. */
+int32_t crt_model_backup(crt_ctx *ctx, int32_t restore);
 
 /* Timings of the phases of the last crt_gn_step / crt_gn_step_device
  * (milliseconds, CUDA events on the context stream): [0] forward factor,
