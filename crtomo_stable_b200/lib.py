@@ -65,6 +65,7 @@ EXPORTS = [
     "crt_forward", "crt_potentials", "crt_jacobian", "crt_set_jacobian", "crt_set_regularizer",
     "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
+    "crt_voltages_noalloc",
 ]
 
 _LIB = None
@@ -124,6 +125,9 @@ def load(path: str = LIB_PATH):
     L.crt_launch_count.restype = C.c_int64
     L.crt_dmisft.argtypes = [C.c_int32, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, f64p, f64p, i32p]
     L.crt_dmisft.restype = C.c_double
+    L.crt_voltages_noalloc.argtypes = [vp, vp, vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                                       C.c_int32, C.c_int32, C.c_int32, vp, vp, vp, vp]
+    L.crt_voltages_noalloc.restype = C.c_int32
     _LIB = L
     return L
 

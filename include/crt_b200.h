@@ -176,6 +176,29 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
 /* Kernel launches enqueued by the context since creation. */
 int64_t crt_launch_count(const crt_ctx *ctx);
 
+/* Allocation-free voltages.  No counterpart in the reference: it exists for
+ * callers that cannot allocate device memory (all of their device memory is
+ * allocated up front, e.g. from their own pool or a framework allocator, or
+ * allocation is forbidden after start-up).  Computes what crt_forward's
+ * last step does -- rtrafo at the electrode nodes and bvolti (mode 0,
+ * sigmaa = -ln V) or bvolt (mode 1, sigmaa = kfak V) -- from a caller-held
+ * kpot.  Every pointer except `stream` is DEVICE memory: kpot complex
+ * kpot(sanz, eanz, kwnanz), kwnwi [kwnanz], enr [eanz] (1-based nodes),
+ * strnr / vnr [nanz], kfak [nanz] or NULL, outputs volt / sigmaa complex
+ * [nanz].  stream: a cudaStream_t (NULL = legacy default stream); the call
+ * synchronises it before returning the errnr (82 zero voltage, 46 / 29 bad
+ * electrode numbers, 3 bad arguments).  It calls no cudaMalloc / cudaFree:
+ * its scratch (the eanz x eanz table of electrode potentials) is a static
+ * device array for at most 512 electrodes (4 MiB per GPU, held until
+ * exit); eanz > 512 is rejected with errnr 3 and a message on stderr.  The
+ * first call on a device looks up the array's device address (once per
+ * device); make that first call before any stream capture.  All calls
+ * share the array, so calls that overlap on the GPU race. */
+int32_t crt_voltages_noalloc(const double *kpot, const double *kwnwi, const int32_t *enr,
+                             const int32_t *strnr, const int32_t *vnr, int32_t sanz, int32_t eanz,
+                             int32_t kwnanz, int32_t nanz, int32_t swrtr, int32_t ldc, int32_t mode,
+                             const double *kfak, double *volt, double *sigmaa, void *stream);
+
 /* Data misfit: src/dmisft.f90:73-137 with chkpo2 (FP64, host).
  * Returns nrmsd; betrms / pharms / npol optional. */
 double crt_dmisft(int32_t nanz, const double *dat, const double *sigmaa, const double *wmatd,
