@@ -1,0 +1,82 @@
+"""The C ABI library without a GPU: it loads, exports every entry point that
+include/crt_b200.h declares, and its host-only entry points agree with the
+oracle."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+from fixtures import GOLDEN
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    with open(os.path.join(ROOT, "include", "crt_b200.h")) as fh:
+        txt = fh.read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(crt_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_entry_point():
+    from crtomo_stable_b200 import lib
+    L = lib.load()
+    names = declared_functions()
+    assert len(names) >= 20
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(lib.EXPORTS) == set(names)
+    assert L.crt_abi_version() == 1
+
+
+def test_rwaven_host_entry_point_matches_oracle():
+    from crtomo_stable_b200 import io, lib
+    from oracle.oracle import OracleProblem
+    for name in ("minimal", "TestModInv", "dc_problem_complex"):
+        base = os.path.join(GOLDEN, name)
+        m = io.read_elem(os.path.join(base, "grid", "elem.dat"))
+        e = io.read_elec(os.path.join(base, "grid", "elec.dat"))
+        d = io.read_volt(os.path.join(base, "mod", "volt.dat"))
+        kwn, kwnwi = lib.rwaven(m, e, d.strnr, d.vnr)
+        op = OracleProblem(m, e, d.strnr, d.vnr)
+        np.testing.assert_allclose(kwn, op.kwn, rtol=1e-14)
+        np.testing.assert_allclose(kwnwi, op.kwnwi, rtol=1e-13)
+
+
+def test_dmisft_host_entry_point_matches_oracle():
+    from crtomo_stable_b200 import lib
+    from oracle import oracle
+    rng = np.random.default_rng(5)
+    n = 300
+    dat = rng.normal(size=n) + 1j * rng.uniform(-3.5, 3.5, n)
+    sa = dat + rng.normal(scale=0.1, size=n) + 1j * rng.normal(scale=0.5, size=n)
+    w = rng.uniform(10, 100, n)
+    wr = rng.uniform(10, 100, n)
+    wp = rng.uniform(10, 100, n)
+    for lfpi in (False, True):
+        a = lib.dmisft(dat, sa, w, wr, wp, lfpi=lfpi)
+        b = oracle.dmisft(dat, sa, w, wr, wp, lfpi=lfpi)
+        np.testing.assert_allclose(a[:3], b[:3], rtol=1e-13)
+        assert a[3] == b[3]
+
+
+def test_create_without_device_fails_loudly():
+    """No silent CPU path: without a CUDA device crt_create returns NULL
+    with an error number."""
+    import pytest
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a CUDA device is present")
+    except ImportError:
+        pass
+    from crtomo_stable_b200 import io, lib
+    from crtomo_stable_b200.lib import CRTError, Context
+    base = os.path.join(GOLDEN, "minimal")
+    m = io.read_elem(os.path.join(base, "grid", "elem.dat"))
+    e = io.read_elec(os.path.join(base, "grid", "elec.dat"))
+    d = io.read_volt(os.path.join(base, "mod", "volt.dat"))
+    with pytest.raises(CRTError) as ei:
+        Context(m, e, d.strnr, d.vnr)
+    assert ei.value.errnr == 200

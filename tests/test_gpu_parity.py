@@ -263,3 +263,19 @@ def test_pivot_error_code():
         ctx.forward(sig, ldc=True)
     assert ei.value.errnr in (27, 28)
     ctx.close()
+
+
+def test_crmod_driver_reproduces_recorded_volt_dat(tmp_path):
+    """CRMod replay on a copied tomodir (2D, fictitious sink): the written
+    volt.dat matches the recorded one."""
+    import os
+    import shutil
+    from crtomo_stable_b200 import crmod, io
+    src = os.path.join(os.path.dirname(__file__), "golden", "grid_decoupling")
+    dst = tmp_path / "td"
+    shutil.copytree(src, dst)
+    golden = io.read_volt(os.path.join(src, "mod", "volt.dat"))
+    crmod.run(str(dst / "exe"), verbose=False)
+    got = io.read_volt(str(dst / "mod" / "volt.dat"))
+    assert np.array_equal(got.strnr, golden.strnr) and np.array_equal(got.vnr, golden.vnr)
+    np.testing.assert_allclose(got.bet, golden.bet, rtol=2e-7)
