@@ -538,7 +538,11 @@ int run_forward(crt_ctx* ctx)
         A.fakws = ctx->d_fakws;
         A.status = ctx->d_status;
         CK(cudaEventRecord(ctx->ev[0], ctx->st));
-        launch_band_factor<T>(A, ctx->st);
+        {
+            const char* fv = std::getenv("CRT_B200_FACTOR");
+            const bool force_v0 = fv && std::strcmp(fv, "v0") == 0;
+            if (force_v0 || !launch_band_factor_blk<T>(A, ctx->st)) launch_band_factor<T>(A, ctx->st);
+        }
         ctx->launches++;
         if (int e = kernel_check(ctx, "band factor")) return e;
         CK(cudaEventRecord(ctx->ev[1], ctx->st));

@@ -45,6 +45,9 @@ struct SolveArgs {
 };
 
 template <typename T> void launch_band_factor(const BandArgs<T>& a, cudaStream_t st);
+// Panel-blocked variant; returns false when its window does not fit in
+// shared memory (the caller then uses launch_band_factor).
+template <typename T> bool launch_band_factor_blk(const BandArgs<T>& a, cudaStream_t st);
 // scratch: one n-vector per launched system (may alias the fused y workspace).
 template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st);
 template <typename T> size_t band_factor_smem(int W);

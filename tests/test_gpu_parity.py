@@ -279,3 +279,36 @@ def test_crmod_driver_reproduces_recorded_volt_dat(tmp_path):
     got = io.read_volt(str(dst / "mod" / "volt.dat"))
     assert np.array_equal(got.strnr, golden.strnr) and np.array_equal(got.vnr, golden.vnr)
     np.testing.assert_allclose(got.bet, golden.bet, rtol=2e-7)
+
+
+@pytest.mark.parametrize("name,ldc", [("minimal", False), ("TestModInv", False), ("TestModInv", True),
+                                      ("grid_decoupling", False)])
+def test_factor_variants_agree(name, ldc, monkeypatch):
+    """The panel-blocked factorisation and the rank-1 variant give the same
+    potentials (both are checked against the oracle elsewhere)."""
+    case = load_forward_case(name)
+    ctx = _ctx(case)
+    _, _, kp_blk = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+    monkeypatch.setenv("CRT_B200_FACTOR", "v0")
+    _, _, kp_v0 = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+    assert np.abs(kp_blk - kp_v0).max() <= RTOL_FP64 * np.abs(kp_v0).max()
+    ctx.close()
+
+
+@pytest.mark.parametrize("nz", [3, 6, 9])
+def test_forward_narrow_band_matches_oracle(nz):
+    """Half-bandwidths below and around the panel width (mb = nz + 1)."""
+    from crtomo_stable_b200 import synth
+    from crtomo_stable_b200.lib import Context
+    from oracle.oracle import OracleProblem
+    xs = np.arange(15, dtype=np.float64)
+    m = synth.structured_mesh(xs, synth.graded_depths(nz, 0.5, 1.2), triangles=True)
+    enr = synth.surface_electrodes(m, xs, np.arange(2.0, 12.0), nz)
+    s, v = synth.encode(synth.dipole_dipole(10, (1, 2), 4))
+    rng = np.random.default_rng(nz)
+    sig = synth.sigma_from(np.exp(rng.uniform(2, 6, m.elanz)), -rng.uniform(1, 20, m.elanz))
+    ctx = Context(m, enr, s, v)
+    _, _, kp = ctx.forward(sig, want_kpot=True)
+    kp_o = OracleProblem(m, enr, s, v).forward(sig)
+    assert np.abs(kp - kp_o).max() <= RTOL_FP64 * np.abs(kp_o).max()
+    ctx.close()
