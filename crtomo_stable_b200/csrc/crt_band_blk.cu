@@ -24,6 +24,10 @@
 namespace {
 
 constexpr int TILE = 4;
+// Tiles are stored 17 elements apart (16 used): consecutive tiles then start
+// in consecutive 16-byte bank groups, so the per-thread tile accesses of a
+// warp do not collide in shared memory.
+constexpr int TSTRIDE = 17;
 
 __device__ __forceinline__ int tile_base(int X, int Y) { return ((X * (X + 1)) >> 1) + Y; }
 
@@ -35,7 +39,7 @@ __device__ __forceinline__ int widx(int x, int y)
         x = y;
         y = t;
     }
-    return tile_base(x >> 2, y >> 2) * 16 + ((x & 3) << 2) + (y & 3);
+    return tile_base(x >> 2, y >> 2) * TSTRIDE + ((x & 3) << 2) + (y & 3);
 }
 
 template <typename T>
@@ -92,14 +96,18 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     const int n = A.n, mb = A.mb, W1 = A.W;    // W1 = mb + 1 (column stride of the HBM factor)
     const int NTR = Wn / TILE;
     const int NTT = NTR * (NTR + 1) / 2;
-    T* win = reinterpret_cast<T*>(smem_raw);              // NTT * 16
-    T* stage = win + (size_t)NTT * 16;                    // PB * W1
+    T* win = reinterpret_cast<T*>(smem_raw);              // NTT * TSTRIDE
+    T* stage = win + (size_t)NTT * TSTRIDE;               // PB * W1
     T* LD = stage + (size_t)PB * W1;                      // PB * PB
     T* bsl = LD + PB * PB;                                // Wn
     T* yP = bsl + Wn;                                     // PB
-    double* fakw = reinterpret_cast<double*>(yP + PB);    // Wn
+    T* LDi = yP + PB;                                     // PB reciprocal pivots
+    double* fakw = reinterpret_cast<double*>(LDi + PB);   // Wn
     double* fakN = fakw + Wn;                             // PB
     unsigned short* tXY = reinterpret_cast<unsigned short*>(fakN + PB);   // NTT
+    unsigned char* dfw = reinterpret_cast<unsigned char*>(tXY + NTT);     // Wn: Dirichlet flag per slot
+    __shared__ unsigned char dfN[PB];                                     // flags of the staged rows
+    __shared__ T colb[32];                                                // column broadcast of the block factor
     __shared__ int s_err;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -119,11 +127,12 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     const cd* bdir = (fuse && A.bdir) ? A.bdir + (size_t)b * n : nullptr;
     const int src = A.enr0[l];
 
-    for (int i = tid; i < NTT * 16; i += NT) win[i] = Sc<T>::zero();
+    for (int i = tid; i < NTT * TSTRIDE; i += NT) win[i] = Sc<T>::zero();
     for (int i = tid; i < PB * W1; i += NT) stage[i] = Sc<T>::zero();
     for (int i = tid; i < Wn; i += NT) {
         bsl[i] = Sc<T>::zero();
         fakw[i] = 0.0;
+        dfw[i] = 0;
     }
     for (int t = tid; t < NTT; t += NT) {
         // decode t -> (X, Y) with X >= Y
@@ -135,15 +144,17 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     if (tid == 0) s_err = 0;
     __syncthreads();
 
-    // Raw entries of rows [r0, r0 + PB) into stage[q][d] (all threads in the
-    // range [t0, NT) take part).
+    // Raw entries of rows [r0, r0 + PB) into stage[q][d].  The entries of
+    // consecutive rows are contiguous in the gather lists, so the threads in
+    // [t0, NT) take one entry each across all PB rows.
     auto stage_rows = [&](int r0, int t0) {
-        for (int q = 0; q < PB; ++q) {
-            const int r = r0 + q;
-            if (r >= n) break;
-            const int e1 = A.row_ptr[r + 1];
-            for (int e = A.row_ptr[r] + (tid - t0); e < e1; e += NT - t0)
-                stage[q * W1 + A.ent_d[e]] = assemble_entry_b(A, e, k, l);
+        if (r0 >= n) return;
+        const int rend = min(r0 + PB, n);
+        const int e0 = A.row_ptr[r0], e1 = A.row_ptr[rend];
+        for (int e = e0 + (tid - t0); e < e1; e += NT - t0) {
+            int q = 0;
+            while (q + 1 < rend - r0 && A.row_ptr[r0 + q + 1] <= e) ++q;
+            stage[q * W1 + A.ent_d[e]] = assemble_entry_b(A, e, k, l);
         }
     };
     // Scaling factors of the staged rows (threads q < PB).
@@ -151,8 +162,10 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
         if (tid < PB) {
             const int r = r0 + tid;
             double f = 1.0;
+            const unsigned char fl = (r < n) ? A.dflag[r] : 0;
+            dfN[tid] = fl;
             if (r < n) {
-                T raw = A.dflag[r] ? Sc<T>::one() : stage[tid * W1];
+                T raw = fl ? Sc<T>::one() : stage[tid * W1];
                 double d = Sc<T>::absval(raw);
                 if (!(d > 0.0)) s_err = CRT_ERR_ZERO_DIAG;
                 else f = 1.0 / sqrt(d);
@@ -166,28 +179,39 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     // c <= r is written (zero outside the band), pairs with later new rows
     // are written by those rows.
     auto scatter_rows = [&](int r0, int s_new, int wlo) {
-        for (int it = tid; it < PB * Wn; it += NT) {
-            const int q = it / Wn, y = it % Wn;
+        const int wm = wlo % Wn;
+#pragma unroll
+        for (int q = 0; q < PB; ++q) {
             const int r = r0 + q;
-            const int c = wlo + ((y - (wlo % Wn)) + Wn) % Wn;    // row held by slot y
-            if (c > r) continue;
-            const int d = r - c;
-            T v = Sc<T>::zero();
-            if (r < n) {
-                if (d == 0) {
-                    T raw = A.dflag[r] ? Sc<T>::one() : stage[q * W1];
-                    v = Sc<T>::normalise(raw, Sc<T>::absval(raw));
-                } else if (d <= mb && !A.dflag[r] && !A.dflag[c]) {
-                    const double fc = (c >= r0) ? fakN[c - r0] : fakw[y];
-                    v = scale(stage[q * W1 + d], fakN[q] * fc);
+            const bool dr = dfN[q] != 0;
+            for (int y = tid; y < Wn; y += NT) {
+                int off = y - wm;
+                if (off < 0) off += Wn;
+                const int c = wlo + off;                      // row held by slot y
+                if (c > r) continue;
+                const int d = r - c;
+                T v = Sc<T>::zero();
+                if (r < n) {
+                    if (d == 0) {
+                        T raw = dr ? Sc<T>::one() : stage[q * W1];
+                        v = Sc<T>::normalise(raw, Sc<T>::absval(raw));
+                    } else if (d <= mb) {
+                        const bool newc = c >= r0;
+                        const bool dc = newc ? (dfN[c - r0] != 0) : (dfw[y] != 0);
+                        if (!dr && !dc) {
+                            const double fc = newc ? fakN[c - r0] : fakw[y];
+                            v = scale(stage[q * W1 + d], fakN[q] * fc);
+                        }
+                    }
                 }
+                win[widx(s_new + q, y)] = v;
             }
-            win[widx(s_new + q, y)] = v;
         }
         __syncthreads();
         if (tid < PB) {
             const int r = r0 + tid;
             fakw[s_new + tid] = fakN[tid];
+            dfw[s_new + tid] = dfN[tid];
             T bb = Sc<T>::zero();
             if (fuse && r < n) bb = scale(rhs_entry_b<T>(r, src, A.lsink, A.nsink0, A.dflag, A.dval, bdir), fakN[tid]);
             bsl[s_new + tid] = bb;
@@ -211,6 +235,8 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
         const int rnew0 = i0 + Wn;
         // ---- phase 1: diagonal block (warp 0) | next rows (warps 1..)
         if (warp == 0) {
+            // lane j holds row j of the diagonal block; column t is broadcast
+            // through colb[] (shared) once it is final
             T a[PB];
             T bj = Sc<T>::zero();
             const int j = lane;
@@ -225,26 +251,31 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
 #pragma unroll
             for (int t = 0; t < PB; ++t) {
                 if (t >= np_) break;
-                // pivot of column t lives in lane t
-                T piv = shfl_T<T>(a[t], t);
-                if (lane == 0 && Sc<T>::bad_pivot(piv)) s_err = CRT_ERR_PIVOT;
-                const T ltt = Sc<T>::sqrt_(piv);
-                if (j == t) a[t] = ltt;
-                if (j > t && j < np_) a[t] = Sc<T>::div(a[t], ltt);
-                // forward substitution of the panel's right-hand side
-                T yt = Sc<T>::zero();
-                if (fuse) {
-                    T bt = shfl_T<T>(bj, t);
-                    yt = Sc<T>::div(bt, ltt);
-                    if (j == t) bj = yt;
+                if (j == t) {
+                    const T piv = a[t];
+                    if (Sc<T>::bad_pivot(piv)) s_err = CRT_ERR_PIVOT;
+                    const T ltt = Sc<T>::sqrt_fast(piv);
+                    const T inv = Sc<T>::recip(ltt);
+                    a[t] = ltt;
+                    LDi[t] = inv;
+                    if (fuse) {
+                        bj = Sc<T>::mul(bj, inv);
+                        yP[t] = bj;
+                    }
                 }
-                // rank-1 update of the remaining block columns
+                __syncwarp();
+                const T inv = LDi[t];
+                if (j > t && j < np_) {
+                    a[t] = Sc<T>::mul(a[t], inv);
+                    colb[j] = a[t];
+                }
+                __syncwarp();
+                // rank-1 update of the remaining block columns and the RHS
 #pragma unroll
-                for (int t2 = t + 1; t2 < PB; ++t2) {
-                    const T l2 = shfl_T<T>(a[t], t2);    // L(t2, t)
-                    if (j >= t2 && j < np_ && t2 < np_) a[t2] -= Sc<T>::mul(a[t], l2);
-                }
-                if (fuse && j > t && j < np_) bj -= Sc<T>::mul(a[t], yt);
+                for (int t2 = t + 1; t2 < PB; ++t2)
+                    if (j >= t2 && j < np_) a[t2] -= Sc<T>::mul(a[t], colb[t2]);
+                if (fuse && j > t && j < np_) bj -= Sc<T>::mul(a[t], yP[t]);
+                __syncwarp();
             }
             if (j < np_) {
 #pragma unroll
@@ -254,20 +285,19 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
                         if (j - t <= mb) Lc[(size_t)(i0 + t) * W1 + (j - t)] = a[t];
                     }
                 }
-                if (fuse) {
-                    yP[j] = bj;
-                    yv[i0 + j] = bj;
-                }
+                if (fuse) yv[i0 + j] = yP[j];
             }
         } else {
             stage_rows(rnew0, 32);
         }
         __syncthreads();
+        // PROBE0
         if (s_err) break;
         // ---- phase 2: rows below the panel solve against the block
         stage_fak(rnew0);
         for (int x = tid; x < Wn; x += NT) {
-            const int dx = (x - s0 + Wn) % Wn;
+            int dx = x - s0;
+            if (dx < 0) dx += Wn;
             if (dx < PB) continue;                         // panel slot
             const int r = i0 + dx;
             if (r >= n || dx > mb + PB - 1) continue;
@@ -281,7 +311,7 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
                 T s = lx[t];
 #pragma unroll
                 for (int t2 = 0; t2 < t; ++t2) s -= Sc<T>::mul(lx[t2], LD[t * PB + t2]);
-                lx[t] = Sc<T>::div(s, LD[t * PB + t]);
+                lx[t] = Sc<T>::mul(s, LDi[t]);
                 if (fuse) bx -= Sc<T>::mul(lx[t], yP[t]);
                 win[widx(x, s0 + t)] = lx[t];
                 const int d = r - (i0 + t);
@@ -290,6 +320,7 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
             if (fuse) bsl[x] = bx;
         }
         __syncthreads();
+        // PROBE1
         // ---- phase 3: trailing update T_xy -= L_x L_y^T on 4 x 4 tiles
         {
             const int P0 = s0 >> 2, P1 = (s0 + PB) >> 2;   // panel tile rows [P0, P1)
@@ -297,7 +328,7 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
                 const int X = tXY[tt] >> 8, Y = tXY[tt] & 0xff;
                 if ((X >= P0 && X < P1) || (Y >= P0 && Y < P1)) continue;
                 T acc[16];
-                T* tp = win + tt * 16;
+                T* tp = win + tt * TSTRIDE;
 #pragma unroll
                 for (int q = 0; q < 16; ++q) acc[q] = tp[q];
                 for (int t = 0; t < np_; ++t) {
@@ -324,9 +355,11 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
             }
         }
         __syncthreads();
+        // PROBE2
         // ---- phase 4: the staged rows enter the freed panel slots
         scatter_rows(rnew0, s0, i0 + PB);
         __syncthreads();
+        // PROBE3
     }
     if (tid == 0) A.status[sys] = s_err;
 }
@@ -338,8 +371,8 @@ static size_t blk_smem(int mb, int* Wn_out)
 {
     const int Wn = ((mb + PB + PB - 1) / PB) * PB;
     const int NTR = Wn / 4, NTT = NTR * (NTR + 1) / 2;
-    size_t s = (size_t)NTT * 16 * sizeof(T) + (size_t)PB * (mb + 1) * sizeof(T) + (size_t)PB * PB * sizeof(T) +
-               (size_t)Wn * sizeof(T) + PB * sizeof(T) + (size_t)Wn * 8 + PB * 8 + (size_t)NTT * 2 + 64;
+    size_t s = (size_t)NTT * TSTRIDE * sizeof(T) + (size_t)PB * (mb + 1) * sizeof(T) + (size_t)PB * PB * sizeof(T) +
+               (size_t)Wn * sizeof(T) + 2 * PB * sizeof(T) + (size_t)Wn * 8 + PB * 8 + (size_t)NTT * 2 + Wn + 64;
     *Wn_out = Wn;
     return s;
 }

@@ -62,9 +62,11 @@ template <> struct Sc<double> {
     static CRT_HD double absval(double a) { return a; }       // scaldc tests a <= 0
     static CRT_HD double normalise(double a, double) { return 1.0; }
     static CRT_HD double sqrt_(double a) { return sqrt(a); }
+    static CRT_HD double sqrt_fast(double a) { return sqrt(a); }
     static CRT_HD bool bad_pivot(double s) { return !(s > 0.0); }
     static CRT_HD double mul(double a, double b) { return a * b; }
     static CRT_HD double div(double a, double b) { return a / b; }
+    static CRT_HD double recip(double a) { return 1.0 / a; }
     static CRT_HD cd to_cd(double a) { return cd{a, 0.0}; }
 };
 template <> struct Sc<cd> {
@@ -74,9 +76,26 @@ template <> struct Sc<cd> {
     static CRT_HD double absval(cd a) { return cabs_(a); }
     static CRT_HD cd normalise(cd a, double d) { return cd{a.x / d, a.y / d}; }
     static CRT_HD cd sqrt_(cd a) { return csqrt_p(a); }
-    static CRT_HD bool bad_pivot(cd s) { return !(cabs_(s) > 0.0); }
+    // principal root with |z| = sqrt(x^2 + y^2) (no overflow scaling; the
+    // pivots of the scaled systems are of order one)
+    static CRT_HD cd sqrt_fast(cd z)
+    {
+        const double r = sqrt(z.x * z.x + z.y * z.y);
+        if (r == 0.0) return cd{0.0, 0.0};
+        const double t = sqrt(0.5 * (r + fabs(z.x)));
+        const double h = 0.5 / t;
+        if (z.x >= 0.0) return cd{t, z.y * h};
+        return cd{fabs(z.y) * h, copysign(t, z.y)};
+    }
+    static CRT_HD bool bad_pivot(cd s) { return !(s.x * s.x + s.y * s.y > 0.0); }
     static CRT_HD cd mul(cd a, cd b) { return a * b; }
     static CRT_HD cd div(cd a, cd b) { return cdiv(a, b); }
+    // 1/a = conj(a) / |a|^2 (the pivots are of order one after scaling)
+    static CRT_HD cd recip(cd a)
+    {
+        const double s = 1.0 / (a.x * a.x + a.y * a.y);
+        return cd{a.x * s, -a.y * s};
+    }
     static CRT_HD cd to_cd(cd a) { return a; }
 };
 

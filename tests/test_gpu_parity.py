@@ -22,6 +22,22 @@ def _ctx(case):
                    lsink=c["cfg"].lsink, nsink=c["cfg"].nsink)
 
 
+def _singular(case):
+    """2D (k = 0) with no-flow on every boundary and no mixed segment: the
+    Neumann Laplacian is singular and each potential field is defined up to
+    an additive constant that depends on the rounding of the last pivot.
+    Voltages and sensitivities (differences) do not see it."""
+    m = case["mesh"]
+    return case["cfg"].swrtr == 0 and not np.any(np.asarray(m.typ) == 11)
+
+
+def _kpot_diff(a, b, singular):
+    if singular:
+        a = a - a.mean(axis=0, keepdims=True)
+        b = b - b.mean(axis=0, keepdims=True)
+    return np.abs(a - b).max()
+
+
 def _oracle(case):
     from oracle.oracle import OracleProblem
     c = case
@@ -64,7 +80,7 @@ def test_forward_matches_oracle_and_golden(name):
     volt_g, sa_g, kpot_g = ctx.forward(case["sigma"], mode=1, want_kpot=True)
     kpot_o = op.forward(case["sigma"], nthreads=4)
     scale = np.abs(kpot_o).max()
-    assert np.abs(kpot_g - kpot_o).max() <= RTOL_FP64 * scale
+    assert _kpot_diff(kpot_g, kpot_o, _singular(case)) <= RTOL_FP64 * scale
     hp = op.rtrafo(kpot_o)
     volt_o, _ = op.bvolt(hp)
     np.testing.assert_allclose(volt_g, volt_o, rtol=RTOL_FP64, atol=RTOL_FP64 * np.abs(volt_o).max())
@@ -291,7 +307,7 @@ def test_factor_variants_agree(name, ldc, monkeypatch):
     _, _, kp_blk = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
     monkeypatch.setenv("CRT_B200_FACTOR", "v0")
     _, _, kp_v0 = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
-    assert np.abs(kp_blk - kp_v0).max() <= RTOL_FP64 * np.abs(kp_v0).max()
+    assert _kpot_diff(kp_blk, kp_v0, _singular(case)) <= RTOL_FP64 * np.abs(kp_v0).max()
     ctx.close()
 
 
