@@ -138,10 +138,10 @@ def make_problem(config: str):
     return s
 
 
-def setup_context(s, device: int):
+def setup_context(s, device: int, precision: int = 0):
     from crtomo_stable_b200 import regularization
     from crtomo_stable_b200.lib import Context
-    ctx = Context(s.mesh, s.enr, s.strnr, s.vnr, device=device)
+    ctx = Context(s.mesh, s.enr, s.strnr, s.vnr, device=device, precision=precision)
     # observed data: forward of the true model + seeded noise
     _, sa_true = ctx.forward(s.sigma)
     rng = np.random.default_rng(20261203)
@@ -254,67 +254,72 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
-    from crtomo_stable_b200.lib import Context
+    from crtomo_stable_b200.lib import PREC_FP64, PREC_MIXED, Context
     s = make_problem(args.config)
-    ctx, dat, wmatd, par0, lam, nb, sm = setup_context(s, local)
-    prm = Context.params(lam, eps=args.eps, ncgmax=args.ncgmax)
-    ctx.set_model(par0)
-    ctx.model_backup(restore=False)
-    # warm-up (identical steps from the same starting model)
-    ncg = 0
-    for _ in range(args.warmup):
-        ctx.model_backup(restore=True)
-        ncg = ctx.gn_step_device(prm)
-    barrier(pg)
-    sampler = ClockSampler(local)
-    sampler.start()
-    launches0 = ctx.launch_count()
-    phase = np.zeros(7)
-    step_ms = []
-    for _ in range(args.steps):
-        ctx.model_backup(restore=True)
-        ncg = ctx.gn_step_device(prm)
-        t = ctx.timings()
-        step_ms.append(t["total"])
-        phase += np.array([t[k] for k in ("factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total")])
-    launches = ctx.launch_count() - launches0
-    barrier(pg)
-    clocks = sampler.stop()
-    t_step = max_over_ranks(pg, local, float(np.mean(step_ms)) / 1e3)
-    phase /= max(args.steps, 1)
-    # end to end through crt_gn_step with host buffers
-    import ctypes as C
-    e2e_ms = []
-    for _ in range(args.steps):
-        p = par0.copy()
-        t0 = time.perf_counter()
-        ctx.gn_step(prm, p)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-    t_e2e = max_over_ranks(pg, local, float(np.mean(e2e_ms)) / 1e3)
     E, N = s.mesh.elanz, len(s.strnr)
+    n, mb, L = s.mesh.sanz, s.mesh.mb, len(s.enr)
+    names = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter"]
+
+    def run_form(precision, steps, warmup, e2e_steps, sample_clocks):
+        ctx, dat, wmatd, par0, lam, nb, sm = setup_context(s, local, precision)
+        prm = Context.params(lam, eps=args.eps, ncgmax=args.ncgmax)
+        ctx.set_model(par0)
+        ctx.model_backup(restore=False)
+        ncg = 0
+        for _ in range(warmup):     # identical steps from the same starting model
+            ctx.model_backup(restore=True)
+            ncg = ctx.gn_step_device(prm)
+        barrier(pg)
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.start()
+        launches0 = ctx.launch_count()
+        phase = np.zeros(7)
+        step_ms = []
+        for _ in range(steps):
+            ctx.model_backup(restore=True)
+            ncg = ctx.gn_step_device(prm)
+            t = ctx.timings()
+            step_ms.append(t["total"])
+            phase += np.array([t[k] for k in names + ["total"]])
+        launches = (ctx.launch_count() - launches0) // max(steps, 1)
+        barrier(pg)
+        clocks = sampler.stop() if sampler else None
+        t_step = max_over_ranks(pg, local, float(np.mean(step_ms)) / 1e3)
+        phase /= max(steps, 1)
+        e2e_ms = []
+        for _ in range(e2e_steps):   # through crt_gn_step with host buffers
+            p = par0.copy()
+            t0 = time.perf_counter()
+            ctx.gn_step(prm, p)
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        t_e2e = max_over_ranks(pg, local, float(np.mean(e2e_ms)) / 1e3) if e2e_ms else None
+        K = ctx.kwn.size
+        ctx.close()
+        return dict(t=t_step, phase=phase, ncg=ncg, launches=int(launches), clocks=clocks, e2e=t_e2e, lam=lam, K=K)
+
+    mixed = run_form(PREC_MIXED, args.steps, args.warmup, args.steps, True)
+    plain = run_form(PREC_FP64, max(1, args.steps // 3), max(1, args.warmup // 3), 0, False)
+    t_step, phase, ncg, K = mixed["t"], mixed["phase"], mixed["ncg"], mixed["K"]
     h2d = E * 16
     d2h = E * 16 + N * 16 + (ncg + 1) * 8 + 8
     # roofline of the dominant phase
     peak_gbs, peak_kind = load_peaks()
-    names = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter"]
     dom = names[int(np.argmax(phase[:6]))]
-    n, mb, L, K = s.mesh.sanz, s.mesh.mb, len(s.enr), ctx.kwn.size
     roof = None
     if dom == "cg_iter" and ncg > 0:
-        bytes_it = 2.0 * N * E * 16 + 6.0 * E * 16 + 3.0 * N * 16
+        jbytes = 8  # complex64 Jacobian in the mixed form
+        bytes_it = 2.0 * N * E * jbytes + 6.0 * E * 16 + 3.0 * N * 16
         ach = bytes_it * ncg / (phase[5] / 1e3) / 1e9
-        roof = {"kernel": "k_cg_jv + k_cg_jhv (J p, J^H W J p)", "bound": "hbm", "achieved": ach,
+        roof = {"kernel": "k_cg_jv + k_cg_jhv (J p, J^H W J p; complex64 J)", "bound": "hbm", "achieved": ach,
                 "peak": peak_gbs, "unit": "GB/s", "frac": ach / peak_gbs, "traffic": None,
-                "peak_source": peak_kind}
+                "peak_source": peak_kind, "algorithmic_bytes_per_iteration": bytes_it}
     else:
-        # the band factorisation: FP64 FMA pipe, report its HBM side and flops
         nsys = K * L
-        flops = nsys * 4.0 * n * mb * mb
-        bytes_f = nsys * (n * (mb + 1) * 16.0 * 2)
+        bytes_f = nsys * (n * (mb + 1) * 16.0)
         ach_gbs = bytes_f / (phase[0] / 1e3) / 1e9 if phase[0] > 0 else 0.0
         roof = {"kernel": f"phase {dom}", "bound": "hbm", "achieved": ach_gbs, "peak": peak_gbs, "unit": "GB/s",
-                "frac": ach_gbs / peak_gbs, "traffic": None, "peak_source": peak_kind,
-                "fp64_tflops": flops / (phase[0] / 1e3) / 1e12 if phase[0] > 0 else None}
+                "frac": ach_gbs / peak_gbs, "traffic": None, "peak_source": peak_kind}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
@@ -326,19 +331,22 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": t_step, "unit": "s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
-                "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128/c64", "data": "synthetic (seeded)",
                 "config": {"workload": f"{args.config}: {E} triangles, n={n}, mb={mb}, {L} electrodes, "
                                        f"{N} readings, K={K}; one GN step from a homogeneous model "
                                        f"(forward {K * L} band systems + Jacobian + CG to rel-res 1e-6)",
-                           "form": "plain FP64 (complex128) factorisation + diagonal-PCG",
-                           "cg_iterations": ncg, "lam": lam,
-                           "l2": "inputs larger than L2 (J alone is %.1f GB)" % (N * E * 16 / 1e9),
+                           "form": "mixed: complex64 Jacobian storage, FP64 accumulation and dots; "
+                                   "complex128 band factorisation; diagonal-PCG",
+                           "cg_iterations": ncg, "lam": mixed["lam"],
+                           "l2": "inputs larger than L2 (J alone is %.1f GB in complex64)" % (N * E * 8 / 1e9),
                            "parallelism": f"replicas x{ws}"},
                 "phases_ms": dict(zip(names + ["total"], [float(x) for x in phase])),
-                "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "roofline": roof, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(launches / args.steps)}
+                "plain_fp64": {"value": plain["t"], "unit": "s", "cg_iterations": plain["ncg"],
+                               "phases_ms": dict(zip(names + ["total"], [float(x) for x in plain["phase"]]))},
+                "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "roofline": roof, "cpu_baseline": cpu, "clocks": mixed["clocks"],
+                "gpu_launches": mixed["launches"]}
         print(json.dumps(line), flush=True)
-    ctx.close()
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

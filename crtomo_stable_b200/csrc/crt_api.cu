@@ -80,6 +80,7 @@ struct crt_ctx {
        *d_ap = nullptr, *d_cgpart = nullptr, *d_par = nullptr, *d_par_backup = nullptr;
     CGState* d_cgst = nullptr;
     int cg_nsplit = 1, cg_ncgmax_alloc = 0;
+    int prec = CRT_PREC_FP64;
 };
 
 namespace {
@@ -151,6 +152,13 @@ int kernel_check(crt_ctx* ctx, const char* what)
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(ctx, CRT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
     return CRT_OK;
+}
+
+size_t sens_elem_bytes(const crt_ctx* ctx, bool real)
+{
+    const bool f32 = ctx->prec == CRT_PREC_MIXED;
+    if (real) return f32 ? sizeof(float) : sizeof(double);
+    return f32 ? sizeof(cf) : sizeof(cd);
 }
 
 // Workspace chunk: how many band systems are factored per launch.
@@ -229,8 +237,9 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
     };
     if (errnr) *errnr = CRT_OK;
     if (!mesh || !sv) return fail(nullptr, CRT_ERR_ARG);
-    if (precision != CRT_PREC_FP64) return fail(nullptr, CRT_ERR_UNSUPPORTED);
+    if (precision != CRT_PREC_FP64 && precision != CRT_PREC_MIXED) return fail(nullptr, CRT_ERR_UNSUPPORTED);
     crt_ctx* ctx = new crt_ctx();
+    ctx->prec = precision;
     ctx->device = device;
     ctx->pi = std::acos(-1.0);
     if (!ck(ctx, cudaSetDevice(device), "cudaSetDevice")) return fail(ctx, CRT_ERR_CUDA);
@@ -698,7 +707,7 @@ int jacobian_device(crt_ctx* ctx, int mode, const double* strom_h)
     if (!ctx->d_sens || ctx->sens_real != (int)real) {
         if (ctx->d_sens) cudaFree(ctx->d_sens);
         ctx->d_sens = nullptr;
-        CK(cudaMalloc(&ctx->d_sens, ne * (real ? sizeof(double) : sizeof(cd))));
+        CK(cudaMalloc(&ctx->d_sens, ne * sens_elem_bytes(ctx, real)));
         ctx->sens_real = real;
     }
     if (strom_h && mode == 2) {
@@ -731,6 +740,7 @@ int jacobian_device(crt_ctx* ctx, int mode, const double* strom_h)
     S.volt = ctx->d_volt;
     S.strom = (mode == 2 && strom_h) ? ctx->d_strom : nullptr;
     S.sens = ctx->d_sens;
+    S.out_prec = ctx->prec == CRT_PREC_MIXED;
     if (kc < ctx->K) {
         if (!ctx->d_part_sens && !dalloc(ctx, &ctx->d_part_sens, ne)) return CRT_ERR_ALLOC;
     }
@@ -756,9 +766,17 @@ extern "C" int32_t crt_jacobian(crt_ctx* ctx, int32_t mode, const double* strom,
     int e = jacobian_device(ctx, mode, strom);
     if (e) return e;
     if (sens) {
-        const size_t bytes = (size_t)ctx->E * ctx->N * (mode == 1 ? sizeof(double) : sizeof(cd));
-        CK(cudaMemcpyAsync(sens, ctx->d_sens, bytes, cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        const size_t ne = (size_t)ctx->E * ctx->N;
+        const size_t vals = ne * (mode == 1 ? 1 : 2);
+        if (ctx->prec == CRT_PREC_MIXED) {
+            std::vector<float> h(vals);
+            CK(cudaMemcpyAsync(h.data(), ctx->d_sens, vals * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            for (size_t q = 0; q < vals; ++q) sens[q] = (double)h[q];
+        } else {
+            CK(cudaMemcpyAsync(sens, ctx->d_sens, vals * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+        }
     }
     return CRT_OK;
 }
@@ -768,15 +786,23 @@ extern "C" int32_t crt_set_jacobian(crt_ctx* ctx, int32_t real, const double* se
     if (!ctx || !sens) return CRT_ERR_ARG;
     CK(cudaSetDevice(ctx->device));
     const size_t ne = (size_t)ctx->E * ctx->N;
-    const size_t bytes = ne * (real ? sizeof(double) : sizeof(cd));
+    const size_t vals = ne * (real ? 1 : 2);
+    const size_t bytes = ne * sens_elem_bytes(ctx, real != 0);
     if (!ctx->d_sens || ctx->sens_real != (real != 0)) {
         if (ctx->d_sens) cudaFree(ctx->d_sens);
         ctx->d_sens = nullptr;
         CK(cudaMalloc(&ctx->d_sens, bytes));
         ctx->sens_real = real != 0;
     }
-    CK(cudaMemcpyAsync(ctx->d_sens, sens, bytes, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    if (ctx->prec == CRT_PREC_MIXED) {
+        std::vector<float> h(vals);
+        for (size_t q = 0; q < vals; ++q) h[q] = (float)sens[q];
+        CK(cudaMemcpyAsync(ctx->d_sens, h.data(), bytes, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    } else {
+        CK(cudaMemcpyAsync(ctx->d_sens, sens, bytes, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
     ctx->have_sens = 1;
     return CRT_OK;
 }
@@ -849,7 +875,7 @@ int ensure_cg_buffers(crt_ctx* ctx, int ncgmax)
 {
     const int M = ctx->E, N = ctx->N;
     if (!ctx->d_cgfac) {
-        int nsplit = std::max(1, std::min(64, (148 * 4) / std::max(1, (N + 255) / 256)));
+        int nsplit = std::max(1, std::min(64, (148 * 8) / std::max(1, (N + 255) / 256)));
         ctx->cg_nsplit = nsplit;
         bool ok = dalloc(ctx, &ctx->d_cgfac, (size_t)M) && dalloc(ctx, &ctx->d_rhs, (size_t)M) &&
                   dalloc(ctx, &ctx->d_p, (size_t)M) && dalloc(ctx, &ctx->d_r, (size_t)M) &&
@@ -872,6 +898,7 @@ CGArgs make_cg_args(crt_ctx* ctx, const crt_cg_params* prm)
     a.M = ctx->E;
     a.N = ctx->N;
     a.jmode = prm->ldc ? 1 : (prm->lfpi ? 2 : 0);
+    a.jprec = ctx->prec == CRT_PREC_MIXED ? 1 : 0;
     a.ltri = ctx->ltri;
     a.nx = ctx->nx;
     a.nnb = ctx->nnb;

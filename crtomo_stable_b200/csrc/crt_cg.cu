@@ -23,12 +23,24 @@ namespace {
 
 constexpr int VEC_NT = 1024;
 
+// J(i, e) as an FP64 complex value: JP selects the storage precision,
+// JM the Jacobian form (complex, real sensdc, real part of complex).
+template <int JP, int JM>
 __device__ __forceinline__ cd jval(const CGArgs& A, int e, int i)
 {
     const size_t o = (size_t)e * A.N + i;
-    if (A.jmode == 1) return cd{static_cast<const double*>(A.J)[o], 0.0};
-    cd v = static_cast<const cd*>(A.J)[o];
-    if (A.jmode == 2) v.y = 0.0;
+    if (JM == 1) {
+        if (JP == 0) return cd{static_cast<const double*>(A.J)[o], 0.0};
+        return cd{(double)static_cast<const float*>(A.J)[o], 0.0};
+    }
+    cd v;
+    if (JP == 0) {
+        v = static_cast<const cd*>(A.J)[o];
+    } else {
+        const cf f = static_cast<const cf*>(A.J)[o];
+        v = cd{(double)f.x, (double)f.y};
+    }
+    if (JM == 2) v.y = 0.0;
     return v;
 }
 
@@ -88,6 +100,13 @@ __device__ __forceinline__ double warp_sum(double v)
     return v;
 }
 
+// Butterfly reduction: every lane receives the warp's total.
+__device__ __forceinline__ double warp_allsum(double v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Deterministic block sum (all threads receive the total).
 template <int NT>
 __device__ double block_sum(double v, double* red)
@@ -108,6 +127,7 @@ __device__ double block_sum(double v, double* red)
 }
 
 // cgfac and scaled RHS, one warp per model cell.
+template <int JP, int JM>
 __global__ void k_cg_setup(CGArgs A, const cd* dat, const cd* sigmaa, const cd* par)
 {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -115,7 +135,7 @@ __global__ void k_cg_setup(CGArgs A, const cd* dat, const cd* sigmaa, const cd* 
     const int e = warp;
     double an = 0.0, arx = 0.0, ary = 0.0;
     for (int i = lane; i < A.N; i += 32) {
-        const cd j = jval(A, e, i);
+        const cd j = jval<JP, JM>(A, e, i);
         const double w = A.wd[i];
         const cd rd = dat[i] - sigmaa[i];
         an += (j.x * j.x + j.y * j.y) * w;
@@ -186,20 +206,42 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A)
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) A.p[e] = A.r[e] + A.p[e] * beta;
 }
 
-// ap partial sums over a column range: thread per reading.
-__global__ void k_cg_jv(CGArgs A)
+// ap partial sums over a column range: thread per reading.  The block stages
+// p o cgfac for JV_CHUNK columns in shared memory and keeps JV_UNROLL
+// independent J loads in flight per thread.
+constexpr int JV_NT = 256, JV_CHUNK = 256, JV_UNROLL = 8;
+
+template <int JP, int JM>
+__global__ void __launch_bounds__(JV_NT) k_cg_jv(CGArgs A)
 {
+    __shared__ cd pcs[JV_CHUNK];
     if (A.st->done) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= A.N) return;
+    const int i = blockIdx.x * JV_NT + threadIdx.x;
+    const bool valid = i < A.N;
     const int split = blockIdx.y;
     const int per = (A.M + A.nsplit - 1) / A.nsplit;
     const int e0 = split * per, e1 = min(A.M, e0 + per);
     cd acc{0.0, 0.0};
-    for (int e = e0; e < e1; ++e) acc += (A.p[e] * jval(A, e, i)) * A.cgfac[e];
-    A.part[(size_t)split * A.N + i] = acc;
+    for (int eb = e0; eb < e1; eb += JV_CHUNK) {
+        const int ne = min(JV_CHUNK, e1 - eb);
+        __syncthreads();
+        if ((int)threadIdx.x < ne) pcs[threadIdx.x] = A.p[eb + threadIdx.x] * A.cgfac[eb + threadIdx.x];
+        __syncthreads();
+        if (!valid) continue;
+        int u = 0;
+        for (; u + JV_UNROLL <= ne; u += JV_UNROLL) {
+            cd jv[JV_UNROLL];
+#pragma unroll
+            for (int q = 0; q < JV_UNROLL; ++q) jv[q] = jval<JP, JM>(A, eb + u + q, i);
+#pragma unroll
+            for (int q = 0; q < JV_UNROLL; ++q) acc += pcs[u + q] * jv[q];
+        }
+        for (; u < ne; ++u) acc += pcs[u] * jval<JP, JM>(A, eb + u, i);
+    }
+    if (valid) A.part[(size_t)split * A.N + i] = acc;
 }
 
+// ap = sum of the partial sums; what the transposed product needs is w o ap.
 __global__ void k_cg_jv_reduce(CGArgs A)
 {
     if (A.st->done) return;
@@ -207,26 +249,55 @@ __global__ void k_cg_jv_reduce(CGArgs A)
     if (i >= A.N) return;
     cd acc{0.0, 0.0};
     for (int s = 0; s < A.nsplit; ++s) acc += A.part[(size_t)s * A.N + i];
-    A.ap[i] = acc;
+    A.ap[i] = acc * A.wd[i];
 }
 
-// b_e = (sum_i conj(J_ie) w_i ap_i + lam (R (cgfac o p))_e) * cgfac_e
+// b_e = (sum_i conj(J_ie) (w o ap)_i + lam (R (cgfac o p))_e) * cgfac_e,
+// one warp per JH_COLS columns sharing the loads of w o ap.
+constexpr int JH_COLS = 4;
+
+template <int JP, int JM>
 __global__ void k_cg_jhv(CGArgs A)
 {
     if (A.st->done) return;
-    const int e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (e >= A.M) return;
-    double ax = 0.0, ay = 0.0;
-    for (int i = lane; i < A.N; i += 32) {
-        const cd t = (conj(jval(A, e, i)) * A.wd[i]) * A.ap[i];
-        ax += t.x;
-        ay += t.y;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    const int ebase = gw * JH_COLS;
+    if (ebase >= A.M) return;
+    const int nc = min(JH_COLS, A.M - ebase);
+    double ax[JH_COLS], ay[JH_COLS];
+#pragma unroll
+    for (int c = 0; c < JH_COLS; ++c) {
+        ax[c] = 0.0;
+        ay[c] = 0.0;
     }
-    ax = warp_sum(ax);
-    ay = warp_sum(ay);
-    if (lane == 0) {
+    for (int i = lane; i < A.N; i += 32) {
+        const cd w = A.ap[i];
+        cd jv[JH_COLS];
+#pragma unroll
+        for (int c = 0; c < JH_COLS; ++c) jv[c] = (c < nc) ? jval<JP, JM>(A, ebase + c, i) : cd{0.0, 0.0};
+#pragma unroll
+        for (int c = 0; c < JH_COLS; ++c) {
+            const cd t = conj(jv[c]) * w;
+            ax[c] += t.x;
+            ay[c] += t.y;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < JH_COLS; ++c) {
+        ax[c] = warp_allsum(ax[c]);
+        ay[c] = warp_allsum(ay[c]);
+    }
+    if (lane < nc) {
+        double bx = 0.0, by = 0.0;
+#pragma unroll
+        for (int c = 0; c < JH_COLS; ++c)
+            if (c == lane) {
+                bx = ax[c];
+                by = ay[c];
+            }
+        const int e = ebase + lane;
         const cd rp = reg_apply_cg(A, A.p, e);
-        const cd b = cd{ax, ay} + rp * A.lam;
+        const cd b = cd{bx, by} + rp * A.lam;
         A.bvec[e] = b * A.cgfac[e];
     }
 }
@@ -283,10 +354,23 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_finish(CGArgs A, int lfpi, double
 
 }  // namespace
 
+#define CRT_CG_DISPATCH(KERNEL, GRID, BLOCK, STREAM, ...)                          \
+    do {                                                                           \
+        const int key = a.jprec * 3 + a.jmode;                                     \
+        switch (key) {                                                             \
+        case 0: KERNEL<0, 0><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;      \
+        case 1: KERNEL<0, 1><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;      \
+        case 2: KERNEL<0, 2><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;      \
+        case 3: KERNEL<1, 0><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;      \
+        case 4: KERNEL<1, 1><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;      \
+        default: KERNEL<1, 2><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;     \
+        }                                                                          \
+    } while (0)
+
 void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s)
 {
     const int threads = 256, warps = threads / 32;
-    k_cg_setup<<<(a.M + warps - 1) / warps, threads, 0, s>>>(a, dat, sigmaa, par);
+    CRT_CG_DISPATCH(k_cg_setup, (a.M + warps - 1) / warps, threads, s, a, dat, sigmaa, par);
 }
 
 void launch_cg_init(const CGArgs& a, cudaStream_t s) { k_cg_init<<<1, VEC_NT, 0, s>>>(a); }
@@ -294,13 +378,14 @@ void launch_cg_init(const CGArgs& a, cudaStream_t s) { k_cg_init<<<1, VEC_NT, 0,
 void launch_cg_iterations(const CGArgs& a, int iters, cudaStream_t s)
 {
     const int nt = 256;
-    dim3 gjv((a.N + nt - 1) / nt, a.nsplit);
+    dim3 gjv((a.N + JV_NT - 1) / JV_NT, a.nsplit);
     const int warps = nt / 32;
     for (int it = 0; it < iters; ++it) {
         k_cg_begin<<<1, VEC_NT, 0, s>>>(a);
-        k_cg_jv<<<gjv, nt, 0, s>>>(a);
+        CRT_CG_DISPATCH(k_cg_jv, gjv, JV_NT, s, a);
         k_cg_jv_reduce<<<(a.N + nt - 1) / nt, nt, 0, s>>>(a);
-        k_cg_jhv<<<(a.M + warps - 1) / warps, nt, 0, s>>>(a);
+        const int cols_per_block = warps * JH_COLS;
+        CRT_CG_DISPATCH(k_cg_jhv, (a.M + cols_per_block - 1) / cols_per_block, nt, s, a);
         k_cg_end<<<1, VEC_NT, 0, s>>>(a);
     }
 }

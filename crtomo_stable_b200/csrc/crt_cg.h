@@ -15,16 +15,17 @@ struct CGState {
 struct CGArgs {
     int M, N;             // manz, nanz
     int jmode;            // 0 complex J (cjggra), 1 real sensdc (ldc), 2 real part of complex J (lfpi)
+    int jprec;            // storage of J: 0 FP64 (cd / double), 1 FP32 (cf / float); arithmetic is FP64
     int ltri, nx, nnb;    // regulariser: 0 five-point (smatm(M,3)), else neighbour list (smatm(M,nnb+1))
     int ncgmax;
     double lam, eps;
-    const void* J;        // [M][N]: cd (jmode 0/2) or double (jmode 1)
+    const void* J;        // [M][N]: cd / cf (jmode 0/2) or double / float (jmode 1)
     const double* wd;     // [N] wmatd * wdfak
     const double* smatm;  // Fortran smatm(M, ncol)
     const int* nachbar;   // Fortran nachbar(M, nnb+1), 1-based, 0 = none
     double* cgfac;        // [M]
     cd* rhs;              // [M] scaled right-hand side (bvec on entry to cjg)
-    cd *p, *r, *bvec, *dpar, *ap;   // [M],[M],[M],[M],[N]
+    cd *p, *r, *bvec, *dpar, *ap;   // [M],[M],[M],[M],[N]: ap holds w o (J p) after the reduction
     cd* part;             // [nsplit][N] partial J*p sums
     int nsplit;
     double* cgres;        // [ncgmax + 2]

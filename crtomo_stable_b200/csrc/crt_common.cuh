@@ -15,6 +15,11 @@ struct __align__(16) cd {
     double x, y;
 };
 
+// complex64 storage element (the Jacobian in the mixed-precision form)
+struct __align__(8) cf {
+    float x, y;
+};
+
 CRT_HD cd mk(double x, double y) { return cd{x, y}; }
 CRT_HD cd operator+(cd a, cd b) { return cd{a.x + b.x, a.y + b.y}; }
 CRT_HD cd operator-(cd a, cd b) { return cd{a.x - b.x, a.y - b.y}; }

@@ -93,23 +93,30 @@ __global__ void __launch_bounds__(NT) k_sens(SensArgs A)
                 A.part[o] = Sc<T>::to_cd(acc);
                 continue;
             }
-            // final scaling
+            // final scaling (FP64), stored in the requested precision
+            cd res;
             if (A.mode == 0) {
                 cd d = Sc<T>::to_cd(acc);
                 if (A.swrtr != 0) d = d / A.pi;
-                cd r = (d * sig) / A.volt[i];
-                reinterpret_cast<cd*>(A.sens)[o] = r;
+                res = (d * sig) / A.volt[i];
             } else if (A.mode == 1) {
                 double d = Sc<T>::to_cd(acc).x;
                 if (A.swrtr != 0) d = d / A.pi;
                 cd q = sig / A.volt[i];
-                reinterpret_cast<double*>(A.sens)[o] = d * q.x;
+                res = cd{d * q.x, 0.0};
             } else {
                 cd d = Sc<T>::to_cd(acc);
                 const double st = A.strom ? A.strom[i] : 1.0;
                 if (A.swrtr == 0) d = d * st;
                 else d = d * (st / A.pi);
-                reinterpret_cast<cd*>(A.sens)[o] = -d;
+                res = -d;
+            }
+            if (A.mode == 1) {
+                if (A.out_prec) reinterpret_cast<float*>(A.sens)[o] = (float)res.x;
+                else reinterpret_cast<double*>(A.sens)[o] = res.x;
+            } else {
+                if (A.out_prec) reinterpret_cast<cf*>(A.sens)[o] = cf{(float)res.x, (float)res.y};
+                else reinterpret_cast<cd*>(A.sens)[o] = res;
             }
         }
     }

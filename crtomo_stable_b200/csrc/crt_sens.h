@@ -7,6 +7,7 @@ struct SensArgs {
     int n, E, L, K, N, nmn, maxnodes, swrtr;
     int mode;              // 0 bsensi (complex, sigma/V), 1 bsendc (real), 2 bsens (CRMod, -strom)
     int kchunk;            // wavenumbers staged per pass
+    int out_prec;          // 0: store sens in FP64 (cd / double), 1: in FP32 (cf / float)
     double pi;
     const cd* kpt;         // [K][n][L]
     const double* elbg;    // [K][E][nmn]
@@ -17,7 +18,7 @@ struct SensArgs {
     const cd* sigma;       // [E]
     const cd* volt;        // [N]
     const double* strom;   // [N] or NULL
-    void* sens;            // [E][N]: cd for modes 0/2, double for mode 1
+    void* sens;            // [E][N]: complex for modes 0/2, real for mode 1 (precision out_prec)
     cd* part;              // [E][N] partial sums when K is split (kchunk < K)
 };
 

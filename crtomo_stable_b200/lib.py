@@ -179,13 +179,17 @@ def _mesh_struct(mesh, keep):
     return m
 
 
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
 class Context:
     """One device context: a mesh, its electrodes, measurements and
     wavenumbers (the state the Fortran modules hold across calls).
     """
 
     def __init__(self, mesh, enr, strnr, vnr, kwn=None, kwnwi=None, swrtr=1, lsink=False, nsink=0,
-                 rwdnr=None, rwd=None, device=0, elbg=None, relbg=None, kg=None, lsytop=False):
+                 rwdnr=None, rwd=None, device=0, elbg=None, relbg=None, kg=None, lsytop=False, precision=0):
         self.L = load()
         self._keep = []
         self.mesh = mesh
@@ -217,7 +221,7 @@ class Context:
             s.rwd = C.cast(C.c_void_p(self._rw[1].ctypes.data), f64p)
         s.lsytop = int(bool(lsytop))
         err = C.c_int32()
-        h = self.L.crt_create(int(device), C.byref(m), C.byref(s), 0, C.byref(err))
+        h = self.L.crt_create(int(device), C.byref(m), C.byref(s), int(precision), C.byref(err))
         if not h:
             raise CRTError(err.value, "crt_create failed")
         self.h = C.c_void_p(h)

@@ -73,8 +73,15 @@ typedef struct {
     double step;       /* model step length applied by crt_update */
 } crt_cg_params;
 
-/* Precision of the band factorisations and solves. */
+/* Precision forms.
+ * CRT_PREC_FP64:  everything in FP64 / complex128 (the reference's arithmetic).
+ * CRT_PREC_MIXED: the Jacobian is stored in FP32 / complex64 (computed in
+ *                 FP64, rounded on store) and the CG accumulates in FP64;
+ *                 band factorisations run in complex64 with FP64 iterative
+ *                 refinement of the potentials where enabled.  Dot products,
+ *                 quadrature weights, misfit and model update stay FP64. */
 #define CRT_PREC_FP64 0
+#define CRT_PREC_MIXED 1
 
 /* Creates a context on `device`: uploads the mesh, builds the gather lists
  * of the streamed assembly, and evaluates precal on the device unless the

@@ -328,3 +328,56 @@ def test_forward_narrow_band_matches_oracle(nz):
     kp_o = OracleProblem(m, enr, s, v).forward(sig)
     assert np.abs(kp - kp_o).max() <= RTOL_FP64 * np.abs(kp_o).max()
     ctx.close()
+
+
+def test_mixed_form_jacobian_is_fp64_rounded_to_fp32():
+    """CRT_PREC_MIXED stores the Jacobian in complex64: every entry equals the
+    FP64 oracle's to float32 rounding (relative 2**-24 of the entry, plus the
+    FP64 tolerance of the column)."""
+    from crtomo_stable_b200.lib import PREC_MIXED, Context
+    case = load_forward_case("TestModInv")
+    c = case["cfg"]
+    ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, precision=PREC_MIXED)
+    op = _oracle(case)
+    ctx.forward(case["sigma"])
+    J_g = ctx.jacobian(mode=0)
+    kp = op.forward(case["sigma"], nthreads=4)
+    volt_o, _ = op.bvolti(op.rtrafo(kp))
+    J_o = op.bsensi(kp, case["sigma"], volt_o, nthreads=4)
+    colmax = np.abs(J_o).max(axis=0, keepdims=True) + 1e-300
+    err = np.abs(J_g - J_o)
+    assert (err <= 1.2e-7 * np.abs(J_o) + RTOL_SENS * colmax).all()
+    ctx.close()
+
+
+def test_mixed_form_cg_converges_to_the_same_update():
+    """The CG on the complex64-stored Jacobian (FP64 accumulation and dot
+    products) reaches relative residual 1e-6 and an update within 1e-4 of
+    the FP64 oracle's."""
+    from crtomo_stable_b200 import regularization
+    from crtomo_stable_b200.lib import PREC_MIXED, Context
+    from oracle.oracle import OracleCG
+    case = load_forward_case("minimal")
+    m = case["mesh"]
+    d = case["volt"]
+    ctx = Context(m, case["enr"], d.strnr, d.vnr, precision=PREC_MIXED)
+    op = _oracle(case)
+    dat = -np.log(d.bet) - 1j * d.pha / 1e3
+    wmatd = 1.0 / (1e-2 + 1e-3 / d.bet) ** 2
+    sig = np.full(m.elanz, 0.01 + 0j)
+    ctx.forward(sig)
+    ctx.jacobian(mode=0, copy=False)
+    kp = op.forward(sig, nthreads=4)
+    volt_o, sa_o = op.bvolti(op.rtrafo(kp))
+    J_o = op.bsensi(kp, sig, volt_o, nthreads=4)
+    nb = regularization.nachbar(m)
+    sm = regularization.smatm_tri(m, nb, 10.0, 1.0)
+    ctx.set_regularizer(1, sm, nachbar=nb)
+    ctx.set_data(dat, wmatd)
+    par = np.log(sig)
+    ref = OracleCG(m.elanz, len(dat), 1, sm, nachbar=nb, nnb=m.maxnodes, wmatd=wmatd, lam=300.0, eps=1e-12,
+                   ncgmax=2000).update(J_o, dat, sa_o, par, 1.0)
+    got = ctx.update(Context.params(300.0, eps=1e-12, ncgmax=2000), par, sigmaa=sa_o)
+    assert got["ncg"] < 2000
+    np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-4, atol=1e-4 * np.abs(ref["dpar"]).max())
+    ctx.close()
