@@ -254,7 +254,7 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
-    from crtomo_stable_b200.lib import PREC_FP64, PREC_MIXED, Context
+    from crtomo_stable_b200.lib import PREC_FP64, PREC_MIXED, PRECOND_BLOCK, PRECOND_JACOBI, Context
     s = make_problem(args.config)
     E, N = s.mesh.elanz, len(s.strnr)
     n, mb, L = s.mesh.sanz, s.mesh.mb, len(s.enr)
@@ -262,7 +262,8 @@ def main():
 
     def run_form(precision, steps, warmup, e2e_steps, sample_clocks):
         ctx, dat, wmatd, par0, lam, nb, sm = setup_context(s, local, precision)
-        prm = Context.params(lam, eps=args.eps, ncgmax=args.ncgmax)
+        pc = PRECOND_BLOCK if precision == PREC_MIXED else PRECOND_JACOBI
+        prm = Context.params(lam, eps=args.eps, ncgmax=args.ncgmax, precond=pc)
         ctx.set_model(par0)
         ctx.model_backup(restore=False)
         ncg = 0
@@ -295,8 +296,10 @@ def main():
             e2e_ms.append((time.perf_counter() - t0) * 1e3)
         t_e2e = max_over_ranks(pg, local, float(np.mean(e2e_ms)) / 1e3) if e2e_ms else None
         K = ctx.kwn.size
+        form, blk, bw = ctx.cg_info()
         ctx.close()
-        return dict(t=t_step, phase=phase, ncg=ncg, launches=int(launches), clocks=clocks, e2e=t_e2e, lam=lam, K=K)
+        return dict(t=t_step, phase=phase, ncg=ncg, launches=int(launches), clocks=clocks, e2e=t_e2e, lam=lam, K=K,
+                    cg_form=form, cg_block=blk, cg_bw=bw)
 
     mixed = run_form(PREC_MIXED, args.steps, args.warmup, args.steps, True)
     plain = run_form(PREC_FP64, max(1, args.steps // 3), max(1, args.warmup // 3), 0, False)
@@ -336,7 +339,10 @@ def main():
                                        f"{N} readings, K={K}; one GN step from a homogeneous model "
                                        f"(forward {K * L} band systems + Jacobian + CG to rel-res 1e-6)",
                            "form": "mixed: complex64 Jacobian storage, FP64 accumulation and dots; "
-                                   "complex128 band factorisation; diagonal-PCG",
+                                   "complex128 band factorisation; CG preconditioned by cgfac and the "
+                                   "block-tridiagonal S^-1 (FP32) of the sparse part" if mixed["cg_form"] == 1 else
+                                   "mixed: complex64 Jacobian storage; diagonal-PCG (block preconditioner unavailable)",
+                           "cg_block": mixed["cg_block"], "cg_bandwidth": mixed["cg_bw"],
                            "cg_iterations": ncg, "lam": mixed["lam"],
                            "l2": "inputs larger than L2 (J alone is %.1f GB in complex64)" % (N * E * 8 / 1e9),
                            "parallelism": f"replicas x{ws}"},

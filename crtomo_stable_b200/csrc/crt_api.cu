@@ -17,6 +17,7 @@
 #include "crt_common.cuh"
 #include "crt_sens.h"
 #include "crt_setup.h"
+#include "crt_spc.h"
 #include "crt_volt.h"
 
 template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>&, T*, cudaStream_t);
@@ -80,6 +81,11 @@ struct crt_ctx {
        *d_ap = nullptr, *d_cgpart = nullptr, *d_par = nullptr, *d_par_backup = nullptr;
     CGState* d_cgst = nullptr;
     int cg_nsplit = 1, cg_ncgmax_alloc = 0;
+    // block preconditioner of the CG (built with the regulariser)
+    SpcPlan spc;
+    std::string spc_why;
+    cd *d_z = nullptr, *d_rold = nullptr;
+    int cg_form = 0;      // form of the last CG: 0 Jacobi (cgfac), 1 block preconditioner
     int prec = CRT_PREC_FP64;
 };
 
@@ -187,6 +193,15 @@ extern "C" const char* crt_last_error(const crt_ctx* ctx) { return ctx ? ctx->er
 
 extern "C" int64_t crt_launch_count(const crt_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+extern "C" int32_t crt_cg_info(const crt_ctx* ctx, int32_t* form, int32_t* block, int32_t* bandwidth)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    if (form) *form = ctx->cg_form;
+    if (block) *block = ctx->spc.ok ? ctx->spc.B : 0;
+    if (bandwidth) *bandwidth = ctx->spc.bw;
+    return CRT_OK;
+}
+
 extern "C" int32_t crt_last_timings(const crt_ctx* ctx, double* ms7)
 {
     if (!ctx || !ms7) return CRT_ERR_ARG;
@@ -217,9 +232,10 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst};
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    spc_plan_free(ctx->spc);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -853,6 +869,9 @@ extern "C" int32_t crt_set_regularizer(crt_ctx* ctx, int32_t ltri, int32_t nx, i
             return CRT_ERR_ALLOC;
     }
     CK(cudaStreamSynchronize(ctx->st));
+    ctx->spc_why.clear();
+    if (int e = spc_plan_build(ctx->spc, M, ltri, nx, nnb, smatm, nachbar, ctx->spc_why))
+        return set_err(ctx, e, "block preconditioner set-up failed");
     return CRT_OK;
 }
 
@@ -882,7 +901,8 @@ int ensure_cg_buffers(crt_ctx* ctx, int ncgmax)
                   dalloc(ctx, &ctx->d_bvec, (size_t)M) && dalloc(ctx, &ctx->d_dpar, (size_t)M) &&
                   dalloc(ctx, &ctx->d_ap, (size_t)N) && dalloc(ctx, &ctx->d_cgpart, (size_t)nsplit * N) &&
                   dalloc(ctx, &ctx->d_cgst, (size_t)1) && dalloc(ctx, &ctx->d_bdpar, (size_t)1) &&
-                  dalloc(ctx, &ctx->d_par, (size_t)M);
+                  dalloc(ctx, &ctx->d_par, (size_t)M) && dalloc(ctx, &ctx->d_z, (size_t)M) &&
+                  dalloc(ctx, &ctx->d_rold, (size_t)M);
         if (!ok) return CRT_ERR_ALLOC;
     }
     if (ctx->cg_ncgmax_alloc < ncgmax + 2) {
@@ -920,6 +940,9 @@ CGArgs make_cg_args(crt_ctx* ctx, const crt_cg_params* prm)
     a.nsplit = ctx->cg_nsplit;
     a.cgres = ctx->d_cgres;
     a.st = ctx->d_cgst;
+    a.pc = 0;
+    a.z = ctx->d_z;
+    a.rold = ctx->d_rold;
     return a;
 }
 
@@ -934,8 +957,21 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
     CGArgs a = make_cg_args(ctx, prm);
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
     launch_cg_setup(a, ctx->d_dat, d_sigmaa, ctx->d_par, ctx->st);
+    ctx->launches += 1;
+    if (prm->precond == CRT_PRECOND_BLOCK && ctx->spc.ok) {
+        // S from cgfac and lam, factored once per update; a breakdown
+        // (non-positive pivot) falls back to the Jacobi form
+        launch_spc_factor(ctx->spc, ctx->d_cgfac, ctx->d_smatm, prm->lam, ctx->st);
+        ctx->launches += 3 + (ctx->spc.nb > 1 ? 1 : 0);
+        int flag = 0;
+        CK(cudaMemcpyAsync(&flag, ctx->spc.d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (int e = kernel_check(ctx, "block preconditioner factor")) return e;
+        a.pc = flag == 0 ? 1 : 0;
+    }
+    ctx->cg_form = a.pc;
     launch_cg_init(a, ctx->st);
-    ctx->launches += 2;
+    ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     if (int e = kernel_check(ctx, "cg setup")) return e;
     // iterate in batches; the device-side stop flag makes surplus launches no-ops
@@ -944,8 +980,8 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
     const int batch = 16;
     while (done_iters < prm->ncgmax) {
         int it = std::min(batch, prm->ncgmax - done_iters);
-        launch_cg_iterations(a, it, ctx->st);
-        ctx->launches += 5 * it;
+        launch_cg_iterations(a, it, &ctx->spc, ctx->st);
+        ctx->launches += (a.pc ? 7 : 5) * it;
         done_iters += it;
         CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));

@@ -18,6 +18,7 @@
 // improvement) use the same kernels with zero imaginary parts, which keeps
 // the real arithmetic of cjggdc exact.
 #include "crt_cg.h"
+#include "crt_spc.h"
 
 namespace {
 
@@ -158,10 +159,14 @@ __global__ void k_cg_setup(CGArgs A, const cd* dat, const cd* sigmaa, const cd* 
 
 __global__ void __launch_bounds__(VEC_NT) k_cg_init(CGArgs A)
 {
+    // cjggdc (src/cg_mod.f90:106-199) iterates on the real part of the
+    // right-hand side (DC) or on its imaginary part (final phase improvement)
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
         A.dpar[e] = cd{0.0, 0.0};
-        A.r[e] = A.rhs[e];
+        const cd b = A.rhs[e];
+        A.r[e] = A.jmode == 0 ? b : cd{A.jmode == 1 ? b.x : b.y, 0.0};
         A.p[e] = cd{0.0, 0.0};
+        if (A.pc) A.rold[e] = cd{0.0, 0.0};
     }
     if (threadIdx.x == 0) {
         CGState s{};
@@ -199,11 +204,63 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A)
             st->ncg = k - 1;
         }
         st->dr = dr;
+        st->num = dr;
     }
     __syncthreads();
     if (s_stop) return;
     beta = (k == 1) ? 0.0 : st->beta;
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) A.p[e] = A.r[e] + A.p[e] * beta;
+}
+
+// Preconditioned head: z = S^-1 r is in A.z.  The stop rule is the
+// reference's (|r|^2 against eps |r0|^2); beta is the flexible
+// (Polak-Ribiere) Re(z^H (r - r_old)) / Re(z_old^H r_old), alpha's
+// numerator Re(r^H z).
+__global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A)
+{
+    __shared__ double red[33];
+    __shared__ int s_stop;
+    __shared__ double s_beta;
+    CGState* st = A.st;
+    if (st->done) return;
+    double v = 0.0, g = 0.0, go = 0.0;
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
+        const cd r = A.r[e], z = A.z[e], ro = A.rold[e];
+        v += cabs2(r);
+        g += r.x * z.x + r.y * z.y;
+        go += ro.x * z.x + ro.y * z.y;
+    }
+    const double dr = block_sum<VEC_NT>(v, red);
+    const double gam = block_sum<VEC_NT>(g, red);
+    const double gold = block_sum<VEC_NT>(go, red);
+    const int k = st->k;
+    if (threadIdx.x == 0) {
+        s_stop = 0;
+        double beta = 0.0;
+        if (k == 1) {
+            st->dr0 = dr * A.eps;
+            if (A.jmode != 0 && dr <= st->dr0) s_stop = 1;
+        } else {
+            if (dr <= st->dr0) s_stop = 1;
+            beta = (gam - gold) / st->gam;
+        }
+        if (s_stop) {
+            st->done = 1;
+            st->ncg = k - 1;
+        }
+        st->dr = dr;
+        st->beta = beta;
+        st->gam = gam;
+        st->num = gam;
+        s_beta = beta;
+    }
+    __syncthreads();
+    if (s_stop) return;
+    const double beta = s_beta;
+    for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
+        A.p[e] = A.z[e] + A.p[e] * beta;
+        A.rold[e] = A.r[e];
+    }
 }
 
 // ap partial sums over a column range: thread per reading.  The block stages
@@ -314,7 +371,7 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_end(CGArgs A)
         v += pp.x * bb.x + pp.y * bb.y;
     }
     const double dr1 = block_sum<VEC_NT>(v, red);
-    const double alpha = st->dr / dr1;
+    const double alpha = st->num / dr1;
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
         A.dpar[e] = A.dpar[e] + A.p[e] * alpha;
         A.r[e] = A.r[e] - A.bvec[e] * alpha;
@@ -375,13 +432,18 @@ void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd*
 
 void launch_cg_init(const CGArgs& a, cudaStream_t s) { k_cg_init<<<1, VEC_NT, 0, s>>>(a); }
 
-void launch_cg_iterations(const CGArgs& a, int iters, cudaStream_t s)
+void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, cudaStream_t s)
 {
     const int nt = 256;
     dim3 gjv((a.N + JV_NT - 1) / JV_NT, a.nsplit);
     const int warps = nt / 32;
     for (int it = 0; it < iters; ++it) {
-        k_cg_begin<<<1, VEC_NT, 0, s>>>(a);
+        if (a.pc) {
+            launch_spc_apply(*spc, a.r, a.z, a.st, s);
+            k_cg_begin_pc<<<1, VEC_NT, 0, s>>>(a);
+        } else {
+            k_cg_begin<<<1, VEC_NT, 0, s>>>(a);
+        }
         CRT_CG_DISPATCH(k_cg_jv, gjv, JV_NT, s, a);
         k_cg_jv_reduce<<<(a.N + nt - 1) / nt, nt, 0, s>>>(a);
         const int cols_per_block = warps * JH_COLS;

@@ -6,6 +6,8 @@
 // Device-resident CG control block (cjgmod scalars).
 struct CGState {
     double dr, dr0, dr1, alpha, beta;
+    double gam;   // preconditioned form: Re(r^H z) of the last iteration head
+    double num;   // numerator of alpha: dr (cjggra) or Re(r^H z) (preconditioned)
     int k;        // next iteration number (1-based)
     int done;     // 1 once the stop rule fired or ncgmax was reached
     int ncg;      // completed iterations
@@ -30,14 +32,21 @@ struct CGArgs {
     int nsplit;
     double* cgres;        // [ncgmax + 2]
     CGState* st;
+    // preconditioned form (pc = 1): z = S^-1 r from the block preconditioner,
+    // rold the residual of the previous head (flexible beta)
+    int pc;
+    cd *z, *rold;
 };
+
+struct SpcPlan;
 
 // update.f90:63-231: cgfac and the scaled RHS from J, the data residual
 // dat - sigmaa and the regularisation gradient lam * R * par.
 void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s);
 // cjggra / cjggdc: resets the state, then runs up to `iters` iterations.
 void launch_cg_init(const CGArgs& a, cudaStream_t s);
-void launch_cg_iterations(const CGArgs& a, int iters, cudaStream_t s);
+// pc = 1 takes the preconditioner `spc` (crt_spc.h) before every head.
+void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, cudaStream_t s);
 // update.f90:300-351: dpar *= cgfac (lfpi: (0, Re dpar) first), par += step
 // dpar, bdpar = step * sum |dpar|^2.
 void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* bdpar, cudaStream_t s);

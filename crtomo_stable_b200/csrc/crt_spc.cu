@@ -1,0 +1,629 @@
+// crt_spc.cu -- block-tridiagonal preconditioner S^-1 for the normal-equation
+// CG (the operator and its scaling are those of src/cg_mod.f90:426-726 and
+// src/update.f90:200-231; the preconditioner itself has no counterpart in
+// the reference, whose CG is preconditioned by cgfac alone).
+//
+// Host: reverse Cuthill-McKee (George-Liu pseudo-peripheral start, neighbours
+// by ascending degree) on the graph of the roughness operator, block size
+// B = roundup(bandwidth, 32), and one assembly entry per off-diagonal
+// non-zero of R that lands in a diagonal block D_q or a sub-diagonal block
+// F_q of the permuted matrix.
+//
+// Device, once per update:
+//   k_spc_diag / k_spc_entries : S = I + lam C (R - diag R) C in blocks
+//   k_spc_factor  (one CTA)    : T_q = D_q - F_q H_{q-1}, H_{q-1} = T_{q-1}^-1 F_q^T,
+//                                T_q^-1 by Gauss-Jordan with the block held in
+//                                registers (SPD: no pivoting)
+//   k_spc_gmul    (nb CTAs)    : G_q = T_q^-1 F_q
+// and per CG iteration:
+//   k_spc_u       (nb CTAs)    : u_q = T_q^-1 r_q on the permuted residual
+//   k_spc_sweep   (one CTA)    : h_q = u_q - G_q h_{q-1}, x_q = h_q - H_q x_{q+1},
+//                                z = x in element order
+// Every thread owns the NB x NB entries (ty + 32a, tx + 32b) of a block,
+// which keeps shared-memory reads broadcast (A operand) or consecutive
+// (B operand) and global accesses coalesced.
+#include "crt_spc.h"
+
+#include <algorithm>
+#include <vector>
+
+#include "crt_cg.h"
+
+namespace {
+
+constexpr int SPC_NT = 1024;
+
+// ---------------------------------------------------------------------------
+// host: ordering
+void rcm_order(int M, const std::vector<int>& xadj, const std::vector<int>& adj, std::vector<int>& order)
+{
+    std::vector<int> deg(M), stamp(M, -1), lev(M, 0), queue;
+    std::vector<char> placed(M, 0);
+    for (int i = 0; i < M; ++i) deg[i] = xadj[i + 1] - xadj[i];
+    queue.reserve(M);
+    order.clear();
+    order.reserve(M);
+    int sid = 0;
+    // BFS over the unplaced nodes reachable from root; returns the depth and
+    // the lowest-degree node of the last level.
+    auto bfs = [&](int root, int& depth, int& cand) {
+        ++sid;
+        queue.clear();
+        queue.push_back(root);
+        stamp[root] = sid;
+        lev[root] = 0;
+        for (size_t h = 0; h < queue.size(); ++h) {
+            const int v = queue[h];
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e) {
+                const int w = adj[e];
+                if (placed[w] || stamp[w] == sid) continue;
+                stamp[w] = sid;
+                lev[w] = lev[v] + 1;
+                queue.push_back(w);
+            }
+        }
+        depth = lev[queue.back()];
+        cand = queue.back();
+        for (int v : queue)
+            if (lev[v] == depth && deg[v] < deg[cand]) cand = v;
+    };
+    std::vector<int> nbr;
+    for (int s0 = 0; s0 < M; ++s0) {
+        if (placed[s0]) continue;
+        int d0, x;
+        bfs(s0, d0, x);
+        int r = s0;
+        for (int v : queue)
+            if (deg[v] < deg[r]) r = v;
+        bfs(r, d0, x);
+        for (int it = 0; it < 16; ++it) {
+            int dx, y;
+            bfs(x, dx, y);
+            if (dx <= d0) break;
+            r = x;
+            d0 = dx;
+            x = y;
+        }
+        size_t head = order.size();
+        order.push_back(r);
+        placed[r] = 1;
+        while (head < order.size()) {
+            const int v = order[head++];
+            nbr.clear();
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e)
+                if (!placed[adj[e]]) nbr.push_back(adj[e]);
+            std::sort(nbr.begin(), nbr.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+            for (int w : nbr) {
+                if (placed[w]) continue;
+                placed[w] = 1;
+                order.push_back(w);
+            }
+        }
+    }
+    std::reverse(order.begin(), order.end());
+}
+
+// ---------------------------------------------------------------------------
+// device helpers
+__device__ __forceinline__ float warp_allsum_f(float v)
+{
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void k_spc_diag(float* DF, int nb, int B)
+{
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nb * B) return;
+    const int q = idx / B, t = idx % B;
+    DF[(size_t)q * B * B + (size_t)t * B + t] = 1.0f;
+}
+
+__global__ void k_spc_entries(const int4* __restrict__ ent, int nent, const double* __restrict__ cgfac,
+                              const double* __restrict__ smatm, double lam, float* DF)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nent) return;
+    const int4 e = ent[k];
+    DF[e.x] = (float)(lam * cgfac[e.y] * smatm[e.w] * cgfac[e.z]);
+}
+
+// One CTA: the sequential block recurrence.
+template <int NB>
+__global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, int nb, int* flag)
+{
+    constexpr int B = 32 * NB, LD = B + 1;
+    extern __shared__ float smem[];
+    float* X = smem;              // [B][LD]   T_{q-1}^-1, then H_{q-1}
+    float* Sg = X + B * LD;       // [32][LD]  staged operand chunk
+    float* rowb = Sg + 32 * LD;   // [2][B]
+    float* colb = rowb + 2 * B;   // [2][B]
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const size_t BB = (size_t)B * B;
+    const float* F = DF + (size_t)nb * BB;
+    int first_bad = 0;
+    for (int q = 0; q < nb; ++q) {
+        float* Dq = DF + (size_t)q * BB;
+        float t[NB][NB];
+        if (q > 0) {
+            const float* Fq = F + (size_t)q * BB;
+            // H = T_{q-1}^-1 F_q^T:  H[r][c] = sum_k X[r][k] Fq[c][k]
+            float h[NB][NB];
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) h[a][b] = 0.0f;
+            for (int k0 = 0; k0 < B; k0 += 32) {
+                __syncthreads();
+                for (int u = tid; u < 32 * B; u += SPC_NT) {
+                    const int kk = u & 31, c = u >> 5;
+                    Sg[kk * LD + c] = Fq[(size_t)c * B + k0 + kk];
+                }
+                __syncthreads();
+#pragma unroll 4
+                for (int kk = 0; kk < 32; ++kk) {
+                    float av[NB], bv[NB];
+#pragma unroll
+                    for (int a = 0; a < NB; ++a) av[a] = X[(ty + 32 * a) * LD + k0 + kk];
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) bv[b] = Sg[kk * LD + tx + 32 * b];
+#pragma unroll
+                    for (int a = 0; a < NB; ++a)
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) h[a][b] = fmaf(av[a], bv[b], h[a][b]);
+                }
+            }
+            __syncthreads();
+            float* Hq = H + (size_t)(q - 1) * BB;
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    const int r = ty + 32 * a, c = tx + 32 * b;
+                    Hq[(size_t)r * B + c] = h[a][b];
+                    X[r * LD + c] = h[a][b];
+                }
+            // T = D_q - F_q H
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) t[a][b] = Dq[(size_t)(ty + 32 * a) * B + tx + 32 * b];
+            for (int k0 = 0; k0 < B; k0 += 32) {
+                __syncthreads();
+                for (int u = tid; u < 32 * B; u += SPC_NT) {
+                    const int kk = u & 31, r = u >> 5;
+                    Sg[kk * LD + r] = Fq[(size_t)r * B + k0 + kk];
+                }
+                __syncthreads();
+#pragma unroll 4
+                for (int kk = 0; kk < 32; ++kk) {
+                    float av[NB], bv[NB];
+#pragma unroll
+                    for (int a = 0; a < NB; ++a) av[a] = Sg[kk * LD + ty + 32 * a];
+#pragma unroll
+                    for (int b = 0; b < NB; ++b) bv[b] = X[(k0 + kk) * LD + tx + 32 * b];
+#pragma unroll
+                    for (int a = 0; a < NB; ++a)
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) t[a][b] = fmaf(-av[a], bv[b], t[a][b]);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) t[a][b] = Dq[(size_t)(ty + 32 * a) * B + tx + 32 * b];
+        }
+        // Gauss-Jordan inversion in place (SPD, no pivoting); row k and
+        // column k are published through double-buffered shared vectors.
+        for (int k = 0; k < B; ++k) {
+            const int buf = (k & 1) * B, ka = k >> 5, kl = k & 31;
+            if (ty == kl) {
+#pragma unroll
+                for (int a = 0; a < NB; ++a)
+                    if (a == ka) {
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) rowb[buf + tx + 32 * b] = t[a][b];
+                    }
+            }
+            if (tx == kl) {
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+                    if (b == ka) {
+#pragma unroll
+                        for (int a = 0; a < NB; ++a) colb[buf + ty + 32 * a] = t[a][b];
+                    }
+            }
+            __syncthreads();
+            float piv = rowb[buf + k];
+            if (!(piv > 0.0f)) {
+                if (first_bad == 0) first_bad = q + 1;
+                piv = 1.0f;
+            }
+            const float pinv = 1.0f / piv;
+#pragma unroll
+            for (int a = 0; a < NB; ++a) {
+                const int i = ty + 32 * a;
+                const float ci = colb[buf + i] * pinv;
+#pragma unroll
+                for (int b = 0; b < NB; ++b) {
+                    const int j = tx + 32 * b;
+                    const float rj = rowb[buf + j];
+                    float v = t[a][b];
+                    if (i == k) v = (j == k) ? pinv : v * pinv;
+                    else if (j == k) v = -v * pinv;
+                    else v = fmaf(-ci, rj, v);
+                    t[a][b] = v;
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < NB; ++a)
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const int r = ty + 32 * a, c = tx + 32 * b;
+                Dq[(size_t)r * B + c] = t[a][b];
+                X[r * LD + c] = t[a][b];
+            }
+    }
+    if (tid == 0) *flag = first_bad;
+}
+
+// G_q = T_q^-1 F_q, one CTA per block q >= 1.
+template <int NB>
+__global__ void __launch_bounds__(SPC_NT, 1) k_spc_gmul(const float* DF, float* G, int nb)
+{
+    constexpr int B = 32 * NB, LD = B + 1;
+    extern __shared__ float smem[];
+    float* As = smem;         // [32][LD]
+    float* Bs = As + 32 * LD; // [32][LD]
+    const int q = blockIdx.x + 1;
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const size_t BB = (size_t)B * B;
+    const float* Ti = DF + (size_t)q * BB;
+    const float* Fq = DF + (size_t)nb * BB + (size_t)q * BB;
+    float g[NB][NB];
+#pragma unroll
+    for (int a = 0; a < NB; ++a)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) g[a][b] = 0.0f;
+    for (int k0 = 0; k0 < B; k0 += 32) {
+        __syncthreads();
+        for (int u = tid; u < 32 * B; u += SPC_NT) {
+            const int kk = u & 31, r = u >> 5;
+            As[kk * LD + r] = Ti[(size_t)r * B + k0 + kk];
+            const int c = u % B, k2 = u / B;
+            Bs[k2 * LD + c] = Fq[(size_t)(k0 + k2) * B + c];
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < 32; ++kk) {
+            float av[NB], bv[NB];
+#pragma unroll
+            for (int a = 0; a < NB; ++a) av[a] = As[kk * LD + ty + 32 * a];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) bv[b] = Bs[kk * LD + tx + 32 * b];
+#pragma unroll
+            for (int a = 0; a < NB; ++a)
+#pragma unroll
+                for (int b = 0; b < NB; ++b) g[a][b] = fmaf(av[a], bv[b], g[a][b]);
+        }
+    }
+    float* Gq = G + (size_t)q * BB;
+#pragma unroll
+    for (int a = 0; a < NB; ++a)
+#pragma unroll
+        for (int b = 0; b < NB; ++b) Gq[(size_t)(ty + 32 * a) * B + tx + 32 * b] = g[a][b];
+}
+
+// u_q = T_q^-1 r_q on the permuted residual (FP32), one CTA per block.
+template <int NB>
+__global__ void __launch_bounds__(SPC_NT) k_spc_u(const float* __restrict__ DF, const int* __restrict__ perm,
+                                                 const cd* __restrict__ r, cf* __restrict__ h,
+                                                 const CGState* __restrict__ st)
+{
+    constexpr int B = 32 * NB;
+    __shared__ cf rv[B];
+    if (st->done) return;
+    const int q = blockIdx.x;
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    if (tid < B) {
+        const int e = perm[q * B + tid];
+        const cd v = e >= 0 ? r[e] : cd{0.0, 0.0};
+        rv[tid] = cf{(float)v.x, (float)v.y};
+    }
+    __syncthreads();
+    const float* Ti = DF + (size_t)q * B * B;
+#pragma unroll
+    for (int a = 0; a < NB; ++a) {
+        const int row = ty + 32 * a;
+        float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const float m = Ti[(size_t)row * B + tx + 32 * b];
+            const cf x = rv[tx + 32 * b];
+            sx = fmaf(m, x.x, sx);
+            sy = fmaf(m, x.y, sy);
+        }
+        sx = warp_allsum_f(sx);
+        sy = warp_allsum_f(sy);
+        if (tx == 0) h[q * B + row] = cf{sx, sy};
+    }
+}
+
+// The two sequential sweeps and the scatter back to element order.
+template <int NB>
+__global__ void __launch_bounds__(SPC_NT, 1) k_spc_sweep(const float* __restrict__ Gm, const float* __restrict__ Hm,
+                                                        const int* __restrict__ perm, cf* h, cd* __restrict__ z,
+                                                        int nb, const CGState* __restrict__ st)
+{
+    constexpr int B = 32 * NB;
+    __shared__ cf v[2][B];
+    if (st->done) return;
+    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const size_t BB = (size_t)B * B;
+    int cur = 0;
+    if (tid < B) v[0][tid] = h[tid];
+    float m[NB][NB], mn[NB][NB];
+    cf un[NB];
+    auto load_mat = [&](const float* base, float (&dst)[NB][NB]) {
+#pragma unroll
+        for (int a = 0; a < NB; ++a)
+#pragma unroll
+            for (int b = 0; b < NB; ++b) dst[a][b] = base[(size_t)(ty + 32 * a) * B + tx + 32 * b];
+    };
+    auto load_vec = [&](int q, cf (&dst)[NB]) {
+        if (tx == 0) {
+#pragma unroll
+            for (int a = 0; a < NB; ++a) dst[a] = h[(size_t)q * B + ty + 32 * a];
+        }
+    };
+    // forward: h_q = u_q - G_q h_{q-1}
+    if (nb > 1) {
+        load_mat(Gm + BB, mn);
+        load_vec(1, un);
+    }
+    __syncthreads();
+    for (int q = 1; q < nb; ++q) {
+        cf u[NB];
+#pragma unroll
+        for (int a = 0; a < NB; ++a) {
+            u[a] = un[a];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) m[a][b] = mn[a][b];
+        }
+        if (q + 1 < nb) {
+            load_mat(Gm + (size_t)(q + 1) * BB, mn);
+            load_vec(q + 1, un);
+        }
+#pragma unroll
+        for (int a = 0; a < NB; ++a) {
+            float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const cf x = v[cur][tx + 32 * b];
+                sx = fmaf(m[a][b], x.x, sx);
+                sy = fmaf(m[a][b], x.y, sy);
+            }
+            sx = warp_allsum_f(sx);
+            sy = warp_allsum_f(sy);
+            if (tx == 0) {
+                const int row = ty + 32 * a;
+                const cf y = cf{u[a].x - sx, u[a].y - sy};
+                v[cur ^ 1][row] = y;
+                h[(size_t)q * B + row] = y;
+            }
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    // backward: x_q = h_q - H_q x_{q+1}; v[cur] holds x_{nb-1} = h_{nb-1}
+    if (nb > 1) {
+        load_mat(Hm + (size_t)(nb - 2) * BB, mn);
+        load_vec(nb - 2, un);
+    }
+    for (int q = nb - 2; q >= 0; --q) {
+        cf u[NB];
+#pragma unroll
+        for (int a = 0; a < NB; ++a) {
+            u[a] = un[a];
+#pragma unroll
+            for (int b = 0; b < NB; ++b) m[a][b] = mn[a][b];
+        }
+        if (q > 0) {
+            load_mat(Hm + (size_t)(q - 1) * BB, mn);
+            load_vec(q - 1, un);
+        }
+#pragma unroll
+        for (int a = 0; a < NB; ++a) {
+            float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const cf x = v[cur][tx + 32 * b];
+                sx = fmaf(m[a][b], x.x, sx);
+                sy = fmaf(m[a][b], x.y, sy);
+            }
+            sx = warp_allsum_f(sx);
+            sy = warp_allsum_f(sy);
+            if (tx == 0) {
+                const int row = ty + 32 * a;
+                const cf y = cf{u[a].x - sx, u[a].y - sy};
+                v[cur ^ 1][row] = y;
+                h[(size_t)q * B + row] = y;
+            }
+        }
+        __syncthreads();
+        cur ^= 1;
+    }
+    __syncthreads();
+    for (int pos = tid; pos < nb * B; pos += SPC_NT) {
+        const int e = perm[pos];
+        if (e >= 0) {
+            const cf x = h[pos];
+            z[e] = cd{(double)x.x, (double)x.y};
+        }
+    }
+}
+
+size_t factor_smem(int B) { return sizeof(float) * ((size_t)B * (B + 1) + 32 * (B + 1) + 4 * B); }
+size_t gmul_smem(int B) { return sizeof(float) * (2 * 32 * (size_t)(B + 1)); }
+
+template <int NB>
+void factor_nb(const SpcPlan& P, cudaStream_t s)
+{
+    const int B = 32 * NB;
+    const size_t fs = factor_smem(B), gs = gmul_smem(B);
+    cudaFuncSetAttribute(k_spc_factor<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs);
+    cudaFuncSetAttribute(k_spc_gmul<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gs);
+    k_spc_factor<NB><<<1, SPC_NT, fs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag);
+    if (P.nb > 1) k_spc_gmul<NB><<<P.nb - 1, SPC_NT, gs, s>>>(P.d_DF, P.d_G, P.nb);
+}
+
+template <int NB>
+void apply_nb(const SpcPlan& P, const cd* r, cd* z, const CGState* st, cudaStream_t s)
+{
+    k_spc_u<NB><<<P.nb, SPC_NT, 0, s>>>(P.d_DF, P.d_perm, r, P.d_h, st);
+    k_spc_sweep<NB><<<1, SPC_NT, 0, s>>>(P.d_G, P.d_H, P.d_perm, P.d_h, z, P.nb, st);
+}
+
+template <typename T>
+bool alloc(T** p, size_t n)
+{
+    return cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess;
+}
+
+}  // namespace
+
+int spc_plan_build(SpcPlan& P, int M, int ltri, int nx, int nnb, const double* smatm, const int* nachbar,
+                   std::string& why)
+{
+    spc_plan_free(P);
+    P.M = M;
+    // directed non-zero off-diagonal entries (i, j, smatm index) of R
+    std::vector<int> ei, ej, es;
+    auto add = [&](int i, int j, long long s) {
+        if (j == i || smatm[s] == 0.0) return;
+        ei.push_back(i);
+        ej.push_back(j);
+        es.push_back((int)s);
+    };
+    if (ltri == 0) {
+        for (int i = 0; i < M; ++i) {
+            if (i > 0) add(i, i - 1, (long long)M + i - 1);
+            if (i < M - 1) add(i, i + 1, (long long)M + i);
+            if (i >= nx) add(i, i - nx, 2LL * M + i - nx);
+            if (i < M - nx) add(i, i + nx, 2LL * M + i);
+        }
+    } else {
+        for (int k = 0; k < nnb; ++k)
+            for (int i = 0; i < M; ++i) {
+                const int id = nachbar[(size_t)k * M + i];
+                if (id > 0) add(i, id - 1, (long long)k * M + i);
+            }
+    }
+    const size_t ne = ei.size();
+    // symmetric adjacency for the ordering
+    std::vector<int> xadj(M + 1, 0), adj;
+    for (size_t k = 0; k < ne; ++k) {
+        xadj[ei[k] + 1]++;
+        xadj[ej[k] + 1]++;
+    }
+    for (int i = 0; i < M; ++i) xadj[i + 1] += xadj[i];
+    adj.resize(xadj[M]);
+    {
+        std::vector<int> fill(xadj.begin(), xadj.end() - 1);
+        for (size_t k = 0; k < ne; ++k) {
+            adj[fill[ei[k]]++] = ej[k];
+            adj[fill[ej[k]]++] = ei[k];
+        }
+    }
+    std::vector<int> order;
+    rcm_order(M, xadj, adj, order);
+    std::vector<int> pos(M);
+    for (int k = 0; k < M; ++k) pos[order[k]] = k;
+    int bw = 0;
+    for (size_t k = 0; k < ne; ++k) bw = std::max(bw, std::abs(pos[ei[k]] - pos[ej[k]]));
+    P.bw = bw;
+    const int B = std::max(32, (bw + 31) / 32 * 32);
+    if (B > SPC_MAX_B) {
+        why = "regulariser bandwidth " + std::to_string(bw) + " after reverse Cuthill-McKee exceeds " +
+              std::to_string(SPC_MAX_B) + "; the block preconditioner is not available for this mesh";
+        return 0;
+    }
+    P.B = B;
+    P.nb = (M + B - 1) / B;
+    P.Mp = P.nb * B;
+    const size_t BB = (size_t)B * B;
+    std::vector<int> perm(P.Mp, -1);
+    for (int k = 0; k < M; ++k) perm[k] = order[k];
+    std::vector<int4> ent;
+    ent.reserve(ne);
+    for (size_t k = 0; k < ne; ++k) {
+        const int pi = pos[ei[k]], pj = pos[ej[k]];
+        const int qi = pi / B, qj = pj / B, ri = pi % B, rj = pj % B;
+        size_t dst;
+        if (qi == qj) dst = (size_t)qi * BB + (size_t)ri * B + rj;
+        else if (qi == qj + 1) dst = (size_t)P.nb * BB + (size_t)qi * BB + (size_t)ri * B + rj;
+        else continue;   // upper block: the transpose of an F entry
+        ent.push_back(int4{(int)dst, ei[k], ej[k], es[k]});
+    }
+    P.nent = (int)ent.size();
+    if (2 * (size_t)P.nb * BB > (size_t)INT32_MAX) {
+        why = "block preconditioner too large for 32-bit entry offsets";
+        return 0;
+    }
+    bool ok = alloc(&P.d_perm, P.Mp) && alloc(&P.d_ent, ent.size()) && alloc(&P.d_DF, 2 * P.nb * BB) &&
+              alloc(&P.d_G, P.nb * BB) && alloc(&P.d_H, P.nb * BB) && alloc(&P.d_h, P.Mp) && alloc(&P.d_flag, 1);
+    if (!ok) {
+        spc_plan_free(P);
+        return CRT_ERR_ALLOC;
+    }
+    if (cudaMemcpy(P.d_perm, perm.data(), perm.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        (ent.size() && cudaMemcpy(P.d_ent, ent.data(), ent.size() * sizeof(int4), cudaMemcpyHostToDevice) != cudaSuccess)) {
+        spc_plan_free(P);
+        return CRT_ERR_CUDA;
+    }
+    P.ok = 1;
+    return 0;
+}
+
+void spc_plan_free(SpcPlan& P)
+{
+    cudaFree(P.d_perm);
+    cudaFree(P.d_ent);
+    cudaFree(P.d_DF);
+    cudaFree(P.d_G);
+    cudaFree(P.d_H);
+    cudaFree(P.d_h);
+    cudaFree(P.d_flag);
+    P = SpcPlan{};
+}
+
+void launch_spc_factor(const SpcPlan& P, const double* cgfac, const double* smatm, double lam, cudaStream_t s)
+{
+    const size_t BB = (size_t)P.B * P.B;
+    cudaMemsetAsync(P.d_DF, 0, 2 * P.nb * BB * sizeof(float), s);
+    k_spc_diag<<<(P.nb * P.B + 255) / 256, 256, 0, s>>>(P.d_DF, P.nb, P.B);
+    if (P.nent) k_spc_entries<<<(P.nent + 255) / 256, 256, 0, s>>>(P.d_ent, P.nent, cgfac, smatm, lam, P.d_DF);
+    switch (P.B / 32) {
+    case 1: factor_nb<1>(P, s); break;
+    case 2: factor_nb<2>(P, s); break;
+    case 3: factor_nb<3>(P, s); break;
+    case 4: factor_nb<4>(P, s); break;
+    case 5: factor_nb<5>(P, s); break;
+    default: factor_nb<6>(P, s); break;
+    }
+}
+
+void launch_spc_apply(const SpcPlan& P, const cd* r, cd* z, const CGState* st, cudaStream_t s)
+{
+    switch (P.B / 32) {
+    case 1: apply_nb<1>(P, r, z, st, s); break;
+    case 2: apply_nb<2>(P, r, z, st, s); break;
+    case 3: apply_nb<3>(P, r, z, st, s); break;
+    case 4: apply_nb<4>(P, r, z, st, s); break;
+    case 5: apply_nb<5>(P, r, z, st, s); break;
+    default: apply_nb<6>(P, r, z, st, s); break;
+    }
+}

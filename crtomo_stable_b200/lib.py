@@ -57,6 +57,7 @@ class crt_cg_params(C.Structure):
     _fields_ = [
         ("lam", C.c_double), ("eps", C.c_double), ("ncgmax", C.c_int32),
         ("ldc", C.c_int32), ("lfpi", C.c_int32), ("step", C.c_double),
+        ("precond", C.c_int32),
     ]
 
 
@@ -65,7 +66,7 @@ EXPORTS = [
     "crt_forward", "crt_potentials", "crt_jacobian", "crt_set_jacobian", "crt_set_regularizer",
     "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
-    "crt_voltages_noalloc",
+    "crt_voltages_noalloc", "crt_cg_info",
 ]
 
 _LIB = None
@@ -121,6 +122,8 @@ def load(path: str = LIB_PATH):
     L.crt_gn_step_device.restype = C.c_int32
     L.crt_last_timings.argtypes = [vp, f64p]
     L.crt_last_timings.restype = C.c_int32
+    L.crt_cg_info.argtypes = [vp, i32p, i32p, i32p]
+    L.crt_cg_info.restype = C.c_int32
     L.crt_launch_count.argtypes = [vp]
     L.crt_launch_count.restype = C.c_int64
     L.crt_dmisft.argtypes = [C.c_int32, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, f64p, f64p, i32p]
@@ -181,6 +184,8 @@ def _mesh_struct(mesh, keep):
 
 PREC_FP64 = 0
 PREC_MIXED = 1
+PRECOND_JACOBI = 0
+PRECOND_BLOCK = 1
 
 
 class Context:
@@ -312,10 +317,11 @@ class Context:
         self._check(self.L.crt_set_data(self.h, _vp(d), _vp(w), _vp(wf)), "crt_set_data")
 
     @staticmethod
-    def params(lam, eps=1e-4, ncgmax=100, ldc=False, lfpi=False, step=1.0):
+    def params(lam, eps=1e-4, ncgmax=100, ldc=False, lfpi=False, step=1.0, precond=0):
         p = crt_cg_params()
         p.lam, p.eps, p.ncgmax = float(lam), float(eps), int(ncgmax)
         p.ldc, p.lfpi, p.step = int(bool(ldc)), int(bool(lfpi)), float(step)
+        p.precond = int(precond)
         return p
 
     def update(self, prm, par, sigmaa=None):
@@ -366,6 +372,13 @@ class Context:
 
     def launch_count(self):
         return int(self.L.crt_launch_count(self.h))
+
+    def cg_info(self):
+        """(form of the last CG, block size of the block preconditioner or 0,
+        regulariser half-bandwidth after reverse Cuthill-McKee)."""
+        f, b, w = C.c_int32(), C.c_int32(), C.c_int32()
+        self._check(self.L.crt_cg_info(self.h, C.byref(f), C.byref(b), C.byref(w)), "crt_cg_info")
+        return f.value, b.value, w.value
 
 
 def dmisft(dat, sigmaa, wmatd, wmatdr=None, wmatdp=None, lfpi=False, lpol=False):

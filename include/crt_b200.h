@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define CRT_B200_ABI_VERSION 1
+#define CRT_B200_ABI_VERSION 2
 
 typedef struct crt_ctx crt_ctx;
 
@@ -71,7 +71,21 @@ typedef struct {
     int32_t ldc;       /* DC inversion: real Jacobian (bsendc), cjggdc */
     int32_t lfpi;      /* final phase improvement: real part of J, imaginary RHS */
     double step;       /* model step length applied by crt_update */
+    int32_t precond;   /* CRT_PRECOND_JACOBI (the reference's cjggra / cjggdc) or
+                          CRT_PRECOND_BLOCK (no reference counterpart) */
 } crt_cg_params;
+
+/* CG forms.
+ * CRT_PRECOND_JACOBI: the reference iteration, preconditioned by cgfac only.
+ * CRT_PRECOND_BLOCK:  additionally preconditioned by S^-1, S the sparse part
+ *   diag(C^2 J^H W J) + lam C R C of the scaled operator (C = diag(cgfac)),
+ *   factored block-tridiagonally in FP32 after a reverse Cuthill-McKee
+ *   ordering of the regulariser's graph; flexible (Polak-Ribiere) beta, the
+ *   reference's stop rule on the true residual.  Falls back to the Jacobi
+ *   form when the ordered bandwidth exceeds 192 or a pivot breaks down
+ *   (crt_cg_info reports which form ran). */
+#define CRT_PRECOND_JACOBI 0
+#define CRT_PRECOND_BLOCK 1
 
 /* Precision forms.
  * CRT_PREC_FP64:  everything in FP64 / complex128 (the reference's arithmetic).
@@ -182,6 +196,12 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
 
 /* Kernel launches enqueued by the context since creation. */
 int64_t crt_launch_count(const crt_ctx *ctx);
+
+/* Form of the last inner CG (CRT_PRECOND_*), block size B of the block
+ * preconditioner (0 when unavailable for this regulariser) and the
+ * regulariser's half-bandwidth after reverse Cuthill-McKee.  Any pointer
+ * may be NULL.  No reference counterpart. */
+int32_t crt_cg_info(const crt_ctx *ctx, int32_t *form, int32_t *block, int32_t *bandwidth);
 
 /* Allocation-free voltages.  No counterpart in the reference: it exists for
  * callers that cannot allocate device memory (all of their device memory is

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_entry_point():
     for n in names:
         assert hasattr(L, n), n
     assert set(lib.EXPORTS) == set(names)
-    assert L.crt_abi_version() == 1
+    assert L.crt_abi_version() == 2
 
 
 def test_rwaven_host_entry_point_matches_oracle():

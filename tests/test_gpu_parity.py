@@ -48,7 +48,7 @@ def _oracle(case):
 def test_library_loads_on_device():
     from crtomo_stable_b200 import lib
     L = lib.load()
-    assert L.crt_abi_version() == 1
+    assert L.crt_abi_version() == 2
 
 
 @pytest.mark.parametrize("name", ["minimal", "TestModInv", "grid_decoupling"])
@@ -379,5 +379,141 @@ def test_mixed_form_cg_converges_to_the_same_update():
                    ncgmax=2000).update(J_o, dat, sa_o, par, 1.0)
     got = ctx.update(Context.params(300.0, eps=1e-12, ncgmax=2000), par, sigmaa=sa_o)
     assert got["ncg"] < 2000
+    np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-4, atol=1e-4 * np.abs(ref["dpar"]).max())
+    ctx.close()
+
+
+def _true_relres(J, wmatd, cgfac, lam, R, rhs, dpar):
+    """|b - A x| / |b| of the scaled system A = C (J^H W J + lam R) C,
+    x = dpar / cgfac, evaluated in FP64 on the host."""
+    x = dpar / cgfac
+    Js = J * cgfac[None, :]
+    Ax = Js.conj().T @ (wmatd * (Js @ x)) + lam * cgfac * (R @ (cgfac * x))
+    return np.linalg.norm(rhs - Ax) / np.linalg.norm(rhs)
+
+
+def _R_tri(sm, nb):
+    import scipy.sparse as sp
+    E = sm.shape[0]
+    nnb = sm.shape[1] - 1
+    rows, cols, vals = [np.arange(E)], [np.arange(E)], [sm[:, nnb]]
+    for k in range(nnb):
+        h = nb[:, k] > 0
+        rows.append(np.arange(E)[h])
+        cols.append(nb[h, k] - 1)
+        vals.append(sm[h, k])
+    return sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(E, E))
+
+
+def test_block_preconditioned_cg_matches_oracle():
+    """The block-preconditioned CG (CRT_PRECOND_BLOCK) reaches the reference's
+    stop rule |r|^2 <= 1e-12 |r0|^2 on the true residual and an update within
+    1e-4 of the FP64 oracle's Jacobi-form CG, in fewer iterations."""
+    from crtomo_stable_b200.lib import PRECOND_BLOCK
+    from oracle.oracle import OracleCG
+    ctx, op, case, dat, wmatd, sig, sa_o, J_o, nb, sm, Context = _setup_cg_case()
+    E = case["mesh"].elanz
+    lam = 300.0
+    ref = OracleCG(E, len(dat), 1, sm, nachbar=nb, nnb=case["mesh"].maxnodes, wmatd=wmatd, lam=lam, eps=1e-12,
+                   ncgmax=2000).update(J_o, dat, sa_o, np.log(sig), 1.0)
+    got = ctx.update(Context.params(lam, eps=1e-12, ncgmax=2000, precond=PRECOND_BLOCK), np.log(sig), sigmaa=sa_o)
+    form, B, bw = ctx.cg_info()
+    assert form == PRECOND_BLOCK and B >= bw and B % 32 == 0
+    assert got["ncg"] < ref["ncg"]
+    np.testing.assert_allclose(got["cgfac"], ref["cgfac"], rtol=1e-11)
+    np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-4, atol=1e-4 * np.abs(ref["dpar"]).max())
+    assert _true_relres(J_o, wmatd, ref["cgfac"], lam, _R_tri(sm, nb), ref["rhs"], got["dpar"]) < 2e-6
+    ctx.close()
+
+
+@pytest.mark.parametrize("ldc", [False, True])
+def test_block_preconditioned_cg_five_point_and_real(ldc):
+    """ltri = 0 (five-point bsmatmreg operator) on a quadrilateral grid, for
+    the complex (cjggra) and the real DC (cjggdc) system: the block form
+    matches the Jacobi form run on the same device-resident Jacobian."""
+    from crtomo_stable_b200 import regularization, synth
+    from crtomo_stable_b200.lib import PRECOND_BLOCK, Context
+    nx, nz, nel = 40, 24, 16
+    xs = np.arange(nx + 1, dtype=np.float64) - 12.0
+    depths = synth.graded_depths(nz, 0.5, 1.05)
+    mesh = synth.structured_mesh(xs, depths, triangles=False)
+    enr = synth.surface_electrodes(mesh, xs, np.arange(nel, dtype=np.float64), nz)
+    strnr, vnr = synth.encode(synth.dipole_dipole(nel, (1, 2), 6))
+    rng = np.random.default_rng(5)
+    sig = synth.sigma_from(np.exp(rng.uniform(np.log(20), np.log(200), mesh.elanz)),
+                           -rng.uniform(1, 20, mesh.elanz))
+    ctx = Context(mesh, enr, strnr, vnr)
+    _, sa = ctx.forward(sig, ldc=ldc)
+    dat = sa + 0.02 * rng.standard_normal(len(sa)) + (0.0 if ldc else 1e-3j * rng.standard_normal(len(sa)))
+    wmatd = np.full(len(sa), 1.0 / 0.02 ** 2)
+    sig0 = np.full(mesh.elanz, np.exp(np.mean(np.log(sig))))
+    _, sa0 = ctx.forward(sig0, ldc=ldc)
+    ctx.jacobian(mode=1 if ldc else 0, copy=False)
+    sm = regularization.smatm_reg(mesh, nx, nz, 1.0, 1.0)
+    ctx.set_regularizer(0, sm, nx=nx)
+    ctx.set_data(dat, wmatd)
+    lam = float(mesh.elanz)
+    par = np.log(sig0)
+    base = ctx.update(Context.params(lam, eps=1e-12, ncgmax=5000, ldc=ldc), par, sigmaa=sa0)
+    assert ctx.cg_info()[0] == 0
+    got = ctx.update(Context.params(lam, eps=1e-12, ncgmax=5000, ldc=ldc, precond=PRECOND_BLOCK), par, sigmaa=sa0)
+    form, B, bw = ctx.cg_info()
+    assert form == PRECOND_BLOCK and bw <= nz + 1
+    assert got["ncg"] * 3 < base["ncg"]
+    np.testing.assert_allclose(got["dpar"], base["dpar"], rtol=1e-4, atol=1e-4 * np.abs(base["dpar"]).max())
+    if ldc:
+        assert np.abs(got["dpar"].imag).max() == 0.0 and np.abs(base["dpar"].imag).max() == 0.0
+    ctx.close()
+
+
+@pytest.mark.parametrize("form", ["ldc", "lfpi"])
+def test_update_real_modes_match_oracle(form):
+    """cjggdc forms from a complex starting model: the DC inversion (real
+    Jacobian bsendc, real part of the right-hand side) and the final phase
+    improvement (real part of J, imaginary part of the right-hand side,
+    dpar = (0, x)); the Jacobi form against the oracle at the reference's
+    stop rule, the block form at rel-res 1e-6."""
+    from crtomo_stable_b200 import regularization
+    from crtomo_stable_b200.lib import PRECOND_BLOCK, Context
+    from oracle.oracle import OracleCG
+    case = load_forward_case("minimal")
+    m = case["mesh"]
+    d = case["volt"]
+    ctx = _ctx(case)
+    op = _oracle(case)
+    dat = -np.log(d.bet) - 1j * d.pha / 1e3
+    wmatd = 1.0 / (1e-2 + 1e-3 / d.bet) ** 2
+    sig = np.full(m.elanz, 0.01 * np.exp(-0.01j))
+    ldc = form == "ldc"
+    ctx.forward(sig, ldc=ldc)
+    ctx.jacobian(mode=1 if ldc else 0, copy=False)
+    kp = op.forward(sig, ldc=ldc, nthreads=4)
+    volt_o, sa_o = op.bvolti(op.rtrafo(kp))
+    nb = regularization.nachbar(m)
+    sm = regularization.smatm_tri(m, nb, 10.0, 1.0)
+    ctx.set_regularizer(1, sm, nachbar=nb)
+    ctx.set_data(dat, wmatd)
+    par = np.log(sig)
+    J = op.bsendc(kp, sig, volt_o, nthreads=4) if ldc else op.bsensi(kp, sig, volt_o, nthreads=4)
+
+    def oracle(eps, ncgmax):
+        cg = OracleCG(m.elanz, len(dat), 1, sm, nachbar=nb, nnb=m.maxnodes, wmatd=wmatd, lam=300.0, eps=eps,
+                      ncgmax=ncgmax, ldc=ldc, lfpi=not ldc)
+        if ldc:
+            return cg.update(None, dat, sa_o, par, 1.0, sensdc=J)
+        return cg.update(J, dat, sa_o, par, 1.0)
+
+    ref = oracle(1e-4, m.elanz // 10)
+    got = ctx.update(Context.params(300.0, eps=1e-4, ncgmax=m.elanz // 10, ldc=ldc, lfpi=not ldc), par, sigmaa=sa_o)
+    assert got["ncg"] == ref["ncg"]
+    np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-7, atol=1e-7 * np.abs(ref["dpar"]).max())
+    if ldc:
+        assert np.abs(got["dpar"].imag).max() == 0.0
+    else:
+        assert np.abs(got["dpar"].real).max() == 0.0
+    ref = oracle(1e-12, 2000)
+    got = ctx.update(Context.params(300.0, eps=1e-12, ncgmax=2000, ldc=ldc, lfpi=not ldc, precond=PRECOND_BLOCK),
+                     par, sigmaa=sa_o)
+    assert ctx.cg_info()[0] == PRECOND_BLOCK
     np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-4, atol=1e-4 * np.abs(ref["dpar"]).max())
     ctx.close()
