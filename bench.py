@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--eps", type=float, default=1e-12, help="|r|^2 <= eps |r0|^2 (1e-12 = rel-res 1e-6)")
     ap.add_argument("--ncgmax", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--forms", default="both", choices=["both", "mixed"],
+                    help="'mixed' skips the plain FP64 comparison run (profiling)")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     return ap.parse_args()
 
@@ -302,7 +304,9 @@ def main():
                     cg_form=form, cg_block=blk, cg_bw=bw)
 
     mixed = run_form(PREC_MIXED, args.steps, args.warmup, args.steps, True)
-    plain = run_form(PREC_FP64, max(1, args.steps // 3), max(1, args.warmup // 3), 0, False)
+    plain = None
+    if args.forms == "both":
+        plain = run_form(PREC_FP64, max(1, args.steps // 3), max(1, args.warmup // 3), 0, False)
     t_step, phase, ncg, K = mixed["t"], mixed["phase"], mixed["ncg"], mixed["K"]
     h2d = E * 16
     d2h = E * 16 + N * 16 + (ncg + 1) * 8 + 8
@@ -347,8 +351,9 @@ def main():
                            "l2": "inputs larger than L2 (J alone is %.1f GB in complex64)" % (N * E * 8 / 1e9),
                            "parallelism": f"replicas x{ws}"},
                 "phases_ms": dict(zip(names + ["total"], [float(x) for x in phase])),
-                "plain_fp64": {"value": plain["t"], "unit": "s", "cg_iterations": plain["ncg"],
-                               "phases_ms": dict(zip(names + ["total"], [float(x) for x in plain["phase"]]))},
+                "plain_fp64": None if plain is None else
+                {"value": plain["t"], "unit": "s", "cg_iterations": plain["ncg"],
+                 "phases_ms": dict(zip(names + ["total"], [float(x) for x in plain["phase"]]))},
                 "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
                 "roofline": roof, "cpu_baseline": cpu, "clocks": mixed["clocks"],
                 "gpu_launches": mixed["launches"]}

@@ -171,7 +171,7 @@ size_t sens_elem_bytes(const crt_ctx* ctx, bool real)
 int plan_chunk(crt_ctx* ctx, int nsys, size_t tsize)
 {
     const size_t slot = (size_t)ctx->n * ctx->W * tsize;
-    size_t budget = (size_t)16 << 30;
+    size_t budget = (size_t)48 << 30;
     if (const char* env = std::getenv("CRT_B200_WORKSPACE_GB")) budget = (size_t)(std::atof(env) * (1u << 30));
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 2);

@@ -221,8 +221,27 @@ __global__ void __launch_bounds__(NT) k_band_factor(BandArgs<T> A)
 // Both sweeps are blocked by BB columns: the off-block part of every column
 // is a coalesced dot/axpy over the column-packed factor, the in-block
 // triangle is solved by one warp.
+template <typename T> __device__ __forceinline__ T shfl_idx_t(T v, int src);
+template <> __device__ __forceinline__ double shfl_idx_t<double>(double v, int src)
+{
+    return __shfl_sync(0xffffffffu, v, src);
+}
+template <> __device__ __forceinline__ cd shfl_idx_t<cd>(cd v, int src)
+{
+    return cd{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+template <typename T> __device__ __forceinline__ T shfl_down_t(T v, int off);
+template <> __device__ __forceinline__ double shfl_down_t<double>(double v, int off)
+{
+    return __shfl_down_sync(0xffffffffu, v, off);
+}
+template <> __device__ __forceinline__ cd shfl_down_t<cd>(cd v, int off)
+{
+    return cd{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)};
+}
+
 template <typename T, int NT, int BB>
-__global__ void __launch_bounds__(NT) k_band_solve(SolveArgs<T> A, T* scratch)
+__global__ void __launch_bounds__(NT, 3) k_band_solve(SolveArgs<T> A, T* scratch)
 {
     __shared__ T tri[BB][BB];
     __shared__ T part[BB];
@@ -293,62 +312,51 @@ __global__ void __launch_bounds__(NT) k_band_solve(SolveArgs<T> A, T* scratch)
         }
     }
     __syncthreads();
-    // Back substitution L^T x = y, blocked from the end.
+    // Back substitution L^T x = y, blocked from the end.  Per block of BB
+    // columns, NT/BB consecutive threads own a column: they keep all loads
+    // of its off-block part in flight for the dot product with the solved
+    // unknowns and stage its in-block entries row-wise (zeros beyond the
+    // band, so no entry of an earlier block survives); one warp then
+    // solves the BB x BB triangle with one unknown per lane (the pivots'
+    // reciprocals are formed off the critical path, and each unknown costs
+    // one shuffle broadcast and one FMA per lane).
+    constexpr int TPC = NT / BB;
+    static_assert(BB == 32 && TPC * BB == NT && (TPC & (TPC - 1)) == 0, "solve layout");
+    __shared__ T trw[BB][BB + 1];   // trw[r][c] = L(c0 + r, c0 + c), r >= c
+    const int col = tid / TPC, sub = tid % TPC;
     for (int c1 = n; c1 > 0; c1 -= BB) {
         const int c0 = max(0, c1 - BB), nb = c1 - c0;
-        // off-block part of every column in the block (one warp per column)
-        for (int cc = warp; cc < nb; cc += NW) {
-            const int c = c0 + cc;
-            T acc = Sc<T>::zero();
-            for (int d = c1 - c + lane; d <= mb && c + d < n; d += 32)
-                acc += Sc<T>::mul(Lc[(size_t)c * W + d], z[c + d]);
-            // warp reduction
-            for (int off = 16; off > 0; off >>= 1) {
-                T o;
-                if constexpr (sizeof(T) == sizeof(double)) {
-                    o = __shfl_down_sync(0xffffffffu, acc, off);
-                } else {
-                    cd a = Sc<T>::to_cd(acc);
-                    cd r;
-                    r.x = __shfl_down_sync(0xffffffffu, a.x, off);
-                    r.y = __shfl_down_sync(0xffffffffu, a.y, off);
-                    o = *reinterpret_cast<T*>(&r);
-                }
-                acc += o;
+        T acc = Sc<T>::zero();
+        if (col < nb) {
+            const int c = c0 + col;
+            const T* Lcol = Lc + (size_t)c * W;
+            const int dmax = min(mb, n - 1 - c);
+            const int din = nb - col;          // d < din: rows inside the block
+            const int dend = max(dmax, din - 1);
+#pragma unroll 8
+            for (int d = sub; d <= dend; d += TPC) {
+                const T v = d <= dmax ? Lcol[d] : Sc<T>::zero();
+                if (d < din) trw[col + d][col] = v;
+                else acc += Sc<T>::mul(v, z[c + d]);
             }
-            if (lane == 0) part[cc] = acc;
         }
-        for (int t = tid; t < BB * BB; t += NT) {
-            int cc = t / BB, d = t % BB;
-            int c = c0 + cc;
-            tri[cc][d] = (cc < nb && d <= mb && c + d < c1) ? Lc[(size_t)c * W + d] : Sc<T>::zero();
-        }
-        if (tid < BB) zb[tid] = (tid < nb) ? z[c0 + tid] : Sc<T>::zero();
+#pragma unroll
+        for (int off = TPC / 2; off > 0; off >>= 1) acc += shfl_down_t(acc, off);
+        if (sub == 0 && col < nb) part[col] = acc;
         __syncthreads();
         if (warp == 0) {
-            for (int cc = nb - 1; cc >= 0; --cc) {
-                T acc = Sc<T>::zero();
-                int d = lane;
-                if (d >= 1 && cc + d < nb) acc = Sc<T>::mul(tri[cc][d], zb[cc + d]);
-                for (int off = 16; off > 0; off >>= 1) {
-                    T o;
-                    if constexpr (sizeof(T) == sizeof(double)) {
-                        o = __shfl_down_sync(0xffffffffu, acc, off);
-                    } else {
-                        cd a = Sc<T>::to_cd(acc);
-                        cd r;
-                        r.x = __shfl_down_sync(0xffffffffu, a.x, off);
-                        r.y = __shfl_down_sync(0xffffffffu, a.y, off);
-                        o = *reinterpret_cast<T*>(&r);
-                    }
-                    acc += o;
-                }
-                if (lane == 0) zb[cc] = Sc<T>::div(zb[cc] - part[cc] - acc, tri[cc][0]);
-                __syncwarp();
+            T v = Sc<T>::zero(), dinv = Sc<T>::zero();
+            if (lane < nb) {
+                v = z[c0 + lane] - part[lane];
+                dinv = Sc<T>::recip(trw[lane][lane]);
             }
+            for (int cc = nb - 1; cc >= 0; --cc) {
+                if (lane == cc) v = Sc<T>::mul(v, dinv);
+                const T x = shfl_idx_t(v, cc);
+                if (lane < cc) v -= Sc<T>::mul(trw[cc][lane], x);
+            }
+            if (lane < nb) z[c0 + lane] = v;
         }
-        __syncthreads();
-        if (tid < nb) z[c0 + tid] = zb[tid];
         __syncthreads();
     }
     // kpot(j, l, k) = pot(j) * fak(j) with pot = -z.

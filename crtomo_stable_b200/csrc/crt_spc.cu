@@ -18,7 +18,7 @@
 // and per CG iteration:
 //   k_spc_u       (nb CTAs)    : u_q = T_q^-1 r_q on the permuted residual
 //   k_spc_sweep   (one CTA)    : h_q = u_q - G_q h_{q-1}, x_q = h_q - H_q x_{q+1},
-//                                z = x in element order
+//                                z = x in element order (G and H column-major)
 // Every thread owns the NB x NB entries (ty + 32a, tx + 32b) of a block,
 // which keeps shared-memory reads broadcast (A operand) or consecutive
 // (B operand) and global accesses coalesced.
@@ -35,9 +35,16 @@ constexpr int SPC_NT = 1024;
 
 // ---------------------------------------------------------------------------
 // host: ordering
+//
+// Per connected component: George-Liu pseudo-peripheral node r, then a
+// Cuthill-McKee breadth-first numbering (neighbours by ascending degree,
+// ties by index) from each of a few candidate roots -- r, the far end of
+// its level structure and the lowest-degree nodes of the last level -- and
+// the numbering with the smallest bandwidth is kept.  The concatenated
+// order is reversed (which does not change the bandwidth).
 void rcm_order(int M, const std::vector<int>& xadj, const std::vector<int>& adj, std::vector<int>& order)
 {
-    std::vector<int> deg(M), stamp(M, -1), lev(M, 0), queue;
+    std::vector<int> deg(M), stamp(M, -1), lev(M, 0), queue, lpos(M, -1), cm, best;
     std::vector<char> placed(M, 0);
     for (int i = 0; i < M; ++i) deg[i] = xadj[i + 1] - xadj[i];
     queue.reserve(M);
@@ -68,6 +75,31 @@ void rcm_order(int M, const std::vector<int>& xadj, const std::vector<int>& adj,
             if (lev[v] == depth && deg[v] < deg[cand]) cand = v;
     };
     std::vector<int> nbr;
+    // Cuthill-McKee numbering of the component from root into cm; returns
+    // its bandwidth.
+    auto cuthill_mckee = [&](int root) {
+        ++sid;
+        cm.clear();
+        cm.push_back(root);
+        stamp[root] = sid;
+        for (size_t head = 0; head < cm.size(); ++head) {
+            const int v = cm[head];
+            nbr.clear();
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e)
+                if (!placed[adj[e]] && stamp[adj[e]] != sid) nbr.push_back(adj[e]);
+            std::sort(nbr.begin(), nbr.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+            for (int w : nbr) {
+                if (stamp[w] == sid) continue;
+                stamp[w] = sid;
+                cm.push_back(w);
+            }
+        }
+        for (size_t k = 0; k < cm.size(); ++k) lpos[cm[k]] = (int)k;
+        int bw = 0;
+        for (int v : cm)
+            for (int e = xadj[v]; e < xadj[v + 1]; ++e) bw = std::max(bw, std::abs(lpos[v] - lpos[adj[e]]));
+        return bw;
+    };
     for (int s0 = 0; s0 < M; ++s0) {
         if (placed[s0]) continue;
         int d0, x;
@@ -84,20 +116,25 @@ void rcm_order(int M, const std::vector<int>& xadj, const std::vector<int>& adj,
             d0 = dx;
             x = y;
         }
-        size_t head = order.size();
-        order.push_back(r);
-        placed[r] = 1;
-        while (head < order.size()) {
-            const int v = order[head++];
-            nbr.clear();
-            for (int e = xadj[v]; e < xadj[v + 1]; ++e)
-                if (!placed[adj[e]]) nbr.push_back(adj[e]);
-            std::sort(nbr.begin(), nbr.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
-            for (int w : nbr) {
-                if (placed[w]) continue;
-                placed[w] = 1;
-                order.push_back(w);
+        // candidate roots
+        std::vector<int> cands{r, x};
+        bfs(r, d0, x);
+        std::vector<int> last;
+        for (int v : queue)
+            if (lev[v] == d0) last.push_back(v);
+        std::sort(last.begin(), last.end(), [&](int a, int b) { return deg[a] != deg[b] ? deg[a] < deg[b] : a < b; });
+        for (size_t k = 0; k < last.size() && k < 4; ++k) cands.push_back(last[k]);
+        int best_bw = -1;
+        for (int c : cands) {
+            const int bw = cuthill_mckee(c);
+            if (best_bw < 0 || bw < best_bw) {
+                best_bw = bw;
+                best = cm;
             }
+        }
+        for (int v : best) {
+            placed[v] = 1;
+            order.push_back(v);
         }
     }
     std::reverse(order.begin(), order.end());
@@ -174,15 +211,17 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, i
                 }
             }
             __syncthreads();
-            float* Hq = H + (size_t)(q - 1) * BB;
 #pragma unroll
             for (int a = 0; a < NB; ++a)
 #pragma unroll
-                for (int b = 0; b < NB; ++b) {
-                    const int r = ty + 32 * a, c = tx + 32 * b;
-                    Hq[(size_t)r * B + c] = h[a][b];
-                    X[r * LD + c] = h[a][b];
-                }
+                for (int b = 0; b < NB; ++b) X[(ty + 32 * a) * LD + tx + 32 * b] = h[a][b];
+            __syncthreads();
+            // the sweep reads H_{q-1} column-major: HT[c][r] = H[r][c]
+            float* Hq = H + (size_t)(q - 1) * BB;
+            for (int u = tid; u < B * B; u += SPC_NT) {
+                const int r = u % B, c = u / B;
+                Hq[(size_t)c * B + r] = X[r * LD + c];
+            }
             // T = D_q - F_q H
 #pragma unroll
             for (int a = 0; a < NB; ++a)
@@ -241,20 +280,35 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, i
                 piv = 1.0f;
             }
             const float pinv = 1.0f / piv;
+            // every entry: t_ij - t_ik t_kj / t_kk; row k and column k are
+            // then overwritten by their owners
 #pragma unroll
             for (int a = 0; a < NB; ++a) {
-                const int i = ty + 32 * a;
-                const float ci = colb[buf + i] * pinv;
+                const float ci = colb[buf + ty + 32 * a] * pinv;
 #pragma unroll
-                for (int b = 0; b < NB; ++b) {
-                    const int j = tx + 32 * b;
-                    const float rj = rowb[buf + j];
-                    float v = t[a][b];
-                    if (i == k) v = (j == k) ? pinv : v * pinv;
-                    else if (j == k) v = -v * pinv;
-                    else v = fmaf(-ci, rj, v);
-                    t[a][b] = v;
-                }
+                for (int b = 0; b < NB; ++b) t[a][b] = fmaf(-ci, rowb[buf + tx + 32 * b], t[a][b]);
+            }
+            if (ty == kl) {
+#pragma unroll
+                for (int a = 0; a < NB; ++a)
+                    if (a == ka) {
+#pragma unroll
+                        for (int b = 0; b < NB; ++b) {
+                            const int j = tx + 32 * b;
+                            t[a][b] = (j == k) ? pinv : rowb[buf + j] * pinv;
+                        }
+                    }
+            }
+            if (tx == kl) {
+#pragma unroll
+                for (int b = 0; b < NB; ++b)
+                    if (b == ka) {
+#pragma unroll
+                        for (int a = 0; a < NB; ++a) {
+                            const int i = ty + 32 * a;
+                            if (i != k) t[a][b] = -colb[buf + i] * pinv;
+                        }
+                    }
             }
         }
         __syncthreads();
@@ -270,14 +324,16 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, i
     if (tid == 0) *flag = first_bad;
 }
 
-// G_q = T_q^-1 F_q, one CTA per block q >= 1.
+// G_q = T_q^-1 F_q stored column-major for the sweep:
+// GT[c][r] = G[r][c] = sum_k F[k][c] Tinv[k][r] (T_q^-1 is symmetric); one
+// CTA per block q >= 1.
 template <int NB>
 __global__ void __launch_bounds__(SPC_NT, 1) k_spc_gmul(const float* DF, float* G, int nb)
 {
     constexpr int B = 32 * NB, LD = B + 1;
     extern __shared__ float smem[];
-    float* As = smem;         // [32][LD]
-    float* Bs = As + 32 * LD; // [32][LD]
+    float* As = smem;         // [32][LD]  F rows k0..k0+31
+    float* Bs = As + 32 * LD; // [32][LD]  Tinv rows k0..k0+31
     const int q = blockIdx.x + 1;
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
     const size_t BB = (size_t)B * B;
@@ -291,10 +347,9 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_gmul(const float* DF, float* 
     for (int k0 = 0; k0 < B; k0 += 32) {
         __syncthreads();
         for (int u = tid; u < 32 * B; u += SPC_NT) {
-            const int kk = u & 31, r = u >> 5;
-            As[kk * LD + r] = Ti[(size_t)r * B + k0 + kk];
-            const int c = u % B, k2 = u / B;
-            Bs[k2 * LD + c] = Fq[(size_t)(k0 + k2) * B + c];
+            const int c = u % B, kk = u / B;
+            As[kk * LD + c] = Fq[(size_t)(k0 + kk) * B + c];
+            Bs[kk * LD + c] = Ti[(size_t)(k0 + kk) * B + c];
         }
         __syncthreads();
 #pragma unroll 4
@@ -352,112 +407,122 @@ __global__ void __launch_bounds__(SPC_NT) k_spc_u(const float* __restrict__ DF, 
     }
 }
 
-// The two sequential sweeps and the scatter back to element order.
+// The two sequential sweeps and the scatter back to element order.  The
+// blocks are read column-major (MT[c][r]); warp g of the 16 owns the column
+// slice [g B/16, (g+1) B/16) and lane l the rows [l NB, l NB + NB), so every
+// load is a contiguous NB-float run of a column (coalesced across the warp)
+// and the next block's slice is prefetched into registers while the
+// current one is used.  The 16 partial sums of a row meet in shared memory.
+constexpr int SW_NT = 512, SW_G = SW_NT / 32;
+
 template <int NB>
-__global__ void __launch_bounds__(SPC_NT, 1) k_spc_sweep(const float* __restrict__ Gm, const float* __restrict__ Hm,
-                                                        const int* __restrict__ perm, cf* h, cd* __restrict__ z,
-                                                        int nb, const CGState* __restrict__ st)
+__device__ __forceinline__ void load_run(const float* __restrict__ p, float (&d)[NB])
 {
-    constexpr int B = 32 * NB;
-    __shared__ cf v[2][B];
+    if constexpr (NB == 4) {
+        const float4 v = *reinterpret_cast<const float4*>(p);
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
+    } else if constexpr (NB == 2) {
+        const float2 v = *reinterpret_cast<const float2*>(p);
+        d[0] = v.x;
+        d[1] = v.y;
+    } else {
+#pragma unroll
+        for (int i = 0; i < NB; ++i) d[i] = p[i];
+    }
+}
+
+template <int NB>
+__global__ void __launch_bounds__(SW_NT, 1) k_spc_sweep(const float* __restrict__ Gm, const float* __restrict__ Hm,
+                                                       const int* __restrict__ perm, cf* h, cd* __restrict__ z,
+                                                       int nb, const CGState* __restrict__ st)
+{
+    constexpr int B = 32 * NB, CPW = B / SW_G;   // columns per warp
+    __shared__ cf v[B];
+    __shared__ cf part[SW_G][B];
     if (st->done) return;
-    const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, g = tid >> 5;
     const size_t BB = (size_t)B * B;
-    int cur = 0;
-    if (tid < B) v[0][tid] = h[tid];
-    float m[NB][NB], mn[NB][NB];
-    cf un[NB];
-    auto load_mat = [&](const float* base, float (&dst)[NB][NB]) {
+    const int r0 = lane * NB, cbase = g * CPW;
+    float m[CPW][NB], mn[CPW][NB];
+    cf un = cf{0.0f, 0.0f};
+    auto load_blk = [&](const float* base, float (&dst)[CPW][NB]) {
 #pragma unroll
-        for (int a = 0; a < NB; ++a)
-#pragma unroll
-            for (int b = 0; b < NB; ++b) dst[a][b] = base[(size_t)(ty + 32 * a) * B + tx + 32 * b];
+        for (int j = 0; j < CPW; ++j) load_run<NB>(base + (size_t)(cbase + j) * B + r0, dst[j]);
     };
-    auto load_vec = [&](int q, cf (&dst)[NB]) {
-        if (tx == 0) {
+    // one step: y = u - M x, with x in v; y replaces v and h_q
+    auto step = [&](int q, const cf u) {
+        float px[NB], py[NB];
 #pragma unroll
-            for (int a = 0; a < NB; ++a) dst[a] = h[(size_t)q * B + ty + 32 * a];
+        for (int i = 0; i < NB; ++i) {
+            px[i] = 0.0f;
+            py[i] = 0.0f;
         }
+#pragma unroll
+        for (int j = 0; j < CPW; ++j) {
+            const cf x = v[cbase + j];
+#pragma unroll
+            for (int i = 0; i < NB; ++i) {
+                px[i] = fmaf(m[j][i], x.x, px[i]);
+                py[i] = fmaf(m[j][i], x.y, py[i]);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < NB; ++i) part[g][r0 + i] = cf{px[i], py[i]};
+        __syncthreads();
+        if (tid < B) {
+            float sx = u.x, sy = u.y;
+#pragma unroll
+            for (int w = 0; w < SW_G; ++w) {
+                const cf pw = part[w][tid];
+                sx -= pw.x;
+                sy -= pw.y;
+            }
+            const cf y = cf{sx, sy};
+            v[tid] = y;
+            h[(size_t)q * B + tid] = y;
+        }
+        __syncthreads();
     };
+    if (tid < B) v[tid] = h[tid];
     // forward: h_q = u_q - G_q h_{q-1}
     if (nb > 1) {
-        load_mat(Gm + BB, mn);
-        load_vec(1, un);
+        load_blk(Gm + BB, mn);
+        if (tid < B) un = h[B + tid];
     }
     __syncthreads();
     for (int q = 1; q < nb; ++q) {
-        cf u[NB];
+        const cf u = un;
 #pragma unroll
-        for (int a = 0; a < NB; ++a) {
-            u[a] = un[a];
+        for (int j = 0; j < CPW; ++j)
 #pragma unroll
-            for (int b = 0; b < NB; ++b) m[a][b] = mn[a][b];
-        }
+            for (int i = 0; i < NB; ++i) m[j][i] = mn[j][i];
         if (q + 1 < nb) {
-            load_mat(Gm + (size_t)(q + 1) * BB, mn);
-            load_vec(q + 1, un);
+            load_blk(Gm + (size_t)(q + 1) * BB, mn);
+            if (tid < B) un = h[(size_t)(q + 1) * B + tid];
         }
-#pragma unroll
-        for (int a = 0; a < NB; ++a) {
-            float sx = 0.0f, sy = 0.0f;
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const cf x = v[cur][tx + 32 * b];
-                sx = fmaf(m[a][b], x.x, sx);
-                sy = fmaf(m[a][b], x.y, sy);
-            }
-            sx = warp_allsum_f(sx);
-            sy = warp_allsum_f(sy);
-            if (tx == 0) {
-                const int row = ty + 32 * a;
-                const cf y = cf{u[a].x - sx, u[a].y - sy};
-                v[cur ^ 1][row] = y;
-                h[(size_t)q * B + row] = y;
-            }
-        }
-        __syncthreads();
-        cur ^= 1;
+        step(q, u);
     }
-    // backward: x_q = h_q - H_q x_{q+1}; v[cur] holds x_{nb-1} = h_{nb-1}
+    // backward: x_q = h_q - H_q x_{q+1}; v holds x_{nb-1} = h_{nb-1}
     if (nb > 1) {
-        load_mat(Hm + (size_t)(nb - 2) * BB, mn);
-        load_vec(nb - 2, un);
+        load_blk(Hm + (size_t)(nb - 2) * BB, mn);
+        if (tid < B) un = h[(size_t)(nb - 2) * B + tid];
     }
     for (int q = nb - 2; q >= 0; --q) {
-        cf u[NB];
+        const cf u = un;
 #pragma unroll
-        for (int a = 0; a < NB; ++a) {
-            u[a] = un[a];
+        for (int j = 0; j < CPW; ++j)
 #pragma unroll
-            for (int b = 0; b < NB; ++b) m[a][b] = mn[a][b];
-        }
+            for (int i = 0; i < NB; ++i) m[j][i] = mn[j][i];
         if (q > 0) {
-            load_mat(Hm + (size_t)(q - 1) * BB, mn);
-            load_vec(q - 1, un);
+            load_blk(Hm + (size_t)(q - 1) * BB, mn);
+            if (tid < B) un = h[(size_t)(q - 1) * B + tid];
         }
-#pragma unroll
-        for (int a = 0; a < NB; ++a) {
-            float sx = 0.0f, sy = 0.0f;
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const cf x = v[cur][tx + 32 * b];
-                sx = fmaf(m[a][b], x.x, sx);
-                sy = fmaf(m[a][b], x.y, sy);
-            }
-            sx = warp_allsum_f(sx);
-            sy = warp_allsum_f(sy);
-            if (tx == 0) {
-                const int row = ty + 32 * a;
-                const cf y = cf{u[a].x - sx, u[a].y - sy};
-                v[cur ^ 1][row] = y;
-                h[(size_t)q * B + row] = y;
-            }
-        }
-        __syncthreads();
-        cur ^= 1;
+        step(q, u);
     }
-    __syncthreads();
-    for (int pos = tid; pos < nb * B; pos += SPC_NT) {
+    for (int pos = tid; pos < nb * B; pos += SW_NT) {
         const int e = perm[pos];
         if (e >= 0) {
             const cf x = h[pos];
@@ -484,7 +549,7 @@ template <int NB>
 void apply_nb(const SpcPlan& P, const cd* r, cd* z, const CGState* st, cudaStream_t s)
 {
     k_spc_u<NB><<<P.nb, SPC_NT, 0, s>>>(P.d_DF, P.d_perm, r, P.d_h, st);
-    k_spc_sweep<NB><<<1, SPC_NT, 0, s>>>(P.d_G, P.d_H, P.d_perm, P.d_h, z, P.nb, st);
+    k_spc_sweep<NB><<<1, SW_NT, 0, s>>>(P.d_G, P.d_H, P.d_perm, P.d_h, z, P.nb, st);
 }
 
 template <typename T>
@@ -494,6 +559,33 @@ bool alloc(T** p, size_t n)
 }
 
 }  // namespace
+
+extern "C" int32_t crt_rcm_order(int32_t n, const int32_t* xadj, const int32_t* adj, int32_t* order,
+                                  int32_t* bandwidth)
+{
+    if (n < 1 || !xadj || !order) return CRT_ERR_ARG;
+    if (xadj[0] != 0) return CRT_ERR_ARG;
+    for (int i = 0; i < n; ++i)
+        if (xadj[i + 1] < xadj[i]) return CRT_ERR_ARG;
+    const int nadj = xadj[n];
+    if (nadj > 0 && !adj) return CRT_ERR_ARG;
+    for (int e = 0; e < nadj; ++e)
+        if (adj[e] < 0 || adj[e] >= n) return CRT_ERR_ARG;
+    std::vector<int> xa(xadj, xadj + n + 1), ad(adj, adj + nadj), ord;
+    rcm_order(n, xa, ad, ord);
+    std::vector<int> pos(n);
+    for (int k = 0; k < n; ++k) {
+        order[k] = ord[k];
+        pos[ord[k]] = k;
+    }
+    if (bandwidth) {
+        int bw = 0;
+        for (int v = 0; v < n; ++v)
+            for (int e = xa[v]; e < xa[v + 1]; ++e) bw = std::max(bw, std::abs(pos[v] - pos[ad[e]]));
+        *bandwidth = bw;
+    }
+    return CRT_OK;
+}
 
 int spc_plan_build(SpcPlan& P, int M, int ltri, int nx, int nnb, const double* smatm, const int* nachbar,
                    std::string& why)

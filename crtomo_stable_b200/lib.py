@@ -66,7 +66,7 @@ EXPORTS = [
     "crt_forward", "crt_potentials", "crt_jacobian", "crt_set_jacobian", "crt_set_regularizer",
     "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
-    "crt_voltages_noalloc", "crt_cg_info",
+    "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order",
 ]
 
 _LIB = None
@@ -124,6 +124,8 @@ def load(path: str = LIB_PATH):
     L.crt_last_timings.restype = C.c_int32
     L.crt_cg_info.argtypes = [vp, i32p, i32p, i32p]
     L.crt_cg_info.restype = C.c_int32
+    L.crt_rcm_order.argtypes = [C.c_int32, i32p, i32p, i32p, i32p]
+    L.crt_rcm_order.restype = C.c_int32
     L.crt_launch_count.argtypes = [vp]
     L.crt_launch_count.restype = C.c_int64
     L.crt_dmisft.argtypes = [C.c_int32, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, f64p, f64p, i32p]
@@ -159,6 +161,21 @@ def rwaven(mesh, enr, strnr, vnr):
     if e:
         raise CRTError(e, "rwaven")
     return kwn[: n.value].copy(), kwnwi[: n.value].copy()
+
+
+def rcm_order(xadj, adj):
+    """Reverse Cuthill-McKee ordering of a CSR graph through the C ABI:
+    (order, bandwidth); order[k] is the vertex at position k."""
+    L = load()
+    xadj = np.ascontiguousarray(xadj, np.int32)
+    adj = np.ascontiguousarray(adj, np.int32)
+    n = len(xadj) - 1
+    order = np.zeros(n, np.int32)
+    bw = C.c_int32()
+    e = L.crt_rcm_order(n, _ptr(xadj, C.c_int32), _ptr(adj, C.c_int32), _ptr(order, C.c_int32), C.byref(bw))
+    if e:
+        raise CRTError(e, "rcm_order")
+    return order, bw.value
 
 
 def _mesh_struct(mesh, keep):

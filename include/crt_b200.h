@@ -203,6 +203,14 @@ int64_t crt_launch_count(const crt_ctx *ctx);
  * may be NULL.  No reference counterpart. */
 int32_t crt_cg_info(const crt_ctx *ctx, int32_t *form, int32_t *block, int32_t *bandwidth);
 
+/* Reverse Cuthill-McKee ordering of an undirected graph in CSR form
+ * (xadj[n+1], adj[xadj[n]], 0-based, both directions of every edge listed):
+ * order[k] = the vertex placed at position k; *bandwidth (may be NULL) =
+ * max |pos(v) - pos(w)| over the edges.  Host-only, no device needed.  The
+ * ordering the block preconditioner uses for the regulariser's graph; the
+ * reference renumbers mesh nodes with Cuthill-McKee in cutmckee/cutmck.f. */
+int32_t crt_rcm_order(int32_t n, const int32_t *xadj, const int32_t *adj, int32_t *order, int32_t *bandwidth);
+
 /* Allocation-free voltages.  No counterpart in the reference: it exists for
  * callers that cannot allocate device memory (all of their device memory is
  * allocated up front, e.g. from their own pool or a framework allocator, or

@@ -118,3 +118,41 @@ def test_crmod_geometric_factors_match_oracle_and_recording():
     np.testing.assert_allclose(kf, op.bkfak(), rtol=1e-13)
     rec = np.loadtxt(os.path.join(case["base"], "exe", "tmp.kfak"))
     np.testing.assert_allclose(kf, rec[:, 1], rtol=6e-4)
+
+
+def test_rcm_order_bandwidth_and_permutation():
+    """crt_rcm_order (host code of the block preconditioner): a permutation
+    whose bandwidth is no worse than scipy's reverse Cuthill-McKee on the
+    element graph of a triangle mesh, and argument checks."""
+    import scipy.sparse as sp
+    from scipy.sparse.csgraph import reverse_cuthill_mckee
+    from crtomo_stable_b200 import regularization, synth
+    from crtomo_stable_b200.lib import CRTError, rcm_order
+    s = synth.small_triangles(nx=30, nz=12)
+    E = s.mesh.elanz
+    nb = regularization.nachbar(s.mesh)
+    rows, cols = [], []
+    for k in range(3):
+        h = nb[:, k] > 0
+        rows.append(np.arange(E)[h])
+        cols.append(nb[h, k] - 1)
+    rows, cols = np.concatenate(rows), np.concatenate(cols)
+    A = sp.csr_matrix((np.ones(len(rows)), (rows, cols)), shape=(E, E))
+    A = (A + A.T).tocsr()
+    order, bw = rcm_order(A.indptr, A.indices)
+    assert np.array_equal(np.sort(order), np.arange(E))
+    pos = np.empty(E, int)
+    pos[order] = np.arange(E)
+    c = A.tocoo()
+    assert bw == np.abs(pos[c.row] - pos[c.col]).max()
+    p = reverse_cuthill_mckee(A, symmetric_mode=True)
+    q = np.empty(E, int)
+    q[p] = np.arange(E)
+    assert bw <= np.abs(q[c.row] - q[c.col]).max()
+    # two components and an isolated vertex
+    xadj = np.array([0, 1, 2, 3, 4, 4])
+    adj = np.array([1, 0, 3, 2])
+    order, bw = rcm_order(xadj, adj)
+    assert sorted(order) == [0, 1, 2, 3, 4] and bw == 1
+    with pytest.raises(CRTError):
+        rcm_order(np.array([0, 1]), np.array([5]))
