@@ -1,6 +1,14 @@
 // crt_band_blk.cu -- panel-blocked band factorisation (the production
 // variant of k_band_factor, same inputs, outputs and arithmetic contract).
 //
+// A preparation pass (k_band_prep_diag / k_band_prep_rows, all rows of all
+// systems in parallel) assembles every row from the gather lists (kompab),
+// applies the Dirichlet edits (randb) and the symmetric scaling (scalab) in
+// FP64 and stores the finished row r row-packed at Lws[r W + d] = A(r, r-d).
+// That is exactly the place of column r of the column-packed factor, which
+// is written only after row r has entered the window, so the factor
+// overwrites the prepared matrix in place.
+//
 // One CTA per band system.  The window holds Wn = roundup(mb + PB, PB) rows
 // in shared memory; row r lives in slot r mod Wn and the symmetric entry of
 // two rows is stored once, at the unordered slot pair, in 4 x 4 tiles
@@ -8,15 +16,14 @@
 // columns [i0, i0 + PB):
 //   1. warp 0 factors the PB x PB diagonal block (unconjugated L L^T, the
 //      recurrence of src/chol.f90:44-78 restricted to the block) and
-//      forward-substitutes the panel's right-hand side; warps 1.. form the
-//      next PB rows from the gather lists (kompab) into a staging buffer;
+//      forward-substitutes the panel's right-hand side; warps 1.. load the
+//      next PB prepared rows into a staging buffer;
 //   2. every window row below the panel solves its PB entries against the
 //      block (L_x = A_x L_D^-T), updates its right-hand side and writes its
 //      L entries to the window and to the column-packed HBM factor;
 //   3. the trailing window is updated by the rank-PB product L_x L_y^T, each
 //      thread accumulating 4 x 4 tiles in registers;
-//   4. the PB staged rows are scaled (scalab), Dirichlet-edited (randb) and
-//      written into the slots the panel freed.
+//   4. the PB staged rows are written into the slots the panel freed.
 // Four CTA barriers per PB columns replace the three per column of the
 // rank-1 variant.
 #include "crt_band.h"
@@ -89,6 +96,70 @@ __device__ __forceinline__ T rhs_entry_b(int r, int src, int lsink, int nsink0, 
     return b;
 }
 
+// System of launch slot b: (k, l) for mixed boundaries, else (k, 0).
+template <typename T>
+__device__ __forceinline__ void sys_kl(const BandArgs<T>& A, int sys, int& k, int& l)
+{
+    if (A.mixed) {
+        k = sys / A.L;
+        l = sys % A.L;
+    } else {
+        k = sys;
+        l = 0;
+    }
+}
+
+// Diagonal of every row: the normalised diagonal entry (scalab: unit modulus
+// in the complex case, 1 in the real one; randb: 1 for a Dirichlet node) and
+// the scaling factor fak = 1 / sqrt(|a_rr|); errnr 27 on a zero diagonal.
+template <typename T>
+__global__ void k_band_prep_diag(BandArgs<T> A)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = A.n;
+    if (idx >= (long long)A.nsys * n) return;
+    const int b = (int)(idx / n), r = (int)(idx % n), sys = A.sys0 + b;
+    int k, l;
+    sys_kl(A, sys, k, l);
+    T raw = Sc<T>::zero();
+    for (int e = A.row_ptr[r]; e < A.row_ptr[r + 1]; ++e)
+        if (A.ent_d[e] == 0) raw = assemble_entry_b(A, e, k, l);
+    if (A.dflag[r]) raw = Sc<T>::one();
+    const double d = Sc<T>::absval(raw);
+    double f = 1.0;
+    if (!(d > 0.0)) A.status[sys] = CRT_ERR_ZERO_DIAG;
+    else f = 1.0 / sqrt(d);
+    A.fakws[(size_t)b * n + r] = f;
+    A.Lws[(size_t)b * A.lstride + (size_t)r * A.W] = Sc<T>::normalise(raw, d);
+}
+
+// Off-diagonal entries of every row, one warp per row: zero fill, then
+// a(r, r-d) * fak_r * fak_(r-d), or 0 when either node is a Dirichlet node.
+template <typename T>
+__global__ void k_band_prep_rows(BandArgs<T> A)
+{
+    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31, n = A.n;
+    if (wid >= (long long)A.nsys * n) return;
+    const int b = (int)(wid / n), r = (int)(wid % n), sys = A.sys0 + b;
+    int k, l;
+    sys_kl(A, sys, k, l);
+    T* row = A.Lws + (size_t)b * A.lstride + (size_t)r * A.W;
+    const double* fk = A.fakws + (size_t)b * n;
+    for (int d = 1 + lane; d <= A.mb; d += 32) row[d] = Sc<T>::zero();
+    __syncwarp();
+    const bool dr = A.dflag[r] != 0;
+    const double fr = fk[r];
+    for (int e = A.row_ptr[r] + lane; e < A.row_ptr[r + 1]; e += 32) {
+        const int d = A.ent_d[e];
+        if (d == 0) continue;
+        const int c = r - d;
+        T v = Sc<T>::zero();
+        if (!dr && A.dflag[c] == 0) v = scale(assemble_entry_b(A, e, k, l), fr * fk[c]);
+        row[d] = v;
+    }
+}
+
 template <typename T, int PB, int NT>
 __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
 {
@@ -102,24 +173,16 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     T* bsl = LD + PB * PB;                                // Wn
     T* yP = bsl + Wn;                                     // PB
     T* LDi = yP + PB;                                     // PB reciprocal pivots
-    double* fakw = reinterpret_cast<double*>(LDi + PB);   // Wn
-    double* fakN = fakw + Wn;                             // PB
-    unsigned short* tXY = reinterpret_cast<unsigned short*>(fakN + PB);   // NTT
-    unsigned char* dfw = reinterpret_cast<unsigned char*>(tXY + NTT);     // Wn: Dirichlet flag per slot
-    __shared__ unsigned char dfN[PB];                                     // flags of the staged rows
+    double* fakN = reinterpret_cast<double*>(LDi + PB);   // PB scaling factors of the staged rows
+    unsigned short* tXY = reinterpret_cast<unsigned short*>(fakN + PB);   // NTT tile coordinates
     __shared__ T colb[32];                                                // column broadcast of the block factor
     __shared__ int s_err;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x, sys = A.sys0 + b;
+    if (A.status[sys] != 0) return;    // zero diagonal found by the preparation pass
     int k, l;
-    if (A.mixed) {
-        k = sys / A.L;
-        l = sys % A.L;
-    } else {
-        k = sys;
-        l = 0;
-    }
+    sys_kl(A, sys, k, l);
     T* Lc = A.Lws + (size_t)b * A.lstride;
     double* fk = A.fakws + (size_t)b * n;
     const bool fuse = A.fuse_rhs != 0;
@@ -131,8 +194,6 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     for (int i = tid; i < PB * W1; i += NT) stage[i] = Sc<T>::zero();
     for (int i = tid; i < Wn; i += NT) {
         bsl[i] = Sc<T>::zero();
-        fakw[i] = 0.0;
-        dfw[i] = 0;
     }
     for (int t = tid; t < NTT; t += NT) {
         // decode t -> (X, Y) with X >= Y
@@ -144,86 +205,44 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     if (tid == 0) s_err = 0;
     __syncthreads();
 
-    // Raw entries of rows [r0, r0 + PB) into stage[q][d].  The entries of
-    // consecutive rows are contiguous in the gather lists, so the threads in
-    // [t0, NT) take one entry each across all PB rows.
-    auto stage_rows = [&](int r0, int t0) {
-        if (r0 >= n) return;
-        const int rend = min(r0 + PB, n);
-        const int e0 = A.row_ptr[r0], e1 = A.row_ptr[rend];
-        for (int e = e0 + (tid - t0); e < e1; e += NT - t0) {
-            int q = 0;
-            while (q + 1 < rend - r0 && A.row_ptr[r0 + q + 1] <= e) ++q;
-            stage[q * W1 + A.ent_d[e]] = assemble_entry_b(A, e, k, l);
+    // Prepared rows [r0, r0 + PB) into stage[q][d] and their scaling factors
+    // into fakN (threads t0 .. NT-1; rows beyond n are zero).
+    auto load_rows = [&](int r0, int t0) {
+        const T* src_rows = Lc + (size_t)r0 * W1;
+        for (int i = tid - t0; i < PB * W1; i += NT - t0) {
+            const int q = i / W1;
+            stage[i] = (r0 + q < n) ? src_rows[i] : Sc<T>::zero();
         }
+        const int q = tid - t0;
+        if (q >= 0 && q < PB) fakN[q] = (r0 + q < n) ? fk[r0 + q] : 1.0;
     };
-    // Scaling factors of the staged rows (threads q < PB).
-    auto stage_fak = [&](int r0) {
-        if (tid < PB) {
-            const int r = r0 + tid;
-            double f = 1.0;
-            const unsigned char fl = (r < n) ? A.dflag[r] : 0;
-            dfN[tid] = fl;
-            if (r < n) {
-                T raw = fl ? Sc<T>::one() : stage[tid * W1];
-                double d = Sc<T>::absval(raw);
-                if (!(d > 0.0)) s_err = CRT_ERR_ZERO_DIAG;
-                else f = 1.0 / sqrt(d);
-                fk[r] = f;
-            }
-            fakN[tid] = f;
-        }
-    };
-    // Scaled staged rows into slots s_new .. s_new+PB-1; the window after the
-    // write holds rows [wlo, wlo + Wn).  Every pair of a new slot with a row
+    // Staged rows into slots s_new .. s_new+PB-1; the window after the write
+    // holds rows [wlo, wlo + Wn).  Every pair of a new slot with a row
     // c <= r is written (zero outside the band), pairs with later new rows
     // are written by those rows.
     auto scatter_rows = [&](int r0, int s_new, int wlo) {
         const int wm = wlo % Wn;
-#pragma unroll
-        for (int q = 0; q < PB; ++q) {
+        for (int i = tid; i < PB * Wn; i += NT) {
+            const int q = i / Wn, y = i % Wn;
             const int r = r0 + q;
-            const bool dr = dfN[q] != 0;
-            for (int y = tid; y < Wn; y += NT) {
-                int off = y - wm;
-                if (off < 0) off += Wn;
-                const int c = wlo + off;                      // row held by slot y
-                if (c > r) continue;
-                const int d = r - c;
-                T v = Sc<T>::zero();
-                if (r < n) {
-                    if (d == 0) {
-                        T raw = dr ? Sc<T>::one() : stage[q * W1];
-                        v = Sc<T>::normalise(raw, Sc<T>::absval(raw));
-                    } else if (d <= mb) {
-                        const bool newc = c >= r0;
-                        const bool dc = newc ? (dfN[c - r0] != 0) : (dfw[y] != 0);
-                        if (!dr && !dc) {
-                            const double fc = newc ? fakN[c - r0] : fakw[y];
-                            v = scale(stage[q * W1 + d], fakN[q] * fc);
-                        }
-                    }
-                }
-                win[widx(s_new + q, y)] = v;
-            }
+            int off = y - wm;
+            if (off < 0) off += Wn;
+            const int c = wlo + off;                      // row held by slot y
+            if (c > r) continue;
+            const int d = r - c;
+            win[widx(s_new + q, y)] = (r < n && d <= mb) ? stage[q * W1 + d] : Sc<T>::zero();
         }
-        __syncthreads();
         if (tid < PB) {
             const int r = r0 + tid;
-            fakw[s_new + tid] = fakN[tid];
-            dfw[s_new + tid] = dfN[tid];
             T bb = Sc<T>::zero();
             if (fuse && r < n) bb = scale(rhs_entry_b<T>(r, src, A.lsink, A.nsink0, A.dflag, A.dval, bdir), fakN[tid]);
             bsl[s_new + tid] = bb;
         }
-        for (int i = tid; i < PB * W1; i += NT) stage[i] = Sc<T>::zero();
     };
 
     // Initial window: rows 0 .. Wn-1, PB at a time.
     for (int r0 = 0; r0 < Wn; r0 += PB) {
-        stage_rows(r0, 0);
-        __syncthreads();
-        stage_fak(r0);
+        load_rows(r0, 0);
         __syncthreads();
         scatter_rows(r0, r0, 0);
         __syncthreads();
@@ -288,13 +307,12 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
                 if (fuse) yv[i0 + j] = yP[j];
             }
         } else {
-            stage_rows(rnew0, 32);
+            load_rows(rnew0, 32);
         }
         __syncthreads();
         // PROBE0
         if (s_err) break;
         // ---- phase 2: rows below the panel solve against the block
-        stage_fak(rnew0);
         for (int x = tid; x < Wn; x += NT) {
             int dx = x - s0;
             if (dx < 0) dx += Wn;
@@ -321,27 +339,38 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
         }
         __syncthreads();
         // PROBE1
-        // ---- phase 3: trailing update T_xy -= L_x L_y^T on 4 x 4 tiles
+        // ---- phase 3: trailing update T_xy -= L_x L_y^T on 4 x 4 tiles.
+        // The panel occupies tile rows [P0, P0 + PB/4); the panel entries of
+        // the rows of tile row X sit in tiles (X, P) when X follows the panel
+        // in slot order (entry (a, t & 3)) and in tiles (P, X) when it
+        // precedes it (entry (t & 3, a)), so their offsets are hoisted.
         {
-            const int P0 = s0 >> 2, P1 = (s0 + PB) >> 2;   // panel tile rows [P0, P1)
+            constexpr int NPT = PB / 4;
+            const int P0 = s0 >> 2;
             for (int tt = tid; tt < NTT; tt += NT) {
                 const int X = tXY[tt] >> 8, Y = tXY[tt] & 0xff;
-                if ((X >= P0 && X < P1) || (Y >= P0 && Y < P1)) continue;
+                if ((X >= P0 && X < P0 + NPT) || (Y >= P0 && Y < P0 + NPT)) continue;
+                int bx[NPT], by[NPT];
+                const bool xa = X > P0, ya = Y > P0;
+#pragma unroll
+                for (int p = 0; p < NPT; ++p) {
+                    bx[p] = (xa ? tile_base(X, P0 + p) : tile_base(P0 + p, X)) * TSTRIDE;
+                    by[p] = (ya ? tile_base(Y, P0 + p) : tile_base(P0 + p, Y)) * TSTRIDE;
+                }
+                const int xt = xa ? 1 : 4, xs = xa ? 4 : 1, yt = ya ? 1 : 4, ys = ya ? 4 : 1;
                 T acc[16];
                 T* tp = win + tt * TSTRIDE;
 #pragma unroll
                 for (int q = 0; q < 16; ++q) acc[q] = tp[q];
-                for (int t = 0; t < np_; ++t) {
+#pragma unroll
+                for (int t = 0; t < PB; ++t) {
+                    if (t >= np_) break;
+                    const int ox = bx[t >> 2] + (t & 3) * xt, oy = by[t >> 2] + (t & 3) * yt;
                     T px[4], py[4];
 #pragma unroll
-                    for (int a = 0; a < 4; ++a) px[a] = win[widx(4 * X + a, s0 + t)];
-                    if (X == Y) {
+                    for (int a = 0; a < 4; ++a) px[a] = win[ox + a * xs];
 #pragma unroll
-                        for (int a = 0; a < 4; ++a) py[a] = px[a];
-                    } else {
-#pragma unroll
-                        for (int a = 0; a < 4; ++a) py[a] = win[widx(4 * Y + a, s0 + t)];
-                    }
+                    for (int a = 0; a < 4; ++a) py[a] = win[oy + a * ys];
 #pragma unroll
                     for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -361,7 +390,7 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
         __syncthreads();
         // PROBE3
     }
-    if (tid == 0) A.status[sys] = s_err;
+    if (tid == 0 && s_err) A.status[sys] = s_err;
 }
 
 }  // namespace
@@ -384,6 +413,9 @@ bool launch_band_factor_blk(const BandArgs<T>& a, cudaStream_t st)
     int Wn = 0;
     const size_t smem = blk_smem<T, PB>(a.mb, &Wn);
     if (smem > 227 * 1024 || Wn / 4 > 255) return false;
+    const long long rows = (long long)a.nsys * a.n;
+    k_band_prep_diag<T><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(a);
+    k_band_prep_rows<T><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, st>>>(a);
     cudaFuncSetAttribute(k_band_factor_blk<T, PB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_band_factor_blk<T, PB, NT><<<a.nsys, NT, smem, st>>>(a, Wn);
     return true;
