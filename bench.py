@@ -30,6 +30,22 @@ sys.path.insert(0, ROOT)
 
 METRIC = "GN-step wall time, learned-PCG/FP32-refined vs plain CG on B200 at rel-res 1e-6"
 
+# CG iterations of the reference's own iteration (cgfac-preconditioned
+# cjggra) to |r|^2 <= 1e-12 |r0|^2 on each synthetic workload, as counted by
+# the FP64 Jacobi form on the device (whose iteration counts equal the
+# oracle's in the parity tests).  The CPU baseline scales its timed CG
+# sample by this count.
+REF_NCG = {"C5": 1589}
+
+# DRAM bytes (read + write) of the band-factor kernel per complex128 system
+# of the C5 workload, from the ncu capture summarised in profiles/ (a C3
+# launch scaled by n (mb + 1) per system); None until captured.
+FACTOR_TRAFFIC_PER_SYSTEM = None
+
+# FP64 FMA pipe of a B200 SM: 64 FMA per clock (non-tensor), used as the
+# roofline of the FP64 band factorisation.
+FP64_FMA_PER_CLK_SM = 64
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -182,7 +198,9 @@ def cpu_sample(s, ncg: int, budget_s: float, nthreads: int):
       Jacobian : `ni` readings (of nanz) on one thread, scaled by
                  nanz / ni / threads (bsensi is OpenMP over readings);
       CG       : two serial cjggra iterations on `nc` model cells (of manz),
-                 scaled by manz / nc and by the device's CG iteration count."""
+                 scaled by manz / nc and by `ncg`, the iteration count of the
+                 reference's own CG (cgfac-preconditioned cjggra) on the
+                 workload."""
     from oracle.oracle import OracleCG, OracleProblem
     from crtomo_stable_b200.lib import rwaven
     m = s.mesh
@@ -216,7 +234,7 @@ def cpu_sample(s, ncg: int, budget_s: float, nthreads: int):
               f"{le} of {L} source electrodes on {min(K, nthreads)} threads (x{L // le}); bsensi on {ni} of "
               f"{N} readings on 1 thread (/{nthreads} threads); 2 serial cjggra iterations on {nc} of {E} "
               f"cells (x{E / nc:.1f} cells, x{ncg} iterations)")
-    return total, dict(forward_s=t_fwd, jacobian_s=t_sens, cg_s=t_cg, sample=sample)
+    return total, dict(forward_s=t_fwd, jacobian_s=t_sens, cg_s=t_cg, sample=sample, cores=nthreads)
 
 
 def run_reference(args, ws, rank, pg):
@@ -226,7 +244,7 @@ def run_reference(args, ws, rank, pg):
         return
     s = make_problem(args.config)
     nthreads = os.cpu_count() or 1
-    ncg_guess = int(os.environ.get("CRT_REF_NCG", "200"))
+    ncg_guess = int(os.environ.get("CRT_REF_NCG", str(REF_NCG.get(args.config, 200))))
     times = []
     info = {}
     for it in range(args.warmup + args.steps):
@@ -261,6 +279,7 @@ def main():
     E, N = s.mesh.elanz, len(s.strnr)
     n, mb, L = s.mesh.sanz, s.mesh.mb, len(s.enr)
     names = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter"]
+    tnames = Context.TIMING_NAMES
 
     def run_form(precision, steps, warmup, e2e_steps, sample_clocks):
         ctx, dat, wmatd, par0, lam, nb, sm = setup_context(s, local, precision)
@@ -277,14 +296,14 @@ def main():
         if sampler:
             sampler.start()
         launches0 = ctx.launch_count()
-        phase = np.zeros(7)
+        phase = np.zeros(len(tnames))
         step_ms = []
         for _ in range(steps):
             ctx.model_backup(restore=True)
             ncg = ctx.gn_step_device(prm)
             t = ctx.timings()
             step_ms.append(t["total"])
-            phase += np.array([t[k] for k in names + ["total"]])
+            phase += np.array([t[k] for k in tnames])
         launches = (ctx.launch_count() - launches0) // max(steps, 1)
         barrier(pg)
         clocks = sampler.stop() if sampler else None
@@ -308,30 +327,40 @@ def main():
     if args.forms == "both":
         plain = run_form(PREC_FP64, max(1, args.steps // 3), max(1, args.warmup // 3), 0, False)
     t_step, phase, ncg, K = mixed["t"], mixed["phase"], mixed["ncg"], mixed["K"]
+    ph = dict(zip(tnames, [float(x) for x in phase]))
     h2d = E * 16
     d2h = E * 16 + N * 16 + (ncg + 1) * 8 + 8
-    # roofline of the dominant phase
     peak_gbs, peak_kind = load_peaks()
-    dom = names[int(np.argmax(phase[:6]))]
-    roof = None
-    if dom == "cg_iter" and ncg > 0:
-        jbytes = 8  # complex64 Jacobian in the mixed form
-        bytes_it = 2.0 * N * E * jbytes + 6.0 * E * 16 + 3.0 * N * 16
-        ach = bytes_it * ncg / (phase[5] / 1e3) / 1e9
-        roof = {"kernel": "k_cg_jv + k_cg_jhv (J p, J^H W J p; complex64 J)", "bound": "hbm", "achieved": ach,
-                "peak": peak_gbs, "unit": "GB/s", "frac": ach / peak_gbs, "traffic": None,
-                "peak_source": peak_kind, "algorithmic_bytes_per_iteration": bytes_it}
-    else:
-        nsys = K * L
-        bytes_f = nsys * (n * (mb + 1) * 16.0)
-        ach_gbs = bytes_f / (phase[0] / 1e3) / 1e9 if phase[0] > 0 else 0.0
-        roof = {"kernel": f"phase {dom}", "bound": "hbm", "achieved": ach_gbs, "peak": peak_gbs, "unit": "GB/s",
-                "frac": ach_gbs / peak_gbs, "traffic": None, "peak_source": peak_kind}
+    sm_mhz = (mixed["clocks"] or {}).get("sm_max_mhz") or 1965.0
+    # dominant kernel: the FP64 band factorisation, compute-bound on the FP64
+    # pipe.  Algorithmic work per system 4 n mb^2 flops (n mb^2 / 2 complex
+    # MACs of 8 flops); per launch = systems per launch x that.
+    nsys = K * L   # mixed boundaries: one factorisation per (k, l)
+    flops = 4.0 * n * mb * mb * nsys
+    nl = max(ph["factor_launches"], 1.0)
+    t_launch_s = ph["factor_kernel"] / nl / 1e3
+    fp64_peak = FP64_FMA_PER_CLK_SM * 2 * 148 * sm_mhz * 1e6 / 1e12
+    ach = flops / nl / t_launch_s / 1e12 if t_launch_s > 0 else 0.0
+    roof = {"kernel": "k_band_factor_blk<cd,8,256> (complex128 band Cholesky + fused forward substitution)",
+            "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak,
+            "traffic": FACTOR_TRAFFIC_PER_SYSTEM * nsys / nl if FACTOR_TRAFFIC_PER_SYSTEM else None,
+            "traffic_unit": "bytes per launch",
+            "peak_source": "FP64 FMA pipe, 64 FMA/clk/SM x 148 SMs at the max SM clock (no FP64 figure in "
+                           "MEASURED_PEAKS.json)",
+            "algorithmic_flops_per_launch": flops / nl, "launch_ms": t_launch_s * 1e3, "launches": nl}
+    roof_cg = None
+    if ncg > 0:
+        bytes_it = 2.0 * N * E * 8 + 6.0 * E * 16 + 3.0 * N * 16   # J (complex64) read twice + vectors
+        ach_cg = bytes_it * ncg / (ph["cg_iter"] / 1e3) / 1e9
+        roof_cg = {"kernel": "CG iteration (k_cg_jv + k_cg_jhv on the complex64 J, preconditioner apply)",
+                   "bound": "hbm", "achieved": ach_cg, "peak": peak_gbs, "unit": "GB/s", "frac": ach_cg / peak_gbs,
+                   "peak_source": peak_kind, "algorithmic_bytes_per_iteration": bytes_it}
+    ref_ncg = plain["ncg"] if plain is not None else REF_NCG.get(args.config, ncg)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            v, info = cpu_sample(s, ncg, args.cpu_sample_s, os.cpu_count() or 1)
-            cpu = {"value": v, "unit": "s", "cores": os.cpu_count() or 1, "kind": "port", "sample": info["sample"],
+            v, info = cpu_sample(s, ref_ncg, args.cpu_sample_s, os.cpu_count() or 1)
+            cpu = {"value": v, "unit": "s", "cores": info["cores"], "kind": "port", "sample": info["sample"],
                    "phases_s": {k: info[k] for k in ("forward_s", "jacobian_s", "cg_s")}}
         except Exception as exc:  # the baseline must not hide the GPU number
             cpu = {"value": None, "unit": "s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
@@ -350,12 +379,12 @@ def main():
                            "cg_iterations": ncg, "lam": mixed["lam"],
                            "l2": "inputs larger than L2 (J alone is %.1f GB in complex64)" % (N * E * 8 / 1e9),
                            "parallelism": f"replicas x{ws}"},
-                "phases_ms": dict(zip(names + ["total"], [float(x) for x in phase])),
+                "phases_ms": ph,
                 "plain_fp64": None if plain is None else
                 {"value": plain["t"], "unit": "s", "cg_iterations": plain["ncg"],
-                 "phases_ms": dict(zip(names + ["total"], [float(x) for x in plain["phase"]]))},
+                 "phases_ms": dict(zip(tnames, [float(x) for x in plain["phase"]]))},
                 "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "roofline": roof, "cpu_baseline": cpu, "clocks": mixed["clocks"],
+                "roofline": roof, "roofline_cg": roof_cg, "cpu_baseline": cpu, "clocks": mixed["clocks"],
                 "gpu_launches": mixed["launches"]}
         print(json.dumps(line), flush=True)
     if pg is not None:

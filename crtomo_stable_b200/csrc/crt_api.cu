@@ -25,8 +25,8 @@ template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>&, T
 struct crt_ctx {
     int device = 0;
     cudaStream_t st = nullptr;
-    cudaEvent_t ev[8] = {};
-    double timings[7] = {0, 0, 0, 0, 0, 0, 0};
+    cudaEvent_t ev[10] = {};
+    double timings[CRT_NTIMINGS] = {};
     int64_t launches = 0;
     std::string err;
 
@@ -206,6 +206,13 @@ extern "C" int32_t crt_last_timings(const crt_ctx* ctx, double* ms7)
 {
     if (!ctx || !ms7) return CRT_ERR_ARG;
     for (int i = 0; i < 7; ++i) ms7[i] = ctx->timings[i];
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_last_timings_ex(const crt_ctx* ctx, double* ms, int32_t n)
+{
+    if (!ctx || !ms || n < 0) return CRT_ERR_ARG;
+    for (int i = 0; i < n && i < CRT_NTIMINGS; ++i) ms[i] = ctx->timings[i];
     return CRT_OK;
 }
 
@@ -526,7 +533,9 @@ int run_forward(crt_ctx* ctx)
         ctx->chunk = chunk;
     }
     chunk = ctx->chunk;
-    float ms_f = 0, ms_s = 0;
+    float ms_f = 0, ms_s = 0, ms_prep = 0, ms_fk = 0;
+    int nfl = 0;
+    bool blk = false;
     for (int s0 = 0; s0 < nfac; s0 += chunk) {
         const int ns = std::min(chunk, nfac - s0);
         BandArgs<T> A{};
@@ -566,9 +575,20 @@ int run_forward(crt_ctx* ctx)
         {
             const char* fv = std::getenv("CRT_B200_FACTOR");
             const bool force_v0 = fv && std::strcmp(fv, "v0") == 0;
-            if (force_v0 || !launch_band_factor_blk<T>(A, ctx->st)) launch_band_factor<T>(A, ctx->st);
+            if (!force_v0 && band_blk_fits<T>(ctx->mb)) {
+                launch_band_prep<T>(A, ctx->st);
+                CK(cudaEventRecord(ctx->ev[8], ctx->st));
+                launch_band_factor_blk<T>(A, ctx->st);
+                ctx->launches += 3;
+                blk = true;
+            } else {
+                launch_band_factor<T>(A, ctx->st);
+                CK(cudaEventRecord(ctx->ev[8], ctx->st));
+                ctx->launches++;
+                blk = false;
+            }
+            ++nfl;
         }
-        ctx->launches++;
         if (int e = kernel_check(ctx, "band factor")) return e;
         CK(cudaEventRecord(ctx->ev[1], ctx->st));
         SolveArgs<T> S{};
@@ -601,14 +621,20 @@ int run_forward(crt_ctx* ctx)
         if (int e = kernel_check(ctx, "band solve")) return e;
         CK(cudaEventRecord(ctx->ev[2], ctx->st));
         CK(cudaEventSynchronize(ctx->ev[2]));
-        float a = 0, b = 0;
+        float a = 0, b = 0, c = 0;
         cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
         cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&c, ctx->ev[0], ctx->ev[8]);
         ms_f += a;
         ms_s += b;
+        if (blk) ms_prep += c;
+        ms_fk += blk ? a - c : a;
     }
     ctx->timings[0] = ms_f;
     ctx->timings[1] = ms_s;
+    ctx->timings[7] = ms_prep;
+    ctx->timings[8] = ms_fk;
+    ctx->timings[9] = nfl;
     return collect_status(ctx, nfac);
 }
 
@@ -1093,10 +1119,11 @@ int gn_step_device(crt_ctx* ctx, const crt_cg_params* prm, int* ncg)
     CK(cudaEventRecord(t0, ctx->st));
     k_exp_model<<<(ctx->E + 255) / 256, 256, 0, ctx->st>>>(ctx->d_par, ctx->d_sigma, ctx->E);
     ctx->launches++;
-    double tm[7] = {0};
+    double tm[CRT_NTIMINGS] = {0};
     int e = forward_common(ctx, prm->ldc, 0, nullptr);
     if (e) return e;
     for (int i = 0; i < 3; ++i) tm[i] = ctx->timings[i];
+    for (int i = 7; i < 10; ++i) tm[i] = ctx->timings[i];
     e = jacobian_device(ctx, prm->ldc ? 1 : 0, nullptr);
     if (e) return e;
     tm[3] = ctx->timings[3];
@@ -1109,7 +1136,7 @@ int gn_step_device(crt_ctx* ctx, const crt_cg_params* prm, int* ncg)
     float tot = 0;
     cudaEventElapsedTime(&tot, t0, ctx->ev[3]);
     tm[6] = tot;
-    for (int i = 0; i < 7; ++i) ctx->timings[i] = tm[i];
+    for (int i = 0; i < CRT_NTIMINGS; ++i) ctx->timings[i] = tm[i];
     return CRT_OK;
 }
 }  // namespace

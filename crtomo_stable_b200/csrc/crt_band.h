@@ -48,6 +48,11 @@ template <typename T> void launch_band_factor(const BandArgs<T>& a, cudaStream_t
 // Panel-blocked variant; returns false when its window does not fit in
 // shared memory (the caller then uses launch_band_factor).
 template <typename T> bool launch_band_factor_blk(const BandArgs<T>& a, cudaStream_t st);
+// Whether the panel-blocked window fits in shared memory for half-bandwidth mb.
+template <typename T> bool band_blk_fits(int mb);
+// Preparation pass of the panel-blocked factor: assembled, Dirichlet-edited
+// and scaled rows written row-packed into a.Lws, scaling factors into a.fakws.
+template <typename T> void launch_band_prep(const BandArgs<T>& a, cudaStream_t st);
 // scratch: one n-vector per launched system (may alias the fused y workspace).
 template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st);
 template <typename T> size_t band_factor_smem(int W);

@@ -14,18 +14,21 @@
 // two rows is stored once, at the unordered slot pair, in 4 x 4 tiles
 // (tile (X, Y), X >= Y, row-major inside the tile).  Per panel of PB
 // columns [i0, i0 + PB):
-//   1. warp 0 factors the PB x PB diagonal block (unconjugated L L^T, the
-//      recurrence of src/chol.f90:44-78 restricted to the block) and
-//      forward-substitutes the panel's right-hand side; warps 1.. load the
-//      next PB prepared rows into a staging buffer;
 //   2. every window row below the panel solves its PB entries against the
-//      block (L_x = A_x L_D^-T), updates its right-hand side and writes its
-//      L entries to the window and to the column-packed HBM factor;
-//   3. the trailing window is updated by the rank-PB product L_x L_y^T, each
-//      thread accumulating 4 x 4 tiles in registers;
+//      block factor (L_x = A_x L_D^-T), updates its right-hand side and
+//      writes its L entries to the window and to the column-packed HBM
+//      factor;
+//   3a. the entries of the next panel's diagonal tiles receive the panel's
+//      rank-PB update (one entry per thread);
+//   3b. warp 0 factors the next PB x PB diagonal block (unconjugated L L^T,
+//      the recurrence of src/chol.f90:44-78 restricted to the block) and
+//      forward-substitutes its right-hand side, while warps 1.. update the
+//      rest of the trailing window by the rank-PB product L_x L_y^T (each
+//      thread accumulating 4 x 4 tiles in registers) and load the next PB
+//      prepared rows into a staging buffer;
 //   4. the PB staged rows are written into the slots the panel freed.
-// Four CTA barriers per PB columns replace the three per column of the
-// rank-1 variant.
+// The first diagonal block is factored before the loop, so the serial
+// block factorisation overlaps the trailing update of the previous panel.
 #include "crt_band.h"
 
 namespace {
@@ -248,70 +251,84 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
         __syncthreads();
     }
 
+    // Diagonal block of the panel starting at row p0 (warp 0): lane j holds
+    // row j of the block; column t is broadcast through colb[] (shared)
+    // once it is final.  Writes LD, the reciprocal pivots LDi, the panel's
+    // forward-substituted RHS yP and the block's L entries.
+    auto diag_block = [&](int p0) {
+        const int sp = p0 % Wn, npp = min(PB, n - p0);
+        T a[PB];
+        T bj = Sc<T>::zero();
+        const int j = lane;
+        if (j < npp) {
+#pragma unroll
+            for (int t = 0; t < PB; ++t) a[t] = (t <= j && t < npp) ? win[widx(sp + j, sp + t)] : Sc<T>::zero();
+            if (fuse) bj = bsl[sp + j];
+        } else {
+#pragma unroll
+            for (int t = 0; t < PB; ++t) a[t] = Sc<T>::zero();
+        }
+#pragma unroll
+        for (int t = 0; t < PB; ++t) {
+            if (t >= npp) break;
+            if (j == t) {
+                const T piv = a[t];
+                if (Sc<T>::bad_pivot(piv)) s_err = CRT_ERR_PIVOT;
+                T ltt, inv;
+                Sc<T>::sqrt_recip(piv, ltt, inv);
+                a[t] = ltt;
+                LDi[t] = inv;
+                if (fuse) {
+                    bj = Sc<T>::mul(bj, inv);
+                    yP[t] = bj;
+                }
+            }
+            __syncwarp();
+            const T inv = LDi[t];
+            if (j > t && j < npp) {
+                a[t] = Sc<T>::mul(a[t], inv);
+                colb[j] = a[t];
+            }
+            __syncwarp();
+            // rank-1 update of the remaining block columns and the RHS
+#pragma unroll
+            for (int t2 = t + 1; t2 < PB; ++t2)
+                if (j >= t2 && j < npp) fms_acc(a[t2], a[t], colb[t2]);
+            if (fuse && j > t && j < npp) fms_acc(bj, a[t], yP[t]);
+            __syncwarp();
+        }
+        if (j < npp) {
+#pragma unroll
+            for (int t = 0; t < PB; ++t) {
+                if (t <= j) {
+                    LD[j * PB + t] = a[t];
+                    if (j - t <= mb) Lc[(size_t)(p0 + t) * W1 + (j - t)] = a[t];
+                }
+            }
+            if (fuse) yv[p0 + j] = yP[j];
+        }
+    };
+    // Offsets of the panel entries of tile row X: the panel occupies tile
+    // rows [P0, P0 + NPT); the panel entries of the rows of tile row X sit in
+    // tiles (X, P) when X follows the panel in slot order (entry (a, t & 3))
+    // and in tiles (P, X) when it precedes it (entry (t & 3, a)).
+    constexpr int NPT = PB / 4;
+    auto panel_offsets = [&](int X, int P0, int (&bo)[NPT], int& ts, int& as) {
+        const bool after = X > P0;
+#pragma unroll
+        for (int p = 0; p < NPT; ++p) bo[p] = (after ? tile_base(X, P0 + p) : tile_base(P0 + p, X)) * TSTRIDE;
+        ts = after ? 1 : 4;
+        as = after ? 4 : 1;
+    };
+
+    if (warp == 0) diag_block(0);
+    __syncthreads();
     for (int i0 = 0; i0 < n; i0 += PB) {
+        if (s_err) break;
         const int s0 = i0 % Wn;
         const int np_ = min(PB, n - i0);
         const int rnew0 = i0 + Wn;
-        // ---- phase 1: diagonal block (warp 0) | next rows (warps 1..)
-        if (warp == 0) {
-            // lane j holds row j of the diagonal block; column t is broadcast
-            // through colb[] (shared) once it is final
-            T a[PB];
-            T bj = Sc<T>::zero();
-            const int j = lane;
-            if (j < np_) {
-#pragma unroll
-                for (int t = 0; t < PB; ++t) a[t] = (t <= j && t < np_) ? win[widx(s0 + j, s0 + t)] : Sc<T>::zero();
-                if (fuse) bj = bsl[s0 + j];
-            } else {
-#pragma unroll
-                for (int t = 0; t < PB; ++t) a[t] = Sc<T>::zero();
-            }
-#pragma unroll
-            for (int t = 0; t < PB; ++t) {
-                if (t >= np_) break;
-                if (j == t) {
-                    const T piv = a[t];
-                    if (Sc<T>::bad_pivot(piv)) s_err = CRT_ERR_PIVOT;
-                    const T ltt = Sc<T>::sqrt_fast(piv);
-                    const T inv = Sc<T>::recip(ltt);
-                    a[t] = ltt;
-                    LDi[t] = inv;
-                    if (fuse) {
-                        bj = Sc<T>::mul(bj, inv);
-                        yP[t] = bj;
-                    }
-                }
-                __syncwarp();
-                const T inv = LDi[t];
-                if (j > t && j < np_) {
-                    a[t] = Sc<T>::mul(a[t], inv);
-                    colb[j] = a[t];
-                }
-                __syncwarp();
-                // rank-1 update of the remaining block columns and the RHS
-#pragma unroll
-                for (int t2 = t + 1; t2 < PB; ++t2)
-                    if (j >= t2 && j < np_) a[t2] -= Sc<T>::mul(a[t], colb[t2]);
-                if (fuse && j > t && j < np_) bj -= Sc<T>::mul(a[t], yP[t]);
-                __syncwarp();
-            }
-            if (j < np_) {
-#pragma unroll
-                for (int t = 0; t < PB; ++t) {
-                    if (t <= j) {
-                        LD[j * PB + t] = a[t];
-                        if (j - t <= mb) Lc[(size_t)(i0 + t) * W1 + (j - t)] = a[t];
-                    }
-                }
-                if (fuse) yv[i0 + j] = yP[j];
-            }
-        } else {
-            load_rows(rnew0, 32);
-        }
-        __syncthreads();
-        // PROBE0
-        if (s_err) break;
+        const int P0 = s0 >> 2;
         // ---- phase 2: rows below the panel solve against the block
         for (int x = tid; x < Wn; x += NT) {
             int dx = x - s0;
@@ -328,9 +345,9 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
                 if (t >= np_) break;
                 T s = lx[t];
 #pragma unroll
-                for (int t2 = 0; t2 < t; ++t2) s -= Sc<T>::mul(lx[t2], LD[t * PB + t2]);
+                for (int t2 = 0; t2 < t; ++t2) fms_acc(s, lx[t2], LD[t * PB + t2]);
                 lx[t] = Sc<T>::mul(s, LDi[t]);
-                if (fuse) bx -= Sc<T>::mul(lx[t], yP[t]);
+                if (fuse) fms_acc(bx, lx[t], yP[t]);
                 win[widx(x, s0 + t)] = lx[t];
                 const int d = r - (i0 + t);
                 if (d <= mb) Lc[(size_t)(i0 + t) * W1 + d] = lx[t];
@@ -338,50 +355,77 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
             if (fuse) bsl[x] = bx;
         }
         __syncthreads();
-        // PROBE1
-        // ---- phase 3: trailing update T_xy -= L_x L_y^T on 4 x 4 tiles.
-        // The panel occupies tile rows [P0, P0 + PB/4); the panel entries of
-        // the rows of tile row X sit in tiles (X, P) when X follows the panel
-        // in slot order (entry (a, t & 3)) and in tiles (P, X) when it
-        // precedes it (entry (t & 3, a)), so their offsets are hoisted.
-        {
-            constexpr int NPT = PB / 4;
-            const int P0 = s0 >> 2;
-            for (int tt = tid; tt < NTT; tt += NT) {
-                const int X = tXY[tt] >> 8, Y = tXY[tt] & 0xff;
-                if ((X >= P0 && X < P0 + NPT) || (Y >= P0 && Y < P0 + NPT)) continue;
-                int bx[NPT], by[NPT];
-                const bool xa = X > P0, ya = Y > P0;
-#pragma unroll
-                for (int p = 0; p < NPT; ++p) {
-                    bx[p] = (xa ? tile_base(X, P0 + p) : tile_base(P0 + p, X)) * TSTRIDE;
-                    by[p] = (ya ? tile_base(Y, P0 + p) : tile_base(P0 + p, Y)) * TSTRIDE;
-                }
-                const int xt = xa ? 1 : 4, xs = xa ? 4 : 1, yt = ya ? 1 : 4, ys = ya ? 4 : 1;
-                T acc[16];
-                T* tp = win + tt * TSTRIDE;
-#pragma unroll
-                for (int q = 0; q < 16; ++q) acc[q] = tp[q];
+        // PROBE0
+        // ---- phase 3a: the trailing update of the next panel's diagonal
+        // tiles, one entry per thread, so that its block can be factored
+        // while the rest of the window is updated.
+        const int inext = i0 + PB;
+        const bool has_next = inext < n;
+        const int P0n = (inext % Wn) >> 2;
+        if (has_next) {
+            constexpr int NDT = NPT * (NPT + 1) / 2;
+            for (int i = tid; i < NDT * 16; i += NT) {
+                const int kt = i >> 4, q = i & 15;
+                int xo = 0;
+                while ((xo + 1) * (xo + 2) / 2 <= kt) ++xo;
+                const int yo = kt - xo * (xo + 1) / 2;
+                const int X = P0n + xo, Y = P0n + yo, a = q >> 2, c = q & 3;
+                if (X == Y && a < c) continue;
+                int bx[NPT], by[NPT], xt, xs, yt, ys;
+                panel_offsets(X, P0, bx, xt, xs);
+                panel_offsets(Y, P0, by, yt, ys);
+                T* tp = win + tile_base(X, Y) * TSTRIDE + q;
+                T acc = *tp;
 #pragma unroll
                 for (int t = 0; t < PB; ++t) {
                     if (t >= np_) break;
-                    const int ox = bx[t >> 2] + (t & 3) * xt, oy = by[t >> 2] + (t & 3) * yt;
-                    T px[4], py[4];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) px[a] = win[ox + a * xs];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) py[a] = win[oy + a * ys];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) acc[a * 4 + c] -= Sc<T>::mul(px[a], py[c]);
+                    fms_acc(acc, win[bx[t >> 2] + (t & 3) * xt + a * xs], win[by[t >> 2] + (t & 3) * yt + c * ys]);
                 }
+                *tp = acc;
+            }
+        }
+        __syncthreads();
+        // PROBE1
+        // ---- phase 3b: warp 0 factors the next diagonal block; warps 1..
+        // update the rest of the window by the rank-PB product L_x L_y^T on
+        // 4 x 4 tiles and then load the next PB prepared rows.
+        if (warp == 0) {
+            if (has_next) diag_block(inext);
+        } else {
+            if (has_next) {
+                for (int tt = tid - 32; tt < NTT; tt += NT - 32) {
+                    const int X = tXY[tt] >> 8, Y = tXY[tt] & 0xff;
+                    if ((X >= P0 && X < P0 + NPT) || (Y >= P0 && Y < P0 + NPT)) continue;
+                    if (X >= P0n && X < P0n + NPT && Y >= P0n && Y < P0n + NPT) continue;   // done in 3a
+                    int bx[NPT], by[NPT], xt, xs, yt, ys;
+                    panel_offsets(X, P0, bx, xt, xs);
+                    panel_offsets(Y, P0, by, yt, ys);
+                    T acc[16];
+                    T* tp = win + tt * TSTRIDE;
 #pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    if (X == Y && (q >> 2) < (q & 3)) continue;   // upper half of a diagonal tile is unused
-                    tp[q] = acc[q];
+                    for (int q = 0; q < 16; ++q) acc[q] = tp[q];
+#pragma unroll
+                    for (int t = 0; t < PB; ++t) {
+                        if (t >= np_) break;
+                        const int ox = bx[t >> 2] + (t & 3) * xt, oy = by[t >> 2] + (t & 3) * yt;
+                        T px[4], py[4];
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) px[a] = win[ox + a * xs];
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) py[a] = win[oy + a * ys];
+#pragma unroll
+                        for (int a = 0; a < 4; ++a)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) fms_acc(acc[a * 4 + c], px[a], py[c]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) {
+                        if (X == Y && (q >> 2) < (q & 3)) continue;   // upper half of a diagonal tile is unused
+                        tp[q] = acc[q];
+                    }
                 }
             }
+            load_rows(rnew0, 32);
         }
         __syncthreads();
         // PROBE2
@@ -407,19 +451,36 @@ static size_t blk_smem(int mb, int* Wn_out)
 }
 
 template <typename T>
+bool band_blk_fits(int mb)
+{
+    int Wn = 0;
+    const size_t smem = blk_smem<T, 8>(mb, &Wn);
+    return smem <= 227 * 1024 && Wn / 4 <= 255;
+}
+
+template <typename T>
+void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
+{
+    const long long rows = (long long)a.nsys * a.n;
+    k_band_prep_diag<T><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(a);
+    k_band_prep_rows<T><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, st>>>(a);
+}
+
+template <typename T>
 bool launch_band_factor_blk(const BandArgs<T>& a, cudaStream_t st)
 {
     constexpr int NT = 256, PB = 8;
     int Wn = 0;
     const size_t smem = blk_smem<T, PB>(a.mb, &Wn);
-    if (smem > 227 * 1024 || Wn / 4 > 255) return false;
-    const long long rows = (long long)a.nsys * a.n;
-    k_band_prep_diag<T><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(a);
-    k_band_prep_rows<T><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, st>>>(a);
+    if (!band_blk_fits<T>(a.mb)) return false;
     cudaFuncSetAttribute(k_band_factor_blk<T, PB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_band_factor_blk<T, PB, NT><<<a.nsys, NT, smem, st>>>(a, Wn);
     return true;
 }
 
+template bool band_blk_fits<double>(int);
+template bool band_blk_fits<cd>(int);
+template void launch_band_prep<double>(const BandArgs<double>&, cudaStream_t);
+template void launch_band_prep<cd>(const BandArgs<cd>&, cudaStream_t);
 template bool launch_band_factor_blk<double>(const BandArgs<double>&, cudaStream_t);
 template bool launch_band_factor_blk<cd>(const BandArgs<cd>&, cudaStream_t);

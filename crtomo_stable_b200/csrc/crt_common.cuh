@@ -11,6 +11,9 @@
 
 #define CRT_HD __host__ __device__ __forceinline__
 
+// entries of crt_last_timings_ex
+#define CRT_NTIMINGS 10
+
 struct __align__(16) cd {
     double x, y;
 };
@@ -69,6 +72,12 @@ template <> struct Sc<double> {
     static CRT_HD double sqrt_(double a) { return sqrt(a); }
     static CRT_HD double sqrt_fast(double a) { return sqrt(a); }
     static CRT_HD bool bad_pivot(double s) { return !(s > 0.0); }
+    // root = sqrt(z) and inv = 1 / root from one reciprocal square root
+    static __device__ __forceinline__ void sqrt_recip(double z, double& root, double& inv)
+    {
+        inv = rsqrt(z);
+        root = z * inv;
+    }
     static CRT_HD double mul(double a, double b) { return a * b; }
     static CRT_HD double div(double a, double b) { return a / b; }
     static CRT_HD double recip(double a) { return 1.0 / a; }
@@ -93,6 +102,24 @@ template <> struct Sc<cd> {
         return cd{fabs(z.y) * h, copysign(t, z.y)};
     }
     static CRT_HD bool bad_pivot(cd s) { return !(s.x * s.x + s.y * s.y > 0.0); }
+    // Principal root of z and its reciprocal from two reciprocal square
+    // roots and no division: with r = |z|, t = sqrt((r + |Re z|)/2) the root
+    // is (t, Im z/(2t)) or (|Im z|/(2t), copysign(t, Im z)), and since
+    // |root|^2 = r, 1/root = conj(root)/r.
+    static __device__ __forceinline__ void sqrt_recip(cd z, cd& root, cd& inv)
+    {
+        const double r2 = z.x * z.x + z.y * z.y;
+        if (!(r2 > 0.0)) {
+            root = cd{0.0, 0.0};
+            inv = cd{0.0, 0.0};
+            return;
+        }
+        const double ir = rsqrt(r2), r = r2 * ir;
+        const double u = 0.5 * (r + fabs(z.x));
+        const double iu = rsqrt(u), t = u * iu, h = 0.5 * iu;
+        root = z.x >= 0.0 ? cd{t, z.y * h} : cd{fabs(z.y) * h, copysign(t, z.y)};
+        inv = cd{root.x * ir, -root.y * ir};
+    }
     static CRT_HD cd mul(cd a, cd b) { return a * b; }
     static CRT_HD cd div(cd a, cd b) { return cdiv(a, b); }
     // 1/a = conj(a) / |a|^2 (the pivots are of order one after scaling)
@@ -103,6 +130,16 @@ template <> struct Sc<cd> {
     }
     static CRT_HD cd to_cd(cd a) { return a; }
 };
+
+// acc -= a * b as fused multiply-adds (4 for complex operands, 1 for real)
+CRT_HD void fms_acc(cd& acc, cd a, cd b)
+{
+    acc.x = fma(-a.x, b.x, acc.x);
+    acc.x = fma(a.y, b.y, acc.x);
+    acc.y = fma(-a.x, b.y, acc.y);
+    acc.y = fma(-a.y, b.x, acc.y);
+}
+CRT_HD void fms_acc(double& acc, double a, double b) { acc = fma(-a, b, acc); }
 
 CRT_HD double scale(double a, double s) { return a * s; }
 CRT_HD cd scale(cd a, double s) { return cd{a.x * s, a.y * s}; }

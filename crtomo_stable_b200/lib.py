@@ -66,7 +66,7 @@ EXPORTS = [
     "crt_forward", "crt_potentials", "crt_jacobian", "crt_set_jacobian", "crt_set_regularizer",
     "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
-    "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order",
+    "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order", "crt_last_timings_ex",
 ]
 
 _LIB = None
@@ -122,6 +122,8 @@ def load(path: str = LIB_PATH):
     L.crt_gn_step_device.restype = C.c_int32
     L.crt_last_timings.argtypes = [vp, f64p]
     L.crt_last_timings.restype = C.c_int32
+    L.crt_last_timings_ex.argtypes = [vp, f64p, C.c_int32]
+    L.crt_last_timings_ex.restype = C.c_int32
     L.crt_cg_info.argtypes = [vp, i32p, i32p, i32p]
     L.crt_cg_info.restype = C.c_int32
     L.crt_rcm_order.argtypes = [C.c_int32, i32p, i32p, i32p, i32p]
@@ -382,10 +384,13 @@ class Context:
         self._check(self.L.crt_gn_step_device(self.h, C.byref(prm), C.byref(ncg)), "crt_gn_step_device")
         return ncg.value
 
+    TIMING_NAMES = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total", "factor_prep",
+                    "factor_kernel", "factor_launches"]
+
     def timings(self):
-        t = np.zeros(7)
-        self.L.crt_last_timings(self.h, _ptr(t, C.c_double))
-        return dict(zip(["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total"], t))
+        t = np.zeros(len(self.TIMING_NAMES))
+        self._check(self.L.crt_last_timings_ex(self.h, _ptr(t, C.c_double), len(t)), "crt_last_timings_ex")
+        return dict(zip(self.TIMING_NAMES, t))
 
     def launch_count(self):
         return int(self.L.crt_launch_count(self.h))

@@ -194,6 +194,13 @@ int32_t crt_model_backup(crt_ctx *ctx, int32_t restore);
  * iterations, [6] total. */
 int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
 
+/* The same and more, up to n entries: [0..6] as crt_last_timings, [7] the
+ * preparation pass of the forward factor (assembly, Dirichlet edits and
+ * scaling of all rows), [8] the factor kernels alone, [9] the number of
+ * factor-kernel launches (one per chunk of systems).  Milliseconds except
+ * [9].  No reference counterpart. */
+int32_t crt_last_timings_ex(const crt_ctx *ctx, double *ms, int32_t n);
+
 /* Kernel launches enqueued by the context since creation. */
 int64_t crt_launch_count(const crt_ctx *ctx);
 
