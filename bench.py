@@ -37,10 +37,11 @@ METRIC = "GN-step wall time, learned-PCG/FP32-refined vs plain CG on B200 at rel
 # sample by this count.
 REF_NCG = {"C5": 1589}
 
-# DRAM bytes (read + write) of the band-factor kernel per complex128 system
-# of the C5 workload, from the ncu capture summarised in profiles/ (a C3
-# launch scaled by n (mb + 1) per system); None until captured.
-FACTOR_TRAFFIC_PER_SYSTEM = None
+# DRAM bytes (read + write) of the band-factor kernel per band entry
+# n (mb + 1) of a complex128 system, from the ncu capture in
+# profiles/k_band_factor_blk_C3.md (4.186 GB for 63 C3 systems: the prepared
+# matrix read once and L written once).
+FACTOR_TRAFFIC_BYTES_PER_ENTRY = 31.8
 
 # FP64 FMA pipe of a B200 SM: 64 FMA per clock (non-tensor), used as the
 # roofline of the FP64 band factorisation.
@@ -343,8 +344,8 @@ def main():
     ach = flops / nl / t_launch_s / 1e12 if t_launch_s > 0 else 0.0
     roof = {"kernel": "k_band_factor_blk<cd,8,256> (complex128 band Cholesky + fused forward substitution)",
             "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak,
-            "traffic": FACTOR_TRAFFIC_PER_SYSTEM * nsys / nl if FACTOR_TRAFFIC_PER_SYSTEM else None,
-            "traffic_unit": "bytes per launch",
+            "traffic": FACTOR_TRAFFIC_BYTES_PER_ENTRY * n * (mb + 1) * nsys / nl,
+            "traffic_unit": "bytes per launch (ncu dram read + write on C3, scaled by n (mb + 1) per system)",
             "peak_source": "FP64 FMA pipe, 64 FMA/clk/SM x 148 SMs at the max SM clock (no FP64 figure in "
                            "MEASURED_PEAKS.json)",
             "algorithmic_flops_per_launch": flops / nl, "launch_ms": t_launch_s * 1e3, "launches": nl}

@@ -225,15 +225,17 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     // are written by those rows.
     auto scatter_rows = [&](int r0, int s_new, int wlo) {
         const int wm = wlo % Wn;
-        for (int i = tid; i < PB * Wn; i += NT) {
-            const int q = i / Wn, y = i % Wn;
-            const int r = r0 + q;
+        for (int y = tid; y < Wn; y += NT) {
             int off = y - wm;
             if (off < 0) off += Wn;
             const int c = wlo + off;                      // row held by slot y
-            if (c > r) continue;
-            const int d = r - c;
-            win[widx(s_new + q, y)] = (r < n && d <= mb) ? stage[q * W1 + d] : Sc<T>::zero();
+#pragma unroll
+            for (int q = 0; q < PB; ++q) {
+                const int r = r0 + q;
+                if (c > r) continue;
+                const int d = r - c;
+                win[widx(s_new + q, y)] = (r < n && d <= mb) ? stage[q * W1 + d] : Sc<T>::zero();
+            }
         }
         if (tid < PB) {
             const int r = r0 + tid;
