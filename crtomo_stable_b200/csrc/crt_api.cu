@@ -18,6 +18,7 @@
 #include "crt_sens.h"
 #include "crt_setup.h"
 #include "crt_spc.h"
+#include "crt_gnn.h"
 #include "crt_volt.h"
 
 template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>&, T*, cudaStream_t);
@@ -84,8 +85,12 @@ struct crt_ctx {
     // block preconditioner of the CG (built with the regulariser)
     SpcPlan spc;
     std::string spc_why;
-    cd *d_z = nullptr, *d_rold = nullptr;
-    int cg_form = 0;      // form of the last CG: 0 Jacobi (cgfac), 1 block preconditioner
+    cd *d_z = nullptr, *d_rold = nullptr, *d_zb = nullptr;
+    CGState* d_live = nullptr;   // a never-done CG state for preconditioner applications outside the CG
+    int cg_form = 0;      // form of the last CG: CRT_PRECOND_*
+    // learned correction of the preconditioner
+    Gnn gnn;
+    int gnn_guard = 0;   // the last solve switched the learned correction off
     int prec = CRT_PREC_FP64;
 };
 
@@ -239,10 +244,11 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold};
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     spc_plan_free(ctx->spc);
+    gnn_free(ctx->gnn);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -898,6 +904,11 @@ extern "C" int32_t crt_set_regularizer(crt_ctx* ctx, int32_t ltri, int32_t nx, i
     ctx->spc_why.clear();
     if (int e = spc_plan_build(ctx->spc, M, ltri, nx, nnb, smatm, nachbar, ctx->spc_why))
         return set_err(ctx, e, "block preconditioner set-up failed");
+    // learned correction: same graph; a graph it cannot hold (more than four
+    // neighbours, not symmetric) leaves it unavailable, which is not an error
+    const int ge = gnn_setup(ctx->gnn, M, ltri, nx, nnb, nachbar);
+    if (ge == CRT_ERR_ALLOC || ge == CRT_ERR_CUDA) return set_err(ctx, ge, "learned preconditioner set-up failed");
+    if (ctx->gnn.ready && gnn_init(ctx->gnn, 1)) return set_err(ctx, CRT_ERR_CUDA, "learned preconditioner init");
     return CRT_OK;
 }
 
@@ -928,8 +939,10 @@ int ensure_cg_buffers(crt_ctx* ctx, int ncgmax)
                   dalloc(ctx, &ctx->d_ap, (size_t)N) && dalloc(ctx, &ctx->d_cgpart, (size_t)nsplit * N) &&
                   dalloc(ctx, &ctx->d_cgst, (size_t)1) && dalloc(ctx, &ctx->d_bdpar, (size_t)1) &&
                   dalloc(ctx, &ctx->d_par, (size_t)M) && dalloc(ctx, &ctx->d_z, (size_t)M) &&
-                  dalloc(ctx, &ctx->d_rold, (size_t)M);
+                  dalloc(ctx, &ctx->d_rold, (size_t)M) && dalloc(ctx, &ctx->d_zb, (size_t)M) &&
+                  dalloc(ctx, &ctx->d_live, (size_t)1);
         if (!ok) return CRT_ERR_ALLOC;
+        if (cudaMemset(ctx->d_live, 0, sizeof(CGState)) != cudaSuccess) return CRT_ERR_CUDA;
     }
     if (ctx->cg_ncgmax_alloc < ncgmax + 2) {
         if (!dalloc(ctx, &ctx->d_cgres, (size_t)ncgmax + 2)) return CRT_ERR_ALLOC;
@@ -969,7 +982,38 @@ CGArgs make_cg_args(crt_ctx* ctx, const crt_cg_params* prm)
     a.pc = 0;
     a.z = ctx->d_z;
     a.rold = ctx->d_rold;
+    a.pc_gnn = 0;
+    a.zb = nullptr;
     return a;
+}
+
+// Block factor and / or message weights of the learned correction for the
+// system whose cgfac was just formed.  A requested piece that is not
+// available (bandwidth, pivot breakdown, untrained network, network trained
+// on the other base) is left out, down to the Jacobi form.
+int prepare_preconditioner(crt_ctx* ctx, const crt_cg_params* prm, bool* use_block, bool* use_gnn)
+{
+    const int pc = prm->precond;
+    *use_block = false;
+    *use_gnn = false;
+    if ((pc == CRT_PRECOND_BLOCK || pc == CRT_PRECOND_BLOCK_GNN) && ctx->spc.ok) {
+        // S from cgfac and lam, factored once per update; a breakdown
+        // (non-positive pivot) drops the block part
+        launch_spc_factor(ctx->spc, ctx->d_cgfac, ctx->d_smatm, prm->lam, ctx->st);
+        ctx->launches += 3 + (ctx->spc.nb > 1 ? 1 : 0);
+        int flag = 0;
+        CK(cudaMemcpyAsync(&flag, ctx->spc.d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (int e = kernel_check(ctx, "block preconditioner factor")) return e;
+        *use_block = flag == 0;
+    }
+    if ((pc == CRT_PRECOND_GNN || pc == CRT_PRECOND_BLOCK_GNN) && ctx->gnn.ready && ctx->gnn.trained &&
+        ctx->gnn.form == (*use_block ? 1 : 0)) {
+        launch_gnn_edges(ctx->gnn, ctx->d_cgfac, ctx->d_smatm, prm->lam, ctx->st);
+        ctx->launches++;
+        *use_gnn = true;
+    }
+    return CRT_OK;
 }
 
 // update.f90 on device-resident J, data, response and model (d_par).
@@ -984,18 +1028,13 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
     launch_cg_setup(a, ctx->d_dat, d_sigmaa, ctx->d_par, ctx->st);
     ctx->launches += 1;
-    if (prm->precond == CRT_PRECOND_BLOCK && ctx->spc.ok) {
-        // S from cgfac and lam, factored once per update; a breakdown
-        // (non-positive pivot) falls back to the Jacobi form
-        launch_spc_factor(ctx->spc, ctx->d_cgfac, ctx->d_smatm, prm->lam, ctx->st);
-        ctx->launches += 3 + (ctx->spc.nb > 1 ? 1 : 0);
-        int flag = 0;
-        CK(cudaMemcpyAsync(&flag, ctx->spc.d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
-        if (int e = kernel_check(ctx, "block preconditioner factor")) return e;
-        a.pc = flag == 0 ? 1 : 0;
-    }
-    ctx->cg_form = a.pc;
+    bool use_block = false, use_gnn = false;
+    if (int e = prepare_preconditioner(ctx, prm, &use_block, &use_gnn)) return e;
+    a.pc = (use_block || use_gnn) ? 1 : 0;
+    a.pc_gnn = use_gnn ? 1 : 0;
+    a.zb = (use_block && use_gnn) ? ctx->d_zb : nullptr;
+    ctx->cg_form = use_block ? (use_gnn ? CRT_PRECOND_BLOCK_GNN : CRT_PRECOND_BLOCK)
+                             : (use_gnn ? CRT_PRECOND_GNN : CRT_PRECOND_JACOBI);
     launch_cg_init(a, ctx->st);
     ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
@@ -1006,8 +1045,9 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
     const int batch = 16;
     while (done_iters < prm->ncgmax) {
         int it = std::min(batch, prm->ncgmax - done_iters);
-        launch_cg_iterations(a, it, &ctx->spc, ctx->st);
-        ctx->launches += (a.pc ? 7 : 5) * it;
+        launch_cg_iterations(a, it, use_block ? &ctx->spc : nullptr, use_gnn ? &ctx->gnn : nullptr, ctx->d_zb,
+                             ctx->st);
+        ctx->launches += (5 + (a.pc ? 1 : 0) + (use_block ? 2 : 0) + (use_gnn ? 7 : 0)) * it;
         done_iters += it;
         CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
@@ -1026,6 +1066,7 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
     CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     if (ncg_out) *ncg_out = hs.ncg;
+    ctx->gnn_guard = use_gnn ? hs.no_gnn : 0;
     return CRT_OK;
 }
 
@@ -1207,4 +1248,248 @@ extern "C" double crt_dmisft(int32_t nanz, const double* dat, const double* sigm
     if (betrms) *betrms = std::sqrt(br / ok);
     if (pharms) *pharms = std::sqrt(ph / ok);
     return std::sqrt(nrm / ok);
+}
+
+// ---------------------------------------------------------------------------
+// Learned correction of the CG preconditioner (no reference counterpart).
+
+extern "C" int32_t crt_gnn_nparam(void) { return GNN_NPARAM; }
+
+extern "C" int32_t crt_gnn_status(const crt_ctx* ctx, int32_t* available, int32_t* trained, int32_t* form,
+                                  int32_t* nrec, int32_t* guard_fired)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    if (available) *available = ctx->gnn.ready;
+    if (trained) *trained = ctx->gnn.trained;
+    if (form) *form = ctx->gnn.form;
+    if (nrec) *nrec = (int32_t)ctx->gnn.recs.size();
+    if (guard_fired) *guard_fired = ctx->gnn_guard;
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_gnn_init(crt_ctx* ctx, uint64_t seed)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    if (!ctx->gnn.ready) return set_err(ctx, CRT_ERR_UNSUPPORTED, "learned preconditioner unavailable (regulariser)");
+    CK(cudaSetDevice(ctx->device));
+    if (gnn_init(ctx->gnn, seed)) return set_err(ctx, CRT_ERR_CUDA, "learned preconditioner init");
+    ctx->gnn.trained = 0;
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_gnn_set_weights(crt_ctx* ctx, const float* w, int32_t n, int32_t form)
+{
+    if (!ctx || !w || n != GNN_NPARAM || (form != 0 && form != 1)) return CRT_ERR_ARG;
+    if (!ctx->gnn.ready) return set_err(ctx, CRT_ERR_UNSUPPORTED, "learned preconditioner unavailable (regulariser)");
+    CK(cudaSetDevice(ctx->device));
+    if (gnn_set_weights(ctx->gnn, w)) return set_err(ctx, CRT_ERR_CUDA, "learned preconditioner weights");
+    ctx->gnn.trained = 1;
+    ctx->gnn.form = form;
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_gnn_get_weights(crt_ctx* ctx, float* w, int32_t n, int32_t* form)
+{
+    if (!ctx || !w || n != GNN_NPARAM) return CRT_ERR_ARG;
+    if (!ctx->gnn.ready) return set_err(ctx, CRT_ERR_UNSUPPORTED, "learned preconditioner unavailable (regulariser)");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemcpy(w, ctx->gnn.d_w, GNN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost));
+    if (form) *form = ctx->gnn.form;
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_gnn_clear(crt_ctx* ctx)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    for (auto& r : ctx->gnn.recs) {
+        cudaFree(r.x);
+        cudaFree(r.t);
+    }
+    for (float* p : ctx->gnn.edge_sets) cudaFree(p);
+    ctx->gnn.recs.clear();
+    ctx->gnn.edge_sets.clear();
+    return CRT_OK;
+}
+
+// Runs the plain (Jacobi-form) CG of the current Gauss-Newton system -- the
+// Jacobian, data, response and model already on the device, as for
+// crt_update -- and records every `stride` iterations the residual r_k and
+// the iterate x_k; after convergence each record becomes the pair
+// (r_k, e_k = x* - x_k) with its base b_k (r_k, or S^-1 r_k when base_block).
+// The model is not changed.
+extern "C" int32_t crt_gnn_collect(crt_ctx* ctx, const crt_cg_params* prm, int32_t base_block, int32_t stride,
+                                   int32_t nmax, int32_t* nrec)
+{
+    if (!ctx || !prm || stride < 1 || nmax < 1) return CRT_ERR_ARG;
+    Gnn& G = ctx->gnn;
+    if (!G.ready) return set_err(ctx, CRT_ERR_UNSUPPORTED, "learned preconditioner unavailable (regulariser)");
+    if (ctx->ltri < 0) return set_err(ctx, CRT_ERR_ARG, "regulariser not set (crt_set_regularizer)");
+    if (!ctx->d_dat) return set_err(ctx, CRT_ERR_ARG, "data not set (crt_set_data)");
+    if (!ctx->have_sens) return set_err(ctx, CRT_ERR_ARG, "no Jacobian (crt_jacobian / crt_set_jacobian)");
+    if (!ctx->have_forward || !ctx->d_par) return set_err(ctx, CRT_ERR_ARG, "no forward response / model");
+    if (prm->ldc != ctx->sens_real) return set_err(ctx, CRT_ERR_ARG, "ldc does not match the Jacobian type");
+    if (!G.recs.empty() && G.form != (base_block ? 1 : 0))
+        return set_err(ctx, CRT_ERR_ARG, "records of the other base exist (crt_gnn_clear first)");
+    if (base_block && !ctx->spc.ok) return set_err(ctx, CRT_ERR_UNSUPPORTED, "block preconditioner unavailable");
+    CK(cudaSetDevice(ctx->device));
+    if (int e = ensure_cg_buffers(ctx, prm->ncgmax)) return e;
+    const int M = ctx->E;
+    CGArgs a = make_cg_args(ctx, prm);
+    launch_cg_setup(a, ctx->d_dat, ctx->d_sigmaa, ctx->d_par, ctx->st);
+    if (base_block) {
+        launch_spc_factor(ctx->spc, ctx->d_cgfac, ctx->d_smatm, prm->lam, ctx->st);
+        int flag = 0;
+        CK(cudaMemcpyAsync(&flag, ctx->spc.d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (flag) return set_err(ctx, CRT_ERR_PIVOT, "block preconditioner breakdown");
+    }
+    launch_gnn_edges(G, ctx->d_cgfac, ctx->d_smatm, prm->lam, ctx->st);
+    float* edges = nullptr;
+    CK(cudaMalloc(&edges, (size_t)M * GNN_D * sizeof(float)));
+    CK(cudaMemcpyAsync(edges, G.d_a, (size_t)M * GNN_D * sizeof(float), cudaMemcpyDeviceToDevice, ctx->st));
+    launch_cg_init(a, ctx->st);
+    cd* raw = nullptr;   // [nmax][2][M]: r_k, x_k
+    if (cudaMalloc(&raw, (size_t)nmax * 2 * M * sizeof(cd)) != cudaSuccess) {
+        cudaFree(edges);
+        return set_err(ctx, CRT_ERR_ALLOC, "record buffers");
+    }
+    int nraw = 0, it = 0;
+    CGState hs{};
+    while (it < prm->ncgmax) {
+        launch_cg_iterations(a, 1, nullptr, nullptr, nullptr, ctx->st);
+        ++it;
+        if (it % stride == 0 || it % 16 == 0) {
+            CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            if (hs.done) break;
+            if (it % stride == 0 && nraw < nmax) {
+                CK(cudaMemcpyAsync(raw + (size_t)nraw * 2 * M, ctx->d_r, M * sizeof(cd), cudaMemcpyDeviceToDevice,
+                                   ctx->st));
+                CK(cudaMemcpyAsync(raw + (size_t)nraw * 2 * M + M, ctx->d_dpar, M * sizeof(cd),
+                                   cudaMemcpyDeviceToDevice, ctx->st));
+                ++nraw;
+            }
+        }
+    }
+    if (int e = kernel_check(ctx, "record CG")) {
+        cudaFree(raw);
+        cudaFree(edges);
+        return e;
+    }
+    const int sys = (int)G.edge_sets.size();
+    G.edge_sets.push_back(edges);
+    for (int k = 0; k < nraw; ++k) {
+        const cd* rk = raw + (size_t)k * 2 * M;
+        const cd* xk = rk + M;
+        const cd* bk = nullptr;
+        if (base_block) {
+            launch_spc_apply(ctx->spc, rk, ctx->d_zb, ctx->d_live, ctx->st);
+            bk = ctx->d_zb;
+        }
+        GnnRecordSet R;
+        R.sys = sys;
+        if (cudaMalloc(&R.x, (size_t)2 * M * sizeof(cf)) != cudaSuccess ||
+            cudaMalloc(&R.t, (size_t)M * sizeof(cf)) != cudaSuccess) {
+            cudaFree(R.x);
+            cudaFree(raw);
+            return set_err(ctx, CRT_ERR_ALLOC, "record buffers");
+        }
+        launch_gnn_make_record(G, R, rk, bk, xk, ctx->d_dpar, ctx->st);
+        double t2 = 0.0;
+        CK(cudaMemcpyAsync(&t2, G.d_scal + 2, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        R.tnorm2 = (float)t2;
+        if (t2 > 0.0) {
+            G.recs.push_back(R);
+        } else {
+            cudaFree(R.x);
+            cudaFree(R.t);
+        }
+    }
+    cudaFree(raw);
+    if (int e = kernel_check(ctx, "records")) return e;
+    G.form = base_block ? 1 : 0;
+    if (nrec) *nrec = (int32_t)G.recs.size();
+    return CRT_OK;
+}
+
+// Adam on the recorded pairs: `epochs` passes in a seeded random order,
+// mini-batches of `batch` records; loss_hist[epoch] = mean record loss.
+extern "C" int32_t crt_gnn_train(crt_ctx* ctx, int32_t epochs, int32_t batch, float lr, uint64_t seed,
+                                 float* loss_hist)
+{
+    if (!ctx || epochs < 1 || batch < 1 || !(lr > 0.0f)) return CRT_ERR_ARG;
+    Gnn& G = ctx->gnn;
+    if (!G.ready) return set_err(ctx, CRT_ERR_UNSUPPORTED, "learned preconditioner unavailable (regulariser)");
+    if (G.recs.empty()) return set_err(ctx, CRT_ERR_ARG, "no records (crt_gnn_collect)");
+    CK(cudaSetDevice(ctx->device));
+    const int nr = (int)G.recs.size();
+    std::vector<int> order(nr);
+    for (int i = 0; i < nr; ++i) order[i] = i;
+    unsigned long long st = seed ^ 0x9e3779b97f4a7c15ULL;
+    for (int ep = 0; ep < epochs; ++ep) {
+        for (int i = nr - 1; i > 0; --i) {   // Fisher-Yates with a 64-bit LCG
+            st = st * 6364136223846793005ULL + 1442695040888963407ULL;
+            const int j = (int)((st >> 33) % (unsigned long long)(i + 1));
+            std::swap(order[i], order[j]);
+        }
+        CK(cudaMemsetAsync(G.d_scal + 1, 0, sizeof(double), ctx->st));
+        for (int b0 = 0; b0 < nr; b0 += batch) {
+            const int b1 = std::min(nr, b0 + batch);
+            for (int q = b0; q < b1; ++q) launch_gnn_record_grad(G, G.recs[order[q]], 1.0f / (b1 - b0), ctx->st);
+            launch_gnn_adam(G, lr, ctx->st);
+        }
+        double L = 0.0;
+        CK(cudaMemcpyAsync(&L, G.d_scal + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (int e = kernel_check(ctx, "training")) return e;
+        if (loss_hist) loss_hist[ep] = (float)(L / nr);
+    }
+    G.trained = 1;
+    return CRT_OK;
+}
+
+// One record's data (for checking the network against a CPU restatement):
+// x [M][4] features, t [M][2] target, a [M][4] message weights, nbr [M][4]
+// neighbours (-1 none), |t|^2.  Any output may be NULL.
+extern "C" int32_t crt_gnn_record(crt_ctx* ctx, int32_t idx, float* x, float* t, float* a, int32_t* nbr,
+                                  float* tnorm2)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    Gnn& G = ctx->gnn;
+    if (idx < 0 || idx >= (int)G.recs.size()) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaStreamSynchronize(ctx->st));
+    const GnnRecordSet& R = G.recs[idx];
+    const size_t M = G.M;
+    if (x) CK(cudaMemcpy(x, R.x, M * 2 * sizeof(cf), cudaMemcpyDeviceToHost));
+    if (t) CK(cudaMemcpy(t, R.t, M * sizeof(cf), cudaMemcpyDeviceToHost));
+    if (a) CK(cudaMemcpy(a, G.edge_sets[R.sys], M * GNN_D * sizeof(float), cudaMemcpyDeviceToHost));
+    if (nbr) CK(cudaMemcpy(nbr, G.d_nbr, M * GNN_D * sizeof(int), cudaMemcpyDeviceToHost));
+    if (tnorm2) *tnorm2 = R.tnorm2;
+    return CRT_OK;
+}
+
+// Loss and weight gradient of one record with the current weights (the
+// weights are not changed).
+extern "C" int32_t crt_gnn_record_grad(crt_ctx* ctx, int32_t idx, float* grad, double* loss)
+{
+    if (!ctx || !grad) return CRT_ERR_ARG;
+    Gnn& G = ctx->gnn;
+    if (idx < 0 || idx >= (int)G.recs.size()) return CRT_ERR_ARG;
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemsetAsync(G.d_g, 0, GNN_NPARAM * sizeof(float), ctx->st));
+    CK(cudaMemsetAsync(G.d_scal + 1, 0, sizeof(double), ctx->st));
+    launch_gnn_record_grad(G, G.recs[idx], 1.0f, ctx->st);
+    CK(cudaMemcpyAsync(grad, G.d_g, GNN_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    double L = 0.0;
+    CK(cudaMemcpyAsync(&L, G.d_scal + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    CK(cudaMemsetAsync(G.d_g, 0, GNN_NPARAM * sizeof(float), ctx->st));
+    if (int e = kernel_check(ctx, "record gradient")) return e;
+    if (loss) *loss = L;
+    return CRT_OK;
 }

@@ -19,6 +19,7 @@
 // the real arithmetic of cjggdc exact.
 #include "crt_cg.h"
 #include "crt_spc.h"
+#include "crt_gnn.h"
 
 namespace {
 
@@ -212,37 +213,67 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A)
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) A.p[e] = A.r[e] + A.p[e] * beta;
 }
 
-// Preconditioned head: z = S^-1 r is in A.z.  The stop rule is the
-// reference's (|r|^2 against eps |r0|^2); beta is the flexible
-// (Polak-Ribiere) Re(z^H (r - r_old)) / Re(z_old^H r_old), alpha's
-// numerator Re(r^H z).
+// Preconditioned head: z (the preconditioner's output) is in A.z.  The stop
+// rule is the reference's (|r|^2 against eps |r0|^2); beta is the flexible
+// (Polak-Ribiere) Re(z^H (r - r_old)) / Re(z_old^H r_old), alpha's numerator
+// Re(r^H z).  With the learned correction (pc_gnn) the head also guards it:
+// a non-descent z or a stalled residual switches it off (no_gnn) and the
+// direction restarts (beta = 0) from the base preconditioner's output.
 __global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A)
 {
     __shared__ double red[33];
-    __shared__ int s_stop;
+    __shared__ int s_stop, s_base;
     __shared__ double s_beta;
     CGState* st = A.st;
     if (st->done) return;
-    double v = 0.0, g = 0.0, go = 0.0;
+    const bool guard = A.pc_gnn != 0;
+    const bool off0 = guard && st->no_gnn;
+    double v = 0.0, g = 0.0, go = 0.0, gb = 0.0, gob = 0.0;
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
-        const cd r = A.r[e], z = A.z[e], ro = A.rold[e];
+        const cd r = A.r[e], ro = A.rold[e];
         v += cabs2(r);
-        g += r.x * z.x + r.y * z.y;
-        go += ro.x * z.x + ro.y * z.y;
+        if (!off0) {
+            const cd z = A.z[e];
+            g += r.x * z.x + r.y * z.y;
+            go += ro.x * z.x + ro.y * z.y;
+        }
+        if (guard) {
+            const cd b = A.zb ? A.zb[e] : r;
+            gb += r.x * b.x + r.y * b.y;
+            gob += ro.x * b.x + ro.y * b.y;
+        }
     }
     const double dr = block_sum<VEC_NT>(v, red);
-    const double gam = block_sum<VEC_NT>(g, red);
-    const double gold = block_sum<VEC_NT>(go, red);
+    const double gam_z = block_sum<VEC_NT>(g, red);
+    const double gold_z = block_sum<VEC_NT>(go, red);
+    const double gam_b = guard ? block_sum<VEC_NT>(gb, red) : 0.0;
+    const double gold_b = guard ? block_sum<VEC_NT>(gob, red) : 0.0;
     const int k = st->k;
     if (threadIdx.x == 0) {
         s_stop = 0;
+        int use_base = off0 ? 1 : 0, restart = 0;
+        if (guard && !off0) {
+            bool bad = !(gam_z > 0.0);
+            if (k == 1) st->dr_chk = dr;
+            else if ((k - 1) % GNN_GUARD_WINDOW == 0) {
+                if (dr > 0.5 * st->dr_chk) bad = true;
+                st->dr_chk = dr;
+            }
+            if (bad) {
+                st->no_gnn = 1;
+                use_base = 1;
+                restart = 1;
+            }
+        }
+        const double gam = use_base ? gam_b : gam_z;
+        const double gold = use_base ? gold_b : gold_z;
         double beta = 0.0;
         if (k == 1) {
             st->dr0 = dr * A.eps;
             if (A.jmode != 0 && dr <= st->dr0) s_stop = 1;
         } else {
             if (dr <= st->dr0) s_stop = 1;
-            beta = (gam - gold) / st->gam;
+            if (!restart) beta = (gam - gold) / st->gam;
         }
         if (s_stop) {
             st->done = 1;
@@ -253,13 +284,17 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A)
         st->gam = gam;
         st->num = gam;
         s_beta = beta;
+        s_base = use_base;
     }
     __syncthreads();
     if (s_stop) return;
     const double beta = s_beta;
+    const bool base = s_base != 0;
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) {
-        A.p[e] = A.z[e] + A.p[e] * beta;
-        A.rold[e] = A.r[e];
+        const cd r = A.r[e];
+        const cd z = base ? (A.zb ? A.zb[e] : r) : A.z[e];
+        A.p[e] = z + A.p[e] * beta;
+        A.rold[e] = r;
     }
 }
 
@@ -432,14 +467,21 @@ void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd*
 
 void launch_cg_init(const CGArgs& a, cudaStream_t s) { k_cg_init<<<1, VEC_NT, 0, s>>>(a); }
 
-void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, cudaStream_t s)
+void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* gnn, cd* zb, cudaStream_t s)
 {
     const int nt = 256;
     dim3 gjv((a.N + JV_NT - 1) / JV_NT, a.nsplit);
     const int warps = nt / 32;
     for (int it = 0; it < iters; ++it) {
         if (a.pc) {
-            launch_spc_apply(*spc, a.r, a.z, a.st, s);
+            if (spc && gnn) {
+                launch_spc_apply(*spc, a.r, zb, a.st, s);
+                launch_gnn_apply(*gnn, a.r, zb, a.z, a.st, s);
+            } else if (spc) {
+                launch_spc_apply(*spc, a.r, a.z, a.st, s);
+            } else {
+                launch_gnn_apply(*gnn, a.r, nullptr, a.z, a.st, s);
+            }
             k_cg_begin_pc<<<1, VEC_NT, 0, s>>>(a);
         } else {
             k_cg_begin<<<1, VEC_NT, 0, s>>>(a);

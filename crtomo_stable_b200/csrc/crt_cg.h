@@ -8,10 +8,11 @@ struct CGState {
     double dr, dr0, dr1, alpha, beta;
     double gam;   // preconditioned form: Re(r^H z) of the last iteration head
     double num;   // numerator of alpha: dr (cjggra) or Re(r^H z) (preconditioned)
+    double dr_chk; // |r|^2 at the last progress check of the learned correction
     int k;        // next iteration number (1-based)
     int done;     // 1 once the stop rule fired or ncgmax was reached
     int ncg;      // completed iterations
-    int pad;
+    int no_gnn;   // 1 once the learned correction has been switched off for this solve
 };
 
 struct CGArgs {
@@ -36,17 +37,30 @@ struct CGArgs {
     // rold the residual of the previous head (flexible beta)
     int pc;
     cd *z, *rold;
+    // learned correction on top of the base preconditioner (pc_gnn = 1):
+    // zb holds the base's output (nullptr: the identity, i.e. r)
+    int pc_gnn;
+    const cd* zb;
 };
 
+// The learned correction is switched off for the rest of a solve when it
+// yields a non-descent direction (Re r^H z <= 0) or when |r|^2 has not
+// halved over GNN_GUARD_WINDOW iterations; the CG then restarts its
+// direction from the base preconditioner.
+constexpr int GNN_GUARD_WINDOW = 50;
+
 struct SpcPlan;
+struct Gnn;
 
 // update.f90:63-231: cgfac and the scaled RHS from J, the data residual
 // dat - sigmaa and the regularisation gradient lam * R * par.
 void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s);
 // cjggra / cjggdc: resets the state, then runs up to `iters` iterations.
 void launch_cg_init(const CGArgs& a, cudaStream_t s);
-// pc = 1 takes the preconditioner `spc` (crt_spc.h) before every head.
-void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, cudaStream_t s);
+// pc = 1 applies the preconditioner before every head: the block factor
+// `spc` (crt_spc.h), the learned correction `gnn` (crt_gnn.h) on top of it
+// (zb holds the block result) or on top of the identity; either may be null.
+void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* gnn, cd* zb, cudaStream_t s);
 // update.f90:300-351: dpar *= cgfac (lfpi: (0, Re dpar) first), par += step
 // dpar, bdpar = step * sum |dpar|^2.
 void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* bdpar, cudaStream_t s);

@@ -67,6 +67,8 @@ EXPORTS = [
     "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
     "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order", "crt_last_timings_ex",
+    "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
+    "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad",
 ]
 
 _LIB = None
@@ -128,6 +130,21 @@ def load(path: str = LIB_PATH):
     L.crt_cg_info.restype = C.c_int32
     L.crt_rcm_order.argtypes = [C.c_int32, i32p, i32p, i32p, i32p]
     L.crt_rcm_order.restype = C.c_int32
+    f32p = P(C.c_float)
+    L.crt_gnn_nparam.restype = C.c_int32
+    L.crt_gnn_status.argtypes = [vp, i32p, i32p, i32p, i32p, i32p]
+    L.crt_gnn_status.restype = C.c_int32
+    L.crt_gnn_init.argtypes = [vp, C.c_uint64]
+    L.crt_gnn_set_weights.argtypes = [vp, f32p, C.c_int32, C.c_int32]
+    L.crt_gnn_get_weights.argtypes = [vp, f32p, C.c_int32, i32p]
+    L.crt_gnn_collect.argtypes = [vp, P(crt_cg_params), C.c_int32, C.c_int32, C.c_int32, i32p]
+    L.crt_gnn_clear.argtypes = [vp]
+    L.crt_gnn_train.argtypes = [vp, C.c_int32, C.c_int32, C.c_float, C.c_uint64, f32p]
+    L.crt_gnn_record.argtypes = [vp, C.c_int32, f32p, f32p, f32p, i32p, f32p]
+    L.crt_gnn_record_grad.argtypes = [vp, C.c_int32, f32p, f64p]
+    for nm in ("crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect", "crt_gnn_clear",
+               "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad"):
+        getattr(L, nm).restype = C.c_int32
     L.crt_launch_count.argtypes = [vp]
     L.crt_launch_count.restype = C.c_int64
     L.crt_dmisft.argtypes = [C.c_int32, vp, vp, vp, vp, vp, C.c_int32, C.c_int32, f64p, f64p, i32p]
@@ -205,6 +222,8 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 PRECOND_JACOBI = 0
 PRECOND_BLOCK = 1
+PRECOND_GNN = 2
+PRECOND_BLOCK_GNN = 3
 
 
 class Context:
@@ -394,6 +413,61 @@ class Context:
 
     def launch_count(self):
         return int(self.L.crt_launch_count(self.h))
+
+    # -- learned correction of the preconditioner -------------------------
+    def gnn_nparam(self):
+        return int(self.L.crt_gnn_nparam())
+
+    def gnn_status(self):
+        v = [C.c_int32() for _ in range(5)]
+        self._check(self.L.crt_gnn_status(self.h, *[C.byref(x) for x in v]), "crt_gnn_status")
+        return dict(zip(["available", "trained", "form", "nrec", "guard_fired"], [x.value for x in v]))
+
+    def gnn_init(self, seed=1):
+        self._check(self.L.crt_gnn_init(self.h, int(seed)), "crt_gnn_init")
+
+    def gnn_set_weights(self, w, form):
+        w = np.ascontiguousarray(w, np.float32)
+        self._check(self.L.crt_gnn_set_weights(self.h, _ptr(w, C.c_float), len(w), int(form)), "crt_gnn_set_weights")
+
+    def gnn_get_weights(self):
+        w = np.zeros(self.gnn_nparam(), np.float32)
+        f = C.c_int32()
+        self._check(self.L.crt_gnn_get_weights(self.h, _ptr(w, C.c_float), len(w), C.byref(f)), "crt_gnn_get_weights")
+        return w, f.value
+
+    def gnn_collect(self, prm, base_block=False, stride=8, nmax=256):
+        n = C.c_int32()
+        self._check(self.L.crt_gnn_collect(self.h, C.byref(prm), int(bool(base_block)), int(stride), int(nmax),
+                                           C.byref(n)), "crt_gnn_collect")
+        return n.value
+
+    def gnn_clear(self):
+        self._check(self.L.crt_gnn_clear(self.h), "crt_gnn_clear")
+
+    def gnn_train(self, epochs=10, batch=8, lr=1e-3, seed=1):
+        hist = np.zeros(epochs, np.float32)
+        self._check(self.L.crt_gnn_train(self.h, int(epochs), int(batch), float(lr), int(seed), _ptr(hist, C.c_float)),
+                    "crt_gnn_train")
+        return hist
+
+    def gnn_record(self, idx):
+        M = self.elanz
+        x = np.zeros((M, 4), np.float32)
+        t = np.zeros((M, 2), np.float32)
+        a = np.zeros((M, 4), np.float32)
+        nb = np.zeros((M, 4), np.int32)
+        tn = C.c_float()
+        self._check(self.L.crt_gnn_record(self.h, int(idx), _ptr(x, C.c_float), _ptr(t, C.c_float),
+                                          _ptr(a, C.c_float), _ptr(nb, C.c_int32), C.byref(tn)), "crt_gnn_record")
+        return dict(x=x, t=t, a=a, nbr=nb, tnorm2=tn.value)
+
+    def gnn_record_grad(self, idx):
+        g = np.zeros(self.gnn_nparam(), np.float32)
+        L_ = C.c_double()
+        self._check(self.L.crt_gnn_record_grad(self.h, int(idx), _ptr(g, C.c_float), C.byref(L_)),
+                    "crt_gnn_record_grad")
+        return g, L_.value
 
     def cg_info(self):
         """(form of the last CG, block size of the block preconditioner or 0,

@@ -86,6 +86,11 @@ typedef struct {
  *   (crt_cg_info reports which form ran). */
 #define CRT_PRECOND_JACOBI 0
 #define CRT_PRECOND_BLOCK 1
+/* The learned correction (crt_gnn_*) added to the identity (Jacobi form) or
+ * to the block preconditioner; used when the network was trained on records
+ * of the same base, else the form without it runs. */
+#define CRT_PRECOND_GNN 2
+#define CRT_PRECOND_BLOCK_GNN 3
 
 /* Precision forms.
  * CRT_PREC_FP64:  everything in FP64 / complex128 (the reference's arithmetic).
@@ -209,6 +214,42 @@ int64_t crt_launch_count(const crt_ctx *ctx);
  * regulariser's half-bandwidth after reverse Cuthill-McKee.  Any pointer
  * may be NULL.  No reference counterpart. */
 int32_t crt_cg_info(const crt_ctx *ctx, int32_t *form, int32_t *block, int32_t *bandwidth);
+
+/* Learned correction of the CG preconditioner (no reference counterpart).
+ * A mesh graph network over the model cells (the regulariser's graph, three
+ * message-passing layers of width 32, tanh, no biases, bf16 weights with FP32
+ * sums) maps the normalised residual and the base preconditioner's output to
+ * a correction: z = base(r) + net(r, base(r)).  It is trained on the GPU on
+ * residual / error pairs recorded from the plain (Jacobi-form) CG of the
+ * inversion itself and used by crt_update / crt_gn_step through
+ * CRT_PRECOND_GNN / CRT_PRECOND_BLOCK_GNN.  The network weights are a flat
+ * FP32 vector of crt_gnn_nparam() entries, matrices stored [in][out]:
+ *   Win[4][32] | (Ws[32][32], Wn[32][32]) x 3 layers | Wout[32][2].
+ * form: 0 trained on the identity base, 1 on the block preconditioner. */
+int32_t crt_gnn_nparam(void);
+/* Whether the network is available for this regulariser, trained, the base
+ * it was trained on, the records held, and whether the last solve's guard
+ * switched it off (a non-descent direction, or |r|^2 not halving over 50
+ * iterations: the CG then finishes with the base preconditioner). */
+int32_t crt_gnn_status(const crt_ctx *ctx, int32_t *available, int32_t *trained, int32_t *form, int32_t *nrec,
+                       int32_t *guard_fired);
+int32_t crt_gnn_init(crt_ctx *ctx, uint64_t seed);
+int32_t crt_gnn_set_weights(crt_ctx *ctx, const float *w, int32_t n, int32_t form);
+int32_t crt_gnn_get_weights(crt_ctx *ctx, float *w, int32_t n, int32_t *form);
+/* Runs the plain CG of the current Gauss-Newton system (as crt_update would,
+ * without changing the model) and records (r_k, x* - x_k) every `stride`
+ * iterations, at most nmax; *nrec = records held in total. */
+int32_t crt_gnn_collect(crt_ctx *ctx, const crt_cg_params *prm, int32_t base_block, int32_t stride,
+                        int32_t nmax, int32_t *nrec);
+int32_t crt_gnn_clear(crt_ctx *ctx);
+/* Adam, seeded shuffles, mini-batches; loss_hist[epochs] = mean record loss
+ * |z - e|^2 / |e - base|^2 (normalised units). */
+int32_t crt_gnn_train(crt_ctx *ctx, int32_t epochs, int32_t batch, float lr, uint64_t seed, float *loss_hist);
+/* One record's features x[M][4], target t[M][2], message weights a[M][4],
+ * neighbours nbr[M][4] (-1 none) and |t|^2, and its loss and gradient with
+ * the current weights (for checking against a CPU restatement). */
+int32_t crt_gnn_record(crt_ctx *ctx, int32_t idx, float *x, float *t, float *a, int32_t *nbr, float *tnorm2);
+int32_t crt_gnn_record_grad(crt_ctx *ctx, int32_t idx, float *grad, double *loss);
 
 /* Reverse Cuthill-McKee ordering of an undirected graph in CSR form
  * (xadj[n+1], adj[xadj[n]], 0-based, both directions of every edge listed):
