@@ -793,7 +793,14 @@ int jacobian_device(crt_ctx* ctx, int mode, const double* strom_h)
         if (!ctx->d_part_sens && !dalloc(ctx, &ctx->d_part_sens, ne)) return CRT_ERR_ALLOC;
     }
     S.part = ctx->d_part_sens;
-    launch_sens(S, smem, real, ctx->st);
+    int LP = 0, gkc = 0, gnt = 0;
+    size_t gsmem = 0;
+    const char* sv = std::getenv("CRT_B200_SENS");
+    const bool force_direct = sv && std::strcmp(sv, "direct") == 0;
+    if (!force_direct && sens_gram_plan(ctx->L, ctx->K, ctx->nkmax, real, &LP, &gkc, &gsmem, &gnt))
+        launch_sens_gram(S, LP, gkc, gsmem, gnt, real, ctx->st);
+    else
+        launch_sens(S, smem, real, ctx->st);
     ctx->launches++;
     CK(cudaEventRecord(ctx->ev[6], ctx->st));
     if (int e = kernel_check(ctx, "sensitivities")) return e;

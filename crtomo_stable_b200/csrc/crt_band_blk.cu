@@ -164,7 +164,7 @@ __global__ void k_band_prep_rows(BandArgs<T> A)
 }
 
 template <typename T, int PB, int NT>
-__global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
+__global__ void __launch_bounds__(NT, 1) k_band_factor_blk(BandArgs<T> A, int Wn)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = A.n, mb = A.mb, W1 = A.W;    // W1 = mb + 1 (column stride of the HBM factor)
@@ -179,6 +179,7 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
     double* fakN = reinterpret_cast<double*>(LDi + PB);   // PB scaling factors of the staged rows
     unsigned short* tXY = reinterpret_cast<unsigned short*>(fakN + PB);   // NTT tile coordinates
     __shared__ T colb[32];                                                // column broadcast of the block factor
+    __shared__ T bN[PB];                                                  // scaled right-hand side of the staged rows
     __shared__ int s_err;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -217,7 +218,14 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
             stage[i] = (r0 + q < n) ? src_rows[i] : Sc<T>::zero();
         }
         const int q = tid - t0;
-        if (q >= 0 && q < PB) fakN[q] = (r0 + q < n) ? fk[r0 + q] : 1.0;
+        if (q >= 0 && q < PB) {
+            const int r = r0 + q;
+            const double f = (r < n) ? fk[r] : 1.0;
+            fakN[q] = f;
+            T bb = Sc<T>::zero();
+            if (fuse && r < n) bb = scale(rhs_entry_b<T>(r, src, A.lsink, A.nsink0, A.dflag, A.dval, bdir), f);
+            bN[q] = bb;
+        }
     };
     // Staged rows into slots s_new .. s_new+PB-1; the window after the write
     // holds rows [wlo, wlo + Wn).  Every pair of a new slot with a row
@@ -237,12 +245,7 @@ __global__ void __launch_bounds__(NT) k_band_factor_blk(BandArgs<T> A, int Wn)
                 win[widx(s_new + q, y)] = (r < n && d <= mb) ? stage[q * W1 + d] : Sc<T>::zero();
             }
         }
-        if (tid < PB) {
-            const int r = r0 + tid;
-            T bb = Sc<T>::zero();
-            if (fuse && r < n) bb = scale(rhs_entry_b<T>(r, src, A.lsink, A.nsink0, A.dflag, A.dval, bdir), fakN[tid]);
-            bsl[s_new + tid] = bb;
-        }
+        if (tid < PB) bsl[s_new + tid] = bN[tid];
     };
 
     // Initial window: rows 0 .. Wn-1, PB at a time.
@@ -471,7 +474,7 @@ void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
 template <typename T>
 bool launch_band_factor_blk(const BandArgs<T>& a, cudaStream_t st)
 {
-    constexpr int NT = 256, PB = 8;
+    constexpr int NT = 512, PB = 8;
     int Wn = 0;
     const size_t smem = blk_smem<T, PB>(a.mb, &Wn);
     if (!band_blk_fits<T>(a.mb)) return false;

@@ -14,6 +14,8 @@
 // contiguous in i (the Fortran sens(nanz, manz) layout).
 #include "crt_sens.h"
 
+#include <algorithm>
+
 __global__ void k_transpose_kpot(const cd* __restrict__ kpot, cd* __restrict__ kpt, int n, int L, int K)
 {
     // kpot[(k*L + l)*n + j] -> kpt[(k*n + j)*L + l], 32x32 tiles per k.
@@ -119,6 +121,168 @@ __global__ void __launch_bounds__(NT) k_sens(SensArgs A)
                 else reinterpret_cast<cd*>(A.sens)[o] = res;
             }
         }
+    }
+}
+
+// Gram form of the same sum.  With Phi_k the nk x L potentials of the
+// element's nodes and E_k its element matrix,
+//   G = sum_k w_k Phi_k^T E_k Phi_k      (L x L, symmetric: E_k is)
+// holds G(a, b) = sum_{mi,mj} E_k(mi, mj) phi_a(mi) phi_b(mj) summed over the
+// wavenumbers, and every reading is the four-term combination
+//   G(P2,C2) - G(P2,C1) - G(P1,C2) + G(P1,C1)
+// of the reciprocity sum of src/bsensi.f90:98-186 (the reference forms the
+// potential differences first; the two orders agree to FP64 rounding of
+// the products).  G is accumulated as a rank-(K nk) product: one thread per
+// 8 x 4 tile of its lower triangle, operands staged per chunk of
+// wavenumbers (Phi_k and w_k E_k Phi_k), then written to shared memory for
+// the readings' gathers.
+constexpr int GR_TA = 8, GR_TB = 4;
+
+__device__ __forceinline__ int gram_idx(int a, int b)
+{
+    if (a < b) {
+        const int t = a;
+        a = b;
+        b = t;
+    }
+    return a * (a + 1) / 2 + b;
+}
+
+template <typename T, int MAXT>
+__global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* sbuf = reinterpret_cast<T*>(smem_raw);
+    const int e = blockIdx.x;
+    const int nk = A.enk[e];
+    const int L = A.L, K = A.K;
+    const int RB = LP / GR_TA, ntile = RB * (RB + 1);
+    const int tid = threadIdx.x;
+    // tile of this thread: row block R, column block Cb <= 2R+1
+    int R = 0;
+    while ((R + 1) * (R + 2) <= tid) ++R;
+    const int Cb = tid - R * (R + 1);
+    const bool has_tile = tid < ntile;
+    T acc[GR_TA][GR_TB];
+#pragma unroll
+    for (int i = 0; i < GR_TA; ++i)
+#pragma unroll
+        for (int j = 0; j < GR_TB; ++j) acc[i][j] = Sc<T>::zero();
+    T* phi = sbuf;                                   // [kc][nk][LP]
+    T* wu = sbuf + (size_t)kc * nk * LP;             // [kc][nk][LP]
+    for (int k0 = 0; k0 < K; k0 += kc) {
+        const int kn = min(kc, K - k0);
+        __syncthreads();
+        for (int t = tid; t < kn * nk * LP; t += blockDim.x) {
+            const int a = t % LP, m = (t / LP) % nk, kk = t / (LP * nk);
+            const int node = A.nrel0[e * A.maxnodes + m];
+            phi[t] = a < L ? ld_phi<T>(A.kpt[((size_t)(k0 + kk) * A.n + node) * L + a]) : Sc<T>::zero();
+        }
+        __syncthreads();
+        for (int t = tid; t < kn * nk * LP; t += blockDim.x) {
+            const int b = t % LP, m = (t / LP) % nk, kk = t / (LP * nk);
+            const double* km = A.elbg + ((size_t)(k0 + kk) * A.E + e) * A.nmn;
+            const double w = A.swrtr ? A.kwnwi[k0 + kk] : 1.0;
+            T v = Sc<T>::zero();
+            for (int m2 = 0; m2 < nk; ++m2) {
+                const int ix = max(m, m2), in = min(m, m2);
+                v += scale(phi[((size_t)kk * nk + m2) * LP + b], km[ix * (ix + 1) / 2 + in]);
+            }
+            wu[t] = scale(v, w);
+        }
+        __syncthreads();
+        if (has_tile) {
+            for (int q = 0; q < kn * nk; ++q) {
+                const T* pa = phi + (size_t)q * LP + R * GR_TA;
+                const T* pb = wu + (size_t)q * LP + Cb * GR_TB;
+                T av[GR_TA], bv[GR_TB];
+#pragma unroll
+                for (int i = 0; i < GR_TA; ++i) av[i] = pa[i];
+#pragma unroll
+                for (int j = 0; j < GR_TB; ++j) bv[j] = pb[j];
+#pragma unroll
+                for (int i = 0; i < GR_TA; ++i)
+#pragma unroll
+                    for (int j = 0; j < GR_TB; ++j) fms_acc(acc[i][j], -av[i], bv[j]);
+            }
+        }
+    }
+    __syncthreads();
+    T* G = sbuf;   // lower triangle, packed
+    if (has_tile) {
+#pragma unroll
+        for (int i = 0; i < GR_TA; ++i)
+#pragma unroll
+            for (int j = 0; j < GR_TB; ++j) {
+                const int a = R * GR_TA + i, b = Cb * GR_TB + j;
+                if (a >= b && a < L) G[a * (a + 1) / 2 + b] = acc[i][j];
+            }
+    }
+    __syncthreads();
+    const cd sig = A.sigma[e];
+    for (int i = tid; i < A.N; i += blockDim.x) {
+        const int4 el = A.elec[i];    // 0-based C1, C2, P1, P2; -1 when absent
+        auto g = [&](int a, int b) { return (a < 0 || b < 0) ? Sc<T>::zero() : G[gram_idx(a, b)]; };
+        const T acc_i = ((g(el.w, el.y) - g(el.w, el.x)) - g(el.z, el.y)) + g(el.z, el.x);
+        cd res;
+        if (A.mode == 0) {
+            cd d = Sc<T>::to_cd(acc_i);
+            if (A.swrtr != 0) d = d / A.pi;
+            res = (d * sig) / A.volt[i];
+        } else if (A.mode == 1) {
+            double d = Sc<T>::to_cd(acc_i).x;
+            if (A.swrtr != 0) d = d / A.pi;
+            const cd q = sig / A.volt[i];
+            res = cd{d * q.x, 0.0};
+        } else {
+            cd d = Sc<T>::to_cd(acc_i);
+            const double st = A.strom ? A.strom[i] : 1.0;
+            if (A.swrtr == 0) d = d * st;
+            else d = d * (st / A.pi);
+            res = -d;
+        }
+        const size_t o = (size_t)e * A.N + i;
+        if (A.mode == 1) {
+            if (A.out_prec) reinterpret_cast<float*>(A.sens)[o] = (float)res.x;
+            else reinterpret_cast<double*>(A.sens)[o] = res.x;
+        } else {
+            if (A.out_prec) reinterpret_cast<cf*>(A.sens)[o] = cf{(float)res.x, (float)res.y};
+            else reinterpret_cast<cd*>(A.sens)[o] = res;
+        }
+    }
+}
+
+bool sens_gram_plan(int L, int K, int nkmax, bool real, int* LP_out, int* kc_out, size_t* smem_out, int* nt_out)
+{
+    const size_t tsz = real ? sizeof(double) : sizeof(cd);
+    const int LP = (L + GR_TA - 1) / GR_TA * GR_TA;
+    const int RB = LP / GR_TA, ntile = RB * (RB + 1);
+    if (nkmax > 4 || ntile > 512) return false;
+    const size_t gbytes = (size_t)LP * (LP + 1) / 2 * tsz;
+    const size_t limit = 200 * 1024;
+    if (gbytes > limit) return false;
+    int kc = K;
+    while (kc > 1 && 2 * (size_t)kc * nkmax * LP * tsz > std::max(gbytes, (size_t)64 * 1024)) --kc;
+    *LP_out = LP;
+    *kc_out = kc;
+    *smem_out = std::max(gbytes, 2 * (size_t)kc * nkmax * LP * tsz);
+    *nt_out = (ntile + 31) / 32 * 32;
+    return true;
+}
+
+void launch_sens_gram(const SensArgs& a, int LP, int kc, size_t smem, int nt, bool real, cudaStream_t st)
+{
+    // up to 320 threads (LP <= 128) the tile's accumulators stay in registers
+    auto go = [&](auto kern) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<a.E, nt, smem, st>>>(a, LP, kc);
+    };
+    if (real) {
+        if (nt <= 320) go(k_sens_gram<double, 320>);
+        else go(k_sens_gram<double, 512>);
+    } else {
+        if (nt <= 320) go(k_sens_gram<cd, 320>);
+        else go(k_sens_gram<cd, 512>);
     }
 }
 

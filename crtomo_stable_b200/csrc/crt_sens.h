@@ -25,3 +25,8 @@ struct SensArgs {
 void launch_transpose_kpot(const cd* kpot, cd* kpt, int n, int L, int K, cudaStream_t st);
 size_t sens_smem(int L, int K, int nkmax, int nmn, int* kchunk, size_t limit, bool real);
 void launch_sens(const SensArgs& a, size_t smem, bool real, cudaStream_t st);
+// Gram form (crt_sens.cu): false when the electrodes or element nodes
+// exceed its limits (L <= 168 for complex potentials, nk <= 4); then the
+// per-reading kernel above is used.
+bool sens_gram_plan(int L, int K, int nkmax, bool real, int* LP, int* kc, size_t* smem, int* nt);
+void launch_sens_gram(const SensArgs& a, int LP, int kc, size_t smem, int nt, bool real, cudaStream_t st);
