@@ -43,9 +43,12 @@ REF_NCG = {"C5": 1589}
 # matrix read once and L written once).
 FACTOR_TRAFFIC_BYTES_PER_ENTRY = 31.8
 
-# FP64 FMA pipe of a B200 SM: 64 FMA per clock (non-tensor), used as the
-# roofline of the FP64 band factorisation.
+# FMA pipes of a B200 SM (non-tensor): 64 FP64 / 128 FP32 FMA per clock,
+# the rooflines of the complex128 / complex64 band factorisation.
 FP64_FMA_PER_CLK_SM = 64
+FP32_FMA_PER_CLK_SM = 128
+# complex64: to be filled from an ncu capture of the complex64 factor
+FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 = None
 
 
 def parse():
@@ -58,6 +61,8 @@ def parse():
     ap.add_argument("--eps", type=float, default=1e-12, help="|r|^2 <= eps |r0|^2 (1e-12 = rel-res 1e-6)")
     ap.add_argument("--ncgmax", type=int, default=20000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--refine", type=int, default=None,
+                    help="FP64 refinement steps of the complex64 forward (default: the library's)")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="'mixed' skips the plain FP64 comparison run (profiling)")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
@@ -284,6 +289,8 @@ def main():
 
     def run_form(precision, steps, warmup, e2e_steps, sample_clocks):
         ctx, dat, wmatd, par0, lam, nb, sm = setup_context(s, local, precision)
+        if args.refine is not None:
+            ctx.set_refinement(args.refine)
         pc = PRECOND_BLOCK if precision == PREC_MIXED else PRECOND_JACOBI
         prm = Context.params(lam, eps=args.eps, ncgmax=args.ncgmax, precond=pc)
         ctx.set_model(par0)
@@ -321,7 +328,7 @@ def main():
         form, blk, bw = ctx.cg_info()
         ctx.close()
         return dict(t=t_step, phase=phase, ncg=ncg, launches=int(launches), clocks=clocks, e2e=t_e2e, lam=lam, K=K,
-                    cg_form=form, cg_block=blk, cg_bw=bw)
+                    cg_form=form, cg_block=blk, cg_bw=bw, c64=precision == PREC_MIXED)
 
     mixed = run_form(PREC_MIXED, args.steps, args.warmup, args.steps, True)
     plain = None
@@ -333,21 +340,30 @@ def main():
     d2h = E * 16 + N * 16 + (ncg + 1) * 8 + 8
     peak_gbs, peak_kind = load_peaks()
     sm_mhz = (mixed["clocks"] or {}).get("sm_max_mhz") or 1965.0
-    # dominant kernel: the FP64 band factorisation, compute-bound on the FP64
-    # pipe.  Algorithmic work per system 4 n mb^2 flops (n mb^2 / 2 complex
-    # MACs of 8 flops); per launch = systems per launch x that.
+    # dominant kernel: the band factorisation -- complex64 on the FP32 pipe
+    # in the mixed form (128 FMA/clk/SM), complex128 on the FP64 pipe
+    # (64 FMA/clk/SM) otherwise.  Algorithmic work per system 4 n mb^2 flops
+    # (n mb^2 / 2 complex MACs of 8 flops); per launch = systems per launch x
+    # that.  Traffic: the prepared matrix read once and L written once,
+    # bytes per band entry from the ncu captures in profiles/.
+    c64 = mixed["c64"]
     nsys = K * L   # mixed boundaries: one factorisation per (k, l)
     flops = 4.0 * n * mb * mb * nsys
     nl = max(ph["factor_launches"], 1.0)
     t_launch_s = ph["factor_kernel"] / nl / 1e3
-    fp64_peak = FP64_FMA_PER_CLK_SM * 2 * 148 * sm_mhz * 1e6 / 1e12
+    fma_clk = FP32_FMA_PER_CLK_SM if c64 else FP64_FMA_PER_CLK_SM
+    pipe_peak = fma_clk * 2 * 148 * sm_mhz * 1e6 / 1e12
     ach = flops / nl / t_launch_s / 1e12 if t_launch_s > 0 else 0.0
-    roof = {"kernel": "k_band_factor_blk<cd,8,256> (complex128 band Cholesky + fused forward substitution)",
-            "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s", "frac": ach / fp64_peak,
-            "traffic": FACTOR_TRAFFIC_BYTES_PER_ENTRY * n * (mb + 1) * nsys / nl,
+    bpe = FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 if c64 else FACTOR_TRAFFIC_BYTES_PER_ENTRY
+    roof = {"kernel": ("k_band_factor_blk<cf,8,256,2> (complex64 band Cholesky + fused forward substitution)" if c64
+                       else "k_band_factor_blk<cd,8,512,1> (complex128 band Cholesky + fused forward substitution)"),
+            "bound": "fp32" if c64 else "fp64", "achieved": ach, "peak": pipe_peak, "unit": "TFLOP/s",
+            "frac": ach / pipe_peak,
+            "traffic": bpe * n * (mb + 1) * nsys / nl if bpe else None,
             "traffic_unit": "bytes per launch (ncu dram read + write on C3, scaled by n (mb + 1) per system)",
-            "peak_source": "FP64 FMA pipe, 64 FMA/clk/SM x 148 SMs at the max SM clock (no FP64 figure in "
-                           "MEASURED_PEAKS.json)",
+            "peak_source": (f"{'FP32' if c64 else 'FP64'} FMA pipe, {fma_clk} FMA/clk/SM x 148 SMs at the max SM "
+                            "clock (the factor runs on the CUDA cores; MEASURED_PEAKS.json holds HBM and bf16 "
+                            "tensor figures only)"),
             "algorithmic_flops_per_launch": flops / nl, "launch_ms": t_launch_s * 1e3, "launches": nl}
     roof_cg = None
     if ncg > 0:
@@ -372,10 +388,12 @@ def main():
                 "config": {"workload": f"{args.config}: {E} triangles, n={n}, mb={mb}, {L} electrodes, "
                                        f"{N} readings, K={K}; one GN step from a homogeneous model "
                                        f"(forward {K * L} band systems + Jacobian + CG to rel-res 1e-6)",
-                           "form": "mixed: complex64 Jacobian storage, FP64 accumulation and dots; "
-                                   "complex128 band factorisation; CG preconditioned by cgfac and the "
-                                   "block-tridiagonal S^-1 (FP32) of the sparse part" if mixed["cg_form"] == 1 else
-                                   "mixed: complex64 Jacobian storage; diagonal-PCG (block preconditioner unavailable)",
+                           "form": ("mixed: band systems assembled and scaled in FP64, factored and solved in "
+                                    "complex64, two FP64 iterative-refinement steps; Jacobian formed in FP64, stored "
+                                    "complex64; CG with FP64 accumulation and dots, preconditioned by cgfac and the "
+                                    "block-tridiagonal S^-1 (FP32) of the sparse part" if mixed["cg_form"] == 1 else
+                                    "mixed; diagonal-PCG (block preconditioner unavailable)"),
+                           "refinement_steps": args.refine if args.refine is not None else 2,
                            "cg_block": mixed["cg_block"], "cg_bandwidth": mixed["cg_bw"],
                            "cg_iterations": ncg, "lam": mixed["lam"],
                            "l2": "inputs larger than L2 (J alone is %.1f GB in complex64)" % (N * E * 8 / 1e9),

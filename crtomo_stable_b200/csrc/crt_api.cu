@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/crt_b200.h"
@@ -50,6 +51,13 @@ struct crt_ctx {
     double *d_elbg = nullptr, *d_relbg = nullptr, *d_kg = nullptr;
     int *d_row_ptr = nullptr, *d_ent_d = nullptr, *d_ent_ptr = nullptr, *d_con_code = nullptr,
         *d_con_sig = nullptr;
+    // entries above the diagonal of every row r: (entry e of row c > r with
+    // offset c - r, row c), for the FP64 residual of the refinement
+    int *d_up_ptr = nullptr, *d_up_ent = nullptr, *d_up_row = nullptr;
+    int nent_rows = 0;         // gather entries per system (row_ptr[n])
+    cd* d_aval = nullptr;      // [chunk][nent_rows] prepared FP64 entries (mixed form)
+    size_t aval_chunk = 0;
+    int nref = 2;   // iterative-refinement steps of the complex64 forward
     unsigned char* d_dflag = nullptr;
     cd* d_dval = nullptr;
     int* d_status = nullptr;    // [max(K*L, K) + 8] per-system errnr; [last] global
@@ -189,6 +197,27 @@ int plan_chunk(crt_ctx* ctx, int nsys, size_t tsize)
     return std::min(c, nsys);
 }
 
+bool upload_upper_lists(crt_ctx* ctx, const AssemblyLists& lists)
+{
+    const int n = (int)lists.row_ptr.size() - 1;
+    std::vector<int> cnt(n + 1, 0);
+    for (int c = 0; c < n; ++c)
+        for (int e = lists.row_ptr[c]; e < lists.row_ptr[c + 1]; ++e)
+            if (lists.ent_d[e] > 0) cnt[c - lists.ent_d[e] + 1]++;
+    for (int r = 0; r < n; ++r) cnt[r + 1] += cnt[r];
+    std::vector<int> ue(cnt[n]), ur(cnt[n]), fill(cnt.begin(), cnt.end() - 1);
+    for (int c = 0; c < n; ++c)
+        for (int e = lists.row_ptr[c]; e < lists.row_ptr[c + 1]; ++e)
+            if (lists.ent_d[e] > 0) {
+                const int r = c - lists.ent_d[e];
+                ue[fill[r]] = e;
+                ur[fill[r]] = c;
+                fill[r]++;
+            }
+    return upload(ctx, &ctx->d_up_ptr, cnt.data(), cnt.size()) && upload(ctx, &ctx->d_up_ent, ue.data(), ue.size()) &&
+           upload(ctx, &ctx->d_up_row, ur.data(), ur.size());
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -211,6 +240,13 @@ extern "C" int32_t crt_last_timings(const crt_ctx* ctx, double* ms7)
 {
     if (!ctx || !ms7) return CRT_ERR_ARG;
     for (int i = 0; i < 7; ++i) ms7[i] = ctx->timings[i];
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_set_refinement(crt_ctx* ctx, int32_t steps)
+{
+    if (!ctx || steps < 0 || steps > 16) return CRT_ERR_ARG;
+    ctx->nref = steps;
     return CRT_OK;
 }
 
@@ -239,7 +275,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
     void* ptrs[] = {ctx->d_nrel0, ctx->d_snr0, ctx->d_etyp, ctx->d_enk, ctx->d_enr0, ctx->d_mixed_rel,
                     ctx->d_strnr, ctx->d_vnr, ctx->d_elec, ctx->d_sx, ctx->d_sy, ctx->d_kwn, ctx->d_kwnwi,
                     ctx->d_elbg, ctx->d_relbg, ctx->d_kg, ctx->d_row_ptr, ctx->d_ent_d, ctx->d_ent_ptr,
-                    ctx->d_con_code, ctx->d_con_sig, ctx->d_dflag, ctx->d_dval, ctx->d_status, ctx->d_sigma,
+                    ctx->d_con_code, ctx->d_con_sig, ctx->d_up_ptr, ctx->d_up_ent, ctx->d_up_row, ctx->d_aval, ctx->d_dflag, ctx->d_dval, ctx->d_status, ctx->d_sigma,
                     ctx->d_kpot, ctx->d_kpt, ctx->d_volt, ctx->d_sigmaa, ctx->d_hel, ctx->d_Lws, ctx->d_yws,
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
@@ -408,6 +444,7 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
               upload(ctx, &ctx->d_ent_ptr, lists.ent_ptr.data(), lists.ent_ptr.size()) &&
               upload(ctx, &ctx->d_con_code, lists.con_code.data(), lists.con_code.size()) &&
               upload(ctx, &ctx->d_con_sig, lists.con_sig.data(), lists.con_sig.size()) &&
+              upload_upper_lists(ctx, lists) && (ctx->nent_rows = lists.row_ptr.back(), true) &&
               upload(ctx, &ctx->d_dflag, dflag.data(), dflag.size()) &&
               upload(ctx, &ctx->d_dval, dval.data(), dval.size());
     if (!ok) return fail(ctx, CRT_ERR_ALLOC);
@@ -539,7 +576,7 @@ int run_forward(crt_ctx* ctx)
         ctx->chunk = chunk;
     }
     chunk = ctx->chunk;
-    float ms_f = 0, ms_s = 0, ms_prep = 0, ms_fk = 0;
+    float ms_f = 0, ms_s = 0, ms_prep = 0, ms_fk = 0, ms_res = 0, ms_cor = 0;
     int nfl = 0;
     bool blk = false;
     for (int s0 = 0; s0 < nfac; s0 += chunk) {
@@ -577,6 +614,16 @@ int run_forward(crt_ctx* ctx)
         A.yws = static_cast<T*>(ctx->d_yws);
         A.fakws = ctx->d_fakws;
         A.status = ctx->d_status;
+        A.aval = nullptr;
+        A.aval_stride = (size_t)ctx->nent_rows;
+        if constexpr (std::is_same<T, cf>::value) {
+            // the refinement's residual reads the prepared entries in FP64
+            if (ctx->aval_chunk < (size_t)chunk) {
+                if (!dalloc(ctx, &ctx->d_aval, (size_t)chunk * ctx->nent_rows)) return CRT_ERR_ALLOC;
+                ctx->aval_chunk = chunk;
+            }
+            A.aval = ctx->d_aval;
+        }
         CK(cudaEventRecord(ctx->ev[0], ctx->st));
         {
             const char* fv = std::getenv("CRT_B200_FACTOR");
@@ -588,7 +635,11 @@ int run_forward(crt_ctx* ctx)
                 ctx->launches += 3;
                 blk = true;
             } else {
-                launch_band_factor<T>(A, ctx->st);
+                if constexpr (std::is_same<T, cf>::value) {
+                    return set_err(ctx, CRT_ERR_UNSUPPORTED, "complex64 factorisation needs the panel-blocked kernel");
+                } else {
+                    launch_band_factor<T>(A, ctx->st);
+                }
                 CK(cudaEventRecord(ctx->ev[8], ctx->st));
                 ctx->launches++;
                 blk = false;
@@ -612,18 +663,40 @@ int run_forward(crt_ctx* ctx)
         S.yws = A.yws;
         S.kpot = ctx->d_kpot;
         S.status = ctx->d_status;
+        T* scr = static_cast<T*>(mixed ? ctx->d_yws : ctx->d_scratch);
         if (mixed) {
             S.sys0 = s0;
             S.nsys = ns;
             S.factor_of_sys_div = 1;
-            launch_band_solve_with_scratch<T>(S, static_cast<T*>(ctx->d_yws), ctx->st);
         } else {
             S.sys0 = s0 * L;
             S.nsys = ns * L;
             S.factor_of_sys_div = L;
-            launch_band_solve_with_scratch<T>(S, static_cast<T*>(ctx->d_scratch), ctx->st);
         }
+        launch_band_solve_with_scratch<T>(S, scr, ctx->st);
         ctx->launches++;
+        if constexpr (std::is_same<T, cf>::value) {
+            // iterative refinement of the complex64 solution: FP64 residual of
+            // the scaled system, complex64 correction solve, FP64 update of kpot
+            for (int it = 0; it < ctx->nref; ++it) {
+                CK(cudaEventRecord(ctx->ev[4], ctx->st));
+                launch_band_residual<T>(A, S.sys0, S.nsys, S.factor_of_sys_div, ctx->d_up_ptr, ctx->d_up_ent,
+                                        ctx->d_up_row, ctx->d_kpot, scr, ctx->st);
+                CK(cudaEventRecord(ctx->ev[5], ctx->st));
+                SolveArgs<T> C = S;
+                C.rhs = scr;
+                C.accumulate = 1;
+                launch_band_solve_with_scratch<T>(C, scr, ctx->st);
+                CK(cudaEventRecord(ctx->ev[9], ctx->st));
+                CK(cudaEventSynchronize(ctx->ev[9]));
+                float t1 = 0, t2 = 0;
+                cudaEventElapsedTime(&t1, ctx->ev[4], ctx->ev[5]);
+                cudaEventElapsedTime(&t2, ctx->ev[5], ctx->ev[9]);
+                ms_res += t1;
+                ms_cor += t2;
+                ctx->launches += 2;
+            }
+        }
         if (int e = kernel_check(ctx, "band solve")) return e;
         CK(cudaEventRecord(ctx->ev[2], ctx->st));
         CK(cudaEventSynchronize(ctx->ev[2]));
@@ -641,6 +714,8 @@ int run_forward(crt_ctx* ctx)
     ctx->timings[7] = ms_prep;
     ctx->timings[8] = ms_fk;
     ctx->timings[9] = nfl;
+    ctx->timings[10] = ms_res;
+    ctx->timings[11] = ms_cor;
     return collect_status(ctx, nfac);
 }
 
@@ -654,7 +729,10 @@ int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
             return CRT_ERR_ALLOC;
     }
     CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(int) * ctx->nstatus, ctx->st));
-    int e = ldc ? run_forward<double>(ctx) : run_forward<cd>(ctx);
+    // the mixed form factors the complex systems in complex64 and refines
+    const char* fv = std::getenv("CRT_B200_FACTOR");
+    const bool c64 = !ldc && ctx->prec == CRT_PREC_MIXED && band_blk_fits<cf>(ctx->mb) && !(fv && std::strcmp(fv, "v0") == 0);
+    int e = ldc ? run_forward<double>(ctx) : (c64 ? run_forward<cf>(ctx) : run_forward<cd>(ctx));
     if (e) return e;
     double* d_kfak = nullptr;
     if (kfak_h && mode == 1) {
@@ -1171,7 +1249,7 @@ int gn_step_device(crt_ctx* ctx, const crt_cg_params* prm, int* ncg)
     int e = forward_common(ctx, prm->ldc, 0, nullptr);
     if (e) return e;
     for (int i = 0; i < 3; ++i) tm[i] = ctx->timings[i];
-    for (int i = 7; i < 10; ++i) tm[i] = ctx->timings[i];
+    for (int i = 7; i < 12; ++i) tm[i] = ctx->timings[i];
     e = jacobian_device(ctx, prm->ldc ? 1 : 0, nullptr);
     if (e) return e;
     tm[3] = ctx->timings[3];

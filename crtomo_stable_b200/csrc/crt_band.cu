@@ -239,15 +239,22 @@ template <> __device__ __forceinline__ cd shfl_down_t<cd>(cd v, int off)
 {
     return cd{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)};
 }
+template <> __device__ __forceinline__ cf shfl_idx_t<cf>(cf v, int src)
+{
+    return cf{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
+}
+template <> __device__ __forceinline__ cf shfl_down_t<cf>(cf v, int off)
+{
+    return cf{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)};
+}
 
 template <typename T, int NT, int BB>
-__global__ void __launch_bounds__(NT, 3) k_band_solve(SolveArgs<T> A, T* scratch)
+__global__ void __launch_bounds__(NT, 2) k_band_solve(SolveArgs<T> A, T* scratch)
 {
     __shared__ T tri[BB][BB];
     __shared__ T part[BB];
     __shared__ T zb[BB];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = NT / 32;
     const int n = A.n, W = A.W, mb = A.mb;
     const int b = blockIdx.x, sys = A.sys0 + b;
     const int slot = b / A.factor_of_sys_div;
@@ -259,53 +266,72 @@ __global__ void __launch_bounds__(NT, 3) k_band_solve(SolveArgs<T> A, T* scratch
 
     // The fused forward pass belongs to the system's own right-hand side:
     // every (k, l) system with mixed boundaries, only electrode 1 otherwise
-    // (the reference refactors for l == 1 and calls kompb for l > 1).
-    const bool use_fused = A.yws && (A.mixed || l == 0);
+    // (the reference refactors for l == 1 and calls kompb for l > 1).  An
+    // explicit right-hand side (the refinement's residual) is solved in full.
+    const bool use_fused = A.yws && !A.rhs && (A.mixed || l == 0);
     if (use_fused) {
         const T* y = A.yws + (size_t)slot * n;
         for (int i = tid; i < n; i += NT) z[i] = y[i];
     } else {
-        // kompb right-hand side: b(enr(l)) = -fak, b(nsink) = +fak.
-        for (int i = tid; i < n; i += NT) z[i] = Sc<T>::zero();
-        __syncthreads();
-        if (tid == 0) {
-            const int src = A.enr0[l];
-            z[src] = scale(-Sc<T>::one(), fk[src]);
-            if (A.lsink) z[A.nsink0] = scale(Sc<T>::one(), fk[A.nsink0]);
-        }
-        __syncthreads();
-        // Forward substitution L y = b, right-looking by blocks.
-        for (int c0 = 0; c0 < n; c0 += BB) {
-            const int c1 = min(n, c0 + BB);
-            // in-block triangle, column-major: tri[c-c0][d]
-            for (int t = tid; t < BB * BB; t += NT) {
-                int cc = t / BB, d = t % BB;
-                int c = c0 + cc;
-                tri[cc][d] = (c < c1 && d <= mb && c + d < c1) ? Lc[(size_t)c * W + d] : Sc<T>::zero();
+        if (A.rhs) {
+            const T* rb = A.rhs + (size_t)b * n;
+            for (int i = tid; i < n; i += NT) z[i] = rb[i];
+        } else {
+            // kompb right-hand side: b(enr(l)) = -fak, b(nsink) = +fak.
+            for (int i = tid; i < n; i += NT) z[i] = Sc<T>::zero();
+            __syncthreads();
+            if (tid == 0) {
+                const int src = A.enr0[l];
+                z[src] = scale(-Sc<T>::one(), fk[src]);
+                if (A.lsink) z[A.nsink0] = scale(Sc<T>::one(), fk[A.nsink0]);
             }
-            if (tid < BB) zb[tid] = (c0 + tid < c1) ? z[c0 + tid] : Sc<T>::zero();
+        }
+        if (tid < BB) zb[tid] = Sc<T>::zero();
+        __syncthreads();
+        // Forward substitution L y = b by blocks of BB rows: the block's
+        // triangle is staged by columns and solved by warp 0 with one unknown
+        // per lane (reciprocal pivots, one shuffle broadcast per unknown);
+        // the following mb rows then take the block's columns right-looking
+        // (coalesced over the rows of a column).
+        for (int c0 = 0; c0 < n; c0 += BB) {
+            const int c1 = min(n, c0 + BB), nb = c1 - c0;
+            for (int t = tid; t < BB * BB; t += NT) {
+                const int cc = t / BB, d = t % BB, c = c0 + cc;
+                tri[cc][d] = (cc < nb && d <= mb && cc + d < nb) ? Lc[(size_t)c * W + d] : Sc<T>::zero();
+            }
             __syncthreads();
             if (warp == 0) {
-                for (int cc = 0; cc < c1 - c0; ++cc) {
-                    T yc = zb[cc];
-                    if (lane == 0) {
-                        yc = Sc<T>::div(yc, tri[cc][0]);
-                        zb[cc] = yc;
-                    }
-                    __syncwarp();
-                    yc = zb[cc];
-                    int d = lane;
-                    if (d >= 1 && cc + d < c1 - c0) zb[cc + d] -= Sc<T>::mul(tri[cc][d], yc);
-                    __syncwarp();
+                T v = Sc<T>::zero(), dinv = Sc<T>::zero();
+                if (lane < nb) {
+                    v = z[c0 + lane];
+                    dinv = Sc<T>::recip(tri[lane][0]);
+                }
+                for (int cc = 0; cc < nb; ++cc) {
+                    if (lane == cc) v = Sc<T>::mul(v, dinv);
+                    const T y = shfl_idx_t(v, cc);
+                    if (lane > cc && lane < nb) v -= Sc<T>::mul(tri[cc][lane - cc], y);
+                }
+                if (lane < nb) {
+                    z[c0 + lane] = v;
+                    zb[lane] = v;
                 }
             }
             __syncthreads();
-            if (tid < BB && c0 + tid < c1) z[c0 + tid] = zb[tid];
-            // rows beyond the block: b_r -= sum_c L(r, c) y_c
+            // rows beyond the block: b_r -= sum_c L(r, c) y_c, eight columns'
+            // loads in flight at a time (coalesced over the rows of a column)
             for (int r = c1 + tid; r < min(n, c1 + mb); r += NT) {
+                const int cc0 = max(0, r - mb - c0);
                 T acc = Sc<T>::zero();
-                for (int cc = max(0, r - mb - c0); cc < c1 - c0; ++cc)
-                    acc += Sc<T>::mul(Lc[(size_t)(c0 + cc) * W + (r - c0 - cc)], zb[cc]);
+                for (int cb = 0; cb < BB; cb += 8) {
+                    T lv[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const int cc = cb + u;
+                        lv[u] = (cc >= cc0 && cc < nb) ? Lc[(size_t)(c0 + cc) * W + (r - c0 - cc)] : Sc<T>::zero();
+                    }
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) acc += Sc<T>::mul(lv[u], zb[cb + u]);
+                }
                 z[r] -= acc;
             }
             __syncthreads();
@@ -359,9 +385,14 @@ __global__ void __launch_bounds__(NT, 3) k_band_solve(SolveArgs<T> A, T* scratch
         }
         __syncthreads();
     }
-    // kpot(j, l, k) = pot(j) * fak(j) with pot = -z.
+    // kpot(j, l, k) = pot(j) * fak(j) with pot = -z (a refinement step adds
+    // the correction's contribution).
     cd* out = A.kpot + ((size_t)k * A.L + l) * n;
-    for (int j = tid; j < n; j += NT) out[j] = Sc<T>::to_cd(scale(-z[j], fk[j]));
+    if (A.accumulate) {
+        for (int j = tid; j < n; j += NT) out[j] = out[j] - Sc<T>::to_cd(z[j]) * fk[j];
+    } else {
+        for (int j = tid; j < n; j += NT) out[j] = Sc<T>::to_cd(scale(-z[j], fk[j]));
+    }
     (void)A.status;
 }
 
@@ -399,3 +430,4 @@ template void launch_band_factor<double>(const BandArgs<double>&, cudaStream_t);
 template void launch_band_factor<cd>(const BandArgs<cd>&, cudaStream_t);
 template void launch_band_solve_with_scratch<double>(const SolveArgs<double>&, double*, cudaStream_t);
 template void launch_band_solve_with_scratch<cd>(const SolveArgs<cd>&, cd*, cudaStream_t);
+template void launch_band_solve_with_scratch<cf>(const SolveArgs<cf>&, cf*, cudaStream_t);

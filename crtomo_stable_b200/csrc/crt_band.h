@@ -27,6 +27,8 @@ struct BandArgs {
     T* yws;                  // [b][n] forward-substitution result
     double* fakws;           // [b][n] scaling factors
     int* status;             // [total systems] errnr per system
+    cd* aval;                // [b][row_ptr[n]] the prepared (scaled, edited) entries in FP64, or NULL
+    size_t aval_stride;
 };
 
 template <typename T>
@@ -42,6 +44,8 @@ struct SolveArgs {
     int factor_of_sys_div;   // workspace slot of system s: (s - sys0) / factor_of_sys_div
     cd* kpot;                // kpot(sanz, eanz, kwnanz) Fortran order
     int* status;
+    const T* rhs;            // [b][n] explicit right-hand sides (refinement), or NULL
+    int accumulate;          // 1: kpot += the solution's contribution instead of kpot =
 };
 
 template <typename T> void launch_band_factor(const BandArgs<T>& a, cudaStream_t st);
@@ -53,6 +57,12 @@ template <typename T> bool band_blk_fits(int mb);
 // Preparation pass of the panel-blocked factor: assembled, Dirichlet-edited
 // and scaled rows written row-packed into a.Lws, scaling factors into a.fakws.
 template <typename T> void launch_band_prep(const BandArgs<T>& a, cudaStream_t st);
+// FP64 residual b^ - A^ z of the scaled systems for a refinement step, z from
+// kpot, A^ from the entries the preparation pass kept in a.aval; solve
+// systems sys0 .. sys0+nsolve-1, factor slot b / div; stored as T.
+template <typename T>
+void launch_band_residual(const BandArgs<T>& a, int sys0, int nsolve, int div, const int* up_ptr, const int* up_ent,
+                          const int* up_row, const cd* kpot, T* rout, cudaStream_t st);
 // scratch: one n-vector per launched system (may alias the fused y workspace).
 template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st);
 template <typename T> size_t band_factor_smem(int W);

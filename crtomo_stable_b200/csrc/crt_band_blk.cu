@@ -52,23 +52,12 @@ __device__ __forceinline__ int widx(int x, int y)
     return tile_base(x >> 2, y >> 2) * TSTRIDE + ((x & 3) << 2) + (y & 3);
 }
 
-template <typename T>
-__device__ __forceinline__ T shfl_T(T v, int src);
-template <>
-__device__ __forceinline__ double shfl_T<double>(double v, int src)
+// One assembled band entry (kompab's sum over the entry's element and
+// boundary contributions), formed in the arithmetic W.
+template <typename W, typename T>
+__device__ __forceinline__ W assemble_entry_w(const BandArgs<T>& A, int e, int k, int l)
 {
-    return __shfl_sync(0xffffffffu, v, src);
-}
-template <>
-__device__ __forceinline__ cd shfl_T<cd>(cd v, int src)
-{
-    return cd{__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src)};
-}
-
-template <typename T>
-__device__ __forceinline__ T assemble_entry_b(const BandArgs<T>& A, int e, int k, int l)
-{
-    T v = Sc<T>::zero();
+    W v = Sc<W>::zero();
     const int c1 = A.ent_ptr[e + 1];
     const double* elbg_k = A.elbg + (size_t)k * A.E * A.nmn;
     for (int c = A.ent_ptr[e]; c < c1; ++c) {
@@ -80,7 +69,7 @@ __device__ __forceinline__ T assemble_entry_b(const BandArgs<T>& A, int e, int k
             const int q = -code - 1;
             coef = A.relbg[q] * A.kg[((size_t)k * A.L + l) * A.R + q / 3];
         }
-        v += scale(Sc<T>::from(A.sigma[A.con_sig[c]]), coef);
+        v += scale(Sc<W>::from(A.sigma[A.con_sig[c]]), coef);
     }
     return v;
 }
@@ -118,22 +107,29 @@ __device__ __forceinline__ void sys_kl(const BandArgs<T>& A, int sys, int& k, in
 template <typename T>
 __global__ void k_band_prep_diag(BandArgs<T> A)
 {
+    using WT = typename Wide<T>::type;   // formed in FP64, stored as T
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n = A.n;
     if (idx >= (long long)A.nsys * n) return;
     const int b = (int)(idx / n), r = (int)(idx % n), sys = A.sys0 + b;
     int k, l;
     sys_kl(A, sys, k, l);
-    T raw = Sc<T>::zero();
+    WT raw = Sc<WT>::zero();
+    int e0 = -1;
     for (int e = A.row_ptr[r]; e < A.row_ptr[r + 1]; ++e)
-        if (A.ent_d[e] == 0) raw = assemble_entry_b(A, e, k, l);
-    if (A.dflag[r]) raw = Sc<T>::one();
-    const double d = Sc<T>::absval(raw);
+        if (A.ent_d[e] == 0) {
+            raw = assemble_entry_w<WT>(A, e, k, l);
+            e0 = e;
+        }
+    if (A.dflag[r]) raw = Sc<WT>::one();
+    const double d = Sc<WT>::absval(raw);
     double f = 1.0;
     if (!(d > 0.0)) A.status[sys] = CRT_ERR_ZERO_DIAG;
     else f = 1.0 / sqrt(d);
     A.fakws[(size_t)b * n + r] = f;
-    A.Lws[(size_t)b * A.lstride + (size_t)r * A.W] = Sc<T>::normalise(raw, d);
+    const WT dn = Sc<WT>::normalise(raw, d);
+    A.Lws[(size_t)b * A.lstride + (size_t)r * A.W] = narrow<T>(dn);
+    if (A.aval && e0 >= 0) A.aval[(size_t)b * A.aval_stride + e0] = Sc<WT>::to_cd(dn);
 }
 
 // Off-diagonal entries of every row, one warp per row: zero fill, then
@@ -157,14 +153,49 @@ __global__ void k_band_prep_rows(BandArgs<T> A)
         const int d = A.ent_d[e];
         if (d == 0) continue;
         const int c = r - d;
-        T v = Sc<T>::zero();
-        if (!dr && A.dflag[c] == 0) v = scale(assemble_entry_b(A, e, k, l), fr * fk[c]);
-        row[d] = v;
+        typename Wide<T>::type v = Sc<typename Wide<T>::type>::zero();
+        if (!dr && A.dflag[c] == 0) v = scale(assemble_entry_w<typename Wide<T>::type>(A, e, k, l), fr * fk[c]);
+        row[d] = narrow<T>(v);
+        if (A.aval) A.aval[(size_t)b * A.aval_stride + e] = Sc<typename Wide<T>::type>::to_cd(v);
     }
 }
 
-template <typename T, int PB, int NT>
-__global__ void __launch_bounds__(NT, 1) k_band_factor_blk(BandArgs<T> A, int Wn)
+// Residual of the scaled system for one step of iterative refinement, in
+// FP64:  r = b^ - A^ z  with  z_c = -kpot_c / fak_c  (kpot = -fak o z), A^
+// the matrix the preparation pass formed (its FP64 entries kept per gather
+// entry in A.aval: the scaled, Dirichlet-edited a(r, c) fak_r fak_c and the
+// normalised diagonal), b^ = fak o rhs.  One thread per row of every
+// system: the row's own entries give the lower part and the diagonal, the
+// transposed list the upper part.  A Dirichlet row is the identity row.
+// The residual is stored in T for the correction solve.  Solve system b is
+// (k, l) = (sys0 + b) / L, % L, its factor slot b / div.
+template <typename T>
+__global__ void k_band_residual(BandArgs<T> A, int sys0, int nsolve, int div, const int* __restrict__ up_ptr,
+                                const int* __restrict__ up_ent, const int* __restrict__ up_row,
+                                const cd* __restrict__ kpot, T* rout)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = A.n;
+    if (idx >= (long long)nsolve * n) return;
+    const int b = (int)(idx / n), r = (int)(idx % n), sys = sys0 + b;
+    const int l = sys % A.L, slot = b / div;
+    const double* fk = A.fakws + (size_t)slot * n;
+    const cd* kp = kpot + (size_t)sys * n;
+    const cd* av = A.aval + (size_t)slot * A.aval_stride;
+    auto zval = [&](int c) { return cd{-kp[c].x / fk[c], -kp[c].y / fk[c]}; };
+    cd acc{0.0, 0.0};
+    if (A.dflag[r]) {
+        acc = zval(r);
+    } else {
+        for (int e = A.row_ptr[r]; e < A.row_ptr[r + 1]; ++e) acc += av[e] * zval(r - A.ent_d[e]);
+        for (int q = up_ptr[r]; q < up_ptr[r + 1]; ++q) acc += av[up_ent[q]] * zval(up_row[q]);
+    }
+    const cd bb = scale(rhs_entry_b<cd>(r, A.enr0[l], A.lsink, A.nsink0, A.dflag, A.dval, nullptr), fk[r]);
+    rout[(size_t)b * n + r] = narrow<T>(bb - acc);
+}
+
+template <typename T, int PB, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int Wn)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = A.n, mb = A.mb, W1 = A.W;    // W1 = mb + 1 (column stride of the HBM factor)
@@ -233,17 +264,15 @@ __global__ void __launch_bounds__(NT, 1) k_band_factor_blk(BandArgs<T> A, int Wn
     // are written by those rows.
     auto scatter_rows = [&](int r0, int s_new, int wlo) {
         const int wm = wlo % Wn;
-        for (int y = tid; y < Wn; y += NT) {
+        for (int i = tid; i < PB * Wn; i += NT) {
+            const int q = i % PB, y = i / PB;             // PB is a power of two
             int off = y - wm;
             if (off < 0) off += Wn;
             const int c = wlo + off;                      // row held by slot y
-#pragma unroll
-            for (int q = 0; q < PB; ++q) {
-                const int r = r0 + q;
-                if (c > r) continue;
-                const int d = r - c;
-                win[widx(s_new + q, y)] = (r < n && d <= mb) ? stage[q * W1 + d] : Sc<T>::zero();
-            }
+            const int r = r0 + q;
+            if (c > r) continue;
+            const int d = r - c;
+            win[widx(s_new + q, y)] = (r < n && d <= mb) ? stage[q * W1 + d] : Sc<T>::zero();
         }
         if (tid < PB) bsl[s_new + tid] = bN[tid];
     };
@@ -474,18 +503,39 @@ void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
 template <typename T>
 bool launch_band_factor_blk(const BandArgs<T>& a, cudaStream_t st)
 {
-    constexpr int NT = 512, PB = 8;
+    constexpr int PB = 8;
     int Wn = 0;
     const size_t smem = blk_smem<T, PB>(a.mb, &Wn);
     if (!band_blk_fits<T>(a.mb)) return false;
-    cudaFuncSetAttribute(k_band_factor_blk<T, PB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_band_factor_blk<T, PB, NT><<<a.nsys, NT, smem, st>>>(a, Wn);
+    // a window that fits twice (complex64, or real FP64) runs as two
+    // 256-thread CTAs per SM, overlapping one system's serial phases with the
+    // other's update; a complex128 window leaves room for one CTA of 512
+    auto go = [&](auto kern, int nt) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<a.nsys, nt, smem, st>>>(a, Wn);
+    };
+    if (2 * smem <= 227 * 1024) go(k_band_factor_blk<T, PB, 256, 2>, 256);
+    else go(k_band_factor_blk<T, PB, 512, 1>, 512);
     return true;
+}
+
+template <typename T>
+void launch_band_residual(const BandArgs<T>& a, int sys0, int nsolve, int div, const int* up_ptr, const int* up_ent,
+                          const int* up_row, const cd* kpot, T* rout, cudaStream_t st)
+{
+    const long long rows = (long long)nsolve * a.n;
+    k_band_residual<T><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(a, sys0, nsolve, div, up_ptr, up_ent, up_row,
+                                                                     kpot, rout);
 }
 
 template bool band_blk_fits<double>(int);
 template bool band_blk_fits<cd>(int);
+template bool band_blk_fits<cf>(int);
 template void launch_band_prep<double>(const BandArgs<double>&, cudaStream_t);
 template void launch_band_prep<cd>(const BandArgs<cd>&, cudaStream_t);
+template void launch_band_prep<cf>(const BandArgs<cf>&, cudaStream_t);
 template bool launch_band_factor_blk<double>(const BandArgs<double>&, cudaStream_t);
 template bool launch_band_factor_blk<cd>(const BandArgs<cd>&, cudaStream_t);
+template bool launch_band_factor_blk<cf>(const BandArgs<cf>&, cudaStream_t);
+template void launch_band_residual<cf>(const BandArgs<cf>&, int, int, int, const int*, const int*, const int*,
+                                       const cd*, cf*, cudaStream_t);

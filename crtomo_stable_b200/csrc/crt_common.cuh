@@ -12,7 +12,7 @@
 #define CRT_HD __host__ __device__ __forceinline__
 
 // entries of crt_last_timings_ex
-#define CRT_NTIMINGS 10
+#define CRT_NTIMINGS 12
 
 struct __align__(16) cd {
     double x, y;
@@ -24,6 +24,12 @@ struct __align__(8) cf {
 };
 
 CRT_HD cd mk(double x, double y) { return cd{x, y}; }
+CRT_HD cf operator+(cf a, cf b) { return cf{a.x + b.x, a.y + b.y}; }
+CRT_HD cf operator-(cf a, cf b) { return cf{a.x - b.x, a.y - b.y}; }
+CRT_HD cf operator-(cf a) { return cf{-a.x, -a.y}; }
+CRT_HD cf operator*(cf a, cf b) { return cf{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x}; }
+CRT_HD cf& operator+=(cf& a, cf b) { a.x += b.x; a.y += b.y; return a; }
+CRT_HD cf& operator-=(cf& a, cf b) { a.x -= b.x; a.y -= b.y; return a; }
 CRT_HD cd operator+(cd a, cd b) { return cd{a.x + b.x, a.y + b.y}; }
 CRT_HD cd operator-(cd a, cd b) { return cd{a.x - b.x, a.y - b.y}; }
 CRT_HD cd operator-(cd a) { return cd{-a.x, -a.y}; }
@@ -141,8 +147,57 @@ CRT_HD void fms_acc(cd& acc, cd a, cd b)
 }
 CRT_HD void fms_acc(double& acc, double a, double b) { acc = fma(-a, b, acc); }
 
+CRT_HD void fms_acc(cf& acc, cf a, cf b)
+{
+    acc.x = fmaf(-a.x, b.x, acc.x);
+    acc.x = fmaf(a.y, b.y, acc.x);
+    acc.y = fmaf(-a.x, b.y, acc.y);
+    acc.y = fmaf(-a.y, b.x, acc.y);
+}
+CRT_HD cf scale(cf a, double s) { return cf{(float)(a.x * s), (float)(a.y * s)}; }
+
 CRT_HD double scale(double a, double s) { return a * s; }
 CRT_HD cd scale(cd a, double s) { return cd{a.x * s, a.y * s}; }
+
+// complex64 storage and arithmetic of the mixed-precision factorisation
+// (the quantities it is formed from are computed in FP64, see crt_band_blk.cu)
+template <> struct Sc<cf> {
+    static CRT_HD cf zero() { return cf{0.0f, 0.0f}; }
+    static CRT_HD cf one() { return cf{1.0f, 0.0f}; }
+    static CRT_HD cf from(cd s) { return cf{(float)s.x, (float)s.y}; }
+    static CRT_HD double absval(cf a) { return hypot((double)a.x, (double)a.y); }
+    static CRT_HD cf normalise(cf a, double d) { return cf{(float)(a.x / d), (float)(a.y / d)}; }
+    static CRT_HD bool bad_pivot(cf s) { return !(s.x * s.x + s.y * s.y > 0.0f); }
+    static __device__ __forceinline__ void sqrt_recip(cf z, cf& root, cf& inv)
+    {
+        const float r2 = z.x * z.x + z.y * z.y;
+        if (!(r2 > 0.0f)) {
+            root = cf{0.0f, 0.0f};
+            inv = cf{0.0f, 0.0f};
+            return;
+        }
+        const float ir = rsqrtf(r2), r = r2 * ir;
+        const float u = 0.5f * (r + fabsf(z.x));
+        const float iu = rsqrtf(u), t = u * iu, h = 0.5f * iu;
+        root = z.x >= 0.0f ? cf{t, z.y * h} : cf{fabsf(z.y) * h, copysignf(t, z.y)};
+        inv = cf{root.x * ir, -root.y * ir};
+    }
+    static CRT_HD cf mul(cf a, cf b) { return a * b; }
+    static CRT_HD cf recip(cf a)
+    {
+        const float s = 1.0f / (a.x * a.x + a.y * a.y);
+        return cf{a.x * s, -a.y * s};
+    }
+    static CRT_HD cd to_cd(cf a) { return cd{(double)a.x, (double)a.y}; }
+};
+
+// FP64 type in which a storage type's values are formed
+template <typename T> struct Wide { using type = T; };
+template <> struct Wide<cf> { using type = cd; };
+template <typename T> CRT_HD T narrow(typename Wide<T>::type v);
+template <> CRT_HD double narrow<double>(double v) { return v; }
+template <> CRT_HD cd narrow<cd>(cd v) { return v; }
+template <> CRT_HD cf narrow<cf>(cd v) { return cf{(float)v.x, (float)v.y}; }
 
 // Reference error numbers (src/error.txt) returned through the C ABI.
 enum crt_errnr : int32_t {

@@ -67,7 +67,7 @@ EXPORTS = [
     "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
     "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order", "crt_last_timings_ex",
-    "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
+    "crt_set_refinement", "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
     "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad",
 ]
 
@@ -124,6 +124,8 @@ def load(path: str = LIB_PATH):
     L.crt_gn_step_device.restype = C.c_int32
     L.crt_last_timings.argtypes = [vp, f64p]
     L.crt_last_timings.restype = C.c_int32
+    L.crt_set_refinement.argtypes = [vp, C.c_int32]
+    L.crt_set_refinement.restype = C.c_int32
     L.crt_last_timings_ex.argtypes = [vp, f64p, C.c_int32]
     L.crt_last_timings_ex.restype = C.c_int32
     L.crt_cg_info.argtypes = [vp, i32p, i32p, i32p]
@@ -404,7 +406,7 @@ class Context:
         return ncg.value
 
     TIMING_NAMES = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total", "factor_prep",
-                    "factor_kernel", "factor_launches"]
+                    "factor_kernel", "factor_launches", "refine_residual", "refine_solve"]
 
     def timings(self):
         t = np.zeros(len(self.TIMING_NAMES))
@@ -413,6 +415,9 @@ class Context:
 
     def launch_count(self):
         return int(self.L.crt_launch_count(self.h))
+
+    def set_refinement(self, steps):
+        self._check(self.L.crt_set_refinement(self.h, int(steps)), "crt_set_refinement")
 
     # -- learned correction of the preconditioner -------------------------
     def gnn_nparam(self):

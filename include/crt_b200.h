@@ -94,13 +94,21 @@ typedef struct {
 
 /* Precision forms.
  * CRT_PREC_FP64:  everything in FP64 / complex128 (the reference's arithmetic).
- * CRT_PREC_MIXED: the Jacobian is stored in FP32 / complex64 (computed in
- *                 FP64, rounded on store) and the CG accumulates in FP64;
- *                 band factorisations run in complex64 with FP64 iterative
- *                 refinement of the potentials where enabled.  Dot products,
- *                 quadrature weights, misfit and model update stay FP64. */
+ * CRT_PREC_MIXED: the complex band systems are assembled and scaled in FP64,
+ *                 factored and solved in complex64, and refined in FP64
+ *                 (crt_set_refinement); the Jacobian is computed in FP64 and
+ *                 stored in complex64; the CG accumulates in FP64.  Dot
+ *                 products, quadrature weights, misfit and model update stay
+ *                 FP64.  The DC (real) systems stay FP64. */
 #define CRT_PREC_FP64 0
 #define CRT_PREC_MIXED 1
+
+/* Steps of FP64 iterative refinement after the complex64 factorisation of
+ * the mixed form (default 2; 0 leaves the complex64 solution): each step
+ * forms the residual of the scaled system in FP64 (re-assembled from the
+ * element matrices) and adds a complex64 correction solve.  No reference
+ * counterpart. */
+int32_t crt_set_refinement(crt_ctx *ctx, int32_t steps);
 
 /* Creates a context on `device`: uploads the mesh, builds the gather lists
  * of the streamed assembly, and evaluates precal on the device unless the
@@ -202,8 +210,9 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
 /* The same and more, up to n entries: [0..6] as crt_last_timings, [7] the
  * preparation pass of the forward factor (assembly, Dirichlet edits and
  * scaling of all rows), [8] the factor kernels alone, [9] the number of
- * factor-kernel launches (one per chunk of systems).  Milliseconds except
- * [9].  No reference counterpart. */
+ * factor-kernel launches (one per chunk of systems), [10] the FP64
+ * residuals and [11] the correction solves of the mixed form's refinement
+ * (both inside [1]).  Milliseconds except [9].  No reference counterpart. */
 int32_t crt_last_timings_ex(const crt_ctx *ctx, double *ms, int32_t n);
 
 /* Kernel launches enqueued by the context since creation. */

@@ -80,3 +80,19 @@ def test_create_without_device_fails_loudly():
     with pytest.raises(CRTError) as ei:
         Context(m, e, d.strnr, d.vnr)
     assert ei.value.errnr == 200
+
+
+def test_library_resolves_its_own_templates():
+    """Every kernel launcher the library instantiates is defined in it (an
+    explicit instantiation missing for one precision would only fail when the
+    library is loaded on a GPU box)."""
+    import shutil
+    import subprocess
+    from crtomo_stable_b200 import build
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not available")
+    lib = build.build()
+    out = subprocess.run([nm, "-D", "--undefined-only", lib], capture_output=True, text=True).stdout
+    own = [ln for ln in out.splitlines() if "launch_" in ln or "crt_" in ln or "gnn_" in ln or "spc_" in ln]
+    assert not own, own

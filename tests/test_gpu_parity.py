@@ -330,14 +330,18 @@ def test_forward_narrow_band_matches_oracle(nz):
     ctx.close()
 
 
-def test_mixed_form_jacobian_is_fp64_rounded_to_fp32():
-    """CRT_PREC_MIXED stores the Jacobian in complex64: every entry equals the
-    FP64 oracle's to float32 rounding (relative 2**-24 of the entry, plus the
-    FP64 tolerance of the column)."""
+@pytest.mark.parametrize("nref", [1, 2])
+def test_mixed_form_jacobian_accuracy(nref):
+    """CRT_PREC_MIXED: potentials from the complex64 factorisation refined in
+    FP64, the Jacobian formed in FP64 and stored in complex64.  With the
+    default two refinement steps the potentials are FP64-accurate and every
+    entry equals the oracle's rounded to float32 (relative 2**-24, plus the
+    FP64 tolerance of the column), well inside the stated 1e-6; a single
+    step leaves errors of a few 1e-6 of the column maximum."""
     from crtomo_stable_b200.lib import PREC_MIXED, Context
     case = load_forward_case("TestModInv")
-    c = case["cfg"]
     ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, precision=PREC_MIXED)
+    ctx.set_refinement(nref)
     op = _oracle(case)
     ctx.forward(case["sigma"])
     J_g = ctx.jacobian(mode=0)
@@ -346,7 +350,11 @@ def test_mixed_form_jacobian_is_fp64_rounded_to_fp32():
     J_o = op.bsensi(kp, case["sigma"], volt_o, nthreads=4)
     colmax = np.abs(J_o).max(axis=0, keepdims=True) + 1e-300
     err = np.abs(J_g - J_o)
-    assert (err <= 1.2e-7 * np.abs(J_o) + RTOL_SENS * colmax).all()
+    print(f"\nmixed Jacobian, {nref} refinement step(s): max error / column max {(err / colmax).max():.1e}")
+    if nref == 1:
+        assert (err / colmax).max() <= 1e-5
+    else:
+        assert (err <= 1.2e-7 * np.abs(J_o) + RTOL_SENS * colmax).all()
     ctx.close()
 
 
@@ -540,3 +548,34 @@ def test_jacobian_gram_and_direct_kernels_agree(name, mode, monkeypatch):
         ctx.close()
     colmax = np.abs(outs[1]).max(axis=0, keepdims=True) + 1e-300
     assert (np.abs(outs[0] - outs[1]) / colmax).max() <= RTOL_SENS
+
+
+@pytest.mark.parametrize("name", ["TestModInv", "minimal", "mixed_surf", "grid_decoupling"])
+def test_mixed_form_forward_is_refined_to_fp64(name):
+    """The mixed form factors the complex systems in complex64 and refines in
+    FP64: with the default two steps the potentials and voltages agree with
+    the FP64 oracle to 1e-9 (the stated target is 1e-6), one step already
+    reaches 1e-6; without refinement the complex64 solution alone is off by
+    far more than FP64 rounding."""
+    from crtomo_stable_b200.lib import PREC_MIXED, Context
+    case = load_forward_case(name)
+    m = case["mesh"]
+    c = case["cfg"]
+    op = _oracle(case)
+    kp_o = op.forward(case["sigma"], nthreads=4)
+    volt_o, _ = op.bvolti(op.rtrafo(kp_o))
+    errs = {}
+    for nref in (2, 1, 0):
+        ctx = Context(m, case["enr"], case["volt"].strnr, case["volt"].vnr, precision=PREC_MIXED,
+                      swrtr=c.swrtr, lsink=c.lsink, nsink=c.nsink)
+        ctx.set_refinement(nref)
+        volt_g, _, kp_g = ctx.forward(case["sigma"], want_kpot=True)
+        scale = np.abs(kp_o).max()
+        errs[nref] = (_kpot_diff(kp_g, kp_o, _singular(case)) / scale,
+                      np.abs(volt_g - volt_o).max() / np.abs(volt_o).max())
+        ctx.close()
+    print(f"\n{name}: two steps kpot {errs[2][0]:.1e} volt {errs[2][1]:.1e}; one step kpot {errs[1][0]:.1e} "
+          f"volt {errs[1][1]:.1e}; complex64 only kpot {errs[0][0]:.1e} volt {errs[0][1]:.1e}")
+    assert errs[2][0] <= 1e-9 and errs[2][1] <= 1e-9
+    assert errs[1][0] <= 1e-6 and errs[1][1] <= 1e-6
+    assert errs[0][0] > 10 * errs[2][0]
