@@ -47,8 +47,8 @@ FACTOR_TRAFFIC_BYTES_PER_ENTRY = 31.8
 # the rooflines of the complex128 / complex64 band factorisation.
 FP64_FMA_PER_CLK_SM = 64
 FP32_FMA_PER_CLK_SM = 128
-# complex64: to be filled from an ncu capture of the complex64 factor
-FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 = None
+# complex64: 4.164 GB for 125 C3 systems (profiles/k_band_factor_blk_C3.md)
+FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 = 15.9
 
 
 def parse():
