@@ -555,7 +555,11 @@ namespace {
 template <typename T>
 int run_forward(crt_ctx* ctx)
 {
-    const int n = ctx->n, W = ctx->W, L = ctx->L, K = ctx->K;
+    const int n = ctx->n, L = ctx->L, K = ctx->K;
+    // column stride of the factor workspace: mb + 1, rounded up to even for
+    // complex64 so every column starts on a 16-byte boundary (the solve's
+    // asynchronous block copies need that)
+    const int W = std::is_same<T, cf>::value ? (ctx->W + 1) / 2 * 2 : ctx->W;
     const bool mixed = ctx->lbeta != 0;
     const int nfac = mixed ? K * L : K;
     const size_t slot_bytes = (size_t)n * W * sizeof(T);

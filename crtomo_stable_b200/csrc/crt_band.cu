@@ -248,12 +248,34 @@ template <> __device__ __forceinline__ cf shfl_down_t<cf>(cf v, int off)
     return cf{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)};
 }
 
+// 16-byte asynchronous global -> shared copies (the prefetch of the solve's
+// next block of columns).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Resident CTAs per SM of the solve: complex64 state is small enough for
+// three (latency hiding across systems), complex128 for two.
+template <typename T> struct SolveOcc { static constexpr int v = 2; };
+// complex64 solves stage the next block of 32 columns of the factor (one
+// contiguous run: the factor is column-packed with an even column stride)
+// in a shared double buffer while the current block is solved
+template <typename T> struct SolvePrefetch { static constexpr bool v = false; };
+template <> struct SolvePrefetch<cf> { static constexpr bool v = true; };
+
 template <typename T, int NT, int BB>
-__global__ void __launch_bounds__(NT, 2) k_band_solve(SolveArgs<T> A, T* scratch)
+__global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> A, T* scratch)
 {
     __shared__ T tri[BB][BB];
     __shared__ T part[BB];
     __shared__ T zb[BB];
+    extern __shared__ __align__(16) unsigned char solve_dyn[];
+    T* lbuf = reinterpret_cast<T*>(solve_dyn);   // [2][BB * W] (prefetching form)
+    constexpr bool PF = SolvePrefetch<T>::v;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = A.n, W = A.W, mb = A.mb;
     const int b = blockIdx.x, sys = A.sys0 + b;
@@ -263,6 +285,14 @@ __global__ void __launch_bounds__(NT, 2) k_band_solve(SolveArgs<T> A, T* scratch
     const T* Lc = A.Lws + (size_t)slot * A.lstride;
     const double* fk = A.fakws + (size_t)slot * n;
     T* z = scratch + (size_t)b * n;
+    // columns [c0, c0 + nb) of the factor into buffer `buf` (async)
+    auto prefetch = [&](int c0, int nb, int buf) {
+        const char* src = reinterpret_cast<const char*>(Lc + (size_t)c0 * W);
+        char* dst = reinterpret_cast<char*>(lbuf + (size_t)buf * BB * W);
+        const int bytes = nb * W * (int)sizeof(T);
+        for (int off = tid * 16; off < bytes; off += NT * 16) cp_async16(dst + off, src + off);
+        cp_async_commit();
+    };
 
     // The fused forward pass belongs to the system's own right-hand side:
     // every (k, l) system with mixed boundaries, only electrode 1 otherwise
@@ -293,11 +323,21 @@ __global__ void __launch_bounds__(NT, 2) k_band_solve(SolveArgs<T> A, T* scratch
         // per lane (reciprocal pivots, one shuffle broadcast per unknown);
         // the following mb rows then take the block's columns right-looking
         // (coalesced over the rows of a column).
+        if constexpr (PF) {
+            prefetch(0, min(n, BB), 0);
+            cp_async_wait_all();
+            __syncthreads();
+        }
+        int fbuf = 0;
         for (int c0 = 0; c0 < n; c0 += BB) {
             const int c1 = min(n, c0 + BB), nb = c1 - c0;
+            const T* blk = PF ? lbuf + (size_t)fbuf * BB * W : Lc + (size_t)c0 * W;   // column c0 + cc at cc * W
+            if constexpr (PF) {
+                if (c1 < n) prefetch(c1, min(n, c1 + BB) - c1, fbuf ^ 1);
+            }
             for (int t = tid; t < BB * BB; t += NT) {
-                const int cc = t / BB, d = t % BB, c = c0 + cc;
-                tri[cc][d] = (cc < nb && d <= mb && cc + d < nb) ? Lc[(size_t)c * W + d] : Sc<T>::zero();
+                const int cc = t / BB, d = t % BB;
+                tri[cc][d] = (cc < nb && d <= mb && cc + d < nb) ? blk[(size_t)cc * W + d] : Sc<T>::zero();
             }
             __syncthreads();
             if (warp == 0) {
@@ -327,14 +367,16 @@ __global__ void __launch_bounds__(NT, 2) k_band_solve(SolveArgs<T> A, T* scratch
 #pragma unroll
                     for (int u = 0; u < 8; ++u) {
                         const int cc = cb + u;
-                        lv[u] = (cc >= cc0 && cc < nb) ? Lc[(size_t)(c0 + cc) * W + (r - c0 - cc)] : Sc<T>::zero();
+                        lv[u] = (cc >= cc0 && cc < nb) ? blk[(size_t)cc * W + (r - c0 - cc)] : Sc<T>::zero();
                     }
 #pragma unroll
                     for (int u = 0; u < 8; ++u) acc += Sc<T>::mul(lv[u], zb[cb + u]);
                 }
                 z[r] -= acc;
             }
+            if constexpr (PF) cp_async_wait_all();
             __syncthreads();
+            fbuf ^= 1;
         }
     }
     __syncthreads();
@@ -350,12 +392,21 @@ __global__ void __launch_bounds__(NT, 2) k_band_solve(SolveArgs<T> A, T* scratch
     static_assert(BB == 32 && TPC * BB == NT && (TPC & (TPC - 1)) == 0, "solve layout");
     __shared__ T trw[BB][BB + 1];   // trw[r][c] = L(c0 + r, c0 + c), r >= c
     const int col = tid / TPC, sub = tid % TPC;
+    if constexpr (PF) {
+        prefetch(max(0, n - BB), n - max(0, n - BB), 0);
+        cp_async_wait_all();
+        __syncthreads();
+    }
+    int bbuf = 0;
     for (int c1 = n; c1 > 0; c1 -= BB) {
         const int c0 = max(0, c1 - BB), nb = c1 - c0;
+        if constexpr (PF) {
+            if (c0 > 0) prefetch(max(0, c0 - BB), c0 - max(0, c0 - BB), bbuf ^ 1);
+        }
         T acc = Sc<T>::zero();
         if (col < nb) {
             const int c = c0 + col;
-            const T* Lcol = Lc + (size_t)c * W;
+            const T* Lcol = PF ? lbuf + (size_t)bbuf * BB * W + (size_t)col * W : Lc + (size_t)c * W;
             const int dmax = min(mb, n - 1 - c);
             const int din = nb - col;          // d < din: rows inside the block
             const int dend = max(dmax, din - 1);
@@ -383,7 +434,9 @@ __global__ void __launch_bounds__(NT, 2) k_band_solve(SolveArgs<T> A, T* scratch
             }
             if (lane < nb) z[c0 + lane] = v;
         }
+        if constexpr (PF) cp_async_wait_all();
         __syncthreads();
+        bbuf ^= 1;
     }
     // kpot(j, l, k) = pot(j) * fak(j) with pot = -z (a refinement step adds
     // the correction's contribution).
@@ -421,7 +474,12 @@ template <typename T>
 void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st)
 {
     constexpr int NT = 256, BB = 32;
-    k_band_solve<T, NT, BB><<<a.nsys, NT, 0, st>>>(a, scratch);
+    size_t dyn = 0;
+    if (SolvePrefetch<T>::v) {
+        dyn = 2 * (size_t)BB * a.W * sizeof(T);
+        cudaFuncSetAttribute(k_band_solve<T, NT, BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    }
+    k_band_solve<T, NT, BB><<<a.nsys, NT, dyn, st>>>(a, scratch);
 }
 
 template size_t band_factor_smem<double>(int);
