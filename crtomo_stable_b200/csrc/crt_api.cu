@@ -100,6 +100,11 @@ struct crt_ctx {
     Gnn gnn;
     int gnn_guard = 0;   // the last solve switched the learned correction off
     int prec = CRT_PREC_FP64;
+    // enqueue-only pass (stream capture into a batch graph): no host
+    // synchronisation, no timing reads, no allocation, status read later
+    int capture = 0;
+    size_t ws_budget = 0;   // factor workspace budget in bytes (0: default)
+    int panel = 0;          // panel width of the last blocked factorisation
 };
 
 namespace {
@@ -151,6 +156,7 @@ int set_err(crt_ctx* ctx, int code, const std::string& msg)
 // First non-zero per-system status (the reference stops at the first error).
 int collect_status(crt_ctx* ctx, int count)
 {
+    if (ctx->capture) return CRT_OK;
     std::vector<int> h(count);
     if (!ck(ctx, cudaMemcpyAsync(h.data(), ctx->d_status, sizeof(int) * count, cudaMemcpyDeviceToHost, ctx->st),
             "status copy"))
@@ -173,6 +179,17 @@ int kernel_check(crt_ctx* ctx, const char* what)
     return CRT_OK;
 }
 
+// Phase timing by the context's events; a captured pass records and reads
+// nothing.
+bool ev_rec(crt_ctx* ctx, int i) { return ctx->capture || ck(ctx, cudaEventRecord(ctx->ev[i], ctx->st), "event record"); }
+bool ev_sync(crt_ctx* ctx, int i) { return ctx->capture || ck(ctx, cudaEventSynchronize(ctx->ev[i]), "event sync"); }
+float ev_ms(crt_ctx* ctx, int a, int b)
+{
+    float ms = 0.0f;
+    if (!ctx->capture) cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]);
+    return ms;
+}
+
 size_t sens_elem_bytes(const crt_ctx* ctx, bool real)
 {
     const bool f32 = ctx->prec == CRT_PREC_MIXED;
@@ -186,6 +203,7 @@ int plan_chunk(crt_ctx* ctx, int nsys, size_t tsize)
     const size_t slot = (size_t)ctx->n * ctx->W * tsize;
     size_t budget = (size_t)48 << 30;
     if (const char* env = std::getenv("CRT_B200_WORKSPACE_GB")) budget = (size_t)(std::atof(env) * (1u << 30));
+    if (ctx->ws_budget) budget = std::min(budget, ctx->ws_budget);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) budget = std::min(budget, free_b / 2);
     int c = (int)std::max<size_t>(1, budget / std::max<size_t>(slot + (size_t)ctx->n * (tsize + 8), 1));
@@ -563,7 +581,9 @@ int run_forward(crt_ctx* ctx)
     const bool mixed = ctx->lbeta != 0;
     const int nfac = mixed ? K * L : K;
     const size_t slot_bytes = (size_t)n * W * sizeof(T);
-    int chunk = plan_chunk(ctx, nfac, sizeof(T));
+    int chunk = ctx->capture ? ctx->chunk : plan_chunk(ctx, nfac, sizeof(T));
+    if (ctx->capture && (ctx->lws_slot_bytes != slot_bytes || !ctx->d_Lws))
+        return set_err(ctx, CRT_ERR_ARG, "captured forward without a prepared workspace");
     // factor workspace
     if (ctx->lws_slot_bytes != slot_bytes || ctx->chunk < chunk || !ctx->d_Lws) {
         if (ctx->d_Lws) cudaFree(ctx->d_Lws);
@@ -628,14 +648,16 @@ int run_forward(crt_ctx* ctx)
             }
             A.aval = ctx->d_aval;
         }
-        CK(cudaEventRecord(ctx->ev[0], ctx->st));
+        if (!ev_rec(ctx, 0)) return CRT_ERR_CUDA;
         {
             const char* fv = std::getenv("CRT_B200_FACTOR");
             const bool force_v0 = fv && std::strcmp(fv, "v0") == 0;
             if (!force_v0 && band_blk_fits<T>(ctx->mb)) {
+                const int pb = band_panel<T>(A, !ctx->capture, ctx->st);
+                ctx->panel = pb;
                 launch_band_prep<T>(A, ctx->st);
-                CK(cudaEventRecord(ctx->ev[8], ctx->st));
-                launch_band_factor_blk<T>(A, ctx->st);
+                if (!ev_rec(ctx, 8)) return CRT_ERR_CUDA;
+                launch_band_factor_blk<T>(A, pb, ctx->st);
                 ctx->launches += 3;
                 blk = true;
             } else {
@@ -644,14 +666,14 @@ int run_forward(crt_ctx* ctx)
                 } else {
                     launch_band_factor<T>(A, ctx->st);
                 }
-                CK(cudaEventRecord(ctx->ev[8], ctx->st));
+                if (!ev_rec(ctx, 8)) return CRT_ERR_CUDA;
                 ctx->launches++;
                 blk = false;
             }
             ++nfl;
         }
         if (int e = kernel_check(ctx, "band factor")) return e;
-        CK(cudaEventRecord(ctx->ev[1], ctx->st));
+        if (!ev_rec(ctx, 1)) return CRT_ERR_CUDA;
         SolveArgs<T> S{};
         S.n = n;
         S.mb = ctx->mb;
@@ -683,31 +705,31 @@ int run_forward(crt_ctx* ctx)
             // iterative refinement of the complex64 solution: FP64 residual of
             // the scaled system, complex64 correction solve, FP64 update of kpot
             for (int it = 0; it < ctx->nref; ++it) {
-                CK(cudaEventRecord(ctx->ev[4], ctx->st));
+                if (!ev_rec(ctx, 4)) return CRT_ERR_CUDA;
                 launch_band_residual<T>(A, S.sys0, S.nsys, S.factor_of_sys_div, ctx->d_up_ptr, ctx->d_up_ent,
                                         ctx->d_up_row, ctx->d_kpot, scr, ctx->st);
-                CK(cudaEventRecord(ctx->ev[5], ctx->st));
+                if (!ev_rec(ctx, 5)) return CRT_ERR_CUDA;
                 SolveArgs<T> C = S;
                 C.rhs = scr;
                 C.accumulate = 1;
                 launch_band_solve_with_scratch<T>(C, scr, ctx->st);
-                CK(cudaEventRecord(ctx->ev[9], ctx->st));
-                CK(cudaEventSynchronize(ctx->ev[9]));
+                if (!ev_rec(ctx, 9)) return CRT_ERR_CUDA;
+                if (!ev_sync(ctx, 9)) return CRT_ERR_CUDA;
                 float t1 = 0, t2 = 0;
-                cudaEventElapsedTime(&t1, ctx->ev[4], ctx->ev[5]);
-                cudaEventElapsedTime(&t2, ctx->ev[5], ctx->ev[9]);
+                t1 = ev_ms(ctx, 4, 5);
+                t2 = ev_ms(ctx, 5, 9);
                 ms_res += t1;
                 ms_cor += t2;
                 ctx->launches += 2;
             }
         }
         if (int e = kernel_check(ctx, "band solve")) return e;
-        CK(cudaEventRecord(ctx->ev[2], ctx->st));
-        CK(cudaEventSynchronize(ctx->ev[2]));
+        if (!ev_rec(ctx, 2)) return CRT_ERR_CUDA;
+        if (!ev_sync(ctx, 2)) return CRT_ERR_CUDA;
         float a = 0, b = 0, c = 0;
-        cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
-        cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
-        cudaEventElapsedTime(&c, ctx->ev[0], ctx->ev[8]);
+        a = ev_ms(ctx, 0, 1);
+        b = ev_ms(ctx, 1, 2);
+        c = ev_ms(ctx, 0, 8);
         ms_f += a;
         ms_s += b;
         if (blk) ms_prep += c;
@@ -720,6 +742,7 @@ int run_forward(crt_ctx* ctx)
     ctx->timings[9] = nfl;
     ctx->timings[10] = ms_res;
     ctx->timings[11] = ms_cor;
+    ctx->timings[12] = blk ? ctx->panel : 0;
     return collect_status(ctx, nfac);
 }
 
@@ -762,14 +785,14 @@ int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
     V.volt = ctx->d_volt;
     V.sigmaa = ctx->d_sigmaa;
     V.status = ctx->d_status + ctx->nstatus - 1;
-    CK(cudaEventRecord(ctx->ev[3], ctx->st));
+    if (!ev_rec(ctx, 3)) return CRT_ERR_CUDA;
     launch_voltages(V, ctx->st);
     ctx->launches += 2;
-    CK(cudaEventRecord(ctx->ev[4], ctx->st));
+    if (!ev_rec(ctx, 4)) return CRT_ERR_CUDA;
     if (int k = kernel_check(ctx, "voltages")) return k;
-    CK(cudaEventSynchronize(ctx->ev[4]));
+    if (!ev_sync(ctx, 4)) return CRT_ERR_CUDA;
     float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev[3], ctx->ev[4]);
+    ms = ev_ms(ctx, 3, 4);
     ctx->timings[2] = ms;
     if (d_kfak) cudaFree(d_kfak);
     int st = collect_status(ctx, ctx->nstatus);
@@ -843,7 +866,7 @@ int jacobian_device(crt_ctx* ctx, int mode, const double* strom_h)
     if (strom_h && mode == 2) {
         if (!upload(ctx, &ctx->d_strom, strom_h, (size_t)ctx->N)) return CRT_ERR_ALLOC;
     }
-    CK(cudaEventRecord(ctx->ev[5], ctx->st));
+    if (!ev_rec(ctx, 5)) return CRT_ERR_CUDA;
     launch_transpose_kpot(ctx->d_kpot, ctx->d_kpt, ctx->n, ctx->L, ctx->K, ctx->st);
     ctx->launches++;
     int kc = 0;
@@ -884,13 +907,29 @@ int jacobian_device(crt_ctx* ctx, int mode, const double* strom_h)
     else
         launch_sens(S, smem, real, ctx->st);
     ctx->launches++;
-    CK(cudaEventRecord(ctx->ev[6], ctx->st));
+    if (!ev_rec(ctx, 6)) return CRT_ERR_CUDA;
     if (int e = kernel_check(ctx, "sensitivities")) return e;
-    CK(cudaEventSynchronize(ctx->ev[6]));
+    if (!ev_sync(ctx, 6)) return CRT_ERR_CUDA;
     float ms = 0;
-    cudaEventElapsedTime(&ms, ctx->ev[5], ctx->ev[6]);
+    ms = ev_ms(ctx, 5, 6);
     ctx->timings[3] = ms;
     ctx->have_sens = 1;
+    return CRT_OK;
+}
+// Host copy of the device Jacobian in FP64 (complex values interleaved).
+int download_sens(crt_ctx* ctx, double* sens)
+{
+    const size_t ne = (size_t)ctx->E * ctx->N;
+    const size_t vals = ne * (ctx->sens_real ? 1 : 2);
+    if (ctx->prec == CRT_PREC_MIXED) {
+        std::vector<float> h(vals);
+        CK(cudaMemcpyAsync(h.data(), ctx->d_sens, vals * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (size_t q = 0; q < vals; ++q) sens[q] = (double)h[q];
+    } else {
+        CK(cudaMemcpyAsync(sens, ctx->d_sens, vals * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
     return CRT_OK;
 }
 }  // namespace
@@ -902,20 +941,7 @@ extern "C" int32_t crt_jacobian(crt_ctx* ctx, int32_t mode, const double* strom,
     CK(cudaSetDevice(ctx->device));
     int e = jacobian_device(ctx, mode, strom);
     if (e) return e;
-    if (sens) {
-        const size_t ne = (size_t)ctx->E * ctx->N;
-        const size_t vals = ne * (mode == 1 ? 1 : 2);
-        if (ctx->prec == CRT_PREC_MIXED) {
-            std::vector<float> h(vals);
-            CK(cudaMemcpyAsync(h.data(), ctx->d_sens, vals * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
-            CK(cudaStreamSynchronize(ctx->st));
-            for (size_t q = 0; q < vals; ++q) sens[q] = (double)h[q];
-        } else {
-            CK(cudaMemcpyAsync(sens, ctx->d_sens, vals * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-            CK(cudaStreamSynchronize(ctx->st));
-        }
-    }
-    return CRT_OK;
+    return sens ? download_sens(ctx, sens) : CRT_OK;
 }
 
 extern "C" int32_t crt_set_jacobian(crt_ctx* ctx, int32_t real, const double* sens)
@@ -1253,7 +1279,7 @@ int gn_step_device(crt_ctx* ctx, const crt_cg_params* prm, int* ncg)
     int e = forward_common(ctx, prm->ldc, 0, nullptr);
     if (e) return e;
     for (int i = 0; i < 3; ++i) tm[i] = ctx->timings[i];
-    for (int i = 7; i < 12; ++i) tm[i] = ctx->timings[i];
+    for (int i = 7; i < CRT_NTIMINGS; ++i) tm[i] = ctx->timings[i];
     e = jacobian_device(ctx, prm->ldc ? 1 : 0, nullptr);
     if (e) return e;
     tm[3] = ctx->timings[3];
@@ -1580,5 +1606,220 @@ extern "C" int32_t crt_gnn_record_grad(crt_ctx* ctx, int32_t idx, float* grad, d
     CK(cudaMemsetAsync(G.d_g, 0, GNN_NPARAM * sizeof(float), ctx->st));
     if (int e = kernel_check(ctx, "record gradient")) return e;
     if (loss) *loss = L;
+    return CRT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batches of independent instances under one CUDA graph.
+//
+// Every context keeps its own stream, device data and workspaces.  The first
+// crt_batch_run runs each context's forward (and Jacobian) once eagerly --
+// which allocates the workspaces and autotunes the band panel width for
+// every (precision, mb) of the batch -- and then captures all of them into
+// one graph: the batch stream records a fork event that every context
+// stream waits on, each context enqueues its forward and Jacobian with host
+// synchronisation, timing reads and allocation switched off, and the batch
+// stream joins all context streams again.  The instances are independent
+// branches of the graph, so uneven instances fill the SMs side by side; a
+// replay is one cudaGraphLaunch.  Per-system status words are read after
+// the replay.
+struct crt_batch {
+    int device = 0;
+    std::vector<crt_ctx*> ctx;
+    int ldc = 0, jac = -1;
+    cudaStream_t st = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<int> status;
+    std::string err;
+};
+
+namespace {
+int batch_enqueue(crt_batch* b, crt_ctx* c)
+{
+    int e = forward_common(c, b->ldc, 0, nullptr);
+    if (!e && b->jac >= 0) e = jacobian_device(c, b->jac, nullptr);
+    return e;
+}
+
+void batch_release(crt_batch* b)
+{
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+}  // namespace
+
+extern "C" crt_batch* crt_batch_create(crt_ctx* const* ctxs, int32_t count, int32_t ldc, int32_t jacobian_mode,
+                                       int32_t* err)
+{
+    auto fail = [&](int code) -> crt_batch* {
+        if (err) *err = code;
+        return nullptr;
+    };
+    if (!ctxs || count < 1 || jacobian_mode < -1 || jacobian_mode > 2) return fail(CRT_ERR_ARG);
+    for (int i = 0; i < count; ++i)
+        if (!ctxs[i] || ctxs[i]->device != ctxs[0]->device) return fail(CRT_ERR_ARG);
+    if (jacobian_mode == 1 && !ldc) return fail(CRT_ERR_ARG);   // bsendc belongs to the DC forward
+    auto* b = new crt_batch();
+    b->device = ctxs[0]->device;
+    b->ctx.assign(ctxs, ctxs + count);
+    b->ldc = ldc != 0;
+    b->jac = jacobian_mode;
+    b->status.assign(count, 0);
+    bool ok = cudaSetDevice(b->device) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreate(&b->t0) == cudaSuccess && cudaEventCreate(&b->t1) == cudaSuccess;
+    b->join.assign(count, nullptr);
+    for (int i = 0; ok && i < count; ++i)
+        ok = cudaEventCreateWithFlags(&b->join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        crt_batch_destroy(b);
+        return fail(CRT_ERR_CUDA);
+    }
+    if (err) *err = CRT_OK;
+    return b;
+}
+
+extern "C" void crt_batch_destroy(crt_batch* b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_release(b);
+    for (cudaEvent_t e : b->join)
+        if (e) cudaEventDestroy(e);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->t0) cudaEventDestroy(b->t0);
+    if (b->t1) cudaEventDestroy(b->t1);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+extern "C" const char* crt_batch_error(const crt_batch* b) { return b ? b->err.c_str() : "no batch"; }
+
+extern "C" int32_t crt_batch_set_models(crt_batch* b, const double* const* sigma)
+{
+    if (!b || !sigma) return CRT_ERR_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return CRT_ERR_CUDA;
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        crt_ctx* ctx = b->ctx[i];
+        if (!sigma[i]) return CRT_ERR_ARG;
+        if (!ctx->d_sigma && !dalloc(ctx, &ctx->d_sigma, (size_t)ctx->E)) return CRT_ERR_ALLOC;
+        CK(cudaMemcpyAsync(ctx->d_sigma, sigma[i], sizeof(cd) * ctx->E, cudaMemcpyHostToDevice, ctx->st));
+    }
+    for (crt_ctx* ctx : b->ctx) CK(cudaStreamSynchronize(ctx->st));
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_batch_run(crt_batch* b, double* ms)
+{
+    if (!b) return CRT_ERR_ARG;
+    if (cudaSetDevice(b->device) != cudaSuccess) return CRT_ERR_CUDA;
+    for (crt_ctx* c : b->ctx)
+        if (!c->d_sigma) {
+            b->err = "crt_batch_run before crt_batch_set_models";
+            return CRT_ERR_ARG;
+        }
+    auto cuda_fail = [&](cudaError_t e, const char* what) {
+        b->err = std::string(what) + ": " + cudaGetErrorString(e);
+        return CRT_ERR_CUDA;
+    };
+    if (!b->exec) {
+        // eager pass: allocations, panel autotuning, status of every instance
+        for (size_t i = 0; i < b->ctx.size(); ++i) {
+            if (int e = batch_enqueue(b, b->ctx[i])) {
+                b->err = "instance " + std::to_string(i) + ": " + b->ctx[i]->err;
+                return e;
+            }
+        }
+        cudaError_t ce = cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal);
+        if (ce != cudaSuccess) return cuda_fail(ce, "begin capture");
+        int failed = 0;
+        ce = cudaEventRecord(b->fork, b->st);
+        for (size_t i = 0; ce == cudaSuccess && !failed && i < b->ctx.size(); ++i) {
+            crt_ctx* c = b->ctx[i];
+            ce = cudaStreamWaitEvent(c->st, b->fork, 0);
+            if (ce != cudaSuccess) break;
+            c->capture = 1;
+            const int e = batch_enqueue(b, c);
+            c->capture = 0;
+            if (e) {
+                b->err = "capturing instance " + std::to_string(i) + ": " + c->err;
+                failed = e;
+                break;
+            }
+            ce = cudaEventRecord(b->join[i], c->st);
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->st, b->join[i], 0);
+        }
+        cudaGraph_t g = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(b->st, &g);
+        if (failed || ce != cudaSuccess || ee != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            if (failed) return failed;
+            return cuda_fail(ce != cudaSuccess ? ce : ee, "graph capture");
+        }
+        b->graph = g;
+        ce = cudaGraphInstantiate(&b->exec, b->graph, 0);
+        if (ce != cudaSuccess) {
+            batch_release(b);
+            return cuda_fail(ce, "graph instantiate");
+        }
+    }
+    cudaError_t ce = cudaEventRecord(b->t0, b->st);
+    if (ce == cudaSuccess) ce = cudaGraphLaunch(b->exec, b->st);
+    if (ce == cudaSuccess) ce = cudaEventRecord(b->t1, b->st);
+    if (ce == cudaSuccess) ce = cudaEventSynchronize(b->t1);
+    if (ce != cudaSuccess) return cuda_fail(ce, "graph launch");
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, b->t0, b->t1);
+    if (ms) *ms = t;
+    int first = CRT_OK;
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        crt_ctx* c = b->ctx[i];
+        b->status[i] = collect_status(c, c->nstatus);
+        if (b->status[i] == CRT_OK) {
+            c->last_ldc = b->ldc;
+            c->have_forward = 1;
+            c->have_sens = b->jac >= 0;
+        } else if (first == CRT_OK) {
+            first = b->status[i];
+            b->err = "instance " + std::to_string(i) + ": " + c->err;
+        }
+    }
+    return first;
+}
+
+extern "C" int32_t crt_batch_status(const crt_batch* b, int32_t i)
+{
+    if (!b || i < 0 || i >= (int)b->ctx.size()) return CRT_ERR_ARG;
+    return b->status[i];
+}
+
+extern "C" int32_t crt_batch_results(crt_batch* b, int32_t i, double* volt, double* sigmaa, double* sens)
+{
+    if (!b || i < 0 || i >= (int)b->ctx.size()) return CRT_ERR_ARG;
+    crt_ctx* ctx = b->ctx[i];
+    if (!ctx->have_forward) return set_err(ctx, CRT_ERR_ARG, "no batch result for this instance");
+    CK(cudaSetDevice(ctx->device));
+    if (volt) CK(cudaMemcpyAsync(volt, ctx->d_volt, sizeof(cd) * ctx->N, cudaMemcpyDeviceToHost, ctx->st));
+    if (sigmaa) CK(cudaMemcpyAsync(sigmaa, ctx->d_sigmaa, sizeof(cd) * ctx->N, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (sens) {
+        if (!ctx->have_sens) return set_err(ctx, CRT_ERR_ARG, "the batch computes no Jacobian");
+        return download_sens(ctx, sens);
+    }
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_set_workspace_limit(crt_ctx* ctx, int64_t bytes)
+{
+    if (!ctx || bytes < 0) return CRT_ERR_ARG;
+    ctx->ws_budget = (size_t)bytes;
     return CRT_OK;
 }

@@ -248,16 +248,6 @@ template <> __device__ __forceinline__ cf shfl_down_t<cf>(cf v, int off)
     return cf{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)};
 }
 
-// 16-byte asynchronous global -> shared copies (the prefetch of the solve's
-// next block of columns).
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
-{
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
 // Resident CTAs per SM of the solve: complex64 state is small enough for
 // three (latency hiding across systems), complex128 for two.
 template <typename T> struct SolveOcc { static constexpr int v = 2; };

@@ -9,7 +9,9 @@
 // is written only after row r has entered the window, so the factor
 // overwrites the prepared matrix in place.
 //
-// One CTA per band system.  The window holds Wn = roundup(mb + PB, PB) rows
+// One CTA per band system.  The panel width PB (4, 8 or 16) is chosen per
+// element type and half-bandwidth by a measuring autotuner (band_panel).
+// The window holds Wn = roundup(mb + PB, PB) rows
 // in shared memory; row r lives in slot r mod Wn and the symmetric entry of
 // two rows is stored once, at the unordered slot pair, in 4 x 4 tiles
 // (tile (X, Y), X >= Y, row-major inside the tile).  Per panel of PB
@@ -30,6 +32,11 @@
 // The first diagonal block is factored before the loop, so the serial
 // block factorisation overlaps the trailing update of the previous panel.
 #include "crt_band.h"
+
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <utility>
 
 namespace {
 
@@ -485,11 +492,27 @@ static size_t blk_smem(int mb, int* Wn_out)
 }
 
 template <typename T>
-bool band_blk_fits(int mb)
+static size_t blk_smem_pb(int pb, int mb, int* Wn)
+{
+    switch (pb) {
+    case 4: return blk_smem<T, 4>(mb, Wn);
+    case 16: return blk_smem<T, 16>(mb, Wn);
+    default: return blk_smem<T, 8>(mb, Wn);
+    }
+}
+
+template <typename T>
+static bool blk_fits_pb(int pb, int mb)
 {
     int Wn = 0;
-    const size_t smem = blk_smem<T, 8>(mb, &Wn);
+    const size_t smem = blk_smem_pb<T>(pb, mb, &Wn);
     return smem <= 227 * 1024 && Wn / 4 <= 255;
+}
+
+template <typename T>
+bool band_blk_fits(int mb)
+{
+    return blk_fits_pb<T>(8, mb);
 }
 
 template <typename T>
@@ -500,23 +523,93 @@ void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
     k_band_prep_rows<T><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, st>>>(a);
 }
 
-template <typename T>
-bool launch_band_factor_blk(const BandArgs<T>& a, cudaStream_t st)
+template <typename T, int PB>
+static void launch_blk_pb(const BandArgs<T>& a, cudaStream_t st)
 {
-    constexpr int PB = 8;
     int Wn = 0;
     const size_t smem = blk_smem<T, PB>(a.mb, &Wn);
-    if (!band_blk_fits<T>(a.mb)) return false;
     // a window that fits twice (complex64, or real FP64) runs as two
     // 256-thread CTAs per SM, overlapping one system's serial phases with the
-    // other's update; a complex128 window leaves room for one CTA of 512
+    // other's update; a larger window leaves room for one CTA of 512
     auto go = [&](auto kern, int nt) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<a.nsys, nt, smem, st>>>(a, Wn);
     };
     if (2 * smem <= 227 * 1024) go(k_band_factor_blk<T, PB, 256, 2>, 256);
     else go(k_band_factor_blk<T, PB, 512, 1>, 512);
+}
+
+template <typename T>
+bool launch_band_factor_blk(const BandArgs<T>& a, int pb, cudaStream_t st)
+{
+    if (!blk_fits_pb<T>(pb, a.mb)) return false;
+    switch (pb) {
+    case 4: launch_blk_pb<T, 4>(a, st); break;
+    case 16: launch_blk_pb<T, 16>(a, st); break;
+    default: launch_blk_pb<T, 8>(a, st); break;
+    }
     return true;
+}
+
+// ---------------------------------------------------------------------------
+// Panel-width autotuner.  The best panel (4, 8 or 16 columns) depends on the
+// element type and the half-bandwidth (window size, CTAs per SM, serial
+// panel phases against the rank-PB update); it is measured once per
+// (type, mb) in the process on the first systems of a real chunk: for each
+// candidate that fits, the preparation pass and the factorisation of up to
+// two waves of systems are run and the factorisation is timed with events.
+// The caller's real pass then prepares and factors the chunk again, so the
+// trials leave no trace but their per-system status, which is cleared.
+// CRT_B200_PANEL = 4 | 8 | 16 fixes the width.
+namespace {
+std::mutex g_panel_mu;
+std::map<std::pair<int, int>, int> g_panel;   // (sizeof(T), mb) -> panel width
+}
+
+template <typename T>
+int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st)
+{
+    if (const char* env = std::getenv("CRT_B200_PANEL")) {
+        const int pb = std::atoi(env);
+        if ((pb == 4 || pb == 8 || pb == 16) && blk_fits_pb<T>(pb, a.mb)) return pb;
+    }
+    const std::pair<int, int> key((int)sizeof(T), a.mb);
+    {
+        std::lock_guard<std::mutex> g(g_panel_mu);
+        auto it = g_panel.find(key);
+        if (it != g_panel.end()) return it->second;
+    }
+    if (!may_tune) return 8;
+    int nsm = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    BandArgs<T> t = a;
+    t.nsys = std::min(a.nsys, 2 * nsm);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    int best = 8;
+    float best_ms = 1e30f;
+    for (int pb : {8, 4, 16}) {
+        if (!blk_fits_pb<T>(pb, a.mb)) continue;
+        launch_band_prep<T>(t, st);
+        cudaEventRecord(e0, st);
+        launch_band_factor_blk<T>(t, pb, st);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess) break;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = pb;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaMemsetAsync(a.status + a.sys0, 0, sizeof(int) * (size_t)t.nsys, st);
+    std::lock_guard<std::mutex> g(g_panel_mu);
+    g_panel[key] = best;
+    return best;
 }
 
 template <typename T>
@@ -534,8 +627,11 @@ template bool band_blk_fits<cf>(int);
 template void launch_band_prep<double>(const BandArgs<double>&, cudaStream_t);
 template void launch_band_prep<cd>(const BandArgs<cd>&, cudaStream_t);
 template void launch_band_prep<cf>(const BandArgs<cf>&, cudaStream_t);
-template bool launch_band_factor_blk<double>(const BandArgs<double>&, cudaStream_t);
-template bool launch_band_factor_blk<cd>(const BandArgs<cd>&, cudaStream_t);
-template bool launch_band_factor_blk<cf>(const BandArgs<cf>&, cudaStream_t);
+template bool launch_band_factor_blk<double>(const BandArgs<double>&, int, cudaStream_t);
+template bool launch_band_factor_blk<cd>(const BandArgs<cd>&, int, cudaStream_t);
+template bool launch_band_factor_blk<cf>(const BandArgs<cf>&, int, cudaStream_t);
+template int band_panel<double>(const BandArgs<double>&, bool, cudaStream_t);
+template int band_panel<cd>(const BandArgs<cd>&, bool, cudaStream_t);
+template int band_panel<cf>(const BandArgs<cf>&, bool, cudaStream_t);
 template void launch_band_residual<cf>(const BandArgs<cf>&, int, int, int, const int*, const int*, const int*,
                                        const cd*, cf*, cudaStream_t);

@@ -12,7 +12,7 @@
 #define CRT_HD __host__ __device__ __forceinline__
 
 // entries of crt_last_timings_ex
-#define CRT_NTIMINGS 12
+#define CRT_NTIMINGS 13
 
 struct __align__(16) cd {
     double x, y;
@@ -198,6 +198,19 @@ template <typename T> CRT_HD T narrow(typename Wide<T>::type v);
 template <> CRT_HD double narrow<double>(double v) { return v; }
 template <> CRT_HD cd narrow<cd>(cd v) { return v; }
 template <> CRT_HD cf narrow<cf>(cd v) { return cf{(float)v.x, (float)v.y}; }
+
+// 16-byte asynchronous global -> shared copies (cp.async, bypassing L1);
+// both addresses 16-byte aligned.  wait_group<N> returns once at most N of
+// the thread's committed groups are still in flight.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { cp_async_wait_group<0>(); }
 
 // Reference error numbers (src/error.txt) returned through the C ABI.
 enum crt_errnr : int32_t {

@@ -11,20 +11,21 @@
 //
 // Device, once per update:
 //   k_spc_diag / k_spc_entries : S = I + lam C (R - diag R) C in blocks
-//   k_spc_factor  (one CTA)    : T_q = D_q - F_q H_{q-1}, H_{q-1} = T_{q-1}^-1 F_q^T,
-//                                T_q^-1 by Gauss-Jordan with the block held in
-//                                registers (SPD: no pivoting)
+//   k_spc_factor_v / k_spc_factor (one CTA) : T_q = D_q - F_q H_{q-1},
+//                                H_{q-1} = T_{q-1}^-1 F_q^T, T_q^-1 by Gauss-Jordan
+//                                with the block held in registers (SPD: no pivoting)
 //   k_spc_gmul    (nb CTAs)    : G_q = T_q^-1 F_q
 // and per CG iteration:
 //   k_spc_u       (nb CTAs)    : u_q = T_q^-1 r_q on the permuted residual
 //   k_spc_sweep   (one CTA)    : h_q = u_q - G_q h_{q-1}, x_q = h_q - H_q x_{q+1},
 //                                z = x in element order (G and H column-major)
-// Every thread owns the NB x NB entries (ty + 32a, tx + 32b) of a block,
-// which keeps shared-memory reads broadcast (A operand) or consecutive
-// (B operand) and global accesses coalesced.
+// The sub-diagonal blocks are stored transposed, FT_q[j][i] = F_q[i][j], so
+// that both products of a block step read rows of their operands.
 #include "crt_spc.h"
 
 #include <algorithm>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "crt_cg.h"
@@ -148,6 +149,18 @@ __device__ __forceinline__ float warp_allsum_f(float v)
     return v;
 }
 
+// f(integral_constant<int, i>) for i = 0 .. N-1, unrolled at compile time
+template <typename F, int... I>
+__device__ __forceinline__ void static_for_seq(F&& f, std::integer_sequence<int, I...>)
+{
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+__device__ __forceinline__ void static_for(F&& f)
+{
+    static_for_seq(f, std::make_integer_sequence<int, N>{});
+}
+
 __global__ void k_spc_diag(float* DF, int nb, int B)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -165,7 +178,172 @@ __global__ void k_spc_entries(const int4* __restrict__ ent, int nent, const doub
     DF[e.x] = (float)(lam * cgfac[e.y] * smatm[e.w] * cgfac[e.z]);
 }
 
-// One CTA: the sequential block recurrence.
+// One CTA: the sequential block recurrence for B <= 128, with (B/8)^2
+// threads; thread (ty, tx) owns an 8 x 8 set of a block's entries in
+// registers: rows 8 ty .. 8 ty + 7 and the two column quads 4 tx .. 4 tx + 3
+// and B/2 + 4 tx .. B/2 + 4 tx + 3 (so that the 16-byte loads of a quarter
+// warp cover consecutive banks).  With X = T_{q-1}^-1 (symmetric) and FT_q
+// in shared memory, both products take k-rows of their operands,
+//   H[r][c] = sum_k X[k][r] FT[k][c],    T[r][c] = D[r][c] - sum_k FT[k][r] H[k][c],
+// so each k step of a thread is four 16-byte shared loads and 64 FMAs; the
+// Gauss-Jordan inversion publishes row and column k through double-buffered
+// vectors (one barrier per step).  FT_{q+1} is copied into the other half of
+// a shared double buffer by cp.async while block q is formed and inverted.
+template <int NB>
+__global__ void __launch_bounds__(16 * NB * NB, 1) k_spc_factor_v(float* DF, float* H, int nb, int* flag)
+{
+    constexpr int B = 32 * NB, TPR = B / 8, NT = TPR * TPR, HB = B / 2;
+    extern __shared__ __align__(16) float smem[];
+    float* X = smem;                  // [B][B]     T_{q-1}^-1, then H_{q-1}
+    float* FTs = X + B * B;           // [2][B][B]  FT_q in half q & 1
+    float* rowb = FTs + 2 * B * B;    // [2][B]
+    float* colb = rowb + 2 * B;       // [2][B]
+    const int tid = threadIdx.x, tx = tid % TPR, ty = tid / TPR;
+    const int r0 = 8 * ty, c0 = 4 * tx;
+    const size_t BB = (size_t)B * B;
+    const float* F = DF + (size_t)nb * BB;
+    auto cidx = [&](int b) { return (b >> 2) * HB + c0 + (b & 3); };
+    auto stage_ft = [&](int q) {
+        const float4* src = reinterpret_cast<const float4*>(F + (size_t)q * BB);
+        float* dst = FTs + (size_t)(q & 1) * BB;
+        for (int i = tid; i < (int)(BB / 4); i += NT) cp_async16(dst + 4 * i, src + i);
+        cp_async_commit();
+    };
+    auto unpack = [](float4 a, float4 b, float (&v)[8]) {
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+        v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+    };
+    // 8 consecutive floats (rows) / this thread's two column quads of a row
+    auto ld_rows = [&](const float* p, float (&v)[8]) {
+        unpack(*reinterpret_cast<const float4*>(p), *reinterpret_cast<const float4*>(p + 4), v);
+    };
+    auto ld_cols = [&](const float* row, float (&v)[8]) {
+        unpack(*reinterpret_cast<const float4*>(row + c0), *reinterpret_cast<const float4*>(row + HB + c0), v);
+    };
+    auto st_rows = [](float* p, const float (&v)[8]) {
+        *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<float4*>(p + 4) = make_float4(v[4], v[5], v[6], v[7]);
+    };
+    auto st_cols = [&](float* row, const float (&v)[8]) {
+        *reinterpret_cast<float4*>(row + c0) = make_float4(v[0], v[1], v[2], v[3]);
+        *reinterpret_cast<float4*>(row + HB + c0) = make_float4(v[4], v[5], v[6], v[7]);
+    };
+    int first_bad = 0;
+    if (nb > 1) stage_ft(1);
+    for (int q = 0; q < nb; ++q) {
+        float* Dq = DF + (size_t)q * BB;
+        float t[8][8];
+#pragma unroll
+        for (int a = 0; a < 8; ++a) ld_cols(Dq + (size_t)(r0 + a) * B, t[a]);
+        if (q > 0) {
+            if (q + 1 < nb) {
+                stage_ft(q + 1);            // the half of FT_{q-1}, long since read
+                cp_async_wait_group<1>();   // FT_q has landed
+            } else {
+                cp_async_wait_all();
+            }
+            __syncthreads();
+            const float* FT = FTs + (size_t)(q & 1) * BB;
+            float h[8][8];
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) h[a][b] = 0.0f;
+#pragma unroll 2
+            for (int k = 0; k < B; ++k) {
+                float xa[8], fb[8];
+                ld_rows(X + k * B + r0, xa);
+                ld_cols(FT + k * B, fb);
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) h[a][b] = fmaf(xa[a], fb[b], h[a][b]);
+            }
+            __syncthreads();
+#pragma unroll
+            for (int a = 0; a < 8; ++a) st_cols(X + (r0 + a) * B, h[a]);
+            // the sweep reads H_{q-1} column-major: HT[c][r] = H[r][c]
+            float* Hq = H + (size_t)(q - 1) * BB;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                float col[8];
+#pragma unroll
+                for (int a = 0; a < 8; ++a) col[a] = h[a][b];
+                st_rows(Hq + (size_t)cidx(b) * B + r0, col);
+            }
+            __syncthreads();
+#pragma unroll 2
+            for (int k = 0; k < B; ++k) {
+                float fa[8], hb[8];
+                ld_rows(FT + k * B + r0, fa);
+                ld_cols(X + k * B, hb);
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) t[a][b] = fmaf(-fa[a], hb[b], t[a][b]);
+            }
+        }
+        // Gauss-Jordan inversion in place (SPD, no pivoting).  Row k = 8 kq +
+        // kr is held by the threads with ty = kq (entry kr); column k by those
+        // with tx = (k mod B/2) / 4 (entry 4 (k >= B/2) + k % 4).  The eight
+        // steps of a row group are unrolled, so a thread's entries of row and
+        // column k are static register indices.
+        auto gj_step = [&](const int k, auto kr_c, auto half_c) {
+            constexpr int kr = decltype(kr_c)::value, kb = 4 * decltype(half_c)::value + (kr & 3);
+            const int buf = (k & 1) * B;
+            const bool row_own = ty == (k >> 3), col_own = tx == ((k % HB) >> 2);
+            if (row_own) st_cols(rowb + buf, t[kr]);
+            if (col_own) {
+                float col[8];
+#pragma unroll
+                for (int a = 0; a < 8; ++a) col[a] = t[a][kb];
+                st_rows(colb + buf + r0, col);
+            }
+            __syncthreads();
+            float piv = rowb[buf + k];
+            if (!(piv > 0.0f)) {
+                if (first_bad == 0) first_bad = q + 1;
+                piv = 1.0f;
+            }
+            const float pinv = __frcp_rn(piv);
+            float cv[8], rv[8];
+            ld_rows(colb + buf + r0, cv);
+            ld_cols(rowb + buf, rv);
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                const float ci = cv[a] * pinv;
+#pragma unroll
+                for (int b = 0; b < 8; ++b) t[a][b] = fmaf(-ci, rv[b], t[a][b]);
+            }
+            if (row_own) {
+#pragma unroll
+                for (int b = 0; b < 8; ++b) t[kr][b] = (cidx(b) == k) ? pinv : rv[b] * pinv;
+            }
+            if (col_own) {
+#pragma unroll
+                for (int a = 0; a < 8; ++a)
+                    if (r0 + a != k) t[a][kb] = -cv[a] * pinv;
+            }
+        };
+        for (int kq = 0; kq < TPR; ++kq) {
+            if (kq < TPR / 2)
+                static_for<8>([&](auto kr) { gj_step(8 * kq + decltype(kr)::value, kr, std::integral_constant<int, 0>{}); });
+            else
+                static_for<8>([&](auto kr) { gj_step(8 * kq + decltype(kr)::value, kr, std::integral_constant<int, 1>{}); });
+        }
+        __syncthreads();
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            st_cols(Dq + (size_t)(r0 + a) * B, t[a]);
+            st_cols(X + (r0 + a) * B, t[a]);
+        }
+    }
+    if (tid == 0) *flag = first_bad;
+}
+
+// One CTA: the sequential block recurrence, for B > 128 (every thread owns
+// the NB x NB entries (ty + 32a, tx + 32b) of a block, operands staged in
+// chunks of 32 k).
 template <int NB>
 __global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, int nb, int* flag)
 {
@@ -183,8 +361,8 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, i
         float* Dq = DF + (size_t)q * BB;
         float t[NB][NB];
         if (q > 0) {
-            const float* Fq = F + (size_t)q * BB;
-            // H = T_{q-1}^-1 F_q^T:  H[r][c] = sum_k X[r][k] Fq[c][k]
+            const float* FTq = F + (size_t)q * BB;
+            // H = T_{q-1}^-1 F_q^T:  H[r][c] = sum_k X[r][k] F_q[c][k]
             float h[NB][NB];
 #pragma unroll
             for (int a = 0; a < NB; ++a)
@@ -193,8 +371,8 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, i
             for (int k0 = 0; k0 < B; k0 += 32) {
                 __syncthreads();
                 for (int u = tid; u < 32 * B; u += SPC_NT) {
-                    const int kk = u & 31, c = u >> 5;
-                    Sg[kk * LD + c] = Fq[(size_t)c * B + k0 + kk];
+                    const int c = u % B, kk = u / B;
+                    Sg[kk * LD + c] = FTq[(size_t)(k0 + kk) * B + c];
                 }
                 __syncthreads();
 #pragma unroll 4
@@ -230,8 +408,8 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_factor(float* DF, float* H, i
             for (int k0 = 0; k0 < B; k0 += 32) {
                 __syncthreads();
                 for (int u = tid; u < 32 * B; u += SPC_NT) {
-                    const int kk = u & 31, r = u >> 5;
-                    Sg[kk * LD + r] = Fq[(size_t)r * B + k0 + kk];
+                    const int r = u % B, kk = u / B;
+                    Sg[kk * LD + r] = FTq[(size_t)(k0 + kk) * B + r];
                 }
                 __syncthreads();
 #pragma unroll 4
@@ -338,7 +516,7 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_gmul(const float* DF, float* 
     const int tid = threadIdx.x, tx = tid & 31, ty = tid >> 5;
     const size_t BB = (size_t)B * B;
     const float* Ti = DF + (size_t)q * BB;
-    const float* Fq = DF + (size_t)nb * BB + (size_t)q * BB;
+    const float* FTq = DF + (size_t)nb * BB + (size_t)q * BB;
     float g[NB][NB];
 #pragma unroll
     for (int a = 0; a < NB; ++a)
@@ -348,8 +526,9 @@ __global__ void __launch_bounds__(SPC_NT, 1) k_spc_gmul(const float* DF, float* 
         __syncthreads();
         for (int u = tid; u < 32 * B; u += SPC_NT) {
             const int c = u % B, kk = u / B;
-            As[kk * LD + c] = Fq[(size_t)(k0 + kk) * B + c];
             Bs[kk * LD + c] = Ti[(size_t)(k0 + kk) * B + c];
+            const int kt = u & 31, ct = u >> 5;     // F[k][c] = FT[c][k], read along k
+            As[kt * LD + ct] = FTq[(size_t)ct * B + k0 + kt];
         }
         __syncthreads();
 #pragma unroll 4
@@ -532,6 +711,7 @@ __global__ void __launch_bounds__(SW_NT, 1) k_spc_sweep(const float* __restrict_
 }
 
 size_t factor_smem(int B) { return sizeof(float) * ((size_t)B * (B + 1) + 32 * (B + 1) + 4 * B); }
+size_t factor_v_smem(int B) { return sizeof(float) * (3 * (size_t)B * B + 4 * B); }
 size_t gmul_smem(int B) { return sizeof(float) * (2 * 32 * (size_t)(B + 1)); }
 
 template <int NB>
@@ -539,9 +719,15 @@ void factor_nb(const SpcPlan& P, cudaStream_t s)
 {
     const int B = 32 * NB;
     const size_t fs = factor_smem(B), gs = gmul_smem(B);
-    cudaFuncSetAttribute(k_spc_factor<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs);
+    if constexpr (NB <= 4) {
+        const size_t vs = factor_v_smem(B);
+        cudaFuncSetAttribute(k_spc_factor_v<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vs);
+        k_spc_factor_v<NB><<<1, 16 * NB * NB, vs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag);
+    } else {
+        cudaFuncSetAttribute(k_spc_factor<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs);
+        k_spc_factor<NB><<<1, SPC_NT, fs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag);
+    }
     cudaFuncSetAttribute(k_spc_gmul<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gs);
-    k_spc_factor<NB><<<1, SPC_NT, fs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag);
     if (P.nb > 1) k_spc_gmul<NB><<<P.nb - 1, SPC_NT, gs, s>>>(P.d_DF, P.d_G, P.nb);
 }
 
@@ -656,7 +842,7 @@ int spc_plan_build(SpcPlan& P, int M, int ltri, int nx, int nnb, const double* s
         const int qi = pi / B, qj = pj / B, ri = pi % B, rj = pj % B;
         size_t dst;
         if (qi == qj) dst = (size_t)qi * BB + (size_t)ri * B + rj;
-        else if (qi == qj + 1) dst = (size_t)P.nb * BB + (size_t)qi * BB + (size_t)ri * B + rj;
+        else if (qi == qj + 1) dst = (size_t)P.nb * BB + (size_t)qi * BB + (size_t)rj * B + ri;   // FT_q
         else continue;   // upper block: the transpose of an F entry
         ent.push_back(int4{(int)dst, ei[k], ej[k], es[k]});
     }

@@ -37,7 +37,7 @@ struct SpcPlan {
     int nent = 0;
     int* d_perm = nullptr;     // [Mp] permuted position -> element (-1: padding)
     int4* d_ent = nullptr;     // [nent] {dst in DF, i, j, smatm index}
-    float* d_DF = nullptr;     // [2][nb][B][B]: D_q (T_q^-1 after the factor), F_q
+    float* d_DF = nullptr;     // [2][nb][B][B]: D_q (T_q^-1 after the factor), F_q^T
     float* d_G = nullptr;      // [nb][B][B]  T_q^-1 F_q       (q >= 1)
     float* d_H = nullptr;      // [nb][B][B]  T_q^-1 F_{q+1}^T (q < nb-1)
     cf* d_h = nullptr;         // [Mp] sweep vector

@@ -68,7 +68,9 @@ EXPORTS = [
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
     "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order", "crt_last_timings_ex",
     "crt_set_refinement", "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
-    "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad",
+    "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad", "crt_batch_create",
+    "crt_batch_destroy", "crt_batch_error", "crt_batch_set_models", "crt_batch_run", "crt_batch_status",
+    "crt_batch_results", "crt_set_workspace_limit",
 ]
 
 _LIB = None
@@ -126,6 +128,22 @@ def load(path: str = LIB_PATH):
     L.crt_last_timings.restype = C.c_int32
     L.crt_set_refinement.argtypes = [vp, C.c_int32]
     L.crt_set_refinement.restype = C.c_int32
+    L.crt_batch_create.argtypes = [P(vp), C.c_int32, C.c_int32, C.c_int32, i32p]
+    L.crt_batch_create.restype = vp
+    L.crt_batch_destroy.argtypes = [vp]
+    L.crt_batch_destroy.restype = None
+    L.crt_batch_error.argtypes = [vp]
+    L.crt_batch_error.restype = C.c_char_p
+    L.crt_batch_set_models.argtypes = [vp, P(vp)]
+    L.crt_batch_set_models.restype = C.c_int32
+    L.crt_batch_run.argtypes = [vp, P(C.c_double)]
+    L.crt_batch_run.restype = C.c_int32
+    L.crt_batch_status.argtypes = [vp, C.c_int32]
+    L.crt_batch_status.restype = C.c_int32
+    L.crt_batch_results.argtypes = [vp, C.c_int32, vp, vp, vp]
+    L.crt_batch_results.restype = C.c_int32
+    L.crt_set_workspace_limit.argtypes = [vp, C.c_int64]
+    L.crt_set_workspace_limit.restype = C.c_int32
     L.crt_last_timings_ex.argtypes = [vp, f64p, C.c_int32]
     L.crt_last_timings_ex.restype = C.c_int32
     L.crt_cg_info.argtypes = [vp, i32p, i32p, i32p]
@@ -406,7 +424,7 @@ class Context:
         return ncg.value
 
     TIMING_NAMES = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total", "factor_prep",
-                    "factor_kernel", "factor_launches", "refine_residual", "refine_solve"]
+                    "factor_kernel", "factor_launches", "refine_residual", "refine_solve", "panel"]
 
     def timings(self):
         t = np.zeros(len(self.TIMING_NAMES))
@@ -418,6 +436,10 @@ class Context:
 
     def set_refinement(self, steps):
         self._check(self.L.crt_set_refinement(self.h, int(steps)), "crt_set_refinement")
+
+    def set_workspace_limit(self, nbytes):
+        """Upper bound of the band-factor workspace (0: default)."""
+        self._check(self.L.crt_set_workspace_limit(self.h, int(nbytes)), "crt_set_workspace_limit")
 
     # -- learned correction of the preconditioner -------------------------
     def gnn_nparam(self):
@@ -495,3 +517,63 @@ def dmisft(dat, sigmaa, wmatd, wmatdr=None, wmatdp=None, lfpi=False, lpol=False)
     r = L.crt_dmisft(len(d), _vp(d), _vp(s), _vp(w), _vp(wr), _vp(wp), int(lfpi), int(lpol), C.byref(br),
                      C.byref(ph), C.byref(npol))
     return r, br.value, ph.value, npol.value
+
+
+class Batch:
+    """Forward (and Jacobian) of many independent contexts as one CUDA graph
+    (crt_batch_*): the contexts are the graph's independent branches; the
+    first run executes every instance eagerly (workspaces, panel autotuning)
+    and captures the graph, later runs replay it."""
+
+    def __init__(self, contexts, ldc=False, jacobian_mode=0):
+        self.L = load()
+        self.contexts = list(contexts)
+        arr = (C.c_void_p * len(self.contexts))(*[c.h.value for c in self.contexts])
+        self._arr = arr
+        err = C.c_int32()
+        h = self.L.crt_batch_create(arr, len(self.contexts), int(bool(ldc)), int(jacobian_mode), C.byref(err))
+        if not h:
+            raise CRTError(err.value, "crt_batch_create failed")
+        self.h = C.c_void_p(h)
+        self.jacobian_mode = int(jacobian_mode)
+        self._sig = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.crt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, e, what):
+        if e:
+            raise CRTError(e, f"{what}: {self.L.crt_batch_error(self.h).decode(errors='replace')}")
+
+    def set_models(self, sigmas):
+        self._sig = [np.ascontiguousarray(s_, np.complex128) for s_ in sigmas]
+        ptrs = (C.c_void_p * len(self._sig))(*[a.ctypes.data for a in self._sig])
+        self._check(self.L.crt_batch_set_models(self.h, ptrs), "crt_batch_set_models")
+
+    def run(self):
+        """Runs (replays) the batch; returns the device time in ms."""
+        ms = C.c_double()
+        self._check(self.L.crt_batch_run(self.h, C.byref(ms)), "crt_batch_run")
+        return ms.value
+
+    def status(self, i):
+        return int(self.L.crt_batch_status(self.h, int(i)))
+
+    def results(self, i, sens=False):
+        c = self.contexts[i]
+        volt = np.zeros(c.nanz, np.complex128)
+        sa = np.zeros(c.nanz, np.complex128)
+        J = None
+        if sens:
+            dt = np.float64 if self.jacobian_mode == 1 else np.complex128
+            J = np.zeros((c.nanz, c.elanz), dt, order="F")
+        self._check(self.L.crt_batch_results(self.h, int(i), _vp(volt), _vp(sa), _vp(J)), "crt_batch_results")
+        return (volt, sa, J) if sens else (volt, sa)

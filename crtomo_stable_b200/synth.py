@@ -270,6 +270,41 @@ def config5(seed: int = SEED0 + 5, nx: int = 235, nz: int = 128) -> Survey:
     return Survey(mesh, enr, strnr, vnr, sigma_from(rho, pha), "C5", nx, nz)
 
 
+def config4(seed: int = SEED0 + 4, count: int = 256, emin: int = 2000, emax: int = 30000) -> List[Survey]:
+    """`count` independent instances of uneven size for the batched forward
+    and Jacobian: split-quadrilateral triangle meshes of E log-uniform in
+    [emin, emax] elements (depth 6-64 cells, so mb = nz + 1 <= 65), L uniform
+    in 24..96 surface electrodes, dipole-dipole readings with a random set of
+    dipole lengths and n up to 4..12 (which puts the wavenumber count of the
+    reference's rwaven rule between 8 and 15), and per-element resistivities
+    log-uniform in 10..1000 Ohm m with phases uniform in -30..-1 mrad."""
+    out = []
+    spacing_sets = [(1,), (1, 2), (1, 2, 3), (1, 2, 4), (1, 3, 6)]
+    for i in range(count):
+        rng = np.random.default_rng([seed, i])
+        E = float(np.exp(rng.uniform(np.log(emin), np.log(emax))))
+        L = int(rng.integers(24, 97))
+        pad = 4
+        nx_min = L + 2 * pad + 2
+        nz = int(min(rng.integers(16, 65), max(6, E // (2 * nx_min))))
+        nx = max(nx_min, int(round(E / (2 * nz))))
+        core = nx - 2 * pad
+        w = 1.5 ** np.arange(1, pad + 1)
+        xs = np.concatenate([-np.cumsum(w)[::-1], np.arange(core + 1, dtype=np.float64), core + np.cumsum(w)])
+        depths = graded_depths(nz, 0.25, 1.04)
+        mesh = structured_mesh(xs, depths, triangles=True)
+        rho = np.exp(rng.uniform(np.log(10.0), np.log(1000.0), mesh.elanz))
+        pha = -rng.uniform(1.0, 30.0, mesh.elanz)
+        step = max(1, core // (L - 1))
+        x_el = (core - step * (L - 1)) // 2 + step * np.arange(L, dtype=np.float64)
+        enr = surface_electrodes(mesh, xs, x_el, nz)
+        spacings = spacing_sets[int(rng.integers(0, len(spacing_sets)))]
+        cfg = dipole_dipole(L, spacings, int(rng.integers(4, 13)))
+        strnr, vnr = encode(cfg)
+        out.append(Survey(mesh, enr, strnr, vnr, sigma_from(rho, pha), f"C4.{i}", nx, nz))
+    return out
+
+
 def small_triangles(seed: int = SEED0 + 100, nx: int = 24, nz: int = 10, nel: int = 12) -> Survey:
     """A small triangle mesh for quick parity tests."""
     rng = np.random.default_rng(seed)

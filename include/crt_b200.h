@@ -105,8 +105,8 @@ typedef struct {
 
 /* Steps of FP64 iterative refinement after the complex64 factorisation of
  * the mixed form (default 2; 0 leaves the complex64 solution): each step
- * forms the residual of the scaled system in FP64 (re-assembled from the
- * element matrices) and adds a complex64 correction solve.  No reference
+ * forms the residual of the scaled system in FP64 (from the FP64 entries of
+ * the prepared matrix) and adds a complex64 correction solve.  No reference
  * counterpart. */
 int32_t crt_set_refinement(crt_ctx *ctx, int32_t steps);
 
@@ -212,7 +212,9 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
  * scaling of all rows), [8] the factor kernels alone, [9] the number of
  * factor-kernel launches (one per chunk of systems), [10] the FP64
  * residuals and [11] the correction solves of the mixed form's refinement
- * (both inside [1]).  Milliseconds except [9].  No reference counterpart. */
+ * (both inside [1]), [12] the panel width of the blocked band factorisation
+ * (chosen by the autotuner; 0 for the unblocked kernel).  Milliseconds
+ * except [9] and [12].  No reference counterpart. */
 int32_t crt_last_timings_ex(const crt_ctx *ctx, double *ms, int32_t n);
 
 /* Kernel launches enqueued by the context since creation. */
@@ -296,6 +298,37 @@ int32_t crt_voltages_noalloc(const double *kpot, const double *kwnwi, const int3
 double crt_dmisft(int32_t nanz, const double *dat, const double *sigmaa, const double *wmatd,
                   const double *wmatdr, const double *wmatdp, int32_t lfpi, int32_t lpol,
                   double *betrms, double *pharms, int32_t *npol);
+
+/* ---------------------------------------------------------------------
+ * Batches of independent instances (no reference counterpart: CRMod runs
+ * one tomodir per process).  Each instance is its own context (mesh,
+ * survey, precision); a batch runs the forward of every instance -- and,
+ * with jacobian_mode >= 0, its Jacobian (0 bsensi, 1 bsendc, 2 bsens) --
+ * as one CUDA graph in which the instances are independent branches.
+ * The first crt_batch_run runs every instance once eagerly (allocating
+ * workspaces and autotuning the band panel width per precision and mb),
+ * then captures and replays the graph; later runs replay it.  The contexts
+ * must live on one device and outlive the batch, and may not be used by
+ * other calls while the batch runs.  ms receives the device time of the
+ * replay.  The results stay on the device in each context as its last
+ * forward (and Jacobian), which later calls on that context use;
+ * crt_batch_results copies them out. */
+typedef struct crt_batch crt_batch;
+crt_batch *crt_batch_create(crt_ctx *const *ctxs, int32_t count, int32_t ldc, int32_t jacobian_mode,
+                            int32_t *err);
+void crt_batch_destroy(crt_batch *b);
+const char *crt_batch_error(const crt_batch *b);
+/* sigma[i]: complex conductivity of instance i (E_i interleaved pairs). */
+int32_t crt_batch_set_models(crt_batch *b, const double *const *sigma);
+int32_t crt_batch_run(crt_batch *b, double *ms);
+/* errnr of instance i in the last run (0 = ok). */
+int32_t crt_batch_status(const crt_batch *b, int32_t i);
+/* volt / sigmaa: [N_i] complex; sens: [N_i, E_i] as crt_jacobian (NULL skips). */
+int32_t crt_batch_results(crt_batch *b, int32_t i, double *volt, double *sigmaa, double *sens);
+/* Upper bound of a context's band-factor workspace in bytes (0: default);
+ * the forward is chunked to fit.  Meant for batches, whose contexts hold
+ * their workspaces side by side. */
+int32_t crt_set_workspace_limit(crt_ctx *ctx, int64_t bytes);
 
 #ifdef __cplusplus
 }
