@@ -403,8 +403,10 @@ def main():
     pipe_peak = fma_clk * 2 * 148 * sm_mhz * 1e6 / 1e12
     ach = flops / nl / t_launch_s / 1e12 if t_launch_s > 0 else 0.0
     bpe = FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 if c64 else FACTOR_TRAFFIC_BYTES_PER_ENTRY
-    roof = {"kernel": ("k_band_factor_blk<cf,8,256,2> (complex64 band Cholesky + fused forward substitution)" if c64
-                       else "k_band_factor_blk<cd,8,512,1> (complex128 band Cholesky + fused forward substitution)"),
+    pb = int(ph.get("panel", 8)) or 8
+    roof = {"kernel": (f"k_band_factor_blk<cf,{pb}> (complex64 band Cholesky + fused forward substitution, "
+                       f"panel width {pb} by the autotuner)" if c64
+                       else f"k_band_factor_blk<cd,{pb}> (complex128 band Cholesky + fused forward substitution)"),
             "bound": "fp32" if c64 else "fp64", "achieved": ach, "peak": pipe_peak, "unit": "TFLOP/s",
             "frac": ach / pipe_peak,
             "traffic": bpe * n * (mb + 1) * nsys / nl if bpe else None,
