@@ -295,6 +295,13 @@ def run_batch(args, ws, rank, local, pg):
     ms = [b.run() for _ in range(args.steps)]
     barrier(pg)
     t = max_over_ranks(pg, local, float(np.mean(ms)) / 1e3)
+    # the same work one instance at a time through the per-context calls
+    # (crt_forward + crt_jacobian, host round trip per instance)
+    t0 = time.perf_counter()
+    for c, s in zip(ctxs, S):
+        c.forward(s.sigma)
+        c.jacobian(0, copy=False)
+    seq_s = time.perf_counter() - t0
     systems = sum(len(c.kwn) * len(s.enr) for c, s in zip(ctxs, S))
     E = [s.mesh.elanz for s in S]
     line = {"metric": "batched forward + Jacobian time of the uneven instances (one graph replay)", "value": t,
@@ -305,7 +312,8 @@ def run_batch(args, ws, rank, local, pg):
                                    f"{sum(len(s.strnr) for s in S)} readings, {systems} band systems",
                        "form": "complex64 band factorisation, two FP64 refinement steps, FP64 Jacobian stored complex64",
                        "workspace_bytes_per_instance": budget, "parallelism": f"replicas x{args.gpus}"},
-            "build_s": build_s, "panels": sorted({int(c.timings()["panel"]) for c in ctxs})}
+            "build_s": build_s, "sequential_calls_s": seq_s,
+            "panels": sorted({int(c.timings()["panel"]) for c in ctxs})}
     b.close()
     for c in ctxs:
         c.close()
