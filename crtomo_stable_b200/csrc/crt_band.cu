@@ -248,9 +248,11 @@ template <> __device__ __forceinline__ cf shfl_down_t<cf>(cf v, int off)
     return cf{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)};
 }
 
-// Resident CTAs per SM of the solve: complex64 state is small enough for
-// three (latency hiding across systems), complex128 for two.
+// Resident CTAs per SM of the solve (latency hiding across systems): two;
+// complex64, whose prefetch double buffer of a 32-column block is 66.5 KB at
+// mb = 129, three (the forward and backward triangles share one buffer).
 template <typename T> struct SolveOcc { static constexpr int v = 2; };
+template <> struct SolveOcc<cf> { static constexpr int v = 3; };
 // complex64 solves stage the next block of 32 columns of the factor (one
 // contiguous run: the factor is column-packed with an even column stride)
 // in a shared double buffer while the current block is solved
@@ -260,7 +262,10 @@ template <> struct SolvePrefetch<cf> { static constexpr bool v = true; };
 template <typename T, int NT, int BB>
 __global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> A, T* scratch)
 {
-    __shared__ T tri[BB][BB];
+    // the forward pass's triangle tri[c][d] and the backward pass's trw[r][c]
+    // share one buffer (the passes are separated by a barrier)
+    __shared__ __align__(16) T trbuf[BB * (BB + 1)];
+    T(*tri)[BB] = reinterpret_cast<T(*)[BB]>(trbuf);
     __shared__ T part[BB];
     __shared__ T zb[BB];
     extern __shared__ __align__(16) unsigned char solve_dyn[];
@@ -380,7 +385,7 @@ __global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> 
     // one shuffle broadcast and one FMA per lane).
     constexpr int TPC = NT / BB;
     static_assert(BB == 32 && TPC * BB == NT && (TPC & (TPC - 1)) == 0, "solve layout");
-    __shared__ T trw[BB][BB + 1];   // trw[r][c] = L(c0 + r, c0 + c), r >= c
+    T(*trw)[BB + 1] = reinterpret_cast<T(*)[BB + 1]>(trbuf);   // trw[r][c] = L(c0 + r, c0 + c), r >= c
     const int col = tid / TPC, sub = tid % TPC;
     if constexpr (PF) {
         prefetch(max(0, n - BB), n - max(0, n - BB), 0);
@@ -468,6 +473,8 @@ void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStrea
     if (SolvePrefetch<T>::v) {
         dyn = 2 * (size_t)BB * a.W * sizeof(T);
         cudaFuncSetAttribute(k_band_solve<T, NT, BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+        cudaFuncSetAttribute(k_band_solve<T, NT, BB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
     }
     k_band_solve<T, NT, BB><<<a.nsys, NT, dyn, st>>>(a, scratch);
 }
