@@ -139,24 +139,32 @@ __global__ void k_band_prep_diag(BandArgs<T> A)
     if (A.aval && e0 >= 0) A.aval[(size_t)b * A.aval_stride + e0] = Sc<WT>::to_cd(dn);
 }
 
-// Off-diagonal entries of every row, one warp per row: zero fill, then
-// a(r, r-d) * fak_r * fak_(r-d), or 0 when either node is a Dirichlet node.
+// Off-diagonal entries of every row, PREP_G lanes per row (a row has a
+// handful of entries below the diagonal, so a warp serves 32 / PREP_G rows):
+// zero fill, then a(r, r-d) * fak_r * fak_(r-d), or 0 when either node is a
+// Dirichlet node.
+constexpr int PREP_G = 8;
+
 template <typename T>
 __global__ void k_band_prep_rows(BandArgs<T> A)
 {
-    const long long wid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31, n = A.n;
-    if (wid >= (long long)A.nsys * n) return;
-    const int b = (int)(wid / n), r = (int)(wid % n), sys = A.sys0 + b;
+    const long long gid = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / PREP_G;
+    const int lane = threadIdx.x % PREP_G, n = A.n;
+    // every lane reaches the warp barrier: the zero fill must be visible
+    // before any lane of the row writes an entry
+    const bool active = gid < (long long)A.nsys * n;
+    const int b = active ? (int)(gid / n) : 0, r = active ? (int)(gid % n) : 0, sys = A.sys0 + b;
+    T* row = A.Lws + (size_t)b * A.lstride + (size_t)r * A.W;
+    if (active)
+        for (int d = 1 + lane; d <= A.mb; d += PREP_G) row[d] = Sc<T>::zero();
+    __syncwarp();
+    if (!active) return;
     int k, l;
     sys_kl(A, sys, k, l);
-    T* row = A.Lws + (size_t)b * A.lstride + (size_t)r * A.W;
     const double* fk = A.fakws + (size_t)b * n;
-    for (int d = 1 + lane; d <= A.mb; d += 32) row[d] = Sc<T>::zero();
-    __syncwarp();
     const bool dr = A.dflag[r] != 0;
     const double fr = fk[r];
-    for (int e = A.row_ptr[r] + lane; e < A.row_ptr[r + 1]; e += 32) {
+    for (int e = A.row_ptr[r] + lane; e < A.row_ptr[r + 1]; e += PREP_G) {
         const int d = A.ent_d[e];
         if (d == 0) continue;
         const int c = r - d;
@@ -520,7 +528,7 @@ void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
 {
     const long long rows = (long long)a.nsys * a.n;
     k_band_prep_diag<T><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(a);
-    k_band_prep_rows<T><<<(unsigned)((rows * 32 + 255) / 256), 256, 0, st>>>(a);
+    k_band_prep_rows<T><<<(unsigned)((rows * PREP_G + 255) / 256), 256, 0, st>>>(a);
 }
 
 template <typename T, int PB>
