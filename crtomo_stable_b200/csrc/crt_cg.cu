@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A)
 // ap partial sums over a column range: thread per reading.  The block stages
 // p o cgfac for JV_CHUNK columns in shared memory and keeps JV_UNROLL
 // independent J loads in flight per thread.
-constexpr int JV_NT = 256, JV_CHUNK = 256, JV_UNROLL = 8;
+constexpr int JV_NT = 256, JV_CHUNK = 256, JV_UNROLL = 16;
 
 template <int JP, int JM>
 __global__ void __launch_bounds__(JV_NT) k_cg_jv(CGArgs A)
@@ -362,7 +362,24 @@ __global__ void k_cg_jhv(CGArgs A)
         ax[c] = 0.0;
         ay[c] = 0.0;
     }
-    for (int i = lane; i < A.N; i += 32) {
+    // two rows per lane and step keep 2 JH_COLS loads of J in flight
+    int i = lane;
+    for (; i + 32 < A.N; i += 64) {
+        const cd w0 = A.ap[i], w1 = A.ap[i + 32];
+        cd j0[JH_COLS], j1[JH_COLS];
+#pragma unroll
+        for (int c = 0; c < JH_COLS; ++c) {
+            j0[c] = (c < nc) ? jval<JP, JM>(A, ebase + c, i) : cd{0.0, 0.0};
+            j1[c] = (c < nc) ? jval<JP, JM>(A, ebase + c, i + 32) : cd{0.0, 0.0};
+        }
+#pragma unroll
+        for (int c = 0; c < JH_COLS; ++c) {
+            const cd t0 = conj(j0[c]) * w0, t1 = conj(j1[c]) * w1;
+            ax[c] += t0.x + t1.x;
+            ay[c] += t0.y + t1.y;
+        }
+    }
+    for (; i < A.N; i += 32) {
         const cd w = A.ap[i];
         cd jv[JH_COLS];
 #pragma unroll
