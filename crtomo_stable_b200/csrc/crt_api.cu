@@ -654,7 +654,7 @@ int run_forward(crt_ctx* ctx)
             const bool force_v0 = fv && std::strcmp(fv, "v0") == 0;
             if (!force_v0 && band_blk_fits<T>(ctx->mb)) {
                 const int pb = band_panel<T>(A, !ctx->capture, ctx->st);
-                ctx->panel = pb;
+                ctx->panel = pb & BAND_PANEL_MASK;
                 launch_band_prep<T>(A, ctx->st);
                 if (!ev_rec(ctx, 8)) return CRT_ERR_CUDA;
                 launch_band_factor_blk<T>(A, pb, ctx->st);

@@ -49,13 +49,18 @@ struct SolveArgs {
 };
 
 template <typename T> void launch_band_factor(const BandArgs<T>& a, cudaStream_t st);
-// Panel-blocked variant with panel width pb (4, 8 or 16); returns false
-// when its window does not fit in shared memory.
-template <typename T> bool launch_band_factor_blk(const BandArgs<T>& a, int pb, cudaStream_t st);
-// Panel width for a's element type and half-bandwidth: the autotuned value
+// Launch configuration of the panel-blocked variant: the panel width (4, 8
+// or 16) in the low bits, BAND_CFG_WIDE for one 512-thread CTA per SM where
+// the window would also fit twice (two 256-thread CTAs otherwise).
+constexpr int BAND_PANEL_MASK = 0xff;
+constexpr int BAND_CFG_WIDE = 0x100;
+// Panel-blocked variant in configuration cfg; returns false when its window
+// does not fit in shared memory.
+template <typename T> bool launch_band_factor_blk(const BandArgs<T>& a, int cfg, cudaStream_t st);
+// Configuration for a's element type and half-bandwidth: the autotuned value
 // of this process; the first call per (type, mb) measures the candidates on
 // up to two waves of a's systems when may_tune (it prepares and factors
-// them, so the caller prepares them again), else returns 8.
+// them, so the caller prepares them again), else returns panel 8.
 template <typename T> int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st);
 // Whether the panel-blocked window fits in shared memory for half-bandwidth mb.
 template <typename T> bool band_blk_fits(int mb);

@@ -33,6 +33,7 @@
 // block factorisation overlaps the trailing update of the previous panel.
 #include "crt_band.h"
 
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -532,46 +533,50 @@ void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
 }
 
 template <typename T, int PB>
-static void launch_blk_pb(const BandArgs<T>& a, cudaStream_t st)
+static void launch_blk_pb(const BandArgs<T>& a, bool one_wide, cudaStream_t st)
 {
     int Wn = 0;
     const size_t smem = blk_smem<T, PB>(a.mb, &Wn);
-    // a window that fits twice (complex64, or real FP64) runs as two
+    // a window that fits twice (complex64, or real FP64) may run as two
     // 256-thread CTAs per SM, overlapping one system's serial phases with the
-    // other's update; a larger window leaves room for one CTA of 512
+    // other's update; otherwise (or when asked) one CTA of 512 per SM
     auto go = [&](auto kern, int nt) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<a.nsys, nt, smem, st>>>(a, Wn);
     };
-    if (2 * smem <= 227 * 1024) go(k_band_factor_blk<T, PB, 256, 2>, 256);
+    if (2 * smem <= 227 * 1024 && !one_wide) go(k_band_factor_blk<T, PB, 256, 2>, 256);
     else go(k_band_factor_blk<T, PB, 512, 1>, 512);
 }
 
 template <typename T>
-bool launch_band_factor_blk(const BandArgs<T>& a, int pb, cudaStream_t st)
+bool launch_band_factor_blk(const BandArgs<T>& a, int cfg, cudaStream_t st)
 {
+    const int pb = cfg & BAND_PANEL_MASK;
+    const bool wide = (cfg & BAND_CFG_WIDE) != 0;
     if (!blk_fits_pb<T>(pb, a.mb)) return false;
     switch (pb) {
-    case 4: launch_blk_pb<T, 4>(a, st); break;
-    case 16: launch_blk_pb<T, 16>(a, st); break;
-    default: launch_blk_pb<T, 8>(a, st); break;
+    case 4: launch_blk_pb<T, 4>(a, wide, st); break;
+    case 16: launch_blk_pb<T, 16>(a, wide, st); break;
+    default: launch_blk_pb<T, 8>(a, wide, st); break;
     }
     return true;
 }
 
 // ---------------------------------------------------------------------------
-// Panel-width autotuner.  The best panel (4, 8 or 16 columns) depends on the
-// element type and the half-bandwidth (window size, CTAs per SM, serial
-// panel phases against the rank-PB update); it is measured once per
+// Panel-width autotuner.  The best panel (4, 8 or 16 columns) and CTA shape
+// (two 256-thread CTAs per SM where the window fits twice, or one of 512)
+// depend on the element type and the half-bandwidth (window size, CTAs per
+// SM, serial panel phases against the rank-PB update); they are measured once per
 // (type, mb) in the process on the first systems of a real chunk: for each
 // candidate that fits, the preparation pass and the factorisation of up to
 // two waves of systems are run and the factorisation is timed with events.
 // The caller's real pass then prepares and factors the chunk again, so the
 // trials leave no trace but their per-system status, which is cleared.
-// CRT_B200_PANEL = 4 | 8 | 16 fixes the width.
+// CRT_B200_PANEL = 4 | 8 | 16 fixes the width; CRT_B200_TUNE_LOG prints the
+// trials to stderr.
 namespace {
 std::mutex g_panel_mu;
-std::map<std::pair<int, int>, int> g_panel;   // (sizeof(T), mb) -> panel width
+std::map<std::pair<int, int>, int> g_panel;   // (sizeof(T), mb) -> launch configuration
 }
 
 template <typename T>
@@ -598,18 +603,26 @@ int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st)
     cudaEventCreate(&e1);
     int best = 8;
     float best_ms = 1e30f;
-    for (int pb : {8, 4, 16}) {
+    for (int cfg : {8, 4, 16, 8 | BAND_CFG_WIDE, 4 | BAND_CFG_WIDE}) {
+        const int pb = cfg & BAND_PANEL_MASK;
         if (!blk_fits_pb<T>(pb, a.mb)) continue;
+        int Wn = 0;
+        if ((cfg & BAND_CFG_WIDE) && 2 * blk_smem_pb<T>(pb, a.mb, &Wn) > 227 * 1024) continue;   // same as pb alone
         launch_band_prep<T>(t, st);
         cudaEventRecord(e0, st);
-        launch_band_factor_blk<T>(t, pb, st);
+        launch_band_factor_blk<T>(t, cfg, st);
         cudaEventRecord(e1, st);
         if (cudaEventSynchronize(e1) != cudaSuccess) break;
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e0, e1);
+        if (std::getenv("CRT_B200_TUNE_LOG")) {
+            const bool twice = 2 * blk_smem_pb<T>(pb, a.mb, &Wn) <= 227 * 1024;
+            std::fprintf(stderr, "band factor autotune: %d-byte entries, mb %d, panel %d, %d threads: %.3f ms\n",
+                         (int)sizeof(T), a.mb, pb, (twice && !(cfg & BAND_CFG_WIDE)) ? 256 : 512, ms);
+        }
         if (ms < best_ms) {
             best_ms = ms;
-            best = pb;
+            best = cfg;
         }
     }
     cudaEventDestroy(e0);
