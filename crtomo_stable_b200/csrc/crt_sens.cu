@@ -169,13 +169,21 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
 #pragma unroll
         for (int j = 0; j < GR_TB; ++j) acc[i][j] = Sc<T>::zero();
     T* phi = sbuf;                                   // [kc][nk][LP]
-    T* wu = sbuf + (size_t)kc * nk * LP;             // [kc][nk][LP]
+    // [kc][nk][GR_TB][LP / GR_TB]: column b at (b % GR_TB) LP/GR_TB + b / GR_TB,
+    // so the tile loads of consecutive column blocks are consecutive words
+    T* wu = sbuf + (size_t)kc * nk * LP;
+    const int LQ = LP / GR_TB;
+    // the element's nodes once, so the potential gathers below do not wait
+    // on an index load each
+    __shared__ int s_node[4];
+    if (tid < nk) s_node[tid] = A.nrel0[e * A.maxnodes + tid];
     for (int k0 = 0; k0 < K; k0 += kc) {
         const int kn = min(kc, K - k0);
         __syncthreads();
+#pragma unroll 4
         for (int t = tid; t < kn * nk * LP; t += blockDim.x) {
             const int a = t % LP, m = (t / LP) % nk, kk = t / (LP * nk);
-            const int node = A.nrel0[e * A.maxnodes + m];
+            const int node = s_node[m];
             phi[t] = a < L ? ld_phi<T>(A.kpt[((size_t)(k0 + kk) * A.n + node) * L + a]) : Sc<T>::zero();
         }
         __syncthreads();
@@ -188,18 +196,18 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
                 const int ix = max(m, m2), in = min(m, m2);
                 v += scale(phi[((size_t)kk * nk + m2) * LP + b], km[ix * (ix + 1) / 2 + in]);
             }
-            wu[t] = scale(v, w);
+            wu[t - b + (b % GR_TB) * LQ + b / GR_TB] = scale(v, w);
         }
         __syncthreads();
         if (has_tile) {
             for (int q = 0; q < kn * nk; ++q) {
                 const T* pa = phi + (size_t)q * LP + R * GR_TA;
-                const T* pb = wu + (size_t)q * LP + Cb * GR_TB;
+                const T* pb = wu + (size_t)q * LP + Cb;
                 T av[GR_TA], bv[GR_TB];
 #pragma unroll
                 for (int i = 0; i < GR_TA; ++i) av[i] = pa[i];
 #pragma unroll
-                for (int j = 0; j < GR_TB; ++j) bv[j] = pb[j];
+                for (int j = 0; j < GR_TB; ++j) bv[j] = pb[j * LQ];
 #pragma unroll
                 for (int i = 0; i < GR_TA; ++i)
 #pragma unroll
