@@ -18,16 +18,17 @@
 // columns [i0, i0 + PB):
 //   2. every window row below the panel solves its PB entries against the
 //      block factor (L_x = A_x L_D^-T), updates its right-hand side and
-//      writes its L entries to the window and to the column-packed HBM
-//      factor;
+//      writes its L entries to a panel buffer (t-major) and to the
+//      column-packed HBM factor;
 //   3a. the entries of the next panel's diagonal tiles receive the panel's
 //      rank-PB update (one entry per thread);
 //   3b. warp 0 factors the next PB x PB diagonal block (unconjugated L L^T,
 //      the recurrence of src/chol.f90:44-78 restricted to the block) and
 //      forward-substitutes its right-hand side, while warps 1.. update the
 //      rest of the trailing window by the rank-PB product L_x L_y^T (each
-//      thread accumulating 4 x 4 tiles in registers) and load the next PB
-//      prepared rows into a staging buffer;
+//      thread accumulating 4 x 4 tiles in registers, the panel columns read
+//      from the panel buffer) and load the next PB prepared rows into a
+//      staging buffer;
 //   4. the PB staged rows are written into the slots the panel freed.
 // The first diagonal block is factored before the loop, so the serial
 // block factorisation overlaps the trailing update of the previous panel.
@@ -210,6 +211,24 @@ __global__ void k_band_residual(BandArgs<T> A, int sys0, int nsolve, int div, co
     rout[(size_t)b * n + r] = narrow<T>(bb - acc);
 }
 
+// Four consecutive window-row entries of a panel column (16-byte aligned).
+template <typename T>
+__device__ __forceinline__ void load4(const T* p, T (&v)[4])
+{
+#pragma unroll
+    for (int a = 0; a < 4; ++a) v[a] = p[a];
+}
+template <>
+__device__ __forceinline__ void load4<cf>(const cf* p, cf (&v)[4])
+{
+    const float4 u = *reinterpret_cast<const float4*>(p);
+    const float4 w = *reinterpret_cast<const float4*>(p + 2);
+    v[0] = cf{u.x, u.y};
+    v[1] = cf{u.z, u.w};
+    v[2] = cf{w.x, w.y};
+    v[3] = cf{w.z, w.w};
+}
+
 template <typename T, int PB, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int Wn)
 {
@@ -225,6 +244,10 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
     T* LDi = yP + PB;                                     // PB reciprocal pivots
     double* fakN = reinterpret_cast<double*>(LDi + PB);   // PB scaling factors of the staged rows
     unsigned short* tXY = reinterpret_cast<unsigned short*>(fakN + PB);   // NTT tile coordinates
+    // the panel's columns L(x, i0 + t) of every window row x, t-major
+    // (pan[t Wn + x]): the trailing updates read them here, so the panel's
+    // slots of the window are free for the next rows while they run
+    T* pan = reinterpret_cast<T*>((reinterpret_cast<size_t>(tXY + NTT) + 15) & ~(size_t)15);
     __shared__ T colb[32];                                                // column broadcast of the block factor
     __shared__ T bN[PB];                                                  // scaled right-hand side of the staged rows
     __shared__ int s_err;
@@ -278,9 +301,9 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
     // holds rows [wlo, wlo + Wn).  Every pair of a new slot with a row
     // c <= r is written (zero outside the band), pairs with later new rows
     // are written by those rows.
-    auto scatter_rows = [&](int r0, int s_new, int wlo) {
+    auto scatter_rows = [&](int r0, int s_new, int wlo, int t0) {
         const int wm = wlo % Wn;
-        for (int i = tid; i < PB * Wn; i += NT) {
+        for (int i = tid - t0; i < PB * Wn; i += NT - t0) {
             const int q = i % PB, y = i / PB;             // PB is a power of two
             int off = y - wm;
             if (off < 0) off += Wn;
@@ -290,14 +313,14 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             const int d = r - c;
             win[widx(s_new + q, y)] = (r < n && d <= mb) ? stage[q * W1 + d] : Sc<T>::zero();
         }
-        if (tid < PB) bsl[s_new + tid] = bN[tid];
+        if (tid - t0 >= 0 && tid - t0 < PB) bsl[s_new + tid - t0] = bN[tid - t0];
     };
 
     // Initial window: rows 0 .. Wn-1, PB at a time.
     for (int r0 = 0; r0 < Wn; r0 += PB) {
         load_rows(r0, 0);
         __syncthreads();
-        scatter_rows(r0, r0, 0);
+        scatter_rows(r0, r0, 0, 0);
         __syncthreads();
     }
 
@@ -358,18 +381,8 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             if (fuse) yv[p0 + j] = yP[j];
         }
     };
-    // Offsets of the panel entries of tile row X: the panel occupies tile
-    // rows [P0, P0 + NPT); the panel entries of the rows of tile row X sit in
-    // tiles (X, P) when X follows the panel in slot order (entry (a, t & 3))
-    // and in tiles (P, X) when it precedes it (entry (t & 3, a)).
+    // the panel occupies tile rows [P0, P0 + NPT) of the window
     constexpr int NPT = PB / 4;
-    auto panel_offsets = [&](int X, int P0, int (&bo)[NPT], int& ts, int& as) {
-        const bool after = X > P0;
-#pragma unroll
-        for (int p = 0; p < NPT; ++p) bo[p] = (after ? tile_base(X, P0 + p) : tile_base(P0 + p, X)) * TSTRIDE;
-        ts = after ? 1 : 4;
-        as = after ? 4 : 1;
-    };
 
     if (warp == 0) diag_block(0);
     __syncthreads();
@@ -385,20 +398,27 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             if (dx < 0) dx += Wn;
             if (dx < PB) continue;                         // panel slot
             const int r = i0 + dx;
-            if (r >= n || dx > mb + PB - 1) continue;
+            if (r >= n || dx > mb + PB - 1) {
+#pragma unroll
+                for (int t = 0; t < PB; ++t) pan[t * Wn + x] = Sc<T>::zero();
+                continue;
+            }
             T lx[PB];
 #pragma unroll
             for (int t = 0; t < PB; ++t) lx[t] = (t < np_) ? win[widx(x, s0 + t)] : Sc<T>::zero();
             T bx = fuse ? bsl[x] : Sc<T>::zero();
 #pragma unroll
             for (int t = 0; t < PB; ++t) {
-                if (t >= np_) break;
+                if (t >= np_) {
+                    pan[t * Wn + x] = Sc<T>::zero();
+                    continue;
+                }
                 T s = lx[t];
 #pragma unroll
                 for (int t2 = 0; t2 < t; ++t2) fms_acc(s, lx[t2], LD[t * PB + t2]);
                 lx[t] = Sc<T>::mul(s, LDi[t]);
                 if (fuse) fms_acc(bx, lx[t], yP[t]);
-                win[widx(x, s0 + t)] = lx[t];
+                pan[t * Wn + x] = lx[t];
                 const int d = r - (i0 + t);
                 if (d <= mb) Lc[(size_t)(i0 + t) * W1 + d] = lx[t];
             }
@@ -421,15 +441,12 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
                 const int yo = kt - xo * (xo + 1) / 2;
                 const int X = P0n + xo, Y = P0n + yo, a = q >> 2, c = q & 3;
                 if (X == Y && a < c) continue;
-                int bx[NPT], by[NPT], xt, xs, yt, ys;
-                panel_offsets(X, P0, bx, xt, xs);
-                panel_offsets(Y, P0, by, yt, ys);
                 T* tp = win + tile_base(X, Y) * TSTRIDE + q;
                 T acc = *tp;
 #pragma unroll
                 for (int t = 0; t < PB; ++t) {
                     if (t >= np_) break;
-                    fms_acc(acc, win[bx[t >> 2] + (t & 3) * xt + a * xs], win[by[t >> 2] + (t & 3) * yt + c * ys]);
+                    fms_acc(acc, pan[t * Wn + 4 * X + a], pan[t * Wn + 4 * Y + c]);
                 }
                 *tp = acc;
             }
@@ -438,7 +455,8 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
         // PROBE1
         // ---- phase 3b: warp 0 factors the next diagonal block; warps 1..
         // update the rest of the window by the rank-PB product L_x L_y^T on
-        // 4 x 4 tiles and then load the next PB prepared rows.
+        // 4 x 4 tiles (the panel columns read from pan) and then load the
+        // next PB prepared rows.
         if (warp == 0) {
             if (has_next) diag_block(inext);
         } else {
@@ -447,9 +465,6 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
                     const int X = tXY[tt] >> 8, Y = tXY[tt] & 0xff;
                     if ((X >= P0 && X < P0 + NPT) || (Y >= P0 && Y < P0 + NPT)) continue;
                     if (X >= P0n && X < P0n + NPT && Y >= P0n && Y < P0n + NPT) continue;   // done in 3a
-                    int bx[NPT], by[NPT], xt, xs, yt, ys;
-                    panel_offsets(X, P0, bx, xt, xs);
-                    panel_offsets(Y, P0, by, yt, ys);
                     T acc[16];
                     T* tp = win + tt * TSTRIDE;
 #pragma unroll
@@ -457,12 +472,9 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
 #pragma unroll
                     for (int t = 0; t < PB; ++t) {
                         if (t >= np_) break;
-                        const int ox = bx[t >> 2] + (t & 3) * xt, oy = by[t >> 2] + (t & 3) * yt;
                         T px[4], py[4];
-#pragma unroll
-                        for (int a = 0; a < 4; ++a) px[a] = win[ox + a * xs];
-#pragma unroll
-                        for (int a = 0; a < 4; ++a) py[a] = win[oy + a * ys];
+                        load4(pan + t * Wn + 4 * X, px);
+                        load4(pan + t * Wn + 4 * Y, py);
 #pragma unroll
                         for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -480,7 +492,7 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
         __syncthreads();
         // PROBE2
         // ---- phase 4: the staged rows enter the freed panel slots
-        scatter_rows(rnew0, s0, i0 + PB);
+        scatter_rows(rnew0, s0, i0 + PB, 0);
         __syncthreads();
         // PROBE3
     }
@@ -495,7 +507,8 @@ static size_t blk_smem(int mb, int* Wn_out)
     const int Wn = ((mb + PB + PB - 1) / PB) * PB;
     const int NTR = Wn / 4, NTT = NTR * (NTR + 1) / 2;
     size_t s = (size_t)NTT * TSTRIDE * sizeof(T) + (size_t)PB * (mb + 1) * sizeof(T) + (size_t)PB * PB * sizeof(T) +
-               (size_t)Wn * sizeof(T) + 2 * PB * sizeof(T) + (size_t)Wn * 8 + PB * 8 + (size_t)NTT * 2 + Wn + 64;
+               (size_t)Wn * sizeof(T) + 2 * PB * sizeof(T) + (size_t)Wn * 8 + PB * 8 + (size_t)NTT * 2 + Wn + 64 +
+               (size_t)PB * Wn * sizeof(T) + 16;
     *Wn_out = Wn;
     return s;
 }
