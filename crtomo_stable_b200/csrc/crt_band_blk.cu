@@ -27,9 +27,10 @@
 //      forward-substitutes its right-hand side, while warps 1.. update the
 //      rest of the trailing window by the rank-PB product L_x L_y^T (each
 //      thread accumulating 4 x 4 tiles in registers, the panel columns read
-//      from the panel buffer) and load the next PB prepared rows into a
-//      staging buffer;
-//   4. the PB staged rows are written into the slots the panel freed.
+//      from the panel buffer), while the next PB prepared rows arrive in a
+//      staging buffer by cp.async; once all of them are through (a barrier
+//      of warps 1.. only), they write the staged rows into the slots the
+//      panel freed.
 // The first diagonal block is factored before the loop, so the serial
 // block factorisation overlaps the trailing update of the previous panel.
 #include "crt_band.h"
@@ -229,6 +230,12 @@ __device__ __forceinline__ void load4<cf>(const cf* p, cf (&v)[4])
     v[3] = cf{w.z, w.w};
 }
 
+// Staged rows copied with 16-byte cp.async: complex entries (8 or 16
+// bytes, and the complex64 column stride is even), so every row run starts
+// on a 16-byte boundary; real FP64 rows may not.
+template <typename T> struct StageAsync { static constexpr bool v = true; };
+template <> struct StageAsync<double> { static constexpr bool v = false; };
+
 template <typename T, int PB, int NT, int MINB>
 __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int Wn)
 {
@@ -281,12 +288,8 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
 
     // Prepared rows [r0, r0 + PB) into stage[q][d] and their scaling factors
     // into fakN (threads t0 .. NT-1; rows beyond n are zero).
-    auto load_rows = [&](int r0, int t0) {
-        const T* src_rows = Lc + (size_t)r0 * W1;
-        for (int i = tid - t0; i < PB * W1; i += NT - t0) {
-            const int q = i / W1;
-            stage[i] = (r0 + q < n) ? src_rows[i] : Sc<T>::zero();
-        }
+    // per-row scaling factors and right-hand sides of the staged rows
+    auto row_meta = [&](int r0, int t0) {
         const int q = tid - t0;
         if (q >= 0 && q < PB) {
             const int r = r0 + q;
@@ -296,6 +299,14 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             if (fuse && r < n) bb = scale(rhs_entry_b<T>(r, src, A.lsink, A.nsink0, A.dflag, A.dval, bdir), f);
             bN[q] = bb;
         }
+    };
+    auto load_rows = [&](int r0, int t0) {
+        const T* src_rows = Lc + (size_t)r0 * W1;
+        for (int i = tid - t0; i < PB * W1; i += NT - t0) {
+            const int q = i / W1;
+            stage[i] = (r0 + q < n) ? src_rows[i] : Sc<T>::zero();
+        }
+        row_meta(r0, t0);
     };
     // Staged rows into slots s_new .. s_new+PB-1; the window after the write
     // holds rows [wlo, wlo + Wn).  Every pair of a new slot with a row
@@ -455,11 +466,22 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
         // PROBE1
         // ---- phase 3b: warp 0 factors the next diagonal block; warps 1..
         // update the rest of the window by the rank-PB product L_x L_y^T on
-        // 4 x 4 tiles (the panel columns read from pan) and then load the
-        // next PB prepared rows.
+        // 4 x 4 tiles (the panel columns read from pan) and then write the
+        // staged rows into the panel's slots.
         if (warp == 0) {
             if (has_next) diag_block(inext);
         } else {
+            // the next PB prepared rows start their way into the staging
+            // buffer (cp.async) and arrive while the tiles are updated
+            const char* srcb = reinterpret_cast<const char*>(Lc + (size_t)rnew0 * W1);
+            char* dstb = reinterpret_cast<char*>(stage);
+            const int bytes = PB * W1 * (int)sizeof(T);
+            const bool async_rows = StageAsync<T>::v && rnew0 + PB <= n && (reinterpret_cast<size_t>(srcb) & 15) == 0 &&
+                                    (reinterpret_cast<size_t>(dstb) & 15) == 0 && (bytes & 15) == 0;
+            if (async_rows) {
+                for (int off = (tid - 32) * 16; off < bytes; off += (NT - 32) * 16) cp_async16(dstb + off, srcb + off);
+                cp_async_commit();
+            }
             if (has_next) {
                 for (int tt = tid - 32; tt < NTT; tt += NT - 32) {
                     const int X = tXY[tt] >> 8, Y = tXY[tt] & 0xff;
@@ -487,13 +509,20 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
                     }
                 }
             }
-            load_rows(rnew0, 32);
+            if (async_rows) {
+                cp_async_wait_all();
+                row_meta(rnew0, 32);
+            } else {
+                load_rows(rnew0, 32);
+            }
+            // warps 1.. only (warp 0 is in the diagonal block): the staged rows
+            // are visible, and every tile update is done, so the panel's
+            // slots take the new rows
+            asm volatile("bar.sync 1, %0;\n" ::"r"(NT - 32) : "memory");
+            scatter_rows(rnew0, s0, i0 + PB, 32);
         }
         __syncthreads();
         // PROBE2
-        // ---- phase 4: the staged rows enter the freed panel slots
-        scatter_rows(rnew0, s0, i0 + PB, 0);
-        __syncthreads();
         // PROBE3
     }
     if (tid == 0 && s_err) A.status[sys] = s_err;
