@@ -200,7 +200,10 @@ __global__ void k_band_residual(BandArgs<T> A, int sys0, int nsolve, int div, co
     const double* fk = A.fakws + (size_t)slot * n;
     const cd* kp = kpot + (size_t)sys * n;
     const cd* av = A.aval + (size_t)slot * A.aval_stride;
-    auto zval = [&](int c) { return cd{-kp[c].x / fk[c], -kp[c].y / fk[c]}; };
+    auto zval = [&](int c) {
+        const double inv = 1.0 / fk[c];   // one division for both components
+        return cd{-kp[c].x * inv, -kp[c].y * inv};
+    };
     cd acc{0.0, 0.0};
     if (A.dflag[r]) {
         acc = zval(r);
@@ -230,6 +233,11 @@ __device__ __forceinline__ void load4<cf>(const cf* p, cf (&v)[4])
     v[3] = cf{w.z, w.w};
 }
 
+// Panel buffer padding (see the kernel): complex64 reads four entries with
+// two 16-byte loads and keeps the rows unpadded (16-byte aligned).
+template <typename T> struct PanPad { static constexpr bool v = true; };
+template <> struct PanPad<cf> { static constexpr bool v = false; };
+
 // Staged rows copied with 16-byte cp.async: complex entries (8 or 16
 // bytes, and the complex64 column stride is even), so every row run starts
 // on a 16-byte boundary; real FP64 rows may not.
@@ -255,6 +263,12 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
     // (pan[t Wn + x]): the trailing updates read them here, so the panel's
     // slots of the window are free for the next rows while they run
     T* pan = reinterpret_cast<T*>((reinterpret_cast<size_t>(tXY + NTT) + 15) & ~(size_t)15);
+    // row x of a panel column at ppos(x); entry types without the 16-byte
+    // vector loads pad every tile row of 4 by one entry, so the tile rows a
+    // warp reads at once fall into different banks
+    constexpr bool PAN_PAD = PanPad<T>::v;
+    const int PS = PAN_PAD ? Wn + Wn / 4 : Wn;   // stride between panel columns
+    auto ppos = [&](int x) { return PAN_PAD ? x + (x >> 2) : x; };
     __shared__ T colb[32];                                                // column broadcast of the block factor
     __shared__ T bN[PB];                                                  // scaled right-hand side of the staged rows
     __shared__ int s_err;
@@ -411,7 +425,7 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             const int r = i0 + dx;
             if (r >= n || dx > mb + PB - 1) {
 #pragma unroll
-                for (int t = 0; t < PB; ++t) pan[t * Wn + x] = Sc<T>::zero();
+                for (int t = 0; t < PB; ++t) pan[t * PS + ppos(x)] = Sc<T>::zero();
                 continue;
             }
             T lx[PB];
@@ -421,7 +435,7 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
 #pragma unroll
             for (int t = 0; t < PB; ++t) {
                 if (t >= np_) {
-                    pan[t * Wn + x] = Sc<T>::zero();
+                    pan[t * PS + ppos(x)] = Sc<T>::zero();
                     continue;
                 }
                 T s = lx[t];
@@ -429,7 +443,7 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
                 for (int t2 = 0; t2 < t; ++t2) fms_acc(s, lx[t2], LD[t * PB + t2]);
                 lx[t] = Sc<T>::mul(s, LDi[t]);
                 if (fuse) fms_acc(bx, lx[t], yP[t]);
-                pan[t * Wn + x] = lx[t];
+                pan[t * PS + ppos(x)] = lx[t];
                 const int d = r - (i0 + t);
                 if (d <= mb) Lc[(size_t)(i0 + t) * W1 + d] = lx[t];
             }
@@ -457,7 +471,7 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
 #pragma unroll
                 for (int t = 0; t < PB; ++t) {
                     if (t >= np_) break;
-                    fms_acc(acc, pan[t * Wn + 4 * X + a], pan[t * Wn + 4 * Y + c]);
+                    fms_acc(acc, pan[t * PS + ppos(4 * X) + a], pan[t * PS + ppos(4 * Y) + c]);
                 }
                 *tp = acc;
             }
@@ -495,8 +509,8 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
                     for (int t = 0; t < PB; ++t) {
                         if (t >= np_) break;
                         T px[4], py[4];
-                        load4(pan + t * Wn + 4 * X, px);
-                        load4(pan + t * Wn + 4 * Y, py);
+                        load4(pan + t * PS + ppos(4 * X), px);
+                        load4(pan + t * PS + ppos(4 * Y), py);
 #pragma unroll
                         for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -537,7 +551,7 @@ static size_t blk_smem(int mb, int* Wn_out)
     const int NTR = Wn / 4, NTT = NTR * (NTR + 1) / 2;
     size_t s = (size_t)NTT * TSTRIDE * sizeof(T) + (size_t)PB * (mb + 1) * sizeof(T) + (size_t)PB * PB * sizeof(T) +
                (size_t)Wn * sizeof(T) + 2 * PB * sizeof(T) + (size_t)Wn * 8 + PB * 8 + (size_t)NTT * 2 + Wn + 64 +
-               (size_t)PB * Wn * sizeof(T) + 16;
+               (size_t)PB * (Wn + Wn / 4) * sizeof(T) + 16;
     *Wn_out = Wn;
     return s;
 }
