@@ -28,9 +28,9 @@
 //      rest of the trailing window by the rank-PB product L_x L_y^T (each
 //      thread accumulating 4 x 4 tiles in registers, the panel columns read
 //      from the panel buffer), while the next PB prepared rows arrive in a
-//      staging buffer by cp.async; once all of them are through (a barrier
-//      of warps 1.. only), they write the staged rows into the slots the
-//      panel freed.
+//      staging buffer by one bulk copy (cp.async.bulk with an mbarrier);
+//      once all of them are through (a barrier of warps 1.. only), they
+//      write the staged rows into the slots the panel freed.
 // The first diagonal block is factored before the loop, so the serial
 // block factorisation overlaps the trailing update of the previous panel.
 #include "crt_band.h"
@@ -233,14 +233,50 @@ __device__ __forceinline__ void load4<cf>(const cf* p, cf (&v)[4])
     v[3] = cf{w.z, w.w};
 }
 
+// mbarrier and bulk-copy helpers for the staged rows (one CTA, no cluster
+// multicast).  The wait gives up after a bounded number of polls and
+// reports failure instead of spinning for ever.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, int count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, int bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, int bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, int phase)
+{
+    const unsigned a = smem_u32(bar);
+    for (int it = 0; it < (1 << 22); ++it) {
+        unsigned ok;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 // Panel buffer padding (see the kernel): complex64 reads four entries with
 // two 16-byte loads and keeps the rows unpadded (16-byte aligned).
 template <typename T> struct PanPad { static constexpr bool v = true; };
 template <> struct PanPad<cf> { static constexpr bool v = false; };
 
-// Staged rows copied with 16-byte cp.async: complex entries (8 or 16
-// bytes, and the complex64 column stride is even), so every row run starts
-// on a 16-byte boundary; real FP64 rows may not.
+// Staged rows copied by one bulk copy (16-byte aligned, a multiple of 16
+// bytes): complex entries (8 or 16 bytes, and the complex64 column stride is
+// even), so every row run starts on a 16-byte boundary; real FP64 rows may
+// not.
 template <typename T> struct StageAsync { static constexpr bool v = true; };
 template <> struct StageAsync<double> { static constexpr bool v = false; };
 
@@ -272,6 +308,7 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
     __shared__ T colb[32];                                                // column broadcast of the block factor
     __shared__ T bN[PB];                                                  // scaled right-hand side of the staged rows
     __shared__ int s_err;
+    __shared__ __align__(8) unsigned long long s_bar;   // mbarrier of the staged rows' bulk copy
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x, sys = A.sys0 + b;
@@ -297,7 +334,11 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
         while (tile_base(X, 0) > t) --X;
         tXY[t] = (unsigned short)((X << 8) | (t - tile_base(X, 0)));
     }
-    if (tid == 0) s_err = 0;
+    if (tid == 0) {
+        s_err = 0;
+        mbar_init(&s_bar, 1);
+    }
+    int bar_phase = 0;
     __syncthreads();
 
     // Prepared rows [r0, r0 + PB) into stage[q][d] and their scaling factors
@@ -410,6 +451,8 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
     constexpr int NPT = PB / 4;
 
     if (warp == 0) diag_block(0);
+    // the staging buffer's next writer is the async (bulk copy) proxy
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     for (int i0 = 0; i0 < n; i0 += PB) {
         if (s_err) break;
@@ -486,15 +529,16 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             if (has_next) diag_block(inext);
         } else {
             // the next PB prepared rows start their way into the staging
-            // buffer (cp.async) and arrive while the tiles are updated
+            // buffer (bulk copy) and arrive while the tiles are updated
             const char* srcb = reinterpret_cast<const char*>(Lc + (size_t)rnew0 * W1);
             char* dstb = reinterpret_cast<char*>(stage);
             const int bytes = PB * W1 * (int)sizeof(T);
             const bool async_rows = StageAsync<T>::v && rnew0 + PB <= n && (reinterpret_cast<size_t>(srcb) & 15) == 0 &&
                                     (reinterpret_cast<size_t>(dstb) & 15) == 0 && (bytes & 15) == 0;
-            if (async_rows) {
-                for (int off = (tid - 32) * 16; off < bytes; off += (NT - 32) * 16) cp_async16(dstb + off, srcb + off);
-                cp_async_commit();
+            if (async_rows && tid == 32) {
+                // one bulk copy (the TMA engine) of the PB contiguous rows
+                mbar_expect_tx(&s_bar, bytes);
+                bulk_g2s(dstb, srcb, bytes, &s_bar);
             }
             if (has_next) {
                 for (int tt = tid - 32; tt < NTT; tt += NT - 32) {
@@ -524,7 +568,8 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
                 }
             }
             if (async_rows) {
-                cp_async_wait_all();
+                if (!mbar_wait(&s_bar, bar_phase)) s_err = CRT_ERR_CUDA;
+                bar_phase ^= 1;
                 row_meta(rnew0, 32);
             } else {
                 load_rows(rnew0, 32);
@@ -534,6 +579,8 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             // slots take the new rows
             asm volatile("bar.sync 1, %0;\n" ::"r"(NT - 32) : "memory");
             scatter_rows(rnew0, s0, i0 + PB, 32);
+            // the staging buffer's next writer is the async (bulk copy) proxy
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         }
         __syncthreads();
         // PROBE2
