@@ -255,7 +255,8 @@ template <typename T> struct SolveOcc { static constexpr int v = 2; };
 template <> struct SolveOcc<cf> { static constexpr int v = 3; };
 // complex64 solves stage the next block of 32 columns of the factor (one
 // contiguous run: the factor is column-packed with an even column stride)
-// in a shared double buffer while the current block is solved
+// in a shared double buffer, by one bulk copy, while the current block is
+// solved
 template <typename T> struct SolvePrefetch { static constexpr bool v = false; };
 template <> struct SolvePrefetch<cf> { static constexpr bool v = true; };
 
@@ -280,13 +281,25 @@ __global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> 
     const T* Lc = A.Lws + (size_t)slot * A.lstride;
     const double* fk = A.fakws + (size_t)slot * n;
     T* z = scratch + (size_t)b * n;
-    // columns [c0, c0 + nb) of the factor into buffer `buf` (async)
+    // columns [c0, c0 + nb) of the factor into buffer `buf` by one bulk
+    // copy (TMA engine) completing on the buffer's mbarrier; pf_wait(buf)
+    // returns once it has landed (bounded: a timeout marks the system)
+    __shared__ __align__(8) unsigned long long pbar[2];
+    int pphase[2] = {0, 0};
+    if (PF && tid == 0) {
+        mbar_init(&pbar[0], 1);
+        mbar_init(&pbar[1], 1);
+    }
     auto prefetch = [&](int c0, int nb, int buf) {
-        const char* src = reinterpret_cast<const char*>(Lc + (size_t)c0 * W);
-        char* dst = reinterpret_cast<char*>(lbuf + (size_t)buf * BB * W);
-        const int bytes = nb * W * (int)sizeof(T);
-        for (int off = tid * 16; off < bytes; off += NT * 16) cp_async16(dst + off, src + off);
-        cp_async_commit();
+        if (tid == 0) {
+            const int bytes = nb * W * (int)sizeof(T);
+            mbar_expect_tx(&pbar[buf], bytes);
+            bulk_g2s(lbuf + (size_t)buf * BB * W, Lc + (size_t)c0 * W, bytes, &pbar[buf]);
+        }
+    };
+    auto pf_wait = [&](int buf) {
+        if (!mbar_wait(&pbar[buf], pphase[buf])) A.status[sys] = CRT_ERR_CUDA;
+        pphase[buf] ^= 1;
     };
 
     // The fused forward pass belongs to the system's own right-hand side:
@@ -320,7 +333,7 @@ __global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> 
         // (coalesced over the rows of a column).
         if constexpr (PF) {
             prefetch(0, min(n, BB), 0);
-            cp_async_wait_all();
+            pf_wait(0);
             __syncthreads();
         }
         int fbuf = 0;
@@ -369,7 +382,11 @@ __global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> 
                 }
                 z[r] -= acc;
             }
-            if constexpr (PF) cp_async_wait_all();
+            if constexpr (PF) {
+                if (c1 < n) pf_wait(fbuf ^ 1);
+                // the buffer just read is the next bulk copy's destination
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            }
             __syncthreads();
             fbuf ^= 1;
         }
@@ -388,8 +405,10 @@ __global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> 
     T(*trw)[BB + 1] = reinterpret_cast<T(*)[BB + 1]>(trbuf);   // trw[r][c] = L(c0 + r, c0 + c), r >= c
     const int col = tid / TPC, sub = tid % TPC;
     if constexpr (PF) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
         prefetch(max(0, n - BB), n - max(0, n - BB), 0);
-        cp_async_wait_all();
+        pf_wait(0);
         __syncthreads();
     }
     int bbuf = 0;
@@ -429,7 +448,10 @@ __global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> 
             }
             if (lane < nb) z[c0 + lane] = v;
         }
-        if constexpr (PF) cp_async_wait_all();
+        if constexpr (PF) {
+            if (c0 > 0) pf_wait(bbuf ^ 1);
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        }
         __syncthreads();
         bbuf ^= 1;
     }

@@ -233,41 +233,6 @@ __device__ __forceinline__ void load4<cf>(const cf* p, cf (&v)[4])
     v[3] = cf{w.z, w.w};
 }
 
-// mbarrier and bulk-copy helpers for the staged rows (one CTA, no cluster
-// multicast).  The wait gives up after a bounded number of polls and
-// reports failure instead of spinning for ever.
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, int count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, int bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, int bytes, unsigned long long* bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, int phase)
-{
-    const unsigned a = smem_u32(bar);
-    for (int it = 0; it < (1 << 22); ++it) {
-        unsigned ok;
-        asm volatile(
-            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(a), "r"(phase)
-            : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-
 // Panel buffer padding (see the kernel): complex64 reads four entries with
 // two 16-byte loads and keeps the rows unpadded (16-byte aligned).
 template <typename T> struct PanPad { static constexpr bool v = true; };
