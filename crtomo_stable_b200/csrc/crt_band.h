@@ -51,9 +51,11 @@ struct SolveArgs {
 template <typename T> void launch_band_factor(const BandArgs<T>& a, cudaStream_t st);
 // Launch configuration of the panel-blocked variant: the panel width (4, 8
 // or 16) in the low bits, BAND_CFG_WIDE for one 512-thread CTA per SM where
-// the window would also fit twice (two 256-thread CTAs otherwise).
+// the window would also fit twice (two 256-thread CTAs otherwise),
+// BAND_CFG_NARROW for four 128-thread CTAs per SM where it fits four times.
 constexpr int BAND_PANEL_MASK = 0xff;
 constexpr int BAND_CFG_WIDE = 0x100;
+constexpr int BAND_CFG_NARROW = 0x200;
 // Panel-blocked variant in configuration cfg; returns false when its window
 // does not fit in shared memory.
 template <typename T> bool launch_band_factor_blk(const BandArgs<T>& a, int cfg, cudaStream_t st);

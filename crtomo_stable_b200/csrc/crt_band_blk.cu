@@ -600,39 +600,54 @@ void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
     k_band_prep_rows<T><<<(unsigned)((rows * PREP_G + 255) / 256), 256, 0, st>>>(a);
 }
 
+// Threads per CTA of a launch configuration for a window of smem bytes: a
+// window that fits twice per SM runs as two 256-thread CTAs (one system's
+// serial phases overlap the other's update), a small one may run as four
+// 128-thread CTAs (BAND_CFG_NARROW), a large one (or BAND_CFG_WIDE) as one
+// CTA of 512.  0: the configuration does not fit.
+static int cfg_threads(int cfg, size_t smem)
+{
+    constexpr size_t lim = 227 * 1024;
+    if (cfg & BAND_CFG_NARROW) return 4 * smem <= lim ? 128 : 0;
+    if (!(cfg & BAND_CFG_WIDE) && 2 * smem <= lim) return 256;
+    return smem <= lim ? 512 : 0;
+}
+
 template <typename T, int PB>
-static void launch_blk_pb(const BandArgs<T>& a, bool one_wide, cudaStream_t st)
+static void launch_blk_pb(const BandArgs<T>& a, int cfg, cudaStream_t st)
 {
     int Wn = 0;
     const size_t smem = blk_smem<T, PB>(a.mb, &Wn);
-    // a window that fits twice (complex64, or real FP64) may run as two
-    // 256-thread CTAs per SM, overlapping one system's serial phases with the
-    // other's update; otherwise (or when asked) one CTA of 512 per SM
     auto go = [&](auto kern, int nt) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<a.nsys, nt, smem, st>>>(a, Wn);
     };
-    if (2 * smem <= 227 * 1024 && !one_wide) go(k_band_factor_blk<T, PB, 256, 2>, 256);
-    else go(k_band_factor_blk<T, PB, 512, 1>, 512);
+    switch (cfg_threads(cfg, smem)) {
+    case 128: go(k_band_factor_blk<T, PB, 128, 4>, 128); break;
+    case 256: go(k_band_factor_blk<T, PB, 256, 2>, 256); break;
+    default: go(k_band_factor_blk<T, PB, 512, 1>, 512); break;
+    }
 }
 
 template <typename T>
 bool launch_band_factor_blk(const BandArgs<T>& a, int cfg, cudaStream_t st)
 {
     const int pb = cfg & BAND_PANEL_MASK;
-    const bool wide = (cfg & BAND_CFG_WIDE) != 0;
     if (!blk_fits_pb<T>(pb, a.mb)) return false;
+    int Wn = 0;
+    if (cfg_threads(cfg, blk_smem_pb<T>(pb, a.mb, &Wn)) == 0) cfg = pb;
     switch (pb) {
-    case 4: launch_blk_pb<T, 4>(a, wide, st); break;
-    case 16: launch_blk_pb<T, 16>(a, wide, st); break;
-    default: launch_blk_pb<T, 8>(a, wide, st); break;
+    case 4: launch_blk_pb<T, 4>(a, cfg, st); break;
+    case 16: launch_blk_pb<T, 16>(a, cfg, st); break;
+    default: launch_blk_pb<T, 8>(a, cfg, st); break;
     }
     return true;
 }
 
 // ---------------------------------------------------------------------------
 // Panel-width autotuner.  The best panel (4, 8 or 16 columns) and CTA shape
-// (two 256-thread CTAs per SM where the window fits twice, or one of 512)
+// (two 256-thread CTAs per SM where the window fits twice, four of 128 where
+// it fits four times, or one of 512)
 // depend on the element type and the half-bandwidth (window size, CTAs per
 // SM, serial panel phases against the rank-PB update); they are measured once per
 // (type, mb) in the process on the first systems of a real chunk: for each
@@ -640,8 +655,9 @@ bool launch_band_factor_blk(const BandArgs<T>& a, int cfg, cudaStream_t st)
 // two waves of systems are run and the factorisation is timed with events.
 // The caller's real pass then prepares and factors the chunk again, so the
 // trials leave no trace but their per-system status, which is cleared.
-// CRT_B200_PANEL = 4 | 8 | 16 fixes the width; CRT_B200_TUNE_LOG prints the
-// trials to stderr.
+// CRT_B200_PANEL = 4 | 8 | 16 fixes the width (with CRT_B200_FACTOR_CTA =
+// 128 | 256 | 512 the CTA shape where the window allows it);
+// CRT_B200_TUNE_LOG prints the trials to stderr.
 namespace {
 std::mutex g_panel_mu;
 std::map<std::pair<int, int>, int> g_panel;   // (sizeof(T), mb) -> launch configuration
@@ -652,7 +668,14 @@ int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st)
 {
     if (const char* env = std::getenv("CRT_B200_PANEL")) {
         const int pb = std::atoi(env);
-        if ((pb == 4 || pb == 8 || pb == 16) && blk_fits_pb<T>(pb, a.mb)) return pb;
+        if ((pb == 4 || pb == 8 || pb == 16) && blk_fits_pb<T>(pb, a.mb)) {
+            int cfg = pb;
+            if (const char* ce = std::getenv("CRT_B200_FACTOR_CTA")) {
+                const int nt = std::atoi(ce);
+                cfg |= nt == 128 ? BAND_CFG_NARROW : nt == 512 ? BAND_CFG_WIDE : 0;
+            }
+            return cfg;
+        }
     }
     const std::pair<int, int> key((int)sizeof(T), a.mb);
     {
@@ -671,11 +694,14 @@ int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st)
     cudaEventCreate(&e1);
     int best = 8;
     float best_ms = 1e30f;
-    for (int cfg : {8, 4, 16, 8 | BAND_CFG_WIDE, 4 | BAND_CFG_WIDE}) {
+    for (int cfg : {8, 4, 16, 8 | BAND_CFG_WIDE, 4 | BAND_CFG_WIDE, 8 | BAND_CFG_NARROW, 4 | BAND_CFG_NARROW}) {
         const int pb = cfg & BAND_PANEL_MASK;
         if (!blk_fits_pb<T>(pb, a.mb)) continue;
         int Wn = 0;
-        if ((cfg & BAND_CFG_WIDE) && 2 * blk_smem_pb<T>(pb, a.mb, &Wn) > 227 * 1024) continue;   // same as pb alone
+        const size_t sm = blk_smem_pb<T>(pb, a.mb, &Wn);
+        const int nt = cfg_threads(cfg, sm);
+        if (nt == 0) continue;
+        if ((cfg & BAND_CFG_WIDE) && cfg_threads(pb, sm) == 512) continue;   // the same as pb alone
         launch_band_prep<T>(t, st);
         cudaEventRecord(e0, st);
         launch_band_factor_blk<T>(t, cfg, st);
@@ -683,11 +709,9 @@ int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st)
         if (cudaEventSynchronize(e1) != cudaSuccess) break;
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (std::getenv("CRT_B200_TUNE_LOG")) {
-            const bool twice = 2 * blk_smem_pb<T>(pb, a.mb, &Wn) <= 227 * 1024;
+        if (std::getenv("CRT_B200_TUNE_LOG"))
             std::fprintf(stderr, "band factor autotune: %d-byte entries, mb %d, panel %d, %d threads: %.3f ms\n",
-                         (int)sizeof(T), a.mb, pb, (twice && !(cfg & BAND_CFG_WIDE)) ? 256 : 512, ms);
-        }
+                         (int)sizeof(T), a.mb, pb, nt, ms);
         if (ms < best_ms) {
             best_ms = ms;
             best = cfg;

@@ -142,3 +142,23 @@ def test_autotuned_panel_is_a_candidate():
     ctx.forward(s.sigma)
     assert ctx.timings()["panel"] in (4, 8, 16)
     ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("cta", [128, 512])
+def test_factor_cta_shapes_match_oracle(cta, precision, monkeypatch):
+    """The CTA shapes the autotuner may choose besides two 256-thread CTAs per
+    SM (forced here): four of 128 threads for small windows, one of 512."""
+    from crtomo_stable_b200 import synth
+    from crtomo_stable_b200.lib import Context
+    from oracle.oracle import OracleProblem
+    s = synth.small_triangles(nx=30, nz=14)
+    monkeypatch.setenv("CRT_B200_PANEL", "8")
+    monkeypatch.setenv("CRT_B200_FACTOR_CTA", str(cta))
+    ctx = Context(s.mesh, s.enr, s.strnr, s.vnr, precision=precision)
+    _, _, kp = ctx.forward(s.sigma, want_kpot=True)
+    kp_o = OracleProblem(s.mesh, s.enr, s.strnr, s.vnr).forward(s.sigma)
+    tol = 1e-10 if precision == 0 else TOL_MIXED
+    assert np.abs(kp - kp_o).max() <= tol * np.abs(kp_o).max()
+    ctx.close()
