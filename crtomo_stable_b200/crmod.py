@@ -143,7 +143,7 @@ def main(argv=None):
     a = ap.parse_args(argv)
     exe = a.exe_dir
     if a.synthetic:
-        exe = write_synthetic_tomodir(a.synthetic, a.out or os.path.join("gpurun_out", "tomodir_" + a.synthetic))
+        exe = write_synthetic_tomodir(a.synthetic, a.out or ("tomodir_" + a.synthetic))
     if not exe:
         ap.error("EXE_DIR or --synthetic required")
     run(exe, device=a.device)

@@ -1,8 +1,8 @@
 """The learned correction of the CG preconditioner (crt_gnn_*): the CPU
 restatement's backward pass against finite differences, the device's loss
 and weight gradients against the restatement, deterministic training, and
-the learned form of the inner solve against the plain one, which stays the
-judge of the update."""
+the learned form of the inner solve against the plain one, whose update it
+must reproduce."""
 import os
 import sys
 
