@@ -261,7 +261,8 @@ template <typename T> struct SolvePrefetch { static constexpr bool v = false; };
 template <> struct SolvePrefetch<cf> { static constexpr bool v = true; };
 
 template <typename T, int NT, int BB>
-__global__ void __launch_bounds__(NT, SolveOcc<T>::v) k_band_solve(SolveArgs<T> A, T* scratch)
+__global__ void __launch_bounds__(NT, NT == 128 ? 2 * SolveOcc<T>::v : SolveOcc<T>::v)
+    k_band_solve(SolveArgs<T> A, T* scratch)
 {
     // the forward pass's triangle tri[c][d] and the backward pass's trw[r][c]
     // share one buffer (the passes are separated by a barrier)
@@ -490,15 +491,20 @@ void launch_band_factor(const BandArgs<T>& a, cudaStream_t st)
 template <typename T>
 void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st)
 {
-    constexpr int NT = 256, BB = 32;
+    constexpr int BB = 32;
     size_t dyn = 0;
-    if (SolvePrefetch<T>::v) {
-        dyn = 2 * (size_t)BB * a.W * sizeof(T);
-        cudaFuncSetAttribute(k_band_solve<T, NT, BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-        cudaFuncSetAttribute(k_band_solve<T, NT, BB>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
-    }
-    k_band_solve<T, NT, BB><<<a.nsys, NT, dyn, st>>>(a, scratch);
+    if (SolvePrefetch<T>::v) dyn = 2 * (size_t)BB * a.W * sizeof(T);
+    auto go = [&](auto kern, int nt) {
+        if (dyn) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+        }
+        kern<<<a.nsys, nt, dyn, st>>>(a, scratch);
+    };
+    // narrow bands: a column has few entries, so half the threads per CTA
+    // and twice the CTAs per SM hide more of the per-block latency
+    if (a.W <= 80) go(k_band_solve<T, 128, BB>, 128);
+    else go(k_band_solve<T, 256, BB>, 256);
 }
 
 template size_t band_factor_smem<double>(int);
