@@ -133,10 +133,11 @@ __global__ void __launch_bounds__(NT) k_sens(SensArgs A)
 // of the reciprocity sum of src/bsensi.f90:98-186 (the reference forms the
 // potential differences first; the two orders agree to FP64 rounding of
 // the products).  G is accumulated as a rank-(K nk) product: one thread per
-// 8 x 4 tile of its lower triangle, operands staged per chunk of
+// 4 x 4 tile of its lower triangle (small tiles: many warps per element),
+// operands staged per chunk of
 // wavenumbers (Phi_k and w_k E_k Phi_k), then written to shared memory for
 // the readings' gathers.
-constexpr int GR_TA = 8, GR_TB = 4;
+constexpr int GR_TA = 4, GR_TB = 4;
 
 __device__ __forceinline__ int gram_idx(int a, int b)
 {
@@ -156,12 +157,12 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
     const int e = blockIdx.x;
     const int nk = A.enk[e];
     const int L = A.L, K = A.K;
-    const int RB = LP / GR_TA, ntile = RB * (RB + 1);
+    const int RB = LP / GR_TA, ntile = RB * (RB + 1) / 2;
     const int tid = threadIdx.x;
-    // tile of this thread: row block R, column block Cb <= 2R+1
+    // tile of this thread: row block R, column block Cb <= R
     int R = 0;
-    while ((R + 1) * (R + 2) <= tid) ++R;
-    const int Cb = tid - R * (R + 1);
+    while ((R + 1) * (R + 2) / 2 <= tid) ++R;
+    const int Cb = tid - R * (R + 1) / 2;
     const bool has_tile = tid < ntile;
     T acc[GR_TA][GR_TB];
 #pragma unroll
@@ -264,8 +265,8 @@ bool sens_gram_plan(int L, int K, int nkmax, bool real, int* LP_out, int* kc_out
 {
     const size_t tsz = real ? sizeof(double) : sizeof(cd);
     const int LP = (L + GR_TA - 1) / GR_TA * GR_TA;
-    const int RB = LP / GR_TA, ntile = RB * (RB + 1);
-    if (nkmax > 4 || ntile > 512) return false;
+    const int RB = LP / GR_TA, ntile = RB * (RB + 1) / 2;
+    if (nkmax > 4 || ntile > 1024) return false;
     const size_t gbytes = (size_t)LP * (LP + 1) / 2 * tsz;
     const size_t limit = 200 * 1024;
     if (gbytes > limit) return false;
@@ -280,17 +281,19 @@ bool sens_gram_plan(int L, int K, int nkmax, bool real, int* LP_out, int* kc_out
 
 void launch_sens_gram(const SensArgs& a, int LP, int kc, size_t smem, int nt, bool real, cudaStream_t st)
 {
-    // up to 320 threads (LP <= 128) the tile's accumulators stay in registers
+    // one thread per tile: 320 threads up to 76 electrodes, 576 up to 132
     auto go = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<a.E, nt, smem, st>>>(a, LP, kc);
     };
     if (real) {
         if (nt <= 320) go(k_sens_gram<double, 320>);
-        else go(k_sens_gram<double, 512>);
+        else if (nt <= 576) go(k_sens_gram<double, 576>);
+        else go(k_sens_gram<double, 1024>);
     } else {
         if (nt <= 320) go(k_sens_gram<cd, 320>);
-        else go(k_sens_gram<cd, 512>);
+        else if (nt <= 576) go(k_sens_gram<cd, 576>);
+        else go(k_sens_gram<cd, 1024>);
     }
 }
 
