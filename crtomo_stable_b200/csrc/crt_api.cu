@@ -105,6 +105,17 @@ struct crt_ctx {
     int capture = 0;
     size_t ws_budget = 0;   // factor workspace budget in bytes (0: default)
     int panel = 0;          // panel width of the last blocked factorisation
+    // timing events of the forward, read after the forward's one host
+    // synchronisation (the status read) instead of one wait per phase
+    std::vector<cudaEvent_t> tev;
+    int tev_n = 0;
+    struct FwdMark {
+        int e0, e8, e1, e2;            // chunk start, after preparation, after factor, end
+        bool blk;
+        std::vector<int> ref;          // per refinement step: residual start, solve start, end
+    };
+    std::vector<FwdMark> fwd_marks;
+    int vol_e0 = -1, vol_e1 = -1;
 };
 
 namespace {
@@ -187,6 +198,25 @@ float ev_ms(crt_ctx* ctx, int a, int b)
 {
     float ms = 0.0f;
     if (!ctx->capture) cudaEventElapsedTime(&ms, ctx->ev[a], ctx->ev[b]);
+    return ms;
+}
+
+// A pooled timing event recorded on the context stream (-1 while capturing).
+int tev_rec(crt_ctx* ctx)
+{
+    if (ctx->capture) return -1;
+    if (ctx->tev_n == (int)ctx->tev.size()) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return -1;
+        ctx->tev.push_back(e);
+    }
+    if (cudaEventRecord(ctx->tev[ctx->tev_n], ctx->st) != cudaSuccess) return -1;
+    return ctx->tev_n++;
+}
+float tev_ms(crt_ctx* ctx, int a, int b)
+{
+    float ms = 0.0f;
+    if (a >= 0 && b >= 0) cudaEventElapsedTime(&ms, ctx->tev[a], ctx->tev[b]);
     return ms;
 }
 
@@ -305,6 +335,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
     gnn_free(ctx->gnn);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->tev) cudaEventDestroy(e);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
 }
@@ -600,7 +631,8 @@ int run_forward(crt_ctx* ctx)
         ctx->chunk = chunk;
     }
     chunk = ctx->chunk;
-    float ms_f = 0, ms_s = 0, ms_prep = 0, ms_fk = 0, ms_res = 0, ms_cor = 0;
+    ctx->tev_n = 0;
+    ctx->fwd_marks.clear();
     int nfl = 0;
     bool blk = false;
     for (int s0 = 0; s0 < nfac; s0 += chunk) {
@@ -648,7 +680,8 @@ int run_forward(crt_ctx* ctx)
             }
             A.aval = ctx->d_aval;
         }
-        if (!ev_rec(ctx, 0)) return CRT_ERR_CUDA;
+        crt_ctx::FwdMark mk{};
+        mk.e0 = tev_rec(ctx);
         {
             const char* fv = std::getenv("CRT_B200_FACTOR");
             const bool force_v0 = fv && std::strcmp(fv, "v0") == 0;
@@ -656,7 +689,7 @@ int run_forward(crt_ctx* ctx)
                 const int pb = band_panel<T>(A, !ctx->capture, ctx->st);
                 ctx->panel = pb & BAND_PANEL_MASK;
                 launch_band_prep<T>(A, ctx->st);
-                if (!ev_rec(ctx, 8)) return CRT_ERR_CUDA;
+                mk.e8 = tev_rec(ctx);
                 launch_band_factor_blk<T>(A, pb, ctx->st);
                 ctx->launches += 3;
                 blk = true;
@@ -666,14 +699,15 @@ int run_forward(crt_ctx* ctx)
                 } else {
                     launch_band_factor<T>(A, ctx->st);
                 }
-                if (!ev_rec(ctx, 8)) return CRT_ERR_CUDA;
+                mk.e8 = tev_rec(ctx);
                 ctx->launches++;
                 blk = false;
             }
             ++nfl;
         }
         if (int e = kernel_check(ctx, "band factor")) return e;
-        if (!ev_rec(ctx, 1)) return CRT_ERR_CUDA;
+        mk.e1 = tev_rec(ctx);
+        mk.blk = blk;
         SolveArgs<T> S{};
         S.n = n;
         S.mb = ctx->mb;
@@ -705,45 +739,50 @@ int run_forward(crt_ctx* ctx)
             // iterative refinement of the complex64 solution: FP64 residual of
             // the scaled system, complex64 correction solve, FP64 update of kpot
             for (int it = 0; it < ctx->nref; ++it) {
-                if (!ev_rec(ctx, 4)) return CRT_ERR_CUDA;
+                mk.ref.push_back(tev_rec(ctx));
                 launch_band_residual<T>(A, S.sys0, S.nsys, S.factor_of_sys_div, ctx->d_up_ptr, ctx->d_up_ent,
                                         ctx->d_up_row, ctx->d_kpot, scr, ctx->st);
-                if (!ev_rec(ctx, 5)) return CRT_ERR_CUDA;
+                mk.ref.push_back(tev_rec(ctx));
                 SolveArgs<T> C = S;
                 C.rhs = scr;
                 C.accumulate = 1;
                 launch_band_solve_with_scratch<T>(C, scr, ctx->st);
-                if (!ev_rec(ctx, 9)) return CRT_ERR_CUDA;
-                if (!ev_sync(ctx, 9)) return CRT_ERR_CUDA;
-                float t1 = 0, t2 = 0;
-                t1 = ev_ms(ctx, 4, 5);
-                t2 = ev_ms(ctx, 5, 9);
-                ms_res += t1;
-                ms_cor += t2;
+                mk.ref.push_back(tev_rec(ctx));
                 ctx->launches += 2;
             }
         }
         if (int e = kernel_check(ctx, "band solve")) return e;
-        if (!ev_rec(ctx, 2)) return CRT_ERR_CUDA;
-        if (!ev_sync(ctx, 2)) return CRT_ERR_CUDA;
-        float a = 0, b = 0, c = 0;
-        a = ev_ms(ctx, 0, 1);
-        b = ev_ms(ctx, 1, 2);
-        c = ev_ms(ctx, 0, 8);
+        mk.e2 = tev_rec(ctx);
+        ctx->fwd_marks.push_back(mk);
+    }
+    ctx->timings[9] = nfl;
+    ctx->timings[12] = blk ? ctx->panel : 0;
+    return CRT_OK;   // per-system status and phase times: read by forward_common
+}
+
+// Phase times of the last forward from its pooled events (after a host
+// synchronisation that covers them).
+void resolve_forward_timings(crt_ctx* ctx)
+{
+    float ms_f = 0, ms_s = 0, ms_prep = 0, ms_fk = 0, ms_res = 0, ms_cor = 0;
+    for (const crt_ctx::FwdMark& m : ctx->fwd_marks) {
+        const float a = tev_ms(ctx, m.e0, m.e1), b = tev_ms(ctx, m.e1, m.e2), c = tev_ms(ctx, m.e0, m.e8);
         ms_f += a;
         ms_s += b;
-        if (blk) ms_prep += c;
-        ms_fk += blk ? a - c : a;
+        if (m.blk) ms_prep += c;
+        ms_fk += m.blk ? a - c : a;
+        for (size_t i = 0; i + 2 < m.ref.size(); i += 3) {
+            ms_res += tev_ms(ctx, m.ref[i], m.ref[i + 1]);
+            ms_cor += tev_ms(ctx, m.ref[i + 1], m.ref[i + 2]);
+        }
     }
     ctx->timings[0] = ms_f;
     ctx->timings[1] = ms_s;
+    ctx->timings[2] = tev_ms(ctx, ctx->vol_e0, ctx->vol_e1);
     ctx->timings[7] = ms_prep;
     ctx->timings[8] = ms_fk;
-    ctx->timings[9] = nfl;
     ctx->timings[10] = ms_res;
     ctx->timings[11] = ms_cor;
-    ctx->timings[12] = blk ? ctx->panel : 0;
-    return collect_status(ctx, nfac);
 }
 
 int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
@@ -785,17 +824,16 @@ int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
     V.volt = ctx->d_volt;
     V.sigmaa = ctx->d_sigmaa;
     V.status = ctx->d_status + ctx->nstatus - 1;
-    if (!ev_rec(ctx, 3)) return CRT_ERR_CUDA;
+    ctx->vol_e0 = tev_rec(ctx);
     launch_voltages(V, ctx->st);
     ctx->launches += 2;
-    if (!ev_rec(ctx, 4)) return CRT_ERR_CUDA;
+    ctx->vol_e1 = tev_rec(ctx);
     if (int k = kernel_check(ctx, "voltages")) return k;
-    if (!ev_sync(ctx, 4)) return CRT_ERR_CUDA;
-    float ms = 0;
-    ms = ev_ms(ctx, 3, 4);
-    ctx->timings[2] = ms;
-    if (d_kfak) cudaFree(d_kfak);
+    // the forward's one host synchronisation: per-system status of the
+    // factorisations and voltages, then the phase times
     int st = collect_status(ctx, ctx->nstatus);
+    if (d_kfak) cudaFree(d_kfak);
+    if (!ctx->capture) resolve_forward_timings(ctx);
     if (st) return st;
     ctx->last_ldc = ldc;
     ctx->have_forward = 1;

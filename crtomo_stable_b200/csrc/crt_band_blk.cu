@@ -438,7 +438,19 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             }
             T lx[PB];
 #pragma unroll
-            for (int t = 0; t < PB; ++t) lx[t] = (t < np_) ? win[widx(x, s0 + t)] : Sc<T>::zero();
+            for (int p = 0; p < NPT; ++p) {
+                // the row's entries of panel tile row P0 + p: tile (X, P) after the
+                // panel in slot order (entry (x & 3, t & 3)), (P, X) before it
+                const int X = x >> 2, P = P0 + p;
+                const int base = (X > P ? tile_base(X, P) * TSTRIDE + ((x & 3) << 2)
+                                        : tile_base(P, X) * TSTRIDE + (x & 3));
+                const int step = X > P ? 1 : 4;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int t = 4 * p + u;
+                    lx[t] = (t < np_) ? win[base + u * step] : Sc<T>::zero();
+                }
+            }
             T bx = fuse ? bsl[x] : Sc<T>::zero();
 #pragma unroll
             for (int t = 0; t < PB; ++t) {
