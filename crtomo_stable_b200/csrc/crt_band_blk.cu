@@ -39,6 +39,7 @@
 #include <cstdlib>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 
 namespace {
@@ -158,8 +159,18 @@ __global__ void k_band_prep_rows(BandArgs<T> A)
     const bool active = gid < (long long)A.nsys * n;
     const int b = active ? (int)(gid / n) : 0, r = active ? (int)(gid % n) : 0, sys = A.sys0 + b;
     T* row = A.Lws + (size_t)b * A.lstride + (size_t)r * A.W;
-    if (active)
-        for (int d = 1 + lane; d <= A.mb; d += PREP_G) row[d] = Sc<T>::zero();
+    if (active) {
+        if constexpr (std::is_same<T, cf>::value) {
+            // complex64 rows start on 16-byte boundaries (even column stride):
+            // entry 1 alone, then pairs (2m, 2m+1) by 16-byte stores; the last
+            // pair may touch entry mb + 1, the row's padding
+            if (lane == 0) row[1] = Sc<T>::zero();
+            float4* pairs = reinterpret_cast<float4*>(row);
+            for (int m = 1 + lane; 2 * m <= A.mb; m += PREP_G) pairs[m] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
+            for (int d = 1 + lane; d <= A.mb; d += PREP_G) row[d] = Sc<T>::zero();
+        }
+    }
     __syncwarp();
     if (!active) return;
     int k, l;
