@@ -67,6 +67,9 @@ def parse():
                     help="'mixed' skips the plain FP64 comparison run (profiling)")
     ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--count", type=int, default=256, help="instances of the batched configuration C4")
+    ap.add_argument("--lambdas", type=int, default=4,
+                    help="lambda candidates of the batched Jacobi-form update measured after the step (0: skip)")
+    ap.add_argument("--lambda-iters", type=int, default=100, help="CG iterations of that measurement")
     return ap.parse_args()
 
 
@@ -321,6 +324,32 @@ def run_batch(args, ws, rank, local, pg):
         print(json.dumps(line), flush=True)
 
 
+def lambda_batch(ctx, Context, lam, par0, nlam, iters, E, N):
+    """Lambda trials side by side: `nlam` Jacobi-form updates (the
+    reference's cjggra) for lambdas spread over two decades around `lam`,
+    on the step's complex64 Jacobian, each run for exactly `iters` CG
+    iterations (eps = 0), through crt_update_lambdas against the same
+    updates one crt_update at a time.  Times are the library's CUDA-event
+    phases (cg set-up + iterations), host copies excluded."""
+    lams = lam * np.logspace(-1.0, 1.0, nlam)
+    prm = Context.params(lam, eps=0.0, ncgmax=iters)
+    ctx.update_lambdas(prm, lams, par0)                      # warm-up
+    got = ctx.update_lambdas(prm, lams, par0)
+    t = ctx.timings()
+    t_batch, t_iter = t["cg_setup"] + t["cg_iter"], t["cg_iter"]
+    t_seq = 0.0
+    for lm in lams:
+        ctx.update(Context.params(lm, eps=0.0, ncgmax=iters), par0)
+        t = ctx.timings()
+        t_seq += t["cg_setup"] + t["cg_iter"]
+    bytes_it = 2.0 * N * E * 8 + nlam * (6.0 * E * 16 + 3.0 * N * 16)   # J (complex64) twice + vectors
+    ach = bytes_it * iters / (t_iter / 1e3) / 1e9
+    return {"candidates": nlam, "iterations": iters, "ncg": [int(x) for x in got["ncg"]],
+            "batched_ms": t_batch, "sequential_ms": t_seq, "speedup": t_seq / t_batch if t_batch > 0 else None,
+            "batched_iteration_ms": t_iter / iters, "achieved_gbs": ach,
+            "form": "Jacobi (cgfac) CG per candidate, complex64 J read once per iteration for all candidates"}
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_init(args)
@@ -382,9 +411,12 @@ def main():
         t_e2e = max_over_ranks(pg, local, float(np.mean(e2e_ms)) / 1e3) if e2e_ms else None
         K = ctx.kwn.size
         form, blk, bw = ctx.cg_info()
+        lam_batch = None
+        if precision == PREC_MIXED and args.lambdas > 0:
+            lam_batch = lambda_batch(ctx, Context, lam, par0, args.lambdas, args.lambda_iters, E, N)
         ctx.close()
         return dict(t=t_step, phase=phase, ncg=ncg, launches=int(launches), clocks=clocks, e2e=t_e2e, lam=lam, K=K,
-                    cg_form=form, cg_block=blk, cg_bw=bw, c64=precision == PREC_MIXED)
+                    cg_form=form, cg_block=blk, cg_bw=bw, c64=precision == PREC_MIXED, lam_batch=lam_batch)
 
     mixed = run_form(PREC_MIXED, args.steps, args.warmup, args.steps, True)
     plain = None
@@ -461,7 +493,8 @@ def main():
                 {"value": plain["t"], "unit": "s", "cg_iterations": plain["ncg"],
                  "phases_ms": dict(zip(tnames, [float(x) for x in plain["phase"]]))},
                 "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "roofline": roof, "roofline_cg": roof_cg, "cpu_baseline": cpu, "clocks": mixed["clocks"],
+                "roofline": roof, "roofline_cg": roof_cg, "lambda_batch": mixed["lam_batch"],
+                "cpu_baseline": cpu, "clocks": mixed["clocks"],
                 "gpu_launches": mixed["launches"]}
         print(json.dumps(line), flush=True)
     if pg is not None:

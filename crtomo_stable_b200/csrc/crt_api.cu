@@ -95,6 +95,10 @@ struct crt_ctx {
     std::string spc_why;
     cd *d_z = nullptr, *d_rold = nullptr, *d_zb = nullptr;
     CGState* d_live = nullptr;   // a never-done CG state for preconditioner applications outside the CG
+    // lambda candidates side by side (crt_update_lambdas): one slab for all
+    // candidates' vectors, grown on demand
+    unsigned char* d_cgl = nullptr;
+    size_t cgl_bytes = 0;
     int cg_form = 0;      // form of the last CG: CRT_PRECOND_*
     // learned correction of the preconditioner
     Gnn gnn;
@@ -328,7 +332,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live};
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     spc_plan_free(ctx->spc);
@@ -1287,6 +1291,118 @@ extern "C" int32_t crt_update(crt_ctx* ctx, const crt_cg_params* prm, const doub
     if (bdpar) CK(cudaMemcpyAsync(bdpar, ctx->d_bdpar, sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     if (ncg) *ncg = n_cg;
+    return CRT_OK;
+}
+
+// Lambda candidates side by side: update.f90 + cjggra / cjggdc for every
+// lambda of a trial set on the same Jacobian, data, response and model.
+extern "C" int32_t crt_update_lambdas(crt_ctx* ctx, const crt_cg_params* prm, int32_t nlam, const double* lams,
+                                      const double* sigmaa, const double* par, double* par_out, double* dpar,
+                                      int32_t* ncg, double* bdpar)
+{
+    if (!ctx || !prm || !lams || !par || !par_out) return CRT_ERR_ARG;
+    if (nlam < 1 || nlam > CGL_MAX) return set_err(ctx, CRT_ERR_ARG, "nlam must be 1 .. 8");
+    for (int b = 0; b < nlam; ++b)
+        if (!(lams[b] >= 0.0) || !std::isfinite(lams[b]))
+            return set_err(ctx, CRT_ERR_ARG, "lambda candidates must be finite and non-negative");
+    if (prm->ncgmax < 0) return set_err(ctx, CRT_ERR_ARG, "ncgmax must be non-negative");
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->ltri < 0) return set_err(ctx, CRT_ERR_ARG, "regulariser not set (crt_set_regularizer)");
+    if (!ctx->d_dat) return set_err(ctx, CRT_ERR_ARG, "data not set (crt_set_data)");
+    if (!ctx->have_sens) return set_err(ctx, CRT_ERR_ARG, "no Jacobian (crt_jacobian / crt_set_jacobian)");
+    if (prm->ldc != ctx->sens_real) return set_err(ctx, CRT_ERR_ARG, "ldc does not match the Jacobian type");
+    if (!sigmaa && !ctx->have_forward) return set_err(ctx, CRT_ERR_ARG, "no forward response for crt_update_lambdas");
+    if (int e = ensure_cg_buffers(ctx, prm->ncgmax)) return e;
+    const size_t M = (size_t)ctx->E, N = (size_t)ctx->N, nl = (size_t)nlam, ns = (size_t)ctx->cg_nsplit;
+    const size_t ncr = (size_t)prm->ncgmax + 2;
+    // slab: cd vectors first (16-byte aligned), then doubles, then the states
+    const size_t n_cd = nl * (6 * M + N + ns * N) + N;   // rhs p r bvec dpar par_out, ap, part; sigmaa
+    const size_t n_d = nl * (M + ncr + 1);                // cgfac, cgres, bdpar
+    const size_t bytes = n_cd * sizeof(cd) + n_d * sizeof(double) + nl * sizeof(CGState);
+    if (ctx->cgl_bytes < bytes) {
+        if (ctx->d_cgl) cudaFree(ctx->d_cgl);
+        ctx->d_cgl = nullptr;
+        ctx->cgl_bytes = 0;
+        if (!dalloc(ctx, &ctx->d_cgl, bytes)) return CRT_ERR_ALLOC;
+        ctx->cgl_bytes = bytes;
+    }
+    cd* pc = reinterpret_cast<cd*>(ctx->d_cgl);
+    auto take_cd = [&](size_t n) { cd* q = pc; pc += n; return q; };
+    cd* v_rhs = take_cd(nl * M);
+    cd* v_p = take_cd(nl * M);
+    cd* v_r = take_cd(nl * M);
+    cd* v_bvec = take_cd(nl * M);
+    cd* v_dpar = take_cd(nl * M);
+    cd* v_par = take_cd(nl * M);
+    cd* v_ap = take_cd(nl * N);
+    cd* v_part = take_cd(nl * ns * N);
+    cd* v_sa = take_cd(N);
+    double* pd = reinterpret_cast<double*>(pc);
+    double* v_cgfac = pd;
+    double* v_cgres = v_cgfac + nl * M;
+    double* v_bdpar = v_cgres + nl * ncr;
+    CGState* v_st = reinterpret_cast<CGState*>(v_bdpar + nl);
+
+    CK(cudaMemcpyAsync(ctx->d_par, par, sizeof(cd) * M, cudaMemcpyHostToDevice, ctx->st));
+    const cd* d_sa = ctx->d_sigmaa;
+    if (sigmaa) {
+        CK(cudaMemcpyAsync(v_sa, sigmaa, sizeof(cd) * N, cudaMemcpyHostToDevice, ctx->st));
+        d_sa = v_sa;
+    }
+    crt_cg_params p1 = *prm;
+    p1.precond = CRT_PRECOND_JACOBI;
+    CGLArgs L{};
+    L.a = make_cg_args(ctx, &p1);
+    L.a.cgfac = v_cgfac;
+    L.a.rhs = v_rhs;
+    L.a.p = v_p;
+    L.a.r = v_r;
+    L.a.bvec = v_bvec;
+    L.a.dpar = v_dpar;
+    L.a.ap = v_ap;
+    L.a.part = v_part;
+    L.a.cgres = v_cgres;
+    L.a.st = v_st;
+    L.a.pc = 0;
+    L.nl = nlam;
+    for (int b = 0; b < nlam; ++b) L.lam[b] = lams[b];
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    launch_cgl_setup(L, ctx->d_dat, d_sa, ctx->d_par, ctx->st);
+    launch_cgl_init(L, ctx->st);
+    ctx->launches += 2;
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    if (int e = kernel_check(ctx, "lambda-batch cg setup")) return e;
+    std::vector<CGState> hs(nl);
+    int done_iters = 0;
+    const int batch = 16;
+    while (done_iters < prm->ncgmax) {
+        const int it = std::min(batch, prm->ncgmax - done_iters);
+        ctx->launches += launch_cgl_iterations(L, it, ctx->st);
+        done_iters += it;
+        CK(cudaMemcpyAsync(hs.data(), v_st, sizeof(CGState) * nl, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        bool all = true;
+        for (const CGState& h : hs) all = all && h.done;
+        if (all) break;
+    }
+    if (int e = kernel_check(ctx, "lambda-batch cg iterations")) return e;
+    launch_cgl_finish(L, prm->lfpi, prm->step, ctx->d_par, v_par, v_bdpar, ctx->st);
+    ctx->launches++;
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[2]));
+    float a1 = 0, a2 = 0;
+    cudaEventElapsedTime(&a1, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&a2, ctx->ev[1], ctx->ev[2]);
+    ctx->timings[4] = a1;
+    ctx->timings[5] = a2;
+    CK(cudaMemcpyAsync(hs.data(), v_st, sizeof(CGState) * nl, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(par_out, v_par, sizeof(cd) * nl * M, cudaMemcpyDeviceToHost, ctx->st));
+    if (dpar) CK(cudaMemcpyAsync(dpar, v_dpar, sizeof(cd) * nl * M, cudaMemcpyDeviceToHost, ctx->st));
+    if (bdpar) CK(cudaMemcpyAsync(bdpar, v_bdpar, sizeof(double) * nl, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (ncg)
+        for (int b = 0; b < nlam; ++b) ncg[b] = hs[b].ncg;
+    ctx->cg_form = CRT_PRECOND_JACOBI;
     return CRT_OK;
 }
 

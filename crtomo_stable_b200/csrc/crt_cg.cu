@@ -46,6 +46,39 @@ __device__ __forceinline__ cd jval(const CGArgs& A, int e, int i)
     return v;
 }
 
+// J(i, e) in its storage type, converted by jcvt: lets a kernel keep a
+// load in flight across a barrier and convert it afterwards.
+template <int JP, int JM>
+struct JRaw {
+    using T = cd;
+};
+template <> struct JRaw<0, 1> { using T = double; };
+template <> struct JRaw<1, 0> { using T = cf; };
+template <> struct JRaw<1, 1> { using T = float; };
+template <> struct JRaw<1, 2> { using T = cf; };
+
+template <int JP, int JM>
+__device__ __forceinline__ typename JRaw<JP, JM>::T jraw(const CGArgs& A, int e, int i)
+{
+    return static_cast<const typename JRaw<JP, JM>::T*>(A.J)[(size_t)e * A.N + i];
+}
+
+template <int JM>
+__device__ __forceinline__ cd jcvt(cd v)
+{
+    if (JM == 2) v.y = 0.0;
+    return v;
+}
+template <int JM>
+__device__ __forceinline__ cd jcvt(cf f)
+{
+    return cd{(double)f.x, JM == 2 ? 0.0 : (double)f.y};
+}
+template <int JM>
+__device__ __forceinline__ cd jcvt(double v) { return cd{v, 0.0}; }
+template <int JM>
+__device__ __forceinline__ cd jcvt(float v) { return cd{(double)v, 0.0}; }
+
 // bp / bptri: (R (cgfac o p))_i
 __device__ cd reg_apply_cg(const CGArgs& A, const cd* p, int i)
 {
@@ -158,7 +191,7 @@ __global__ void k_cg_setup(CGArgs A, const cd* dat, const cd* sigmaa, const cd* 
     }
 }
 
-__global__ void __launch_bounds__(VEC_NT) k_cg_init(CGArgs A)
+__device__ void cg_init_body(const CGArgs& A)
 {
     // cjggdc (src/cg_mod.f90:106-199) iterates on the real part of the
     // right-hand side (DC) or on its imaginary part (final phase improvement)
@@ -178,8 +211,10 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_init(CGArgs A)
     }
 }
 
+__global__ void __launch_bounds__(VEC_NT) k_cg_init(CGArgs A) { cg_init_body(A); }
+
 // Iteration head: dr = |r|^2, stop rule, beta, p = r + beta p.
-__global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A)
+__device__ void cg_begin_body(const CGArgs& A)
 {
     __shared__ double red[33];
     __shared__ int s_stop;
@@ -212,6 +247,8 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A)
     beta = (k == 1) ? 0.0 : st->beta;
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) A.p[e] = A.r[e] + A.p[e] * beta;
 }
+
+__global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A) { cg_begin_body(A); }
 
 // Preconditioned head: z (the preconditioner's output) is in A.z.  The stop
 // rule is the reference's (|r|^2 against eps |r0|^2); beta is the flexible
@@ -412,7 +449,7 @@ __global__ void k_cg_jhv(CGArgs A)
 }
 
 // Iteration tail: alpha = dr / Re(p^H b), dpar += alpha p, r -= alpha b.
-__global__ void __launch_bounds__(VEC_NT) k_cg_end(CGArgs A)
+__device__ void cg_end_body(const CGArgs& A)
 {
     __shared__ double red[33];
     CGState* st = A.st;
@@ -441,8 +478,10 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_end(CGArgs A)
     }
 }
 
-__global__ void __launch_bounds__(VEC_NT) k_cg_finish(CGArgs A, int lfpi, double step, cd* par,
-                                                      double* bdpar)
+__global__ void __launch_bounds__(VEC_NT) k_cg_end(CGArgs A) { cg_end_body(A); }
+
+__device__ void cg_finish_body(const CGArgs& A, int lfpi, double step, const cd* par_in, cd* par,
+                               double* bdpar)
 {
     __shared__ double red[33];
     double v = 0.0;
@@ -451,13 +490,278 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_finish(CGArgs A, int lfpi, double
         if (lfpi) d = cd{0.0, d.x};
         d = d * A.cgfac[e];
         A.dpar[e] = d;
-        par[e] = par[e] + d * step;
+        par[e] = par_in[e] + d * step;
         v += d.x * d.x + d.y * d.y;
     }
     const double s = block_sum<VEC_NT>(v, red);
     if (threadIdx.x == 0) {
         *bdpar = s * step;
         A.cgres[0] = (double)(float)A.st->ncg;
+    }
+}
+
+__global__ void __launch_bounds__(VEC_NT) k_cg_finish(CGArgs A, int lfpi, double step, cd* par,
+                                                      double* bdpar)
+{
+    cg_finish_body(A, lfpi, step, par, par, bdpar);
+}
+
+// ---------------------------------------------------------------------------
+// Lambda candidates side by side (CGLArgs): candidate b's view of the buffers.
+__device__ __forceinline__ CGArgs cgl_cand(const CGLArgs& L, int b)
+{
+    CGArgs A = L.a;
+    const size_t M = (size_t)A.M, N = (size_t)A.N;
+    A.lam = L.lam[b];
+    A.cgfac += b * M;
+    A.rhs += b * M;
+    A.p += b * M;
+    A.r += b * M;
+    A.bvec += b * M;
+    A.dpar += b * M;
+    A.ap += b * N;
+    A.part += (size_t)b * A.nsplit * N;
+    A.cgres += (size_t)b * (A.ncgmax + 2);
+    A.st += b;
+    return A;
+}
+
+__device__ __forceinline__ bool cgl_all_done(const CGLArgs& L)
+{
+    for (int b = 0; b < L.nl; ++b)
+        if (!L.a.st[b].done) return false;
+    return true;
+}
+
+// k_cg_setup for every candidate: the sums over the readings do not depend
+// on lambda and are formed once per cell.
+template <int JP, int JM>
+__global__ void k_cgl_setup(CGLArgs L, const cd* dat, const cd* sigmaa, const cd* par)
+{
+    const CGArgs& A = L.a;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= A.M) return;
+    const int e = warp;
+    double an = 0.0, arx = 0.0, ary = 0.0;
+    for (int i = lane; i < A.N; i += 32) {
+        const cd j = jval<JP, JM>(A, e, i);
+        const double w = A.wd[i];
+        const cd rd = dat[i] - sigmaa[i];
+        an += (j.x * j.x + j.y * j.y) * w;
+        const cd t = conj(j) * w * rd;
+        arx += t.x;
+        ary += t.y;
+    }
+    an = warp_sum(an);
+    arx = warp_sum(arx);
+    ary = warp_sum(ary);
+    if (lane == 0) {
+        const cd rg = reg_apply_par(A, par, e);
+        for (int b = 0; b < L.nl; ++b) {
+            const double lam = L.lam[b];
+            const double dum = an + lam * reg_diag(A, e);
+            const double cg = 1.0 / sqrt(dum);
+            A.cgfac[(size_t)b * A.M + e] = cg;
+            const cd rb = cd{arx, ary} - rg * lam;
+            A.rhs[(size_t)b * A.M + e] = rb * cg;
+        }
+    }
+}
+
+// One CTA per candidate for the O(M) vector work.
+__global__ void __launch_bounds__(VEC_NT) k_cgl_init(CGLArgs L) { cg_init_body(cgl_cand(L, blockIdx.x)); }
+__global__ void __launch_bounds__(VEC_NT) k_cgl_begin(CGLArgs L) { cg_begin_body(cgl_cand(L, blockIdx.x)); }
+__global__ void __launch_bounds__(VEC_NT) k_cgl_end(CGLArgs L) { cg_end_body(cgl_cand(L, blockIdx.x)); }
+__global__ void __launch_bounds__(VEC_NT) k_cgl_finish(CGLArgs L, int lfpi, double step, const cd* par_in,
+                                                       cd* par_out, double* bdpar)
+{
+    const int b = blockIdx.x;
+    cg_finish_body(cgl_cand(L, b), lfpi, step, par_in, par_out + (size_t)b * L.a.M, bdpar + b);
+}
+
+// k_cg_jv for NL candidates (slots b >= nl carry zeros): each J entry loaded
+// once feeds NL accumulators.
+template <int JP, int JM, int NL>
+__global__ void __launch_bounds__(JV_NT) k_cgl_jv(CGLArgs L)
+{
+    __shared__ cd pcs[NL][JV_CHUNK];
+    if (cgl_all_done(L)) return;
+    const CGArgs& A = L.a;
+    const size_t M = (size_t)A.M;
+    const int i = blockIdx.x * JV_NT + threadIdx.x;
+    const bool valid = i < A.N;
+    const int split = blockIdx.y;
+    const int per = (A.M + A.nsplit - 1) / A.nsplit;
+    const int e0 = split * per, e1 = min(A.M, e0 + per);
+    cd acc[NL];
+#pragma unroll
+    for (int b = 0; b < NL; ++b) acc[b] = cd{0.0, 0.0};
+    for (int eb = e0; eb < e1; eb += JV_CHUNK) {
+        const int ne = min(JV_CHUNK, e1 - eb);
+        __syncthreads();
+        if ((int)threadIdx.x < ne) {
+            const int e = eb + threadIdx.x;
+#pragma unroll
+            for (int b = 0; b < NL; ++b)
+                pcs[b][threadIdx.x] = b < L.nl ? A.p[b * M + e] * A.cgfac[b * M + e] : cd{0.0, 0.0};
+        }
+        __syncthreads();
+        if (!valid) continue;
+        int u = 0;
+        for (; u + JV_UNROLL <= ne; u += JV_UNROLL) {
+            cd jv[JV_UNROLL];
+#pragma unroll
+            for (int q = 0; q < JV_UNROLL; ++q) jv[q] = jval<JP, JM>(A, eb + u + q, i);
+#pragma unroll
+            for (int q = 0; q < JV_UNROLL; ++q) {
+#pragma unroll
+                for (int b = 0; b < NL; ++b) acc[b] += pcs[b][u + q] * jv[q];
+            }
+        }
+        for (; u < ne; ++u) {
+            const cd jv = jval<JP, JM>(A, eb + u, i);
+#pragma unroll
+            for (int b = 0; b < NL; ++b) acc[b] += pcs[b][u] * jv;
+        }
+    }
+    if (!valid) return;
+#pragma unroll
+    for (int b = 0; b < NL; ++b)
+        if (b < L.nl) A.part[((size_t)b * A.nsplit + split) * A.N + i] = acc[b];
+}
+
+// k_cg_jv_reduce per candidate (grid.y = candidate).
+__global__ void k_cgl_jv_reduce(CGLArgs L)
+{
+    const CGArgs A = cgl_cand(L, blockIdx.y);
+    if (A.st->done) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.N) return;
+    cd acc{0.0, 0.0};
+    for (int s = 0; s < A.nsplit; ++s) acc += A.part[(size_t)s * A.N + i];
+    A.ap[i] = acc * A.wd[i];
+}
+
+// k_cg_jhv for NL candidates: one warp per CglCols columns, a CTA of 8
+// warps walks the readings in chunks of CglRows.  Every warp of the CTA
+// needs the chunk's w o ap of all candidates, so the CTA stages it once in
+// shared memory (cp.async, double-buffered); the J loads of the next chunk
+// and its staging are issued before the current chunk is consumed, which
+// keeps two chunks of loads in flight per warp.  Lane b * CglCols + c
+// writes candidate b's column ebase + c.
+constexpr int CGL_JH_NT = 256;
+template <int NL>
+struct CglCols {
+    static constexpr int value = NL <= 2 ? 4 : (NL <= 4 ? 2 : 1);
+};
+template <int NL>
+struct CglRows {   // two rows per lane with 4 columns, four otherwise (pairs of rows)
+    static constexpr int value = NL <= 2 ? 64 : 128;
+};
+
+template <int JP, int JM, int NL>
+__global__ void __launch_bounds__(CGL_JH_NT, 2) k_cgl_jhv(CGLArgs L)
+{
+    constexpr int NC = CglCols<NL>::value, RC = CglRows<NL>::value, RPL = RC / 32;
+    static_assert(NL * NC <= 32, "one lane per (candidate, column)");
+    using RT = typename JRaw<JP, JM>::T;
+    __shared__ cd s_ap[2][NL][RC];
+    if (cgl_all_done(L)) return;   // the same for every thread of the grid
+    const CGArgs& A = L.a;
+    const size_t N = (size_t)A.N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ebase = (blockIdx.x * (CGL_JH_NT / 32) + warp) * NC;
+    // warps past the last column still take part in the staging barriers
+    const int nc = max(0, min(NC, A.M - ebase));
+    double ax[NL][NC], ay[NL][NC];
+#pragma unroll
+    for (int b = 0; b < NL; ++b)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            ax[b][c] = 0.0;
+            ay[b][c] = 0.0;
+        }
+    // w o ap of rows r0 .. r0 + RC into buffer `buf`: copies for the entries
+    // that exist, zeros for the rest (empty candidate slots, rows past N)
+    auto stage = [&](int buf, int r0) {
+        for (int t = threadIdx.x; t < NL * RC; t += CGL_JH_NT) {
+            const int b = t / RC, rr = t - b * RC, i = r0 + rr;
+            if (b < L.nl && i < A.N)
+                cp_async16(&s_ap[buf][b][rr], A.ap + b * N + i);
+            else
+                s_ap[buf][b][rr] = cd{0.0, 0.0};
+        }
+        cp_async_commit();
+    };
+    auto load = [&](RT (&dst)[RPL][NC], int r0) {
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            const int i = r0 + q * 32 + lane;
+#pragma unroll
+            for (int c = 0; c < NC; ++c) dst[q][c] = (c < nc && i < A.N) ? jraw<JP, JM>(A, ebase + c, i) : RT{};
+        }
+    };
+    RT jn[RPL][NC];
+    load(jn, 0);
+    stage(0, 0);
+    int buf = 0;
+    for (int r0 = 0; r0 < A.N; r0 += RC, buf ^= 1) {
+        RT jr[RPL][NC];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q)
+#pragma unroll
+            for (int c = 0; c < NC; ++c) jr[q][c] = jn[q][c];
+        const bool more = r0 + RC < A.N;   // uniform over the CTA
+        if (more) {
+            // buffer buf ^ 1 was last read before the trailing barrier of
+            // the previous chunk
+            load(jn, r0 + RC);
+            stage(buf ^ 1, r0 + RC);
+            cp_async_wait_group<1>();
+        } else {
+            cp_async_wait_group<0>();
+        }
+        __syncthreads();   // chunk r0's w o ap is in shared memory
+        // rows in pairs (lane + 64 k, lane + 64 k + 32) summed as k_cg_jhv
+        // sums them; zero rows past N add exact zeros
+#pragma unroll
+        for (int q = 0; q < RPL; q += 2) {
+#pragma unroll
+            for (int b = 0; b < NL; ++b) {
+                const cd w0 = s_ap[buf][b][q * 32 + lane], w1 = s_ap[buf][b][(q + 1) * 32 + lane];
+#pragma unroll
+                for (int c = 0; c < NC; ++c) {
+                    const cd t0 = conj(jcvt<JM>(jr[q][c])) * w0, t1 = conj(jcvt<JM>(jr[q + 1][c])) * w1;
+                    ax[b][c] += t0.x + t1.x;
+                    ay[b][c] += t0.y + t1.y;
+                }
+            }
+        }
+        __syncthreads();   // readers of `buf` are done before it is staged again
+    }
+#pragma unroll
+    for (int b = 0; b < NL; ++b)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            ax[b][c] = warp_allsum(ax[b][c]);
+            ay[b][c] = warp_allsum(ay[b][c]);
+        }
+    const int mb = lane / NC, mc = lane % NC;
+    if (mb < L.nl && mb < NL && mc < nc) {
+        double bx = 0.0, by = 0.0;
+#pragma unroll
+        for (int b = 0; b < NL; ++b)
+#pragma unroll
+            for (int c = 0; c < NC; ++c)
+                if (b == mb && c == mc) {
+                    bx = ax[b][c];
+                    by = ay[b][c];
+                }
+        const CGArgs C = cgl_cand(L, mb);
+        const int e = ebase + mc;
+        const cd rp = reg_apply_cg(C, C.p, e);
+        const cd bv = cd{bx, by} + rp * C.lam;
+        C.bvec[e] = bv * C.cgfac[e];
     }
 }
 
@@ -514,4 +818,65 @@ void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* g
 void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* bdpar, cudaStream_t s)
 {
     k_cg_finish<<<1, VEC_NT, 0, s>>>(a, lfpi, step, par, bdpar);
+}
+
+// ---------------------------------------------------------------------------
+// Lambda candidates side by side.
+#define CRT_CGL_DISPATCH(KERNEL, NL, GRID, BLOCK, STREAM, ...)                     \
+    do {                                                                           \
+        const int key = L.a.jprec * 3 + L.a.jmode;                                 \
+        switch (key) {                                                             \
+        case 0: KERNEL<0, 0, NL><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;  \
+        case 1: KERNEL<0, 1, NL><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;  \
+        case 2: KERNEL<0, 2, NL><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;  \
+        case 3: KERNEL<1, 0, NL><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;  \
+        case 4: KERNEL<1, 1, NL><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break;  \
+        default: KERNEL<1, 2, NL><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__); break; \
+        }                                                                          \
+    } while (0)
+
+namespace {
+
+template <int NL>
+void cgl_matvecs(const CGLArgs& L, cudaStream_t s)
+{
+    const CGArgs& a = L.a;
+    const int nt = 256;
+    const dim3 gjv((a.N + JV_NT - 1) / JV_NT, a.nsplit);
+    CRT_CGL_DISPATCH(k_cgl_jv, NL, gjv, JV_NT, s, L);
+    k_cgl_jv_reduce<<<dim3((a.N + nt - 1) / nt, L.nl), nt, 0, s>>>(L);
+    const int cols_per_block = (CGL_JH_NT / 32) * CglCols<NL>::value;
+    CRT_CGL_DISPATCH(k_cgl_jhv, NL, (a.M + cols_per_block - 1) / cols_per_block, CGL_JH_NT, s, L);
+}
+
+}  // namespace
+
+void launch_cgl_setup(const CGLArgs& L, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s)
+{
+    const CGArgs& a = L.a;
+    const int threads = 256, warps = threads / 32;
+    CRT_CG_DISPATCH(k_cgl_setup, (a.M + warps - 1) / warps, threads, s, L, dat, sigmaa, par);
+}
+
+void launch_cgl_init(const CGLArgs& L, cudaStream_t s) { k_cgl_init<<<L.nl, VEC_NT, 0, s>>>(L); }
+
+int launch_cgl_iterations(const CGLArgs& L, int iters, cudaStream_t s)
+{
+    for (int it = 0; it < iters; ++it) {
+        k_cgl_begin<<<L.nl, VEC_NT, 0, s>>>(L);
+        if (L.nl <= 2)
+            cgl_matvecs<2>(L, s);
+        else if (L.nl <= 4)
+            cgl_matvecs<4>(L, s);
+        else
+            cgl_matvecs<8>(L, s);
+        k_cgl_end<<<L.nl, VEC_NT, 0, s>>>(L);
+    }
+    return 5 * iters;
+}
+
+void launch_cgl_finish(const CGLArgs& L, int lfpi, double step, const cd* par_in, cd* par_out, double* bdpar,
+                       cudaStream_t s)
+{
+    k_cgl_finish<<<L.nl, VEC_NT, 0, s>>>(L, lfpi, step, par_in, par_out, bdpar);
 }

@@ -64,3 +64,27 @@ void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* g
 // update.f90:300-351: dpar *= cgfac (lfpi: (0, Re dpar) first), par += step
 // dpar, bdpar = step * sum |dpar|^2.
 void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* bdpar, cudaStream_t s);
+
+// Several lambda candidates on one Jacobian.  Each lambda trial of the
+// reference's inversion loop (src/inv.f90:769-912) runs update.f90 with
+// cjggra / cjggdc on the same J; here up to CGL_MAX of them run side by side
+// and the two matvecs of an iteration read every J entry once for all of
+// them.  Candidate b keeps its vectors at offset b * M of the buffers in
+// `a` (ap at b * N, the partial sums at b * nsplit * N, cgres at
+// b * (ncgmax + 2)) and its control block at st + b; `a.lam` is unused.
+// Jacobi form only (pc = 0).  Every candidate's arithmetic is the
+// single solve's, in the same order.
+constexpr int CGL_MAX = 8;
+struct CGLArgs {
+    CGArgs a;
+    int nl;
+    double lam[CGL_MAX];
+};
+
+void launch_cgl_setup(const CGLArgs& L, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s);
+void launch_cgl_init(const CGLArgs& L, cudaStream_t s);
+// returns the number of kernel launches enqueued
+int launch_cgl_iterations(const CGLArgs& L, int iters, cudaStream_t s);
+// par_out[b * M ...] = par_in + step * cgfac_b o dpar_b; bdpar[b] as crt_update
+void launch_cgl_finish(const CGLArgs& L, int lfpi, double step, const cd* par_in, cd* par_out, double* bdpar,
+                       cudaStream_t s);

@@ -64,7 +64,7 @@ class crt_cg_params(C.Structure):
 EXPORTS = [
     "crt_abi_version", "crt_create", "crt_destroy", "crt_last_error", "crt_rwaven", "crt_precal",
     "crt_forward", "crt_potentials", "crt_jacobian", "crt_set_jacobian", "crt_set_regularizer",
-    "crt_set_data", "crt_set_configs", "crt_update", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
+    "crt_set_data", "crt_set_configs", "crt_update", "crt_update_lambdas", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
     "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order", "crt_last_timings_ex",
     "crt_set_refinement", "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
@@ -114,6 +114,8 @@ def load(path: str = LIB_PATH):
     L.crt_set_data.restype = C.c_int32
     L.crt_update.argtypes = [vp, P(crt_cg_params), vp, vp, vp, vp, vp, i32p, f64p]
     L.crt_update.restype = C.c_int32
+    L.crt_update_lambdas.argtypes = [vp, P(crt_cg_params), C.c_int32, f64p, vp, vp, vp, vp, i32p, f64p]
+    L.crt_update_lambdas.restype = C.c_int32
     L.crt_gn_step.argtypes = [vp, P(crt_cg_params), vp, vp, vp, i32p, f64p]
     L.crt_gn_step.restype = C.c_int32
     L.crt_set_model.argtypes = [vp, vp]
@@ -395,6 +397,23 @@ class Context:
                                       _vp(cgres), C.byref(ncg), C.byref(bd)), "crt_update")
         return dict(par=par_, dpar=dpar, cgfac=cgfac, cgres=cgres[: ncg.value + 1], ncg=ncg.value,
                     bdpar=bd.value)
+
+    def update_lambdas(self, prm, lams, par, sigmaa=None):
+        """crt_update for every lambda in `lams` (1 .. 8 candidates, Jacobi
+        form) on one Jacobian; each CG iteration reads J once for all."""
+        lam_ = np.ascontiguousarray(lams, np.float64)
+        nl = int(lam_.size)
+        M = self.elanz
+        par_ = np.ascontiguousarray(par, np.complex128)
+        out = np.zeros((nl, M), np.complex128)
+        dpar = np.zeros((nl, M), np.complex128)
+        ncg = np.zeros(nl, np.int32)
+        bd = np.zeros(nl)
+        sa = None if sigmaa is None else np.ascontiguousarray(sigmaa, np.complex128)
+        self._check(self.L.crt_update_lambdas(self.h, C.byref(prm), nl, _ptr(lam_, C.c_double), _vp(sa), _vp(par_),
+                                              _vp(out), _vp(dpar), _ptr(ncg, C.c_int32), _ptr(bd, C.c_double)),
+                    "crt_update_lambdas")
+        return dict(par=out, dpar=dpar, ncg=ncg, bdpar=bd)
 
     def gn_step(self, prm, par):
         par_ = np.array(par, np.complex128)

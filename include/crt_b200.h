@@ -182,6 +182,20 @@ int32_t crt_set_data(crt_ctx *ctx, const double *dat, const double *wmatd, const
 int32_t crt_update(crt_ctx *ctx, const crt_cg_params *prm, const double *sigmaa, double *par,
                    double *dpar, double *cgfac, double *cgres, int32_t *ncg, double *bdpar);
 
+/* Lambda candidates side by side.  The reference's inversion loop
+ * (src/inv.f90:769-912) tries one lambda after another, each trial one
+ * src/update.f90 pass with cjggra / cjggdc on the same Jacobian; this call
+ * runs nlam (1 .. 8) such updates at once, and every CG iteration reads J
+ * once for all candidates.  Candidate b is crt_update with prm->lam =
+ * lams[b] in the Jacobi form (prm->lam and prm->precond are ignored), from
+ * the same sigmaa (NULL = the last crt_forward) and par (complex [manz],
+ * not modified).  par_out: complex [nlam][manz], par + step * dpar_b.
+ * Optional (NULL to skip): dpar complex [nlam][manz], ncg [nlam],
+ * bdpar [nlam]. */
+int32_t crt_update_lambdas(crt_ctx *ctx, const crt_cg_params *prm, int32_t nlam, const double *lams,
+                           const double *sigmaa, const double *par, double *par_out, double *dpar,
+                           int32_t *ncg, double *bdpar);
+
 /* One Gauss-Newton step of the reference loop (src/inv.f90:426-495,
  * :739-743, :924-933): sigma = exp(par); forward + bvolti; bsensi (or
  * bsendc); update.  par is updated in place.  Outputs as crt_update plus

@@ -1,0 +1,150 @@
+"""Lambda candidates side by side (crt_update_lambdas).
+
+The reference's inversion loop (src/inv.f90:769-912) runs one
+src/update.f90 pass (cjggra / cjggdc) per lambda trial on the same
+Jacobian.  The batched call runs up to eight of them at once with one read
+of J per CG iteration for all candidates; each candidate must give what
+crt_update gives for its lambda, and what the oracle's update gives.
+
+Tolerances: against the oracle as the single update's parity test (ncg
+equal, dpar to 1e-7 of its largest entry at the reference's stop rule).
+Against crt_update on the same device: each candidate solves the same
+system with the same recurrences, only the matvecs sum in another order
+(fused complex multiply-adds, chunked rows), so at the reference's stop
+rule (tens of iterations) ncg is equal and dpar agrees to 1e-10; at
+rel-res 1e-6 (hundreds of iterations) two solutions that both meet the
+residual bound may differ by the condition number times it, and the test
+asks for ncg within 2 and dpar to 1e-4 (the bound the other rel-res 1e-6
+CG tests use against the oracle).
+"""
+import numpy as np
+import pytest
+
+from fixtures import load_forward_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(name="minimal", precision=0, ldc=False, sig0=0.01 + 0j):
+    from crtomo_stable_b200 import regularization
+    from crtomo_stable_b200.lib import Context
+    case = load_forward_case(name)
+    m = case["mesh"]
+    d = case["volt"]
+    ctx = Context(m, case["enr"], d.strnr, d.vnr, swrtr=case["cfg"].swrtr, lsink=case["cfg"].lsink,
+                  nsink=case["cfg"].nsink, precision=precision)
+    dat = -np.log(d.bet) - 1j * d.pha / 1e3
+    wmatd = 1.0 / (1e-2 + 1e-3 / d.bet) ** 2
+    sig = np.full(m.elanz, sig0)
+    ctx.forward(sig, ldc=ldc)
+    ctx.jacobian(mode=1 if ldc else 0, copy=False)
+    nb = regularization.nachbar(m)
+    sm = regularization.smatm_tri(m, nb, 10.0, 1.0)
+    ctx.set_regularizer(1, sm, nachbar=nb)
+    ctx.set_data(dat, wmatd)
+    return ctx, case, dat, wmatd, sig, nb, sm
+
+
+def _close(got, ref, rtol):
+    np.testing.assert_allclose(got, ref, rtol=rtol, atol=rtol * np.abs(ref).max())
+
+
+def test_lambda_candidates_match_oracle():
+    from crtomo_stable_b200.lib import Context
+    from oracle.oracle import OracleCG, OracleProblem
+    ctx, case, dat, wmatd, sig, nb, sm = _case()
+    m = case["mesh"]
+    op = OracleProblem(m, case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=case["cfg"].swrtr,
+                       lsink=case["cfg"].lsink, nsink=case["cfg"].nsink)
+    kp = op.forward(sig, nthreads=4)
+    volt_o, sa_o = op.bvolti(op.rtrafo(kp))
+    J_o = op.bsensi(kp, sig, volt_o, nthreads=4)
+    lams = np.array([30.0, 300.0, 3000.0])
+    eps, ncgmax = 1e-4, m.elanz // 10
+    par = np.log(sig)
+    got = ctx.update_lambdas(Context.params(0.0, eps=eps, ncgmax=ncgmax, step=0.5), lams, par, sigmaa=sa_o)
+    for b, lam in enumerate(lams):
+        cg = OracleCG(m.elanz, len(dat), 1, sm, nachbar=nb, nnb=m.maxnodes, wmatd=wmatd, lam=lam, eps=eps,
+                      ncgmax=ncgmax)
+        ref = cg.update(J_o, dat, sa_o, par, 0.5)
+        assert got["ncg"][b] == ref["ncg"], (lam, got["ncg"][b], ref["ncg"])
+        _close(got["dpar"][b], ref["dpar"], 1e-7)
+        np.testing.assert_allclose(got["bdpar"][b], ref["bdpar"], rtol=1e-8)
+        _close(got["par"][b], par + 0.5 * got["dpar"][b], 1e-15)
+    # the candidates differ from one another (lambda reaches the solve)
+    assert np.abs(got["dpar"][0] - got["dpar"][2]).max() > 1e-3 * np.abs(got["dpar"][0]).max()
+    ctx.close()
+
+
+@pytest.mark.parametrize("nlam", [1, 2, 3, 5, 8])
+def test_lambda_candidates_equal_single_updates(nlam):
+    """Every slot count of the matvec kernels (2, 4 and 8 candidates per J
+    read, with empty slots) and candidates that stop at different
+    iterations."""
+    from crtomo_stable_b200.lib import Context
+    ctx, case, dat, wmatd, sig, nb, sm = _case()
+    m = case["mesh"]
+    par = np.log(sig)
+    lams = 3.0 * 10.0 ** np.linspace(0.0, 3.5, nlam)
+    for eps, ncgmax, rtol, dn in ((1e-4, m.elanz // 10, 1e-10, 0), (1e-12, 2000, 1e-4, 2)):
+        got = ctx.update_lambdas(Context.params(0.0, eps=eps, ncgmax=ncgmax), lams, par)
+        for b, lam in enumerate(lams):
+            one = ctx.update(Context.params(lam, eps=eps, ncgmax=ncgmax), par)
+            assert abs(int(got["ncg"][b]) - one["ncg"]) <= dn, (eps, lam, got["ncg"][b], one["ncg"])
+            _close(got["dpar"][b], one["dpar"], rtol)
+            np.testing.assert_allclose(got["bdpar"][b], one["bdpar"], rtol=max(rtol, 1e-12))
+        if eps == 1e-12 and nlam > 1:
+            assert len(set(got["ncg"].tolist())) > 1   # the candidates stopped at different iterations
+    ctx.close()
+
+
+@pytest.mark.parametrize("form", ["ldc", "lfpi"])
+def test_lambda_candidates_real_modes(form):
+    """cjggdc forms: the DC inversion (real Jacobian) and the final phase
+    improvement (real part of J, imaginary right-hand side)."""
+    from crtomo_stable_b200.lib import Context
+    ldc = form == "ldc"
+    ctx, case, dat, wmatd, sig, nb, sm = _case(ldc=ldc, sig0=0.01 * np.exp(-0.01j))
+    m = case["mesh"]
+    par = np.log(sig)
+    lams = np.array([100.0, 1000.0])
+    prm = Context.params(0.0, eps=1e-4, ncgmax=m.elanz // 10, ldc=ldc, lfpi=not ldc)
+    got = ctx.update_lambdas(prm, lams, par)
+    for b, lam in enumerate(lams):
+        one = ctx.update(Context.params(lam, eps=1e-4, ncgmax=m.elanz // 10, ldc=ldc, lfpi=not ldc), par)
+        assert got["ncg"][b] == one["ncg"]
+        _close(got["dpar"][b], one["dpar"], 1e-10)
+        if ldc:
+            assert np.abs(got["dpar"][b].imag).max() == 0.0
+        else:
+            assert np.abs(got["dpar"][b].real).max() == 0.0
+    ctx.close()
+
+
+def test_lambda_candidates_mixed_precision():
+    """Complex64-stored Jacobian (FP64 accumulation), as in the mixed form."""
+    from crtomo_stable_b200.lib import PREC_MIXED, Context
+    ctx, case, dat, wmatd, sig, nb, sm = _case(precision=PREC_MIXED)
+    m = case["mesh"]
+    par = np.log(sig)
+    lams = np.array([50.0, 500.0, 5000.0, 50000.0])
+    got = ctx.update_lambdas(Context.params(0.0, eps=1e-4, ncgmax=m.elanz // 10), lams, par)
+    for b, lam in enumerate(lams):
+        one = ctx.update(Context.params(lam, eps=1e-4, ncgmax=m.elanz // 10), par)
+        assert got["ncg"][b] == one["ncg"]
+        _close(got["dpar"][b], one["dpar"], 1e-10)
+    ctx.close()
+
+
+def test_lambda_candidates_reject_bad_arguments():
+    from crtomo_stable_b200.lib import CRTError, Context
+    ctx, case, dat, wmatd, sig, nb, sm = _case()
+    par = np.log(sig)
+    prm = Context.params(0.0, eps=1e-4, ncgmax=10)
+    for lams in ([], [1.0] * 9, [10.0, -1.0], [np.nan]):
+        with pytest.raises(CRTError):
+            ctx.update_lambdas(prm, np.array(lams, np.float64), par)
+    # the context stays usable
+    got = ctx.update_lambdas(prm, np.array([10.0]), par)
+    assert got["ncg"][0] > 0
+    ctx.close()
