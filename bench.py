@@ -324,13 +324,14 @@ def run_batch(args, ws, rank, local, pg):
         print(json.dumps(line), flush=True)
 
 
-def lambda_batch(ctx, Context, lam, par0, nlam, iters, E, N):
-    """Lambda trials side by side: `nlam` Jacobi-form updates (the
-    reference's cjggra) for lambdas spread over two decades around `lam`,
-    on the step's complex64 Jacobian, each run for exactly `iters` CG
-    iterations (eps = 0), through crt_update_lambdas against the same
-    updates one crt_update at a time.  Times are the library's CUDA-event
-    phases (cg set-up + iterations), host copies excluded."""
+def lambda_batch(ctx, Context, lam, par0, nlam, iters, E, N, eps, ncgmax, precond_block):
+    """Lambda trials side by side: `nlam` updates for lambdas spread over
+    two decades around `lam`, on the step's complex64 Jacobian, through
+    crt_update_lambdas against the same updates one crt_update at a time:
+    in the Jacobi form (the reference's cjggra) for exactly `iters` CG
+    iterations (eps = 0), and in the block-preconditioned form to the
+    step's stop rule.  Times are the library's CUDA-event phases (cg set-up,
+    preconditioner factors and iterations), host copies excluded."""
     lams = lam * np.logspace(-1.0, 1.0, nlam)
     prm = Context.params(lam, eps=0.0, ncgmax=iters)
     ctx.update_lambdas(prm, lams, par0)                      # warm-up
@@ -344,10 +345,33 @@ def lambda_batch(ctx, Context, lam, par0, nlam, iters, E, N):
         t_seq += t["cg_setup"] + t["cg_iter"]
     bytes_it = 2.0 * N * E * 8 + nlam * (6.0 * E * 16 + 3.0 * N * 16)   # J (complex64) twice + vectors
     ach = bytes_it * iters / (t_iter / 1e3) / 1e9
-    return {"candidates": nlam, "iterations": iters, "ncg": [int(x) for x in got["ncg"]],
-            "batched_ms": t_batch, "sequential_ms": t_seq, "speedup": t_seq / t_batch if t_batch > 0 else None,
-            "batched_iteration_ms": t_iter / iters, "achieved_gbs": ach,
-            "form": "Jacobi (cgfac) CG per candidate, complex64 J read once per iteration for all candidates"}
+    # the block-preconditioned form at the step's stop rule (rel-res 1e-6):
+    # one S factor per candidate, factors and sweeps side by side
+    pb = Context.params(lam, eps=eps, ncgmax=ncgmax, precond=precond_block)
+    ctx.update_lambdas(pb, lams, par0)                       # warm-up
+    gb = ctx.update_lambdas(pb, lams, par0)
+    t = ctx.timings()
+    tb_batch = t["cg_setup"] + t["cg_iter"]
+    form_b = ctx.cg_info()[0]
+    tb_seq, ncg_seq = 0.0, []
+    for lm in lams:
+        r = ctx.update(Context.params(lm, eps=eps, ncgmax=ncgmax, precond=precond_block), par0)
+        t = ctx.timings()
+        tb_seq += t["cg_setup"] + t["cg_iter"]
+        ncg_seq.append(int(r["ncg"]))
+    return {"candidates": nlam, "lams": [float(x) for x in lams],
+            "jacobi": {"iterations": iters, "ncg": [int(x) for x in got["ncg"]],
+                       "batched_ms": t_batch, "sequential_ms": t_seq,
+                       "speedup": t_seq / t_batch if t_batch > 0 else None,
+                       "batched_iteration_ms": t_iter / iters, "achieved_gbs": ach,
+                       "form": "Jacobi (cgfac) CG per candidate (the reference's cjggra), exactly `iterations` "
+                               "iterations, complex64 J read once per iteration for all candidates"},
+            "block": {"ncg": [int(x) for x in gb["ncg"]], "ncg_sequential": ncg_seq,
+                      "batched_ms": tb_batch, "sequential_ms": tb_seq,
+                      "speedup": tb_seq / tb_batch if tb_batch > 0 else None, "cg_form": int(form_b),
+                      "form": "block-preconditioned CG per candidate to rel-res 1e-6 (the GN step's solve): "
+                              "one S factor per candidate, factors and sweeps on parallel streams, batched "
+                              "matvecs"}}
 
 
 def main():
@@ -413,7 +437,8 @@ def main():
         form, blk, bw = ctx.cg_info()
         lam_batch = None
         if precision == PREC_MIXED and args.lambdas > 0:
-            lam_batch = lambda_batch(ctx, Context, lam, par0, args.lambdas, args.lambda_iters, E, N)
+            lam_batch = lambda_batch(ctx, Context, lam, par0, args.lambdas, args.lambda_iters, E, N, args.eps,
+                                     args.ncgmax, PRECOND_BLOCK)
         ctx.close()
         return dict(t=t_step, phase=phase, ncg=ncg, launches=int(launches), clocks=clocks, e2e=t_e2e, lam=lam, K=K,
                     cg_form=form, cg_block=blk, cg_bw=bw, c64=precision == PREC_MIXED, lam_batch=lam_batch)

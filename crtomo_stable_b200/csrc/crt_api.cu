@@ -99,6 +99,13 @@ struct crt_ctx {
     // candidates' vectors, grown on demand
     unsigned char* d_cgl = nullptr;
     size_t cgl_bytes = 0;
+    // block form of the batch: each candidate's preconditioner factor
+    // buffers, and streams on which the candidates' one-CTA factor and
+    // sweep kernels run side by side
+    std::vector<SpcPlan> spc_c;
+    cudaStream_t cstr[CGL_MAX] = {};
+    cudaEvent_t cev_fork = nullptr;
+    cudaEvent_t cev_join[CGL_MAX] = {};
     int cg_form = 0;      // form of the last CG: CRT_PRECOND_*
     // learned correction of the preconditioner
     Gnn gnn;
@@ -335,7 +342,13 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (SpcPlan& c : ctx->spc_c) spc_plan_free_clone(c);
     spc_plan_free(ctx->spc);
+    for (int b = 0; b < CGL_MAX; ++b) {
+        if (ctx->cstr[b]) cudaStreamDestroy(ctx->cstr[b]);
+        if (ctx->cev_join[b]) cudaEventDestroy(ctx->cev_join[b]);
+    }
+    if (ctx->cev_fork) cudaEventDestroy(ctx->cev_fork);
     gnn_free(ctx->gnn);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
@@ -1059,6 +1072,9 @@ extern "C" int32_t crt_set_regularizer(crt_ctx* ctx, int32_t ltri, int32_t nx, i
     }
     CK(cudaStreamSynchronize(ctx->st));
     ctx->spc_why.clear();
+    // the lambda candidates' factor buffers follow the plan they were cloned from
+    for (SpcPlan& c : ctx->spc_c) spc_plan_free_clone(c);
+    ctx->spc_c.clear();
     if (int e = spc_plan_build(ctx->spc, M, ltri, nx, nnb, smatm, nachbar, ctx->spc_why))
         return set_err(ctx, e, "block preconditioner set-up failed");
     // learned correction: same graph; a graph it cannot hold (more than four
@@ -1316,7 +1332,7 @@ extern "C" int32_t crt_update_lambdas(crt_ctx* ctx, const crt_cg_params* prm, in
     const size_t M = (size_t)ctx->E, N = (size_t)ctx->N, nl = (size_t)nlam, ns = (size_t)ctx->cg_nsplit;
     const size_t ncr = (size_t)prm->ncgmax + 2;
     // slab: cd vectors first (16-byte aligned), then doubles, then the states
-    const size_t n_cd = nl * (6 * M + N + ns * N) + N;   // rhs p r bvec dpar par_out, ap, part; sigmaa
+    const size_t n_cd = nl * (8 * M + N + ns * N) + N;   // rhs p r bvec dpar par_out z rold, ap, part; sigmaa
     const size_t n_d = nl * (M + ncr + 1);                // cgfac, cgres, bdpar
     const size_t bytes = n_cd * sizeof(cd) + n_d * sizeof(double) + nl * sizeof(CGState);
     if (ctx->cgl_bytes < bytes) {
@@ -1334,6 +1350,8 @@ extern "C" int32_t crt_update_lambdas(crt_ctx* ctx, const crt_cg_params* prm, in
     cd* v_bvec = take_cd(nl * M);
     cd* v_dpar = take_cd(nl * M);
     cd* v_par = take_cd(nl * M);
+    cd* v_z = take_cd(nl * M);
+    cd* v_rold = take_cd(nl * M);
     cd* v_ap = take_cd(nl * N);
     cd* v_part = take_cd(nl * ns * N);
     cd* v_sa = take_cd(N);
@@ -1363,28 +1381,90 @@ extern "C" int32_t crt_update_lambdas(crt_ctx* ctx, const crt_cg_params* prm, in
     L.a.part = v_part;
     L.a.cgres = v_cgres;
     L.a.st = v_st;
+    L.a.z = v_z;
+    L.a.rold = v_rold;
     L.a.pc = 0;
+    L.a.pc_gnn = 0;
+    L.a.zb = nullptr;
     L.nl = nlam;
-    for (int b = 0; b < nlam; ++b) L.lam[b] = lams[b];
+    for (int b = 0; b < nlam; ++b) {
+        L.lam[b] = lams[b];
+        L.slot[b] = b;
+    }
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
     launch_cgl_setup(L, ctx->d_dat, d_sa, ctx->d_par, ctx->st);
+    ctx->launches += 1;
+    // block form: every candidate's S from its cgfac and lambda, factored
+    // side by side; a breakdown of any candidate's factor runs the whole
+    // batch in the Jacobi form
+    bool use_block = false;
+    if ((prm->precond == CRT_PRECOND_BLOCK || prm->precond == CRT_PRECOND_BLOCK_GNN) && ctx->spc.ok) {
+        if (ctx->spc_c.size() < nl) ctx->spc_c.resize(nl);
+        for (size_t b = 0; b < nl; ++b) {
+            if (!ctx->spc_c[b].ok)
+                if (int e = spc_plan_clone(ctx->spc, ctx->spc_c[b]))
+                    return set_err(ctx, e, "block preconditioner buffers of a lambda candidate");
+            if (!ctx->cstr[b]) CK(cudaStreamCreateWithFlags(&ctx->cstr[b], cudaStreamNonBlocking));
+            if (!ctx->cev_join[b]) CK(cudaEventCreateWithFlags(&ctx->cev_join[b], cudaEventDisableTiming));
+        }
+        if (!ctx->cev_fork) CK(cudaEventCreateWithFlags(&ctx->cev_fork, cudaEventDisableTiming));
+        CK(cudaEventRecord(ctx->cev_fork, ctx->st));
+        for (size_t b = 0; b < nl; ++b) {
+            CK(cudaStreamWaitEvent(ctx->cstr[b], ctx->cev_fork, 0));
+            launch_spc_factor(ctx->spc_c[b], v_cgfac + b * M, ctx->d_smatm, lams[b], ctx->cstr[b]);
+            CK(cudaEventRecord(ctx->cev_join[b], ctx->cstr[b]));
+            CK(cudaStreamWaitEvent(ctx->st, ctx->cev_join[b], 0));
+            ctx->launches += 3 + (ctx->spc.nb > 1 ? 1 : 0);
+        }
+        std::vector<int> flags(nl, 0);
+        for (size_t b = 0; b < nl; ++b)
+            CK(cudaMemcpyAsync(&flags[b], ctx->spc_c[b].d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (int e = kernel_check(ctx, "lambda-batch block preconditioner factors")) return e;
+        use_block = true;
+        for (int f : flags) use_block = use_block && f == 0;
+    }
+    L.a.pc = use_block ? 1 : 0;
     launch_cgl_init(L, ctx->st);
-    ctx->launches += 2;
+    ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     if (int e = kernel_check(ctx, "lambda-batch cg setup")) return e;
     std::vector<CGState> hs(nl);
     int done_iters = 0;
-    const int batch = 16;
+    // iterations between host reads of the candidates' states; at each read
+    // the candidates still iterating are compacted into the first positions
+    // (fewer slots in the matvecs, fewer sweeps)
+    const int batch = 8;
     while (done_iters < prm->ncgmax) {
         const int it = std::min(batch, prm->ncgmax - done_iters);
-        ctx->launches += launch_cgl_iterations(L, it, ctx->st);
+        if (use_block) {
+            for (int k = 0; k < it; ++k) {
+                // z = S^-1 r of every active candidate on its stream, then the batched iteration
+                CK(cudaEventRecord(ctx->cev_fork, ctx->st));
+                for (int q = 0; q < L.nl; ++q) {
+                    const size_t b = (size_t)L.slot[q];
+                    CK(cudaStreamWaitEvent(ctx->cstr[b], ctx->cev_fork, 0));
+                    launch_spc_apply(ctx->spc_c[b], v_r + b * M, v_z + b * M, v_st + b, ctx->cstr[b]);
+                    CK(cudaEventRecord(ctx->cev_join[b], ctx->cstr[b]));
+                    CK(cudaStreamWaitEvent(ctx->st, ctx->cev_join[b], 0));
+                }
+                ctx->launches += 2 * L.nl + launch_cgl_iteration_pc(L, ctx->st);
+            }
+        } else {
+            ctx->launches += launch_cgl_iterations(L, it, ctx->st);
+        }
         done_iters += it;
         CK(cudaMemcpyAsync(hs.data(), v_st, sizeof(CGState) * nl, cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
-        bool all = true;
-        for (const CGState& h : hs) all = all && h.done;
-        if (all) break;
+        int na = 0;
+        for (int b = 0; b < nlam; ++b)
+            if (!hs[b].done) L.slot[na++] = b;
+        if (na == 0) break;
+        L.nl = na;
     }
+    // finish every candidate
+    L.nl = nlam;
+    for (int b = 0; b < nlam; ++b) L.slot[b] = b;
     if (int e = kernel_check(ctx, "lambda-batch cg iterations")) return e;
     launch_cgl_finish(L, prm->lfpi, prm->step, ctx->d_par, v_par, v_bdpar, ctx->st);
     ctx->launches++;
@@ -1402,7 +1482,7 @@ extern "C" int32_t crt_update_lambdas(crt_ctx* ctx, const crt_cg_params* prm, in
     CK(cudaStreamSynchronize(ctx->st));
     if (ncg)
         for (int b = 0; b < nlam; ++b) ncg[b] = hs[b].ncg;
-    ctx->cg_form = CRT_PRECOND_JACOBI;
+    ctx->cg_form = use_block ? CRT_PRECOND_BLOCK : CRT_PRECOND_JACOBI;
     return CRT_OK;
 }
 

@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A) { cg_begin_body(A
 // Re(r^H z).  With the learned correction (pc_gnn) the head also guards it:
 // a non-descent z or a stalled residual switches it off (no_gnn) and the
 // direction restarts (beta = 0) from the base preconditioner's output.
-__global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A)
+__device__ void cg_begin_pc_body(const CGArgs& A)
 {
     __shared__ double red[33];
     __shared__ int s_stop, s_base;
@@ -334,6 +334,8 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A)
         A.rold[e] = r;
     }
 }
+
+__global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A) { cg_begin_pc_body(A); }
 
 // ap partial sums over a column range: thread per reading.  The block stages
 // p o cgfac for JV_CHUNK columns in shared memory and keeps JV_UNROLL
@@ -507,11 +509,13 @@ __global__ void __launch_bounds__(VEC_NT) k_cg_finish(CGArgs A, int lfpi, double
 }
 
 // ---------------------------------------------------------------------------
-// Lambda candidates side by side (CGLArgs): candidate b's view of the buffers.
-__device__ __forceinline__ CGArgs cgl_cand(const CGLArgs& L, int b)
+// Lambda candidates side by side (CGLArgs): the view of the buffers of the
+// candidate in position k (slot L.slot[k]).
+__device__ __forceinline__ CGArgs cgl_cand(const CGLArgs& L, int k)
 {
     CGArgs A = L.a;
     const size_t M = (size_t)A.M, N = (size_t)A.N;
+    const int b = L.slot[k];
     A.lam = L.lam[b];
     A.cgfac += b * M;
     A.rhs += b * M;
@@ -519,6 +523,8 @@ __device__ __forceinline__ CGArgs cgl_cand(const CGLArgs& L, int b)
     A.r += b * M;
     A.bvec += b * M;
     A.dpar += b * M;
+    A.z += b * M;
+    A.rold += b * M;
     A.ap += b * N;
     A.part += (size_t)b * A.nsplit * N;
     A.cgres += (size_t)b * (A.ncgmax + 2);
@@ -529,7 +535,7 @@ __device__ __forceinline__ CGArgs cgl_cand(const CGLArgs& L, int b)
 __device__ __forceinline__ bool cgl_all_done(const CGLArgs& L)
 {
     for (int b = 0; b < L.nl; ++b)
-        if (!L.a.st[b].done) return false;
+        if (!L.a.st[L.slot[b]].done) return false;
     return true;
 }
 
@@ -558,12 +564,13 @@ __global__ void k_cgl_setup(CGLArgs L, const cd* dat, const cd* sigmaa, const cd
     if (lane == 0) {
         const cd rg = reg_apply_par(A, par, e);
         for (int b = 0; b < L.nl; ++b) {
-            const double lam = L.lam[b];
+            const int sb = L.slot[b];
+            const double lam = L.lam[sb];
             const double dum = an + lam * reg_diag(A, e);
             const double cg = 1.0 / sqrt(dum);
-            A.cgfac[(size_t)b * A.M + e] = cg;
+            A.cgfac[(size_t)sb * A.M + e] = cg;
             const cd rb = cd{arx, ary} - rg * lam;
-            A.rhs[(size_t)b * A.M + e] = rb * cg;
+            A.rhs[(size_t)sb * A.M + e] = rb * cg;
         }
     }
 }
@@ -571,12 +578,13 @@ __global__ void k_cgl_setup(CGLArgs L, const cd* dat, const cd* sigmaa, const cd
 // One CTA per candidate for the O(M) vector work.
 __global__ void __launch_bounds__(VEC_NT) k_cgl_init(CGLArgs L) { cg_init_body(cgl_cand(L, blockIdx.x)); }
 __global__ void __launch_bounds__(VEC_NT) k_cgl_begin(CGLArgs L) { cg_begin_body(cgl_cand(L, blockIdx.x)); }
+__global__ void __launch_bounds__(VEC_NT) k_cgl_begin_pc(CGLArgs L) { cg_begin_pc_body(cgl_cand(L, blockIdx.x)); }
 __global__ void __launch_bounds__(VEC_NT) k_cgl_end(CGLArgs L) { cg_end_body(cgl_cand(L, blockIdx.x)); }
 __global__ void __launch_bounds__(VEC_NT) k_cgl_finish(CGLArgs L, int lfpi, double step, const cd* par_in,
                                                        cd* par_out, double* bdpar)
 {
-    const int b = blockIdx.x;
-    cg_finish_body(cgl_cand(L, b), lfpi, step, par_in, par_out + (size_t)b * L.a.M, bdpar + b);
+    const int b = L.slot[blockIdx.x];
+    cg_finish_body(cgl_cand(L, blockIdx.x), lfpi, step, par_in, par_out + (size_t)b * L.a.M, bdpar + b);
 }
 
 // k_cg_jv for NL candidates (slots b >= nl carry zeros): each J entry loaded
@@ -603,7 +611,7 @@ __global__ void __launch_bounds__(JV_NT) k_cgl_jv(CGLArgs L)
             const int e = eb + threadIdx.x;
 #pragma unroll
             for (int b = 0; b < NL; ++b)
-                pcs[b][threadIdx.x] = b < L.nl ? A.p[b * M + e] * A.cgfac[b * M + e] : cd{0.0, 0.0};
+                pcs[b][threadIdx.x] = b < L.nl ? A.p[L.slot[b] * M + e] * A.cgfac[L.slot[b] * M + e] : cd{0.0, 0.0};
         }
         __syncthreads();
         if (!valid) continue;
@@ -627,7 +635,7 @@ __global__ void __launch_bounds__(JV_NT) k_cgl_jv(CGLArgs L)
     if (!valid) return;
 #pragma unroll
     for (int b = 0; b < NL; ++b)
-        if (b < L.nl) A.part[((size_t)b * A.nsplit + split) * A.N + i] = acc[b];
+        if (b < L.nl) A.part[((size_t)L.slot[b] * A.nsplit + split) * A.N + i] = acc[b];
 }
 
 // k_cg_jv_reduce per candidate (grid.y = candidate).
@@ -687,7 +695,7 @@ __global__ void __launch_bounds__(CGL_JH_NT, 2) k_cgl_jhv(CGLArgs L)
         for (int t = threadIdx.x; t < NL * RC; t += CGL_JH_NT) {
             const int b = t / RC, rr = t - b * RC, i = r0 + rr;
             if (b < L.nl && i < A.N)
-                cp_async16(&s_ap[buf][b][rr], A.ap + b * N + i);
+                cp_async16(&s_ap[buf][b][rr], A.ap + L.slot[b] * N + i);
             else
                 s_ap[buf][b][rr] = cd{0.0, 0.0};
         }
@@ -873,6 +881,19 @@ int launch_cgl_iterations(const CGLArgs& L, int iters, cudaStream_t s)
         k_cgl_end<<<L.nl, VEC_NT, 0, s>>>(L);
     }
     return 5 * iters;
+}
+
+int launch_cgl_iteration_pc(const CGLArgs& L, cudaStream_t s)
+{
+    k_cgl_begin_pc<<<L.nl, VEC_NT, 0, s>>>(L);
+    if (L.nl <= 2)
+        cgl_matvecs<2>(L, s);
+    else if (L.nl <= 4)
+        cgl_matvecs<4>(L, s);
+    else
+        cgl_matvecs<8>(L, s);
+    k_cgl_end<<<L.nl, VEC_NT, 0, s>>>(L);
+    return 5;
 }
 
 void launch_cgl_finish(const CGLArgs& L, int lfpi, double step, const cd* par_in, cd* par_out, double* bdpar,

@@ -71,20 +71,30 @@ void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* b
 // and the two matvecs of an iteration read every J entry once for all of
 // them.  Candidate b keeps its vectors at offset b * M of the buffers in
 // `a` (ap at b * N, the partial sums at b * nsplit * N, cgres at
-// b * (ncgmax + 2)) and its control block at st + b; `a.lam` is unused.
-// Jacobi form only (pc = 0).  Every candidate's arithmetic is the
+// b * (ncgmax + 2), z and rold at b * M) and its control block at st + b;
+// `a.lam` is unused.  `slot` maps the nl positions of a launch to
+// candidates, so that the candidates still iterating can be compacted into
+// fewer positions once others have stopped (set-up, init and finish take
+// every candidate with the identity map).  Jacobi form (pc = 0, launch_cgl_iterations) or the
+// block-preconditioned form (pc = 1, launch_cgl_iteration_pc after the
+// caller has applied each candidate's preconditioner into its z; the
+// learned correction is not batched).  Every candidate's arithmetic is the
 // single solve's, in the same order.
 constexpr int CGL_MAX = 8;
 struct CGLArgs {
     CGArgs a;
-    int nl;
-    double lam[CGL_MAX];
+    int nl;                 // candidates taking part in the launch
+    int slot[CGL_MAX];      // position -> candidate (buffer slot); the identity unless compacted
+    double lam[CGL_MAX];    // per candidate (by slot)
 };
 
 void launch_cgl_setup(const CGLArgs& L, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s);
 void launch_cgl_init(const CGLArgs& L, cudaStream_t s);
 // returns the number of kernel launches enqueued
 int launch_cgl_iterations(const CGLArgs& L, int iters, cudaStream_t s);
+// one preconditioned iteration (head, matvecs, tail) of every candidate;
+// returns the number of kernel launches
+int launch_cgl_iteration_pc(const CGLArgs& L, cudaStream_t s);
 // par_out[b * M ...] = par_in + step * cgfac_b o dpar_b; bdpar[b] as crt_update
 void launch_cgl_finish(const CGLArgs& L, int lfpi, double step, const cd* par_in, cd* par_out, double* bdpar,
                        cudaStream_t s);

@@ -878,6 +878,37 @@ void spc_plan_free(SpcPlan& P)
     P = SpcPlan{};
 }
 
+int spc_plan_clone(const SpcPlan& src, SpcPlan& dst)
+{
+    spc_plan_free_clone(dst);
+    if (!src.ok) return CRT_ERR_ARG;
+    dst = src;   // ordering, entry list and sizes are shared
+    dst.ok = 0;
+    dst.d_DF = nullptr;
+    dst.d_G = dst.d_H = nullptr;
+    dst.d_h = nullptr;
+    dst.d_flag = nullptr;
+    const size_t BB = (size_t)src.B * src.B;
+    const bool ok = alloc(&dst.d_DF, 2 * src.nb * BB) && alloc(&dst.d_G, src.nb * BB) &&
+                    alloc(&dst.d_H, src.nb * BB) && alloc(&dst.d_h, src.Mp) && alloc(&dst.d_flag, 1);
+    if (!ok) {
+        spc_plan_free_clone(dst);
+        return CRT_ERR_ALLOC;
+    }
+    dst.ok = 1;
+    return 0;
+}
+
+void spc_plan_free_clone(SpcPlan& P)
+{
+    cudaFree(P.d_DF);
+    cudaFree(P.d_G);
+    cudaFree(P.d_H);
+    cudaFree(P.d_h);
+    cudaFree(P.d_flag);
+    P = SpcPlan{};
+}
+
 void launch_spc_factor(const SpcPlan& P, const double* cgfac, const double* smatm, double lam, cudaStream_t s)
 {
     const size_t BB = (size_t)P.B * P.B;

@@ -53,6 +53,12 @@ constexpr int SPC_MAX_B = 192;
 int spc_plan_build(SpcPlan& P, int M, int ltri, int nx, int nnb, const double* smatm, const int* nachbar,
                    std::string& why);
 void spc_plan_free(SpcPlan& P);
+// A plan with its own factor buffers (D/F, G, H, sweep vector, flag) that
+// shares `src`'s ordering and entry list (device pointers included), for a
+// second factor of the same S pattern (another lambda).  Freed with
+// spc_plan_free_clone, before `src` is freed.
+int spc_plan_clone(const SpcPlan& src, SpcPlan& dst);
+void spc_plan_free_clone(SpcPlan& P);
 
 // Assembles S from cgfac, lam and the device copy of smatm, and factors it.
 void launch_spc_factor(const SpcPlan& P, const double* cgfac, const double* smatm, double lam, cudaStream_t s);

@@ -187,9 +187,13 @@ int32_t crt_update(crt_ctx *ctx, const crt_cg_params *prm, const double *sigmaa,
  * src/update.f90 pass with cjggra / cjggdc on the same Jacobian; this call
  * runs nlam (1 .. 8) such updates at once, and every CG iteration reads J
  * once for all candidates.  Candidate b is crt_update with prm->lam =
- * lams[b] in the Jacobi form (prm->lam and prm->precond are ignored), from
- * the same sigmaa (NULL = the last crt_forward) and par (complex [manz],
- * not modified).  par_out: complex [nlam][manz], par + step * dpar_b.
+ * lams[b] (prm->lam is ignored) from the same sigmaa (NULL = the last
+ * crt_forward) and par (complex [manz], not modified), in the Jacobi form,
+ * or with prm->precond CRT_PRECOND_BLOCK (or _BLOCK_GNN: the learned
+ * correction is not batched) in the block form with one factor per
+ * candidate; if the block preconditioner is unavailable or any
+ * candidate's factor breaks down, the batch runs in the Jacobi form
+ * (crt_cg_info reports which).  par_out: complex [nlam][manz], par + step * dpar_b.
  * Optional (NULL to skip): dpar complex [nlam][manz], ncg [nlam],
  * bdpar [nlam]. */
 int32_t crt_update_lambdas(crt_ctx *ctx, const crt_cg_params *prm, int32_t nlam, const double *lams,

@@ -148,3 +148,31 @@ def test_lambda_candidates_reject_bad_arguments():
     got = ctx.update_lambdas(prm, np.array([10.0]), par)
     assert got["ncg"][0] > 0
     ctx.close()
+
+
+@pytest.mark.parametrize("form", ["complex", "ldc"])
+def test_lambda_candidates_block_form_equal_single_updates(form):
+    """Block-preconditioned batch: one factor of S per candidate (its own
+    cgfac and lambda), the candidates' factors and sweeps side by side; each
+    candidate reproduces crt_update in the block form."""
+    from crtomo_stable_b200.lib import PRECOND_BLOCK, Context
+    ldc = form == "ldc"
+    ctx, case, dat, wmatd, sig, nb, sm = _case(ldc=ldc, sig0=0.01 * np.exp(-0.01j) if ldc else 0.01 + 0j)
+    m = case["mesh"]
+    par = np.log(sig)
+    lams = np.array([10.0, 100.0, 1000.0])
+    for eps, ncgmax, rtol, dn in ((1e-4, m.elanz // 10, 1e-10, 0), (1e-12, 2000, 1e-4, 2)):
+        prm = Context.params(0.0, eps=eps, ncgmax=ncgmax, ldc=ldc, precond=PRECOND_BLOCK)
+        got = ctx.update_lambdas(prm, lams, par)
+        assert ctx.cg_info()[0] == PRECOND_BLOCK
+        for b, lam in enumerate(lams):
+            one = ctx.update(Context.params(lam, eps=eps, ncgmax=ncgmax, ldc=ldc, precond=PRECOND_BLOCK), par)
+            assert ctx.cg_info()[0] == PRECOND_BLOCK
+            assert abs(int(got["ncg"][b]) - one["ncg"]) <= dn, (eps, lam, got["ncg"][b], one["ncg"])
+            _close(got["dpar"][b], one["dpar"], rtol)
+    # and the batch agrees with its own Jacobi form at rel-res 1e-6
+    jac = ctx.update_lambdas(Context.params(0.0, eps=1e-12, ncgmax=5000, ldc=ldc), lams, par)
+    assert ctx.cg_info()[0] == 0
+    for b in range(len(lams)):
+        _close(got["dpar"][b], jac["dpar"][b], 1e-4)
+    ctx.close()
