@@ -287,11 +287,13 @@ class Inversion:
             rp += self.smatm[:, n] * par
         return float(np.sum((rp * np.conj(par)).real))
 
-    def first_step(self, eps: float = 1e-4, ncgmax: Optional[int] = None, step: float = 1.0):
-        """IT 0 and the first UP row of inv.ctr: forward at the starting
-        model, misfit, Jacobian, lam0, update, forward at the new model."""
-        if self.lam0 is None:
-            raise NotImplementedError("lam0 from blam0's Jacobian estimate is not wired up yet")
+    def _start(self):
+        """Forward at the starting model, the set-up polarity check, misfit
+        and Jacobian (src/inv.f90:426-519, :739-743).  Runs once per
+        Inversion: the polarity check edits the data it keeps."""
+        if getattr(self, "_started", False):
+            raise RuntimeError("the starting pass of this Inversion has already run")
+        self._started = True
         sig0 = self.start_model()
         ldc = self.cfg.ldc
         volt, sa0 = self.ctx.forward(sig0, ldc=ldc, mode=0)
@@ -307,6 +309,36 @@ class Inversion:
         self.ctx.jacobian(mode=1 if ldc else 0, copy=False)
         if np.any(vnr != d.vnr):
             self.ctx.set_configs(d.strnr, vnr)
+        return sig0, sa0, nrmsd0
+
+    def trial_lambdas(self, lams, eps: float = 1e-4, ncgmax: Optional[int] = None, step: float = 1.0,
+                      precond: int = 0):
+        """The lambda trials of src/inv.f90:769-912 for the first update, side
+        by side: after the starting pass, one crt_update_lambdas call gives
+        every candidate's model (1 .. 8 lambdas, one read of J per CG
+        iteration for all), and each model is forwarded for the misfit and
+        roughness the reference's lambda logic compares."""
+        sig0, sa0, nrmsd0 = self._start()
+        ldc = self.cfg.ldc
+        lam_ = np.asarray(lams, np.float64)
+        prm = Context.params(0.0, eps=eps, ncgmax=ncgmax or self.ncgmax, ldc=ldc, step=step, precond=precond)
+        par = np.log(sig0)
+        up = self.ctx.update_lambdas(prm, lam_, par, sigmaa=sa0)
+        trials = []
+        for b, lam in enumerate(lam_):
+            p = up["par"][b]
+            _, sa = self.ctx.forward(np.exp(p), ldc=ldc, mode=0)
+            trials.append(dict(lam=float(lam), ncg=int(up["ncg"][b]), bdpar=float(up["bdpar"][b]),
+                               nrmsd=self.misfit(sa)[0], rough=self.roughness(p), par=p, sigmaa=sa))
+        return dict(nrmsd0=nrmsd0, sigmaa0=sa0, trials=trials)
+
+    def first_step(self, eps: float = 1e-4, ncgmax: Optional[int] = None, step: float = 1.0):
+        """IT 0 and the first UP row of inv.ctr: forward at the starting
+        model, misfit, Jacobian, lam0, update, forward at the new model."""
+        if self.lam0 is None:
+            raise NotImplementedError("lam0 from blam0's Jacobian estimate is not wired up yet")
+        sig0, sa0, nrmsd0 = self._start()
+        ldc = self.cfg.ldc
         prm = Context.params(self.lam0, eps=eps, ncgmax=ncgmax or self.ncgmax, ldc=ldc, step=step)
         par = np.log(sig0)
         up = self.ctx.update(prm, par, sigmaa=sa0)

@@ -176,3 +176,33 @@ def test_lambda_candidates_block_form_equal_single_updates(form):
     for b in range(len(lams)):
         _close(got["dpar"][b], jac["dpar"][b], 1e-4)
     ctx.close()
+
+
+def test_inversion_lambda_trials_match_first_step():
+    """The driver's lambda trials on the golden `minimal` tomodir: the trial
+    at lam0 reproduces the first update (inv.ctr UP 1 is checked against
+    first_step elsewhere), and every trial's model is forwarded."""
+    import os
+    from crtomo_stable_b200 import inversion, io
+    base = os.path.join(os.path.dirname(__file__), "golden", "minimal")
+    cfg = inversion.read_crtomo_cfg(os.path.join(base, "exe", "crtomo.cfg"))
+    mesh = io.read_elem(os.path.join(base, "grid", "elem.dat"))
+    enr = io.read_elec(os.path.join(base, "grid", "elec.dat"))
+    data = inversion.error_model(io.read_volt(os.path.join(base, "mod", "volt.dat")), cfg)
+    inv1 = inversion.Inversion(mesh, enr, data, cfg)
+    ref = inv1.first_step()
+    inv1.close()
+    inv2 = inversion.Inversion(mesh, enr, data, cfg)
+    lam0 = inv2.lam0
+    res = inv2.trial_lambdas([lam0 / 10.0, lam0, lam0 * 10.0])
+    inv2.close()
+    assert res["nrmsd0"] == ref["nrmsd0"]
+    t = res["trials"][1]
+    assert t["lam"] == ref["lam"] and t["ncg"] == ref["ncg"]
+    np.testing.assert_allclose(t["par"], ref["par"], rtol=1e-10, atol=1e-10 * np.abs(ref["par"]).max())
+    for k in ("nrmsd", "rough"):
+        assert abs(t[k] / ref[k + ("1" if k == "nrmsd" else "")] - 1) < 1e-9
+    assert abs(t["bdpar"] / ref["bdpar"] - 1) < 1e-9
+    # a smaller lambda fits the data at least as well and is rougher
+    lo, hi = res["trials"][0], res["trials"][2]
+    assert lo["rough"] > t["rough"] > hi["rough"]
