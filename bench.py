@@ -313,7 +313,8 @@ def run_batch(args, ws, rank, local, pg):
             "dtype": "c64/c128", "data": "synthetic (seeded)",
             "config": {"workload": f"C4: {len(S)} instances, E {min(E)}-{max(E)} (sum {sum(E)}), "
                                    f"{sum(len(s.strnr) for s in S)} readings, {systems} band systems",
-                       "form": "complex64 band factorisation, two FP64 refinement steps, FP64 Jacobian stored complex64",
+                       "form": "complex64 band factorisation, adaptive FP64 refinement (at most 8 steps, to normwise "
+                               "backward error 1e-14), FP64 Jacobian stored complex64",
                        "workspace_bytes_per_instance": budget, "parallelism": f"replicas x{args.gpus}"},
             "build_s": build_s, "sequential_calls_s": seq_s,
             "panels": sorted({int(c.timings()["panel"]) for c in ctxs})}
@@ -504,11 +505,12 @@ def main():
                                        f"{N} readings, K={K}; one GN step from a homogeneous model "
                                        f"(forward {K * L} band systems + Jacobian + CG to rel-res 1e-6)",
                            "form": ("mixed: band systems assembled and scaled in FP64, factored and solved in "
-                                    "complex64, two FP64 iterative-refinement steps; Jacobian formed in FP64, stored "
+                                    "complex64, adaptive FP64 iterative refinement (at most 8 steps, each system to normwise backward "
+                                    "error 1e-14); Jacobian formed in FP64, stored "
                                     "complex64; CG with FP64 accumulation and dots, preconditioned by cgfac and the "
                                     "block-tridiagonal S^-1 (FP32) of the sparse part" if mixed["cg_form"] == 1 else
                                     "mixed; diagonal-PCG (block preconditioner unavailable)"),
-                           "refinement_steps": args.refine if args.refine is not None else 2,
+                           "refinement_steps": (f"at most {args.refine}" if args.refine is not None else "adaptive, at most 8"),
                            "cg_block": mixed["cg_block"], "cg_bandwidth": mixed["cg_bw"],
                            "cg_iterations": ncg, "lam": mixed["lam"],
                            "l2": "inputs larger than L2 (J alone is %.1f GB in complex64)" % (N * E * 8 / 1e9),

@@ -57,7 +57,12 @@ struct crt_ctx {
     int nent_rows = 0;         // gather entries per system (row_ptr[n])
     cd* d_aval = nullptr;      // [chunk][nent_rows] prepared FP64 entries (mixed form)
     size_t aval_chunk = 0;
-    int nref = 2;   // iterative-refinement steps of the complex64 forward
+    // iterative refinement of the complex64 forward: at most nref steps; a
+    // system stops once its componentwise backward error is at most ref_tau
+    int nref = 8;
+    double ref_tau = 1e-14;
+    unsigned long long* d_omega = nullptr;   // [2 steps][chunk * L][2] backward-error maxima
+    size_t omega_cap = 0;
     unsigned char* d_dflag = nullptr;
     cd* d_dval = nullptr;
     int* d_status = nullptr;    // [max(K*L, K) + 8] per-system errnr; [last] global
@@ -339,7 +344,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl};
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (SpcPlan& c : ctx->spc_c) spc_plan_free_clone(c);
@@ -647,6 +652,14 @@ int run_forward(crt_ctx* ctx)
         ctx->lws_slot_bytes = slot_bytes;
         ctx->chunk = chunk;
     }
+    if (std::is_same<T, cf>::value && ctx->omega_cap < (size_t)ctx->chunk * L) {
+        if (ctx->capture) return set_err(ctx, CRT_ERR_ARG, "captured forward without a prepared workspace");
+        if (ctx->d_omega) cudaFree(ctx->d_omega);
+        ctx->d_omega = nullptr;
+        ctx->omega_cap = 0;
+        CK(cudaMalloc((void**)&ctx->d_omega, 4 * sizeof(unsigned long long) * (size_t)ctx->chunk * L));
+        ctx->omega_cap = (size_t)ctx->chunk * L;
+    }
     chunk = ctx->chunk;
     ctx->tev_n = 0;
     ctx->fwd_marks.clear();
@@ -754,15 +767,23 @@ int run_forward(crt_ctx* ctx)
         ctx->launches++;
         if constexpr (std::is_same<T, cf>::value) {
             // iterative refinement of the complex64 solution: FP64 residual of
-            // the scaled system, complex64 correction solve, FP64 update of kpot
+            // the scaled system and its componentwise backward error, complex64
+            // correction solve, FP64 update of kpot; a system whose backward
+            // error has reached ref_tau (the FP64 floor) takes no further steps
             for (int it = 0; it < ctx->nref; ++it) {
+                unsigned long long* om_cur = ctx->d_omega + (size_t)(it & 1) * 2 * ctx->omega_cap;
+                const unsigned long long* om_prev =
+                    it ? ctx->d_omega + (size_t)((it - 1) & 1) * 2 * ctx->omega_cap : nullptr;
+                CK(cudaMemsetAsync(om_cur, 0, 2 * sizeof(unsigned long long) * S.nsys, ctx->st));
                 mk.ref.push_back(tev_rec(ctx));
                 launch_band_residual<T>(A, S.sys0, S.nsys, S.factor_of_sys_div, ctx->d_up_ptr, ctx->d_up_ent,
-                                        ctx->d_up_row, ctx->d_kpot, scr, ctx->st);
+                                        ctx->d_up_row, ctx->d_kpot, scr, om_prev, om_cur, ctx->ref_tau, ctx->st);
                 mk.ref.push_back(tev_rec(ctx));
                 SolveArgs<T> C = S;
                 C.rhs = scr;
                 C.accumulate = 1;
+                C.skip_omega = om_cur;
+                C.skip_tau = ctx->ref_tau;
                 launch_band_solve_with_scratch<T>(C, scr, ctx->st);
                 mk.ref.push_back(tev_rec(ctx));
                 ctx->launches += 2;

@@ -276,6 +276,9 @@ __global__ void __launch_bounds__(NT, NT == 128 ? 2 * SolveOcc<T>::v : SolveOcc<
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = A.n, W = A.W, mb = A.mb;
     const int b = blockIdx.x, sys = A.sys0 + b;
+    // a refinement correction of a system already at the FP64 floor is skipped
+    // (uniform over the CTA, before any barrier)
+    if (A.skip_omega && refine_done(A.skip_omega, b, A.skip_tau)) return;
     const int slot = b / A.factor_of_sys_div;
     // solve systems are always (k, l) pairs, sys = k * L + l
     const int k = sys / A.L, l = sys % A.L;

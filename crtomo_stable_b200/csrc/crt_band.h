@@ -46,7 +46,21 @@ struct SolveArgs {
     int* status;
     const T* rhs;            // [b][n] explicit right-hand sides (refinement), or NULL
     int accumulate;          // 1: kpot += the solution's contribution instead of kpot =
+    // refinement: system b is skipped once refine_done(skip_omega, b,
+    // skip_tau); NULL solves every system
+    const unsigned long long* skip_omega;
+    double skip_tau;
 };
+
+// Normwise backward error of refinement system b from om[2b] = max_r |r_r|
+// and om[2b + 1] = max_r (sum_c |a_rc| |z_c| + |b_r|) (bits of non-negative
+// doubles, |x| = |Re x| + |Im x|): converged when the ratio is at most tau.
+__device__ __forceinline__ bool refine_done(const unsigned long long* om, int b, double tau)
+{
+    const double r = __longlong_as_double((long long)om[2 * b]);
+    const double d = __longlong_as_double((long long)om[2 * b + 1]);
+    return r <= tau * d;
+}
 
 template <typename T> void launch_band_factor(const BandArgs<T>& a, cudaStream_t st);
 // Launch configuration of the panel-blocked variant: the panel width (4, 8
@@ -72,9 +86,15 @@ template <typename T> void launch_band_prep(const BandArgs<T>& a, cudaStream_t s
 // FP64 residual b^ - A^ z of the scaled systems for a refinement step, z from
 // kpot, A^ from the entries the preparation pass kept in a.aval; solve
 // systems sys0 .. sys0+nsolve-1, factor slot b / div; stored as T.
+// Also the two maxima of each system's normwise backward error (see
+// refine_done) into om_cur[2b], om_cur[2b + 1] (atomic maxima over the rows;
+// om_cur zeroed beforehand).  A system that refine_done(om_prev, b, tau)
+// reports converged at an earlier step (om_prev NULL: none) is not
+// recomputed and its maxima carry over into om_cur.
 template <typename T>
 void launch_band_residual(const BandArgs<T>& a, int sys0, int nsolve, int div, const int* up_ptr, const int* up_ent,
-                          const int* up_row, const cd* kpot, T* rout, cudaStream_t st);
+                          const int* up_row, const cd* kpot, T* rout, const unsigned long long* om_prev,
+                          unsigned long long* om_cur, double tau, cudaStream_t st);
 // scratch: one n-vector per launched system (may alias the fused y workspace).
 template <typename T> void launch_band_solve_with_scratch(const SolveArgs<T>& a, T* scratch, cudaStream_t st);
 template <typename T> size_t band_factor_smem(int W);

@@ -198,15 +198,25 @@ __global__ void k_band_prep_rows(BandArgs<T> A)
 // transposed list the upper part.  A Dirichlet row is the identity row.
 // The residual is stored in T for the correction solve.  Solve system b is
 // (k, l) = (sys0 + b) / L, % L, its factor slot b / div.
+__device__ __forceinline__ double cabs1(cd v) { return fabs(v.x) + fabs(v.y); }
+
 template <typename T>
 __global__ void k_band_residual(BandArgs<T> A, int sys0, int nsolve, int div, const int* __restrict__ up_ptr,
                                 const int* __restrict__ up_ent, const int* __restrict__ up_row,
-                                const cd* __restrict__ kpot, T* rout)
+                                const cd* __restrict__ kpot, T* rout, const unsigned long long* om_prev,
+                                unsigned long long* om_cur, double tau)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n = A.n;
     if (idx >= (long long)nsolve * n) return;
     const int b = (int)(idx / n), r = (int)(idx % n), sys = sys0 + b;
+    if (om_prev && refine_done(om_prev, b, tau)) {   // converged at an earlier step
+        if (r == 0) {
+            om_cur[2 * b] = om_prev[2 * b];
+            om_cur[2 * b + 1] = om_prev[2 * b + 1];
+        }
+        return;
+    }
     const int l = sys % A.L, slot = b / div;
     const double* fk = A.fakws + (size_t)slot * n;
     const cd* kp = kpot + (size_t)sys * n;
@@ -216,14 +226,49 @@ __global__ void k_band_residual(BandArgs<T> A, int sys0, int nsolve, int div, co
         return cd{-kp[c].x * inv, -kp[c].y * inv};
     };
     cd acc{0.0, 0.0};
+    double den = 0.0;   // sum_c |a_rc| |z_c|
     if (A.dflag[r]) {
         acc = zval(r);
+        den = cabs1(acc);
     } else {
-        for (int e = A.row_ptr[r]; e < A.row_ptr[r + 1]; ++e) acc += av[e] * zval(r - A.ent_d[e]);
-        for (int q = up_ptr[r]; q < up_ptr[r + 1]; ++q) acc += av[up_ent[q]] * zval(up_row[q]);
+        for (int e = A.row_ptr[r]; e < A.row_ptr[r + 1]; ++e) {
+            const cd a = av[e], zc = zval(r - A.ent_d[e]);
+            acc += a * zc;
+            den += cabs1(a) * cabs1(zc);
+        }
+        for (int q = up_ptr[r]; q < up_ptr[r + 1]; ++q) {
+            const cd a = av[up_ent[q]], zc = zval(up_row[q]);
+            acc += a * zc;
+            den += cabs1(a) * cabs1(zc);
+        }
     }
     const cd bb = scale(rhs_entry_b<cd>(r, A.enr0[l], A.lsink, A.nsink0, A.dflag, A.dval, nullptr), fk[r]);
-    rout[(size_t)b * n + r] = narrow<T>(bb - acc);
+    const cd res = bb - acc;
+    rout[(size_t)b * n + r] = narrow<T>(res);
+    if (om_cur) {
+        // max |r_r| and max (sum_c |a_rc||z_c| + |b_r|) of the system: a warp
+        // whose lanes all hold rows of one system reduces first (one atomic
+        // per warp and quantity instead of one per row)
+        unsigned long long vr = (unsigned long long)__double_as_longlong(cabs1(res));
+        unsigned long long vd = (unsigned long long)__double_as_longlong(den + cabs1(bb));
+        const unsigned mask = __activemask();
+        const int lane = threadIdx.x & 31;
+        const int b0 = __shfl_sync(mask, b, __ffs(mask) - 1);
+        if (mask == 0xffffffffu && __all_sync(mask, b == b0)) {
+            for (int o = 16; o > 0; o >>= 1) {
+                const unsigned long long ur = __shfl_xor_sync(mask, vr, o), ud = __shfl_xor_sync(mask, vd, o);
+                vr = ur > vr ? ur : vr;
+                vd = ud > vd ? ud : vd;
+            }
+            if (lane == 0) {
+                atomicMax(&om_cur[2 * b], vr);
+                atomicMax(&om_cur[2 * b + 1], vd);
+            }
+        } else {
+            atomicMax(&om_cur[2 * b], vr);
+            atomicMax(&om_cur[2 * b + 1], vd);
+        }
+    }
 }
 
 // Four consecutive window-row entries of a panel column (16-byte aligned).
@@ -750,11 +795,12 @@ int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st)
 
 template <typename T>
 void launch_band_residual(const BandArgs<T>& a, int sys0, int nsolve, int div, const int* up_ptr, const int* up_ent,
-                          const int* up_row, const cd* kpot, T* rout, cudaStream_t st)
+                          const int* up_row, const cd* kpot, T* rout, const unsigned long long* om_prev,
+                          unsigned long long* om_cur, double tau, cudaStream_t st)
 {
     const long long rows = (long long)nsolve * a.n;
     k_band_residual<T><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(a, sys0, nsolve, div, up_ptr, up_ent, up_row,
-                                                                     kpot, rout);
+                                                                     kpot, rout, om_prev, om_cur, tau);
 }
 
 template bool band_blk_fits<double>(int);
@@ -770,4 +816,5 @@ template int band_panel<double>(const BandArgs<double>&, bool, cudaStream_t);
 template int band_panel<cd>(const BandArgs<cd>&, bool, cudaStream_t);
 template int band_panel<cf>(const BandArgs<cf>&, bool, cudaStream_t);
 template void launch_band_residual<cf>(const BandArgs<cf>&, int, int, int, const int*, const int*, const int*,
-                                       const cd*, cf*, cudaStream_t);
+                                       const cd*, cf*, const unsigned long long*, unsigned long long*, double,
+                                       cudaStream_t);

@@ -553,10 +553,11 @@ def test_jacobian_gram_and_direct_kernels_agree(name, mode, monkeypatch):
 @pytest.mark.parametrize("name", ["TestModInv", "minimal", "mixed_surf", "grid_decoupling"])
 def test_mixed_form_forward_is_refined_to_fp64(name):
     """The mixed form factors the complex systems in complex64 and refines in
-    FP64: with the default two steps the potentials and voltages agree with
-    the FP64 oracle to 1e-9 (the stated target is 1e-6), one step already
-    reaches 1e-6; without refinement the complex64 solution alone is off by
-    far more than FP64 rounding."""
+    FP64: with at most two steps the potentials and voltages of these small
+    meshes agree with the FP64 oracle to 1e-9 (the stated target is 1e-6),
+    one step already reaches 1e-6; without refinement the complex64 solution
+    alone is off by far more than FP64 rounding.  (The default allows up to
+    8 adaptive steps, which the benchmark mesh needs: see the C5 test.)"""
     from crtomo_stable_b200.lib import PREC_MIXED, Context
     case = load_forward_case(name)
     m = case["mesh"]
@@ -579,3 +580,28 @@ def test_mixed_form_forward_is_refined_to_fp64(name):
     assert errs[2][0] <= 1e-9 and errs[2][1] <= 1e-9
     assert errs[1][0] <= 1e-6 and errs[1][1] <= 1e-6
     assert errs[0][0] > 10 * errs[2][0]
+
+
+def test_mixed_form_default_refinement_on_the_benchmark_mesh():
+    """On the 60k-triangle benchmark survey (C5: n = 30,444, mb = 129, 128
+    electrodes, 16 wavenumbers) the low-wavenumber systems are
+    ill-conditioned enough that each refinement step gains only about one
+    digit; the default adaptive refinement (up to 8 steps, each system
+    until its normwise backward error reaches 1e-14) must still meet the
+    1e-6 target against the FP64 form: every reading's voltage to 1e-6
+    relative, the potentials to 1e-6 of their maximum."""
+    from crtomo_stable_b200 import synth
+    from crtomo_stable_b200.lib import PREC_FP64, PREC_MIXED, Context
+    s = synth.CONFIGS["C5"]()
+    rho0 = float(np.exp(np.mean(np.log(np.abs(1.0 / s.sigma)))))
+    sig = np.full(s.mesh.elanz, 1.0 / rho0 + 0j)   # the GN step's starting model
+    c = Context(s.mesh, s.enr, s.strnr, s.vnr, precision=PREC_FP64)
+    v64, _, k64 = c.forward(sig, want_kpot=True)
+    c.close()
+    c = Context(s.mesh, s.enr, s.strnr, s.vnr, precision=PREC_MIXED)
+    v, _, k = c.forward(sig, want_kpot=True)
+    c.close()
+    ek = np.abs(k - k64).max() / np.abs(k64).max()
+    ev = (np.abs(v - v64) / np.abs(v64)).max()
+    print(f"\nC5 default refinement: potentials {ek:.1e} of max, voltages {ev:.1e} per reading")
+    assert ek <= 1e-6 and ev <= 1e-6
