@@ -314,6 +314,13 @@ extern "C" int32_t crt_set_refinement(crt_ctx* ctx, int32_t steps)
     return CRT_OK;
 }
 
+extern "C" int32_t crt_set_refinement_tol(crt_ctx* ctx, double tau)
+{
+    if (!ctx || !(tau >= 0.0) || !(tau < 1.0)) return CRT_ERR_ARG;
+    ctx->ref_tau = tau;
+    return CRT_OK;
+}
+
 extern "C" int32_t crt_last_timings_ex(const crt_ctx* ctx, double* ms, int32_t n)
 {
     if (!ctx || !ms || n < 0) return CRT_ERR_ARG;

@@ -67,7 +67,7 @@ EXPORTS = [
     "crt_set_data", "crt_set_configs", "crt_update", "crt_update_lambdas", "crt_gn_step", "crt_set_model", "crt_gn_step_device",
     "crt_get_model", "crt_model_backup", "crt_last_timings", "crt_launch_count", "crt_dmisft",
     "crt_voltages_noalloc", "crt_cg_info", "crt_rcm_order", "crt_last_timings_ex",
-    "crt_set_refinement", "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
+    "crt_set_refinement", "crt_set_refinement_tol", "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
     "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad", "crt_batch_create",
     "crt_batch_destroy", "crt_batch_error", "crt_batch_set_models", "crt_batch_run", "crt_batch_status",
     "crt_batch_results", "crt_set_workspace_limit",
@@ -130,6 +130,8 @@ def load(path: str = LIB_PATH):
     L.crt_last_timings.restype = C.c_int32
     L.crt_set_refinement.argtypes = [vp, C.c_int32]
     L.crt_set_refinement.restype = C.c_int32
+    L.crt_set_refinement_tol.argtypes = [vp, C.c_double]
+    L.crt_set_refinement_tol.restype = C.c_int32
     L.crt_batch_create.argtypes = [P(vp), C.c_int32, C.c_int32, C.c_int32, i32p]
     L.crt_batch_create.restype = vp
     L.crt_batch_destroy.argtypes = [vp]
@@ -455,6 +457,10 @@ class Context:
 
     def set_refinement(self, steps):
         self._check(self.L.crt_set_refinement(self.h, int(steps)), "crt_set_refinement")
+
+    def set_refinement_tol(self, tau):
+        """Normwise backward error at which a system's refinement stops."""
+        self._check(self.L.crt_set_refinement_tol(self.h, float(tau)), "crt_set_refinement_tol")
 
     def set_workspace_limit(self, nbytes):
         """Upper bound of the band-factor workspace (0: default)."""

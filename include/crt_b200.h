@@ -106,13 +106,17 @@ typedef struct {
 /* Steps of FP64 iterative refinement after the complex64 factorisation of
  * the mixed form: at most `steps` (default 8; 0 leaves the complex64
  * solution).  Each step forms the residual of the scaled system in FP64
- * (from the FP64 entries of the prepared matrix) and its componentwise
- * backward error max_r |r_r| / (sum_c |a_rc| |z_c| + |b_r|), and adds a
- * complex64 correction solve; a system whose backward error is at most
- * 1e-14 (the FP64 floor) takes no further steps, so well-conditioned
- * systems stop after one or two while the ill-conditioned low-wavenumber
- * systems keep refining.  No reference counterpart. */
+ * (from the FP64 entries of the prepared matrix) and its normwise
+ * backward error max_r |r_r| / max_r (sum_c |a_rc| |z_c| + |b_r|), and adds
+ * a complex64 correction solve; a system whose backward error is at most
+ * the tolerance (crt_set_refinement_tol, default 1e-14, the FP64 floor)
+ * takes no further steps, so well-conditioned systems stop after a few
+ * while the ill-conditioned low-wavenumber systems keep refining.  No
+ * reference counterpart. */
 int32_t crt_set_refinement(crt_ctx *ctx, int32_t steps);
+/* Normwise backward error at which a system's refinement stops (default
+ * 1e-14; 0 runs every step for every system).  No reference counterpart. */
+int32_t crt_set_refinement_tol(crt_ctx *ctx, double tau);
 
 /* Creates a context on `device`: uploads the mesh, builds the gather lists
  * of the streamed assembly, and evaluates precal on the device unless the
