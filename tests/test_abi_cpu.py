@@ -96,3 +96,18 @@ def test_library_resolves_its_own_templates():
     out = subprocess.run([nm, "-D", "--undefined-only", lib], capture_output=True, text=True).stdout
     own = [ln for ln in out.splitlines() if "launch_" in ln or "crt_" in ln or "gnn_" in ln or "spc_" in ln]
     assert not own, own
+
+
+def test_null_context_is_rejected_before_any_device_work():
+    """Entry points given no context return errnr 3 (inconsistent input)
+    without touching a device: the refinement controls and the batched
+    lambda update."""
+    from crtomo_stable_b200 import lib
+    L = lib.load()
+    assert L.crt_set_refinement(None, 2) == 3
+    assert L.crt_set_refinement_tol(None, 1e-14) == 3
+    lams = np.array([1.0, 10.0])
+    par = np.zeros(4, np.complex128)
+    out = np.zeros(8, np.complex128)
+    assert L.crt_update_lambdas(None, None, 2, lams.ctypes.data_as(C.POINTER(C.c_double)), None,
+                                C.c_void_p(par.ctypes.data), C.c_void_p(out.ctypes.data), None, None, None) == 3
