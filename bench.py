@@ -38,16 +38,16 @@ METRIC = "GN-step wall time, learned-PCG/FP32-refined vs plain CG on B200 at rel
 REF_NCG = {"C5": 1589}
 
 # DRAM bytes (read + write) of the band-factor kernel per band entry
-# n (mb + 1) of a complex128 system, from the ncu capture in
-# profiles/k_band_factor_blk_C3.md (4.186 GB for 63 C3 systems: the prepared
-# matrix read once and L written once).
+# n (mb + 1) of a complex128 system, from an ncu capture of the factor on
+# the 200 x 100 quadrilateral survey (mb = 102): 4.186 GB for 63 systems,
+# the prepared matrix read once and L written once.
 FACTOR_TRAFFIC_BYTES_PER_ENTRY = 31.8
 
 # FMA pipes of a B200 SM (non-tensor): 64 FP64 / 128 FP32 FMA per clock,
 # the rooflines of the complex128 / complex64 band factorisation.
 FP64_FMA_PER_CLK_SM = 64
 FP32_FMA_PER_CLK_SM = 128
-# complex64: 4.164 GB for 125 C3 systems (profiles/k_band_factor_blk_C3.md)
+# complex64: 4.164 GB for 125 systems of the same survey
 FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 = 15.9
 
 
@@ -459,7 +459,7 @@ def main():
     # (64 FMA/clk/SM) otherwise.  Algorithmic work per system 4 n mb^2 flops
     # (n mb^2 / 2 complex MACs of 8 flops); per launch = systems per launch x
     # that.  Traffic: the prepared matrix read once and L written once,
-    # bytes per band entry from the ncu captures in profiles/.
+    # bytes per band entry from the ncu captures named above.
     c64 = mixed["c64"]
     nsys = K * L   # mixed boundaries: one factorisation per (k, l)
     flops = 4.0 * n * mb * mb * nsys

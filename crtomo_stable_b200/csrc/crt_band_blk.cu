@@ -526,7 +526,6 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             if (fuse) bsl[x] = bx;
         }
         __syncthreads();
-        // PROBE0
         // ---- phase 3a: the trailing update of the next panel's diagonal
         // tiles, one entry per thread, so that its block can be factored
         // while the rest of the window is updated.
@@ -553,7 +552,6 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             }
         }
         __syncthreads();
-        // PROBE1
         // ---- phase 3b: warp 0 factors the next diagonal block; warps 1..
         // update the rest of the window by the rank-PB product L_x L_y^T on
         // 4 x 4 tiles (the panel columns read from pan) and then write the
@@ -616,8 +614,6 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         }
         __syncthreads();
-        // PROBE2
-        // PROBE3
     }
     if (tid == 0 && s_err) A.status[sys] = s_err;
 }

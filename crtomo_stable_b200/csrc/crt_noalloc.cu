@@ -145,6 +145,13 @@ extern "C" int32_t crt_voltages_noalloc(const double* kpot, const double* kwnwi,
                      (int)eanz, CRT_NOALLOC_MAX_EANZ);
         return CRT_ERR_ARG;
     }
+    // an error left pending by earlier, unrelated work is reported as such
+    // (and left in place for its owner) rather than charged to this call
+    if (cudaError_t pre = cudaPeekAtLastError(); pre != cudaSuccess) {
+        std::fprintf(stderr, "crt_voltages_noalloc: a CUDA error was pending before the call: %s\n",
+                     cudaGetErrorString(pre));
+        return CRT_ERR_CUDA;
+    }
     NoallocSymbols sym;
     if (int e = noalloc_symbols(&sym)) return e;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -156,6 +163,7 @@ extern "C" int32_t crt_voltages_noalloc(const double* kpot, const double* kwnwi,
     k_noalloc_volt<<<(nanz + 255) / 256, 256, 0, st>>>(sym.hel, strnr, vnr, kfak, eanz, nanz, ldc, mode,
                                                        reinterpret_cast<cd*>(volt), reinterpret_cast<cd*>(sigmaa),
                                                        sym.status);
+    // nothing was pending on entry, so a launch error seen here is this call's
     if (cudaGetLastError() != cudaSuccess) return CRT_ERR_CUDA;
     int status = 0;
     if (cudaMemcpyAsync(&status, sym.status, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess) return CRT_ERR_CUDA;

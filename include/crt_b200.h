@@ -307,7 +307,9 @@ int32_t crt_rcm_order(int32_t n, const int32_t *xadj, const int32_t *adj, int32_
  * strnr / vnr [nanz], kfak [nanz] or NULL, outputs volt / sigmaa complex
  * [nanz].  stream: a cudaStream_t (NULL = legacy default stream); the call
  * synchronises it before returning the errnr (82 zero voltage, 46 / 29 bad
- * electrode numbers, 3 bad arguments).  It calls no cudaMalloc / cudaFree:
+ * electrode numbers, 3 bad arguments; 200 when a CUDA error from earlier
+ * work was already pending on entry, which is left pending for its owner
+ * and named on stderr).  It calls no cudaMalloc / cudaFree:
  * its scratch (the eanz x eanz table of electrode potentials) is a static
  * device array for at most 512 electrodes (4 MiB per GPU, held until
  * exit); eanz > 512 is rejected with errnr 3 and a message on stderr.  The
