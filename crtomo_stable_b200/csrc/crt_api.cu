@@ -65,6 +65,13 @@ struct crt_ctx {
     size_t omega_cap = 0;
     unsigned char* d_dflag = nullptr;
     cd* d_dval = nullptr;
+    // randb2 right-hand-side moves of non-zero boundary.dat values: the rows
+    // coupled to such a node, per row the gather entries and the nodes
+    // (CSR), and the per-system moves of the current chunk [chunk][n]
+    int ndc_rows = 0;
+    int *d_dc_rows = nullptr, *d_dc_ptr = nullptr, *d_dc_ent = nullptr, *d_dc_node = nullptr;
+    cd* d_bdir = nullptr;
+    size_t bdir_chunk = 0;
     int* d_status = nullptr;    // [max(K*L, K) + 8] per-system errnr; [last] global
     int nstatus = 0;
 
@@ -351,7 +358,8 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega};
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega,
+                    ctx->d_dc_rows, ctx->d_dc_ptr, ctx->d_dc_ent, ctx->d_dc_node, ctx->d_bdir};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (SpcPlan& c : ctx->spc_c) spc_plan_free_clone(c);
@@ -442,7 +450,7 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
         }
     }
     std::vector<int> et(m.elanz), enk(m.elanz), mixed_rel;
-    std::vector<unsigned char> dflag(ctx->n, 0);
+    std::vector<unsigned char> dflag(ctx->n, 0), t13(ctx->n, 0);
     std::vector<cd> dval(ctx->n, cd{0.0, 0.0});
     {
         int row = 0;
@@ -466,7 +474,11 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
                     mixed_rel.push_back(rel);
                 } else if (m.typ[t] == 13) {
                     ctx->lrandb = 1;
-                    for (int q = 0; q < m.selanz[t]; ++q) dflag[m.nrel[(size_t)q * m.ntot + row] - 1] = 1;
+                    for (int q = 0; q < m.selanz[t]; ++q) {
+                        const int node = m.nrel[(size_t)q * m.ntot + row] - 1;
+                        dflag[node] = 1;
+                        t13[node] = 1;
+                    }
                 }
             }
     }
@@ -476,18 +488,43 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
         ctx->lrandb2 = 1;
         for (int i = 0; i < sv->rwdanz; ++i) {
             int node = sv->rwdnr[i] - 1;
+            if (node < 0 || node >= ctx->n)
+                return fail(ctx, set_err(ctx, CRT_ERR_ARG, "boundary.dat node number out of range"));
             dflag[node] = 2;
             dval[node] = cd{sv->rwd[2 * i], sv->rwd[2 * i + 1]};
         }
-        // boundary.dat couplings moved to the RHS are not streamed yet
-        bool nonzero = false;
-        for (int i = 0; i < sv->rwdanz; ++i) nonzero |= (sv->rwd[2 * i] != 0.0 || sv->rwd[2 * i + 1] != 0.0);
-        if (nonzero)
-            return fail(ctx, set_err(ctx, CRT_ERR_UNSUPPORTED, "non-zero boundary.dat values are not supported yet"));
     }
     AssemblyLists lists;
     int e = build_assembly_lists(m, lists);
     if (e) return fail(ctx, set_err(ctx, e, "band width violated in kompab (errnr 19)"));
+    // randb2 (src/randb2.f90:39-79): a free row r coupled to a boundary.dat
+    // node c with a non-zero value receives value(c) a(r, c) on its right-hand
+    // side.  randb runs first and has zeroed the rows and columns of the
+    // type-13 nodes, so a boundary.dat node that is also a type-13 node
+    // couples to nothing, and type-13 rows keep b = 0.
+    std::vector<int> dc_rows, dc_ptr(1, 0), dc_ent, dc_node;
+    if (ctx->lrandb2) {
+        std::vector<std::vector<std::pair<int, int>>> per_row(ctx->n);
+        auto coupled = [&](int c) { return dflag[c] == 2 && !t13[c] && (dval[c].x != 0.0 || dval[c].y != 0.0); };
+        for (int r = 0; r < ctx->n; ++r)
+            for (int q = lists.row_ptr[r]; q < lists.row_ptr[r + 1]; ++q) {
+                const int d = lists.ent_d[q];
+                if (d == 0) continue;
+                const int c = r - d;   // entry (r, c) = (c, r), c < r
+                if (dflag[r] == 0 && coupled(c)) per_row[r].push_back({q, c});
+                if (dflag[c] == 0 && coupled(r)) per_row[c].push_back({q, r});
+            }
+        for (int r = 0; r < ctx->n; ++r) {
+            if (per_row[r].empty()) continue;
+            dc_rows.push_back(r);
+            for (auto& pr : per_row[r]) {
+                dc_ent.push_back(pr.first);
+                dc_node.push_back(pr.second);
+            }
+            dc_ptr.push_back((int)dc_ent.size());
+        }
+        ctx->ndc_rows = (int)dc_rows.size();
+    }
 
     std::vector<int> snr0(ctx->n), enr0(ctx->L);
     for (int i = 0; i < ctx->n; ++i) snr0[i] = mesh->snr[i] - 1;
@@ -525,6 +562,11 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
               upload_upper_lists(ctx, lists) && (ctx->nent_rows = lists.row_ptr.back(), true) &&
               upload(ctx, &ctx->d_dflag, dflag.data(), dflag.size()) &&
               upload(ctx, &ctx->d_dval, dval.data(), dval.size());
+    if (ok && ctx->ndc_rows > 0)
+        ok = upload(ctx, &ctx->d_dc_rows, dc_rows.data(), dc_rows.size()) &&
+             upload(ctx, &ctx->d_dc_ptr, dc_ptr.data(), dc_ptr.size()) &&
+             upload(ctx, &ctx->d_dc_ent, dc_ent.data(), dc_ent.size()) &&
+             upload(ctx, &ctx->d_dc_node, dc_node.data(), dc_node.size());
     if (!ok) return fail(ctx, CRT_ERR_ALLOC);
     ctx->nstatus = std::max(ctx->K * ctx->L, ctx->K) + 8;
     if (!dalloc(ctx, &ctx->d_status, (size_t)ctx->nstatus)) return fail(ctx, CRT_ERR_ALLOC);
@@ -667,6 +709,17 @@ int run_forward(crt_ctx* ctx)
         CK(cudaMalloc((void**)&ctx->d_omega, 4 * sizeof(unsigned long long) * (size_t)ctx->chunk * L));
         ctx->omega_cap = (size_t)ctx->chunk * L;
     }
+    if (ctx->ndc_rows > 0 && ctx->bdir_chunk < (size_t)ctx->chunk) {
+        if (ctx->capture) return set_err(ctx, CRT_ERR_ARG, "captured forward without a prepared workspace");
+        if (ctx->d_bdir) cudaFree(ctx->d_bdir);
+        ctx->d_bdir = nullptr;
+        ctx->bdir_chunk = 0;
+        CK(cudaMalloc((void**)&ctx->d_bdir, sizeof(cd) * (size_t)n * ctx->chunk));
+        // rows without couplings stay zero; the coupled rows are rewritten
+        // for every chunk
+        CK(cudaMemsetAsync(ctx->d_bdir, 0, sizeof(cd) * (size_t)n * ctx->chunk, ctx->st));
+        ctx->bdir_chunk = ctx->chunk;
+    }
     chunk = ctx->chunk;
     ctx->tev_n = 0;
     ctx->fwd_marks.clear();
@@ -698,7 +751,7 @@ int run_forward(crt_ctx* ctx)
         A.sigma = ctx->d_sigma;
         A.dflag = ctx->d_dflag;
         A.dval = ctx->d_dval;
-        A.bdir = nullptr;
+        A.bdir = ctx->ndc_rows > 0 ? ctx->d_bdir : nullptr;
         A.enr0 = ctx->d_enr0;
         A.lsink = ctx->lsink;
         A.nsink0 = ctx->nsink - 1;
@@ -719,6 +772,11 @@ int run_forward(crt_ctx* ctx)
         }
         crt_ctx::FwdMark mk{};
         mk.e0 = tev_rec(ctx);
+        if (ctx->ndc_rows > 0) {
+            launch_band_dir_rhs<T>(A, ctx->ndc_rows, ctx->d_dc_rows, ctx->d_dc_ptr, ctx->d_dc_ent, ctx->d_dc_node,
+                                   ctx->d_bdir, ctx->st);
+            ctx->launches++;
+        }
         {
             const char* fv = std::getenv("CRT_B200_FACTOR");
             const bool force_v0 = fv && std::strcmp(fv, "v0") == 0;

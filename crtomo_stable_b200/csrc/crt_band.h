@@ -83,6 +83,12 @@ template <typename T> bool band_blk_fits(int mb);
 // Preparation pass of the panel-blocked factor: assembled, Dirichlet-edited
 // and scaled rows written row-packed into a.Lws, scaling factors into a.fakws.
 template <typename T> void launch_band_prep(const BandArgs<T>& a, cudaStream_t st);
+// Right-hand-side moves of non-zero boundary.dat values (randb2 / randbdc2)
+// for a's systems: bdir[b][rows[i]] = sum_q value(node[q]) a(ent[q]) over
+// q in [ptr[i], ptr[i+1]); the other rows of bdir are left as they are.
+template <typename T>
+void launch_band_dir_rhs(const BandArgs<T>& a, int nrows, const int* rows, const int* ptr, const int* ent,
+                         const int* node, cd* bdir, cudaStream_t st);
 // FP64 residual b^ - A^ z of the scaled systems for a refinement step, z from
 // kpot, A^ from the entries the preparation pass kept in a.aval; solve
 // systems sys0 .. sys0+nsolve-1, factor slot b / div; stored as T.

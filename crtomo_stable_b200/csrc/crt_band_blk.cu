@@ -143,6 +143,29 @@ __global__ void k_band_prep_diag(BandArgs<T> A)
     if (A.aval && e0 >= 0) A.aval[(size_t)b * A.aval_stride + e0] = Sc<WT>::to_cd(dn);
 }
 
+// randb2 / randbdc2 (src/randb2.f90:39-79): the couplings of the prescribed
+// boundary.dat values move to the right-hand side of the free rows before
+// scaling, b(r) += value(c) a(r, c) for every boundary.dat node c coupled to
+// row r, with a the assembled (unscaled, FP64) entry of the system.  One
+// thread per (system, row with couplings); couplings listed per row
+// (ptr / ent / node: the gather entry of a(max(r,c), |r-c|) and c).  The
+// real path takes the real part of the values through Sc<double>::from.
+template <typename T>
+__global__ void k_band_dir_rhs(BandArgs<T> A, int nrows, const int* __restrict__ rows, const int* __restrict__ ptr,
+                               const int* __restrict__ ent, const int* __restrict__ node, cd* __restrict__ bdir)
+{
+    using WT = typename Wide<T>::type;
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)A.nsys * nrows) return;
+    const int b = (int)(idx / nrows), i = (int)(idx % nrows), sys = A.sys0 + b;
+    int k, l;
+    sys_kl(A, sys, k, l);
+    cd s{0.0, 0.0};
+    for (int q = ptr[i]; q < ptr[i + 1]; ++q)
+        s += Sc<WT>::to_cd(assemble_entry_w<WT>(A, ent[q], k, l)) * A.dval[node[q]];
+    bdir[(size_t)b * A.n + rows[i]] = s;
+}
+
 // Off-diagonal entries of every row, PREP_G lanes per row (a row has a
 // handful of entries below the diagonal, so a warp serves 32 / PREP_G rows):
 // zero fill, then a(r, r-d) * fak_r * fak_(r-d), or 0 when either node is a
@@ -242,7 +265,11 @@ __global__ void k_band_residual(BandArgs<T> A, int sys0, int nsolve, int div, co
             den += cabs1(a) * cabs1(zc);
         }
     }
-    const cd bb = scale(rhs_entry_b<cd>(r, A.enr0[l], A.lsink, A.nsink0, A.dflag, A.dval, nullptr), fk[r]);
+    // the boundary.dat couplings belong to the refactored systems' own
+    // right-hand sides (every system with mixed boundaries, electrode 1
+    // otherwise); the kompb right-hand sides of the others have none
+    const cd* bd = (A.bdir && (A.mixed || l == 0)) ? A.bdir + (size_t)slot * n : nullptr;
+    const cd bb = scale(rhs_entry_b<cd>(r, A.enr0[l], A.lsink, A.nsink0, A.dflag, A.dval, bd), fk[r]);
     const cd res = bb - acc;
     rout[(size_t)b * n + r] = narrow<T>(res);
     if (om_cur) {
@@ -664,6 +691,14 @@ void launch_band_prep(const BandArgs<T>& a, cudaStream_t st)
     k_band_prep_rows<T><<<(unsigned)((rows * PREP_G + 255) / 256), 256, 0, st>>>(a);
 }
 
+template <typename T>
+void launch_band_dir_rhs(const BandArgs<T>& a, int nrows, const int* rows, const int* ptr, const int* ent,
+                         const int* node, cd* bdir, cudaStream_t st)
+{
+    const long long m = (long long)a.nsys * nrows;
+    if (m > 0) k_band_dir_rhs<T><<<(unsigned)((m + 255) / 256), 256, 0, st>>>(a, nrows, rows, ptr, ent, node, bdir);
+}
+
 // Threads per CTA of a launch configuration for a window of smem bytes: a
 // window that fits twice per SM runs as two 256-thread CTAs (one system's
 // serial phases overlap the other's update), a small one may run as four
@@ -802,6 +837,12 @@ void launch_band_residual(const BandArgs<T>& a, int sys0, int nsolve, int div, c
 template bool band_blk_fits<double>(int);
 template bool band_blk_fits<cd>(int);
 template bool band_blk_fits<cf>(int);
+template void launch_band_dir_rhs<double>(const BandArgs<double>&, int, const int*, const int*, const int*,
+                                          const int*, cd*, cudaStream_t);
+template void launch_band_dir_rhs<cd>(const BandArgs<cd>&, int, const int*, const int*, const int*, const int*, cd*,
+                                      cudaStream_t);
+template void launch_band_dir_rhs<cf>(const BandArgs<cf>&, int, const int*, const int*, const int*, const int*, cd*,
+                                      cudaStream_t);
 template void launch_band_prep<double>(const BandArgs<double>&, cudaStream_t);
 template void launch_band_prep<cd>(const BandArgs<cd>&, cudaStream_t);
 template void launch_band_prep<cf>(const BandArgs<cf>&, cudaStream_t);

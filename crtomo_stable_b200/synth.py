@@ -52,8 +52,10 @@ def graded_depths(nz: int, dz0: float, growth: float) -> np.ndarray:
 
 
 def structured_mesh(xs: np.ndarray, depths: np.ndarray, triangles: bool,
-                    topo=None) -> Mesh:
-    """Quadrilateral (type 8) or split-quadrilateral triangle (type 3) grid."""
+                    topo=None, side_type: int = 11) -> Mesh:
+    """Quadrilateral (type 8) or split-quadrilateral triangle (type 3) grid.
+    The sides and the bottom are mixed boundaries (side_type 11) or
+    homogeneous Dirichlet boundaries (side_type 13, src/randb.f90)."""
     nx, nz = len(xs) - 1, len(depths) - 1
     ncol = nz + 1
 
@@ -102,7 +104,7 @@ def structured_mesh(xs: np.ndarray, depths: np.ndarray, triangles: bool,
     nrel[E:E + R12, :2] = np.array(top, dtype=np.int32)
     nrel[E + R12:, :2] = np.array(mixed, dtype=np.int32)
     mb = int(max(np.max(np.array(area), axis=1) - np.min(np.array(area), axis=1)))
-    typ = np.array([3 if triangles else 8, 12, 11], np.int32)
+    typ = np.array([3 if triangles else 8, 12, side_type], np.int32)
     nel = np.array([E, R12, R11], np.int32)
     sel = np.array([nk, 2, 2], np.int32)
     rnr = np.array(rnr_top + rnr_mixed, np.int32)
