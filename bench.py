@@ -65,7 +65,6 @@ def parse():
                     help="FP64 refinement steps of the complex64 forward (default: the library's)")
     ap.add_argument("--forms", default="both", choices=["both", "mixed"],
                     help="'mixed' skips the plain FP64 comparison run (profiling)")
-    ap.add_argument("--cpu-sample-s", type=float, default=20.0)
     ap.add_argument("--count", type=int, default=256, help="instances of the batched configuration C4")
     ap.add_argument("--lambdas", type=int, default=4,
                     help="lambda candidates of the batched Jacobi-form update measured after the step (0: skip)")
@@ -200,76 +199,202 @@ def load_peaks():
 
 
 # ---------------------------------------------------------------------------
-def cpu_sample(s, ncg: int, budget_s: float, nthreads: int):
-    """The FP64 oracle (restatement of the Fortran path, OpenMP as the
-    reference) on a bounded sample of the same GN step, scaled to one step:
-      forward  : all wavenumbers x `le` source electrodes (of eanz) with the
-                 reference's OpenMP over wavenumbers, scaled by eanz / le;
-      Jacobian : `ni` readings (of nanz) on one thread, scaled by
-                 nanz / ni / threads (bsensi is OpenMP over readings);
-      CG       : two serial cjggra iterations on `nc` model cells (of manz),
-                 scaled by manz / nc and by `ncg`, the iteration count of the
-                 reference's own CG (cgfac-preconditioned cjggra) on the
-                 workload."""
-    from oracle.oracle import OracleCG, OracleProblem
-    from crtomo_stable_b200.lib import rwaven
+def workload_name(s, K: int) -> str:
+    """The workload string both arms print (identical for the same survey)."""
     m = s.mesh
-    L, N, E = len(s.enr), len(s.strnr), m.elanz
-    kwn, kwnwi = rwaven(m, s.enr, s.strnr, s.vnr)
-    K = len(kwn)
-    one = np.array([1], np.int32)
-    zero = np.array([0], np.int32)
-    le = 1
-    op_f = OracleProblem(m, s.enr[:le], one, zero, kwn=kwn, kwnwi=kwnwi)
+    kind = "triangles" if int(m.typ[0]) == 3 else "quadrilaterals"
+    L, N = len(s.enr), len(s.strnr)
+    return (f"{s.name}: {m.elanz} {kind}, n={m.sanz}, mb={m.mb}, {L} electrodes, {N} readings, K={K}; one GN step "
+            f"from a homogeneous model (forward {K * L} band systems + Jacobian + CG to rel-res 1e-6)")
+
+
+def _cpu_problem(s):
+    """Oracle problem of the survey (wavenumbers from the oracle's own rwaven,
+    precal of all electrodes), the homogeneous starting model, a data
+    vector and weights for the CG timing (the starting model's response
+    stands in for the data: a CG iteration's cost does not depend on the
+    values) and the regulariser (ltri = 1, as the GPU arm)."""
+    from crtomo_stable_b200 import regularization
+    from oracle.oracle import OracleProblem
+    m = s.mesh
+    op = OracleProblem(m, s.enr, s.strnr, s.vnr)
+    rho0 = float(np.exp(np.mean(np.log(np.abs(1.0 / s.sigma)))))
+    sig0 = np.full(m.elanz, 1.0 / rho0 + 0j)
+    nb = regularization.nachbar(m)
+    sm = regularization.smatm_tri(m, nb, 1.0, 1.0)
+    return op, sig0, nb, sm
+
+
+def guided_makespan(n: int, threads: int, min_chunk: int) -> int:
+    """Readings of the busiest thread when OpenMP's SCHEDULE(GUIDED, c)
+    hands out n equal-cost iterations to `threads` threads (chunk =
+    max(c, ceil(remaining / threads)), each to the thread that frees first)."""
+    import heapq
+    load = [0] * max(threads, 1)
+    heapq.heapify(load)
+    rem = n
+    while rem > 0:
+        ch = min(rem, max(min_chunk, -(-rem // max(threads, 1))))
+        heapq.heappush(load, heapq.heappop(load) + ch)
+        rem -= ch
+    return max(load)
+
+
+def _cg_iteration_s(J, E, N, nb, sm, lam, iters=2):
+    """Seconds per serial cjggra iteration (src/cg_mod.f90:426-518, no
+    OpenMP in the reference) on the given Jacobian: `iters` iterations at
+    eps = 0 on a unit right-hand side."""
+    from oracle.oracle import OracleCG
+    cg = OracleCG(E, N, 1, sm, nachbar=nb, nnb=sm.shape[1] - 1, wmatd=np.ones(N), lam=lam, eps=0.0, ncgmax=iters)
     t = time.perf_counter()
-    op_f.forward(s.sigma, nthreads=min(K, nthreads))
-    t_fwd = (time.perf_counter() - t) * (L / le)
-    ni = 4
-    op_j = OracleProblem(m, s.enr, s.strnr[:ni], s.vnr[:ni], kwn=kwn, kwnwi=kwnwi)
+    _, _, ncg = cg.cjggra(J, np.ones(E), np.ones(E, np.complex128))
+    return (time.perf_counter() - t) / max(ncg, 1)
+
+
+def oracle_full_step(s, nthreads: int, ncg_ref: int):
+    """The reference's CPU path (the oracle: the FP64 C restatement of the
+    Fortran, OpenMP where the reference has it) on the whole workload,
+    measured once: the complete forward (every wavenumber x source electrode
+    system; OpenMP over wavenumbers with min(K, cores) threads as
+    src/inv.f90:426-484) with rtrafo and bvolti, and the complete bsensi
+    (every reading; OpenMP over readings on all cores as
+    src/bsensi.f90:90-96).  The CG is not run to its end (at rel-res 1e-6 the
+    reference's serial cjggra needs ncg_ref iterations, hours on this
+    survey): two iterations on the real Jacobian give its per-iteration time
+    and the projection ncg_ref x that, reported apart from the measured
+    value."""
+    op, sig0, nb, sm = _cpu_problem(s)
+    m = s.mesh
+    E, N, K = m.elanz, len(s.strnr), len(op.kwn)
+    tf = min(K, nthreads)
+    # warm-up: one source electrode's systems (threads spun up, pages in)
+    from oracle.oracle import OracleProblem
+    one, zero = np.array([1], np.int32), np.array([0], np.int32)
+    OracleProblem(m, s.enr[:1], one, zero, kwn=op.kwn, kwnwi=op.kwnwi).forward(sig0, nthreads=tf)
+    t0 = time.perf_counter()
+    kp = op.forward(sig0, nthreads=tf)
+    volt, sa = op.bvolti(op.rtrafo(kp))
+    t1 = time.perf_counter()
+    J = op.bsensi(kp, sig0, volt, nthreads=nthreads)
+    t2 = time.perf_counter()
+    del kp
+    lam = float(max(E, N))
+    t_it = _cg_iteration_s(J, E, N, nb, sm, lam)
+    return dict(forward_s=t1 - t0, jacobian_s=t2 - t1, cg_iteration_s=t_it, projected_cg_s=t_it * ncg_ref,
+                ncg_ref=ncg_ref, forward_threads=tf, jacobian_threads=nthreads, K=K)
+
+
+def cpu_sample(s, nthreads: int, ncg_ref: int, le: int = 16, ni_frac: float = 0.125, ni_max: int = 96):
+    """A bounded sample of the same step on the oracle, extrapolated (and
+    labelled so): the forward of all wavenumbers for `le` of the L source
+    electrodes (min(K, cores) threads), scaled by L / le -- the systems of
+    one electrode cost the same as any other's; bsensi for a sample of the
+    readings on one thread, scaled to all readings and divided by the
+    parallel width of the reference's schedule; the serial CG iteration timed
+    twice on a Jacobian of the full size, projected to ncg_ref iterations.
+    The scaling method is checked end to end on the 60 x 20 survey (C1),
+    where the whole step runs in seconds (validate_scaling)."""
+    from oracle.oracle import OracleProblem
+    op, sig0, nb, sm = _cpu_problem(s)
+    m = s.mesh
+    L, N, E, K = len(s.enr), len(s.strnr), m.elanz, len(op.kwn)
+    tf = min(K, nthreads)
+    le = min(le, L)
+    one, zero = np.array([1], np.int32), np.array([0], np.int32)
+    opf = OracleProblem(m, s.enr[:le], one, zero, kwn=op.kwn, kwnwi=op.kwnwi)
+    opf.forward(sig0, nthreads=tf)   # warm-up
+    t = time.perf_counter()
+    opf.forward(sig0, nthreads=tf)
+    t_fwd = (time.perf_counter() - t) * L / le
+    # bsensi: `ni` readings on one thread, scaled to the readings of the
+    # busiest thread under the reference's SCHEDULE(GUIDED, 256) (a
+    # reading's cost does not depend on which reading it is)
+    ni = max(1, min(ni_max, int(N * ni_frac)))
+    span = guided_makespan(N, nthreads, 256)
+    width = N / span
+    opj = OracleProblem(m, s.enr, s.strnr[:ni], s.vnr[:ni], kwn=op.kwn, kwnwi=op.kwnwi)
     kp = np.zeros((m.sanz, L, K), np.complex128, order="F")
     t = time.perf_counter()
-    op_j.bsensi(kp, s.sigma, np.ones(ni, np.complex128), nthreads=1)
-    t_sens = (time.perf_counter() - t) * N / ni / nthreads
-    nc = min(E, 2048)
-    J = np.full((N, nc), 1e-3 + 0j, order="F")
-    sm = np.zeros((nc, 4), order="F")
-    sm[:, 3] = 1.0
-    nb = np.zeros((nc, 4), np.int32, order="F")
-    cg = OracleCG(nc, N, 1, sm, nachbar=nb, nnb=3, wmatd=np.ones(N), lam=1.0, eps=0.0, ncgmax=2)
-    t = time.perf_counter()
-    cg.cjggra(J, np.ones(nc), np.ones(nc, np.complex128))
-    t_cg = (time.perf_counter() - t) / 2.0 * (E / nc) * ncg
-    total = t_fwd + t_sens + t_cg
-    sample = (f"oracle (FP64 C restatement, OpenMP like the reference): forward of all {K} wavenumbers x "
-              f"{le} of {L} source electrodes on {min(K, nthreads)} threads (x{L // le}); bsensi on {ni} of "
-              f"{N} readings on 1 thread (/{nthreads} threads); 2 serial cjggra iterations on {nc} of {E} "
-              f"cells (x{E / nc:.1f} cells, x{ncg} iterations)")
-    return total, dict(forward_s=t_fwd, jacobian_s=t_sens, cg_s=t_cg, sample=sample, cores=nthreads)
+    opj.bsensi(kp, sig0, np.ones(ni, np.complex128), nthreads=1)
+    t_jac = (time.perf_counter() - t) / ni * span
+    del kp
+    J = np.full((N, E), 1e-3 + 1e-4j, order="F")
+    t_it = _cg_iteration_s(J, E, N, nb, sm, float(max(E, N)))
+    del J
+    sample = (f"oracle (FP64 C restatement, OpenMP as the reference), extrapolated: forward of all {K} "
+              f"wavenumbers x {le} of {L} source electrodes on {tf} threads (x{L / le:g}); bsensi on {ni} of {N} "
+              f"readings on 1 thread, scaled to the {span} readings of the busiest of {nthreads} threads under GUIDED(256); CG projected: 2 serial cjggra iterations on the "
+              f"full-size {N} x {E} Jacobian x {ncg_ref} iterations")
+    return dict(forward_s=t_fwd, jacobian_s=t_jac, cg_iteration_s=t_it, projected_cg_s=t_it * ncg_ref,
+                sample=sample, cores=nthreads)
+
+
+def validate_scaling(nthreads: int):
+    """The sampling of cpu_sample checked end to end on C1 (60 x 20 quads,
+    40 electrodes, 268 readings), where the oracle's whole step -- forward,
+    bsensi and the CG run to rel-res 1e-6 -- is measured in seconds: the
+    measured phases beside the same extrapolations (forward from 4 of 40
+    electrodes, bsensi from 1/8 of the readings, the CG from two iterations
+    times the iteration count the measured run needed)."""
+    from crtomo_stable_b200 import synth
+    from oracle.oracle import OracleCG, OracleProblem
+    s = synth.config1()
+    op, sig0, nb, sm = _cpu_problem(s)
+    m = s.mesh
+    L, N, E, K = len(s.enr), len(s.strnr), m.elanz, len(op.kwn)
+    tf = min(K, nthreads)
+    op.forward(sig0, nthreads=tf)   # warm-up
+    t0 = time.perf_counter()
+    kp = op.forward(sig0, nthreads=tf)
+    volt, sa = op.bvolti(op.rtrafo(kp))
+    t1 = time.perf_counter()
+    J = op.bsensi(kp, sig0, volt, nthreads=nthreads)
+    t2 = time.perf_counter()
+    lam = float(max(E, N))
+    cg = OracleCG(E, N, 1, sm, nachbar=nb, nnb=sm.shape[1] - 1, wmatd=np.ones(N), lam=lam, eps=1e-12, ncgmax=50000)
+    t3 = time.perf_counter()
+    _, _, ncg = cg.cjggra(J, np.ones(E), np.ones(E, np.complex128))
+    t4 = time.perf_counter()
+    est = cpu_sample(s, nthreads, ncg, le=4)
+    measured = {"forward_s": t1 - t0, "jacobian_s": t2 - t1, "cg_s": t4 - t3, "cg_iterations": int(ncg)}
+    extrap = {"forward_s": est["forward_s"], "jacobian_s": est["jacobian_s"], "cg_s": est["projected_cg_s"]}
+    return {"workload": "C1 (60 x 20 quadrilaterals, 40 electrodes, 268 readings, K=%d)" % K,
+            "measured": measured, "extrapolated": extrap,
+            "ratio_extrapolated_to_measured": {k: extrap[k] / measured[k] for k in extrap if measured[k] > 0}}
 
 
 def run_reference(args, ws, rank, pg):
-    """--impl reference: the oracle (FP64 restatement of the Fortran/OpenMP
-    path; the Fortran reference cannot be built here) on the host cores."""
+    """--impl reference: the reference's CPU path on the host cores -- the
+    oracle, because the Fortran reference cannot be built here -- on the
+    same survey and model as the GPU arm.  It loads no library of this
+    repository's product (the oracle computes its own wavenumbers).  One
+    complete forward + Jacobian is measured: at ~1-2 minutes per step the
+    requested --steps cannot all run within a few minutes, so the line
+    reports the repeats it ran in "steps" (and the requested ones beside)."""
     if rank != 0:
         return
     s = make_problem(args.config)
     nthreads = os.cpu_count() or 1
-    ncg_guess = int(os.environ.get("CRT_REF_NCG", str(REF_NCG.get(args.config, 200))))
-    times = []
-    info = {}
-    for it in range(args.warmup + args.steps):
-        t, info = cpu_sample(s, ncg_guess, args.cpu_sample_s, nthreads)
-        if it >= args.warmup:
-            times.append(t)
-    v = float(np.median(times))
-    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+    ncg_ref = int(os.environ.get("CRT_REF_NCG", str(REF_NCG.get(args.config, 200))))
+    r = oracle_full_step(s, nthreads, ncg_ref)
+    v = r["forward_s"] + r["jacobian_s"]
+    line = {"metric": METRIC, "value": v, "unit": "s", "n_gpus": args.gpus, "steps": 1,
+            "warmup": 1, "steps_requested": args.steps, "warmup_requested": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic (seeded)",
-            "config": {"workload": f"{args.config}: one GN step (forward+Jacobian+CG rel-res 1e-6)",
-                       "parallelism": "host cores"},
+            "config": {"workload": workload_name(s, r["K"]), "parallelism": "host cores"},
             "impl": "reference",
+            "value_covers": ("forward + Jacobian of the GN step, measured in full (all systems, all readings); "
+                             "the step's CG is excluded from value and projected in projected_cg_s"),
+            "phases_s": {"forward": r["forward_s"], "jacobian": r["jacobian_s"]},
+            "projected_cg_s": r["projected_cg_s"],
+            "projected_cg": (f"{r['ncg_ref']} serial cjggra iterations (the count of the reference's "
+                             f"Jacobi-preconditioned CG to rel-res 1e-6 on this survey) x "
+                             f"{r['cg_iteration_s']:.3f} s per iteration measured on the real Jacobian"),
             "cpu_baseline": {"value": v, "unit": "s", "cores": nthreads, "kind": "port",
-                             "sample": info.get("sample", "")},
+                             "sample": (f"oracle (FP64 C restatement of the Fortran path, OpenMP as the reference): "
+                                        f"one complete forward ({r['forward_threads']} threads, one per wavenumber) "
+                                        f"and one complete bsensi ({r['jacobian_threads']} threads), measured")},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -492,18 +617,22 @@ def main():
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            v, info = cpu_sample(s, ref_ncg, args.cpu_sample_s, os.cpu_count() or 1)
+            nth = os.cpu_count() or 1
+            info = cpu_sample(s, nth, ref_ncg)
+            v = info["forward_s"] + info["jacobian_s"]
             cpu = {"value": v, "unit": "s", "cores": info["cores"], "kind": "port", "sample": info["sample"],
-                   "phases_s": {k: info[k] for k in ("forward_s", "jacobian_s", "cg_s")}}
+                   "extrapolated": True,
+                   "value_covers": "forward + Jacobian of the GN step (the CG is projected apart)",
+                   "phases_s": {"forward": info["forward_s"], "jacobian": info["jacobian_s"]},
+                   "projected_cg_s": info["projected_cg_s"], "cg_iteration_s": info["cg_iteration_s"],
+                   "scaling_check": validate_scaling(nth)}
         except Exception as exc:  # the baseline must not hide the GPU number
             cpu = {"value": None, "unit": "s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
     if rank == 0:
         line = {"metric": METRIC, "value": t_step, "unit": "s", "n_gpus": ws, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128/c64", "data": "synthetic (seeded)",
-                "config": {"workload": f"{args.config}: {E} triangles, n={n}, mb={mb}, {L} electrodes, "
-                                       f"{N} readings, K={K}; one GN step from a homogeneous model "
-                                       f"(forward {K * L} band systems + Jacobian + CG to rel-res 1e-6)",
+                "config": {"workload": workload_name(s, K),
                            "form": ("mixed: band systems assembled and scaled in FP64, factored and solved in "
                                     "complex64, adaptive FP64 iterative refinement (at most 8 steps, each system to normwise backward "
                                     "error 1e-14); Jacobian formed in FP64, stored "

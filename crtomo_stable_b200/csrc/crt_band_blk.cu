@@ -265,11 +265,20 @@ __global__ void k_band_residual(BandArgs<T> A, int sys0, int nsolve, int div, co
             den += cabs1(a) * cabs1(zc);
         }
     }
-    // the boundary.dat couplings belong to the refactored systems' own
-    // right-hand sides (every system with mixed boundaries, electrode 1
-    // otherwise); the kompb right-hand sides of the others have none
-    const cd* bd = (A.bdir && (A.mixed || l == 0)) ? A.bdir + (size_t)slot * n : nullptr;
-    const cd bb = scale(rhs_entry_b<cd>(r, A.enr0[l], A.lsink, A.nsink0, A.dflag, A.dval, bd), fk[r]);
+    // The refactored systems (every system with mixed boundaries, electrode
+    // 1 otherwise) carry kompab's right-hand side with the Dirichlet edits
+    // (randb / randb2, their boundary.dat couplings in bdir); the others are
+    // kompb's (src/kompb.f90:39-66): -1 at the source, +1 at the sink, no
+    // edits, as in the reference's loop.
+    cd b0;
+    if (A.mixed || l == 0) {
+        const cd* bd = A.bdir ? A.bdir + (size_t)slot * n : nullptr;
+        b0 = rhs_entry_b<cd>(r, A.enr0[l], A.lsink, A.nsink0, A.dflag, A.dval, bd);
+    } else {
+        b0 = cd{r == A.enr0[l] ? -1.0 : 0.0, 0.0};
+        if (A.lsink && r == A.nsink0) b0 = cd{1.0, 0.0};
+    }
+    const cd bb = scale(b0, fk[r]);
     const cd res = bb - acc;
     rout[(size_t)b * n + r] = narrow<T>(res);
     if (om_cur) {
