@@ -12,8 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcrt_b200.so")
-SOURCES = ["crt_setup.cu", "crt_band.cu", "crt_band_blk.cu", "crt_volt.cu", "crt_sens.cu", "crt_cg.cu", "crt_spc.cu", "crt_gnn.cu", "crt_api.cu", "crt_noalloc.cu"]
-HEADERS = ["crt_common.cuh", "crt_setup.h", "crt_band.h", "crt_volt.h", "crt_sens.h", "crt_cg.h", "crt_spc.h", "crt_gnn.h"]
+SOURCES = ["crt_setup.cu", "crt_band.cu", "crt_band_blk.cu", "crt_volt.cu", "crt_sens.cu", "crt_cg.cu", "crt_spc.cu", "crt_gnn.cu", "crt_schur.cu", "crt_api.cu", "crt_noalloc.cu"]
+HEADERS = ["crt_common.cuh", "crt_setup.h", "crt_band.h", "crt_volt.h", "crt_sens.h", "crt_cg.h", "crt_spc.h", "crt_gnn.h", "crt_schur.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-O3", "-I" + os.path.join(HERE, "..", "include")]

@@ -16,6 +16,7 @@
 #include "crt_band.h"
 #include "crt_cg.h"
 #include "crt_common.cuh"
+#include "crt_schur.h"
 #include "crt_sens.h"
 #include "crt_setup.h"
 #include "crt_spc.h"
@@ -139,6 +140,21 @@ struct crt_ctx {
     };
     std::vector<FwdMark> fwd_marks;
     int vol_e0 = -1, vol_e1 = -1;
+    // forward by elimination of the mixed-boundary nodes (crt_schur.cu):
+    // the plan (host and device), its workspaces and the phase events of the
+    // last run
+    int fwd_form = CRT_FORWARD_AUTO;
+    int schur_ok = 0, schur_used = 0;
+    SchurHost schur_h;
+    SchurArgs schur{};
+    std::vector<void*> schur_bufs;    // plan arrays
+    int *d_sI_row_ptr = nullptr, *d_sI_ent_d = nullptr, *d_sI_ent_ptr = nullptr, *d_sI_con_code = nullptr,
+        *d_sI_con_sig = nullptr;
+    unsigned char* d_sI_dflag = nullptr;
+    void *d_sLI = nullptr, *d_sX = nullptr, *d_sS0 = nullptr, *d_sS = nullptr, *d_sxg = nullptr, *d_scval = nullptr;
+    double* d_sfak = nullptr;
+    int sS_chunk = 0;
+    int sev[5] = {-1, -1, -1, -1, -1};   // after the factor, msolve, S0, Cholesky, rebuild
 };
 
 namespace {
@@ -328,6 +344,29 @@ extern "C" int32_t crt_set_refinement_tol(crt_ctx* ctx, double tau)
     return CRT_OK;
 }
 
+extern "C" int32_t crt_set_forward_form(crt_ctx* ctx, int32_t form)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    if (form != CRT_FORWARD_AUTO && form != CRT_FORWARD_DIRECT && form != CRT_FORWARD_SCHUR)
+        return set_err(ctx, CRT_ERR_ARG, "unknown forward form");
+    if (form == CRT_FORWARD_SCHUR && !ctx->schur_ok)
+        return set_err(ctx, CRT_ERR_UNSUPPORTED,
+                       "the Schur form needs mixed boundaries, no Dirichlet nodes and at most 768 boundary nodes");
+    ctx->fwd_form = form;
+    return CRT_OK;
+}
+
+extern "C" int32_t crt_forward_info(const crt_ctx* ctx, int32_t* form, int32_t* nboundary, int32_t* ninterior,
+                                    int32_t* mb_interior)
+{
+    if (!ctx) return CRT_ERR_ARG;
+    if (form) *form = ctx->have_forward ? (ctx->schur_used ? CRT_FORWARD_SCHUR : CRT_FORWARD_DIRECT) : CRT_FORWARD_AUTO;
+    if (nboundary) *nboundary = ctx->schur_ok ? ctx->schur_h.m : 0;
+    if (ninterior) *ninterior = ctx->schur_ok ? ctx->schur_h.nI : 0;
+    if (mb_interior) *mb_interior = ctx->schur_ok ? ctx->schur_h.mbI : 0;
+    return CRT_OK;
+}
+
 extern "C" int32_t crt_last_timings_ex(const crt_ctx* ctx, double* ms, int32_t n)
 {
     if (!ctx || !ms || n < 0) return CRT_ERR_ARG;
@@ -350,6 +389,11 @@ extern "C" void crt_destroy(crt_ctx* ctx)
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
+    for (void* p : ctx->schur_bufs)
+        if (p) cudaFree(p);
+    void* sws[] = {ctx->d_sLI, ctx->d_sX, ctx->d_sS0, ctx->d_sS, ctx->d_sxg, ctx->d_scval, ctx->d_sfak};
+    for (void* p : sws)
+        if (p) cudaFree(p);
     void* ptrs[] = {ctx->d_nrel0, ctx->d_snr0, ctx->d_etyp, ctx->d_enk, ctx->d_enr0, ctx->d_mixed_rel,
                     ctx->d_strnr, ctx->d_vnr, ctx->d_elec, ctx->d_sx, ctx->d_sy, ctx->d_kwn, ctx->d_kwnwi,
                     ctx->d_elbg, ctx->d_relbg, ctx->d_kg, ctx->d_row_ptr, ctx->d_ent_d, ctx->d_ent_ptr,
@@ -568,6 +612,65 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
              upload(ctx, &ctx->d_dc_ent, dc_ent.data(), dc_ent.size()) &&
              upload(ctx, &ctx->d_dc_node, dc_node.data(), dc_node.size());
     if (!ok) return fail(ctx, CRT_ERR_ALLOC);
+    // Schur form of the forward: mixed boundaries without Dirichlet nodes;
+    // the boundary set is every node of a type-11 segment
+    if (ctx->lbeta && !ctx->lrandb && !ctx->lrandb2) {
+        std::vector<int> gnodes;
+        for (int rel : mixed_rel)
+            for (int q = 0; q < 2; ++q) gnodes.push_back(nrel0[(size_t)(m.elanz + rel) * m.maxnodes + q]);
+        SchurHost& H = ctx->schur_h;
+        if (schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H) == CRT_OK &&
+            schur_msolve_smem<cd>(H.mbI, H.mbI + 1) <= 227 * 1024 &&
+            (size_t)(16 + 1) * H.m * sizeof(cd) <= 227 * 1024 && band_factor_smem<cd>(H.mbI + 1) <= 227 * 1024) {
+            auto up = [&](int** d, const std::vector<int>& v) {
+                const std::vector<int> one(1, 0);
+                const std::vector<int>& src = v.empty() ? one : v;
+                if (!upload(ctx, d, src.data(), src.size())) return false;
+                ctx->schur_bufs.push_back(*d);
+                return true;
+            };
+            SchurArgs& S = ctx->schur;
+            int *p_permI = nullptr, *p_gam = nullptr, *p_pis = nullptr, *p_pgs = nullptr, *p_gip = nullptr,
+                *p_gipos = nullptr, *p_gient = nullptr, *p_gig = nullptr, *p_ggg = nullptr, *p_ggh = nullptr,
+                *p_gge = nullptr, *p_co = nullptr, *p_bs = nullptr;
+            const AssemblyLists& li = H.lists_I;
+            std::vector<unsigned char> zf(H.nI, 0);
+            bool su = up(&p_permI, H.permI) && up(&p_gam, H.gam) && up(&p_pis, H.posI_src) && up(&p_pgs, H.posG_src) &&
+                      up(&p_gip, H.gi_ptr) && up(&p_gipos, H.gi_pos) && up(&p_gient, H.gi_ent) && up(&p_gig, H.gi_g) &&
+                      up(&p_ggg, H.gg_g) && up(&p_ggh, H.gg_h) && up(&p_gge, H.gg_ent) && up(&p_co, H.col_order) &&
+                      up(&p_bs, H.blk_start) && up(&ctx->d_sI_row_ptr, li.row_ptr) && up(&ctx->d_sI_ent_d, li.ent_d) &&
+                      up(&ctx->d_sI_ent_ptr, li.ent_ptr) && up(&ctx->d_sI_con_code, li.con_code) &&
+                      up(&ctx->d_sI_con_sig, li.con_sig) && upload(ctx, &ctx->d_sI_dflag, zf.data(), zf.size());
+            if (!su) return fail(ctx, CRT_ERR_ALLOC);
+            ctx->schur_bufs.push_back(ctx->d_sI_dflag);
+            S.nI = H.nI;
+            S.m = H.m;
+            S.L = ctx->L;
+            S.K = ctx->K;
+            S.ncol = ctx->L + H.m;
+            S.mbI = H.mbI;
+            S.nblk = (int)H.blk_start.size();
+            S.ncpl = (int)H.gi_pos.size();
+            S.ngg = (int)H.gg_ent.size();
+            S.permI = p_permI;
+            S.gam = p_gam;
+            S.posI_src = p_pis;
+            S.posG_src = p_pgs;
+            S.posI_sink = H.posI_sink;
+            S.posG_sink = H.posG_sink;
+            S.lsink = ctx->lsink;
+            S.gi_ptr = p_gip;
+            S.gi_pos = p_gipos;
+            S.gi_ent = p_gient;
+            S.gi_g = p_gig;
+            S.gg_g = p_ggg;
+            S.gg_h = p_ggh;
+            S.gg_ent = p_gge;
+            S.col_order = p_co;
+            S.blk_start = p_bs;
+            ctx->schur_ok = 1;
+        }
+    }
     ctx->nstatus = std::max(ctx->K * ctx->L, ctx->K) + 8;
     if (!dalloc(ctx, &ctx->d_status, (size_t)ctx->nstatus)) return fail(ctx, CRT_ERR_ALLOC);
     if (!ck(ctx, cudaMemsetAsync(ctx->d_status, 0, sizeof(int) * ctx->nstatus, ctx->st), "memset")) return fail(ctx, CRT_ERR_CUDA);
@@ -863,6 +966,146 @@ int run_forward(crt_ctx* ctx)
     return CRT_OK;   // per-system status and phase times: read by forward_common
 }
 
+// Bytes of the Schur form's workspaces (sized for complex128).
+size_t schur_bytes(const crt_ctx* ctx, int chunk)
+{
+    const SchurHost& H = ctx->schur_h;
+    const size_t K = ctx->K, L = ctx->L, nI = H.nI, m = H.m;
+    return sizeof(cd) * (K * nI * (H.mbI + 2) + K * (L + m) * nI + K * std::max<size_t>(H.gi_pos.size(), 1) +
+                         K * m * m + K * L * m + (size_t)chunk * m * m) +
+           sizeof(double) * K * nI;
+}
+
+// Whether this forward runs in the Schur form.
+bool use_schur(const crt_ctx* ctx)
+{
+    if (!ctx->schur_ok || ctx->fwd_form == CRT_FORWARD_DIRECT) return false;
+    const char* fv = std::getenv("CRT_B200_FORWARD");
+    if (fv && std::strcmp(fv, "direct") == 0) return false;
+    if (ctx->d_sLI) return true;   // workspaces exist (a captured forward may not allocate)
+    const size_t chunk = std::min<size_t>((size_t)ctx->K * ctx->L, 2048);
+    return ctx->ws_budget == 0 || schur_bytes(ctx, (int)chunk) <= ctx->ws_budget;
+}
+
+// Forward in the Schur form (crt_schur.h): interior factorisation per
+// wavenumber, multi-RHS band solve of [r_I | A_IG], S0 = -A_GI Y, dense
+// Cholesky of every S_l with its boundary solve, rebuild of kpot.  FP64
+// arithmetic (T = complex128, or double for the real DC systems).
+template <typename T>
+int run_forward_schur(crt_ctx* ctx)
+{
+    const SchurHost& H = ctx->schur_h;
+    const int K = ctx->K, L = ctx->L, nI = H.nI, m = H.m;
+    // column stride of the interior factor: mbI + 1, even for real entries
+    // so that every column starts on a 16-byte boundary (bulk copies)
+    const int WI = std::is_same<T, double>::value ? (H.mbI + 2) / 2 * 2 : H.mbI + 1;
+    const int ncol = L + m, ncpl = (int)H.gi_pos.size();
+    if (!ctx->d_sLI) {
+        if (ctx->capture) return set_err(ctx, CRT_ERR_ARG, "captured forward without a prepared workspace");
+        // the per-(k, l) Schur matrices in chunks of at most 8 GiB
+        const size_t per = sizeof(cd) * (size_t)m * m;
+        ctx->sS_chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)K * L, (8ull << 30) / per));
+        CK(cudaMalloc(&ctx->d_sLI, sizeof(cd) * (size_t)K * nI * (H.mbI + 2)));
+        CK(cudaMalloc((void**)&ctx->d_sfak, sizeof(double) * (size_t)K * nI));
+        CK(cudaMalloc(&ctx->d_sX, sizeof(cd) * (size_t)K * ncol * nI));
+        CK(cudaMalloc(&ctx->d_scval, sizeof(cd) * (size_t)K * std::max(ncpl, 1)));
+        CK(cudaMalloc(&ctx->d_sS0, sizeof(cd) * (size_t)K * m * m));
+        CK(cudaMalloc(&ctx->d_sxg, sizeof(cd) * (size_t)K * L * m));
+        CK(cudaMalloc(&ctx->d_sS, per * ctx->sS_chunk));
+    }
+    T* X = static_cast<T*>(ctx->d_sX);
+    T* cval = static_cast<T*>(ctx->d_scval);
+    T* S0 = static_cast<T*>(ctx->d_sS0);
+    T* xg = static_cast<T*>(ctx->d_sxg);
+    T* Sws = static_cast<T*>(ctx->d_sS);
+    T* LI = static_cast<T*>(ctx->d_sLI);
+    SchurArgs S = ctx->schur;
+    S.WI = WI;
+    S.status = ctx->d_status;
+    // the full mesh's assembly data (entries of A_IG and A_GG(l))
+    BandArgs<T> Af{};
+    Af.n = ctx->n;
+    Af.mb = ctx->mb;
+    Af.L = L;
+    Af.K = K;
+    Af.mixed = 1;
+    Af.E = ctx->E;
+    Af.R = std::max(ctx->R, 1);
+    Af.nmn = ctx->nmn;
+    Af.row_ptr = ctx->d_row_ptr;
+    Af.ent_d = ctx->d_ent_d;
+    Af.ent_ptr = ctx->d_ent_ptr;
+    Af.con_code = ctx->d_con_code;
+    Af.con_sig = ctx->d_con_sig;
+    Af.elbg = ctx->d_elbg;
+    Af.relbg = ctx->d_relbg;
+    Af.kg = ctx->d_kg;
+    Af.sigma = ctx->d_sigma;
+    Af.status = ctx->d_status;
+    // the interior systems A_II, one per wavenumber
+    BandArgs<T> AI = Af;
+    AI.n = nI;
+    AI.mb = H.mbI;
+    AI.W = WI;
+    AI.sys0 = 0;
+    AI.nsys = K;
+    AI.mixed = 0;
+    AI.fuse_rhs = 0;
+    AI.row_ptr = ctx->d_sI_row_ptr;
+    AI.ent_d = ctx->d_sI_ent_d;
+    AI.ent_ptr = ctx->d_sI_ent_ptr;
+    AI.con_code = ctx->d_sI_con_code;
+    AI.con_sig = ctx->d_sI_con_sig;
+    AI.dflag = ctx->d_sI_dflag;
+    AI.dval = ctx->d_dval;
+    AI.bdir = nullptr;
+    AI.enr0 = S.posI_src;
+    AI.lsink = 0;
+    AI.nsink0 = 0;
+    AI.Lws = LI;
+    AI.lstride = (size_t)nI * WI;
+    AI.yws = nullptr;
+    AI.fakws = ctx->d_sfak;
+    AI.aval = nullptr;
+    ctx->tev_n = 0;
+    ctx->fwd_marks.clear();
+    crt_ctx::FwdMark mk{};
+    mk.e0 = tev_rec(ctx);
+    CK(cudaMemsetAsync(X, 0, sizeof(T) * (size_t)K * ncol * nI, ctx->st));
+    launch_schur_rhs<T>(S, Af, X, cval, ctx->st);
+    bool blk = false;
+    if (band_blk_fits<T>(H.mbI)) {
+        const int pb = band_panel<T>(AI, !ctx->capture, ctx->st);
+        ctx->panel = pb & BAND_PANEL_MASK;
+        launch_band_prep<T>(AI, ctx->st);
+        mk.e8 = tev_rec(ctx);
+        launch_band_factor_blk<T>(AI, pb, ctx->st);
+        blk = true;
+    } else {
+        mk.e8 = tev_rec(ctx);
+        launch_band_factor<T>(AI, ctx->st);
+    }
+    if (int e = kernel_check(ctx, "interior factor")) return e;
+    mk.e1 = tev_rec(ctx);
+    mk.blk = blk;
+    launch_schur_msolve<T>(S, LI, AI.lstride, ctx->d_sfak, X, ctx->st);
+    ctx->sev[0] = tev_rec(ctx);
+    launch_schur_s0<T>(S, X, cval, S0, ctx->st);
+    ctx->sev[1] = tev_rec(ctx);
+    for (int s0 = 0; s0 < K * L; s0 += ctx->sS_chunk)
+        launch_schur_chol<T>(S, Af, S0, X, cval, Sws, xg, s0, std::min(ctx->sS_chunk, K * L - s0), ctx->st);
+    ctx->sev[2] = tev_rec(ctx);
+    launch_schur_out<T>(S, X, xg, ctx->n, ctx->d_kpot, ctx->st);
+    if (int e = kernel_check(ctx, "Schur kernels")) return e;
+    mk.e2 = tev_rec(ctx);
+    ctx->sev[3] = mk.e2;
+    ctx->fwd_marks.push_back(mk);
+    ctx->launches += 10 + (K * L + ctx->sS_chunk - 1) / ctx->sS_chunk;
+    ctx->timings[9] = 1;
+    ctx->timings[12] = blk ? ctx->panel : 0;
+    return CRT_OK;
+}
+
 // Phase times of the last forward from its pooled events (after a host
 // synchronisation that covers them).
 void resolve_forward_timings(crt_ctx* ctx)
@@ -886,6 +1129,15 @@ void resolve_forward_timings(crt_ctx* ctx)
     ctx->timings[8] = ms_fk;
     ctx->timings[10] = ms_res;
     ctx->timings[11] = ms_cor;
+    // Schur form: multi-RHS solve, S0 + boundary Cholesky, rebuild
+    if (ctx->schur_used && !ctx->fwd_marks.empty()) {
+        const crt_ctx::FwdMark& m0 = ctx->fwd_marks[0];
+        ctx->timings[13] = tev_ms(ctx, m0.e1, ctx->sev[0]);
+        ctx->timings[14] = tev_ms(ctx, ctx->sev[0], ctx->sev[2]);
+        ctx->timings[15] = tev_ms(ctx, ctx->sev[2], ctx->sev[3]);
+    } else {
+        ctx->timings[13] = ctx->timings[14] = ctx->timings[15] = 0.0;
+    }
 }
 
 int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
@@ -901,7 +1153,12 @@ int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
     // the mixed form factors the complex systems in complex64 and refines
     const char* fv = std::getenv("CRT_B200_FACTOR");
     const bool c64 = !ldc && ctx->prec == CRT_PREC_MIXED && band_blk_fits<cf>(ctx->mb) && !(fv && std::strcmp(fv, "v0") == 0);
-    int e = ldc ? run_forward<double>(ctx) : (c64 ? run_forward<cf>(ctx) : run_forward<cd>(ctx));
+    ctx->schur_used = use_schur(ctx);
+    int e;
+    if (ctx->schur_used)
+        e = ldc ? run_forward_schur<double>(ctx) : run_forward_schur<cd>(ctx);
+    else
+        e = ldc ? run_forward<double>(ctx) : (c64 ? run_forward<cf>(ctx) : run_forward<cd>(ctx));
     if (e) return e;
     double* d_kfak = nullptr;
     if (kfak_h && mode == 1) {

@@ -31,6 +31,29 @@ struct BandArgs {
     size_t aval_stride;
 };
 
+// One assembled band entry of system (k, l): kompab's sum over the entry's
+// element and mixed-boundary contributions (src/kompab.f90:80-128), formed in
+// the arithmetic W (FP64 or complex128) from the gather lists of A.
+template <typename W, typename T>
+__device__ __forceinline__ W band_assemble_entry(const BandArgs<T>& A, int e, int k, int l)
+{
+    W v = Sc<W>::zero();
+    const int c1 = A.ent_ptr[e + 1];
+    const double* elbg_k = A.elbg + (size_t)k * A.E * A.nmn;
+    for (int c = A.ent_ptr[e]; c < c1; ++c) {
+        const int code = A.con_code[c];
+        double coef;
+        if (code >= 0) {
+            coef = elbg_k[code];
+        } else {
+            const int q = -code - 1;
+            coef = A.relbg[q] * A.kg[((size_t)k * A.L + l) * A.R + q / 3];
+        }
+        v += scale(Sc<W>::from(A.sigma[A.con_sig[c]]), coef);
+    }
+    return v;
+}
+
 template <typename T>
 struct SolveArgs {
     int n, mb, W;

@@ -63,26 +63,11 @@ __device__ __forceinline__ int widx(int x, int y)
     return tile_base(x >> 2, y >> 2) * TSTRIDE + ((x & 3) << 2) + (y & 3);
 }
 
-// One assembled band entry (kompab's sum over the entry's element and
-// boundary contributions), formed in the arithmetic W.
+// One assembled band entry, formed in the arithmetic W.
 template <typename W, typename T>
 __device__ __forceinline__ W assemble_entry_w(const BandArgs<T>& A, int e, int k, int l)
 {
-    W v = Sc<W>::zero();
-    const int c1 = A.ent_ptr[e + 1];
-    const double* elbg_k = A.elbg + (size_t)k * A.E * A.nmn;
-    for (int c = A.ent_ptr[e]; c < c1; ++c) {
-        const int code = A.con_code[c];
-        double coef;
-        if (code >= 0) {
-            coef = elbg_k[code];
-        } else {
-            const int q = -code - 1;
-            coef = A.relbg[q] * A.kg[((size_t)k * A.L + l) * A.R + q / 3];
-        }
-        v += scale(Sc<W>::from(A.sigma[A.con_sig[c]]), coef);
-    }
-    return v;
+    return band_assemble_entry<W>(A, e, k, l);
 }
 
 template <typename T>
@@ -785,16 +770,20 @@ int band_panel(const BandArgs<T>& a, bool may_tune, cudaStream_t st)
             return cfg;
         }
     }
-    const std::pair<int, int> key((int)sizeof(T), a.mb);
+    int nsm = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    // tuned separately for launches of at most one system per SM (the
+    // interior systems of the Schur form: one per wavenumber), where no
+    // second system shares an SM
+    const int few = a.nsys <= nsm ? 1 : 0;
+    const std::pair<int, int> key(((int)sizeof(T) << 1) | few, a.mb);
     {
         std::lock_guard<std::mutex> g(g_panel_mu);
         auto it = g_panel.find(key);
         if (it != g_panel.end()) return it->second;
     }
     if (!may_tune) return 8;
-    int nsm = 148, dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     BandArgs<T> t = a;
     t.nsys = std::min(a.nsys, 2 * nsm);
     cudaEvent_t e0, e1;

@@ -70,7 +70,7 @@ EXPORTS = [
     "crt_set_refinement", "crt_set_refinement_tol", "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
     "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad", "crt_batch_create",
     "crt_batch_destroy", "crt_batch_error", "crt_batch_set_models", "crt_batch_run", "crt_batch_status",
-    "crt_batch_results", "crt_set_workspace_limit",
+    "crt_batch_results", "crt_set_workspace_limit", "crt_set_forward_form", "crt_forward_info",
 ]
 
 _LIB = None
@@ -148,6 +148,10 @@ def load(path: str = LIB_PATH):
     L.crt_batch_results.restype = C.c_int32
     L.crt_set_workspace_limit.argtypes = [vp, C.c_int64]
     L.crt_set_workspace_limit.restype = C.c_int32
+    L.crt_set_forward_form.argtypes = [vp, C.c_int32]
+    L.crt_set_forward_form.restype = C.c_int32
+    L.crt_forward_info.argtypes = [vp, i32p, i32p, i32p, i32p]
+    L.crt_forward_info.restype = C.c_int32
     L.crt_last_timings_ex.argtypes = [vp, f64p, C.c_int32]
     L.crt_last_timings_ex.restype = C.c_int32
     L.crt_cg_info.argtypes = [vp, i32p, i32p, i32p]
@@ -248,6 +252,9 @@ PRECOND_JACOBI = 0
 PRECOND_BLOCK = 1
 PRECOND_GNN = 2
 PRECOND_BLOCK_GNN = 3
+FORWARD_AUTO = 0
+FORWARD_DIRECT = 1
+FORWARD_SCHUR = 2
 
 
 class Context:
@@ -445,7 +452,8 @@ class Context:
         return ncg.value
 
     TIMING_NAMES = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total", "factor_prep",
-                    "factor_kernel", "factor_launches", "refine_residual", "refine_solve", "panel"]
+                    "factor_kernel", "factor_launches", "refine_residual", "refine_solve", "panel",
+                    "schur_msolve", "schur_chol", "schur_out"]
 
     def timings(self):
         t = np.zeros(len(self.TIMING_NAMES))
@@ -454,6 +462,16 @@ class Context:
 
     def launch_count(self):
         return int(self.L.crt_launch_count(self.h))
+
+    def set_forward_form(self, form):
+        """FORWARD_AUTO, FORWARD_DIRECT or FORWARD_SCHUR (crt_set_forward_form)."""
+        self._check(self.L.crt_set_forward_form(self.h, int(form)), "crt_set_forward_form")
+
+    def forward_info(self):
+        """(form of the last forward, boundary nodes, interior nodes, interior band)."""
+        v = [C.c_int32() for _ in range(4)]
+        self._check(self.L.crt_forward_info(self.h, *(C.byref(x) for x in v)), "crt_forward_info")
+        return tuple(x.value for x in v)
 
     def set_refinement(self, steps):
         self._check(self.L.crt_set_refinement(self.h, int(steps)), "crt_set_refinement")

@@ -118,6 +118,35 @@ int32_t crt_set_refinement(crt_ctx *ctx, int32_t steps);
  * 1e-14; 0 runs every step for every system).  No reference counterpart. */
 int32_t crt_set_refinement_tol(crt_ctx *ctx, double tau);
 
+/* Forms of the forward model with mixed boundaries.
+ * CRT_FORWARD_DIRECT: the reference's loop -- one assembled, scaled and
+ *   factored band system per wavenumber and source electrode (kompab,
+ *   scalab, chol, vre), in the context's precision form.
+ * CRT_FORWARD_SCHUR: the same systems solved by block elimination of the
+ *   mixed-boundary nodes G (every node of a type-11 segment), the only rows
+ *   and columns in which the systems of different electrodes differ
+ *   (src/kompab.f90:113-117): per wavenumber one band factorisation of the
+ *   interior matrix and a multi-RHS solve of the source vectors and the
+ *   interior-boundary couplings; per (wavenumber, electrode) a dense
+ *   Cholesky of the m x m Schur complement on G and the rebuild of the
+ *   interior potentials.  FP64 / complex128 arithmetic throughout in both
+ *   precision forms (no refinement needed); needs no Dirichlet nodes and
+ *   m <= 768.  The same potentials up to rounding.  No reference
+ *   counterpart.
+ * CRT_FORWARD_AUTO (default): the Schur form where it applies (and its
+ *   workspaces fit a workspace limit set by crt_set_workspace_limit), the
+ *   direct form otherwise. */
+#define CRT_FORWARD_AUTO 0
+#define CRT_FORWARD_DIRECT 1
+#define CRT_FORWARD_SCHUR 2
+int32_t crt_set_forward_form(crt_ctx *ctx, int32_t form);
+/* Form of the last forward (CRT_FORWARD_DIRECT / _SCHUR; _AUTO before the
+ * first), the boundary and interior node counts of the Schur split and the
+ * interior half-bandwidth (0 when the Schur form does not apply).  Any
+ * pointer may be NULL.  No reference counterpart. */
+int32_t crt_forward_info(const crt_ctx *ctx, int32_t *form, int32_t *nboundary, int32_t *ninterior,
+                         int32_t *mb_interior);
+
 /* Creates a context on `device`: uploads the mesh, builds the gather lists
  * of the streamed assembly, and evaluates precal on the device unless the
  * survey provides elbg/relbg/kg.  Replaces the set-up part of
@@ -239,8 +268,10 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
  * factor-kernel launches (one per chunk of systems), [10] the FP64
  * residuals and [11] the correction solves of the mixed form's refinement
  * (both inside [1]), [12] the panel width of the blocked band factorisation
- * (chosen by the autotuner; 0 for the unblocked kernel).  Milliseconds
- * except [9] and [12].  No reference counterpart. */
+ * (chosen by the autotuner; 0 for the unblocked kernel), and in the Schur
+ * form (inside [1]) [13] the multi-RHS interior solve, [14] S0 and the
+ * boundary Cholesky with its solve, [15] the rebuild of the potentials.
+ * Milliseconds except [9] and [12].  No reference counterpart. */
 int32_t crt_last_timings_ex(const crt_ctx *ctx, double *ms, int32_t n);
 
 /* Kernel launches enqueued by the context since creation. */

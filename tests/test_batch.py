@@ -70,6 +70,7 @@ def test_batch_graph_matches_eager_calls_and_oracle():
         assert b.status(i) == 0
         v, sa, J = b.results(i, sens=True)
         e = Context(s.mesh, s.enr, s.strnr, s.vnr, precision=PREC_MIXED)
+        e.set_workspace_limit(32 << 20)   # the same forward form as the batch's context
         ve, sae = e.forward(s.sigma)
         Je = e.jacobian(0)
         np.testing.assert_allclose(v, ve, rtol=RTOL_SAME, atol=RTOL_SAME * np.abs(ve).max())

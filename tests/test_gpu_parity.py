@@ -557,8 +557,10 @@ def test_mixed_form_forward_is_refined_to_fp64(name):
     meshes agree with the FP64 oracle to 1e-9 (the stated target is 1e-6),
     one step already reaches 1e-6; without refinement the complex64 solution
     alone is off by far more than FP64 rounding.  (The default allows up to
-    8 adaptive steps, which the benchmark mesh needs: see the C5 test.)"""
-    from crtomo_stable_b200.lib import PREC_MIXED, Context
+    8 adaptive steps, which the benchmark mesh needs: see the C5 test.)
+    The direct (per-system) form is forced: the Schur form of mixed
+    boundaries is FP64 throughout and has no refinement."""
+    from crtomo_stable_b200.lib import FORWARD_DIRECT, PREC_MIXED, Context
     case = load_forward_case(name)
     m = case["mesh"]
     c = case["cfg"]
@@ -570,6 +572,7 @@ def test_mixed_form_forward_is_refined_to_fp64(name):
         ctx = Context(m, case["enr"], case["volt"].strnr, case["volt"].vnr, precision=PREC_MIXED,
                       swrtr=c.swrtr, lsink=c.lsink, nsink=c.nsink)
         ctx.set_refinement(nref)
+        ctx.set_forward_form(FORWARD_DIRECT)
         volt_g, _, kp_g = ctx.forward(case["sigma"], want_kpot=True)
         scale = np.abs(kp_o).max()
         errs[nref] = (_kpot_diff(kp_g, kp_o, _singular(case)) / scale,

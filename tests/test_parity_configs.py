@@ -165,6 +165,22 @@ def test_dirichlet_edits_match_oracle(side_type, rwd, ldc, precision):
 
 
 # ---------------------------------------------------------------------------
+def _true_relres_5pt(J, wmatd, cgfac, lam, sm, nx, rhs, dpar):
+    """|b - A x| / |b| of the scaled system A = C (J^H W J + lam R) C with the
+    five-point R of src/cg_mod.f90:547-577 (bp), x = dpar / cgfac, in FP64."""
+    import scipy.sparse as sp
+    M = sm.shape[0]
+    i = np.arange(M)
+    rows = [i, i[1:], i[:-1], i[nx:], i[:-nx]]
+    cols = [i, i[:-1], i[1:], i[:-nx], i[nx:]]
+    vals = [sm[:, 0], sm[:-1, 1], sm[:-1, 1], sm[:-nx, 2], sm[:-nx, 2]]
+    R = sp.csr_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(M, M))
+    x = dpar / cgfac
+    Js = J * cgfac[None, :]
+    Ax = Js.conj().T @ (wmatd * (Js @ x)) + lam * cgfac * (R @ (cgfac * x))
+    return np.linalg.norm(rhs - Ax) / np.linalg.norm(rhs)
+
+
 @pytest.mark.parametrize("eps,ncgmax", [(1e-4, None), (1e-12, 3000)])
 def test_five_point_regulariser_cg_matches_oracle(eps, ncgmax):
     """ltri = 0: the five-point smoothing operator of bsmatmreg
@@ -173,8 +189,9 @@ def test_five_point_regulariser_cg_matches_oracle(eps, ncgmax):
     C1 grid (60 x 20 cells) with its device Jacobian.  At the reference's
     stop rule and iteration cap (1e-4, manz/10): equal iteration counts,
     cgfac to 1e-11, dpar to 1e-7 of its maximum, the float32 residual
-    history to 1e-5; at rel-res 1e-6: iteration counts within 2, dpar to
-    1e-6 of its maximum."""
+    history to 1e-5; at rel-res 1e-6: iteration counts within 2, the true
+    relative residual of the device update in the oracle's system below
+    2e-6, dpar to 1e-4 of its maximum."""
     from crtomo_stable_b200 import regularization, synth
     from crtomo_stable_b200.lib import Context
     from oracle.oracle import OracleCG, OracleProblem
@@ -211,9 +228,12 @@ def test_five_point_regulariser_cg_matches_oracle(eps, ncgmax):
         np.testing.assert_allclose(got["bdpar"], ref["bdpar"], rtol=1e-8)
     else:
         # hundreds of iterations in a different summation order: the
-        # iteration count within 2, the update to 1e-6 of its maximum
+        # iteration count within 2, the device update's true relative
+        # residual in the oracle's FP64 system below 2e-6 (the stop rule is
+        # 1e-6), the update to 1e-4 of its maximum
         assert got["ncg"] < ncg_cap and abs(got["ncg"] - ref["ncg"]) <= 2
-        np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-6, atol=1e-6 * np.abs(ref["dpar"]).max())
+        assert _true_relres_5pt(J_o, wmatd, ref["cgfac"], lam, sm, s.nx, ref["rhs"], got["dpar"]) < 2e-6
+        np.testing.assert_allclose(got["dpar"], ref["dpar"], rtol=1e-4, atol=1e-4 * np.abs(ref["dpar"]).max())
     ctx.close()
 
 
@@ -315,3 +335,58 @@ def test_c5_mixed_form_against_fp64_form_and_oracle_slice():
         print(f"C5 oracle slice ({len(rows)} readings, {len(els)} electrodes), precision {prec}: "
               f"voltages {evr:.1e}, Jacobian rows / row max {ejr:.1e}")
         assert evr <= tv and ejr <= tj
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("name,ldc,precision", [("minimal", False, 0), ("TestModInv", False, 0), ("TestModInv", True, 0),
+                                                ("mixed_surf", False, 1), ("non_ordered", False, 0),
+                                                ("Lambda_search", False, 1)])
+def test_schur_form_matches_direct_form_and_oracle(name, ldc, precision):
+    """The forward by elimination of the mixed-boundary nodes (one interior
+    factorisation per wavenumber, dense Schur complement per electrode)
+    against the reference's per-system loop on the device and against the
+    oracle: potentials and voltages to 1e-10 (both forms FP64 here; the
+    Schur form is FP64 in the mixed precision form too)."""
+    from fixtures import load_forward_case
+    from crtomo_stable_b200.lib import FORWARD_DIRECT, FORWARD_SCHUR, Context
+    case = load_forward_case(name)
+    c = case["cfg"]
+    ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=c.swrtr, lsink=c.lsink,
+                  nsink=c.nsink, precision=precision)
+    form, m, nI, mbI = ctx.forward_info()
+    assert m > 0 and nI + m == case["mesh"].sanz and 0 < mbI <= case["mesh"].mb
+    ctx.set_forward_form(FORWARD_SCHUR)
+    v_s, sa_s, kp_s = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+    assert ctx.forward_info()[0] == FORWARD_SCHUR
+    ctx.set_forward_form(FORWARD_DIRECT)
+    v_d, sa_d, kp_d = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+    assert ctx.forward_info()[0] == FORWARD_DIRECT
+    from oracle.oracle import OracleProblem
+    op = OracleProblem(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=c.swrtr,
+                       lsink=c.lsink, nsink=c.nsink, kwn=ctx.kwn, kwnwi=ctx.kwnwi)
+    kp_o = op.forward(case["sigma"], ldc=ldc, nthreads=_threads())
+    volt_o, _ = op.bvolti(op.rtrafo(kp_o))
+    scale = np.abs(kp_o).max()
+    assert np.abs(kp_s - kp_o).max() <= RTOL_FP64 * scale
+    assert np.abs(kp_s - kp_d).max() <= (RTOL_FP64 if precision == 0 or ldc else 1e-9) * scale
+    np.testing.assert_allclose(v_s, volt_o, rtol=RTOL_FP64, atol=RTOL_FP64 * np.abs(volt_o).max())
+    if ldc:
+        assert np.abs(kp_s.imag).max() == 0.0
+    ctx.close()
+
+
+def test_schur_form_is_refused_where_it_does_not_apply():
+    """No mixed boundary (the 2D decoupling grid): the Schur form does not
+    apply, the setter says so (errnr 201) and the direct form runs."""
+    from fixtures import load_forward_case
+    from crtomo_stable_b200.lib import FORWARD_DIRECT, FORWARD_SCHUR, CRTError, Context
+    case = load_forward_case("grid_decoupling")
+    c = case["cfg"]
+    ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=c.swrtr, lsink=c.lsink,
+                  nsink=c.nsink)
+    with pytest.raises(CRTError) as ei:
+        ctx.set_forward_form(FORWARD_SCHUR)
+    assert ei.value.errnr == 201
+    ctx.forward(case["sigma"])
+    assert ctx.forward_info()[:2] == (FORWARD_DIRECT, 0)
+    ctx.close()
