@@ -151,10 +151,11 @@ struct crt_ctx {
     int *d_sI_row_ptr = nullptr, *d_sI_ent_d = nullptr, *d_sI_ent_ptr = nullptr, *d_sI_con_code = nullptr,
         *d_sI_con_sig = nullptr;
     unsigned char* d_sI_dflag = nullptr;
-    void *d_sLI = nullptr, *d_sX = nullptr, *d_sS0 = nullptr, *d_sS = nullptr, *d_sxg = nullptr, *d_scval = nullptr;
+    void *d_sLI = nullptr, *d_sLrev = nullptr, *d_sX = nullptr, *d_sC = nullptr, *d_sS = nullptr, *d_sxg = nullptr,
+         *d_scval = nullptr;
     double* d_sfak = nullptr;
     int sS_chunk = 0;
-    int sev[5] = {-1, -1, -1, -1, -1};   // after the factor, msolve, S0, Cholesky, rebuild
+    int sev[5] = {-1, -1, -1, -1, -1};   // after the forward sweep, the Gram products, the Cholesky, the back sweep
 };
 
 namespace {
@@ -391,7 +392,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     for (void* p : ctx->schur_bufs)
         if (p) cudaFree(p);
-    void* sws[] = {ctx->d_sLI, ctx->d_sX, ctx->d_sS0, ctx->d_sS, ctx->d_sxg, ctx->d_scval, ctx->d_sfak};
+    void* sws[] = {ctx->d_sLI, ctx->d_sLrev, ctx->d_sX, ctx->d_sC, ctx->d_sS, ctx->d_sxg, ctx->d_scval, ctx->d_sfak};
     for (void* p : sws)
         if (p) cudaFree(p);
     void* ptrs[] = {ctx->d_nrel0, ctx->d_snr0, ctx->d_etyp, ctx->d_enk, ctx->d_enr0, ctx->d_mixed_rel,
@@ -620,7 +621,7 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
             for (int q = 0; q < 2; ++q) gnodes.push_back(nrel0[(size_t)(m.elanz + rel) * m.maxnodes + q]);
         SchurHost& H = ctx->schur_h;
         if (schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H) == CRT_OK &&
-            schur_msolve_smem<cd>(H.mbI, H.mbI + 1) <= 227 * 1024 &&
+            schur_sweep_smem<cd>(H.mbI, H.mbI + 1, SCHUR_MS_R) <= 227 * 1024 &&
             (size_t)(16 + 1) * H.m * sizeof(cd) <= 227 * 1024 && band_factor_smem<cd>(H.mbI + 1) <= 227 * 1024) {
             auto up = [&](int** d, const std::vector<int>& v) {
                 const std::vector<int> one(1, 0);
@@ -632,13 +633,15 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
             SchurArgs& S = ctx->schur;
             int *p_permI = nullptr, *p_gam = nullptr, *p_pis = nullptr, *p_pgs = nullptr, *p_gip = nullptr,
                 *p_gipos = nullptr, *p_gient = nullptr, *p_gig = nullptr, *p_ggg = nullptr, *p_ggh = nullptr,
-                *p_gge = nullptr, *p_co = nullptr, *p_bs = nullptr;
+                *p_gge = nullptr, *p_co = nullptr, *p_bs = nullptr, *p_first = nullptr, *p_gsort = nullptr,
+                *p_gfirst = nullptr;
             const AssemblyLists& li = H.lists_I;
             std::vector<unsigned char> zf(H.nI, 0);
             bool su = up(&p_permI, H.permI) && up(&p_gam, H.gam) && up(&p_pis, H.posI_src) && up(&p_pgs, H.posG_src) &&
                       up(&p_gip, H.gi_ptr) && up(&p_gipos, H.gi_pos) && up(&p_gient, H.gi_ent) && up(&p_gig, H.gi_g) &&
                       up(&p_ggg, H.gg_g) && up(&p_ggh, H.gg_h) && up(&p_gge, H.gg_ent) && up(&p_co, H.col_order) &&
-                      up(&p_bs, H.blk_start) && up(&ctx->d_sI_row_ptr, li.row_ptr) && up(&ctx->d_sI_ent_d, li.ent_d) &&
+                      up(&p_bs, H.blk_start) && up(&p_first, H.first) && up(&p_gsort, H.gsort) &&
+                      up(&p_gfirst, H.gfirst) && up(&ctx->d_sI_row_ptr, li.row_ptr) && up(&ctx->d_sI_ent_d, li.ent_d) &&
                       up(&ctx->d_sI_ent_ptr, li.ent_ptr) && up(&ctx->d_sI_con_code, li.con_code) &&
                       up(&ctx->d_sI_con_sig, li.con_sig) && upload(ctx, &ctx->d_sI_dflag, zf.data(), zf.size());
             if (!su) return fail(ctx, CRT_ERR_ALLOC);
@@ -668,6 +671,9 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
             S.gg_ent = p_gge;
             S.col_order = p_co;
             S.blk_start = p_bs;
+            S.first = p_first;
+            S.gsort = p_gsort;
+            S.gfirst = p_gfirst;
             ctx->schur_ok = 1;
         }
     }
@@ -971,8 +977,8 @@ size_t schur_bytes(const crt_ctx* ctx, int chunk)
 {
     const SchurHost& H = ctx->schur_h;
     const size_t K = ctx->K, L = ctx->L, nI = H.nI, m = H.m;
-    return sizeof(cd) * (K * nI * (H.mbI + 2) + K * (L + m) * nI + K * std::max<size_t>(H.gi_pos.size(), 1) +
-                         K * m * m + K * L * m + (size_t)chunk * m * m) +
+    return sizeof(cd) * (2 * K * nI * (H.mbI + 2) + K * (L + m) * nI + K * std::max<size_t>(H.gi_pos.size(), 1) +
+                         K * (L + m) * m + K * L * m + (size_t)chunk * m * m) +
            sizeof(double) * K * nI;
 }
 
@@ -988,9 +994,10 @@ bool use_schur(const crt_ctx* ctx)
 }
 
 // Forward in the Schur form (crt_schur.h): interior factorisation per
-// wavenumber, multi-RHS band solve of [r_I | A_IG], S0 = -A_GI Y, dense
-// Cholesky of every S_l with its boundary solve, rebuild of kpot.  FP64
-// arithmetic (T = complex128, or double for the real DC systems).
+// wavenumber, forward sweep of [F r_I | F A_IG], Gram products V^T [u^ | V^],
+// dense Cholesky of every S_l with its boundary solve, z^ = u^ - V^ p_G and
+// the back sweep into kpot.  FP64 arithmetic (T = complex128, or double for
+// the real DC systems).
 template <typename T>
 int run_forward_schur(crt_ctx* ctx)
 {
@@ -1006,19 +1013,21 @@ int run_forward_schur(crt_ctx* ctx)
         const size_t per = sizeof(cd) * (size_t)m * m;
         ctx->sS_chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)K * L, (8ull << 30) / per));
         CK(cudaMalloc(&ctx->d_sLI, sizeof(cd) * (size_t)K * nI * (H.mbI + 2)));
+        CK(cudaMalloc(&ctx->d_sLrev, sizeof(cd) * (size_t)K * nI * (H.mbI + 2)));
         CK(cudaMalloc((void**)&ctx->d_sfak, sizeof(double) * (size_t)K * nI));
         CK(cudaMalloc(&ctx->d_sX, sizeof(cd) * (size_t)K * ncol * nI));
         CK(cudaMalloc(&ctx->d_scval, sizeof(cd) * (size_t)K * std::max(ncpl, 1)));
-        CK(cudaMalloc(&ctx->d_sS0, sizeof(cd) * (size_t)K * m * m));
+        CK(cudaMalloc(&ctx->d_sC, sizeof(cd) * (size_t)K * ncol * m));
         CK(cudaMalloc(&ctx->d_sxg, sizeof(cd) * (size_t)K * L * m));
         CK(cudaMalloc(&ctx->d_sS, per * ctx->sS_chunk));
     }
     T* X = static_cast<T*>(ctx->d_sX);
     T* cval = static_cast<T*>(ctx->d_scval);
-    T* S0 = static_cast<T*>(ctx->d_sS0);
+    T* Cg = static_cast<T*>(ctx->d_sC);
     T* xg = static_cast<T*>(ctx->d_sxg);
     T* Sws = static_cast<T*>(ctx->d_sS);
     T* LI = static_cast<T*>(ctx->d_sLI);
+    T* Lrev = static_cast<T*>(ctx->d_sLrev);
     SchurArgs S = ctx->schur;
     S.WI = WI;
     S.status = ctx->d_status;
@@ -1071,36 +1080,40 @@ int run_forward_schur(crt_ctx* ctx)
     ctx->fwd_marks.clear();
     crt_ctx::FwdMark mk{};
     mk.e0 = tev_rec(ctx);
-    CK(cudaMemsetAsync(X, 0, sizeof(T) * (size_t)K * ncol * nI, ctx->st));
-    launch_schur_rhs<T>(S, Af, X, cval, ctx->st);
-    bool blk = false;
-    if (band_blk_fits<T>(H.mbI)) {
-        const int pb = band_panel<T>(AI, !ctx->capture, ctx->st);
+    const bool blk = band_blk_fits<T>(H.mbI);
+    int pb = 0;
+    if (blk) {
+        pb = band_panel<T>(AI, !ctx->capture, ctx->st);
         ctx->panel = pb & BAND_PANEL_MASK;
-        launch_band_prep<T>(AI, ctx->st);
-        mk.e8 = tev_rec(ctx);
+        launch_band_prep<T>(AI, ctx->st);   // the scaling factors for the right-hand sides
+    }
+    CK(cudaMemsetAsync(X, 0, sizeof(T) * (size_t)K * ncol * nI, ctx->st));
+    mk.e8 = tev_rec(ctx);
+    if (blk) {
+        launch_schur_rhs<T>(S, Af, ctx->d_sfak, X, cval, ctx->st);
         launch_band_factor_blk<T>(AI, pb, ctx->st);
-        blk = true;
     } else {
-        mk.e8 = tev_rec(ctx);
-        launch_band_factor<T>(AI, ctx->st);
+        launch_band_factor<T>(AI, ctx->st);   // forms fak as it goes
+        launch_schur_rhs<T>(S, Af, ctx->d_sfak, X, cval, ctx->st);
     }
     if (int e = kernel_check(ctx, "interior factor")) return e;
     mk.e1 = tev_rec(ctx);
     mk.blk = blk;
-    launch_schur_msolve<T>(S, LI, AI.lstride, ctx->d_sfak, X, ctx->st);
+    launch_schur_transpose<T>(S, LI, Lrev, ctx->st);
+    launch_schur_forward<T>(S, LI, X, ctx->st);
     ctx->sev[0] = tev_rec(ctx);
-    launch_schur_s0<T>(S, X, cval, S0, ctx->st);
+    launch_schur_gram<T>(S, X, Cg, ctx->st);
     ctx->sev[1] = tev_rec(ctx);
     for (int s0 = 0; s0 < K * L; s0 += ctx->sS_chunk)
-        launch_schur_chol<T>(S, Af, S0, X, cval, Sws, xg, s0, std::min(ctx->sS_chunk, K * L - s0), ctx->st);
+        launch_schur_chol<T>(S, Af, Cg, Sws, xg, s0, std::min(ctx->sS_chunk, K * L - s0), ctx->st);
     ctx->sev[2] = tev_rec(ctx);
-    launch_schur_out<T>(S, X, xg, ctx->n, ctx->d_kpot, ctx->st);
+    launch_schur_zrebuild<T>(S, X, xg, ctx->st);
+    launch_schur_back<T>(S, Lrev, ctx->d_sfak, X, xg, ctx->n, ctx->d_kpot, ctx->st);
     if (int e = kernel_check(ctx, "Schur kernels")) return e;
     mk.e2 = tev_rec(ctx);
     ctx->sev[3] = mk.e2;
     ctx->fwd_marks.push_back(mk);
-    ctx->launches += 10 + (K * L + ctx->sS_chunk - 1) / ctx->sS_chunk;
+    ctx->launches += 11 + (K * L + ctx->sS_chunk - 1) / ctx->sS_chunk;
     ctx->timings[9] = 1;
     ctx->timings[12] = blk ? ctx->panel : 0;
     return CRT_OK;
@@ -1129,7 +1142,8 @@ void resolve_forward_timings(crt_ctx* ctx)
     ctx->timings[8] = ms_fk;
     ctx->timings[10] = ms_res;
     ctx->timings[11] = ms_cor;
-    // Schur form: multi-RHS solve, S0 + boundary Cholesky, rebuild
+    // Schur form: forward sweep, Gram products + boundary Cholesky,
+    // rebuild + back sweep
     if (ctx->schur_used && !ctx->fwd_marks.empty()) {
         const crt_ctx::FwdMark& m0 = ctx->fwd_marks[0];
         ctx->timings[13] = tev_ms(ctx, m0.e1, ctx->sev[0]);

@@ -1,24 +1,27 @@
 // crt_schur.cu -- forward model by elimination of the mixed-boundary nodes
-// (see crt_schur.h for the algebra).  Kernels:
+// (see crt_schur.h for the algebra).  Kernels, in the order they run:
 //
-//   k_schur_rhs_src / k_schur_rhs_cpl  right-hand sides [r_I | A_IG] of the
-//       multi-RHS solve, one column per source electrode and per boundary
-//       node, and the coupling values a(g, i) kept for the later steps;
-//   k_schur_msolve  forward and back substitution of SCHUR_MS_R columns per
-//       CTA against one wavenumber's interior factor: the factor streams
-//       through shared memory in blocks of SCHUR_MS_BB columns (one bulk
-//       copy per block, double-buffered, bounded mbarrier wait), the
-//       right-hand sides live in a sliding window of rows; each block is a
-//       16-row triangle (one half-warp per column, shuffle broadcasts) and a
-//       (mb x 16) x (16 x 32) update of the rows below it (4 x 4 register
-//       tiles) -- in the back pass the mirrored dot products;
-//   k_schur_s0      S0 = -A_GI Y per wavenumber;
-//   k_schur_chol    per (k, l): S_l = S0 + A_GG(l), right-looking blocked
-//       Cholesky (unconjugated, complex symmetric as src/chol.f90:44-78)
-//       with a 16-column panel in shared memory and 4 x 4 register tiles for
-//       the trailing update, then the two triangular solves for p_G;
-//   k_schur_out     kpot = w - Y p_G (a 64 x 32 tiled GEMM per wavenumber)
-//       on the interior rows, p_G on the boundary rows.
+//   k_schur_rhs_src / k_schur_rhs_cpl  the columns F r_I (one per source
+//       electrode) and F A_IG (one per boundary node) of the interior
+//       solves, and the coupling values a(g, i) kept for later steps;
+//   k_schur_transpose  the interior factor reversed and row-packed, so the
+//       back substitution runs as a forward sweep;
+//   k_schur_sweep   banded triangular sweep of R columns per CTA (forward for
+//       all columns, each block from its first non-zero row; back for the
+//       source columns): the factor streams through shared memory in blocks
+//       of 16 columns (one bulk copy each, double-buffered, bounded
+//       mbarrier wait), the right-hand sides in a window of rows that arrive
+//       by cp.async two blocks ahead; per block a 16-row triangle (half-warp
+//       per column, shuffle broadcasts) and an (mb x 16) x (16 x R) update
+//       in 4 x 4 register tiles;
+//   k_schur_gram    C = V^T [u^ | V^] per wavenumber (tiled GEMM that skips
+//       the rows where a column is still zero);
+//   k_schur_chol    per (k, l): S_l = A_GG(l) - V^T V^, right-looking
+//       blocked Cholesky (unconjugated, complex symmetric as
+//       src/chol.f90:44-78) with a 16-column panel in shared memory, the
+//       forward solve fused into the factorisation, the back solve by panels;
+//   k_schur_zrebuild  z^ = u^ - V^ p_G (tiled GEMM);
+//   k_schur_out_gam p_G into kpot at the boundary nodes.
 #include "crt_schur.h"
 
 #include <algorithm>
@@ -105,6 +108,12 @@ int schur_plan_host(const AssemblyLists& full, int n, const std::vector<int>& ga
         if (o.posI_src[l] >= 0) first[l] = std::min(first[l], o.posI_src[l]);
         if (o.posI_sink >= 0) first[l] = std::min(first[l], o.posI_sink);
     }
+    o.first = first;
+    o.gsort.resize(o.m);
+    std::iota(o.gsort.begin(), o.gsort.end(), 0);
+    std::stable_sort(o.gsort.begin(), o.gsort.end(), [&](int a, int b) { return first[o.L + a] < first[o.L + b]; });
+    o.gfirst.resize(o.m);
+    for (int q = 0; q < o.m; ++q) o.gfirst[q] = first[o.L + o.gsort[q]];
     // columns by their first non-zero row, so that a block's forward pass
     // starts where its earliest column does
     const int ncol = o.L + o.m;
@@ -129,22 +138,6 @@ template <> __device__ __forceinline__ cd shfl_w<cd>(cd v, int src, int width)
 {
     return cd{__shfl_sync(0xffffffffu, v.x, src, width), __shfl_sync(0xffffffffu, v.y, src, width)};
 }
-template <typename T> __device__ __forceinline__ T shfl_xor1(T v);
-template <> __device__ __forceinline__ double shfl_xor1<double>(double v) { return __shfl_xor_sync(0xffffffffu, v, 1); }
-template <> __device__ __forceinline__ cd shfl_xor1<cd>(cd v)
-{
-    return cd{__shfl_xor_sync(0xffffffffu, v.x, 1), __shfl_xor_sync(0xffffffffu, v.y, 1)};
-}
-template <typename T> __device__ __forceinline__ T shfl_down_full(T v, int off);
-template <> __device__ __forceinline__ double shfl_down_full<double>(double v, int off)
-{
-    return __shfl_down_sync(0xffffffffu, v, off);
-}
-template <> __device__ __forceinline__ cd shfl_down_full<cd>(cd v, int off)
-{
-    return cd{__shfl_down_sync(0xffffffffu, v.x, off), __shfl_down_sync(0xffffffffu, v.y, off)};
-}
-
 // acc += a b (complex: four fused multiply-adds)
 __device__ __forceinline__ void fma_acc(cd& acc, cd a, cd b)
 {
@@ -155,21 +148,43 @@ __device__ __forceinline__ void fma_acc(cd& acc, cd a, cd b)
 }
 __device__ __forceinline__ void fma_acc(double& acc, double a, double b) { acc = fma(a, b, acc); }
 
+template <typename T> __device__ __forceinline__ T shfl_xor_t(T v, int mask);
+template <> __device__ __forceinline__ double shfl_xor_t<double>(double v, int mask)
+{
+    return __shfl_xor_sync(0xffffffffu, v, mask);
+}
+template <> __device__ __forceinline__ cd shfl_xor_t<cd>(cd v, int mask)
+{
+    return cd{__shfl_xor_sync(0xffffffffu, v.x, mask), __shfl_xor_sync(0xffffffffu, v.y, mask)};
+}
+
+// one element global -> shared, asynchronously (cp.async; both addresses
+// aligned to the element)
+template <typename T> __device__ __forceinline__ void cp_async_elem(T* dst, const T* src);
+template <> __device__ __forceinline__ void cp_async_elem<cd>(cd* dst, const cd* src) { cp_async16(dst, src); }
+template <> __device__ __forceinline__ void cp_async_elem<double>(double* dst, const double* src)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(src) : "memory");
+}
+
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void k_schur_rhs_src(SchurArgs s, T* X)
+__global__ void k_schur_rhs_src(SchurArgs s, const double* __restrict__ fakws, T* X)
 {
     const int idx = blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= s.K * s.L) return;
     const int k = idx / s.L, l = idx % s.L;
     T* col = X + ((size_t)k * s.ncol + l) * s.nI;
-    // r = e_src - e_sink (A pot = r; the reference's b = -r, src/kompab.f90)
-    if (s.posI_src[l] >= 0) col[s.posI_src[l]] = Sc<T>::one();
-    if (s.lsink && s.posI_sink >= 0) col[s.posI_sink] -= Sc<T>::one();
+    const double* fk = fakws + (size_t)k * s.nI;
+    // r = e_src - e_sink (A pot = r; the reference's b = -r, src/kompab.f90),
+    // scaled by fak
+    if (s.posI_src[l] >= 0) col[s.posI_src[l]] = scale(Sc<T>::one(), fk[s.posI_src[l]]);
+    if (s.lsink && s.posI_sink >= 0) col[s.posI_sink] -= scale(Sc<T>::one(), fk[s.posI_sink]);
 }
 
 template <typename T>
-__global__ void k_schur_rhs_cpl(SchurArgs s, BandArgs<T> A, T* X, T* cval)
+__global__ void k_schur_rhs_cpl(SchurArgs s, BandArgs<T> A, const double* __restrict__ fakws, T* X, T* cval)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= (long long)s.K * s.ncpl) return;
@@ -177,36 +192,60 @@ __global__ void k_schur_rhs_cpl(SchurArgs s, BandArgs<T> A, T* X, T* cval)
     // an interior-boundary entry has area contributions only (l unused)
     const T a = band_assemble_entry<T>(A, s.gi_ent[q], k, 0);
     cval[idx] = a;
-    X[((size_t)k * s.ncol + s.L + s.gi_g[q]) * s.nI + s.gi_pos[q]] = a;
+    const int i = s.gi_pos[q];
+    X[((size_t)k * s.ncol + s.L + s.gi_g[q]) * s.nI + i] = scale(a, fakws[(size_t)k * s.nI + i]);
+}
+
+// Lrev[k][c'][d] = L(r, r - d), r = n - 1 - c' (0 where r - d < 0).
+template <typename T>
+__global__ void k_schur_transpose(SchurArgs s, const T* __restrict__ Lws, T* Lrev)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = s.nI, W = s.WI;
+    const long long per = (long long)n * W;
+    if (idx >= (long long)s.K * per) return;
+    const int k = (int)(idx / per), cp = (int)((idx % per) / W), d = (int)(idx % W);
+    const int r = n - 1 - cp, c = r - d;
+    const T* Lk = Lws + (size_t)k * per;
+    Lrev[idx] = (c >= 0 && d <= s.mbI) ? Lk[(size_t)c * W + d] : Sc<T>::zero();
 }
 
 // ---------------------------------------------------------------------------
-// Multi-RHS band solve: grid (column blocks, K).  Window Z[WZ][R] in shared
-// memory, row r at slot r mod WZ, WZ >= mb + 2 BB so that the rows entering
-// for the next block never share a slot with a row still in use.
+// Banded lower-triangular sweep L z = b for R columns per CTA: grid (column
+// blocks, K).  The factor's columns stream through shared memory BB at a
+// time (one bulk copy each, double-buffered, bounded mbarrier wait); the
+// right-hand sides live in a window Z[WZ][R] (row r at slot r mod WZ,
+// WZ >= mb + 3 BB), their rows arriving by cp.async two blocks ahead of
+// use.  Per block: the BB x BB triangle (one half-warp per column, shuffle
+// broadcasts), the finished rows out, and the (mb x BB) x (BB x R) update
+// of the rows below (4 x 4 register tiles).
+//   back == 0: forward sweep of X's columns (col_order, from each block's
+//     first non-zero row), in place;
+//   back == 1: the back sweep L^T x^ = z^ of the source columns: Lws holds
+//     the reversed row-packed factor and the rows are read reversed; the
+//     solution goes out as kpot = fak x^ at the interior rows' nodes.
 template <typename T, int NT, int R, int BB>
-__global__ void __launch_bounds__(NT, 1) k_schur_msolve(SchurArgs s, const T* __restrict__ Lws, size_t lstride,
-                                                        const double* __restrict__ fakws, T* X, int WZ)
+__global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __restrict__ Lws,
+                                                       const double* __restrict__ fakws, T* X, cd* kpot, int n_kpot,
+                                                       int WZ, int back)
 {
-    static_assert(BB == 16 && R % 4 == 0 && NT % 16 == 0 && R % (NT / 16) == 0, "msolve layout");
-    extern __shared__ __align__(16) unsigned char ms_dyn[];
+    static_assert(BB == 16 && R % 4 == 0 && R <= 32 && NT % 32 == 0 && NT >= R, "sweep layout");
+    extern __shared__ __align__(16) unsigned char sw_dyn[];
     const int W = s.WI, n = s.nI, mb = s.mbI;
-    T* Lb = reinterpret_cast<T*>(ms_dyn);                              // [2][BB * W]
-    T* Z = Lb + 2 * BB * W;                                            // [WZ][R]
-    double* fz = reinterpret_cast<double*>(Z + (size_t)WZ * R);        // [WZ]
+    T* Lb = reinterpret_cast<T*>(sw_dyn);   // [2][BB * W]
+    T* Z = Lb + 2 * BB * W;                 // [WZ][R]
     __shared__ T dinv[BB];
     __shared__ int colid[R];
     __shared__ __align__(8) unsigned long long bar[2];
     __shared__ int s_err;
     const int tid = threadIdx.x;
     const int blk = blockIdx.x, k = blockIdx.y;
-    const int start = s.blk_start[blk];
+    const int start = back ? 0 : s.blk_start[blk];
     if (start >= n) return;   // every column of the block is zero, and so is its solution
-    const T* Lk = Lws + (size_t)k * lstride;
-    const double* fk = fakws + (size_t)k * n;
+    const T* Lk = Lws + (size_t)k * n * W;
     if (tid < R) {
         const int c = blk * R + tid;
-        colid[tid] = c < s.ncol ? s.col_order[c] : -1;
+        colid[tid] = back ? (c < s.L ? c : -1) : (c < s.ncol ? s.col_order[c] : -1);
     }
     if (tid == 0) {
         s_err = 0;
@@ -214,206 +253,232 @@ __global__ void __launch_bounds__(NT, 1) k_schur_msolve(SchurArgs s, const T* __
         mbar_init(&bar[1], 1);
     }
     __syncthreads();
-    int ph[2] = {0, 0};
+    int ph0 = 0, ph1 = 0;
     auto colp = [&](int j) { return X + ((size_t)k * s.ncol + colid[j]) * n; };
-    // factor columns [c0, c0 + nb) (one contiguous run of the column-packed
-    // factor) into buffer `buf` by one bulk copy
     auto fetch = [&](int c0, int buf) {
         if (tid == 0) {
-            const int nb = min(BB, n - c0);
-            const int bytes = nb * W * (int)sizeof(T);
+            const int bytes = min(BB, n - c0) * W * (int)sizeof(T);
             mbar_expect_tx(&bar[buf], bytes);
             bulk_g2s(Lb + (size_t)buf * BB * W, Lk + (size_t)c0 * W, bytes, &bar[buf]);
         }
     };
     auto wait = [&](int buf) {
-        if (!mbar_wait(&bar[buf], ph[buf])) s_err = 1;
-        ph[buf] ^= 1;
+        int& ph = buf ? ph1 : ph0;
+        if (!mbar_wait(&bar[buf], ph)) s_err = 1;
+        ph ^= 1;
     };
-    // rows [r0, r1) of every column into the window; scaled (fak o b) for
-    // the forward pass, as stored (z) for the back pass
-    auto load_rows = [&](int r0, int r1, bool scale_in) {
+    // rows [r0, r1) of every column into their slots, one commit group
+    auto issue_rows = [&](int r0, int r1) {
         const int nr = r1 - r0;
         for (int idx = tid; idx < nr * R; idx += NT) {
             const int j = idx / nr, r = r0 + idx % nr;
-            const double f = fk[r];
-            T v = Sc<T>::zero();
-            if (colid[j] >= 0) {
-                v = colp(j)[r];
-                if (scale_in) v = scale(v, f);
-            }
-            Z[(r % WZ) * R + j] = v;
-            if (j == 0) fz[r % WZ] = f;
+            T* dst = Z + (size_t)(r % WZ) * R + j;
+            if (colid[j] >= 0) cp_async_elem<T>(dst, colp(j) + (back ? n - 1 - r : r));
+            else *dst = Sc<T>::zero();
         }
+        cp_async_commit();
     };
-
-    // ---- forward substitution L z = fak o b from the block's first row
-    load_rows(start, min(n, start + BB + mb), true);
+    issue_rows(start, min(n, start + BB + mb));
+    issue_rows(min(n, start + BB + mb), min(n, start + 2 * BB + mb));
     fetch(start, 0);
-    int buf = 0;
+    cp_async_wait_group<1>();
     __syncthreads();
+    int buf = 0;
     for (int c0 = start; c0 < n; c0 += BB) {
         const int nb = min(BB, n - c0);
         wait(buf);
         if (c0 + BB < n) fetch(c0 + BB, buf ^ 1);
+        // the rows two blocks ahead (their slots held rows finished a block ago)
+        issue_rows(min(n, c0 + 2 * BB + mb), min(n, c0 + 3 * BB + mb));
         const T* Lc = Lb + (size_t)buf * BB * W;
         if (tid < nb) dinv[tid] = Sc<T>::recip(Lc[tid * W]);
         __syncthreads();
-        {   // the block's triangle: one half-warp per column, lane t = row c0 + t
-            const int hw = tid >> 4, t = tid & 15;
-            for (int j = hw; j < R; j += NT / 16) {
-                T v = t < nb ? Z[((c0 + t) % WZ) * R + j] : Sc<T>::zero();
-                for (int u = 0; u < nb; ++u) {
-                    if (t == u) v = Sc<T>::mul(v, dinv[u]);
-                    const T y = shfl_w(v, u, 16);
-                    if (t > u && t < nb && t - u <= mb) fms_acc(v, Lc[u * W + (t - u)], y);
+        // the block's rows sit in consecutive slots (WZ is a multiple of BB)
+        const int sb = c0 % WZ;
+        if (tid < R) {   // the block's triangle: a lane per column, its 16 rows in registers
+            const int j = tid;
+            T z[BB];
+#pragma unroll
+            for (int t = 0; t < BB; ++t) z[t] = t < nb ? Z[(size_t)(sb + t) * R + j] : Sc<T>::zero();
+#pragma unroll
+            for (int u = 0; u < BB; ++u) {
+                if (u < nb) {
+                    z[u] = Sc<T>::mul(z[u], dinv[u]);
+#pragma unroll
+                    for (int t = u + 1; t < BB; ++t)
+                        if (t < nb && t - u <= mb) fms_acc(z[t], Lc[u * W + (t - u)], z[u]);
                 }
-                if (t < nb) Z[((c0 + t) % WZ) * R + j] = v;
             }
+#pragma unroll
+            for (int t = 0; t < BB; ++t)
+                if (t < nb) Z[(size_t)(sb + t) * R + j] = z[t];
         }
         __syncthreads();
-        // the block's rows are final: out to X
+        // the block's rows are final: out
         for (int idx = tid; idx < nb * R; idx += NT) {
             const int j = idx / nb, t = idx % nb;
-            if (colid[j] >= 0) colp(j)[c0 + t] = Z[((c0 + t) % WZ) * R + j];
+            if (colid[j] < 0) continue;
+            const int r = c0 + t;
+            const T v = Z[(size_t)(sb + t) * R + j];
+            if (!back) {
+                colp(j)[r] = v;
+            } else {
+                const int i = n - 1 - r;
+                kpot[((size_t)k * s.L + colid[j]) * n_kpot + s.permI[i]] =
+                    Sc<T>::to_cd(scale(v, fakws[(size_t)k * n + i]));
+            }
         }
-        {   // rows [c0 + nb, c0 + nb + mb) take the block's columns
+        {   // rows [c0 + nb, c0 + nb + mb) take the block's columns: a thread
+            // owns rows rq + NQ a and columns jq + (R/4) c, so a warp's loads
+            // fall on consecutive words
             const int rlo = c0 + nb, rhi = min(n, c0 + nb + mb);
-            const int nq = (rhi - rlo + 3) / 4;
-            for (int tile = tid; tile < nq * (R / 4); tile += NT) {
-                const int r0 = rlo + 4 * (tile / (R / 4)), j0 = 4 * (tile % (R / 4));
+            const int NQ = (rhi - rlo + 3) >> 2;
+            constexpr int RJ = R / 4;
+            for (int tile = tid; tile < NQ * RJ; tile += NT) {
+                const int rq = tile / RJ, jq = tile % RJ;
                 T acc[4][4];
+                int sl[4];
 #pragma unroll
-                for (int a = 0; a < 4; ++a)
+                for (int a = 0; a < 4; ++a) {
+                    const int r = rlo + rq + NQ * a;
+                    sl[a] = r < rhi ? r % WZ : -1;
 #pragma unroll
                     for (int c = 0; c < 4; ++c)
-                        acc[a][c] = r0 + a < rhi ? Z[((r0 + a) % WZ) * R + j0 + c] : Sc<T>::zero();
-                for (int u = 0; u < nb; ++u) {
-                    T zc[4], lv[4];
+                        acc[a][c] = sl[a] >= 0 ? Z[(size_t)sl[a] * R + jq + RJ * c] : Sc<T>::zero();
+                }
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) zc[c] = Z[((c0 + u) % WZ) * R + j0 + c];
+                for (int u = 0; u < BB; ++u) {
+                    if (u < nb) {
+                        T zc[4], lv[4];
 #pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        const int d = r0 + a - (c0 + u);
-                        lv[a] = (r0 + a < rhi && d <= mb) ? Lc[u * W + d] : Sc<T>::zero();
+                        for (int c = 0; c < 4; ++c) zc[c] = Z[(size_t)(sb + u) * R + jq + RJ * c];
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) {
+                            const int d = rlo + rq + NQ * a - (c0 + u);
+                            lv[a] = (sl[a] >= 0 && d <= mb) ? Lc[u * W + d] : Sc<T>::zero();
+                        }
+#pragma unroll
+                        for (int a = 0; a < 4; ++a)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c) fms_acc(acc[a][c], lv[a], zc[c]);
                     }
-#pragma unroll
-                    for (int a = 0; a < 4; ++a)
-#pragma unroll
-                        for (int c = 0; c < 4; ++c) fms_acc(acc[a][c], lv[a], zc[c]);
                 }
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
-                    if (r0 + a < rhi)
+                    if (sl[a] >= 0)
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) Z[((r0 + a) % WZ) * R + j0 + c] = acc[a][c];
+                        for (int c = 0; c < 4; ++c) Z[(size_t)sl[a] * R + jq + RJ * c] = acc[a][c];
             }
         }
-        // the rows the next block reaches enter the window
-        if (c0 + BB < n) load_rows(min(n, c0 + BB + mb), min(n, c0 + 2 * BB + mb), true);
         // the buffer just read is the destination of the bulk copy after next
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        cp_async_wait_group<1>();   // the rows of the next block have landed
         __syncthreads();
         buf ^= 1;
     }
-
-    // ---- back substitution L^T x = z from the last block; the window holds
-    // the solved rows [c1, c1 + mb) and the block's z rows [c0, c1)
-    const int last0 = (n - 1) / BB * BB;
-    load_rows(last0, n, false);
-    fetch(last0, buf);
-    __syncthreads();
-    for (int c0 = last0; c0 >= 0; c0 -= BB) {
-        const int nb = min(BB, n - c0), c1 = c0 + nb;
-        wait(buf);
-        if (c0 > 0) fetch(c0 - BB, buf ^ 1);
-        const T* Lc = Lb + (size_t)buf * BB * W;
-        if (tid < nb) dinv[tid] = Sc<T>::recip(Lc[tid * W]);
-        {   // z_t -= sum over solved rows r >= c1 of L(r, c0 + t) x_r: thread
-            // (t, 4 columns, half of the rows), halves combined by a shuffle
-            const int half = tid & 1, combo = tid >> 1;
-            const int t = combo >> 3, j0 = 4 * (combo & 7);
-            T acc[4] = {Sc<T>::zero(), Sc<T>::zero(), Sc<T>::zero(), Sc<T>::zero()};
-            if (t < nb) {
-                const int rend = min(n, c0 + t + mb + 1);
-                for (int r = c1 + half; r < rend; r += 2) {
-                    const T lv = Lc[t * W + (r - c0 - t)];
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) fma_acc(acc[c], lv, Z[(r % WZ) * R + j0 + c]);
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[c] += shfl_xor1(acc[c]);
-            if (half == 0 && t < nb)
-#pragma unroll
-                for (int c = 0; c < 4; ++c) Z[((c0 + t) % WZ) * R + j0 + c] -= acc[c];
-        }
-        __syncthreads();
-        {   // the block's triangle of L^T, from its last row up
-            const int hw = tid >> 4, t = tid & 15;
-            for (int j = hw; j < R; j += NT / 16) {
-                T v = t < nb ? Z[((c0 + t) % WZ) * R + j] : Sc<T>::zero();
-                for (int u = nb - 1; u >= 0; --u) {
-                    if (t == u) v = Sc<T>::mul(v, dinv[u]);
-                    const T x = shfl_w(v, u, 16);
-                    if (t < u && u - t <= mb) fms_acc(v, Lc[t * W + (u - t)], x);
-                }
-                if (t < nb) Z[((c0 + t) % WZ) * R + j] = v;
-            }
-        }
-        __syncthreads();
-        // x = fak o x^ out to X; the next block's z rows enter
-        for (int idx = tid; idx < nb * R; idx += NT) {
-            const int j = idx / nb, t = idx % nb;
-            const int sl = (c0 + t) % WZ;
-            if (colid[j] >= 0) colp(j)[c0 + t] = scale(Z[sl * R + j], fz[sl]);
-        }
-        if (c0 > 0) load_rows(c0 - BB, c0, false);
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        __syncthreads();
-        buf ^= 1;
-    }
+    cp_async_wait_group<0>();
     if (tid == 0 && s_err) atomicMax(&s.status[k], (int)CRT_ERR_CUDA);
 }
 
 // ---------------------------------------------------------------------------
+// C[k][c][g] = sum_i V^[i][g] X[i][c] over the rows where both columns can
+// be non-zero; tiles 64 (g) x 32 (c), 128 threads of 4 x 4.  The tiles of
+// the V^T V^ block above its diagonal are skipped (the Cholesky reads the
+// lower triangle).
 template <typename T>
-__global__ void k_schur_s0(SchurArgs s, const T* __restrict__ X, const T* __restrict__ cval, T* S0)
+__global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __restrict__ X, T* C)
 {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long mm = (long long)s.m * s.m;
-    if (idx >= (long long)s.K * mm) return;
-    const int k = (int)(idx / mm);
-    const int h = (int)((idx % mm) / s.m), g = (int)(idx % s.m);
-    if (g < h) return;
-    const T* Y = X + ((size_t)k * s.ncol + s.L + h) * s.nI;
-    const T* cv = cval + (size_t)k * s.ncpl;
-    T acc = Sc<T>::zero();
-    for (int q = s.gi_ptr[g]; q < s.gi_ptr[g + 1]; ++q) fma_acc(acc, cv[q], Y[s.gi_pos[q]]);
-    S0[(size_t)k * mm + (size_t)h * s.m + g] = -acc;
+    constexpr int TG = 64, TC = 32, TI = 16;
+    __shared__ T As[TI][TG + 1];
+    __shared__ T Bs[TI][TC + 1];
+    __shared__ int s_i0;
+    const int tid = threadIdx.x, k = blockIdx.z;
+    const int g0 = blockIdx.x * TG, c0 = blockIdx.y * TC;
+    const int m = s.m, L = s.L, nI = s.nI, ncol = s.ncol;
+    if (c0 >= L && c0 - L > g0 + TG - 1) return;
+    if (tid == 0) {
+        int fg = nI, fc = nI;
+        for (int q = 0; q < TG && g0 + q < m; ++q) fg = min(fg, s.first[L + g0 + q]);
+        for (int q = 0; q < TC && c0 + q < ncol; ++q) fc = min(fc, s.first[c0 + q]);
+        s_i0 = max(fg, fc) / TI * TI;
+    }
+    __syncthreads();
+    const int ti = tid % 16, tc = tid / 16;
+    T acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] = Sc<T>::zero();
+    const T* Xk = X + (size_t)k * ncol * nI;
+    for (int i0 = s_i0; i0 < nI; i0 += TI) {
+        for (int idx = tid; idx < TI * TG; idx += 128) {
+            const int gg = idx / TI, ii = idx % TI;
+            As[ii][gg] = (g0 + gg < m && i0 + ii < nI) ? Xk[(size_t)(L + g0 + gg) * nI + i0 + ii] : Sc<T>::zero();
+        }
+        for (int idx = tid; idx < TI * TC; idx += 128) {
+            const int cc = idx / TI, ii = idx % TI;
+            Bs[ii][cc] = (c0 + cc < ncol && i0 + ii < nI) ? Xk[(size_t)(c0 + cc) * nI + i0 + ii] : Sc<T>::zero();
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int ii = 0; ii < TI; ++ii) {
+            T a4[4], b4[4];
+            // rows ti + 16 a, columns tc + 8 c: a warp reads consecutive words
+#pragma unroll
+            for (int a = 0; a < 4; ++a) a4[a] = As[ii][ti + 16 * a];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) b4[c] = Bs[ii][tc + 8 * c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) fma_acc(acc[a][c], a4[a], b4[c]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const int cc = c0 + tc + 8 * c;
+        if (cc >= ncol) continue;
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int g = g0 + ti + 16 * a;
+            if (g < m) C[((size_t)k * ncol + cc) * m + g] = acc[a][c];
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Dense Cholesky of the Schur complements: one CTA per (k, l) system.
+// Dense Cholesky of the Schur complements, one CTA per (k, l) system:
+// S = A_GG(l) - C_VV (lower triangle, column-major, in the workspace),
+// right-looking with an NB-column panel in shared memory; the forward solve
+// L y = r_G - C[l] rides along each column, the back solve L^T x = y goes
+// panel by panel from the last (dot products of the panel columns, then the
+// panel's triangle on one warp).
 template <typename T, int NT, int NB>
-__global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A, const T* __restrict__ S0,
-                                                      const T* __restrict__ X, const T* __restrict__ cval, T* Sws,
+__global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A, const T* __restrict__ C, T* Sws,
                                                       T* xg, int sys0)
 {
+    static_assert(NT == 256 && NB == 16, "chol layout");
     extern __shared__ __align__(16) unsigned char ch_dyn[];
     const int m = s.m;
-    T* P = reinterpret_cast<T*>(ch_dyn);   // panel [NB][m]
+    T* P = reinterpret_cast<T*>(ch_dyn);   // panel [NB][m]: P[t m + r] = L(r, p0 + t)
     T* y = P + (size_t)NB * m;             // [m]
-    __shared__ T red[NT / 32];
     __shared__ int s_err;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x, sys = sys0 + b, k = sys / s.L, l = sys % s.L;
     T* S = Sws + (size_t)b * m * m;
-    const T* S0k = S0 + (size_t)k * m * m;
+    const T* Ck = C + (size_t)k * s.ncol * m;
     if (tid == 0) s_err = 0;
-    // S = S0[k] (lower triangle), plus A_GG(l)
-    for (int c = 0; c < m; ++c)
-        for (int r = c + tid; r < m; r += NT) S[(size_t)c * m + r] = S0k[(size_t)c * m + r];
+    for (int c = 0; c < m; ++c) {
+        const T* src = Ck + (size_t)(s.L + c) * m;
+        for (int r = c + tid; r < m; r += NT) S[(size_t)c * m + r] = -src[r];
+    }
+    for (int g = tid; g < m; g += NT) {
+        T v = -Ck[(size_t)l * m + g];
+        if (g == s.posG_src[l]) v += Sc<T>::one();
+        if (s.lsink && g == s.posG_sink) v -= Sc<T>::one();
+        y[g] = v;
+    }
     __syncthreads();
     for (int q = tid; q < s.ngg; q += NT) {
         const T a = band_assemble_entry<T>(A, s.gg_ent[q], k, l);
@@ -431,9 +496,17 @@ __global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A
             if (Sc<T>::bad_pivot(piv)) s_err = CRT_ERR_PIVOT;
             T root, inv;
             Sc<T>::sqrt_recip(piv, root, inv);
-            __syncthreads();   // every thread has read the pivot
-            for (int r = c + 1 + tid; r < m; r += NT) P[t * m + r] = Sc<T>::mul(P[t * m + r], inv);
-            if (tid == 0) P[t * m + c] = root;
+            const T yc = Sc<T>::mul(y[c], inv);
+            __syncthreads();   // every thread has read the pivot and y[c]
+            for (int r = c + 1 + tid; r < m; r += NT) {
+                const T lv = Sc<T>::mul(P[t * m + r], inv);
+                P[t * m + r] = lv;
+                fms_acc(y[r], lv, yc);
+            }
+            if (tid == 0) {
+                P[t * m + c] = root;
+                y[c] = yc;
+            }
             __syncthreads();
             const int rows = m - c - 1;
             for (int idx = tid; idx < (nb - t - 1) * rows; idx += NT) {
@@ -445,42 +518,60 @@ __global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A
         if (s_err) break;
         for (int t = 0; t < nb; ++t)
             for (int r = p0 + t + tid; r < m; r += NT) S[(size_t)(p0 + t) * m + r] = P[t * m + r];
-        // trailing update of the lower triangle below the panel, 4 x 4 tiles
+        // trailing update of the lower triangle below the panel by 64 x 64
+        // super-tiles (their lower triangle on the diagonal): thread (ti, tj)
+        // owns rows ti + 16 a and columns tj + 16 c of each, so a warp's
+        // loads of S are two 256-byte runs and its panel reads consecutive
+        // words; the next super-tile's entries load while the current one
+        // is updated
         const int q0 = p0 + nb, mt = m - q0;
         if (mt > 0) {
-            const int T4 = (mt + 3) / 4, ntile = T4 * (T4 + 1) / 2;
-            for (int tile = tid; tile < ntile; tile += NT) {
-                int X4 = (int)((sqrtf(8.0f * tile + 1.0f) - 1.0f) * 0.5f);
-                while ((X4 + 1) * (X4 + 2) / 2 <= tile) ++X4;
-                while (X4 * (X4 + 1) / 2 > tile) --X4;
-                const int Y4 = tile - X4 * (X4 + 1) / 2;
-                const int r0 = q0 + 4 * X4, cc0 = q0 + 4 * Y4;
-                T acc[4][4];
+            const int NS = (mt + 63) / 64, nst = NS * (NS + 1) / 2;
+            const int ti = tid & 15, tj = tid >> 4;
+            auto st_origin = [&](int st, int& R0, int& C0) {
+                int SX = (int)((sqrtf(8.0f * st + 1.0f) - 1.0f) * 0.5f);
+                while ((SX + 1) * (SX + 2) / 2 <= st) ++SX;
+                while (SX * (SX + 1) / 2 > st) --SX;
+                R0 = q0 + 64 * SX;
+                C0 = q0 + 64 * (st - SX * (SX + 1) / 2);
+            };
+            auto st_load = [&](int st, T (&v)[4][4]) {
+                int R0, C0;
+                st_origin(st, R0, C0);
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        const int r = r0 + a, cc = cc0 + c;
-                        acc[a][c] = (r < m && cc < m && r >= cc) ? S[(size_t)cc * m + r] : Sc<T>::zero();
+                        const int r = R0 + ti + 16 * a, cc = C0 + tj + 16 * c;
+                        v[a][c] = (r < m && cc < m && r >= cc) ? S[(size_t)cc * m + r] : Sc<T>::zero();
                     }
+            };
+            T cur[4][4], nxt[4][4];
+            st_load(0, cur);
+            for (int st = 0; st < nst; ++st) {
+                if (st + 1 < nst) st_load(st + 1, nxt);
+                int R0, C0;
+                st_origin(st, R0, C0);
                 for (int t = 0; t < nb; ++t) {
                     T pr[4], pc[4];
 #pragma unroll
                     for (int a = 0; a < 4; ++a) {
-                        pr[a] = r0 + a < m ? P[t * m + r0 + a] : Sc<T>::zero();
-                        pc[a] = cc0 + a < m ? P[t * m + cc0 + a] : Sc<T>::zero();
+                        const int r = R0 + ti + 16 * a, cc = C0 + tj + 16 * a;
+                        pr[a] = r < m ? P[t * m + r] : Sc<T>::zero();
+                        pc[a] = cc < m ? P[t * m + cc] : Sc<T>::zero();
                     }
 #pragma unroll
                     for (int a = 0; a < 4; ++a)
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) fms_acc(acc[a][c], pr[a], pc[c]);
+                        for (int c = 0; c < 4; ++c) fms_acc(cur[a][c], pr[a], pc[c]);
                 }
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
 #pragma unroll
                     for (int c = 0; c < 4; ++c) {
-                        const int r = r0 + a, cc = cc0 + c;
-                        if (r < m && cc < m && r >= cc) S[(size_t)cc * m + r] = acc[a][c];
+                        const int r = R0 + ti + 16 * a, cc = C0 + tj + 16 * c;
+                        if (r < m && cc < m && r >= cc) S[(size_t)cc * m + r] = cur[a][c];
+                        cur[a][c] = nxt[a][c];
                     }
             }
         }
@@ -490,37 +581,30 @@ __global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A
         if (tid == 0) atomicMax(&s.status[sys], s_err);
         return;
     }
-    // right-hand side r_G - A_GI w_l
-    const T* w = X + ((size_t)k * s.ncol + l) * s.nI;
-    const T* cv = cval + (size_t)k * s.ncpl;
-    for (int g = tid; g < m; g += NT) {
-        T v = Sc<T>::zero();
-        if (g == s.posG_src[l]) v = Sc<T>::one();
-        if (s.lsink && g == s.posG_sink) v -= Sc<T>::one();
-        for (int q = s.gi_ptr[g]; q < s.gi_ptr[g + 1]; ++q) fms_acc(v, cv[q], w[s.gi_pos[q]]);
-        y[g] = v;
-    }
-    __syncthreads();
-    // L y' = y, column by column
-    for (int c = 0; c < m; ++c) {
-        const T yc = Sc<T>::mul(y[c], Sc<T>::recip(S[(size_t)c * m + c]));
+    // L^T x = y, panel by panel from the last
+    for (int p0 = (m - 1) / NB * NB; p0 >= 0; p0 -= NB) {
+        const int nb = min(NB, m - p0);
+        for (int t = 0; t < nb; ++t)
+            for (int r = p0 + tid; r < m; r += NT) P[t * m + r] = S[(size_t)(p0 + t) * m + r];
         __syncthreads();
-        if (tid == 0) y[c] = yc;
-        for (int r = c + 1 + tid; r < m; r += NT) fms_acc(y[r], S[(size_t)c * m + r], yc);
-        __syncthreads();
-    }
-    // L^T x = y', one dot product per unknown from the last
-    for (int c = m - 1; c >= 0; --c) {
-        T part = Sc<T>::zero();
-        for (int r = c + 1 + tid; r < m; r += NT) fma_acc(part, S[(size_t)c * m + r], y[r]);
+        {   // y[p0 + t] -= sum over solved rows r >= p0 + nb of L(r, p0 + t) x_r
+            const int t = tid >> 4, sl = tid & 15;
+            T part = Sc<T>::zero();
+            if (t < nb)
+                for (int r = p0 + nb + sl; r < m; r += 16) fma_acc(part, P[t * m + r], y[r]);
 #pragma unroll
-        for (int off = 16; off > 0; off >>= 1) part += shfl_down_full(part, off);
-        if (lane == 0) red[warp] = part;
+            for (int off = 8; off > 0; off >>= 1) part += shfl_xor_t(part, off);
+            if (sl == 0 && t < nb) y[p0 + t] -= part;
+        }
         __syncthreads();
-        if (tid == 0) {
-            T tot = Sc<T>::zero();
-            for (int q = 0; q < NT / 32; ++q) tot += red[q];
-            y[c] = Sc<T>::mul(y[c] - tot, Sc<T>::recip(S[(size_t)c * m + c]));
+        if (warp == 0) {   // the panel's triangle of L^T, lane t = row p0 + t
+            T v = lane < nb ? y[p0 + lane] : Sc<T>::zero();
+            for (int u = nb - 1; u >= 0; --u) {
+                if (lane == u) v = Sc<T>::mul(v, Sc<T>::recip(P[u * m + p0 + u]));
+                const T x = shfl_w(v, u, 32);
+                if (lane < u) fms_acc(v, P[lane * m + p0 + u], x);
+            }
+            if (lane < nb) y[p0 + lane] = v;
         }
         __syncthreads();
     }
@@ -528,10 +612,11 @@ __global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A
 }
 
 // ---------------------------------------------------------------------------
-// kpot on the interior rows: w_l - Y p_G, tile 64 rows x 32 electrodes.
+// z^_l = u^_l - V^ p_G: tiles of 64 interior rows x 32 electrodes; the
+// boundary columns in the order of their first row, so a tile stops at the
+// first column that is zero on all its rows.
 template <typename T>
-__global__ void __launch_bounds__(128) k_schur_out(SchurArgs s, const T* __restrict__ X, const T* __restrict__ xg,
-                                                   int n, cd* kpot)
+__global__ void __launch_bounds__(128) k_schur_zrebuild(SchurArgs s, T* X, const T* __restrict__ xg)
 {
     constexpr int TI = 64, TL = 32, TG = 16;
     __shared__ T As[TG][TI + 1];
@@ -539,30 +624,33 @@ __global__ void __launch_bounds__(128) k_schur_out(SchurArgs s, const T* __restr
     const int tid = threadIdx.x;
     const int k = blockIdx.z, i0 = blockIdx.x * TI, l0 = blockIdx.y * TL;
     const int ti = tid % 16, tl = tid / 16;
-    const int m = s.m, nI = s.nI;
+    const int m = s.m, nI = s.nI, L = s.L;
+    T* Xk = X + (size_t)k * s.ncol * nI;
     T acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[a][c] = Sc<T>::zero();
-    for (int g0 = 0; g0 < m; g0 += TG) {
+    for (int q0 = 0; q0 < m; q0 += TG) {
+        if (s.gfirst[q0] >= i0 + TI) break;
         for (int idx = tid; idx < TG * TI; idx += 128) {
             const int gg = idx / TI, ii = idx % TI;
-            As[gg][ii] = (g0 + gg < m && i0 + ii < nI) ? X[((size_t)k * s.ncol + s.L + g0 + gg) * nI + i0 + ii]
-                                                       : Sc<T>::zero();
+            const int g = q0 + gg < m ? s.gsort[q0 + gg] : -1;
+            As[gg][ii] = (g >= 0 && i0 + ii < nI) ? Xk[(size_t)(L + g) * nI + i0 + ii] : Sc<T>::zero();
         }
         for (int idx = tid; idx < TG * TL; idx += 128) {
             const int ll = idx / TG, gg = idx % TG;
-            Bs[gg][ll] = (g0 + gg < m && l0 + ll < s.L) ? xg[((size_t)k * s.L + l0 + ll) * m + g0 + gg] : Sc<T>::zero();
+            const int g = q0 + gg < m ? s.gsort[q0 + gg] : -1;
+            Bs[gg][ll] = (g >= 0 && l0 + ll < L) ? xg[((size_t)k * L + l0 + ll) * m + g] : Sc<T>::zero();
         }
         __syncthreads();
 #pragma unroll 4
         for (int gg = 0; gg < TG; ++gg) {
             T a4[4], b4[4];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) a4[a] = As[gg][ti * 4 + a];
+            for (int a = 0; a < 4; ++a) a4[a] = As[gg][ti + 16 * a];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) b4[c] = Bs[gg][tl * 4 + c];
+            for (int c = 0; c < 4; ++c) b4[c] = Bs[gg][tl + 8 * c];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -572,14 +660,12 @@ __global__ void __launch_bounds__(128) k_schur_out(SchurArgs s, const T* __restr
     }
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        const int l = l0 + tl * 4 + c;
-        if (l >= s.L) continue;
+        const int l = l0 + tl + 8 * c;
+        if (l >= L) continue;
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
-            const int i = i0 + ti * 4 + a;
-            if (i >= nI) continue;
-            const T v = X[((size_t)k * s.ncol + l) * nI + i] - acc[a][c];
-            kpot[((size_t)k * s.L + l) * n + s.permI[i]] = Sc<T>::to_cd(v);
+            const int i = i0 + ti + 16 * a;
+            if (i < nI) Xk[(size_t)l * nI + i] -= acc[a][c];
         }
     }
 }
@@ -594,81 +680,103 @@ __global__ void k_schur_out_gam(SchurArgs s, const T* __restrict__ xg, int n, cd
     kpot[kl * n + s.gam[g]] = Sc<T>::to_cd(xg[idx]);
 }
 
-template <typename T>
-int ms_wz(int mbI)
-{
-    return (mbI + 2 * SCHUR_MS_BB + SCHUR_MS_BB - 1) / SCHUR_MS_BB * SCHUR_MS_BB;
-}
+// window rows: mb + 3 BB (the rows of a block, the band below it, and two
+// blocks arriving ahead), a multiple of BB
+int sweep_wz(int mbI) { return (mbI + 4 * SCHUR_MS_BB - 1) / SCHUR_MS_BB * SCHUR_MS_BB; }
+
+constexpr int SWEEP_NT = 288;   // 4 x 4 update tiles of a 129-row band at R = 32 in one round
 
 }  // namespace
 
 // ---------------------------------------------------------------------------
 template <typename T>
-size_t schur_msolve_smem(int mbI, int WI)
+size_t schur_sweep_smem(int mbI, int WI, int R)
 {
-    const int WZ = ms_wz<T>(mbI);
-    return (size_t)2 * SCHUR_MS_BB * WI * sizeof(T) + (size_t)WZ * SCHUR_MS_R * sizeof(T) + (size_t)WZ * sizeof(double);
+    return (size_t)2 * SCHUR_MS_BB * WI * sizeof(T) + (size_t)sweep_wz(mbI) * R * sizeof(T);
 }
 
 template <typename T>
-void launch_schur_rhs(const SchurArgs& s, const BandArgs<T>& full, T* X, T* cval, cudaStream_t st)
+void launch_schur_rhs(const SchurArgs& s, const BandArgs<T>& full, const double* fakws, T* X, T* cval, cudaStream_t st)
 {
     const int ns = s.K * s.L;
-    k_schur_rhs_src<T><<<(ns + 127) / 128, 128, 0, st>>>(s, X);
+    k_schur_rhs_src<T><<<(ns + 127) / 128, 128, 0, st>>>(s, fakws, X);
     const long long nc = (long long)s.K * s.ncpl;
-    if (nc > 0) k_schur_rhs_cpl<T><<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(s, full, X, cval);
+    if (nc > 0) k_schur_rhs_cpl<T><<<(unsigned)((nc + 255) / 256), 256, 0, st>>>(s, full, fakws, X, cval);
 }
 
 template <typename T>
-void launch_schur_msolve(const SchurArgs& s, const T* Lws, size_t lstride, const double* fakws, T* X, cudaStream_t st)
+void launch_schur_transpose(const SchurArgs& s, const T* Lws, T* Lrev, cudaStream_t st)
 {
-    constexpr int NT = 256;
-    const size_t smem = schur_msolve_smem<T>(s.mbI, s.WI);
-    auto kern = k_schur_msolve<T, NT, SCHUR_MS_R, SCHUR_MS_BB>;
+    const long long tot = (long long)s.K * s.nI * s.WI;
+    k_schur_transpose<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, Lws, Lrev);
+}
+
+template <typename T>
+void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t st)
+{
+    const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_MS_R);
+    auto kern = k_schur_sweep<T, SWEEP_NT, SCHUR_MS_R, SCHUR_MS_BB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid(s.nblk, s.K);
-    kern<<<grid, NT, smem, st>>>(s, Lws, lstride, fakws, X, ms_wz<T>(s.mbI));
+    kern<<<grid, SWEEP_NT, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
 }
 
 template <typename T>
-void launch_schur_s0(const SchurArgs& s, const T* X, const T* cval, T* S0, cudaStream_t st)
+void launch_schur_gram(const SchurArgs& s, const T* X, T* C, cudaStream_t st)
 {
-    const long long tot = (long long)s.K * s.m * s.m;
-    k_schur_s0<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, X, cval, S0);
+    dim3 grid((s.m + 63) / 64, (s.ncol + 31) / 32, s.K);
+    k_schur_gram<T><<<grid, 128, 0, st>>>(s, X, C);
 }
 
 template <typename T>
-void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* S0, const T* X, const T* cval, T* Sws,
-                       T* xg, int sys0, int nsys, cudaStream_t st)
+void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* C, T* Sws, T* xg, int sys0, int nsys,
+                       cudaStream_t st)
 {
     constexpr int NT = 256, NB = 16;
     const size_t smem = ((size_t)NB * s.m + s.m) * sizeof(T);
     auto kern = k_schur_chol<T, NT, NB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kern<<<nsys, NT, smem, st>>>(s, full, S0, X, cval, Sws, xg, sys0);
+    kern<<<nsys, NT, smem, st>>>(s, full, C, Sws, xg, sys0);
 }
 
 template <typename T>
-void launch_schur_out(const SchurArgs& s, const T* X, const T* xg, int n, cd* kpot, cudaStream_t st)
+void launch_schur_zrebuild(const SchurArgs& s, T* X, const T* xg, cudaStream_t st)
 {
     dim3 grid((s.nI + 63) / 64, (s.L + 31) / 32, s.K);
-    k_schur_out<T><<<grid, 128, 0, st>>>(s, X, xg, n, kpot);
+    k_schur_zrebuild<T><<<grid, 128, 0, st>>>(s, X, xg);
+}
+
+template <typename T>
+void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, const T* X, const T* xg, int n,
+                       cd* kpot, cudaStream_t st)
+{
+    constexpr int NT = 160;   // 4 x 4 update tiles of a 129-row band at R = 16 in one round
+    const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_BK_R);
+    auto kern = k_schur_sweep<T, NT, SCHUR_BK_R, SCHUR_MS_BB>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((s.L + SCHUR_BK_R - 1) / SCHUR_BK_R, s.K);
+    kern<<<grid, NT, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);
     const long long tot = (long long)s.K * s.L * s.m;
     k_schur_out_gam<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, xg, n, kpot);
 }
 
-template size_t schur_msolve_smem<cd>(int, int);
-template size_t schur_msolve_smem<double>(int, int);
-template void launch_schur_rhs<cd>(const SchurArgs&, const BandArgs<cd>&, cd*, cd*, cudaStream_t);
-template void launch_schur_rhs<double>(const SchurArgs&, const BandArgs<double>&, double*, double*, cudaStream_t);
-template void launch_schur_msolve<cd>(const SchurArgs&, const cd*, size_t, const double*, cd*, cudaStream_t);
-template void launch_schur_msolve<double>(const SchurArgs&, const double*, size_t, const double*, double*,
-                                          cudaStream_t);
-template void launch_schur_s0<cd>(const SchurArgs&, const cd*, const cd*, cd*, cudaStream_t);
-template void launch_schur_s0<double>(const SchurArgs&, const double*, const double*, double*, cudaStream_t);
-template void launch_schur_chol<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, const cd*, const cd*, cd*, cd*,
-                                    int, int, cudaStream_t);
-template void launch_schur_chol<double>(const SchurArgs&, const BandArgs<double>&, const double*, const double*,
-                                        const double*, double*, double*, int, int, cudaStream_t);
-template void launch_schur_out<cd>(const SchurArgs&, const cd*, const cd*, int, cd*, cudaStream_t);
-template void launch_schur_out<double>(const SchurArgs&, const double*, const double*, int, cd*, cudaStream_t);
+template size_t schur_sweep_smem<cd>(int, int, int);
+template size_t schur_sweep_smem<double>(int, int, int);
+template void launch_schur_rhs<cd>(const SchurArgs&, const BandArgs<cd>&, const double*, cd*, cd*, cudaStream_t);
+template void launch_schur_rhs<double>(const SchurArgs&, const BandArgs<double>&, const double*, double*, double*,
+                                       cudaStream_t);
+template void launch_schur_transpose<cd>(const SchurArgs&, const cd*, cd*, cudaStream_t);
+template void launch_schur_transpose<double>(const SchurArgs&, const double*, double*, cudaStream_t);
+template void launch_schur_forward<cd>(const SchurArgs&, const cd*, cd*, cudaStream_t);
+template void launch_schur_forward<double>(const SchurArgs&, const double*, double*, cudaStream_t);
+template void launch_schur_gram<cd>(const SchurArgs&, const cd*, cd*, cudaStream_t);
+template void launch_schur_gram<double>(const SchurArgs&, const double*, double*, cudaStream_t);
+template void launch_schur_chol<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, cd*, cd*, int, int, cudaStream_t);
+template void launch_schur_chol<double>(const SchurArgs&, const BandArgs<double>&, const double*, double*, double*,
+                                        int, int, cudaStream_t);
+template void launch_schur_zrebuild<cd>(const SchurArgs&, cd*, const cd*, cudaStream_t);
+template void launch_schur_zrebuild<double>(const SchurArgs&, double*, const double*, cudaStream_t);
+template void launch_schur_back<cd>(const SchurArgs&, const cd*, const double*, const cd*, const cd*, int, cd*,
+                                    cudaStream_t);
+template void launch_schur_back<double>(const SchurArgs&, const double*, const double*, const double*, const double*,
+                                        int, cd*, cudaStream_t);

@@ -8,17 +8,23 @@
 // and nothing else.  Splitting the nodes into G and the interior I,
 //
 //     [ A_II   A_IG    ] [p_I]   [r_I]        A_II, A_IG independent of l,
-//     [ A_GI   A_GG(l) ] [p_G] = [r_G]        r = e_src(l) - e_sink,
+//     [ A_GI   A_GG(l) ] [p_G] = [r_G]        r = e_src(l) - e_sink.
 //
-// gives p_I = w_l - Y p_G with w_l = A_II^-1 r_I, Y = A_II^-1 A_IG, and
-// S_l p_G = r_G - A_GI w_l with the Schur complement S_l = A_GG(l) - A_GI Y.
-// Per wavenumber: one band factorisation of A_II (the same prepared,
-// scaled, unconjugated L L^T kernels as the direct path) and a multi-RHS
-// band solve of the L + m columns [r_I | A_IG]; per (k, l): a dense m x m
-// complex-symmetric Cholesky of S_l and the rebuild of p_I by a GEMM.  The
-// arithmetic is FP64 (complex128 or real) throughout; the result equals the
-// reference's per-system elimination up to rounding (same matrix, a
-// different elimination order).
+// With the interior factor F A_II F = L L^T (F = diag(fak), the scaled,
+// unconjugated factorisation of the direct path), u^ = L^-1 F r_I and
+// V^ = L^-1 F A_IG:
+//
+//     S_l p_G = r_G - V^T u^_l,     S_l = A_GG(l) - V^T V^,
+//     p_I = F L^-T (u^_l - V^ p_G).
+//
+// Per wavenumber: one band factorisation of A_II, a forward sweep of the
+// L + m columns [F r_I | F A_IG] (each from its first non-zero row) and the
+// Gram products V^T [u^ | V^]; per (k, l) a dense m x m complex-symmetric
+// Cholesky of S_l with its two triangular solves; then z^ = u^ - V^ p_G (a
+// GEMM) and one back sweep per source column.  The arithmetic is FP64
+// (complex128 or real) throughout; the result equals the reference's
+// per-system elimination up to rounding (the same matrix, another
+// elimination order).
 #pragma once
 
 #include <vector>
@@ -28,8 +34,10 @@
 
 // Largest boundary set the dense Schur kernels take (panel in shared memory).
 constexpr int SCHUR_MMAX = 768;
-// Columns per CTA of the multi-RHS band solve and its column block.
+// Columns per CTA of the forward sweep (all columns) and of the back sweep
+// (the source columns), and the row block of both.
 constexpr int SCHUR_MS_R = 32;
+constexpr int SCHUR_BK_R = 16;
 constexpr int SCHUR_MS_BB = 16;
 
 // Host-side plan: node split, interior assembly lists, couplings.
@@ -50,6 +58,8 @@ struct SchurHost {
     // multi-RHS solve: columns ordered by their first non-zero interior
     // row; blocks of SCHUR_MS_R columns and their first rows
     std::vector<int> col_order, blk_start;
+    std::vector<int> first;         // [L + m] first non-zero interior row of each column
+    std::vector<int> gsort, gfirst; // boundary positions by first row, and those rows
 };
 
 // Builds the plan from the full mesh's gather lists, the boundary nodes
@@ -67,34 +77,47 @@ struct SchurArgs {
     const int *gi_ptr, *gi_pos, *gi_ent, *gi_g;
     const int *gg_g, *gg_h, *gg_ent;
     const int *col_order, *blk_start;
+    const int* first;        // [ncol] first non-zero interior row of column c
+    const int* gsort;        // [m] boundary positions ordered by their column's first row
+    const int* gfirst;       // [m] first row of gsort[q]'s column
     int* status;             // [K * L] errnr per (k, l); the interior factor uses [0, K)
 };
 
-// Right-hand sides of the multi-RHS solve, X[k][c][i] (zeroed by the
-// caller): +1 at the source's interior row and -1 at the sink's (columns
-// c < L), the couplings a(i, g) of A_IG (columns L + g, also kept in
-// cval[k][q] for the later steps).
+// Right-hand sides of the interior solves, X[k][c][i] (zeroed by the
+// caller), scaled by the interior factor's fak (so after the preparation
+// pass): fak_i (+1 at the source's interior row, -1 at the sink's) in
+// columns c < L, fak_i a(i, g) of A_IG in columns L + g; the unscaled
+// coupling values a(g, i) also into cval[k][q].
 template <typename T>
-void launch_schur_rhs(const SchurArgs& s, const BandArgs<T>& full, T* X, T* cval, cudaStream_t st);
-// Forward and back substitution with the interior factors (Lws, fakws as
-// the band kernels leave them, column stride WI) of every column: X is
-// overwritten by A_II^-1 X.  Uses the plan's column order and block starts.
+void launch_schur_rhs(const SchurArgs& s, const BandArgs<T>& full, const double* fakws, T* X, T* cval,
+                      cudaStream_t st);
+// Reversed row-packed copy of the interior factors for the back sweep:
+// Lrev[k][c'][d] = L(n-1-c', n-1-c'-d), so that L^T in reversed numbering
+// is lower-triangular banded with the forward sweep's layout.
 template <typename T>
-void launch_schur_msolve(const SchurArgs& s, const T* Lws, size_t lstride, const double* fakws, T* X,
-                         cudaStream_t st);
-// S0[k] = -A_GI Y (lower triangle, column-major m x m) for every k.
+void launch_schur_transpose(const SchurArgs& s, const T* Lws, T* Lrev, cudaStream_t st);
+// Forward sweep: X <- L^-1 X in place for every column (u^ = L^-1 F r_I,
+// V^ = L^-1 F A_IG), each column block from its first non-zero row.
 template <typename T>
-void launch_schur_s0(const SchurArgs& s, const T* X, const T* cval, T* S0, cudaStream_t st);
-// Systems sys0 .. sys0+nsys-1 (sys = k L + l): S_l = S0[k] + A_GG(l) into
-// the workspace Sws[b] (m x m each), its Cholesky factor in place, and the
-// boundary potentials xg[sys][g] = S_l^-1 (r_G - A_GI w_l).
+void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t st);
+// Gram products C[k][c][g] = sum_i V^[i][g] X[i][c] (c < L: A_GI w_l;
+// c >= L: the lower triangle of A_GI Y = -S0), column-major with m rows.
 template <typename T>
-void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* S0, const T* X, const T* cval,
-                       T* Sws, T* xg, int sys0, int nsys, cudaStream_t st);
-// kpot(node, l, k) for every node: p_I = w_l - Y p_G on the interior rows,
-// p_G on the boundary rows (complex128 Fortran layout; real systems with
-// zero imaginary parts).
+void launch_schur_gram(const SchurArgs& s, const T* X, T* C, cudaStream_t st);
+// Systems sys0 .. sys0+nsys-1 (sys = k L + l): S_l = A_GG(l) - C_VV[k]
+// into the workspace Sws[b] (m x m each), its Cholesky factor in place, and
+// the boundary potentials xg[sys][g] = S_l^-1 (r_G - C[k][l]).
 template <typename T>
-void launch_schur_out(const SchurArgs& s, const T* X, const T* xg, int n, cd* kpot, cudaStream_t st);
-// Dynamic shared memory of the multi-RHS solve for the interior band mbI.
-template <typename T> size_t schur_msolve_smem(int mbI, int WI);
+void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* C, T* Sws, T* xg, int sys0, int nsys,
+                       cudaStream_t st);
+// z^_l = u^_l - V^ p_G (in place on the columns l < L of X).
+template <typename T>
+void launch_schur_zrebuild(const SchurArgs& s, T* X, const T* xg, cudaStream_t st);
+// Back sweep L^T x^ = z^ of the columns l < L with the reversed factor,
+// kpot(node, l, k) = fak x^ on the interior rows and p_G on the boundary
+// rows (complex128 Fortran layout; real systems with zero imaginary parts).
+template <typename T>
+void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, const T* X, const T* xg, int n,
+                       cd* kpot, cudaStream_t st);
+// Dynamic shared memory of a sweep for the interior band mbI with R columns.
+template <typename T> size_t schur_sweep_smem(int mbI, int WI, int R);

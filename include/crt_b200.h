@@ -269,8 +269,9 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
  * residuals and [11] the correction solves of the mixed form's refinement
  * (both inside [1]), [12] the panel width of the blocked band factorisation
  * (chosen by the autotuner; 0 for the unblocked kernel), and in the Schur
- * form (inside [1]) [13] the multi-RHS interior solve, [14] S0 and the
- * boundary Cholesky with its solve, [15] the rebuild of the potentials.
+ * form (inside [1]) [13] the forward sweep of the interior columns, [14]
+ * their Gram products and the boundary Cholesky with its solves, [15] the
+ * rebuild and the back sweep into the potentials.
  * Milliseconds except [9] and [12].  No reference counterpart. */
 int32_t crt_last_timings_ex(const crt_ctx *ctx, double *ms, int32_t n);
 
