@@ -37,18 +37,9 @@ METRIC = "GN-step wall time, learned-PCG/FP32-refined vs plain CG on B200 at rel
 # sample by this count.
 REF_NCG = {"C5": 1589}
 
-# DRAM bytes (read + write) of the band-factor kernel per band entry
-# n (mb + 1) of a complex128 system, from an ncu capture of the factor on
-# the 200 x 100 quadrilateral survey (mb = 102): 4.186 GB for 63 systems,
-# the prepared matrix read once and L written once.
-FACTOR_TRAFFIC_BYTES_PER_ENTRY = 31.8
-
-# FMA pipes of a B200 SM (non-tensor): 64 FP64 / 128 FP32 FMA per clock,
-# the rooflines of the complex128 / complex64 band factorisation.
+# FP64 FMA pipe of a B200 SM (non-tensor): 64 FMA per clock, the roofline
+# of the forward's FP64 kernels.
 FP64_FMA_PER_CLK_SM = 64
-FP32_FMA_PER_CLK_SM = 128
-# complex64: 4.164 GB for 125 systems of the same survey
-FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 = 15.9
 
 
 def parse():
@@ -196,6 +187,52 @@ def load_peaks():
             d = json.load(fh)
         return float(d.get("hbm_gbs", 6650.0)), "measured"
     return 6650.0, "fallback"
+
+
+def schur_work(s, K: int, m_boundary: int, n_interior: int, mb_interior: int):
+    """Algorithmic complex multiply-adds of the Schur-form kernels (8 flops
+    each) on survey s with K wavenumbers: the boundary set G is every node of
+    a type-11 segment, a column's first non-zero interior row is its
+    source's row (source columns) or that of the first interior neighbour
+    of its boundary node (coupling columns); the forward sweep runs each
+    column from that row, the Gram products over the rows where both columns
+    can be non-zero, the rebuild over V^'s non-zero rows, the back sweep and
+    the interior factorisation over the whole band."""
+    m = s.mesh
+    n = m.sanz
+    typ = np.repeat(m.typ, m.nelanz)
+    rows = np.nonzero(typ == 11)[0]
+    isg = np.zeros(n, bool)
+    isg[np.unique(m.nrel[rows, :2].ravel()) - 1] = True
+    posI = -np.ones(n, np.int64)
+    posI[~isg] = np.arange(int((~isg).sum()))
+    gpos = -np.ones(n, np.int64)
+    gpos[isg] = np.arange(int(isg.sum()))
+    nI, M, L, mb = n_interior, m_boundary, len(s.enr), mb_interior
+    assert nI == int((~isg).sum()) and M == int(isg.sum())
+    nk = int(m.selanz[0])
+    area = m.nrel[: m.elanz, :nk] - 1
+    first_g = np.full(M, nI)
+    ga, gb = [], []
+    for a in range(nk):
+        for b in range(nk):
+            ga.append(area[:, a])
+            gb.append(area[:, b])
+    ga, gb = np.concatenate(ga), np.concatenate(gb)
+    sel = isg[ga] & ~isg[gb]
+    np.minimum.at(first_g, gpos[ga[sel]], posI[gb[sel]])
+    first_s = posI[s.enr - 1]
+    first_s = np.where(first_s < 0, nI, first_s)
+    fg = np.sort(first_g)
+    vtv = sum(float(np.sum(nI - np.maximum(f, fg[: i + 1]))) for i, f in enumerate(fg))
+    vtu = float(sum(np.sum(nI - np.maximum(f, first_s)) for f in first_g))
+    return {
+        "factor": K * nI * mb * mb / 2.0,
+        "forward": K * float(np.sum(nI - first_g) + np.sum(nI - first_s)) * mb,
+        "gram": K * (vtv + vtu),
+        "chol": K * L * (M ** 3 / 6.0 + M * M),
+        "back": K * (float(np.sum(nI - first_g)) * L + L * nI * mb),
+    }
 
 
 # ---------------------------------------------------------------------------
@@ -515,15 +552,17 @@ def main():
             pg.barrier()
             pg.destroy_process_group()
         return
-    from crtomo_stable_b200.lib import PREC_FP64, PREC_MIXED, PRECOND_BLOCK, PRECOND_JACOBI, Context
+    from crtomo_stable_b200.lib import (FORWARD_AUTO, FORWARD_DIRECT, PREC_FP64, PREC_MIXED, PRECOND_BLOCK,
+                                        PRECOND_JACOBI, Context)
     s = make_problem(args.config)
     E, N = s.mesh.elanz, len(s.strnr)
     n, mb, L = s.mesh.sanz, s.mesh.mb, len(s.enr)
     names = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter"]
     tnames = Context.TIMING_NAMES
 
-    def run_form(precision, steps, warmup, e2e_steps, sample_clocks):
+    def run_form(precision, steps, warmup, e2e_steps, sample_clocks, fwd_form=FORWARD_AUTO):
         ctx, dat, wmatd, par0, lam, nb, sm = setup_context(s, local, precision)
+        ctx.set_forward_form(fwd_form)
         if args.refine is not None:
             ctx.set_refinement(args.refine)
         pc = PRECOND_BLOCK if precision == PREC_MIXED else PRECOND_JACOBI
@@ -565,47 +604,54 @@ def main():
         if precision == PREC_MIXED and args.lambdas > 0:
             lam_batch = lambda_batch(ctx, Context, lam, par0, args.lambdas, args.lambda_iters, E, N, args.eps,
                                      args.ncgmax, PRECOND_BLOCK)
+        finfo = ctx.forward_info()
         ctx.close()
         return dict(t=t_step, phase=phase, ncg=ncg, launches=int(launches), clocks=clocks, e2e=t_e2e, lam=lam, K=K,
+                    finfo=finfo,
                     cg_form=form, cg_block=blk, cg_bw=bw, c64=precision == PREC_MIXED, lam_batch=lam_batch)
 
     mixed = run_form(PREC_MIXED, args.steps, args.warmup, args.steps, True)
     plain = None
     if args.forms == "both":
-        plain = run_form(PREC_FP64, max(1, args.steps // 3), max(1, args.warmup // 3), 0, False)
+        # the reference's algorithm on the GPU: one FP64 band system per
+        # wavenumber and electrode, the Jacobi-preconditioned CG
+        plain = run_form(PREC_FP64, max(1, args.steps // 3), max(1, args.warmup // 3), 0, False, FORWARD_DIRECT)
     t_step, phase, ncg, K = mixed["t"], mixed["phase"], mixed["ncg"], mixed["K"]
     ph = dict(zip(tnames, [float(x) for x in phase]))
     h2d = E * 16
     d2h = E * 16 + N * 16 + (ncg + 1) * 8 + 8
     peak_gbs, peak_kind = load_peaks()
     sm_mhz = (mixed["clocks"] or {}).get("sm_max_mhz") or 1965.0
-    # dominant kernel: the band factorisation -- complex64 on the FP32 pipe
-    # in the mixed form (128 FMA/clk/SM), complex128 on the FP64 pipe
-    # (64 FMA/clk/SM) otherwise.  Algorithmic work per system 4 n mb^2 flops
-    # (n mb^2 / 2 complex MACs of 8 flops); per launch = systems per launch x
-    # that.  Traffic: the prepared matrix read once and L written once,
-    # bytes per band entry from the ncu captures named above.
-    c64 = mixed["c64"]
-    nsys = K * L   # mixed boundaries: one factorisation per (k, l)
-    flops = 4.0 * n * mb * mb * nsys
-    nl = max(ph["factor_launches"], 1.0)
-    t_launch_s = ph["factor_kernel"] / nl / 1e3
-    fma_clk = FP32_FMA_PER_CLK_SM if c64 else FP64_FMA_PER_CLK_SM
-    pipe_peak = fma_clk * 2 * 148 * sm_mhz * 1e6 / 1e12
-    ach = flops / nl / t_launch_s / 1e12 if t_launch_s > 0 else 0.0
-    bpe = FACTOR_TRAFFIC_BYTES_PER_ENTRY_C64 if c64 else FACTOR_TRAFFIC_BYTES_PER_ENTRY
-    pb = int(ph.get("panel", 8)) or 8
-    roof = {"kernel": (f"k_band_factor_blk<cf,{pb}> (complex64 band Cholesky + fused forward substitution, "
-                       f"panel width {pb} by the autotuner)" if c64
-                       else f"k_band_factor_blk<cd,{pb}> (complex128 band Cholesky + fused forward substitution)"),
-            "bound": "fp32" if c64 else "fp64", "achieved": ach, "peak": pipe_peak, "unit": "TFLOP/s",
-            "frac": ach / pipe_peak,
-            "traffic": bpe * n * (mb + 1) * nsys / nl if bpe else None,
-            "traffic_unit": "bytes per launch (ncu dram read + write on C3, scaled by n (mb + 1) per system)",
-            "peak_source": (f"{'FP32' if c64 else 'FP64'} FMA pipe, {fma_clk} FMA/clk/SM x 148 SMs at the max SM "
-                            "clock (the factor runs on the CUDA cores; MEASURED_PEAKS.json holds HBM and bf16 "
-                            "tensor figures only)"),
-            "algorithmic_flops_per_launch": flops / nl, "launch_ms": t_launch_s * 1e3, "launches": nl}
+    # Rooflines of the forward's kernels.  In the Schur form (mixed
+    # boundaries) every kernel computes in FP64 on the CUDA cores: the FP64
+    # FMA pipe (64 FMA / clk / SM x 148 SMs at the max SM clock) is the peak
+    # of each; achieved = algorithmic flops (schur_work: 8 per complex
+    # multiply-add) / the kernel's CUDA-event time in the step.  The
+    # dominant one (the longest) is the line's `roofline`.
+    fp64_peak = FP64_FMA_PER_CLK_SM * 2 * 148 * sm_mhz * 1e6 / 1e12
+    form_used, m_b, n_i, mb_i = mixed["finfo"]
+    kernels = []
+    if form_used == 2:
+        w = schur_work(s, K, m_b, n_i, mb_i)
+        for name, key, label in (("factor", "factor_kernel", "k_band_factor_blk<cd> (interior band Cholesky, one system per wavenumber)"),
+                                 ("forward", "schur_forward", "k_schur_sweep (forward sweep of [F r_I | F A_IG]) + factor transpose"),
+                                 ("gram", "schur_gram", "k_schur_gram (V^T [u^ | V^])"),
+                                 ("chol", "schur_chol", "k_schur_chol (dense Cholesky of every S_l, fused forward solve, back solve)"),
+                                 ("back", "schur_back", "k_schur_zrebuild + k_schur_sweep back + k_schur_out_gam")):
+            t_ms = ph.get(key, 0.0)
+            fl = 8.0 * w[name]
+            ach = fl / (t_ms / 1e3) / 1e12 if t_ms > 0 else 0.0
+            kernels.append({"kernel": label, "ms": t_ms, "flops": fl, "achieved": ach, "peak": fp64_peak,
+                            "unit": "TFLOP/s", "frac": ach / fp64_peak})
+    dom = max(kernels, key=lambda k_: k_["ms"]) if kernels else None
+    roof = None
+    if dom is not None:
+        roof = {"kernel": dom["kernel"], "bound": "fp64", "achieved": dom["achieved"], "peak": fp64_peak,
+                "unit": "TFLOP/s", "frac": dom["frac"], "traffic": None,
+                "traffic_unit": "bytes per launch (ncu dram read + write)",
+                "peak_source": ("FP64 FMA pipe, 64 FMA/clk/SM x 148 SMs at the max SM clock (the Schur kernels run "
+                                "in FP64 on the CUDA cores; MEASURED_PEAKS.json holds HBM and bf16 tensor figures only)"),
+                "algorithmic_flops_per_launch": dom["flops"], "launch_ms": dom["ms"], "launches": 1.0}
     roof_cg = None
     if ncg > 0:
         bytes_it = 2.0 * N * E * 8 + 6.0 * E * 16 + 3.0 * N * 16   # J (complex64) read twice + vectors
@@ -633,13 +679,15 @@ def main():
                 "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128/c64", "data": "synthetic (seeded)",
                 "config": {"workload": workload_name(s, K),
-                           "form": ("mixed: band systems assembled and scaled in FP64, factored and solved in "
-                                    "complex64, adaptive FP64 iterative refinement (at most 8 steps, each system to normwise backward "
-                                    "error 1e-14); Jacobian formed in FP64, stored "
-                                    "complex64; CG with FP64 accumulation and dots, preconditioned by cgfac and the "
-                                    "block-tridiagonal S^-1 (FP32) of the sparse part" if mixed["cg_form"] == 1 else
-                                    "mixed; diagonal-PCG (block preconditioner unavailable)"),
-                           "refinement_steps": (f"at most {args.refine}" if args.refine is not None else "adaptive, at most 8"),
+                           "form": (("forward by elimination of the mixed-boundary nodes in FP64 (one interior band "
+                                     "factorisation per wavenumber, dense Schur complement per electrode)"
+                                     if mixed["finfo"][0] == 2 else
+                                     "forward per band system: complex64 factorisation with adaptive FP64 refinement")
+                                    + "; Jacobian formed in FP64, stored complex64; CG with FP64 accumulation and dots, "
+                                    + ("preconditioned by cgfac and the block-tridiagonal S^-1 (FP32) of the sparse part"
+                                       if mixed["cg_form"] == 1 else "diagonal-PCG (block preconditioner unavailable)")),
+                           "plain_form": ("FP64 per band system (the reference's loop) and the reference's "
+                                          "Jacobi-preconditioned CG, on the GPU"),
                            "cg_block": mixed["cg_block"], "cg_bandwidth": mixed["cg_bw"],
                            "cg_iterations": ncg, "lam": mixed["lam"],
                            "l2": "inputs larger than L2 (J alone is %.1f GB in complex64)" % (N * E * 8 / 1e9),
@@ -649,7 +697,7 @@ def main():
                 {"value": plain["t"], "unit": "s", "cg_iterations": plain["ncg"],
                  "phases_ms": dict(zip(tnames, [float(x) for x in plain["phase"]]))},
                 "e2e": {"value": mixed["e2e"], "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "roofline": roof, "roofline_cg": roof_cg, "lambda_batch": mixed["lam_batch"],
+                "roofline": roof, "kernels_forward": kernels, "roofline_cg": roof_cg, "lambda_batch": mixed["lam_batch"],
                 "cpu_baseline": cpu, "clocks": mixed["clocks"],
                 "gpu_launches": mixed["launches"]}
         print(json.dumps(line), flush=True)

@@ -1142,15 +1142,16 @@ void resolve_forward_timings(crt_ctx* ctx)
     ctx->timings[8] = ms_fk;
     ctx->timings[10] = ms_res;
     ctx->timings[11] = ms_cor;
-    // Schur form: forward sweep, Gram products + boundary Cholesky,
-    // rebuild + back sweep
+    // Schur form: forward sweep, Gram products, boundary Cholesky, rebuild
+    // + back sweep
     if (ctx->schur_used && !ctx->fwd_marks.empty()) {
         const crt_ctx::FwdMark& m0 = ctx->fwd_marks[0];
         ctx->timings[13] = tev_ms(ctx, m0.e1, ctx->sev[0]);
-        ctx->timings[14] = tev_ms(ctx, ctx->sev[0], ctx->sev[2]);
-        ctx->timings[15] = tev_ms(ctx, ctx->sev[2], ctx->sev[3]);
+        ctx->timings[14] = tev_ms(ctx, ctx->sev[0], ctx->sev[1]);
+        ctx->timings[15] = tev_ms(ctx, ctx->sev[1], ctx->sev[2]);
+        ctx->timings[16] = tev_ms(ctx, ctx->sev[2], ctx->sev[3]);
     } else {
-        ctx->timings[13] = ctx->timings[14] = ctx->timings[15] = 0.0;
+        ctx->timings[13] = ctx->timings[14] = ctx->timings[15] = ctx->timings[16] = 0.0;
     }
 }
 

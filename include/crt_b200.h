@@ -270,8 +270,8 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
  * (both inside [1]), [12] the panel width of the blocked band factorisation
  * (chosen by the autotuner; 0 for the unblocked kernel), and in the Schur
  * form (inside [1]) [13] the forward sweep of the interior columns, [14]
- * their Gram products and the boundary Cholesky with its solves, [15] the
- * rebuild and the back sweep into the potentials.
+ * their Gram products, [15] the boundary Cholesky with its solves, [16]
+ * the rebuild and the back sweep into the potentials.
  * Milliseconds except [9] and [12].  No reference counterpart. */
 int32_t crt_last_timings_ex(const crt_ctx *ctx, double *ms, int32_t n);
 
