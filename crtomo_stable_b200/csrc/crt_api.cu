@@ -1212,7 +1212,9 @@ int forward_common(crt_ctx* ctx, int ldc, int mode, const double* kfak_h)
     if (st) return st;
     ctx->last_ldc = ldc;
     ctx->have_forward = 1;
-    ctx->have_sens = 0;
+    // the Jacobian stays that of the model it was computed at (the
+    // reference's sens is kept across the lambda and step-length trials,
+    // src/inv.f90:769-912, until the next accepted iterate recomputes it)
     return CRT_OK;
 }
 
@@ -1394,6 +1396,29 @@ extern "C" int32_t crt_set_configs(crt_ctx* ctx, const int32_t* strnr, const int
         if (std::min({e1, e2, e3, e4}) < 0 || std::max({e1, e2, e3, e4}) > ctx->L)
             return set_err(ctx, 46, "electrode number out of range (errnr 46)");
         elec[i] = make_int4(e1 - 1, e2 - 1, e3 - 1, e4 - 1);
+    }
+    // Readings whose potential electrodes were swapped (chkpol.f90:84-87,
+    // :113-116): the stored response follows, volt -> -volt and sigmaa's
+    // phase moved by pi into (-pi, pi], so that the Jacobian of the last
+    // forward (dV / V) keeps its sign.
+    std::vector<int> swapped;
+    if (ctx->have_forward && (int)ctx->vnr_h.size() == ctx->N)
+        for (int i = 0; i < ctx->N; ++i) {
+            const int o = ctx->vnr_h[i], v = vnr[i];
+            if (o != v && (o % 10000) == v / 10000 && o / 10000 == (v % 10000) && strnr[i] == ctx->strnr_h[i])
+                swapped.push_back(i);
+        }
+    if (!swapped.empty()) {
+        std::vector<cd> vo(ctx->N), sa(ctx->N);
+        CK(cudaMemcpyAsync(vo.data(), ctx->d_volt, sizeof(cd) * ctx->N, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaMemcpyAsync(sa.data(), ctx->d_sigmaa, sizeof(cd) * ctx->N, cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (int i : swapped) {
+            vo[i] = -vo[i];
+            sa[i].y += sa[i].y > 0.0 ? -ctx->pi : ctx->pi;
+        }
+        CK(cudaMemcpyAsync(ctx->d_volt, vo.data(), sizeof(cd) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->d_sigmaa, sa.data(), sizeof(cd) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
     }
     CK(cudaMemcpyAsync(ctx->d_strnr, strnr, sizeof(int) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->d_vnr, vnr, sizeof(int) * ctx->N, cudaMemcpyHostToDevice, ctx->st));
@@ -1602,6 +1627,102 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// blam0 (src/blam0.f90:131-167): jtj(j) = |sum_i sum_k conj(J_ij) J_ik w_i|
+// = |sum_i conj(J_ij) w_i s_i| with the row sums s = J 1: two passes over
+// the device-resident Jacobian instead of the reference's O(N M^2) loop.
+// `real` selects the real Jacobian (ldc: sensdc) or, with `re_part`, the
+// real part of the complex one (final phase improvement).
+namespace {
+
+template <typename S> __device__ __forceinline__ cd jval(const S* J, size_t idx);
+template <> __device__ __forceinline__ cd jval<cd>(const cd* J, size_t idx) { return J[idx]; }
+template <> __device__ __forceinline__ cd jval<cf>(const cf* J, size_t idx)
+{
+    return cd{(double)J[idx].x, (double)J[idx].y};
+}
+template <> __device__ __forceinline__ cd jval<double>(const double* J, size_t idx) { return cd{J[idx], 0.0}; }
+template <> __device__ __forceinline__ cd jval<float>(const float* J, size_t idx) { return cd{(double)J[idx], 0.0}; }
+
+template <typename S>
+__global__ void k_blam0_rowsum(const S* __restrict__ J, int N, int M, int re_part, cd* s)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    cd acc{0.0, 0.0};
+    for (int j = 0; j < M; ++j) acc += jval<S>(J, (size_t)j * N + i);
+    if (re_part) acc.y = 0.0;
+    s[i] = acc;
+}
+
+// one warp per model cell: |sum_i conj(J_ij) wd_i s_i|
+template <typename S>
+__global__ void k_blam0_col(const S* __restrict__ J, int N, int M, int re_part, const double* __restrict__ wd,
+                            const cd* __restrict__ s, double* jtj)
+{
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (j >= M) return;
+    cd acc{0.0, 0.0};
+    for (int i = lane; i < N; i += 32) {
+        cd a = jval<S>(J, (size_t)j * N + i);
+        if (re_part) a.y = 0.0;
+        acc += conj(a) * (s[i] * wd[i]);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
+    }
+    if (lane == 0) jtj[j] = hypot(acc.x, acc.y);
+}
+
+template <typename S>
+void blam0_launch(const crt_ctx* ctx, int re_part, cd* s, double* jtj)
+{
+    const S* J = static_cast<const S*>(ctx->d_sens);
+    k_blam0_rowsum<S><<<(ctx->N + 255) / 256, 256, 0, ctx->st>>>(J, ctx->N, ctx->E, re_part, s);
+    k_blam0_col<S><<<(ctx->E * 32 + 255) / 256, 256, 0, ctx->st>>>(J, ctx->N, ctx->E, re_part, ctx->d_wd, s, jtj);
+}
+
+}  // namespace
+
+extern "C" int32_t crt_blam0(crt_ctx* ctx, int32_t ldc, int32_t lfpi, double alfx, double alfz, double* lammax)
+{
+    if (!ctx || !lammax || !(alfx + alfz > 0.0)) return CRT_ERR_ARG;
+    if (!ctx->have_sens || !ctx->d_sens) return set_err(ctx, CRT_ERR_ARG, "crt_blam0 before crt_jacobian");
+    if (!ctx->d_wd) return set_err(ctx, CRT_ERR_ARG, "crt_blam0 before crt_set_data");
+    if ((ldc != 0) != (ctx->sens_real != 0))
+        return set_err(ctx, CRT_ERR_ARG, "crt_blam0: ldc does not match the stored Jacobian");
+    CK(cudaSetDevice(ctx->device));
+    cd* s = nullptr;
+    double* jtj = nullptr;
+    CK(cudaMalloc((void**)&s, sizeof(cd) * (size_t)ctx->N));
+    if (cudaMalloc((void**)&jtj, sizeof(double) * (size_t)ctx->E) != cudaSuccess) {
+        cudaFree(s);
+        return set_err(ctx, CRT_ERR_CUDA, "cudaMalloc of the blam0 sums");
+    }
+    const bool f32 = ctx->prec == CRT_PREC_MIXED;
+    if (ldc) {
+        if (f32) blam0_launch<float>(ctx, 0, s, jtj);
+        else blam0_launch<double>(ctx, 0, s, jtj);
+    } else {
+        if (f32) blam0_launch<cf>(ctx, lfpi != 0, s, jtj);
+        else blam0_launch<cd>(ctx, lfpi != 0, s, jtj);
+    }
+    ctx->launches += 2;
+    std::vector<double> h(ctx->E);
+    int e = kernel_check(ctx, "blam0");
+    if (!e && cudaMemcpyAsync(h.data(), jtj, sizeof(double) * ctx->E, cudaMemcpyDeviceToHost, ctx->st) != cudaSuccess)
+        e = set_err(ctx, CRT_ERR_CUDA, "blam0 copy");
+    if (!e && cudaStreamSynchronize(ctx->st) != cudaSuccess) e = set_err(ctx, CRT_ERR_CUDA, "blam0 sync");
+    cudaFree(s);
+    cudaFree(jtj);
+    if (e) return e;
+    double tot = 0.0;
+    for (double v : h) tot += v;
+    *lammax = tot / (double)ctx->E * 2.0 / (alfx + alfz) * 5.0;
+    return CRT_OK;
+}
 
 extern "C" int32_t crt_set_model(crt_ctx* ctx, const double* par)
 {

@@ -16,7 +16,14 @@ from typing import Optional
 import numpy as np
 
 from . import io, regularization
-from .lib import Context, dmisft
+from .lib import Context, CRTError, dmisft
+
+
+def _quot(a: float, b: float) -> float:
+    """a / b with IEEE semantics (0 / 0 = NaN, which fails every comparison,
+    as in the reference's Fortran)."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return float(np.float64(a) / np.float64(b))
 
 
 @dataclasses.dataclass
@@ -232,12 +239,18 @@ class Inversion:
     """Device-backed CRTomo state for one tomodir-like problem."""
 
     def __init__(self, mesh: io.Mesh, enr, data: DataSet, cfg: CRTomoConfig, device: int = 0,
-                 lam0: Optional[float] = None):
+                 lam0: Optional[float] = None, ctx=None):
+        """ctx: the problem's device context; default a new Context on
+        `device`.  Any object with Context's set_regularizer / set_data /
+        set_configs / forward / jacobian / update / blam0 / close methods
+        can stand in (the loop's host logic is independent of it)."""
         self.mesh = mesh
         self.cfg = cfg
         self.data = data
-        self.ctx = Context(mesh, enr, data.strnr, data.vnr, swrtr=cfg.swrtr, lsink=cfg.lsink,
-                           nsink=cfg.nsink, device=device)
+        if ctx is None:
+            ctx = Context(mesh, enr, data.strnr, data.vnr, swrtr=cfg.swrtr, lsink=cfg.lsink,
+                          nsink=cfg.nsink, device=device)
+        self.ctx = ctx
         self.manz = mesh.elanz
         self.nanz = len(data.dat)
         if cfg.ltri == 0:
@@ -266,8 +279,9 @@ class Inversion:
         d = self.data
         return dmisft(d.dat, sigmaa, d.wmatd, d.wmatdr, d.wmatdp)
 
-    def roughness(self, par) -> float:
-        """src/brough_mod.f90 (lprior = lfpi = .false.)."""
+    def roughness(self, par, lfpi: bool = False) -> float:
+        """src/brough_mod.f90 (lprior = .false.): Re(R p . conj(p)), or
+        Im(R p) . Im(p) in the final phase improvement."""
         if self.cfg.ltri == 0:
             sm = self.smatm
             M, nx = self.manz, self.cfg.nx
@@ -285,6 +299,8 @@ class Inversion:
                 has = nb > 0
                 rp[has] += self.smatm[has, j] * par[nb[has] - 1]
             rp += self.smatm[:, n] * par
+        if lfpi:
+            return float(np.sum(rp.imag * par.imag))
         return float(np.sum((rp * np.conj(par)).real))
 
     def _start(self):
@@ -350,8 +366,263 @@ class Inversion:
         return dict(nrmsd0=nrmsd0, nrmsd1=nrmsd1, bdpar=up["bdpar"], rough=rough, ncg=up["ncg"],
                     cgres=up["cgres"], lam=self.lam0, par=par1, sigmaa0=sa0, sigmaa1=sa1)
 
+    # -- the whole Gauss-Newton loop ----------------------------------------
+    # control constants of src/rall.f90:196-220
+    NRMSDM, MQRMS, STPMIN, BDMIN, NLAM, FSTART, FSTOP = 1.0, 2e-2, 1e-3, 1e-3, 30, 0.5, 0.9
+
+    def _polarity(self, sigmaa, setup: bool):
+        """chkpol (src/chkpol.f90:43-128) on the current data: corrected data,
+        swapped potential electrodes and excluded readings go to the device;
+        returns the corrected response."""
+        d = self.data
+        dat, sa, vnr, wdfak = chkpol(d.dat, sigmaa, d.vnr, lsetup=setup)
+        changed_v = np.any(vnr != d.vnr)
+        self.data = dataclasses.replace(d, dat=dat, vnr=vnr, wdfak=wdfak)
+        self.ctx.set_data(dat, self.data.wmatd, wdfak)
+        if changed_v:
+            self.ctx.set_configs(d.strnr, vnr)
+        return sa
+
+    def _misfit(self, sigmaa, lfpi: bool):
+        """dmisft (src/dmisft.f90:75-125): every reading, each with its local
+        phase correction (chkpo2)."""
+        d = self.data
+        return dmisft(d.dat, sigmaa, d.wmatd, d.wmatdr, d.wmatdp, lfpi=lfpi)
+
+    def _lam0(self, lfpi: bool, lamnull_fpi: float) -> float:
+        """blam0 (src/blam0.f90:45-167): the presets, else the Jacobian
+        estimate on the device."""
+        c = self.cfg
+        if not lfpi and self.lam0 is not None:
+            return self.lam0
+        if (c.llamf & 1) or lamnull_fpi > np.finfo(float).eps:
+            return float(lamnull_fpi)
+        return self.ctx.blam0(c.alfx, c.alfz, ldc=c.ldc, lfpi=lfpi)
+
+    def run(self, itmax: Optional[int] = None, eps: float = 1e-4, precond: int = 0, lamnull_fpi: float = 0.0,
+            ncgmax: Optional[int] = None):
+        """The Gauss-Newton loop of src/inv.f90:332-956 around the device
+        calls: forward and bvolti at every trial model, chkpol and dmisft,
+        the stop tests (:562-605), the final phase improvement (:606-684),
+        the Jacobian at every accepted iterate (:702-745), the lambda search
+        (:769-880: blam0 at the start of a stage, the multiplicative update
+        by dlam, the step halving and parfit's parabolic step length,
+        :880-912) and update / bsigma / brough (:914-944).  refsig
+        (:949) only matters for singularity removal, which is not built.
+        Returns the inv.ctr rows (kont2, src/kont2.f90) as dicts, the model
+        of every accepted iterate (wout), the final model and response, and
+        the stop code (the reference's errnr2: 79 iterations, 80 optimal
+        RMS, 81 no CHI improvement, 92 repeated step length, 109 minimal
+        update; 82 a zero voltage, the model reset to the last iterate)."""
+        c = self.cfg
+        if c.lrobust:
+            raise NotImplementedError("robust data weighting (lrobust) is outside the implemented path")
+        itmax = c.itmax if itmax is None else itmax
+        ncgmax = ncgmax or self.ncgmax
+        ldc = c.ldc
+        lfphai = c.lfphai and not ldc
+        lffhom = c.stabp0 < 0
+        rows, models = [], []
+        it = itr = 0
+        lsetup, lsetip, lfpi, llam, ldlami, lstep, lfstep = True, False, False, False, True, False, False
+        step, stpalt, alam = 1.0, 1.0, 0.0
+        rmsalt, lamalt, bdpar, bdalt = 0.0, 1.0, 1.0, 1.0
+        if c.llamf & 1:
+            lamalt = c.lamfix
+        lam, dlam, dlalt, ldlamf, rmsreg = 0.0, 1.0, 1.0, False, 0.0
+        ncg, ncg2, rough = 0, 0, 0.0
+        sigma = self.start_model()
+        sigma2, sgmaa2 = sigma.copy(), None
+        dpar = np.zeros(self.manz, np.complex128)
+        dpar2 = dpar.copy()
+        stop = 0
+        while True:
+            try:
+                _, sigmaa = self.ctx.forward(sigma, ldc=ldc, mode=0)
+            except CRTError as exc:    # bvolti: zero voltage -> back to the last iterate
+                if exc.errnr != 82 or sgmaa2 is None:
+                    raise
+                sigma, sigmaa, stop = sigma2, sgmaa2, 82
+                break
+            if lsetup or lsetip:
+                sigmaa = self._polarity(sigmaa, True)
+            nrmsd, betrms, pharms, npol = self._misfit(sigmaa, lfpi)
+            if nrmsd < 1e-12:
+                nrmsd = self.NRMSDM * (1.0 - self.MQRMS)
+            if it == 0 and not rows:
+                models.append(sigma.copy())
+            rows.append(self._kont2_row(lsetup or lsetip, llam and not lstep, lfpi, it, itr, nrmsd, bdpar, lam,
+                                        rough, ncg, betrms, pharms, npol, step))
+            if llam and not lstep:
+                sigmaa = self._polarity(sigmaa, lsetup or lsetip)
+                errnr2 = 0
+                if stpalt == 0.0:
+                    errnr2 = 92
+                if abs(1.0 - rmsalt / nrmsd) <= self.MQRMS:
+                    errnr2 = 81
+                if abs(1.0 - nrmsd / self.NRMSDM) <= self.MQRMS and ldlamf:
+                    errnr2 = 80
+                if it >= itmax:
+                    errnr2 = 79
+                if abs(1.0 - _quot(bdpar, bdalt)) < self.BDMIN:
+                    errnr2 = 109
+                if errnr2:
+                    if lfphai and errnr2 != 79:
+                        # final phase improvement: phase weights, lambda search
+                        # restarted, phase-only update
+                        models.append(sigma.copy())
+                        self.data = dataclasses.replace(self.data, wmatd=self.data.wmatdp.copy())
+                        self.ctx.set_data(self.data.dat, self.data.wmatd, self.data.wdfak)
+                        lfpi, lsetip, lfphai, llam, ldlami, lfstep, step = True, True, False, False, True, True, 1.0
+                        if lffhom:
+                            a = np.abs(sigma)
+                            sigma = a * complex(math.cos(c.pha0 / 1e3), -math.sin(c.pha0 / 1e3))
+                            lsetup = True
+                            continue
+                        lsetup = False
+                        nrmsd, betrms, pharms, npol = self._misfit(sigmaa, lfpi)
+                        rows.append(self._kont2_row(True, False, lfpi, it, itr, nrmsd, bdpar, lam, rough, ncg,
+                                                    betrms, pharms, npol, step))
+                    else:
+                        stop = errnr2
+                        break
+                else:
+                    lamalt = lam
+                    models.append(sigma.copy())
+            if (llam and not lstep) or lsetup or lsetip:
+                it += 1
+                itr, rmsreg, dlam, dlalt, ldlamf, bdpar, bdalt = 0, 0.0, 1.0, 1.0, False, 1.0, 1.0
+                rmsalt = nrmsd
+                if it > 1:
+                    lamalt = lam
+                sigma2, sgmaa2 = sigma.copy(), sigmaa.copy()
+                self.ctx.jacobian(mode=1 if ldc else 0, copy=False)
+            else:
+                sigma, sigmaa = sigma2.copy(), sgmaa2.copy()
+            if itmax == 0:
+                stop = 109
+                break
+            if c.llamf & 1:
+                lam = c.lamfix
+                if (c.llamf & 2) and it > 1:
+                    lam = c.lamfix / (2.0 * (it - 1))
+                llam = False
+                lsetup = lsetip = False
+            elif not lstep:
+                if llam:
+                    llam, step = False, 1.0
+                else:
+                    itr += 1
+                    lr = math.log(nrmsd / self.NRMSDM)
+                    search = ((((nrmsd < rmsreg and itr <= self.NLAM) or (dlam > 1.0 and itr <= self.NLAM))
+                               and (not ldlamf or dlalt <= 1.0) and abs(1.0 - _quot(bdpar, bdalt)) > self.BDMIN
+                               and abs(1.0 - rmsreg / self.NRMSDM) > self.MQRMS) or rmsreg == 0.0)
+                    if search:
+                        if lsetup or lsetip:
+                            lam = self._lam0(lfpi, lamnull_fpi)
+                            lamalt = lam
+                        else:
+                            dlalt = dlam
+                            if ldlami:
+                                ldlami = False
+                                alam = max(abs(lr), math.log(1.0 + self.MQRMS))
+                                dlam = self.FSTART
+                            else:
+                                alam = max(alam, abs(lr))
+                                dlam = math.exp(math.log(self.FSTOP) * math.copysign(1.0, lr)
+                                                + math.log(self.FSTART / self.FSTOP) * lr / alam)
+                            lam *= dlam
+                            if dlalt > 1.0 and dlam < 1.0:
+                                ldlamf = True
+                    else:
+                        # no CHI decrease: back to the last lambda, shorter step
+                        llam = True
+                        lam /= dlam
+                        if lfstep:
+                            lfstep = False
+                        else:
+                            lstep, step = True, 0.5
+                    if lsetup or lsetip:
+                        lsetup = lsetip = False
+                    elif not lstep:
+                        rmsreg = nrmsd
+            else:
+                lstep = False
+                step = parfit(rmsalt, nrmsd, rmsreg, self.NRMSDM, self.STPMIN)
+                stpalt = 0.0 if (step == self.STPMIN and stpalt == self.STPMIN) else step
+            # bpar, update, bsigma, brough
+            par = np.log(sigma)
+            bdalt = bdpar
+            if not llam:
+                dpar2, ncg2 = dpar, ncg
+                prm = Context.params(lam, eps=eps, ncgmax=ncgmax, ldc=ldc, lfpi=lfpi, step=step, precond=precond)
+                up = self.ctx.update(prm, par, sigmaa=sigmaa)
+                par, dpar, ncg, bdpar = up["par"], up["dpar"], up["ncg"], up["bdpar"]
+            else:
+                dpar, ncg = dpar2, ncg2
+                par = par + step * dpar
+                bdpar = float(np.sum(np.abs(dpar) ** 2)) * step
+            sigma = np.exp(par)
+            rough = self.roughness(par, lfpi)
+            if c.llamf & 1:
+                llam = True
+        models.append(sigma.copy())      # the final wout (inv.f90:1026)
+        return dict(rows=rows, models=models, sigma=sigma, sigmaa=sigmaa, stop=stop, it=it)
+
+    @staticmethod
+    def _kont2_row(first, accepted, lfpi, it, itr, nrmsd, bdpar, lam, rough, ncg, betrms, pharms, npol, step):
+        """One control row of inv.ctr (src/kont2.f90:63-128): IT / PIT rows of
+        a starting pass or an accepted iterate, UP / PUP rows of the lambda
+        and step-length trials."""
+        p = "P" if lfpi else ""
+        if first:
+            return dict(kind=p + "IT", it=it, rms=nrmsd, betrms=betrms, pharms=pharms, npol=npol)
+        if accepted:
+            return dict(kind=p + "IT", it=it, rms=nrmsd, step=bdpar, lam=lam, rough=rough, ncg=ncg, betrms=betrms,
+                        pharms=pharms, npol=npol, steplength=step)
+        return dict(kind=p + "UP", it=itr, rms=nrmsd, step=bdpar, lam=lam, rough=rough, ncg=ncg, steplength=step)
+
     def close(self):
         self.ctx.close()
+
+
+def parfit(fa: float, fb: float, fc: float, fmin: float, smin: float) -> float:
+    """src/parfit.f90:38-186: the step length where the parabola through the
+    misfits (0, fa), (0.5, fb), (1, fc) has its minimum, or where the misfit
+    crosses fmin by linear interpolation, clamped to [smin, 1]."""
+    a, b, c = 0.0, 0.5, 1.0
+
+    def parab():
+        num = (b - a) ** 2 * (fb - fc) - (b - c) ** 2 * (fb - fa)
+        den = (b - a) * (fb - fc) - (b - c) * (fb - fa)
+        return b - num / (2.0 * den)
+
+    lin_ab = lambda: a + (b - a) * (fmin - fa) / (fb - fa)  # noqa: E731
+    lin_bc = lambda: b + (c - b) * (fmin - fb) / (fc - fb)  # noqa: E731
+    if fa > fb:
+        if fb <= fc:
+            if fb <= fmin:
+                step = lin_bc() if (fa < fmin and fc > fa) else lin_ab()
+            else:
+                step = parab()
+        else:
+            step = lin_ab() if fb <= fmin else (lin_bc() if fc <= fmin else c)
+    elif fa < fb:
+        if fb >= fc:
+            if fb >= fmin:
+                step = lin_bc() if (fa > fmin and fc < fa) else lin_ab()
+            else:
+                step = parab()
+        else:
+            step = lin_ab() if fb >= fmin else (lin_bc() if fc >= fmin else c)
+    else:
+        if fb > fc:
+            step = parab() if fb < fmin else (lin_bc() if fc <= fmin else c)
+        elif fb < fc:
+            step = parab() if fb > fmin else (lin_bc() if fc >= fmin else c)
+        else:
+            step = smin
+    return min(c, max(smin, step))
 
 
 def load_tomodir_inversion(exe_dir: str, device: int = 0) -> Inversion:

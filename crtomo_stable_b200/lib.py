@@ -70,7 +70,7 @@ EXPORTS = [
     "crt_set_refinement", "crt_set_refinement_tol", "crt_gnn_nparam", "crt_gnn_status", "crt_gnn_init", "crt_gnn_set_weights", "crt_gnn_get_weights", "crt_gnn_collect",
     "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad", "crt_batch_create",
     "crt_batch_destroy", "crt_batch_error", "crt_batch_set_models", "crt_batch_run", "crt_batch_status",
-    "crt_batch_results", "crt_set_workspace_limit", "crt_set_forward_form", "crt_forward_info",
+    "crt_batch_results", "crt_set_workspace_limit", "crt_set_forward_form", "crt_forward_info", "crt_blam0",
 ]
 
 _LIB = None
@@ -148,6 +148,8 @@ def load(path: str = LIB_PATH):
     L.crt_batch_results.restype = C.c_int32
     L.crt_set_workspace_limit.argtypes = [vp, C.c_int64]
     L.crt_set_workspace_limit.restype = C.c_int32
+    L.crt_blam0.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double, f64p]
+    L.crt_blam0.restype = C.c_int32
     L.crt_set_forward_form.argtypes = [vp, C.c_int32]
     L.crt_set_forward_form.restype = C.c_int32
     L.crt_forward_info.argtypes = [vp, i32p, i32p, i32p, i32p]
@@ -462,6 +464,13 @@ class Context:
 
     def launch_count(self):
         return int(self.L.crt_launch_count(self.h))
+
+    def blam0(self, alfx, alfz, ldc=False, lfpi=False):
+        """lambda_0 from the device-resident Jacobian (crt_blam0)."""
+        v = C.c_double()
+        self._check(self.L.crt_blam0(self.h, int(bool(ldc)), int(bool(lfpi)), float(alfx), float(alfz),
+                                     C.byref(v)), "crt_blam0")
+        return v.value
 
     def set_forward_form(self, form):
         """FORWARD_AUTO, FORWARD_DIRECT or FORWARD_SCHUR (crt_set_forward_form)."""

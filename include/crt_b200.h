@@ -195,7 +195,11 @@ int32_t crt_jacobian(crt_ctx *ctx, int32_t mode, const double *strom, double *se
 int32_t crt_set_jacobian(crt_ctx *ctx, int32_t real, const double *sens);
 
 /* Replaces the measurement configurations (same nanz), e.g. after the
- * polarity check of src/chkpol.f90 swapped potential electrodes. */
+ * polarity check of src/chkpol.f90 swapped potential electrodes.  A reading
+ * whose new vnr is its old one with the two potential electrodes swapped
+ * (same strnr) also gets the stored response of the last forward flipped,
+ * as chkpol does (volt -> -volt, the phase of sigmaa moved by pi), so that
+ * crt_jacobian after this call matches the swapped configuration. */
 int32_t crt_set_configs(crt_ctx *ctx, const int32_t *strnr, const int32_t *vnr);
 
 /* Regularisation operator R (src/bsmatm_mod.f90): ltri 0 five-point
@@ -236,6 +240,14 @@ int32_t crt_update(crt_ctx *ctx, const crt_cg_params *prm, const double *sigmaa,
 int32_t crt_update_lambdas(crt_ctx *ctx, const crt_cg_params *prm, int32_t nlam, const double *lams,
                            const double *sigmaa, const double *par, double *par_out, double *dpar,
                            int32_t *ncg, double *bdpar);
+
+/* lambda_0 of src/blam0.f90:131-167 from the device-resident Jacobian and
+ * the weights of crt_set_data (wmatd * wdfak): lammax = 5 * 2/(alfx+alfz)
+ * * sum_j |sum_i conj(J_ij) w_i sum_k J_ik| / manz, with the real Jacobian
+ * (ldc, as stored by crt_jacobian mode 1) or the real part of the complex
+ * one (lfpi).  Two passes over J instead of the reference's O(N M^2) loop;
+ * the presets of src/blam0.f90:45-77 are the caller's. */
+int32_t crt_blam0(crt_ctx *ctx, int32_t ldc, int32_t lfpi, double alfx, double alfz, double *lammax);
 
 /* One Gauss-Newton step of the reference loop (src/inv.f90:426-495,
  * :739-743, :924-933): sigma = exp(par); forward + bvolti; bsensi (or

@@ -1482,3 +1482,88 @@ double orc_dmisft(int nanz, const dcplx *dat, const dcplx *sigmaa, const double 
     if (pharms) *pharms = sqrt(ph / idum);
     return sqrt(nrmsd / (double)idum);
 }
+
+/* src/blam0.f90:131-167 (the Jacobian estimate, no preset): jtj(j) =
+ * |sum_i sum_k conj(J_ij) J_ik w_i wdfak_i| (real parts for lfpi, sensdc
+ * for ldc), lammax = 5 * 2/(alfx+alfz) * sum_j jtj(j) / manz.  The triple
+ * loop of the reference, O(nanz manz^2): small problems only. */
+double orc_blam0(const orc_cg_params *c, const dcplx *sens, const double *sensdc, double alfx, double alfz)
+{
+    const int M = c->manz, N = c->nanz;
+    double tot = 0.0;
+    for (int j = 0; j < M; ++j) {
+        if (c->ldc || c->lfpi) {
+            double dum = 0.0;
+            for (int i = 0; i < N; ++i)
+                for (int k = 0; k < M; ++k) {
+                    const double a = c->ldc ? sensdc[i + (size_t)j * N] : creal(sens[i + (size_t)j * N]);
+                    const double b = c->ldc ? sensdc[i + (size_t)k * N] : creal(sens[i + (size_t)k * N]);
+                    dum += a * b * c->wmatd[i] * (double)c->wdfak[i];
+                }
+            tot += fabs(dum);
+        } else {
+            dcplx cdum = 0.0;
+            for (int i = 0; i < N; ++i)
+                for (int k = 0; k < M; ++k)
+                    cdum += conj(sens[i + (size_t)j * N]) * sens[i + (size_t)k * N] *
+                            (c->wmatd[i] * (double)c->wdfak[i]);
+            tot += cabs(cdum);
+        }
+    }
+    double lammax = tot / (double)M;
+    lammax = lammax * 2.0 / (alfx + alfz);
+    return lammax * 5.0;
+}
+
+/* src/parfit.f90:38-186: step length at the minimum of the parabola through
+ * (0, fa), (0.5, fb), (1, fc), or where it crosses fmin, clamped to
+ * [smin, 1]. */
+double orc_parfit(double fa, double fb, double fc, double fmin, double smin)
+{
+    const double a = 0.0, b = 0.5, c = 1.0;
+    double step = c;
+#define ORC_PARAB() (b - ((b - a) * (b - a) * (fb - fc) - (b - c) * (b - c) * (fb - fa)) / \
+                         (2.0 * ((b - a) * (fb - fc) - (b - c) * (fb - fa))))
+    if (fa > fb) {
+        if (fb <= fc) {
+            if (fb <= fmin) {
+                if (fa < fmin && fc > fa) step = b + (c - b) * (fmin - fb) / (fc - fb);
+                else step = a + (b - a) * (fmin - fa) / (fb - fa);
+            } else {
+                step = ORC_PARAB();
+            }
+        } else {
+            if (fb <= fmin) step = a + (b - a) * (fmin - fa) / (fb - fa);
+            else if (fc <= fmin) step = b + (c - b) * (fmin - fb) / (fc - fb);
+            else step = c;
+        }
+    } else if (fa < fb) {
+        if (fb >= fc) {
+            if (fb >= fmin) {
+                if (fa > fmin && fc < fa) step = b + (c - b) * (fmin - fb) / (fc - fb);
+                else step = a + (b - a) * (fmin - fa) / (fb - fa);
+            } else {
+                step = ORC_PARAB();
+            }
+        } else {
+            if (fb >= fmin) step = a + (b - a) * (fmin - fa) / (fb - fa);
+            else if (fc >= fmin) step = b + (c - b) * (fmin - fb) / (fc - fb);
+            else step = c;
+        }
+    } else {
+        if (fb > fc) {
+            if (fb < fmin) step = ORC_PARAB();
+            else if (fc <= fmin) step = b + (c - b) * (fmin - fb) / (fc - fb);
+            else step = c;
+        } else if (fb < fc) {
+            if (fb > fmin) step = ORC_PARAB();
+            else if (fc >= fmin) step = b + (c - b) * (fmin - fb) / (fc - fb);
+            else step = c;
+        } else {
+            step = smin;
+        }
+    }
+#undef ORC_PARAB
+    if (step < smin) step = smin;
+    return step > c ? c : step;
+}

@@ -166,6 +166,13 @@ void orc_cjggdc(const orc_cg_params *c, const dcplx *sens, const double *sensdc,
 /* src/brough_mod.f90 (tri / reg, lprior = .false.) */
 double orc_brough(const orc_cg_params *c, const dcplx *par);
 
+/* src/blam0.f90:131-167: lambda_0 from the Jacobian (no preset), the
+ * reference's O(nanz manz^2) loop; uses c->wmatd, c->wdfak, c->ldc,
+ * c->lfpi. */
+double orc_blam0(const orc_cg_params *c, const dcplx *sens, const double *sensdc, double alfx, double alfz);
+/* src/parfit.f90:38-186: step length from the misfits at steps 0, 0.5, 1. */
+double orc_parfit(double fa, double fb, double fc, double fmin, double smin);
+
 /* src/dmisft.f90:73-137 with chkpo2 (lrobust = ldiff = .false.).
  * Returns nrmsd; betrms/pharms optional. */
 double orc_dmisft(int nanz, const dcplx *dat, const dcplx *sigmaa,

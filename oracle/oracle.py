@@ -105,6 +105,10 @@ def _declare(L):
     L.orc_brough.restype = C.c_double
     L.orc_dmisft.argtypes = [C.c_int, vp, vp, f64p, f64p, f64p, C.c_int, C.c_int, f64p, f64p, i32p]
     L.orc_dmisft.restype = C.c_double
+    L.orc_blam0.argtypes = [CP, vp, vp, C.c_double, C.c_double]
+    L.orc_blam0.restype = C.c_double
+    L.orc_parfit.argtypes = [C.c_double] * 5
+    L.orc_parfit.restype = C.c_double
     L.orc_bessk0.argtypes = [C.c_double]
     L.orc_bessk0.restype = C.c_double
     L.orc_bessk1.argtypes = [C.c_double]
@@ -351,6 +355,12 @@ class OracleCG:
                           _p(cgres, C.c_double), C.byref(ncg))
         return dpar, cgres[: ncg.value + 1], ncg.value
 
+    def blam0(self, sens=None, sensdc=None, alfx=1.0, alfz=1.0):
+        """lambda_0 of src/blam0.f90:131-167 from the Jacobian."""
+        s_ = np.asfortranarray(sens if sens is not None else np.zeros((1, 1)), np.complex128)
+        d_ = np.asfortranarray(sensdc if sensdc is not None else np.zeros((1, 1)), np.float64)
+        return self.L.orc_blam0(C.byref(self.c), _v(s_), _v(d_), float(alfx), float(alfz))
+
     def brough(self, par):
         p = np.ascontiguousarray(par, np.complex128)
         return self.L.orc_brough(C.byref(self.c), _v(p))
@@ -369,3 +379,8 @@ def dmisft(dat, sigmaa, wmatd, wmatdr=None, wmatdp=None, lfpi=False, lpol=False)
                      None if wr is None else _p(wr, C.c_double), None if wp is None else _p(wp, C.c_double),
                      int(lfpi), int(lpol), C.byref(br), C.byref(ph), C.byref(npol))
     return r, br.value, ph.value, npol.value
+
+
+def parfit(fa, fb, fc, fmin=1.0, smin=1e-3):
+    """src/parfit.f90:38-186."""
+    return lib().orc_parfit(float(fa), float(fb), float(fc), float(fmin), float(smin))

@@ -68,3 +68,67 @@ def read_eps_ctr_first_block(path):
                 j += 1
             break
     return np.array(out)
+
+
+def _printed_tol(tok):
+    """Half a unit in the last printed digit of an inv.ctr number."""
+    t = tok.upper()
+    mant, _, ex = t.partition("E")
+    dec = len(mant.split(".")[1]) if "." in mant else 0
+    return 0.5 * 10.0 ** (-dec) * 10.0 ** (int(ex) if ex else 0)
+
+
+def read_inv_ctr_trajectory(path):
+    """Every control row of inv.ctr (src/kont2.f90): starting rows (IT / PIT
+    with rms, betrms, pharms, npol), lambda / step trials (UP / PUP with rms,
+    stepsize, lambda, roughness, CG steps, steplength) and accepted iterates
+    (IT / PIT with all of them), each value with its print tolerance, and the
+    marker of a phase-model reset."""
+    rows = []
+    names_setup = ("rms", "betrms", "pharms", "npol")
+    names_up = ("rms", "step", "lam", "rough", "ncg", "steplength")
+    names_it = ("rms", "step", "lam", "rough", "ncg", "betrms", "pharms", "npol", "steplength")
+    with open(path) as fh:
+        for ln in fh:
+            t = ln.split()
+            if "Resetting phase model" in ln:
+                rows.append(dict(kind="RESET"))
+                continue
+            if not t or t[0] not in ("IT", "UP", "PIT", "PUP") or len(t) < 3:
+                continue
+            vals = t[2:]
+            if t[0] in ("UP", "PUP"):
+                names = names_up
+            elif len(vals) == len(names_it):
+                names = names_it
+            else:
+                names = names_setup
+            r = dict(kind=t[0], it=int(t[1]), setup=names is names_setup, tol={})
+            for n, v in zip(names, vals):
+                if v.upper() == "NAN":
+                    continue
+                r[n] = int(v) if n in ("ncg", "npol") else float(v)
+                r["tol"][n] = _printed_tol(v)
+            rows.append(r)
+    return rows
+
+
+def compare_trajectory(got, gold, slack=1.5, rel_extra=0.0):
+    """Mismatches between Inversion.run rows and recorded rows, value by
+    value within `slack` times the print tolerance (plus rel_extra relative);
+    CG steps and excluded-reading counts exactly."""
+    bad = []
+    gold = [g for g in gold if g["kind"] != "RESET"]
+    for i, (a, g) in enumerate(zip(got, gold)):
+        if a["kind"] != g["kind"] or a["it"] != g["it"]:
+            bad.append((i, "kind/it", (a["kind"], a["it"]), (g["kind"], g["it"])))
+            continue
+        for n, tol in g["tol"].items():
+            if n not in a:
+                continue
+            if n in ("ncg", "npol"):
+                if int(a[n]) != g[n]:
+                    bad.append((i, n, a[n], g[n]))
+            elif abs(a[n] - g[n]) > slack * tol + rel_extra * abs(g[n]):
+                bad.append((i, n, a[n], g[n]))
+    return bad
