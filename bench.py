@@ -60,6 +60,10 @@ def parse():
     ap.add_argument("--lambdas", type=int, default=4,
                     help="lambda candidates of the batched Jacobi-form update measured after the step (0: skip)")
     ap.add_argument("--lambda-iters", type=int, default=100, help="CG iterations of that measurement")
+    ap.add_argument("--inversion", action="store_true",
+                    help="run the configuration's whole Gauss-Newton inversion (inv.f90's loop) to its stop "
+                         "criterion and print one JSON line with its iterations and wall time")
+    ap.add_argument("--itmax", type=int, default=20, help="iteration limit of --inversion")
     return ap.parse_args()
 
 
@@ -537,9 +541,53 @@ def lambda_batch(ctx, Context, lam, par0, nlam, iters, E, N, eps, ncgmax, precon
                               "matvecs"}}
 
 
+def run_inversion(args, local):
+    """The complete inversion of a synthetic survey through Inversion.run:
+    forward at every trial model, Jacobian at every iterate, lambda search,
+    step-length control, stop tests; wall time on the host around the whole
+    loop (every device call in it is synchronous)."""
+    from crtomo_stable_b200 import inversion
+    s = make_problem(args.config)
+    inv = inversion.synthetic_inversion(s, device=local, itmax=args.itmax)
+    calls = {"forward": 0, "jacobian": 0, "update": 0}
+    ctx = inv.ctx
+    for name in calls:
+        fn = getattr(ctx, name)
+
+        def counted(*a, _fn=fn, _n=name, **k):
+            calls[_n] += 1
+            return _fn(*a, **k)
+        setattr(ctx, name, counted)
+    t0 = time.perf_counter()
+    res = inv.run()
+    wall = time.perf_counter() - t0
+    rows = res["rows"]
+    its = [r for r in rows if r["kind"] == "IT"]
+    m = s.mesh
+    print(json.dumps({
+        "metric": "full GN inversion wall time", "value": round(wall, 3), "unit": "s", "impl": "ours",
+        "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+        "config": {"workload": f"{s.name}: {m.elanz} elements, {len(s.enr)} electrodes, {len(s.strnr)} readings, "
+                               f"3 % + 0.1 mrad noise, homogeneous start, itmax {args.itmax}"},
+        "stop_errnr": res["stop"], "iterations": res["it"], "rms_start": round(its[0]["rms"], 4),
+        "rms_final": round(its[-1]["rms"], 4), "lambda_final": its[-1].get("lam"),
+        "forwards": calls["forward"], "jacobians": calls["jacobian"], "updates": calls["update"],
+        "cg_steps": int(sum(r.get("ncg", 0) for r in rows if r["kind"] in ("UP", "PUP"))),
+        "rows": [{k: (round(v, 5) if isinstance(v, float) else v) for k, v in r.items()} for r in rows],
+    }))
+    inv.close()
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_init(args)
+    if args.inversion:
+        if rank == 0:
+            run_inversion(args, local)
+        if pg is not None:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
     if args.config == "C4" and args.impl == "ours":
         run_batch(args, ws, rank, local, pg)
         if pg is not None:

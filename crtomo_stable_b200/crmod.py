@@ -21,7 +21,7 @@ import time
 
 import numpy as np
 
-from . import io
+from . import io, writers
 
 
 def bkfak(mesh, enr, strnr, vnr) -> np.ndarray:
@@ -77,18 +77,20 @@ def run(exe_dir: str, device: int = 0, verbose: bool = True) -> dict:
         os.makedirs(os.path.dirname(path), exist_ok=True)
         io.write_volt(path, strnr, vnr, sigmaa)
         out["volt"] = path
-    if cfg.lsens:
-        sens = ctx.jacobian(mode=2)
-        path = io.resolve(exe_dir, cfg.sens)
-        os.makedirs(os.path.dirname(path), exist_ok=True)
-        np.save(path + ".npy", sens)
-        out["sens"] = path + ".npy"
     if cfg.lpot:
+        # bpot / wpot (src/bpot.f90, src/wpot.f90): one file per reading
         hpot = ctx.potentials()
         path = io.resolve(exe_dir, cfg.pot)
         os.makedirs(os.path.dirname(path), exist_ok=True)
-        np.save(path + ".npy", hpot)
-        out["pot"] = path + ".npy"
+        nx, ny = mesh.node_xy(np.arange(1, mesh.sanz + 1))
+        out["pot"] = writers.write_potentials(path, hpot, strnr, nx, ny)
+    if cfg.lsens:
+        # bsens + wsens (src/bsens.f90, src/wsens.f90): one file per reading
+        sens = ctx.jacobian(mode=2)
+        path = io.resolve(exe_dir, cfg.sens)
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        espx, espy = mesh.midpoints()
+        out["sens"] = writers.write_sensitivities(path, sens, espx, espy)
     tm = ctx.timings()
     ctx.close()
     if verbose:

@@ -1676,6 +1676,24 @@ __global__ void k_blam0_col(const S* __restrict__ J, int N, int M, int re_part, 
     if (lane == 0) jtj[j] = hypot(acc.x, acc.y);
 }
 
+// Coverage (bbsens.f90:52-78): one warp per model cell, sum_i |J_ij| w_i
+// (|Re J_ij| for part 1); w = the caller's weights or sqrt(wmatd wdfak).
+template <typename S>
+__global__ void k_coverage_col(const S* __restrict__ J, int N, int M, int re_part, const double* __restrict__ w,
+                               int w_is_sq, double* csens)
+{
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (j >= M) return;
+    double acc = 0.0;
+    for (int i = lane; i < N; i += 32) {
+        const cd a = jval<S>(J, (size_t)j * N + i);
+        const double wi = w_is_sq ? sqrt(w[i]) : w[i];
+        acc += (re_part ? fabs(a.x) : hypot(a.x, a.y)) * wi;
+    }
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+    if (lane == 0) csens[j] = acc;
+}
+
 template <typename S>
 void blam0_launch(const crt_ctx* ctx, int re_part, cd* s, double* jtj)
 {
@@ -1722,6 +1740,45 @@ extern "C" int32_t crt_blam0(crt_ctx* ctx, int32_t ldc, int32_t lfpi, double alf
     for (double v : h) tot += v;
     *lammax = tot / (double)ctx->E * 2.0 / (alfx + alfz) * 5.0;
     return CRT_OK;
+}
+
+extern "C" int32_t crt_coverage(crt_ctx* ctx, int32_t part, const double* weight, double* csens)
+{
+    if (!ctx || !csens || part < 0 || part > 1) return CRT_ERR_ARG;
+    if (!ctx->have_sens || !ctx->d_sens) return set_err(ctx, CRT_ERR_ARG, "crt_coverage before crt_jacobian");
+    if (!weight && !ctx->d_wd) return set_err(ctx, CRT_ERR_ARG, "crt_coverage without weights before crt_set_data");
+    CK(cudaSetDevice(ctx->device));
+    double *w = nullptr, *cs = nullptr;
+    CK(cudaMalloc((void**)&cs, sizeof(double) * (size_t)ctx->E));
+    if (weight) {
+        if (cudaMalloc((void**)&w, sizeof(double) * (size_t)ctx->N) != cudaSuccess) {
+            cudaFree(cs);
+            return set_err(ctx, CRT_ERR_CUDA, "cudaMalloc of the coverage weights");
+        }
+        if (cudaMemcpyAsync(w, weight, sizeof(double) * ctx->N, cudaMemcpyHostToDevice, ctx->st) != cudaSuccess) {
+            cudaFree(cs);
+            cudaFree(w);
+            return set_err(ctx, CRT_ERR_CUDA, "coverage weights copy");
+        }
+    }
+    const double* wd = weight ? w : ctx->d_wd;
+    const int sq = weight ? 0 : 1, g = (ctx->E * 32 + 255) / 256;
+    const bool f32 = ctx->prec == CRT_PREC_MIXED;
+    if (ctx->sens_real) {
+        if (f32) k_coverage_col<float><<<g, 256, 0, ctx->st>>>(static_cast<const float*>(ctx->d_sens), ctx->N, ctx->E, 0, wd, sq, cs);
+        else k_coverage_col<double><<<g, 256, 0, ctx->st>>>(static_cast<const double*>(ctx->d_sens), ctx->N, ctx->E, 0, wd, sq, cs);
+    } else {
+        if (f32) k_coverage_col<cf><<<g, 256, 0, ctx->st>>>(static_cast<const cf*>(ctx->d_sens), ctx->N, ctx->E, part, wd, sq, cs);
+        else k_coverage_col<cd><<<g, 256, 0, ctx->st>>>(static_cast<const cd*>(ctx->d_sens), ctx->N, ctx->E, part, wd, sq, cs);
+    }
+    ctx->launches++;
+    int e = kernel_check(ctx, "coverage");
+    if (!e && cudaMemcpyAsync(csens, cs, sizeof(double) * ctx->E, cudaMemcpyDeviceToHost, ctx->st) != cudaSuccess)
+        e = set_err(ctx, CRT_ERR_CUDA, "coverage copy");
+    if (!e && cudaStreamSynchronize(ctx->st) != cudaSuccess) e = set_err(ctx, CRT_ERR_CUDA, "coverage sync");
+    cudaFree(cs);
+    if (w) cudaFree(w);
+    return e;
 }
 
 extern "C" int32_t crt_set_model(crt_ctx* ctx, const double* par)

@@ -15,7 +15,7 @@ from typing import Optional
 
 import numpy as np
 
-from . import io, regularization
+from . import io, regularization, writers
 from .lib import Context, CRTError, dmisft
 
 
@@ -400,7 +400,7 @@ class Inversion:
         return self.ctx.blam0(c.alfx, c.alfz, ldc=c.ldc, lfpi=lfpi)
 
     def run(self, itmax: Optional[int] = None, eps: float = 1e-4, precond: int = 0, lamnull_fpi: float = 0.0,
-            ncgmax: Optional[int] = None):
+            ncgmax: Optional[int] = None, out_dir: Optional[str] = None):
         """The Gauss-Newton loop of src/inv.f90:332-956 around the device
         calls: forward and bvolti at every trial model, chkpol and dmisft,
         the stop tests (:562-605), the final phase improvement (:606-684),
@@ -413,7 +413,11 @@ class Inversion:
         of every accepted iterate (wout), the final model and response, and
         the stop code (the reference's errnr2: 79 iterations, 80 optimal
         RMS, 81 no CHI improvement, 92 repeated step length, 109 minimal
-        update; 82 a zero voltage, the model reset to the last iterate)."""
+        update; 82 a zero voltage, the model reset to the last iterate).
+        With out_dir, the files of an inversion directory are written as the
+        reference writes them: rhoNN.* / voltNN.dat at every wout, and at
+        the end coverage.mag (bbsens, from the last Jacobian) and the rows of
+        inv.ctr."""
         c = self.cfg
         if c.lrobust:
             raise NotImplementedError("robust data weighting (lrobust) is outside the implemented path")
@@ -422,7 +426,20 @@ class Inversion:
         ldc = c.ldc
         lfphai = c.lfphai and not ldc
         lffhom = c.stabp0 < 0
-        rows, models = [], []
+        rows, models, events = [], [], {}
+        espx, espy = self.mesh.midpoints()
+        betrms = pharms = 0.0
+
+        def wout(it_, sig_, sa_):
+            d = self.data
+            models.append(dict(it=it_, sigma=sig_.copy(), sigmaa=sa_.copy(), betrms=betrms, pharms=pharms,
+                               vnr=d.vnr.copy(), wdfak=d.wdfak.copy()))
+            if out_dir:
+                writers.write_model(out_dir, it_, espx, espy, sig_, betrms, pharms, ldc)
+                writers.write_volt_iterate(out_dir, it_, d.strnr, d.vnr, sa_, d.wdfak, ldc)
+
+        if out_dir:
+            os.makedirs(out_dir, exist_ok=True)
         it = itr = 0
         lsetup, lsetip, lfpi, llam, ldlami, lstep, lfstep = True, False, False, False, True, False, False
         step, stpalt, alam = 1.0, 1.0, 0.0
@@ -450,7 +467,7 @@ class Inversion:
             if nrmsd < 1e-12:
                 nrmsd = self.NRMSDM * (1.0 - self.MQRMS)
             if it == 0 and not rows:
-                models.append(sigma.copy())
+                wout(0, sigma, sigmaa)
             rows.append(self._kont2_row(lsetup or lsetip, llam and not lstep, lfpi, it, itr, nrmsd, bdpar, lam,
                                         rough, ncg, betrms, pharms, npol, step))
             if llam and not lstep:
@@ -470,7 +487,8 @@ class Inversion:
                     if lfphai and errnr2 != 79:
                         # final phase improvement: phase weights, lambda search
                         # restarted, phase-only update
-                        models.append(sigma.copy())
+                        wout(it, sigma, sigmaa)
+                        events.setdefault(len(rows), []).append("FPI")
                         self.data = dataclasses.replace(self.data, wmatd=self.data.wmatdp.copy())
                         self.ctx.set_data(self.data.dat, self.data.wmatd, self.data.wdfak)
                         lfpi, lsetip, lfphai, llam, ldlami, lfstep, step = True, True, False, False, True, True, 1.0
@@ -478,6 +496,7 @@ class Inversion:
                             a = np.abs(sigma)
                             sigma = a * complex(math.cos(c.pha0 / 1e3), -math.sin(c.pha0 / 1e3))
                             lsetup = True
+                            events.setdefault(len(rows), []).append("RESET")
                             continue
                         lsetup = False
                         nrmsd, betrms, pharms, npol = self._misfit(sigmaa, lfpi)
@@ -488,7 +507,7 @@ class Inversion:
                         break
                 else:
                     lamalt = lam
-                    models.append(sigma.copy())
+                    wout(it, sigma, sigmaa)
             if (llam and not lstep) or lsetup or lsetip:
                 it += 1
                 itr, rmsreg, dlam, dlalt, ldlamf, bdpar, bdalt = 0, 0.0, 1.0, 1.0, False, 1.0, 1.0
@@ -566,8 +585,22 @@ class Inversion:
             rough = self.roughness(par, lfpi)
             if c.llamf & 1:
                 llam = True
-        models.append(sigma.copy())      # the final wout (inv.f90:1026)
-        return dict(rows=rows, models=models, sigma=sigma, sigmaa=sigmaa, stop=stop, it=it)
+        wout(it, sigma, sigmaa)            # the final wout (inv.f90:1026)
+        if out_dir:
+            self._write_coverage(os.path.join(out_dir, "coverage.mag"), lfpi, espx, espy)
+            writers.write_inv_ctr_rows(os.path.join(out_dir, "inv.ctr"), rows, events)
+        return dict(rows=rows, models=models, sigma=sigma, sigmaa=sigmaa, stop=stop, it=it, events=events)
+
+    def _write_coverage(self, path: str, lfpi: bool, espx, espy):
+        """bbsens (src/bbsens.f90) on the device-resident Jacobian: the
+        weights of the current phase (lelerr: wmatd_cri, else wmatdr, in the
+        final phase improvement; wmatd otherwise), |Re J| for the FPI file."""
+        c, d = self.cfg, self.data
+        lelerr = (not c.lfphai and not c.ldc) or bool(c.mswitch & (1 << 5))
+        w, w_fpi = writers.bbsens_weights(d.wmatd, d.wmatdr, d.wmatd_cri, d.wdfak, lfpi, lelerr)
+        cs = self.ctx.coverage(0, w)
+        cs_fpi = self.ctx.coverage(1, w_fpi) if w_fpi is not None else None
+        return writers.write_coverage(path, espx, espy, cs, cs_fpi)
 
     @staticmethod
     def _kont2_row(first, accepted, lfpi, it, itr, nrmsd, bdpar, lam, rough, ncg, betrms, pharms, npol, step):
@@ -672,3 +705,32 @@ def chkpol(dat: np.ndarray, sigmaa: np.ndarray, vnr: np.ndarray, lsetup: bool, l
             sigmaa[i] = complex(resig, imsig + isig * pi)
             dat[i] = complex(redat, imdat + idat * pi)
     return dat, sigmaa, vnr, wdfak
+
+
+def synthetic_inversion(s, device: int = 0, itmax: int = 20, precision: int = 0, noise=(0.03, 0.1),
+                        seed: int = 20261203, bet0: float = 100.0, pha0: float = 0.0, ctx=None) -> Inversion:
+    """A complex inversion of a synthetic survey (crtomo_stable_b200.synth):
+    the 'observed' data are the true model's response with seeded Gaussian
+    noise (relative magnitude noise[0], phase noise[1] mrad), the error model
+    of src/rdati.f90 with the same levels (A1 = 100 noise[0] %, A3 =
+    noise[1] mrad), the regular-grid smoothness regulariser of
+    src/bsmatm_mod.f90:190-362 on quadrilateral grids (nx x nz elements, row
+    by row) or the triangular one otherwise, lambda_0 from blam0's Jacobian
+    estimate, a homogeneous start (bet0 Ohm m, pha0 mrad) and no final phase
+    improvement.  ctx: a stand-in context (as for Inversion), default a
+    new device Context."""
+    if ctx is None:
+        ctx = Context(s.mesh, s.enr, s.strnr, s.vnr, device=device, precision=precision)
+    _, sa_true = ctx.forward(s.sigma)
+    rng = np.random.default_rng(seed)
+    bet = np.exp(-sa_true.real) * (1.0 + noise[0] * rng.standard_normal(len(sa_true)))
+    pha = -1e3 * sa_true.imag + noise[1] * rng.standard_normal(len(sa_true))
+    d = io.Data(np.asarray(s.strnr, np.int32), np.asarray(s.vnr, np.int32), np.abs(bet), pha)
+    quads = int(s.mesh.typ[0]) == 8 and s.nx * s.nz == s.mesh.elanz
+    cfg = CRTomoConfig(mswitch=0, elem="", elec="", volt="", ramd="", ldiff=False,
+                       nx=s.nx if quads else 0, nz=s.nz if quads else 0, alfx=1.0, alfz=1.0, itmax=itmax,
+                       ldc=False, lrobust=False, lfphai=False, stabw0=100.0 * noise[0], stabm0=0.0, stabpA1=0.0,
+                       stabpB=0.0, stabpA2=0.0, stabp0=noise[1], lrho0=True, bet0=bet0, pha0=pha0,
+                       lagain=False, swrtr=1, lsink=False, nsink=0, lrandb2=False, randb="",
+                       ltri=0 if quads else 1)
+    return Inversion(s.mesh, s.enr, error_model(d, cfg), cfg, ctx=ctx)

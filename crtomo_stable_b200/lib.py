@@ -71,6 +71,7 @@ EXPORTS = [
     "crt_gnn_clear", "crt_gnn_train", "crt_gnn_record", "crt_gnn_record_grad", "crt_batch_create",
     "crt_batch_destroy", "crt_batch_error", "crt_batch_set_models", "crt_batch_run", "crt_batch_status",
     "crt_batch_results", "crt_set_workspace_limit", "crt_set_forward_form", "crt_forward_info", "crt_blam0",
+    "crt_coverage",
 ]
 
 _LIB = None
@@ -150,6 +151,8 @@ def load(path: str = LIB_PATH):
     L.crt_set_workspace_limit.restype = C.c_int32
     L.crt_blam0.argtypes = [vp, C.c_int32, C.c_int32, C.c_double, C.c_double, f64p]
     L.crt_blam0.restype = C.c_int32
+    L.crt_coverage.argtypes = [vp, C.c_int32, vp, vp]
+    L.crt_coverage.restype = C.c_int32
     L.crt_set_forward_form.argtypes = [vp, C.c_int32]
     L.crt_set_forward_form.restype = C.c_int32
     L.crt_forward_info.argtypes = [vp, i32p, i32p, i32p, i32p]
@@ -475,6 +478,14 @@ class Context:
     def set_forward_form(self, form):
         """FORWARD_AUTO, FORWARD_DIRECT or FORWARD_SCHUR (crt_set_forward_form)."""
         self._check(self.L.crt_set_forward_form(self.h, int(form)), "crt_set_forward_form")
+
+    def coverage(self, part=0, weight=None):
+        """csens (bbsens.f90) from the device-resident Jacobian (crt_coverage):
+        sum_i |J_ij| w_i, |Re J_ij| for part 1; weight None = sqrt(wmatd wdfak)."""
+        w = None if weight is None else np.ascontiguousarray(weight, np.float64)
+        out = np.zeros(self.elanz)
+        self._check(self.L.crt_coverage(self.h, int(part), _vp(w), _vp(out)), "crt_coverage")
+        return out
 
     def forward_info(self):
         """(form of the last forward, boundary nodes, interior nodes, interior band)."""

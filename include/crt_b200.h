@@ -249,6 +249,15 @@ int32_t crt_update_lambdas(crt_ctx *ctx, const crt_cg_params *prm, int32_t nlam,
  * the presets of src/blam0.f90:45-77 are the caller's. */
 int32_t crt_blam0(crt_ctx *ctx, int32_t ldc, int32_t lfpi, double alfx, double alfz, double *lammax);
 
+/* Coverage of src/bbsens.f90:52-78 from the device-resident Jacobian:
+ * csens[j] = sum_i |J_ij| w_i (part 0; |Re J_ij| for part 1, the final
+ * phase improvement's csens_fpi; the real Jacobian of crt_jacobian mode 1
+ * takes part 0).  weight: [nanz] per-reading weights (bbsens's
+ * sqrt(wmatd_cri | wmatdr | wmatd) * wdfak), or NULL for sqrt(wmatd * wdfak)
+ * of crt_set_data.  The normalisation and log10 of the written file are
+ * the caller's. */
+int32_t crt_coverage(crt_ctx *ctx, int32_t part, const double *weight, double *csens);
+
 /* One Gauss-Newton step of the reference loop (src/inv.f90:426-495,
  * :739-743, :924-933): sigma = exp(par); forward + bvolti; bsensi (or
  * bsendc); update.  par is updated in place.  Outputs as crt_update plus

@@ -17,7 +17,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = {
     "minimal": ("minimal/Reference", [
         "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg",
-        "exe/crtomo.cfg", "inv/volt00.dat", "inv/eps.ctr", "inv/inv.ctr", "inv/cjg.ctr"]),
+        "exe/crtomo.cfg", "inv/volt00.dat", "inv/eps.ctr", "inv/inv.ctr", "inv/cjg.ctr",
+        "inv/volt01.dat", "inv/volt02.dat", "inv/volt03.dat", "inv/coverage.mag", "inv/coverage.mag_fpi"]
+        + [f"inv/rho{i:02d}.{e}" for i in range(4) for e in ("mag", "pha", "modl")]),
     "TestModInv": ("TestModInv/Reference", [
         "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg"]),
     "Lambda_search": ("Lambda_search/Test", [
@@ -35,7 +37,7 @@ CASES = {
         "inv/inv.ctr", "inv/volt00.dat"]),
     "dc_problem_complex": ("DC_Problem/Complex", [
         "grid/elem.dat", "grid/elec.dat", "mod/volt.dat", "exe/crtomo.cfg", "inv/eps.ctr",
-        "inv/inv.ctr", "inv/cjg.ctr"]),
+        "inv/inv.ctr", "inv/cjg.ctr", "inv/rho00.mag", "inv/rho01.mag", "inv/rho01.modl"]),
 }
 
 

@@ -93,5 +93,13 @@ class OracleContext:
         _P.ldc, _P.lfpi = ldc, lfpi
         return self._cg(_P).blam0(sens=self.sens, sensdc=self.sensdc, alfx=alfx, alfz=alfz)
 
+    def coverage(self, part=0, weight=None):
+        """bbsens's column sums (src/bbsens.f90:52-70) of the resident
+        Jacobian in numpy."""
+        w = np.sqrt(self.wmatd * self.wdfak) if weight is None else np.asarray(weight)
+        J = self.sensdc if self.sens is None else self.sens
+        a = np.abs(J.real) if (part == 1 and self.sens is not None) else np.abs(J)
+        return (a * w[:, None]).sum(axis=0)
+
     def close(self):
         pass

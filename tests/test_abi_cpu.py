@@ -30,6 +30,28 @@ def test_library_exports_every_declared_entry_point():
     assert L.crt_abi_version() == 2
 
 
+def test_fortran_module_binds_every_entry_point():
+    """include/crt_b200.f90 has one BIND(C) interface per header function,
+    and INTEGRATION.md shows that file verbatim."""
+    with open(os.path.join(ROOT, "include", "crt_b200.f90")) as fh:
+        mod = fh.read()
+    bound = re.findall(r"NAME='(crt_[a-z0-9_]+)'", mod)
+    assert sorted(bound) == declared_functions()
+    assert len(bound) == len(set(bound))
+    # each interface's dummy-argument count matches the C prototype
+    with open(os.path.join(ROOT, "include", "crt_b200.h")) as fh:
+        h = re.sub(r"/\*.*?\*/", "", fh.read(), flags=re.S)
+    for name in bound:
+        proto = re.search(r"\b" + name + r"\s*\(([^;]*?)\)\s*;", h, flags=re.S).group(1)
+        nc = 0 if proto.strip() in ("", "void") else proto.count(",") + 1
+        head = re.search(r"(?:FUNCTION|SUBROUTINE)\s+" + name + r"\s*\(([^)]*)\)", mod, flags=re.S).group(1)
+        head = head.replace("&", " ")
+        nf = 0 if not head.strip() else head.count(",") + 1
+        assert nc == nf, (name, nc, nf)
+    with open(os.path.join(ROOT, "INTEGRATION.md")) as fh:
+        assert mod in fh.read()
+
+
 def test_rwaven_host_entry_point_matches_oracle():
     from crtomo_stable_b200 import io, lib
     from oracle.oracle import OracleProblem

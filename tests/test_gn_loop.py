@@ -14,12 +14,14 @@ import pytest
 
 from fixtures import GOLDEN, compare_trajectory, read_inv_ctr_trajectory
 
-# DC_Problem/Complex was recorded by an older release (its eps.ctr and
-# inv.ctr headers have another layout).  Its first lambda trial of iteration
-# 1 (UP 0, lambda 2816) differs from the current source's arithmetic while
-# the model responses of IT 0 and IT 1 (eps.ctr) and the next trial (UP 1,
-# lambda 1408, same Jacobian) agree to print precision; the rows compared
-# are those up to IT 1 and that UP 1.
+# DC_Problem/Complex: at iteration 1 the CG stop rule |r|^2 <= eps |r0|^2
+# is decided at the rounding level.  The device and oracle Jacobians agree to
+# 4e-10 of each row's maximum, yet the trial at lambda 2816 (UP 0) takes 33
+# CG steps with the device's J and 35 with the oracle's, and the trial at
+# lambda 1408 (UP 1) 26 and 28.  The recording has 33 and 28: the device
+# reproduces its UP 0, the oracle its UP 1.  The loop's later branches follow
+# these counts, so the rows compared are IT 0 .. IT 1 (5 rows) and the one
+# trial each arithmetic reproduces.
 DCC_ROWS = 5
 # Print precision plus 0.2 % relative: most trials stop at ncgmax (30 CG
 # steps on minimal), where the truncated iteration carries the rounding
@@ -79,6 +81,7 @@ def test_gn_loop_dc_problem_complex_trajectory_oracle():
     assert compare_trajectory(res["rows"][:DCC_ROWS], gold[:DCC_ROWS], rel_extra=REL) == []
     assert compare_trajectory([res["rows"][DCC_ROWS + 1]], [gold[DCC_ROWS + 1]], rel_extra=REL) == []
     assert res["rows"][DCC_ROWS]["kind"] == "UP" and res["rows"][DCC_ROWS]["lam"] == 2816.0
+    assert abs(res["rows"][DCC_ROWS]["ncg"] - gold[DCC_ROWS]["ncg"]) <= 2
 
 
 def test_gn_loop_stops_at_itmax_and_fixed_lambda():
@@ -138,7 +141,8 @@ def test_gn_loop_dc_problem_complex_trajectory_device():
     res = inv.run(itmax=2)
     gold = read_inv_ctr_trajectory(os.path.join(GOLDEN, "dc_problem_complex", "inv", "inv.ctr"))
     assert compare_trajectory(res["rows"][:DCC_ROWS], gold[:DCC_ROWS], rel_extra=REL) == []
-    assert compare_trajectory([res["rows"][DCC_ROWS + 1]], [gold[DCC_ROWS + 1]], rel_extra=REL) == []
+    assert compare_trajectory([res["rows"][DCC_ROWS]], [gold[DCC_ROWS]], rel_extra=REL) == []
+    assert abs(res["rows"][DCC_ROWS + 1]["ncg"] - gold[DCC_ROWS + 1]["ncg"]) <= 2
     inv.close()
 
 
@@ -166,4 +170,142 @@ def test_blam0_device_matches_oracle(mode):
     else:
         ref = cg.blam0(sens=J, alfx=c.alfx, alfz=c.alfz)
     assert abs(got / ref - 1) < 1e-10
+    inv.close()
+
+
+def _small_survey():
+    """36 x 12 quadrilaterals, 24 surface electrodes, dipole-dipole a = 1, 2
+    (n <= 6), a 10 Ohm m / -20 mrad block in 100 Ohm m / -5 mrad."""
+    from crtomo_stable_b200 import synth
+    xs = np.linspace(-6.0, 30.0, 37)
+    mesh = synth.structured_mesh(xs, synth.graded_depths(12, 0.5, 1.1), triangles=False)
+    cx, cy = synth.centroids(mesh)
+    rho = np.full(mesh.elanz, 100.0)
+    pha = np.full(mesh.elanz, -5.0)
+    blk = synth._ellipse_mask(cx, cy, 12.0, -2.5, 3.0, 1.5)
+    rho[blk], pha[blk] = 10.0, -20.0
+    enr = synth.surface_electrodes(mesh, xs, np.arange(24, dtype=np.float64), 12)
+    strnr, vnr = synth.encode(synth.dipole_dipole(24, (1, 2), 6))
+    return synth.Survey(mesh, enr, strnr, vnr, synth.sigma_from(rho, pha), "small", 36, 12)
+
+
+def _synthetic_run(ctx=None):
+    from crtomo_stable_b200 import inversion
+    s = _small_survey()
+    if ctx == "oracle":
+        ctx = _oracle_ctx(s.mesh, s.enr, s.strnr, s.vnr)
+    inv = inversion.synthetic_inversion(s, ctx=ctx)
+    res = inv.run()
+    inv.close()
+    return res
+
+
+def test_gn_loop_synthetic_converges_oracle():
+    """A complete complex inversion (five-point regulariser, lambda_0 from
+    blam0's Jacobian estimate) of noisy synthetic data runs to the RMS stop
+    criterion."""
+    res = _synthetic_run("oracle")
+    its = [r for r in res["rows"] if r["kind"] == "IT"]
+    assert res["stop"] in (80, 81, 109)
+    assert its[0]["rms"] > 10 and 0.9 < its[-1]["rms"] < 1.2
+    assert all(b["rms"] < a["rms"] * 1.05 for a, b in zip(its, its[1:]))
+
+
+@pytest.mark.gpu
+def test_gn_loop_synthetic_device_matches_oracle():
+    """The same inversion on the device follows the oracle's trajectory row
+    by row: same branches, same CG step counts, misfits, lambdas,
+    roughness and step sizes to 1e-5 (the FP64 Schur-form forward and the
+    oracle's band solves round differently; the differences grow through the
+    truncated CG solves of later iterations)."""
+    dev = _synthetic_run(None)
+    orc = _synthetic_run("oracle")
+    assert [(r["kind"], r["it"]) for r in dev["rows"]] == [(r["kind"], r["it"]) for r in orc["rows"]]
+    for a, b in zip(dev["rows"], orc["rows"]):
+        if "ncg" in b:
+            assert a["ncg"] == b["ncg"]
+        for k in ("rms", "lam", "rough", "step"):
+            if k in b:
+                assert abs(a[k] - b[k]) <= 1e-5 * max(abs(b[k]), 1e-3), (k, a, b)
+    assert dev["stop"] == orc["stop"]
+    np.testing.assert_allclose(dev["sigma"], orc["sigma"], rtol=1e-5)
+
+
+def _table(path, skip=1):
+    rows = []
+    with open(path) as fh:
+        for ln in fh.read().splitlines()[skip:]:
+            t = ln.split()
+            if t and not t[0].startswith("Max"):
+                rows.append([float(x) for x in t])
+    return np.array(rows)
+
+
+# (file, column, tolerance, relative?) of the minimal inversion's outputs
+# against the recorded inv/ directory: log10 |rho| and coverage in log10
+# units, |R| of voltNN.dat and 1/Re(sigma) of .modl relative
+MINIMAL_FILES = [(f"rho{i:02d}.mag", 2, 5e-4, False) for i in range(4)] + \
+    [(f"rho{i:02d}.pha", 2, 1e-6, False) for i in range(4)] + \
+    [(f"rho{i:02d}.modl", 0, 2e-3, True) for i in range(4)] + \
+    [(f"volt{i:02d}.dat", 2, 2e-3, True) for i in range(4)] + \
+    [("coverage.mag", 2, 1e-3, False), ("coverage.mag_fpi", 2, 1e-3, False)]
+
+
+def _check_minimal_outputs(out_dir, res):
+    gold = os.path.join(GOLDEN, "minimal", "inv")
+    for f, col, tol, rel in MINIMAL_FILES:
+        a, b = _table(os.path.join(out_dir, f)), _table(os.path.join(gold, f))
+        assert a.shape == b.shape, f
+        # coordinates and the integer columns exactly
+        if f.startswith("volt"):
+            np.testing.assert_array_equal(a[:, [0, 1, 4]], b[:, [0, 1, 4]])
+        elif not f.endswith(".modl"):
+            np.testing.assert_allclose(a[:, :2], b[:, :2], rtol=0, atol=1e-6)
+        d = np.abs(a[:, col] - b[:, col])
+        lim = tol * (np.abs(b[:, col]) if rel else 1.0) + (5e-4 if rel else 0.0)
+        assert np.all(d <= lim), (f, float(d.max()))
+    # the written inv.ctr reads back as the run's rows
+    back = read_inv_ctr_trajectory(os.path.join(out_dir, "inv.ctr"))
+    assert compare_trajectory(res["rows"], back, slack=1.01) == []
+    assert [g["kind"] for g in back if g["kind"] == "RESET"] == ["RESET"]
+
+
+def test_gn_loop_minimal_outputs_oracle(tmp_path):
+    """wout (rhoNN.mag / .pha / .modl, voltNN.dat at IT 0, 1, 2, the switch
+    to the phase improvement and the end), bbsens (coverage.mag and
+    coverage.mag_fpi) and inv.ctr of the minimal inversion against the
+    recorded files."""
+    inv = _setup("minimal", _oracle_ctx)
+    res = inv.run(out_dir=str(tmp_path))
+    _check_minimal_outputs(str(tmp_path), res)
+
+
+@pytest.mark.gpu
+def test_gn_loop_minimal_outputs_device(tmp_path):
+    """The same files from the device path, coverage from crt_coverage."""
+    inv = _setup("minimal")
+    res = inv.run(out_dir=str(tmp_path))
+    _check_minimal_outputs(str(tmp_path), res)
+    inv.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["complex", "fpi", "dc"])
+def test_coverage_device_matches_numpy(mode):
+    """crt_coverage against the column sums of the copied Jacobian, with the
+    caller's weights and with the default sqrt(wmatd wdfak)."""
+    inv = _setup("minimal")
+    d = inv.data
+    ldc = mode == "dc"
+    sig = inv.start_model() * np.exp(0.4 * np.cos(np.arange(inv.manz)) + 0.2j * np.sin(np.arange(inv.manz)) * (not ldc))
+    inv.ctx.forward(sig, ldc=ldc)
+    wdfak = (np.arange(len(d.dat)) % 4 != 1).astype(np.int32)
+    inv.ctx.set_data(d.dat, d.wmatd, wdfak)
+    J = inv.ctx.jacobian(mode=1 if ldc else 0, copy=True)
+    part = 1 if mode == "fpi" else 0
+    a = np.abs(J.real) if part else np.abs(J)
+    w = np.linspace(0.5, 2.0, len(d.dat))
+    np.testing.assert_allclose(inv.ctx.coverage(part, w), (a * w[:, None]).sum(0), rtol=1e-12)
+    w0 = np.sqrt(d.wmatd * wdfak)
+    np.testing.assert_allclose(inv.ctx.coverage(part), (a * w0[:, None]).sum(0), rtol=1e-12)
     inv.close()

@@ -608,3 +608,46 @@ def test_mixed_form_default_refinement_on_the_benchmark_mesh():
     ev = (np.abs(v - v64) / np.abs(v64)).max()
     print(f"\nC5 default refinement: potentials {ek:.1e} of max, voltages {ev:.1e} per reading")
     assert ek <= 1e-6 and ev <= 1e-6
+
+
+@pytest.mark.gpu
+def test_crmod_driver_writes_sensitivity_and_potential_files(tmp_path):
+    """CRMod with potentials and sensitivities switched on: one wsens file
+    per reading (|sum_j J_ij|, phase, then x, y, Re, Im per cell) and one
+    wpot file per reading (the current dipole's potential per node), both
+    against the oracle's bsens / rtrafo."""
+    import os
+    import shutil
+    from crtomo_stable_b200 import crmod, io
+    from oracle.oracle import OracleProblem
+    src = os.path.join(os.path.dirname(__file__), "golden", "minimal")
+    dst = tmp_path / "td"
+    shutil.copytree(src, dst)
+    d = io.read_volt(os.path.join(src, "mod", "volt.dat"))
+    os.makedirs(dst / "config", exist_ok=True)
+    io.write_config(str(dst / "config" / "config.dat"), d.strnr, d.vnr)
+    cfg = (dst / "exe" / "crmod.cfg").read_text().splitlines()
+    cfg[5] = "T                ! potentials ?"
+    cfg[9] = "T               ! sensitivities ?"
+    (dst / "exe" / "crmod.cfg").write_text("\n".join(cfg) + "\n")
+    out = crmod.run(str(dst / "exe"), verbose=False)
+    n = len(d.strnr)
+    assert len(out["sens"]) == n and len(out["pot"]) == n
+    assert os.path.basename(out["sens"][0]) == "sens01.dat" and os.path.basename(out["pot"][11]) == "pot12.dat"
+    case = load_forward_case("minimal")
+    op = OracleProblem(case["mesh"], case["enr"], d.strnr, d.vnr)
+    kp = op.forward(case["sigma"])
+    J = op.bsens(kp)
+    hp = op.rtrafo(kp)
+    for i in (0, 5, n - 1):
+        with open(out["sens"][i]) as fh:
+            rows = [[float(x) for x in ln.split()] for ln in fh if ln.strip()]
+        s = J[i].sum()
+        assert abs(rows[0][0] / abs(s) - 1) < 1e-6
+        got = np.array(rows[1:])
+        np.testing.assert_allclose(got[:, 2] + 1j * got[:, 3], J[i], rtol=1e-6, atol=1e-6 * np.abs(J[i]).max())
+        e1, e2 = int(d.strnr[i]) % 10000, int(d.strnr[i]) // 10000
+        ref = hp[:, e2 - 1] - hp[:, e1 - 1]
+        with open(out["pot"][i]) as fh:
+            pv = np.array([[float(x) for x in ln.split()] for ln in fh if ln.strip()])
+        np.testing.assert_allclose(pv[:, 2] + 1j * pv[:, 3], ref, rtol=1e-6, atol=1e-6 * np.abs(ref).max())
