@@ -24,6 +24,9 @@
 //   k_schur_out_gam p_G into kpot at the boundary nodes.
 #include "crt_schur.h"
 
+#include <cstdlib>
+#include <cstring>
+
 #include <algorithm>
 #include <cstdio>
 #include <numeric>
@@ -454,11 +457,15 @@ __global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __rest
 // L y = r_G - C[l] rides along each column, the back solve L^T x = y goes
 // panel by panel from the last (dot products of the panel columns, then the
 // panel's triangle on one warp).
-template <typename T, int NT, int NB>
-__global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A, const T* __restrict__ C, T* Sws,
-                                                      T* xg, int sys0)
+//
+// PF: the next super-tile's entries are loaded into registers while the
+// current one is updated (one CTA per SM); without, two CTAs share an SM and
+// hide each other's latency.
+template <typename T, int NT, int NB, bool PF>
+__global__ void __launch_bounds__(NT, PF ? 1 : 2) k_schur_chol(SchurArgs s, BandArgs<T> A, const T* __restrict__ C,
+                                                               T* Sws, T* xg, int sys0)
 {
-    static_assert(NT == 256 && NB == 16, "chol layout");
+    static_assert(NT == 256 && NB <= 16, "chol layout");
     extern __shared__ __align__(16) unsigned char ch_dyn[];
     const int m = s.m;
     T* P = reinterpret_cast<T*>(ch_dyn);   // panel [NB][m]: P[t m + r] = L(r, p0 + t)
@@ -549,7 +556,7 @@ __global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A
             T cur[4][4], nxt[4][4];
             st_load(0, cur);
             for (int st = 0; st < nst; ++st) {
-                if (st + 1 < nst) st_load(st + 1, nxt);
+                if (PF && st + 1 < nst) st_load(st + 1, nxt);
                 int R0, C0;
                 st_origin(st, R0, C0);
                 for (int t = 0; t < nb; ++t) {
@@ -571,8 +578,9 @@ __global__ void __launch_bounds__(NT, 1) k_schur_chol(SchurArgs s, BandArgs<T> A
                     for (int c = 0; c < 4; ++c) {
                         const int r = R0 + ti + 16 * a, cc = C0 + tj + 16 * c;
                         if (r < m && cc < m && r >= cc) S[(size_t)cc * m + r] = cur[a][c];
-                        cur[a][c] = nxt[a][c];
+                        if (PF) cur[a][c] = nxt[a][c];
                     }
+                if (!PF && st + 1 < nst) st_load(st + 1, cur);
             }
         }
         __syncthreads();
@@ -732,11 +740,24 @@ template <typename T>
 void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* C, T* Sws, T* xg, int sys0, int nsys,
                        cudaStream_t st)
 {
-    constexpr int NT = 256, NB = 16;
-    const size_t smem = ((size_t)NB * s.m + s.m) * sizeof(T);
-    auto kern = k_schur_chol<T, NT, NB>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kern<<<nsys, NT, smem, st>>>(s, full, C, Sws, xg, sys0);
+    // one CTA per SM with 16-column panels and the register prefetch, or two
+    // CTAs per SM with 12-column panels where two such panels fit
+    // (CRT_B200_SCHUR_CHOL=1 / 2 forces the form)
+    constexpr int NT = 256;
+    const size_t smem16 = ((size_t)16 * s.m + s.m) * sizeof(T), smem12 = ((size_t)12 * s.m + s.m) * sizeof(T);
+    const char* ev = std::getenv("CRT_B200_SCHUR_CHOL");
+    bool two = 2 * (smem12 + 1024) <= 227 * 1024;
+    if (ev && std::strcmp(ev, "1") == 0) two = false;
+    if (ev && std::strcmp(ev, "2") == 0 && 2 * (smem12 + 1024) <= 227 * 1024) two = true;
+    if (two) {
+        auto kern = k_schur_chol<T, NT, 12, false>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem12);
+        kern<<<nsys, NT, smem12, st>>>(s, full, C, Sws, xg, sys0);
+    } else {
+        auto kern = k_schur_chol<T, NT, 16, true>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem16);
+        kern<<<nsys, NT, smem16, st>>>(s, full, C, Sws, xg, sys0);
+    }
 }
 
 template <typename T>

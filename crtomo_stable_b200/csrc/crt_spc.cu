@@ -24,6 +24,9 @@
 #include "crt_spc.h"
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <type_traits>
 #include <utility>
 #include <vector>
@@ -189,8 +192,14 @@ __global__ void k_spc_entries(const int4* __restrict__ ent, int nent, const doub
 // Gauss-Jordan inversion publishes row and column k through double-buffered
 // vectors (one barrier per step).  FT_{q+1} is copied into the other half of
 // a shared double buffer by cp.async while block q is formed and inverted.
+//
+// With segs, CTA b runs the recurrence over the blocks segs[b].x ..
+// segs[b].y only (a segment's interior, its first block without coupling);
+// without, over 0 .. nb-1.  A non-positive pivot is reported through flag
+// (zeroed by the caller).
 template <int NB>
-__global__ void __launch_bounds__(16 * NB * NB, 1) k_spc_factor_v(float* DF, float* H, int nb, int* flag)
+__global__ void __launch_bounds__(16 * NB * NB, 1) k_spc_factor_v(float* DF, float* H, int nb, int* flag,
+                                                                   const int2* __restrict__ segs)
 {
     constexpr int B = 32 * NB, TPR = B / 8, NT = TPR * TPR, HB = B / 2;
     extern __shared__ __align__(16) float smem[];
@@ -229,14 +238,16 @@ __global__ void __launch_bounds__(16 * NB * NB, 1) k_spc_factor_v(float* DF, flo
         *reinterpret_cast<float4*>(row + HB + c0) = make_float4(v[4], v[5], v[6], v[7]);
     };
     int first_bad = 0;
-    if (nb > 1) stage_ft(1);
-    for (int q = 0; q < nb; ++q) {
+    const int2 sg = segs ? segs[blockIdx.x] : make_int2(0, nb - 1);
+    const int qs = sg.x, qe = sg.y;
+    if (qe > qs) stage_ft(qs + 1);
+    for (int q = qs; q <= qe; ++q) {
         float* Dq = DF + (size_t)q * BB;
         float t[8][8];
 #pragma unroll
         for (int a = 0; a < 8; ++a) ld_cols(Dq + (size_t)(r0 + a) * B, t[a]);
-        if (q > 0) {
-            if (q + 1 < nb) {
+        if (q > qs) {
+            if (q + 1 <= qe) {
                 stage_ft(q + 1);            // the half of FT_{q-1}, long since read
                 cp_async_wait_group<1>();   // FT_q has landed
             } else {
@@ -338,7 +349,7 @@ __global__ void __launch_bounds__(16 * NB * NB, 1) k_spc_factor_v(float* DF, flo
             st_cols(X + (r0 + a) * B, t[a]);
         }
     }
-    if (tid == 0) *flag = first_bad;
+    if (first_bad && tid == 0) atomicExch(flag, first_bad);
 }
 
 // One CTA: the sequential block recurrence, for B > 128 (every thread owns
@@ -613,10 +624,15 @@ __device__ __forceinline__ void load_run(const float* __restrict__ p, float (&d)
     }
 }
 
+//
+// With segs, CTA b sweeps the blocks segs[b].x .. segs[b].y of h in place
+// (a segment's interior); with perm, the result is scattered to z in element
+// order (the single chain).
 template <int NB>
 __global__ void __launch_bounds__(SW_NT, 1) k_spc_sweep(const float* __restrict__ Gm, const float* __restrict__ Hm,
                                                        const int* __restrict__ perm, cf* h, cd* __restrict__ z,
-                                                       int nb, const CGState* __restrict__ st)
+                                                       int nb, const CGState* __restrict__ st,
+                                                       const int2* __restrict__ segs)
 {
     constexpr int B = 32 * NB, CPW = B / SW_G;   // columns per warp
     __shared__ cf v[B];
@@ -665,42 +681,45 @@ __global__ void __launch_bounds__(SW_NT, 1) k_spc_sweep(const float* __restrict_
         }
         __syncthreads();
     };
-    if (tid < B) v[tid] = h[tid];
+    const int2 sg = segs ? segs[blockIdx.x] : make_int2(0, nb - 1);
+    const int qs = sg.x, qe = sg.y;
+    if (tid < B) v[tid] = h[(size_t)qs * B + tid];
     // forward: h_q = u_q - G_q h_{q-1}
-    if (nb > 1) {
-        load_blk(Gm + BB, mn);
-        if (tid < B) un = h[B + tid];
+    if (qe > qs) {
+        load_blk(Gm + (size_t)(qs + 1) * BB, mn);
+        if (tid < B) un = h[(size_t)(qs + 1) * B + tid];
     }
     __syncthreads();
-    for (int q = 1; q < nb; ++q) {
+    for (int q = qs + 1; q <= qe; ++q) {
         const cf u = un;
 #pragma unroll
         for (int j = 0; j < CPW; ++j)
 #pragma unroll
             for (int i = 0; i < NB; ++i) m[j][i] = mn[j][i];
-        if (q + 1 < nb) {
+        if (q + 1 <= qe) {
             load_blk(Gm + (size_t)(q + 1) * BB, mn);
             if (tid < B) un = h[(size_t)(q + 1) * B + tid];
         }
         step(q, u);
     }
-    // backward: x_q = h_q - H_q x_{q+1}; v holds x_{nb-1} = h_{nb-1}
-    if (nb > 1) {
-        load_blk(Hm + (size_t)(nb - 2) * BB, mn);
-        if (tid < B) un = h[(size_t)(nb - 2) * B + tid];
+    // backward: x_q = h_q - H_q x_{q+1}; v holds x_qe = h_qe
+    if (qe > qs) {
+        load_blk(Hm + (size_t)(qe - 1) * BB, mn);
+        if (tid < B) un = h[(size_t)(qe - 1) * B + tid];
     }
-    for (int q = nb - 2; q >= 0; --q) {
+    for (int q = qe - 1; q >= qs; --q) {
         const cf u = un;
 #pragma unroll
         for (int j = 0; j < CPW; ++j)
 #pragma unroll
             for (int i = 0; i < NB; ++i) m[j][i] = mn[j][i];
-        if (q > 0) {
+        if (q > qs) {
             load_blk(Hm + (size_t)(q - 1) * BB, mn);
             if (tid < B) un = h[(size_t)(q - 1) * B + tid];
         }
         step(q, u);
     }
+    if (!perm) return;
     for (int pos = tid; pos < nb * B; pos += SW_NT) {
         const int e = perm[pos];
         if (e >= 0) {
@@ -708,6 +727,326 @@ __global__ void __launch_bounds__(SW_NT, 1) k_spc_sweep(const float* __restrict_
             z[e] = cd{(double)x.x, (double)x.y};
         }
     }
+}
+
+// ---------------------------------------------------------------------------
+// Segmented form: block products on one CTA of (B/8)^2 threads, the layout of
+// k_spc_factor_v (thread (ty, tx): rows 8 ty .. 8 ty + 7, column quads
+// 4 tx .. and B/2 + 4 tx ..).  Operands are staged in shared memory as k-rows,
+// At[k][r] = A[r][k] and Bk[k][c] = B[k][c], with the row stride B + 4.
+template <int NB>
+struct BlkMM {
+    static constexpr int B = 32 * NB, TPR = B / 8, NT = TPR * TPR, HB = B / 2, LDS = B + 4;
+    int tid, r0, c0;
+    __device__ BlkMM() : tid(threadIdx.x), r0(8 * (threadIdx.x / TPR)), c0(4 * (threadIdx.x % TPR)) {}
+    __device__ int col(int b) const { return (b >> 2) * HB + c0 + (b & 3); }
+    // dst[k][j] = src[k][j] (src row-major B x B in global memory)
+    __device__ void stage(float* dst, const float* __restrict__ src) const
+    {
+        for (int i = tid; i < B * B / 4; i += NT) {
+            const int k = (4 * i) / B, j = (4 * i) % B;
+            cp_async16(dst + k * LDS + j, src + 4 * (size_t)i);
+        }
+        cp_async_commit();
+    }
+    // dst[k][j] = src[j][k]
+    __device__ void stage_t(float* dst, const float* __restrict__ src) const
+    {
+        for (int i = tid; i < B * B; i += NT) {
+            const int j = i / B, k = i % B;
+            dst[k * LDS + j] = src[i];
+        }
+    }
+    // acc (+)= sum_k At[k][r] Bk[k][c]
+    __device__ void mma(const float* At, const float* Bk, float (&acc)[8][8]) const
+    {
+#pragma unroll 2
+        for (int k = 0; k < B; ++k) {
+            const float4 a0 = *reinterpret_cast<const float4*>(At + k * LDS + r0);
+            const float4 a1 = *reinterpret_cast<const float4*>(At + k * LDS + r0 + 4);
+            const float4 b0 = *reinterpret_cast<const float4*>(Bk + k * LDS + c0);
+            const float4 b1 = *reinterpret_cast<const float4*>(Bk + k * LDS + HB + c0);
+            const float xa[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+            const float xb[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) acc[a][b] = fmaf(xa[a], xb[b], acc[a][b]);
+        }
+    }
+    __device__ void zero(float (&acc)[8][8]) const
+    {
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+#pragma unroll
+            for (int b = 0; b < 8; ++b) acc[a][b] = 0.0f;
+    }
+    // C row-major in global memory (ld B): load / store this thread's entries
+    __device__ void load(const float* __restrict__ C, float (&v)[8][8]) const
+    {
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const float4 x = *reinterpret_cast<const float4*>(C + (size_t)(r0 + a) * B + c0);
+            const float4 y = *reinterpret_cast<const float4*>(C + (size_t)(r0 + a) * B + HB + c0);
+            v[a][0] = x.x; v[a][1] = x.y; v[a][2] = x.z; v[a][3] = x.w;
+            v[a][4] = y.x; v[a][5] = y.y; v[a][6] = y.z; v[a][7] = y.w;
+        }
+    }
+    __device__ void store(float* C, const float (&v)[8][8]) const
+    {
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            *reinterpret_cast<float4*>(C + (size_t)(r0 + a) * B + c0) = make_float4(v[a][0], v[a][1], v[a][2], v[a][3]);
+            *reinterpret_cast<float4*>(C + (size_t)(r0 + a) * B + HB + c0) = make_float4(v[a][4], v[a][5], v[a][6], v[a][7]);
+        }
+    }
+    // into shared memory as k-rows (row stride LDS) for the next product
+    __device__ void store_s(float* Cs, const float (&v)[8][8]) const
+    {
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            *reinterpret_cast<float4*>(Cs + (r0 + a) * LDS + c0) = make_float4(v[a][0], v[a][1], v[a][2], v[a][3]);
+            *reinterpret_cast<float4*>(Cs + (r0 + a) * LDS + HB + c0) = make_float4(v[a][4], v[a][5], v[a][6], v[a][7]);
+        }
+    }
+    // C^T row-major in global memory (the F^T layout of DF)
+    __device__ void store_t(float* C, const float (&v)[8][8]) const
+    {
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            float* p = C + (size_t)col(b) * B + r0;
+            *reinterpret_cast<float4*>(p) = make_float4(v[0][b], v[1][b], v[2][b], v[3][b]);
+            *reinterpret_cast<float4*>(p + 4) = make_float4(v[4][b], v[5][b], v[6][b], v[7][b]);
+        }
+    }
+};
+
+template <int NB>
+constexpr size_t spike_smem() { return sizeof(float) * 2 * (size_t)(32 * NB) * (32 * NB + 4); }
+
+// The spikes of segment p (CTA 2p: V_p, CTA 2p + 1: W_p), from the segment
+// factor (T_q^-1 in DF, G and H column-major):
+//   V: X_s = T_s^-1 F_s, X_q = -G_q X_{q-1};  V[ie] = X_ie, V[q] = X_q - H_q V[q+1]
+//   W: W[ie] = T_ie^-1 F_e^T,  W[q] = -H_q W[q+1]
+// (s, ie the segment's first and last interior blocks, e its separator).
+template <int NB>
+__global__ void __launch_bounds__(16 * NB * NB, 1) k_spc_spike(const float* __restrict__ DF, const float* __restrict__ Gm,
+                                                              const float* __restrict__ Hm, const int2* __restrict__ segs,
+                                                              int nseg, int nb, float* V, float* W)
+{
+    using M = BlkMM<NB>;
+    constexpr int B = M::B, LDS = M::LDS;
+    extern __shared__ __align__(16) float smem[];
+    float* At = smem;
+    float* Bk = smem + B * LDS;
+    const M mm;
+    const int p = blockIdx.x >> 1, right = blockIdx.x & 1;
+    if (right ? p >= nseg - 1 : p == 0) return;
+    const int s = segs[p].x, ie = segs[p].y;
+    const size_t BB = (size_t)B * B;
+    const float* FT = DF + (size_t)nb * BB;
+    float acc[8][8];
+    if (!right) {
+        // X_s = T_s^-1 F_s: At = T_s^-1 (symmetric), Bk[k][c] = F_s[k][c] = FT_s[c][k]
+        mm.stage(At, DF + (size_t)s * BB);
+        mm.stage_t(Bk, FT + (size_t)s * BB);
+        cp_async_wait_all();
+        __syncthreads();
+        mm.zero(acc);
+        mm.mma(At, Bk, acc);
+        mm.store(V + (size_t)s * BB, acc);
+        for (int q = s + 1; q <= ie; ++q) {
+            __syncthreads();                       // At / Bk of the last product are consumed
+            mm.store_s(Bk, acc);                   // X_{q-1}
+            mm.stage(At, Gm + (size_t)q * BB);     // At[k][r] = G_q[r][k] = GT_q[k][r]
+            cp_async_wait_all();
+            __syncthreads();
+            mm.zero(acc);
+            mm.mma(At, Bk, acc);
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) acc[a][b] = -acc[a][b];
+            mm.store(V + (size_t)q * BB, acc);
+        }
+        // back: acc holds V[ie] = X_ie
+        for (int q = ie - 1; q >= s; --q) {
+            __syncthreads();
+            mm.store_s(Bk, acc);                   // V[q+1]
+            mm.stage(At, Hm + (size_t)q * BB);     // At[k][r] = H_q[r][k] = HT_q[k][r]
+            cp_async_wait_all();
+            __syncthreads();
+            float x[8][8];
+            mm.load(V + (size_t)q * BB, x);        // X_q
+            mm.zero(acc);
+            mm.mma(At, Bk, acc);
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) acc[a][b] = x[a][b] - acc[a][b];
+            mm.store(V + (size_t)q * BB, acc);
+        }
+    } else {
+        const int e = ie + 1;
+        // W[ie] = T_ie^-1 F_e^T: Bk[k][c] = F_e^T[k][c] = FT_e[k][c]
+        mm.stage(At, DF + (size_t)ie * BB);
+        mm.stage(Bk, FT + (size_t)e * BB);
+        cp_async_wait_all();
+        __syncthreads();
+        mm.zero(acc);
+        mm.mma(At, Bk, acc);
+        mm.store(W + (size_t)ie * BB, acc);
+        for (int q = ie - 1; q >= s; --q) {
+            __syncthreads();
+            mm.store_s(Bk, acc);                   // W[q+1]
+            mm.stage(At, Hm + (size_t)q * BB);
+            cp_async_wait_all();
+            __syncthreads();
+            mm.zero(acc);
+            mm.mma(At, Bk, acc);
+#pragma unroll
+            for (int a = 0; a < 8; ++a)
+#pragma unroll
+                for (int b = 0; b < 8; ++b) acc[a][b] = -acc[a][b];
+            mm.store(W + (size_t)q * BB, acc);
+        }
+    }
+}
+
+// The separators' Schur complement, one CTA per separator p (block e):
+//   Sd_p = D_e - F_e W[e-1] - F_{e+1}^T V[e+1]     -> DFc[p]       (row-major)
+//   So_p = -F_e V[e-1]  (p >= 1)                   -> DFc[nc + p]  as So_p^T
+template <int NB>
+__global__ void __launch_bounds__(16 * NB * NB, 1) k_spc_reduced(const float* __restrict__ DF,
+                                                                const float* __restrict__ V,
+                                                                const float* __restrict__ W,
+                                                                const int* __restrict__ sep, int nc, int nb,
+                                                                float* DFc)
+{
+    using M = BlkMM<NB>;
+    constexpr int B = M::B, LDS = M::LDS;
+    extern __shared__ __align__(16) float smem[];
+    float* At = smem;
+    float* Bk = smem + B * LDS;
+    const M mm;
+    const int p = blockIdx.x, e = sep[p];
+    const size_t BB = (size_t)B * B;
+    const float* FT = DF + (size_t)nb * BB;
+    float acc[8][8], d[8][8];
+    mm.load(DF + (size_t)e * BB, d);                    // D_e (the segment factors leave it)
+    // F_e W[e-1]: At[k][r] = F_e[r][k] = FT_e[k][r]
+    mm.stage(At, FT + (size_t)e * BB);
+    mm.stage(Bk, W + (size_t)(e - 1) * BB);
+    cp_async_wait_all();
+    __syncthreads();
+    mm.zero(acc);
+    mm.mma(At, Bk, acc);
+    __syncthreads();
+    // F_{e+1}^T V[e+1]: At[k][r] = F_{e+1}[k][r] = FT_{e+1}[r][k]
+    mm.stage_t(At, FT + (size_t)(e + 1) * BB);
+    mm.stage(Bk, V + (size_t)(e + 1) * BB);
+    cp_async_wait_all();
+    __syncthreads();
+    mm.mma(At, Bk, acc);
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) d[a][b] -= acc[a][b];
+    mm.store(DFc + (size_t)p * BB, d);
+    if (p == 0) return;
+    __syncthreads();
+    // So_p = -F_e V[e-1]
+    mm.stage(At, FT + (size_t)e * BB);
+    mm.stage(Bk, V + (size_t)(e - 1) * BB);
+    cp_async_wait_all();
+    __syncthreads();
+    mm.zero(acc);
+    mm.mma(At, Bk, acc);
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = -acc[a][b];
+    mm.store_t(DFc + (size_t)(nc + p) * BB, acc);
+}
+
+// Separators' right-hand sides and their first step, one CTA (B threads) per
+// separator p (block e):  g = r_e - F_e y[e-1] - F_{e+1}^T y[e+1],
+// hc_p = Tc_p^-1 g  (Tc_p^-1 symmetric, in DFc[p] after the reduced factor).
+template <int NB>
+__global__ void __launch_bounds__(32 * NB) k_spc_sep_rhs(const float* __restrict__ DF, const float* __restrict__ DFc,
+                                                        const int* __restrict__ sep, const int* __restrict__ perm,
+                                                        const cd* __restrict__ r, const cf* __restrict__ h,
+                                                        cf* __restrict__ hc, int nb, const CGState* __restrict__ st)
+{
+    constexpr int B = 32 * NB;
+    __shared__ cf yl[B], yr[B], g[B];
+    if (st->done) return;
+    const int p = blockIdx.x, e = sep[p], t = threadIdx.x;
+    const size_t BB = (size_t)B * B;
+    const float* FTe = DF + (size_t)nb * BB + (size_t)e * BB;
+    const float* FTn = DF + (size_t)nb * BB + (size_t)(e + 1) * BB;
+    yl[t] = h[(size_t)(e - 1) * B + t];
+    yr[t] = h[(size_t)(e + 1) * B + t];
+    const int el = perm[(size_t)e * B + t];
+    const cd rv = el >= 0 ? r[el] : cd{0.0, 0.0};
+    __syncthreads();
+    float sx = (float)rv.x, sy = (float)rv.y;
+    for (int k = 0; k < B; ++k) {
+        // (F_e y)_t = sum_k FT_e[k][t] y_k ;  (F_{e+1}^T y)_t = sum_k FT_{e+1}[t][k] y_k
+        const float a = FTe[(size_t)k * B + t], b = FTn[(size_t)t * B + k];
+        sx -= a * yl[k].x + b * yr[k].x;
+        sy -= a * yl[k].y + b * yr[k].y;
+    }
+    g[t] = cf{sx, sy};
+    __syncthreads();
+    const float* Tc = DFc + (size_t)p * BB;
+    float ux = 0.0f, uy = 0.0f;
+    for (int k = 0; k < B; ++k) {
+        const float m = Tc[(size_t)k * B + t];
+        ux = fmaf(m, g[k].x, ux);
+        uy = fmaf(m, g[k].y, uy);
+    }
+    hc[(size_t)p * B + t] = cf{ux, uy};
+}
+
+// x_q = y_q - V[q] x_{c_{p-1}} - W[q] x_{c_p} for the interior blocks of
+// segment p, x = xc_p for separator p; scattered to z in element order.  One
+// CTA (B threads) per block.
+template <int NB>
+__global__ void __launch_bounds__(32 * NB) k_spc_correct(const float* __restrict__ V, const float* __restrict__ W,
+                                                        const int* __restrict__ bseg, const int* __restrict__ perm,
+                                                        const cf* __restrict__ h, const cf* __restrict__ hc,
+                                                        cd* __restrict__ z, int nseg, const CGState* __restrict__ st)
+{
+    constexpr int B = 32 * NB;
+    __shared__ cf xl[B], xr[B];
+    if (st->done) return;
+    const int q = blockIdx.x, t = threadIdx.x, sp = bseg[q];
+    const size_t BB = (size_t)B * B;
+    cf x;
+    if (sp < 0) {
+        x = hc[(size_t)(-1 - sp) * B + t];
+    } else {
+        const bool left = sp > 0, rightc = sp < nseg - 1;
+        xl[t] = left ? hc[(size_t)(sp - 1) * B + t] : cf{0.0f, 0.0f};
+        xr[t] = rightc ? hc[(size_t)sp * B + t] : cf{0.0f, 0.0f};
+        __syncthreads();
+        x = h[(size_t)q * B + t];
+        const float* Vq = V + (size_t)q * BB + (size_t)t * B;
+        const float* Wq = W + (size_t)q * BB + (size_t)t * B;
+        if (left)
+            for (int k = 0; k < B; ++k) {
+                x.x -= Vq[k] * xl[k].x;
+                x.y -= Vq[k] * xl[k].y;
+            }
+        if (rightc)
+            for (int k = 0; k < B; ++k) {
+                x.x -= Wq[k] * xr[k].x;
+                x.y -= Wq[k] * xr[k].y;
+            }
+    }
+    const int el = perm[(size_t)q * B + t];
+    if (el >= 0) z[el] = cd{(double)x.x, (double)x.y};
 }
 
 size_t factor_smem(int B) { return sizeof(float) * ((size_t)B * (B + 1) + 32 * (B + 1) + 4 * B); }
@@ -719,15 +1058,31 @@ void factor_nb(const SpcPlan& P, cudaStream_t s)
 {
     const int B = 32 * NB;
     const size_t fs = factor_smem(B), gs = gmul_smem(B);
+    cudaMemsetAsync(P.d_flag, 0, sizeof(int), s);
+    cudaFuncSetAttribute(k_spc_gmul<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gs);
     if constexpr (NB <= 4) {
         const size_t vs = factor_v_smem(B);
         cudaFuncSetAttribute(k_spc_factor_v<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vs);
-        k_spc_factor_v<NB><<<1, 16 * NB * NB, vs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag);
+        if (P.nseg > 0) {
+            // segment interiors side by side, their spikes, the separators'
+            // Schur complement and its factor
+            constexpr size_t ss = spike_smem<NB>();
+            k_spc_factor_v<NB><<<P.nseg, 16 * NB * NB, vs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag, P.d_seg);
+            k_spc_gmul<NB><<<P.nb - 1, SPC_NT, gs, s>>>(P.d_DF, P.d_G, P.nb);
+            cudaFuncSetAttribute(k_spc_spike<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+            k_spc_spike<NB><<<2 * P.nseg, 16 * NB * NB, ss, s>>>(P.d_DF, P.d_G, P.d_H, P.d_seg, P.nseg, P.nb,
+                                                                  P.d_V, P.d_W);
+            cudaFuncSetAttribute(k_spc_reduced<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ss);
+            k_spc_reduced<NB><<<P.nc, 16 * NB * NB, ss, s>>>(P.d_DF, P.d_V, P.d_W, P.d_sep, P.nc, P.nb, P.d_DFc);
+            k_spc_factor_v<NB><<<1, 16 * NB * NB, vs, s>>>(P.d_DFc, P.d_Hc, P.nc, P.d_flag, nullptr);
+            if (P.nc > 1) k_spc_gmul<NB><<<P.nc - 1, SPC_NT, gs, s>>>(P.d_DFc, P.d_Gc, P.nc);
+            return;
+        }
+        k_spc_factor_v<NB><<<1, 16 * NB * NB, vs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag, nullptr);
     } else {
         cudaFuncSetAttribute(k_spc_factor<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs);
         k_spc_factor<NB><<<1, SPC_NT, fs, s>>>(P.d_DF, P.d_H, P.nb, P.d_flag);
     }
-    cudaFuncSetAttribute(k_spc_gmul<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gs);
     if (P.nb > 1) k_spc_gmul<NB><<<P.nb - 1, SPC_NT, gs, s>>>(P.d_DF, P.d_G, P.nb);
 }
 
@@ -735,7 +1090,16 @@ template <int NB>
 void apply_nb(const SpcPlan& P, const cd* r, cd* z, const CGState* st, cudaStream_t s)
 {
     k_spc_u<NB><<<P.nb, SPC_NT, 0, s>>>(P.d_DF, P.d_perm, r, P.d_h, st);
-    k_spc_sweep<NB><<<1, SW_NT, 0, s>>>(P.d_G, P.d_H, P.d_perm, P.d_h, z, P.nb, st);
+    if constexpr (NB <= 4) {
+        if (P.nseg > 0) {
+            k_spc_sweep<NB><<<P.nseg, SW_NT, 0, s>>>(P.d_G, P.d_H, nullptr, P.d_h, nullptr, P.nb, st, P.d_seg);
+            k_spc_sep_rhs<NB><<<P.nc, 32 * NB, 0, s>>>(P.d_DF, P.d_DFc, P.d_sep, P.d_perm, r, P.d_h, P.d_hc, P.nb, st);
+            k_spc_sweep<NB><<<1, SW_NT, 0, s>>>(P.d_Gc, P.d_Hc, nullptr, P.d_hc, nullptr, P.nc, st, nullptr);
+            k_spc_correct<NB><<<P.nb, 32 * NB, 0, s>>>(P.d_V, P.d_W, P.d_bseg, P.d_perm, P.d_h, P.d_hc, z, P.nseg, st);
+            return;
+        }
+    }
+    k_spc_sweep<NB><<<1, SW_NT, 0, s>>>(P.d_G, P.d_H, P.d_perm, P.d_h, z, P.nb, st, nullptr);
 }
 
 template <typename T>
@@ -743,6 +1107,51 @@ bool alloc(T** p, size_t n)
 {
     return cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)) == cudaSuccess;
 }
+
+// Segments of the chain: about sqrt(nb) of them (the sequential work per
+// application is ~ 2 nb / nseg + 2 nseg block steps), each of at least four
+// blocks; the last block of every segment but the last is a separator.
+void segment_layout(int nb, std::vector<int2>& seg, std::vector<int>& bseg, std::vector<int>& sep)
+{
+    int ns = (int)std::lround(std::sqrt((double)nb));
+    ns = std::max(2, std::min(ns, nb / 4));
+    seg.clear();
+    sep.clear();
+    bseg.assign(nb, 0);
+    for (int p = 0; p < ns; ++p) {
+        const int b0 = (int)((long long)nb * p / ns), b1 = (int)((long long)nb * (p + 1) / ns);   // [b0, b1)
+        const bool last = p == ns - 1;
+        const int ie = last ? b1 - 1 : b1 - 2;
+        seg.push_back(make_int2(b0, ie));
+        for (int q = b0; q <= ie; ++q) bseg[q] = p;
+        if (!last) {
+            sep.push_back(b1 - 1);
+            bseg[b1 - 1] = -1 - p;
+        }
+    }
+}
+
+// Device buffers of the segmented form that every factor owns (spikes and
+// the separators' system).
+bool alloc_seg_factor(SpcPlan& P)
+{
+    const size_t BB = (size_t)P.B * P.B;
+    return alloc(&P.d_V, P.nb * BB) && alloc(&P.d_W, P.nb * BB) && alloc(&P.d_DFc, 2 * (size_t)P.nc * BB) &&
+           alloc(&P.d_Gc, P.nc * BB) && alloc(&P.d_Hc, P.nc * BB) && alloc(&P.d_hc, (size_t)P.nc * P.B);
+}
+
+void free_seg_factor(SpcPlan& P)
+{
+    cudaFree(P.d_V);
+    cudaFree(P.d_W);
+    cudaFree(P.d_DFc);
+    cudaFree(P.d_Gc);
+    cudaFree(P.d_Hc);
+    cudaFree(P.d_hc);
+    P.d_V = P.d_W = P.d_DFc = P.d_Gc = P.d_Hc = nullptr;
+    P.d_hc = nullptr;
+}
+
 
 }  // namespace
 
@@ -862,6 +1271,28 @@ int spc_plan_build(SpcPlan& P, int M, int ltri, int nx, int nnb, const double* s
         spc_plan_free(P);
         return CRT_ERR_CUDA;
     }
+    // segmented form for B <= 128 and long chains (CRT_B200_SPC=single keeps
+    // the single chain)
+    const char* sv = std::getenv("CRT_B200_SPC");
+    const bool single = sv && std::strcmp(sv, "single") == 0;
+    if (!single && B <= 128 && P.nb >= 32) {
+        std::vector<int2> seg;
+        std::vector<int> bseg, sep;
+        segment_layout(P.nb, seg, bseg, sep);
+        P.nseg = (int)seg.size();
+        P.nc = (int)sep.size();
+        if (!alloc(&P.d_seg, seg.size()) || !alloc(&P.d_bseg, bseg.size()) || !alloc(&P.d_sep, sep.size()) ||
+            !alloc_seg_factor(P)) {
+            spc_plan_free(P);
+            return CRT_ERR_ALLOC;
+        }
+        if (cudaMemcpy(P.d_seg, seg.data(), seg.size() * sizeof(int2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(P.d_bseg, bseg.data(), bseg.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(P.d_sep, sep.data(), sep.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+            spc_plan_free(P);
+            return CRT_ERR_CUDA;
+        }
+    }
     P.ok = 1;
     return 0;
 }
@@ -875,6 +1306,10 @@ void spc_plan_free(SpcPlan& P)
     cudaFree(P.d_H);
     cudaFree(P.d_h);
     cudaFree(P.d_flag);
+    cudaFree(P.d_seg);
+    cudaFree(P.d_bseg);
+    cudaFree(P.d_sep);
+    free_seg_factor(P);
     P = SpcPlan{};
 }
 
@@ -882,15 +1317,18 @@ int spc_plan_clone(const SpcPlan& src, SpcPlan& dst)
 {
     spc_plan_free_clone(dst);
     if (!src.ok) return CRT_ERR_ARG;
-    dst = src;   // ordering, entry list and sizes are shared
+    dst = src;   // ordering, entry list, segment layout and sizes are shared
     dst.ok = 0;
     dst.d_DF = nullptr;
     dst.d_G = dst.d_H = nullptr;
     dst.d_h = nullptr;
     dst.d_flag = nullptr;
+    dst.d_V = dst.d_W = dst.d_DFc = dst.d_Gc = dst.d_Hc = nullptr;
+    dst.d_hc = nullptr;
     const size_t BB = (size_t)src.B * src.B;
     const bool ok = alloc(&dst.d_DF, 2 * src.nb * BB) && alloc(&dst.d_G, src.nb * BB) &&
-                    alloc(&dst.d_H, src.nb * BB) && alloc(&dst.d_h, src.Mp) && alloc(&dst.d_flag, 1);
+                    alloc(&dst.d_H, src.nb * BB) && alloc(&dst.d_h, src.Mp) && alloc(&dst.d_flag, 1) &&
+                    (src.nseg == 0 || alloc_seg_factor(dst));
     if (!ok) {
         spc_plan_free_clone(dst);
         return CRT_ERR_ALLOC;
@@ -906,6 +1344,7 @@ void spc_plan_free_clone(SpcPlan& P)
     cudaFree(P.d_H);
     cudaFree(P.d_h);
     cudaFree(P.d_flag);
+    free_seg_factor(P);
     P = SpcPlan{};
 }
 

@@ -23,6 +23,22 @@
 // The preconditioner is FP32 and therefore not exactly linear; the CG that
 // uses it takes the flexible (Polak-Ribiere) beta and keeps the reference's
 // stop rule on the true residual |r|^2 <= eps |r0|^2.
+//
+// Segmented form (B <= 128, nb >= 32): the block chain is cut into nseg
+// segments; the last block of each segment but the last is a separator.
+// The segments' interiors I_p are factored side by side (one CTA each), the
+// spikes V_p = A_Ip^-1 E_first F_{s_p} and W_p = A_Ip^-1 E_last F_{e_p}^T
+// are formed by chains of block products, and the separators' Schur
+// complement (block tridiagonal, nseg - 1 blocks)
+//     Sd_p = D_{e_p} - F_{e_p} W_p[e_p - 1] - F_{e_p+1}^T V_{p+1}[e_p + 1]
+//     So_p = - F_{e_p} V_p[e_p - 1]          (row c_p, column c_{p-1})
+// is factored by the same recurrence.  An application solves the interiors
+// side by side (y = A_I^-1 r_I), the separators from
+// g_p = r_{c_p} - F_{e_p} y[e_p - 1] - F_{e_p+1}^T y[e_p + 1], and corrects
+// the interiors, x_q = y_q - V_p[q] x_{c_{p-1}} - W_p[q] x_{c_p}, all blocks
+// in parallel.  The result is S^-1 r as for the single chain (another
+// elimination order, the same FP32 arithmetic per block); the sequential
+// chains shrink from nb block steps to about nb / nseg + nseg.
 #pragma once
 
 #include <string>
@@ -42,6 +58,17 @@ struct SpcPlan {
     float* d_H = nullptr;      // [nb][B][B]  T_q^-1 F_{q+1}^T (q < nb-1)
     cf* d_h = nullptr;         // [Mp] sweep vector
     int* d_flag = nullptr;     // [1] 0 ok, else 1 + block of the first non-positive pivot
+    // segmented form (nseg = 0: the single chain)
+    int nseg = 0, nc = 0;
+    int2* d_seg = nullptr;     // [nseg] first and last interior block of each segment (shared by clones)
+    int* d_bseg = nullptr;     // [nb] segment of an interior block, -(1 + p) for separator p (shared)
+    int* d_sep = nullptr;      // [nc] block of separator p (shared)
+    float* d_V = nullptr;      // [nb][B][B] row-major, left spikes (interior blocks of segments p >= 1)
+    float* d_W = nullptr;      // [nb][B][B] row-major, right spikes (segments p < nseg - 1)
+    float* d_DFc = nullptr;    // [2][nc][B][B] separators' Schur complement: Sd_p, So_p^T
+    float* d_Gc = nullptr;     // [nc][B][B] its G (column-major)
+    float* d_Hc = nullptr;     // [nc][B][B] its H (column-major)
+    cf* d_hc = nullptr;        // [nc B] separators' sweep vector
 };
 
 constexpr int SPC_MAX_B = 192;

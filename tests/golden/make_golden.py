@@ -26,9 +26,11 @@ CASES = {
         "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg",
         "exe/tmp.kfak"]),
     "mixed_surf": ("2.5D_mixed_surf/Reference", [
-        "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg"]),
+        "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg",
+        "exe/crtomo.cfg", "inv/rho04.mag", "inv/rho04.pha", "inv/volt04.dat", "inv/coverage.mag"]),
     "non_ordered": ("non-ordered_boundary_conditions/Reference", [
-        "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg"]),
+        "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg",
+        "exe/crtomo.cfg", "inv/rho04.mag", "inv/rho04.pha", "inv/volt04.dat", "inv/coverage.mag"]),
     "grid_decoupling": ("GridDecoupling/regular_grids/01_no_decoupling", [
         "grid/elem.dat", "grid/elec.dat", "rho/rho.dat", "mod/volt.dat", "exe/crmod.cfg",
         "config/config.dat"]),

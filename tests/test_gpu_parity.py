@@ -651,3 +651,52 @@ def test_crmod_driver_writes_sensitivity_and_potential_files(tmp_path):
         with open(out["pot"][i]) as fh:
             pv = np.array([[float(x) for x in ln.split()] for ln in fh if ln.strip()])
         np.testing.assert_allclose(pv[:, 2] + 1j * pv[:, 3], ref, rtol=1e-6, atol=1e-6 * np.abs(ref).max())
+
+
+def _five_point_cg_case(nx, nz, ldc=False, weight=1.0):
+    from crtomo_stable_b200 import regularization, synth
+    from crtomo_stable_b200.lib import Context
+    xs = np.arange(nx + 1, dtype=np.float64) - 10.0
+    depths = synth.graded_depths(nz, 0.4, 1.04)
+    mesh = synth.structured_mesh(xs, depths, triangles=False)
+    nel = 16
+    enr = synth.surface_electrodes(mesh, xs, np.arange(nel, dtype=np.float64), nz)
+    strnr, vnr = synth.encode(synth.dipole_dipole(nel, (1, 2), 6))
+    rng = np.random.default_rng(11)
+    sig = synth.sigma_from(np.exp(rng.uniform(np.log(20), np.log(200), mesh.elanz)), -rng.uniform(1, 20, mesh.elanz))
+    ctx = Context(mesh, enr, strnr, vnr)
+    _, sa = ctx.forward(sig, ldc=ldc)
+    dat = sa + 0.02 * rng.standard_normal(len(sa))
+    wmatd = np.full(len(sa), weight / 0.02 ** 2)
+    sig0 = np.full(mesh.elanz, np.exp(np.mean(np.log(sig))))
+    _, sa0 = ctx.forward(sig0, ldc=ldc)
+    ctx.jacobian(mode=1 if ldc else 0, copy=False)
+    ctx.set_regularizer(0, regularization.smatm_reg(mesh, nx, nz, 1.0, 1.0), nx=nx)
+    ctx.set_data(dat, wmatd)
+    return ctx, np.log(sig0), sa0, float(mesh.elanz), Context
+
+
+@pytest.mark.parametrize("nx,nz", [(30, 60), (60, 40)])
+def test_segmented_block_preconditioner_matches_single_chain(nx, nz, monkeypatch):
+    """Chains of 57 and 38 blocks (B = 32, 64) take the segmented form
+    (separators, spikes, the separators' Schur complement).  It applies the
+    same S^-1 as the single chain, so the block CG takes the same number of
+    iterations (+-1 for the FP32 rounding of another elimination order) and
+    gives the same update, at the usual lambda and at 100 times it (where
+    S^-1 is nearly the inverse of the CG operator)."""
+    from crtomo_stable_b200.lib import PRECOND_BLOCK
+    out = {}
+    for form in ("segmented", "single"):
+        if form == "single":
+            monkeypatch.setenv("CRT_B200_SPC", "single")
+        ctx, par, sa0, lam, Context = _five_point_cg_case(nx, nz)
+        for f in (1.0, 100.0):
+            got = ctx.update(Context.params(f * lam, eps=1e-12, ncgmax=3000, precond=PRECOND_BLOCK), par,
+                             sigmaa=sa0)
+            assert ctx.cg_info()[0] == PRECOND_BLOCK
+            out[form, f] = got
+        ctx.close()
+    for f in (1.0, 100.0):
+        a, b = out["segmented", f], out["single", f]
+        assert abs(a["ncg"] - b["ncg"]) <= 1, (f, a["ncg"], b["ncg"])
+        np.testing.assert_allclose(a["dpar"], b["dpar"], rtol=1e-5, atol=1e-5 * np.abs(b["dpar"]).max())
