@@ -620,8 +620,12 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
         for (int rel : mixed_rel)
             for (int q = 0; q < 2; ++q) gnodes.push_back(nrel0[(size_t)(m.elanz + rel) * m.maxnodes + q]);
         SchurHost& H = ctx->schur_h;
-        if (schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H) == CRT_OK &&
-            schur_sweep_smem<cd>(H.mbI, H.mbI + 1, SCHUR_MS_R) <= 227 * 1024 &&
+        // forward-sweep column blocks: 32 columns (one CTA per SM) or 16
+        // (two CTAs per SM; CRT_B200_SCHUR_R=16)
+        const char* rv = std::getenv("CRT_B200_SCHUR_R");
+        const int sweep_r = (rv && std::strcmp(rv, "16") == 0) ? 16 : SCHUR_MS_R;
+        if (schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H, sweep_r) == CRT_OK &&
+            schur_sweep_smem<cd>(H.mbI, H.mbI + 1, sweep_r) <= 227 * 1024 &&
             (size_t)(16 + 1) * H.m * sizeof(cd) <= 227 * 1024 && band_factor_smem<cd>(H.mbI + 1) <= 227 * 1024) {
             auto up = [&](int** d, const std::vector<int>& v) {
                 const std::vector<int> one(1, 0);
@@ -653,6 +657,7 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
             S.ncol = ctx->L + H.m;
             S.mbI = H.mbI;
             S.nblk = (int)H.blk_start.size();
+            S.R = H.R;
             S.ncpl = (int)H.gi_pos.size();
             S.ngg = (int)H.gg_ent.size();
             S.permI = p_permI;
@@ -1030,6 +1035,8 @@ int run_forward_schur(crt_ctx* ctx)
     T* Lrev = static_cast<T*>(ctx->d_sLrev);
     SchurArgs S = ctx->schur;
     S.WI = WI;
+    S.k0 = 0;
+    S.nk = K;
     S.status = ctx->d_status;
     // the full mesh's assembly data (entries of A_IG and A_GG(l))
     BandArgs<T> Af{};

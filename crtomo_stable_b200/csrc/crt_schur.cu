@@ -35,9 +35,10 @@
 // ---------------------------------------------------------------------------
 // Host plan.
 int schur_plan_host(const AssemblyLists& full, int n, const std::vector<int>& gamma_nodes,
-                    const std::vector<int>& enr0, int lsink, int nsink0, SchurHost& o)
+                    const std::vector<int>& enr0, int lsink, int nsink0, SchurHost& o, int R)
 {
     o = SchurHost{};
+    o.R = R;
     o.n = n;
     o.L = (int)enr0.size();
     std::vector<int> posI(n, -1), posG(n, -1);
@@ -123,7 +124,7 @@ int schur_plan_host(const AssemblyLists& full, int n, const std::vector<int>& ga
     o.col_order.resize(ncol);
     std::iota(o.col_order.begin(), o.col_order.end(), 0);
     std::stable_sort(o.col_order.begin(), o.col_order.end(), [&](int a, int b) { return first[a] < first[b]; });
-    for (int b0 = 0; b0 < ncol; b0 += SCHUR_MS_R) {
+    for (int b0 = 0; b0 < ncol; b0 += R) {
         const int f = first[o.col_order[b0]];
         o.blk_start.push_back(f >= o.nI ? o.nI : f / SCHUR_MS_BB * SCHUR_MS_BB);
     }
@@ -206,11 +207,11 @@ __global__ void k_schur_transpose(SchurArgs s, const T* __restrict__ Lws, T* Lre
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int n = s.nI, W = s.WI;
     const long long per = (long long)n * W;
-    if (idx >= (long long)s.K * per) return;
-    const int k = (int)(idx / per), cp = (int)((idx % per) / W), d = (int)(idx % W);
+    if (idx >= (long long)s.nk * per) return;
+    const int k = s.k0 + (int)(idx / per), cp = (int)((idx % per) / W), d = (int)(idx % W);
     const int r = n - 1 - cp, c = r - d;
     const T* Lk = Lws + (size_t)k * per;
-    Lrev[idx] = (c >= 0 && d <= s.mbI) ? Lk[(size_t)c * W + d] : Sc<T>::zero();
+    Lrev[(size_t)k * per + idx % per] = (c >= 0 && d <= s.mbI) ? Lk[(size_t)c * W + d] : Sc<T>::zero();
 }
 
 // ---------------------------------------------------------------------------
@@ -242,7 +243,7 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
     __shared__ __align__(8) unsigned long long bar[2];
     __shared__ int s_err;
     const int tid = threadIdx.x;
-    const int blk = blockIdx.x, k = blockIdx.y;
+    const int blk = blockIdx.x, k = s.k0 + blockIdx.y;
     const int start = back ? 0 : s.blk_start[blk];
     if (start >= n) return;   // every column of the block is zero, and so is its solution
     const T* Lk = Lws + (size_t)k * n * W;
@@ -395,7 +396,7 @@ __global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __rest
     __shared__ T As[TI][TG + 1];
     __shared__ T Bs[TI][TC + 1];
     __shared__ int s_i0;
-    const int tid = threadIdx.x, k = blockIdx.z;
+    const int tid = threadIdx.x, k = s.k0 + blockIdx.z;
     const int g0 = blockIdx.x * TG, c0 = blockIdx.y * TC;
     const int m = s.m, L = s.L, nI = s.nI, ncol = s.ncol;
     if (c0 >= L && c0 - L > g0 + TG - 1) return;
@@ -630,7 +631,7 @@ __global__ void __launch_bounds__(128) k_schur_zrebuild(SchurArgs s, T* X, const
     __shared__ T As[TG][TI + 1];
     __shared__ T Bs[TG][TL + 1];
     const int tid = threadIdx.x;
-    const int k = blockIdx.z, i0 = blockIdx.x * TI, l0 = blockIdx.y * TL;
+    const int k = s.k0 + blockIdx.z, i0 = blockIdx.x * TI, l0 = blockIdx.y * TL;
     const int ti = tid % 16, tl = tid / 16;
     const int m = s.m, nI = s.nI, L = s.L;
     T* Xk = X + (size_t)k * s.ncol * nI;
@@ -682,10 +683,10 @@ template <typename T>
 __global__ void k_schur_out_gam(SchurArgs s, const T* __restrict__ xg, int n, cd* kpot)
 {
     const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)s.K * s.L * s.m) return;
+    if (idx >= (long long)s.nk * s.L * s.m) return;
     const int g = (int)(idx % s.m);
-    const long long kl = idx / s.m;   // k L + l
-    kpot[kl * n + s.gam[g]] = Sc<T>::to_cd(xg[idx]);
+    const long long kl = (long long)s.k0 * s.L + idx / s.m;   // k L + l
+    kpot[kl * n + s.gam[g]] = Sc<T>::to_cd(xg[kl * s.m + g]);
 }
 
 // window rows: mb + 3 BB (the rows of a block, the band below it, and two
@@ -715,24 +716,30 @@ void launch_schur_rhs(const SchurArgs& s, const BandArgs<T>& full, const double*
 template <typename T>
 void launch_schur_transpose(const SchurArgs& s, const T* Lws, T* Lrev, cudaStream_t st)
 {
-    const long long tot = (long long)s.K * s.nI * s.WI;
+    const long long tot = (long long)s.nk * s.nI * s.WI;
     k_schur_transpose<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, Lws, Lrev);
 }
 
 template <typename T>
 void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t st)
 {
-    const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_MS_R);
-    auto kern = k_schur_sweep<T, SWEEP_NT, SCHUR_MS_R, SCHUR_MS_BB>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid(s.nblk, s.K);
-    kern<<<grid, SWEEP_NT, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+    const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, s.R);
+    dim3 grid(s.nblk, s.nk);
+    if (s.R == 16) {   // the back sweep's tiling: 4 x 4 tiles of a 129-row band at R = 16
+        auto kern = k_schur_sweep<T, 160, 16, SCHUR_MS_BB>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, 160, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+    } else {
+        auto kern = k_schur_sweep<T, SWEEP_NT, SCHUR_MS_R, SCHUR_MS_BB>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, SWEEP_NT, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+    }
 }
 
 template <typename T>
 void launch_schur_gram(const SchurArgs& s, const T* X, T* C, cudaStream_t st)
 {
-    dim3 grid((s.m + 63) / 64, (s.ncol + 31) / 32, s.K);
+    dim3 grid((s.m + 63) / 64, (s.ncol + 31) / 32, s.nk);
     k_schur_gram<T><<<grid, 128, 0, st>>>(s, X, C);
 }
 
@@ -763,7 +770,7 @@ void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* C, 
 template <typename T>
 void launch_schur_zrebuild(const SchurArgs& s, T* X, const T* xg, cudaStream_t st)
 {
-    dim3 grid((s.nI + 63) / 64, (s.L + 31) / 32, s.K);
+    dim3 grid((s.nI + 63) / 64, (s.L + 31) / 32, s.nk);
     k_schur_zrebuild<T><<<grid, 128, 0, st>>>(s, X, xg);
 }
 
@@ -775,9 +782,9 @@ void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, c
     const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_BK_R);
     auto kern = k_schur_sweep<T, NT, SCHUR_BK_R, SCHUR_MS_BB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((s.L + SCHUR_BK_R - 1) / SCHUR_BK_R, s.K);
+    dim3 grid((s.L + SCHUR_BK_R - 1) / SCHUR_BK_R, s.nk);
     kern<<<grid, NT, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);
-    const long long tot = (long long)s.K * s.L * s.m;
+    const long long tot = (long long)s.nk * s.L * s.m;
     k_schur_out_gam<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, xg, n, kpot);
 }
 

@@ -58,6 +58,7 @@ struct SchurHost {
     // multi-RHS solve: columns ordered by their first non-zero interior
     // row; blocks of SCHUR_MS_R columns and their first rows
     std::vector<int> col_order, blk_start;
+    int R = SCHUR_MS_R;             // columns per block of the forward sweep (16 or 32)
     std::vector<int> first;         // [L + m] first non-zero interior row of each column
     std::vector<int> gsort, gfirst; // boundary positions by first row, and those rows
 };
@@ -67,11 +68,13 @@ struct SchurHost {
 // when the split is unusable (no interior or no boundary node, or m above
 // SCHUR_MMAX).
 int schur_plan_host(const AssemblyLists& full, int n, const std::vector<int>& gamma_nodes,
-                    const std::vector<int>& enr0, int lsink, int nsink0, SchurHost& out);
+                    const std::vector<int>& enr0, int lsink, int nsink0, SchurHost& out, int R = SCHUR_MS_R);
 
 // Device arguments of the Schur kernels (one context's plan).
 struct SchurArgs {
     int nI, m, L, K, ncol, mbI, WI, nblk, ncpl, ngg;
+    int k0, nk;              // wavenumbers k0 .. k0 + nk - 1 of a launch (transpose .. back)
+    int R;                   // columns per block of the forward sweep (16: two CTAs per SM, 32: one)
     const int *permI, *gam, *posI_src, *posG_src;
     int posI_sink, posG_sink, lsink;
     const int *gi_ptr, *gi_pos, *gi_ent, *gi_g;
