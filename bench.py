@@ -235,6 +235,11 @@ def schur_work(s, K: int, m_boundary: int, n_interior: int, mb_interior: int):
         "forward": K * float(np.sum(nI - first_g) + np.sum(nI - first_s)) * mb,
         "gram": K * (vtv + vtu),
         "chol": K * L * (M ** 3 / 6.0 + M * M),
+        # iterative form: one reference factor per 16 electrodes, then per
+        # system and iteration the residual (S0 x) and the two triangular
+        # solves, m^2 each (times the mean iteration count, supplied later)
+        "chol_ref": K * ((L + 15) // 16) * (M ** 3 / 6.0 + M * M),
+        "chol_it": K * L * 2.0 * M * M,
         "back": K * (float(np.sum(nI - first_g)) * L + L * nI * mb),
     }
 
@@ -681,10 +686,16 @@ def main():
     kernels = []
     if form_used == 2:
         w = schur_work(s, K, m_b, n_i, mb_i)
+        it_mean = ph.get("schur_iter", 0.0)
+        chol_label = ("k_schur_chol (dense Cholesky of every S_l, fused forward solve, back solve)" if it_mean == 0 else
+                      "k_schur_s0 + k_schur_chol<REF> (a reference factor per 16 electrodes) + k_schur_iter "
+                      "(preconditioned iteration per electrode, %.1f iterations)" % it_mean)
+        if it_mean > 0:
+            w["chol"] = w["chol_ref"] + it_mean * w["chol_it"]
         for name, key, label in (("factor", "factor_kernel", "k_band_factor_blk<cd> (interior band Cholesky, one system per wavenumber)"),
                                  ("forward", "schur_forward", "k_schur_sweep (forward sweep of [F r_I | F A_IG]) + factor transpose"),
                                  ("gram", "schur_gram", "k_schur_gram (V^T [u^ | V^])"),
-                                 ("chol", "schur_chol", "k_schur_chol (dense Cholesky of every S_l, fused forward solve, back solve)"),
+                                 ("chol", "schur_chol", chol_label),
                                  ("back", "schur_back", "k_schur_zrebuild + k_schur_sweep back + k_schur_out_gam")):
             t_ms = ph.get(key, 0.0)
             fl = 8.0 * w[name]

@@ -152,9 +152,11 @@ struct crt_ctx {
         *d_sI_con_sig = nullptr;
     unsigned char* d_sI_dflag = nullptr;
     void *d_sLI = nullptr, *d_sLrev = nullptr, *d_sX = nullptr, *d_sC = nullptr, *d_sS = nullptr, *d_sxg = nullptr,
-         *d_scval = nullptr;
+         *d_scval = nullptr, *d_sS0 = nullptr;
     double* d_sfak = nullptr;
+    int* d_snonconv = nullptr;   // systems the iterative Schur solve did not converge on
     int sS_chunk = 0;
+    double schur_iter_mean = 0;  // the last Schur forward's iterations per electrode system (0: the Cholesky)
     int sev[5] = {-1, -1, -1, -1, -1};   // after the forward sweep, the Gram products, the Cholesky, the back sweep
 };
 
@@ -392,7 +394,8 @@ extern "C" void crt_destroy(crt_ctx* ctx)
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     for (void* p : ctx->schur_bufs)
         if (p) cudaFree(p);
-    void* sws[] = {ctx->d_sLI, ctx->d_sLrev, ctx->d_sX, ctx->d_sC, ctx->d_sS, ctx->d_sxg, ctx->d_scval, ctx->d_sfak};
+    void* sws[] = {ctx->d_sLI, ctx->d_sLrev, ctx->d_sX, ctx->d_sC, ctx->d_sS, ctx->d_sxg, ctx->d_scval, ctx->d_sfak,
+                   ctx->d_sS0, ctx->d_snonconv};
     for (void* p : sws)
         if (p) cudaFree(p);
     void* ptrs[] = {ctx->d_nrel0, ctx->d_snr0, ctx->d_etyp, ctx->d_enk, ctx->d_enr0, ctx->d_mixed_rel,
@@ -638,14 +641,15 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
             int *p_permI = nullptr, *p_gam = nullptr, *p_pis = nullptr, *p_pgs = nullptr, *p_gip = nullptr,
                 *p_gipos = nullptr, *p_gient = nullptr, *p_gig = nullptr, *p_ggg = nullptr, *p_ggh = nullptr,
                 *p_gge = nullptr, *p_co = nullptr, *p_bs = nullptr, *p_first = nullptr, *p_gsort = nullptr,
-                *p_gfirst = nullptr;
+                *p_gfirst = nullptr, *p_bdp = nullptr, *p_bdc = nullptr, *p_bde = nullptr;
             const AssemblyLists& li = H.lists_I;
             std::vector<unsigned char> zf(H.nI, 0);
             bool su = up(&p_permI, H.permI) && up(&p_gam, H.gam) && up(&p_pis, H.posI_src) && up(&p_pgs, H.posG_src) &&
                       up(&p_gip, H.gi_ptr) && up(&p_gipos, H.gi_pos) && up(&p_gient, H.gi_ent) && up(&p_gig, H.gi_g) &&
                       up(&p_ggg, H.gg_g) && up(&p_ggh, H.gg_h) && up(&p_gge, H.gg_ent) && up(&p_co, H.col_order) &&
                       up(&p_bs, H.blk_start) && up(&p_first, H.first) && up(&p_gsort, H.gsort) &&
-                      up(&p_gfirst, H.gfirst) && up(&ctx->d_sI_row_ptr, li.row_ptr) && up(&ctx->d_sI_ent_d, li.ent_d) &&
+                      up(&p_gfirst, H.gfirst) && up(&p_bdp, H.bd_ptr) && up(&p_bdc, H.bd_col) && up(&p_bde, H.bd_ent) &&
+                      up(&ctx->d_sI_row_ptr, li.row_ptr) && up(&ctx->d_sI_ent_d, li.ent_d) &&
                       up(&ctx->d_sI_ent_ptr, li.ent_ptr) && up(&ctx->d_sI_con_code, li.con_code) &&
                       up(&ctx->d_sI_con_sig, li.con_sig) && upload(ctx, &ctx->d_sI_dflag, zf.data(), zf.size());
             if (!su) return fail(ctx, CRT_ERR_ALLOC);
@@ -679,6 +683,11 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
             S.first = p_first;
             S.gsort = p_gsort;
             S.gfirst = p_gfirst;
+            S.bd_ptr = p_bdp;
+            S.bd_col = p_bdc;
+            S.bd_ent = p_bde;
+            S.grp = 0;
+            S.ngrp = 0;
             ctx->schur_ok = 1;
         }
     }
@@ -1111,8 +1120,40 @@ int run_forward_schur(crt_ctx* ctx)
     ctx->sev[0] = tev_rec(ctx);
     launch_schur_gram<T>(S, X, Cg, ctx->st);
     ctx->sev[1] = tev_rec(ctx);
-    for (int s0 = 0; s0 < K * L; s0 += ctx->sS_chunk)
-        launch_schur_chol<T>(S, Af, Cg, Sws, xg, s0, std::min(ctx->sS_chunk, K * L - s0), ctx->st);
+    // The electrode systems S_l = S0 + D_l: by the iteration preconditioned
+    // with one factor per group of electrodes (the mixed-boundary parts D_l
+    // of nearby electrodes differ little), or each by its own Cholesky
+    // (CRT_B200_SCHUR_SOLVE=direct, a capture, or when the iteration does
+    // not converge on every system).
+    const char* sv_env = std::getenv("CRT_B200_SCHUR_SOLVE");
+    const bool want_iter = !(sv_env && std::strcmp(sv_env, "direct") == 0);
+    const char* gv = std::getenv("CRT_B200_SCHUR_GROUP");
+    int grp = gv ? std::atoi(gv) : 16;
+    grp = std::max(1, std::min(grp, L));
+    const int ngrp = (L + grp - 1) / grp;
+    bool iter = want_iter && !ctx->capture && L >= 2 && ctx->sS_chunk >= K * ngrp &&
+                schur_iter_smem<T>(m) <= 227 * 1024;
+    ctx->schur_iter_mean = 0.0;
+    if (iter) {
+        if (!ctx->d_sS0) CK(cudaMalloc(&ctx->d_sS0, sizeof(T) * (size_t)K * m * m));
+        if (!ctx->d_snonconv) CK(cudaMalloc((void**)&ctx->d_snonconv, 2 * sizeof(int)));
+        S.grp = grp;
+        S.ngrp = ngrp;
+        T* S0 = static_cast<T*>(ctx->d_sS0);
+        CK(cudaMemsetAsync(ctx->d_snonconv, 0, 2 * sizeof(int), ctx->st));
+        launch_schur_s0<T>(S, Af, Cg, S0, ctx->st);
+        launch_schur_ref<T>(S, Af, S0, Sws, ctx->d_snonconv, ctx->st);
+        launch_schur_iter<T>(S, Af, Cg, S0, Sws, xg, 40, 1e-15, ctx->d_snonconv, ctx->st);
+        int nc[2] = {0, 0};
+        CK(cudaMemcpyAsync(nc, ctx->d_snonconv, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        ctx->launches += 4;
+        if (nc[0] == 0) ctx->schur_iter_mean = (double)nc[1] / (double)(K * L);
+        else iter = false;
+    }
+    if (!iter)
+        for (int s0 = 0; s0 < K * L; s0 += ctx->sS_chunk)
+            launch_schur_chol<T>(S, Af, Cg, Sws, xg, s0, std::min(ctx->sS_chunk, K * L - s0), ctx->st);
     ctx->sev[2] = tev_rec(ctx);
     launch_schur_zrebuild<T>(S, X, xg, ctx->st);
     launch_schur_back<T>(S, Lrev, ctx->d_sfak, X, xg, ctx->n, ctx->d_kpot, ctx->st);
@@ -1157,8 +1198,9 @@ void resolve_forward_timings(crt_ctx* ctx)
         ctx->timings[14] = tev_ms(ctx, ctx->sev[0], ctx->sev[1]);
         ctx->timings[15] = tev_ms(ctx, ctx->sev[1], ctx->sev[2]);
         ctx->timings[16] = tev_ms(ctx, ctx->sev[2], ctx->sev[3]);
+        ctx->timings[17] = ctx->schur_iter_mean;
     } else {
-        ctx->timings[13] = ctx->timings[14] = ctx->timings[15] = ctx->timings[16] = 0.0;
+        ctx->timings[13] = ctx->timings[14] = ctx->timings[15] = ctx->timings[16] = ctx->timings[17] = 0.0;
     }
 }
 

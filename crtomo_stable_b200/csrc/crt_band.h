@@ -54,6 +54,34 @@ __device__ __forceinline__ W band_assemble_entry(const BandArgs<T>& A, int e, in
     return v;
 }
 
+// The area (part 0) or mixed-boundary (part 1) contributions of one band
+// entry: the boundary coefficients kg averaged over the electrodes l0 ..
+// l0 + nl - 1 (nl = 1: electrode l0's).
+template <typename W, typename T>
+__device__ __forceinline__ W band_assemble_part(const BandArgs<T>& A, int e, int k, int l0, int nl, int part)
+{
+    W v = Sc<W>::zero();
+    const int c1 = A.ent_ptr[e + 1];
+    const double* elbg_k = A.elbg + (size_t)k * A.E * A.nmn;
+    for (int c = A.ent_ptr[e]; c < c1; ++c) {
+        const int code = A.con_code[c];
+        double coef;
+        if (code >= 0) {
+            if (part != 0) continue;
+            coef = elbg_k[code];
+        } else {
+            if (part != 1) continue;
+            const int q = -code - 1;
+            const double* kq = A.kg + ((size_t)k * A.L + l0) * A.R + q / 3;
+            double sk = 0.0;
+            for (int j = 0; j < nl; ++j) sk += kq[(size_t)j * A.R];
+            coef = A.relbg[q] * (sk / nl);
+        }
+        v += scale(Sc<W>::from(A.sigma[A.con_sig[c]]), coef);
+    }
+    return v;
+}
+
 template <typename T>
 struct SolveArgs {
     int n, mb, W;

@@ -12,7 +12,7 @@
 #define CRT_HD __host__ __device__ __forceinline__
 
 // entries of crt_last_timings_ex
-#define CRT_NTIMINGS 17
+#define CRT_NTIMINGS 18
 
 struct __align__(16) cd {
     double x, y;

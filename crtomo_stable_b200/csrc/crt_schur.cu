@@ -90,6 +90,28 @@ int schur_plan_host(const AssemblyLists& full, int n, const std::vector<int>& ga
             li.max_row_entries = std::max(li.max_row_entries, li.row_ptr.back() - li.row_ptr[li.row_ptr.size() - 2]);
         }
     }
+    // rows of D_l: the G-G entries with a mixed-boundary contribution, both
+    // triangles, by row
+    {
+        std::vector<std::vector<std::pair<int, int>>> bd(o.m);
+        for (size_t q = 0; q < o.gg_ent.size(); ++q) {
+            const int e = o.gg_ent[q];
+            bool mixed = false;
+            for (int c = full.ent_ptr[e]; c < full.ent_ptr[e + 1]; ++c) mixed |= full.con_code[c] < 0;
+            if (!mixed) continue;
+            bd[o.gg_g[q]].push_back({o.gg_h[q], e});
+            if (o.gg_g[q] != o.gg_h[q]) bd[o.gg_h[q]].push_back({o.gg_g[q], e});
+        }
+        o.bd_ptr.assign(1, 0);
+        for (int g = 0; g < o.m; ++g) {
+            std::sort(bd[g].begin(), bd[g].end());
+            for (auto& he : bd[g]) {
+                o.bd_col.push_back(he.first);
+                o.bd_ent.push_back(he.second);
+            }
+            o.bd_ptr.push_back((int)o.bd_col.size());
+        }
+    }
     o.gi_ptr.assign(1, 0);
     std::vector<int> first(o.L + o.m, o.nI);
     for (int g = 0; g < o.m; ++g) {
@@ -462,9 +484,13 @@ __global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __rest
 // PF: the next super-tile's entries are loaded into registers while the
 // current one is updated (one CTA per SM); without, two CTAs share an SM and
 // hide each other's latency.
-template <typename T, int NT, int NB, bool PF>
+// REF: the reference factors of the iterative form instead, one per
+// (wavenumber, electrode group) b: S0 + the group's mean mixed-boundary part
+// (S0 from C), factored in place without a right-hand side; a non-positive
+// pivot is counted in *nonconv.
+template <typename T, int NT, int NB, bool PF, bool REF = false>
 __global__ void __launch_bounds__(NT, PF ? 1 : 2) k_schur_chol(SchurArgs s, BandArgs<T> A, const T* __restrict__ C,
-                                                               T* Sws, T* xg, int sys0)
+                                                               T* Sws, T* xg, int sys0, int* nonconv = nullptr)
 {
     static_assert(NT == 256 && NB <= 16, "chol layout");
     extern __shared__ __align__(16) unsigned char ch_dyn[];
@@ -473,24 +499,39 @@ __global__ void __launch_bounds__(NT, PF ? 1 : 2) k_schur_chol(SchurArgs s, Band
     T* y = P + (size_t)NB * m;             // [m]
     __shared__ int s_err;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int b = blockIdx.x, sys = sys0 + b, k = sys / s.L, l = sys % s.L;
+    const int b = blockIdx.x, sys = sys0 + b;
+    const int k = REF ? b / s.ngrp : sys / s.L, l = REF ? (b % s.ngrp) * s.grp : sys % s.L;
     T* S = Sws + (size_t)b * m * m;
     const T* Ck = C + (size_t)k * s.ncol * m;
     if (tid == 0) s_err = 0;
-    for (int c = 0; c < m; ++c) {
-        const T* src = Ck + (size_t)(s.L + c) * m;
-        for (int r = c + tid; r < m; r += NT) S[(size_t)c * m + r] = -src[r];
-    }
-    for (int g = tid; g < m; g += NT) {
-        T v = -Ck[(size_t)l * m + g];
-        if (g == s.posG_src[l]) v += Sc<T>::one();
-        if (s.lsink && g == s.posG_sink) v -= Sc<T>::one();
-        y[g] = v;
-    }
-    __syncthreads();
-    for (int q = tid; q < s.ngg; q += NT) {
-        const T a = band_assemble_entry<T>(A, s.gg_ent[q], k, l);
-        S[(size_t)s.gg_h[q] * m + s.gg_g[q]] += a;
+    if constexpr (REF) {
+        const T* S0k = C;   // REF: C is S0 ([k][m][m], both triangles)
+        for (int c = 0; c < m; ++c)
+            for (int r = c + tid; r < m; r += NT) S[(size_t)c * m + r] = S0k[((size_t)k * m + c) * m + r];
+        for (int g = tid; g < m; g += NT) y[g] = Sc<T>::zero();
+        __syncthreads();
+        const int nl = min(s.grp, s.L - l);
+        for (int g = tid; g < m; g += NT)
+            for (int q = s.bd_ptr[g]; q < s.bd_ptr[g + 1]; ++q) {
+                const int h = s.bd_col[q];
+                if (h <= g) S[(size_t)h * m + g] += band_assemble_part<T>(A, s.bd_ent[q], k, l, nl, 1);
+            }
+    } else {
+        for (int c = 0; c < m; ++c) {
+            const T* src = Ck + (size_t)(s.L + c) * m;
+            for (int r = c + tid; r < m; r += NT) S[(size_t)c * m + r] = -src[r];
+        }
+        for (int g = tid; g < m; g += NT) {
+            T v = -Ck[(size_t)l * m + g];
+            if (g == s.posG_src[l]) v += Sc<T>::one();
+            if (s.lsink && g == s.posG_sink) v -= Sc<T>::one();
+            y[g] = v;
+        }
+        __syncthreads();
+        for (int q = tid; q < s.ngg; q += NT) {
+            const T a = band_assemble_entry<T>(A, s.gg_ent[q], k, l);
+            S[(size_t)s.gg_h[q] * m + s.gg_g[q]] += a;
+        }
     }
     __syncthreads();
     for (int p0 = 0; p0 < m; p0 += NB) {
@@ -586,6 +627,10 @@ __global__ void __launch_bounds__(NT, PF ? 1 : 2) k_schur_chol(SchurArgs s, Band
         }
         __syncthreads();
     }
+    if constexpr (REF) {
+        if (s_err && tid == 0) atomicAdd(nonconv, 1);
+        return;
+    }
     if (s_err) {
         if (tid == 0) atomicMax(&s.status[sys], s_err);
         return;
@@ -618,6 +663,252 @@ __global__ void __launch_bounds__(NT, PF ? 1 : 2) k_schur_chol(SchurArgs s, Band
         __syncthreads();
     }
     for (int g = tid; g < m; g += NT) xg[(size_t)sys * m + g] = y[g];
+}
+
+// |Re| + |Im| (the convergence test's magnitude)
+__device__ __forceinline__ double mag1(double a) { return fabs(a); }
+__device__ __forceinline__ double mag1(cd a) { return fabs(a.x) + fabs(a.y); }
+
+// ---------------------------------------------------------------------------
+// Iterative form.  S0[k] = A_GG^area - V^T V^, both triangles, column-major:
+// first -C_VV (C's lower triangle, mirrored), then the area part of every G-G
+// entry (each pair g >= h occurs once in the gg list).
+template <typename T>
+__global__ void k_schur_s0_vv(SchurArgs s, const T* __restrict__ C, T* S0)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = s.m;
+    if (idx >= (long long)s.K * m * m) return;
+    const int k = (int)(idx / ((long long)m * m)), c = (int)((idx / m) % m), r = (int)(idx % m);
+    const int hi = max(r, c), lo = min(r, c);
+    S0[idx] = -C[((size_t)k * s.ncol + s.L + lo) * m + hi];
+}
+
+template <typename T>
+__global__ void k_schur_s0_area(SchurArgs s, BandArgs<T> A, T* S0)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)s.K * s.ngg) return;
+    const int k = (int)(idx / s.ngg), q = (int)(idx % s.ngg), m = s.m;
+    const T a = band_assemble_part<T>(A, s.gg_ent[q], k, 0, 1, 0);
+    const int g = s.gg_g[q], h = s.gg_h[q];
+    T* Sk = S0 + (size_t)k * m * m;
+    Sk[(size_t)h * m + g] += a;
+    if (g != h) Sk[(size_t)g * m + h] += a;
+}
+
+// The preconditioned iteration for SCHUR_IT_NS systems of one electrode
+// group (one CTA): x_0 = 0, r = b - S_l x, z = S_ref^-1 r, x += z, until
+// max |z| <= tol max |x| for every system.  X and R/Z live in shared memory
+// ([m][NS], row-major); S0 and the reference factor stream from L2.  The
+// products S0 X read S0 by columns (coalesced over the rows); D_l X uses the
+// boundary rows (bd_*); the triangular solves go by 16-column panels (one
+// warp per system solves a panel's triangle, all threads update the rows
+// below, or, backwards, reduce the solved rows into the panel).
+constexpr int SCHUR_IT_NS = 8;
+constexpr int SCHUR_IT_NT = 256;
+constexpr int SCHUR_IT_PB = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, BandArgs<T> A, const T* __restrict__ C,
+                                                              const T* __restrict__ S0, const T* __restrict__ Lref,
+                                                              T* xg, int maxit, double tol, int* nonconv)
+{
+    constexpr int NS = SCHUR_IT_NS, NT = SCHUR_IT_NT, PB = SCHUR_IT_PB;
+    extern __shared__ __align__(16) unsigned char it_dyn[];
+    const int m = s.m, L = s.L;
+    T* X = reinterpret_cast<T*>(it_dyn);   // [m][NS]
+    T* Z = X + (size_t)m * NS;              // [m][NS]
+    __shared__ double s_dx[NS], s_x[NS], s_dprev[NS];
+    __shared__ int s_go;
+    __shared__ T Ld[PB][PB + 1];   // the panel's diagonal block, Ld[c][r] = L(p0 + r, p0 + c)
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int cpg = (s.grp + NS - 1) / NS;             // CTAs per group
+    const int b = blockIdx.x, half = b % cpg, kg = b / cpg, g = kg % s.ngrp, k = kg / s.ngrp;
+    const int l0 = g * s.grp + half * NS;
+    const int l1 = min(min(L, (g + 1) * s.grp), l0 + NS);
+    const int ns = l1 - l0;
+    if (ns <= 0) return;
+    const T* Ck = C + (size_t)k * s.ncol * m;
+    const T* Sk = S0 + (size_t)k * m * m;
+    const T* Lg = Lref + (size_t)kg * m * m;
+    auto bval = [&](int r, int j) {
+        const int l = l0 + j;
+        T v = -Ck[(size_t)l * m + r];
+        if (r == s.posG_src[l]) v += Sc<T>::one();
+        if (s.lsink && r == s.posG_sink) v -= Sc<T>::one();
+        return v;
+    };
+    for (int i = tid; i < m * NS; i += NT) {
+        const int r = i / NS, j = i % NS;
+        X[i] = Sc<T>::zero();
+        Z[i] = j < ns ? bval(r, j) : Sc<T>::zero();
+    }
+    __syncthreads();
+    int it = 0;
+    for (;; ++it) {
+        if (it > 0) {
+            // Z = b - S0 X - D_l X (rows r = tid, tid + NT, ...)
+            for (int r = tid; r < m; r += NT) {
+                T acc[NS];
+#pragma unroll
+                for (int j = 0; j < NS; ++j) acc[j] = j < ns ? bval(r, j) : Sc<T>::zero();
+#pragma unroll 4
+                for (int c = 0; c < m; ++c) {
+                    const T a = Sk[(size_t)c * m + r];
+#pragma unroll
+                    for (int j = 0; j < NS; ++j) fms_acc(acc[j], a, X[c * NS + j]);
+                }
+                for (int q = s.bd_ptr[r]; q < s.bd_ptr[r + 1]; ++q) {
+                    const int c = s.bd_col[q], e = s.bd_ent[q];
+#pragma unroll
+                    for (int j = 0; j < NS; ++j)
+                        if (j < ns) fms_acc(acc[j], band_assemble_part<T>(A, e, k, l0 + j, 1, 1), X[c * NS + j]);
+                }
+#pragma unroll
+                for (int j = 0; j < NS; ++j) Z[r * NS + j] = acc[j];
+            }
+            __syncthreads();
+        }
+        // the panel's diagonal block into shared memory (all threads)
+        auto stage_diag = [&](int p0, int nb) {
+            for (int i = tid; i < PB * PB; i += NT) {
+                const int c = i / PB, r = i % PB;
+                Ld[c][r] = (c < nb && r < nb && r >= c) ? Lg[(size_t)(p0 + c) * m + p0 + r] : Sc<T>::zero();
+            }
+        };
+        // forward: L y = z, by panels
+        for (int p0 = 0; p0 < m; p0 += PB) {
+            const int nb = min(PB, m - p0);
+            stage_diag(p0, nb);
+            __syncthreads();
+            if (warp < NS) {   // warp j: system j, lane t: row p0 + t
+                const int j = warp;
+                T v = lane < nb ? Z[(p0 + lane) * NS + j] : Sc<T>::zero();
+#pragma unroll
+                for (int u = 0; u < PB; ++u) {
+                    if (u < nb) {
+                        if (lane == u) v = Sc<T>::mul(v, Sc<T>::recip(Ld[u][u]));
+                        const T xu = shfl_w(v, u, 32);
+                        if (lane > u && lane < nb) fms_acc(v, Ld[u][lane], xu);
+                    }
+                }
+                if (lane < nb) Z[(p0 + lane) * NS + j] = v;
+            }
+            __syncthreads();
+            for (int r = p0 + nb + tid; r < m; r += NT) {
+                T acc[NS];
+#pragma unroll
+                for (int j = 0; j < NS; ++j) acc[j] = Z[r * NS + j];
+                T a[PB];
+#pragma unroll
+                for (int u = 0; u < PB; ++u) a[u] = u < nb ? Lg[(size_t)(p0 + u) * m + r] : Sc<T>::zero();
+#pragma unroll
+                for (int u = 0; u < PB; ++u)
+#pragma unroll
+                    for (int j = 0; j < NS; ++j) fms_acc(acc[j], a[u], Z[(p0 + u) * NS + j]);
+#pragma unroll
+                for (int j = 0; j < NS; ++j) Z[r * NS + j] = acc[j];
+            }
+            __syncthreads();
+        }
+        // backward: L^T x = y, by panels from the last
+        for (int p0 = (m - 1) / PB * PB; p0 >= 0; p0 -= PB) {
+            const int nb = min(PB, m - p0);
+            {   // y[p0 + t] -= sum over solved rows r >= p0 + nb of L(r, p0 + t) x_r: 16 threads per column t
+                const int t = tid >> 4, sl = tid & 15;
+                T part[NS];
+#pragma unroll
+                for (int j = 0; j < NS; ++j) part[j] = Sc<T>::zero();
+                if (t < nb) {
+                    const T* col = Lg + (size_t)(p0 + t) * m;
+#pragma unroll 4
+                    for (int r = p0 + nb + sl; r < m; r += 16) {
+                        const T a = col[r];
+#pragma unroll
+                        for (int j = 0; j < NS; ++j) fma_acc(part[j], a, Z[r * NS + j]);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < NS; ++j) {
+#pragma unroll
+                    for (int off = 8; off > 0; off >>= 1) part[j] += shfl_xor_t(part[j], off);
+                }
+                __syncthreads();
+                if (sl == 0 && t < nb)
+#pragma unroll
+                    for (int j = 0; j < NS; ++j) Z[(p0 + t) * NS + j] -= part[j];
+            }
+            stage_diag(p0, nb);
+            __syncthreads();
+            if (warp < NS) {   // the panel's triangle of L^T, lane t = row p0 + t
+                const int j = warp;
+                T v = lane < nb ? Z[(p0 + lane) * NS + j] : Sc<T>::zero();
+#pragma unroll
+                for (int u = PB - 1; u >= 0; --u) {
+                    if (u < nb) {
+                        if (lane == u) v = Sc<T>::mul(v, Sc<T>::recip(Ld[u][u]));
+                        const T xu = shfl_w(v, u, 32);
+                        if (lane < u) fms_acc(v, Ld[lane][u], xu);
+                    }
+                }
+                if (lane < nb) Z[(p0 + lane) * NS + j] = v;
+            }
+            __syncthreads();
+        }
+        // x += z; convergence: max |z| <= tol max |x| per system
+        if (tid < NS) {
+            s_dx[tid] = 0.0;
+            s_x[tid] = 0.0;
+        }
+        __syncthreads();
+        {
+            const int j = tid % NS;
+            double dmax = 0.0, xmax = 0.0;
+            for (int r = tid / NS; r < m; r += NT / NS) {
+                const T z = Z[r * NS + j];
+                const T x = X[r * NS + j] + z;
+                X[r * NS + j] = x;
+                dmax = fmax(dmax, mag1(z));
+                xmax = fmax(xmax, mag1(x));
+            }
+            // the NT / NS threads of system j: lanes j, j + NS, ... of each warp, then the warps
+#pragma unroll
+            for (int off = 16; off >= NS; off >>= 1) {
+                dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
+                xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, off));
+            }
+            if (lane < NS) {
+                atomicMax(reinterpret_cast<unsigned long long*>(&s_dx[j]), __double_as_longlong(dmax));
+                atomicMax(reinterpret_cast<unsigned long long*>(&s_x[j]), __double_as_longlong(xmax));
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            // converged: the correction at tol of the solution, or no longer
+            // contracting at the rounding level of the residual (a small
+            // correction that did not halve)
+            int go = 0;
+            for (int j = 0; j < ns; ++j) {
+                const bool done = s_dx[j] <= tol * s_x[j] ||
+                                  (it >= 2 && s_dx[j] > 0.5 * s_dprev[j] && s_dx[j] <= 1e-9 * s_x[j]);
+                go |= !done;
+                s_dprev[j] = s_dx[j];
+            }
+            s_go = go;
+        }
+        __syncthreads();
+        if (!s_go) break;
+        if (it + 1 >= maxit) {
+            if (tid == 0) atomicAdd(nonconv, ns);
+            return;
+        }
+    }
+    if (tid == 0) atomicAdd(nonconv + 1, ns * (it + 1));   // system-iterations, for the work count
+    for (int i = tid; i < m * ns; i += NT) {
+        const int j = i / m, r = i % m;
+        xg[((size_t)k * L + l0 + j) * m + r] = X[r * NS + j];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -759,12 +1050,52 @@ void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* C, 
     if (two) {
         auto kern = k_schur_chol<T, NT, 12, false>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem12);
-        kern<<<nsys, NT, smem12, st>>>(s, full, C, Sws, xg, sys0);
+        kern<<<nsys, NT, smem12, st>>>(s, full, C, Sws, xg, sys0, nullptr);
     } else {
         auto kern = k_schur_chol<T, NT, 16, true>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem16);
-        kern<<<nsys, NT, smem16, st>>>(s, full, C, Sws, xg, sys0);
+        kern<<<nsys, NT, smem16, st>>>(s, full, C, Sws, xg, sys0, nullptr);
     }
+}
+
+template <typename T>
+void launch_schur_s0(const SchurArgs& s, const BandArgs<T>& full, const T* C, T* S0, cudaStream_t st)
+{
+    const long long tot = (long long)s.K * s.m * s.m;
+    k_schur_s0_vv<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, C, S0);
+    const long long ng = (long long)s.K * s.ngg;
+    if (ng > 0) k_schur_s0_area<T><<<(unsigned)((ng + 255) / 256), 256, 0, st>>>(s, full, S0);
+}
+
+template <typename T>
+void launch_schur_ref(const SchurArgs& s, const BandArgs<T>& full, const T* S0, T* Lref, int* nonconv, cudaStream_t st)
+{
+    constexpr int NT = 256;
+    const size_t smem12 = ((size_t)12 * s.m + s.m) * sizeof(T), smem16 = ((size_t)16 * s.m + s.m) * sizeof(T);
+    const int nref = s.K * s.ngrp;
+    if (2 * (smem12 + 1024) <= 227 * 1024) {
+        auto kern = k_schur_chol<T, NT, 12, false, true>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem12);
+        kern<<<nref, NT, smem12, st>>>(s, full, S0, Lref, nullptr, 0, nonconv);
+    } else {
+        auto kern = k_schur_chol<T, NT, 16, true, true>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem16);
+        kern<<<nref, NT, smem16, st>>>(s, full, S0, Lref, nullptr, 0, nonconv);
+    }
+}
+
+template <typename T>
+size_t schur_iter_smem(int m) { return 2 * (size_t)m * SCHUR_IT_NS * sizeof(T); }
+
+template <typename T>
+void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, const T* S0, const T* Lref, T* xg,
+                       int maxit, double tol, int* nonconv, cudaStream_t st)
+{
+    const size_t smem = schur_iter_smem<T>(s.m);
+    const int cpg = (s.grp + SCHUR_IT_NS - 1) / SCHUR_IT_NS;
+    auto kern = k_schur_iter<T>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern<<<s.K * s.ngrp * cpg, SCHUR_IT_NT, smem, st>>>(s, full, C, S0, Lref, xg, maxit, tol, nonconv);
 }
 
 template <typename T>
@@ -808,3 +1139,14 @@ template void launch_schur_back<cd>(const SchurArgs&, const cd*, const double*, 
                                     cudaStream_t);
 template void launch_schur_back<double>(const SchurArgs&, const double*, const double*, const double*, const double*,
                                         int, cd*, cudaStream_t);
+template void launch_schur_s0<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, cd*, cudaStream_t);
+template void launch_schur_s0<double>(const SchurArgs&, const BandArgs<double>&, const double*, double*, cudaStream_t);
+template void launch_schur_ref<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, cd*, int*, cudaStream_t);
+template void launch_schur_ref<double>(const SchurArgs&, const BandArgs<double>&, const double*, double*, int*,
+                                       cudaStream_t);
+template void launch_schur_iter<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, const cd*, const cd*, cd*, int,
+                                    double, int*, cudaStream_t);
+template void launch_schur_iter<double>(const SchurArgs&, const BandArgs<double>&, const double*, const double*,
+                                        const double*, double*, int, double, int*, cudaStream_t);
+template size_t schur_iter_smem<cd>(int);
+template size_t schur_iter_smem<double>(int);

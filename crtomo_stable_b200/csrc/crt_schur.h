@@ -55,6 +55,10 @@ struct SchurHost {
     // G-G entries (g >= h) of A_GG(l): full gather entries (area and
     // mixed-boundary contributions)
     std::vector<int> gg_g, gg_h, gg_ent;
+    // rows of the mixed-boundary part D_l of A_GG(l) (both triangles): per
+    // boundary position g, the columns h and gather entries of the G-G
+    // entries with a mixed-boundary contribution
+    std::vector<int> bd_ptr, bd_col, bd_ent;
     // multi-RHS solve: columns ordered by their first non-zero interior
     // row; blocks of SCHUR_MS_R columns and their first rows
     std::vector<int> col_order, blk_start;
@@ -80,6 +84,8 @@ struct SchurArgs {
     const int *gi_ptr, *gi_pos, *gi_ent, *gi_g;
     const int *gg_g, *gg_h, *gg_ent;
     const int *col_order, *blk_start;
+    const int *bd_ptr, *bd_col, *bd_ent;
+    int grp, ngrp;           // iterative Schur solve: electrodes per reference factor, groups
     const int* first;        // [ncol] first non-zero interior row of column c
     const int* gsort;        // [m] boundary positions ordered by their column's first row
     const int* gfirst;       // [m] first row of gsort[q]'s column
@@ -113,6 +119,28 @@ void launch_schur_gram(const SchurArgs& s, const T* X, T* C, cudaStream_t st);
 template <typename T>
 void launch_schur_chol(const SchurArgs& s, const BandArgs<T>& full, const T* C, T* Sws, T* xg, int sys0, int nsys,
                        cudaStream_t st);
+// Iterative form of the Schur solves (replaces launch_schur_chol).  Per
+// wavenumber S_l = S0 + D_l, S0 = A_GG^area - V^T V^ (electrode independent),
+// D_l the mixed-boundary part.  launch_schur_s0 forms S0 (full, column-major,
+// [k][m][m]); launch_schur_ref factors one reference S0 + mean_{l in group}
+// D_l per (k, group of s.grp electrodes) into Lref[(k ngrp + g)][m][m];
+// launch_schur_iter solves every S_l p_G = r_G - C[k][l] by the preconditioned
+// iteration x += S_ref^-1 (b - S_l x) until the correction is below tol
+// |x|_inf, at most maxit steps; systems that do not get there are counted
+// in nonconv[0] (device memory, two ints zeroed by the caller; nonconv[1]
+// sums the iterations of the converged systems), and the caller then solves
+// them all by the per-system Cholesky instead.
+template <typename T>
+void launch_schur_s0(const SchurArgs& s, const BandArgs<T>& full, const T* C, T* S0, cudaStream_t st);
+template <typename T>
+void launch_schur_ref(const SchurArgs& s, const BandArgs<T>& full, const T* S0, T* Lref, int* nonconv,
+                      cudaStream_t st);
+// Shared memory of the iteration's CTA (X and Z for SCHUR_IT_NS systems).
+template <typename T> size_t schur_iter_smem(int m);
+template <typename T>
+void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, const T* S0, const T* Lref, T* xg,
+                       int maxit, double tol, int* nonconv, cudaStream_t st);
+
 // z^_l = u^_l - V^ p_G (in place on the columns l < L of X).
 template <typename T>
 void launch_schur_zrebuild(const SchurArgs& s, T* X, const T* xg, cudaStream_t st);

@@ -458,7 +458,7 @@ class Context:
 
     TIMING_NAMES = ["factor", "solve", "volt", "jacobian", "cg_setup", "cg_iter", "total", "factor_prep",
                     "factor_kernel", "factor_launches", "refine_residual", "refine_solve", "panel",
-                    "schur_forward", "schur_gram", "schur_chol", "schur_back"]
+                    "schur_forward", "schur_gram", "schur_chol", "schur_back", "schur_iter"]
 
     def timings(self):
         t = np.zeros(len(self.TIMING_NAMES))

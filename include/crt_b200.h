@@ -291,9 +291,12 @@ int32_t crt_last_timings(const crt_ctx *ctx, double *ms7);
  * (both inside [1]), [12] the panel width of the blocked band factorisation
  * (chosen by the autotuner; 0 for the unblocked kernel), and in the Schur
  * form (inside [1]) [13] the forward sweep of the interior columns, [14]
- * their Gram products, [15] the boundary Cholesky with its solves, [16]
- * the rebuild and the back sweep into the potentials.
- * Milliseconds except [9] and [12].  No reference counterpart. */
+ * their Gram products, [15] the electrode systems' solves (the iteration
+ * with its reference factors, or the per-system Cholesky), [16] the rebuild
+ * and the back sweep into the potentials, [17] the mean number of
+ * iterations per electrode system when they were solved by the iteration,
+ * 0 when by the Cholesky.
+ * Milliseconds except [9], [12] and [17].  No reference counterpart. */
 int32_t crt_last_timings_ex(const crt_ctx *ctx, double *ms, int32_t n);
 
 /* Kernel launches enqueued by the context since creation. */

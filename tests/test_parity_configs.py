@@ -375,6 +375,34 @@ def test_schur_form_matches_direct_form_and_oracle(name, ldc, precision):
     ctx.close()
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,ldc", [("minimal", False), ("mixed_surf", False), ("TestModInv", True)])
+def test_schur_iteration_matches_schur_cholesky(name, ldc, monkeypatch):
+    """The electrode systems S_l solved by the iteration preconditioned with
+    one factor per group of electrodes (the default) and by their own
+    Cholesky each: the same potentials to 1e-11 of their maximum, and the
+    iteration ran (its mean count is reported) and converged (on
+    TestModInv's DC systems in about 20 steps, on the 60k-triangle
+    benchmark mesh in fewer than 10)."""
+    from fixtures import load_forward_case
+    from crtomo_stable_b200.lib import FORWARD_SCHUR, Context
+    case = load_forward_case(name)
+    c = case["cfg"]
+    out = {}
+    for form in ("iter", "direct"):
+        if form == "direct":
+            monkeypatch.setenv("CRT_B200_SCHUR_SOLVE", "direct")
+        ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=c.swrtr,
+                      lsink=c.lsink, nsink=c.nsink)
+        ctx.set_forward_form(FORWARD_SCHUR)
+        _, _, kp = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+        out[form] = (kp, ctx.timings()["schur_iter"])
+        ctx.close()
+    assert 1.0 <= out["iter"][1] < 40.0 and out["direct"][1] == 0.0   # 40: the iteration limit
+    scale = np.abs(out["direct"][0]).max()
+    assert np.abs(out["iter"][0] - out["direct"][0]).max() <= 1e-11 * scale
+
+
 def test_schur_form_is_refused_where_it_does_not_apply():
     """No mixed boundary (the 2D decoupling grid): the Schur form does not
     apply, the setter says so (errnr 201) and the direct form runs."""
