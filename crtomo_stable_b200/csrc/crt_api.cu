@@ -152,7 +152,7 @@ struct crt_ctx {
         *d_sI_con_sig = nullptr;
     unsigned char* d_sI_dflag = nullptr;
     void *d_sLI = nullptr, *d_sLrev = nullptr, *d_sX = nullptr, *d_sC = nullptr, *d_sS = nullptr, *d_sxg = nullptr,
-         *d_scval = nullptr, *d_sS0 = nullptr;
+         *d_scval = nullptr, *d_sS0 = nullptr, *d_sDv = nullptr;
     double* d_sfak = nullptr;
     int* d_snonconv = nullptr;   // systems the iterative Schur solve did not converge on
     int sS_chunk = 0;
@@ -395,7 +395,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
     for (void* p : ctx->schur_bufs)
         if (p) cudaFree(p);
     void* sws[] = {ctx->d_sLI, ctx->d_sLrev, ctx->d_sX, ctx->d_sC, ctx->d_sS, ctx->d_sxg, ctx->d_scval, ctx->d_sfak,
-                   ctx->d_sS0, ctx->d_snonconv};
+                   ctx->d_sS0, ctx->d_sDv, ctx->d_snonconv};
     for (void* p : sws)
         if (p) cudaFree(p);
     void* ptrs[] = {ctx->d_nrel0, ctx->d_snr0, ctx->d_etyp, ctx->d_enk, ctx->d_enr0, ctx->d_mixed_rel,
@@ -1131,23 +1131,32 @@ int run_forward_schur(crt_ctx* ctx)
     int grp = gv ? std::atoi(gv) : 16;
     grp = std::max(1, std::min(grp, L));
     const int ngrp = (L + grp - 1) / grp;
+    // the iteration pays where its CTAs (eight systems each) fill the GPU
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
     bool iter = want_iter && !ctx->capture && L >= 2 && ctx->sS_chunk >= K * ngrp &&
-                schur_iter_smem<T>(m) <= 227 * 1024;
+                schur_iter_smem<T>(m) <= 227 * 1024 &&
+                (K * L / 8 >= nsm || (sv_env && std::strcmp(sv_env, "iter") == 0));
     ctx->schur_iter_mean = 0.0;
     if (iter) {
         if (!ctx->d_sS0) CK(cudaMalloc(&ctx->d_sS0, sizeof(T) * (size_t)K * m * m));
+        const int nbd = (int)ctx->schur_h.bd_col.size();
+        if (!ctx->d_sDv) CK(cudaMalloc(&ctx->d_sDv, sizeof(T) * std::max<size_t>(1, (size_t)K * L * nbd)));
+        S.nbd = nbd;
         if (!ctx->d_snonconv) CK(cudaMalloc((void**)&ctx->d_snonconv, 2 * sizeof(int)));
         S.grp = grp;
         S.ngrp = ngrp;
         T* S0 = static_cast<T*>(ctx->d_sS0);
         CK(cudaMemsetAsync(ctx->d_snonconv, 0, 2 * sizeof(int), ctx->st));
+        T* Dv = static_cast<T*>(ctx->d_sDv);
         launch_schur_s0<T>(S, Af, Cg, S0, ctx->st);
+        launch_schur_dvals<T>(S, Af, Dv, ctx->st);
         launch_schur_ref<T>(S, Af, S0, Sws, ctx->d_snonconv, ctx->st);
-        launch_schur_iter<T>(S, Af, Cg, S0, Sws, xg, 40, 1e-15, ctx->d_snonconv, ctx->st);
+        launch_schur_iter<T>(S, Af, Cg, S0, Sws, Dv, xg, 40, 1e-15, ctx->d_snonconv, ctx->st);
         int nc[2] = {0, 0};
         CK(cudaMemcpyAsync(nc, ctx->d_snonconv, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
-        ctx->launches += 4;
+        ctx->launches += 5;
         if (nc[0] == 0) ctx->schur_iter_mean = (double)nc[1] / (double)(K * L);
         else iter = false;
     }

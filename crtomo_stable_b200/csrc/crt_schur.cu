@@ -699,8 +699,9 @@ __global__ void k_schur_s0_area(SchurArgs s, BandArgs<T> A, T* S0)
 
 // The preconditioned iteration for SCHUR_IT_NS systems of one electrode
 // group (one CTA): x_0 = 0, r = b - S_l x, z = S_ref^-1 r, x += z, until
-// max |z| <= tol max |x| for every system.  X and R/Z live in shared memory
-// ([m][NS], row-major); S0 and the reference factor stream from L2.  The
+// max |z| <= tol max |x| for every system.  X and R/Z live in shared memory,
+// a system's column contiguous ([NS][m], so that threads over rows touch
+// consecutive words); S0 and the reference factor stream from L2.  The
 // products S0 X read S0 by columns (coalesced over the rows); D_l X uses the
 // boundary rows (bd_*); the triangular solves go by 16-column panels (one
 // warp per system solves a panel's triangle, all threads update the rows
@@ -710,15 +711,27 @@ constexpr int SCHUR_IT_NT = 256;
 constexpr int SCHUR_IT_PB = 16;
 
 template <typename T>
+__global__ void k_schur_dvals(SchurArgs s, BandArgs<T> A, T* Dv)
+{
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)s.K * s.L * s.nbd) return;
+    const int q = (int)(idx % s.nbd);
+    const long long kl = idx / s.nbd;
+    const int k = (int)(kl / s.L), l = (int)(kl % s.L);
+    Dv[idx] = band_assemble_part<T>(A, s.bd_ent[q], k, l, 1, 1);
+}
+
+template <typename T>
 __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, BandArgs<T> A, const T* __restrict__ C,
                                                               const T* __restrict__ S0, const T* __restrict__ Lref,
-                                                              T* xg, int maxit, double tol, int* nonconv)
+                                                              const T* __restrict__ Dv, T* xg, int maxit,
+                                                              double tol, int* nonconv)
 {
     constexpr int NS = SCHUR_IT_NS, NT = SCHUR_IT_NT, PB = SCHUR_IT_PB;
     extern __shared__ __align__(16) unsigned char it_dyn[];
     const int m = s.m, L = s.L;
-    T* X = reinterpret_cast<T*>(it_dyn);   // [m][NS]
-    T* Z = X + (size_t)m * NS;              // [m][NS]
+    T* X = reinterpret_cast<T*>(it_dyn);   // [NS][m]: system j's column at j m
+    T* Z = X + (size_t)m * NS;              // [NS][m]
     __shared__ double s_dx[NS], s_x[NS], s_dprev[NS];
     __shared__ int s_go;
     __shared__ T Ld[PB][PB + 1];   // the panel's diagonal block, Ld[c][r] = L(p0 + r, p0 + c)
@@ -740,7 +753,7 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
         return v;
     };
     for (int i = tid; i < m * NS; i += NT) {
-        const int r = i / NS, j = i % NS;
+        const int j = i / m, r = i % m;
         X[i] = Sc<T>::zero();
         Z[i] = j < ns ? bval(r, j) : Sc<T>::zero();
     }
@@ -757,16 +770,17 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
                 for (int c = 0; c < m; ++c) {
                     const T a = Sk[(size_t)c * m + r];
 #pragma unroll
-                    for (int j = 0; j < NS; ++j) fms_acc(acc[j], a, X[c * NS + j]);
+                    for (int j = 0; j < NS; ++j) fms_acc(acc[j], a, X[j * m + c]);
                 }
+                const T* Dk = Dv + ((size_t)k * L + l0) * s.nbd;
                 for (int q = s.bd_ptr[r]; q < s.bd_ptr[r + 1]; ++q) {
-                    const int c = s.bd_col[q], e = s.bd_ent[q];
+                    const int c = s.bd_col[q];
 #pragma unroll
                     for (int j = 0; j < NS; ++j)
-                        if (j < ns) fms_acc(acc[j], band_assemble_part<T>(A, e, k, l0 + j, 1, 1), X[c * NS + j]);
+                        if (j < ns) fms_acc(acc[j], Dk[(size_t)j * s.nbd + q], X[j * m + c]);
                 }
 #pragma unroll
-                for (int j = 0; j < NS; ++j) Z[r * NS + j] = acc[j];
+                for (int j = 0; j < NS; ++j) Z[j * m + r] = acc[j];
             }
             __syncthreads();
         }
@@ -784,7 +798,7 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
             __syncthreads();
             if (warp < NS) {   // warp j: system j, lane t: row p0 + t
                 const int j = warp;
-                T v = lane < nb ? Z[(p0 + lane) * NS + j] : Sc<T>::zero();
+                T v = lane < nb ? Z[j * m + p0 + lane] : Sc<T>::zero();
 #pragma unroll
                 for (int u = 0; u < PB; ++u) {
                     if (u < nb) {
@@ -793,22 +807,22 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
                         if (lane > u && lane < nb) fms_acc(v, Ld[u][lane], xu);
                     }
                 }
-                if (lane < nb) Z[(p0 + lane) * NS + j] = v;
+                if (lane < nb) Z[j * m + p0 + lane] = v;
             }
             __syncthreads();
             for (int r = p0 + nb + tid; r < m; r += NT) {
                 T acc[NS];
 #pragma unroll
-                for (int j = 0; j < NS; ++j) acc[j] = Z[r * NS + j];
+                for (int j = 0; j < NS; ++j) acc[j] = Z[j * m + r];
                 T a[PB];
 #pragma unroll
                 for (int u = 0; u < PB; ++u) a[u] = u < nb ? Lg[(size_t)(p0 + u) * m + r] : Sc<T>::zero();
 #pragma unroll
                 for (int u = 0; u < PB; ++u)
 #pragma unroll
-                    for (int j = 0; j < NS; ++j) fms_acc(acc[j], a[u], Z[(p0 + u) * NS + j]);
+                    for (int j = 0; j < NS; ++j) fms_acc(acc[j], a[u], Z[j * m + p0 + u]);
 #pragma unroll
-                for (int j = 0; j < NS; ++j) Z[r * NS + j] = acc[j];
+                for (int j = 0; j < NS; ++j) Z[j * m + r] = acc[j];
             }
             __syncthreads();
         }
@@ -826,7 +840,7 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
                     for (int r = p0 + nb + sl; r < m; r += 16) {
                         const T a = col[r];
 #pragma unroll
-                        for (int j = 0; j < NS; ++j) fma_acc(part[j], a, Z[r * NS + j]);
+                        for (int j = 0; j < NS; ++j) fma_acc(part[j], a, Z[j * m + r]);
                     }
                 }
 #pragma unroll
@@ -837,13 +851,13 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
                 __syncthreads();
                 if (sl == 0 && t < nb)
 #pragma unroll
-                    for (int j = 0; j < NS; ++j) Z[(p0 + t) * NS + j] -= part[j];
+                    for (int j = 0; j < NS; ++j) Z[j * m + p0 + t] -= part[j];
             }
             stage_diag(p0, nb);
             __syncthreads();
             if (warp < NS) {   // the panel's triangle of L^T, lane t = row p0 + t
                 const int j = warp;
-                T v = lane < nb ? Z[(p0 + lane) * NS + j] : Sc<T>::zero();
+                T v = lane < nb ? Z[j * m + p0 + lane] : Sc<T>::zero();
 #pragma unroll
                 for (int u = PB - 1; u >= 0; --u) {
                     if (u < nb) {
@@ -852,7 +866,7 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
                         if (lane < u) fms_acc(v, Ld[lane][u], xu);
                     }
                 }
-                if (lane < nb) Z[(p0 + lane) * NS + j] = v;
+                if (lane < nb) Z[j * m + p0 + lane] = v;
             }
             __syncthreads();
         }
@@ -863,22 +877,25 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
         }
         __syncthreads();
         {
-            const int j = tid % NS;
+            // the NT / NS threads of system j (NT / NS a multiple of 32):
+            // rows r = i, i + NT / NS, ..., then their warps
+            constexpr int TPS = NT / NS;
+            static_assert(TPS % 32 == 0, "whole warps per system");
+            const int j = tid / TPS, i = tid % TPS;
             double dmax = 0.0, xmax = 0.0;
-            for (int r = tid / NS; r < m; r += NT / NS) {
-                const T z = Z[r * NS + j];
-                const T x = X[r * NS + j] + z;
-                X[r * NS + j] = x;
+            for (int r = i; r < m; r += TPS) {
+                const T z = Z[j * m + r];
+                const T x = X[j * m + r] + z;
+                X[j * m + r] = x;
                 dmax = fmax(dmax, mag1(z));
                 xmax = fmax(xmax, mag1(x));
             }
-            // the NT / NS threads of system j: lanes j, j + NS, ... of each warp, then the warps
 #pragma unroll
-            for (int off = 16; off >= NS; off >>= 1) {
+            for (int off = 16; off > 0; off >>= 1) {
                 dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
                 xmax = fmax(xmax, __shfl_xor_sync(0xffffffffu, xmax, off));
             }
-            if (lane < NS) {
+            if (lane == 0) {
                 atomicMax(reinterpret_cast<unsigned long long*>(&s_dx[j]), __double_as_longlong(dmax));
                 atomicMax(reinterpret_cast<unsigned long long*>(&s_x[j]), __double_as_longlong(xmax));
             }
@@ -907,7 +924,7 @@ __global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, Band
     if (tid == 0) atomicAdd(nonconv + 1, ns * (it + 1));   // system-iterations, for the work count
     for (int i = tid; i < m * ns; i += NT) {
         const int j = i / m, r = i % m;
-        xg[((size_t)k * L + l0 + j) * m + r] = X[r * NS + j];
+        xg[((size_t)k * L + l0 + j) * m + r] = X[j * m + r];
     }
 }
 
@@ -1088,14 +1105,21 @@ template <typename T>
 size_t schur_iter_smem(int m) { return 2 * (size_t)m * SCHUR_IT_NS * sizeof(T); }
 
 template <typename T>
-void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, const T* S0, const T* Lref, T* xg,
-                       int maxit, double tol, int* nonconv, cudaStream_t st)
+void launch_schur_dvals(const SchurArgs& s, const BandArgs<T>& full, T* Dv, cudaStream_t st)
+{
+    const long long tot = (long long)s.K * s.L * s.nbd;
+    if (tot > 0) k_schur_dvals<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, full, Dv);
+}
+
+template <typename T>
+void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, const T* S0, const T* Lref,
+                       const T* Dv, T* xg, int maxit, double tol, int* nonconv, cudaStream_t st)
 {
     const size_t smem = schur_iter_smem<T>(s.m);
     const int cpg = (s.grp + SCHUR_IT_NS - 1) / SCHUR_IT_NS;
     auto kern = k_schur_iter<T>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    kern<<<s.K * s.ngrp * cpg, SCHUR_IT_NT, smem, st>>>(s, full, C, S0, Lref, xg, maxit, tol, nonconv);
+    kern<<<s.K * s.ngrp * cpg, SCHUR_IT_NT, smem, st>>>(s, full, C, S0, Lref, Dv, xg, maxit, tol, nonconv);
 }
 
 template <typename T>
@@ -1144,9 +1168,11 @@ template void launch_schur_s0<double>(const SchurArgs&, const BandArgs<double>&,
 template void launch_schur_ref<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, cd*, int*, cudaStream_t);
 template void launch_schur_ref<double>(const SchurArgs&, const BandArgs<double>&, const double*, double*, int*,
                                        cudaStream_t);
-template void launch_schur_iter<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, const cd*, const cd*, cd*, int,
-                                    double, int*, cudaStream_t);
+template void launch_schur_dvals<cd>(const SchurArgs&, const BandArgs<cd>&, cd*, cudaStream_t);
+template void launch_schur_dvals<double>(const SchurArgs&, const BandArgs<double>&, double*, cudaStream_t);
+template void launch_schur_iter<cd>(const SchurArgs&, const BandArgs<cd>&, const cd*, const cd*, const cd*,
+                                    const cd*, cd*, int, double, int*, cudaStream_t);
 template void launch_schur_iter<double>(const SchurArgs&, const BandArgs<double>&, const double*, const double*,
-                                        const double*, double*, int, double, int*, cudaStream_t);
+                                        const double*, const double*, double*, int, double, int*, cudaStream_t);
 template size_t schur_iter_smem<cd>(int);
 template size_t schur_iter_smem<double>(int);

@@ -86,6 +86,7 @@ struct SchurArgs {
     const int *col_order, *blk_start;
     const int *bd_ptr, *bd_col, *bd_ent;
     int grp, ngrp;           // iterative Schur solve: electrodes per reference factor, groups
+    int nbd;                 // entries of the boundary rows (bd_ptr[m])
     const int* first;        // [ncol] first non-zero interior row of column c
     const int* gsort;        // [m] boundary positions ordered by their column's first row
     const int* gfirst;       // [m] first row of gsort[q]'s column
@@ -137,9 +138,13 @@ void launch_schur_ref(const SchurArgs& s, const BandArgs<T>& full, const T* S0, 
                       cudaStream_t st);
 // Shared memory of the iteration's CTA (X and Z for SCHUR_IT_NS systems).
 template <typename T> size_t schur_iter_smem(int m);
+// Dv[(k L + l) nbd + q] = the mixed-boundary value of boundary-row entry q
+// (bd_*) for electrode l at wavenumber k (nbd = bd_ptr[m]).
 template <typename T>
-void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, const T* S0, const T* Lref, T* xg,
-                       int maxit, double tol, int* nonconv, cudaStream_t st);
+void launch_schur_dvals(const SchurArgs& s, const BandArgs<T>& full, T* Dv, cudaStream_t st);
+template <typename T>
+void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, const T* S0, const T* Lref,
+                       const T* Dv, T* xg, int maxit, double tol, int* nonconv, cudaStream_t st);
 
 // z^_l = u^_l - V^ p_G (in place on the columns l < L of X).
 template <typename T>
