@@ -108,6 +108,10 @@ struct crt_ctx {
     std::string spc_why;
     cd *d_z = nullptr, *d_rold = nullptr, *d_zb = nullptr;
     CGState* d_live = nullptr;   // a never-done CG state for preconditioner applications outside the CG
+    // fused matvec of the CG (k_cg_fused): reduction ring, tickets, error word
+    unsigned char* d_cgf = nullptr;
+    size_t cgf_bytes = 0;
+    int cgf_grid = 0;
     // lambda candidates side by side (crt_update_lambdas): one slab for all
     // candidates' vectors, grown on demand
     unsigned char* d_cgl = nullptr;
@@ -406,7 +410,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega,
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega, ctx->d_cgf,
                     ctx->d_dc_rows, ctx->d_dc_ptr, ctx->d_dc_ent, ctx->d_dc_node, ctx->d_bdir};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1601,6 +1605,48 @@ CGArgs make_cg_args(crt_ctx* ctx, const crt_cg_params* prm)
     return a;
 }
 
+// The fused matvec (one read of J per CG iteration, complex64 Jacobians)
+// when CRT_B200_CG_FUSED=1 asks for it; the two-pass kernels otherwise (on
+// the 60k-cell benchmark the fused form is slower: every row block waits
+// for a grid-wide exchange).  Sets the fused fields of `a`; allocates the
+// reduction ring once per context.
+int setup_cg_fused(crt_ctx* ctx, CGArgs* a)
+{
+    a->fused = 0;
+    const char* ev = std::getenv("CRT_B200_CG_FUSED");
+    if (!ev || std::strcmp(ev, "1") != 0) return CRT_OK;
+    int nsm = 0, smem = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device));
+    CK(cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device));
+    if (!cg_fused_fits(*a, nsm, (size_t)smem)) return CRT_OK;
+    const size_t part = (size_t)CGF_Q * nsm * CGF_R * sizeof(cd), v = (size_t)CGF_Q * CGF_R * sizeof(cd);
+    const size_t words = (size_t)CGF_Q * 8 + 8 + (size_t)CGF_Q * 4 + 4;
+    const size_t bytes = part + v + words;
+    if (ctx->cgf_bytes < bytes) {
+        if (ctx->d_cgf) cudaFree(ctx->d_cgf);
+        ctx->d_cgf = nullptr;
+        ctx->cgf_bytes = 0;
+        if (cudaMalloc(&ctx->d_cgf, bytes) != cudaSuccess) return set_err(ctx, CRT_ERR_ALLOC, "fused CG workspace");
+        CK(cudaMemsetAsync(ctx->d_cgf, 0, bytes, ctx->st));
+        ctx->cgf_bytes = bytes;
+    }
+    ctx->cgf_grid = nsm;
+    // row blocks between the two uses of a tile: long enough for the grid's
+    // partial sums to arrive, short enough for the tiles to stay in L2
+    int lag = 8;
+    if (const char* lv = std::getenv("CRT_B200_CG_FUSED_LAG")) lag = std::atoi(lv);
+    a->flag_lag = std::max(CGF_S, std::min(CGF_Q - 1, lag));
+    a->fused = 1;
+    a->fper = (a->M + nsm - 1) / nsm;
+    a->fpart = reinterpret_cast<cd*>(ctx->d_cgf);
+    a->fv = reinterpret_cast<cd*>(ctx->d_cgf + part);
+    a->fflag = reinterpret_cast<unsigned long long*>(ctx->d_cgf + part + v);
+    a->fepoch = a->fflag + CGF_Q;
+    a->fcnt = reinterpret_cast<int*>(a->fepoch + 1);
+    a->ferr = a->fcnt + CGF_Q;
+    return CRT_OK;
+}
+
 // Block factor and / or message weights of the learned correction for the
 // system whose cgfac was just formed.  A requested piece that is not
 // available (bandwidth, pivot breakdown, untrained network, network trained
@@ -1649,6 +1695,7 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
     a.zb = (use_block && use_gnn) ? ctx->d_zb : nullptr;
     ctx->cg_form = use_block ? (use_gnn ? CRT_PRECOND_BLOCK_GNN : CRT_PRECOND_BLOCK)
                              : (use_gnn ? CRT_PRECOND_GNN : CRT_PRECOND_JACOBI);
+    if (int e = setup_cg_fused(ctx, &a)) return e;
     launch_cg_init(a, ctx->st);
     ctx->launches += 1;
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
@@ -1661,13 +1708,24 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
         int it = std::min(batch, prm->ncgmax - done_iters);
         launch_cg_iterations(a, it, use_block ? &ctx->spc : nullptr, use_gnn ? &ctx->gnn : nullptr, ctx->d_zb,
                              ctx->st);
-        ctx->launches += (5 + (a.pc ? 1 : 0) + (use_block ? 2 : 0) + (use_gnn ? 7 : 0)) * it;
+        ctx->launches += ((a.fused ? 3 : 5) + (a.pc ? 1 : 0) + (use_block ? 2 : 0) + (use_gnn ? 7 : 0)) * it;
         done_iters += it;
         CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
         if (hs.done) break;
     }
     if (int e = kernel_check(ctx, "cg iterations")) return e;
+    if (a.fused) {
+        int ferr = 0;
+        CK(cudaMemcpyAsync(&ferr, a.ferr, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        if (ferr) {
+            // the ring's counters are left mid-block: start it afresh
+            CK(cudaMemsetAsync(ctx->d_cgf, 0, ctx->cgf_bytes, ctx->st));
+            CK(cudaStreamSynchronize(ctx->st));
+            return set_err(ctx, CRT_ERR_CUDA, "fused CG matvec: a wait for the grid's partial sums gave up");
+        }
+    }
     launch_cg_finish(a, prm->lfpi, prm->step, ctx->d_par, ctx->d_bdpar, ctx->st);
     ctx->launches++;
     CK(cudaEventRecord(ctx->ev[2], ctx->st));

@@ -161,33 +161,77 @@ __device__ double block_sum(double v, double* red)
     return r;
 }
 
-// cgfac and scaled RHS, one warp per model cell.
+// cgfac and scaled RHS: one warp per SU_COLS model cells, a CTA of SU_NT / 32
+// warps; the readings' weights and residuals dat - sigmaa are staged in
+// shared memory per chunk of SU_CHUNK readings (read once per CTA, not once
+// per cell).  Lane l sums the rows l + 32 k in order, as one warp per cell
+// would.
+constexpr int SU_COLS = 4, SU_NT = 256, SU_CHUNK = 1024;
+
 template <int JP, int JM>
-__global__ void k_cg_setup(CGArgs A, const cd* dat, const cd* sigmaa, const cd* par)
+__global__ void __launch_bounds__(SU_NT) k_cg_setup(CGArgs A, const cd* dat, const cd* sigmaa, const cd* par)
 {
-    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (warp >= A.M) return;
-    const int e = warp;
-    double an = 0.0, arx = 0.0, ary = 0.0;
-    for (int i = lane; i < A.N; i += 32) {
-        const cd j = jval<JP, JM>(A, e, i);
-        const double w = A.wd[i];
-        const cd rd = dat[i] - sigmaa[i];
-        an += (j.x * j.x + j.y * j.y) * w;
-        const cd t = conj(j) * w * rd;
-        arx += t.x;
-        ary += t.y;
+    using RT = typename JRaw<JP, JM>::T;
+    __shared__ double s_w[SU_CHUNK];
+    __shared__ cd s_rd[SU_CHUNK];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ebase = (blockIdx.x * (SU_NT / 32) + warp) * SU_COLS;
+    const int nc = max(0, min(SU_COLS, A.M - ebase));
+    const int N = A.N;
+    double an[SU_COLS], arx[SU_COLS], ary[SU_COLS];
+#pragma unroll
+    for (int c = 0; c < SU_COLS; ++c) an[c] = arx[c] = ary[c] = 0.0;
+    for (int r0 = 0; r0 < N; r0 += SU_CHUNK) {
+        const int r1 = min(N, r0 + SU_CHUNK);
+        __syncthreads();
+        for (int t = threadIdx.x; t < r1 - r0; t += SU_NT) {
+            s_w[t] = A.wd[r0 + t];
+            s_rd[t] = dat[r0 + t] - sigmaa[r0 + t];
+        }
+        __syncthreads();
+        if (nc == 0) continue;
+        for (int i = r0 + lane; i < r1; i += 64) {
+            RT j0[SU_COLS], j1[SU_COLS];
+            const bool two = i + 32 < r1;
+#pragma unroll
+            for (int c = 0; c < SU_COLS; ++c) {
+                j0[c] = c < nc ? jraw<JP, JM>(A, ebase + c, i) : RT{};
+                j1[c] = (c < nc && two) ? jraw<JP, JM>(A, ebase + c, i + 32) : RT{};
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (q == 1 && !two) break;
+                const int ii = i + 32 * q - r0;
+                const double w = s_w[ii];
+                const cd rd = s_rd[ii];
+#pragma unroll
+                for (int c = 0; c < SU_COLS; ++c) {
+                    const cd j = jcvt<JM>(q == 0 ? j0[c] : j1[c]);
+                    an[c] += (j.x * j.x + j.y * j.y) * w;
+                    const cd t = conj(j) * w * rd;
+                    arx[c] += t.x;
+                    ary[c] += t.y;
+                }
+            }
+        }
     }
-    an = warp_sum(an);
-    arx = warp_sum(arx);
-    ary = warp_sum(ary);
+    if (nc == 0) return;
+#pragma unroll
+    for (int c = 0; c < SU_COLS; ++c) {
+        an[c] = warp_sum(an[c]);
+        arx[c] = warp_sum(arx[c]);
+        ary[c] = warp_sum(ary[c]);
+    }
     if (lane == 0) {
-        const double dum = an + A.lam * reg_diag(A, e);
-        const double cg = 1.0 / sqrt(dum);
-        A.cgfac[e] = cg;
-        const cd rg = reg_apply_par(A, par, e);
-        const cd b = cd{arx, ary} - rg * A.lam;
-        A.rhs[e] = b * cg;
+        for (int c = 0; c < nc; ++c) {
+            const int e = ebase + c;
+            const double dum = an[c] + A.lam * reg_diag(A, e);
+            const double cg = 1.0 / sqrt(dum);
+            A.cgfac[e] = cg;
+            const cd rg = reg_apply_par(A, par, e);
+            const cd b = cd{arx[c], ary[c]} - rg * A.lam;
+            A.rhs[e] = b * cg;
+        }
     }
 }
 
@@ -384,52 +428,91 @@ __global__ void k_cg_jv_reduce(CGArgs A)
 }
 
 // b_e = (sum_i conj(J_ie) (w o ap)_i + lam (R (cgfac o p))_e) * cgfac_e,
-// one warp per JH_COLS columns sharing the loads of w o ap.
-constexpr int JH_COLS = 4;
+// one warp per JH_COLS columns, a CTA of JH_NT / 32 warps.  Every warp reads
+// all of w o ap, so the CTA stages it in shared memory in chunks of
+// JH_CHUNK readings (cp.async, double-buffered): L2 serves w o ap once per
+// CTA instead of once per warp.  Lane l sums the rows in pairs
+// (l + 64 k, l + 64 k + 32), two pairs' loads in flight, then a rest of
+// single rows past the last pair: the same order for every chunk size.
+constexpr int JH_COLS = 4, JH_NT = 256, JH_CHUNK = 1024;
 
 template <int JP, int JM>
-__global__ void k_cg_jhv(CGArgs A)
+__global__ void __launch_bounds__(JH_NT) k_cg_jhv(CGArgs A)
 {
+    using RT = typename JRaw<JP, JM>::T;
+    __shared__ __align__(16) cd s_ap[2][JH_CHUNK];
     if (A.st->done) return;
-    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    const int ebase = gw * JH_COLS;
-    if (ebase >= A.M) return;
-    const int nc = min(JH_COLS, A.M - ebase);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int ebase = (blockIdx.x * (JH_NT / 32) + warp) * JH_COLS;
+    // warps past the last column still take part in the staging barriers
+    const int nc = max(0, min(JH_COLS, A.M - ebase));
+    const int N = A.N;
+    auto stage = [&](int buf, int r0) {
+        const int nr = min(JH_CHUNK, N - r0);
+        for (int t = threadIdx.x; t < nr; t += JH_NT) cp_async16(&s_ap[buf][t], A.ap + r0 + t);
+        cp_async_commit();
+    };
     double ax[JH_COLS], ay[JH_COLS];
 #pragma unroll
     for (int c = 0; c < JH_COLS; ++c) {
         ax[c] = 0.0;
         ay[c] = 0.0;
     }
-    // two rows per lane and step keep 2 JH_COLS loads of J in flight
-    int i = lane;
-    for (; i + 32 < A.N; i += 64) {
-        const cd w0 = A.ap[i], w1 = A.ap[i + 32];
-        cd j0[JH_COLS], j1[JH_COLS];
+    auto pair = [&](const RT (&j0)[JH_COLS], const RT (&j1)[JH_COLS], cd w0, cd w1) {
 #pragma unroll
         for (int c = 0; c < JH_COLS; ++c) {
-            j0[c] = (c < nc) ? jval<JP, JM>(A, ebase + c, i) : cd{0.0, 0.0};
-            j1[c] = (c < nc) ? jval<JP, JM>(A, ebase + c, i + 32) : cd{0.0, 0.0};
-        }
-#pragma unroll
-        for (int c = 0; c < JH_COLS; ++c) {
-            const cd t0 = conj(j0[c]) * w0, t1 = conj(j1[c]) * w1;
+            const cd t0 = conj(jcvt<JM>(j0[c])) * w0, t1 = conj(jcvt<JM>(j1[c])) * w1;
             ax[c] += t0.x + t1.x;
             ay[c] += t0.y + t1.y;
         }
-    }
-    for (; i < A.N; i += 32) {
-        const cd w = A.ap[i];
-        cd jv[JH_COLS];
+    };
+    auto ld = [&](RT (&dst)[JH_COLS], int i) {
 #pragma unroll
-        for (int c = 0; c < JH_COLS; ++c) jv[c] = (c < nc) ? jval<JP, JM>(A, ebase + c, i) : cd{0.0, 0.0};
-#pragma unroll
-        for (int c = 0; c < JH_COLS; ++c) {
-            const cd t = conj(jv[c]) * w;
-            ax[c] += t.x;
-            ay[c] += t.y;
+        for (int c = 0; c < JH_COLS; ++c) dst[c] = c < nc ? jraw<JP, JM>(A, ebase + c, i) : RT{};
+    };
+    stage(0, 0);
+    int buf = 0;
+    for (int r0 = 0; r0 < N; r0 += JH_CHUNK, buf ^= 1) {
+        if (r0 + JH_CHUNK < N) {
+            stage(buf ^ 1, r0 + JH_CHUNK);
+            cp_async_wait_group<1>();
+        } else {
+            cp_async_wait_group<0>();
         }
+        __syncthreads();
+        const int r1 = min(N, r0 + JH_CHUNK);
+        const cd* w = s_ap[buf] - r0;
+        int i = r0 + lane;
+        if (nc > 0) {
+            for (; i + 96 < r1; i += 128) {
+                RT j0[JH_COLS], j1[JH_COLS], j2[JH_COLS], j3[JH_COLS];
+                ld(j0, i);
+                ld(j1, i + 32);
+                ld(j2, i + 64);
+                ld(j3, i + 96);
+                pair(j0, j1, w[i], w[i + 32]);
+                pair(j2, j3, w[i + 64], w[i + 96]);
+            }
+            for (; i + 32 < r1; i += 64) {
+                RT j0[JH_COLS], j1[JH_COLS];
+                ld(j0, i);
+                ld(j1, i + 32);
+                pair(j0, j1, w[i], w[i + 32]);
+            }
+            for (; i < r1; i += 32) {
+                RT j0[JH_COLS];
+                ld(j0, i);
+#pragma unroll
+                for (int c = 0; c < JH_COLS; ++c) {
+                    const cd t = conj(jcvt<JM>(j0[c])) * w[i];
+                    ax[c] += t.x;
+                    ay[c] += t.y;
+                }
+            }
+        }
+        __syncthreads();   // readers of `buf` are done before it is staged again
     }
+    if (nc == 0) return;
 #pragma unroll
     for (int c = 0; c < JH_COLS; ++c) {
         ax[c] = warp_allsum(ax[c]);
@@ -447,6 +530,200 @@ __global__ void k_cg_jhv(CGArgs A)
         const cd rp = reg_apply_cg(A, A.p, e);
         const cd b = cd{bx, by} + rp * A.lam;
         A.bvec[e] = b * A.cgfac[e];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Fused matvec: b = (J^H (w o J p) + lam R (cgfac o p)) o cgfac from ONE read
+// of J.  The kernel is persistent, one CTA per SM (cooperative launch, so
+// every CTA is resident).  CTA c owns the column range [c per, (c+1) per);
+// the readings are cut into row blocks of CGF_R.  Per block, the CTA copies
+// its tile of J (per columns x CGF_R readings, complex64, 8-byte cp.async,
+// CGF_S stages in flight) into shared memory and
+//   1. forms its partial sums of (J p)_i over its columns and publishes
+//      them to a ring slot; the CTA that arrives last at the slot adds the
+//      grid's partials in CTA order (deterministic), multiplies by w and
+//      releases the slot with the block's ticket;
+//   2. one block later (the other CTAs' partials have arrived meanwhile)
+//      waits for the previous block's ticket and accumulates
+//      conj(J_ie) (w o J p)_i into its columns from the tile still held in
+//      shared memory.
+// A column's sum over the readings is formed in reading order, every
+// reading's sum over the columns in a fixed order.  Waits are bounded:
+// a wait that gives up sets *ferr and every CTA leaves.
+// Tile layout: element (column e, reading r) of a stage at e * CGF_R +
+// (r ^ (e & 15)), so the copies, the row-wise reads of step 1 and the
+// column-wise reads of step 2 are all free of bank conflicts.
+constexpr long CGF_POLL_LIMIT = 1L << 21;
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem_src) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];\n" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;\n" ::"l"(p), "l"(v) : "memory");
+}
+
+__device__ __forceinline__ cd ldcg_cd(const cd* p)
+{
+    const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+    return cd{v.x, v.y};
+}
+
+__device__ __forceinline__ void stcg_cd(cd* p, cd v) { __stcg(reinterpret_cast<double2*>(p), make_double2(v.x, v.y)); }
+
+// Thread 0: wait until the slot's ticket reaches `want`; false when the wait
+// gave up (or another CTA's did).
+__device__ bool cgf_wait(const CGArgs& A, const unsigned long long* flag, unsigned long long want)
+{
+    long polls = 0;
+    while (ld_acquire_u64(flag) < want) {
+        if (*(volatile int*)A.ferr) return false;
+        if (++polls > CGF_POLL_LIMIT) {
+            atomicExch(A.ferr, 1);
+            return false;
+        }
+        __nanosleep(64);
+    }
+    return true;
+}
+
+// Issue the copies of row block b into stage `st` (rows past N read as 0).
+__device__ __forceinline__ void cgf_load(const CGArgs& A, cf* T, int e0, int ne, int b)
+{
+    const int i0 = b * CGF_R, nr = min(CGF_R, A.N - i0);
+    const cf* J = static_cast<const cf*>(A.J);
+    for (int idx = threadIdx.x; idx < ne * CGF_R; idx += CGF_NT) {
+        const int e = idx >> 4, r = idx & 15;
+        cf* dst = T + e * CGF_R + (r ^ (e & 15));
+        if (r < nr) cp_async8(dst, J + (size_t)(e0 + e) * A.N + i0 + r);
+        else *dst = cf{0.f, 0.f};
+    }
+}
+
+template <int JM>
+__global__ void __launch_bounds__(CGF_NT, 1) k_cg_fused(CGArgs A)
+{
+    extern __shared__ __align__(16) unsigned char cgf_smem[];
+    __shared__ int s_last, s_ok;   // separate words: a slow warp may still read one after a barrier
+    if (A.st->done) return;
+    const int c = blockIdx.x, G = gridDim.x, tid = threadIdx.x;
+    const int per = A.fper, e0 = c * per, ne = max(0, min(per, A.M - e0));
+    const int nblk = (A.N + CGF_R - 1) / CGF_R;
+    cf* tiles = reinterpret_cast<cf*>(cgf_smem);
+    cd* pcs = reinterpret_cast<cd*>(tiles + (size_t)2 * CGF_S * per * CGF_R);
+    cd* red = pcs + per;                  // [CGF_NT / CGF_R][CGF_R]
+    cd* sv = red + CGF_NT;                // [CGF_R]
+    const unsigned long long tbase = *A.fepoch * (unsigned long long)nblk;
+
+    for (int t = tid; t < ne; t += CGF_NT) pcs[t] = A.p[e0 + t] * A.cgfac[e0 + t];
+    // copy group g (one per iteration, CGF_S iterations ahead) holds the tile
+    // of row block g for step 1 (stage g % CGF_S, from HBM) and that of
+    // block g - L for step 2 (stage CGF_S + (g - L) % CGF_S, read again
+    // while it is still in L2); L >= CGF_S, so the first groups hold no
+    // step-2 tile
+    const int L = A.flag_lag;
+    auto vstage = [&](int blk) { return tiles + (size_t)(blk % CGF_S) * per * CGF_R; };
+    auto hstage = [&](int blk) { return tiles + (size_t)(CGF_S + blk % CGF_S) * per * CGF_R; };
+#pragma unroll
+    for (int s = 0; s < CGF_S; ++s) {
+        if (s < nblk) cgf_load(A, vstage(s), e0, ne, s);
+        cp_async_commit();
+    }
+    cd acc{0.0, 0.0};
+    const int g = tid >> 4, r = tid & 15;   // step 1: column group g, reading r
+    bool ok = true;
+    for (int b = 0; b < nblk + L; ++b) {
+        cp_async_wait_group<CGF_S - 1>();
+        __syncthreads();
+        if (b < nblk) {
+            // 1. partial sums of (J p)_i over this CTA's columns
+            const cf* T = vstage(b);
+            cd s{0.0, 0.0};
+            for (int j = g; j < ne; j += CGF_NT / CGF_R) s += pcs[j] * jcvt<JM>(T[j * CGF_R + (r ^ (j & 15))]);
+            red[g * CGF_R + r] = s;
+            __syncthreads();
+            const int slot = b % CGF_Q;
+            if (tid < CGF_R) {
+                cd t{0.0, 0.0};
+                for (int q = 0; q < CGF_NT / CGF_R; ++q) t += red[q * CGF_R + tid];
+                stcg_cd(A.fpart + ((size_t)slot * G + c) * CGF_R + tid, t);
+                __threadfence();
+            }
+            __syncthreads();
+            if (tid == 0) s_last = atomicAdd(A.fcnt + slot, 1) == G - 1;
+            __syncthreads();
+            if (s_last) {
+                // the grid's partials of block b, added in CTA order
+                __threadfence();
+                cd t{0.0, 0.0};
+                for (int q = g; q < G; q += CGF_NT / CGF_R) t += ldcg_cd(A.fpart + ((size_t)slot * G + q) * CGF_R + r);
+                red[g * CGF_R + r] = t;
+                __syncthreads();
+                if (tid < CGF_R) {
+                    cd ap{0.0, 0.0};
+                    for (int q = 0; q < CGF_NT / CGF_R; ++q) ap += red[q * CGF_R + tid];
+                    const int i = b * CGF_R + tid;
+                    const cd v = i < A.N ? ap * A.wd[i] : cd{0.0, 0.0};
+                    if (i < A.N) A.ap[i] = v;
+                    stcg_cd(A.fv + (size_t)slot * CGF_R + tid, v);
+                    __threadfence();
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    A.fcnt[slot] = 0;
+                    __threadfence();
+                    st_release_u64(A.fflag + slot, tbase + (unsigned long long)b + 1ull);
+                }
+            }
+        }
+        const int h = b - L;
+        if (h >= 0) {
+            // 2. block h's w o (J p) (published while this CTA went on with
+            // step 1 of later blocks), conj(J) times it into the columns
+            const int slot = h % CGF_Q;
+            if (tid == 0) {
+                s_ok = cgf_wait(A, A.fflag + slot, tbase + (unsigned long long)h + 1ull);
+                __threadfence();
+            }
+            __syncthreads();
+            if (!s_ok) {
+                ok = false;
+                break;
+            }
+            if (tid < CGF_R) sv[tid] = ldcg_cd(A.fv + (size_t)slot * CGF_R + tid);
+            __syncthreads();
+            if (tid < ne) {
+                const cf* T = hstage(h) + tid * CGF_R;
+#pragma unroll
+                for (int q = 0; q < CGF_R; ++q) acc += conj(jcvt<JM>(T[q ^ (tid & 15)])) * sv[q];
+            }
+        }
+        __syncthreads();
+        // the stages used in this iteration take the tiles of group b + CGF_S
+        const int gn = b + CGF_S;
+        if (gn < nblk) cgf_load(A, vstage(gn), e0, ne, gn);
+        if (gn - L >= 0 && gn - L < nblk) cgf_load(A, hstage(gn - L), e0, ne, gn - L);
+        cp_async_commit();
+    }
+    if (!ok) {
+        cp_async_wait_all();
+        return;
+    }
+    if (tid < ne) {
+        const int e = e0 + tid;
+        const cd rp = reg_apply_cg(A, A.p, e);
+        A.bvec[e] = (acc + rp * A.lam) * A.cgfac[e];
     }
 }
 
@@ -473,6 +750,7 @@ __device__ void cg_end_body(const CGArgs& A)
         st->dr1 = st->dr;
         A.cgres[k] = (double)(float)(A.eps * st->dr / st->dr0);
         st->k = k + 1;
+        if (A.fused) *A.fepoch += 1;
         if (k + 1 > A.ncgmax) {
             st->done = 1;
             st->ncg = A.ncgmax;
@@ -790,17 +1068,39 @@ __global__ void __launch_bounds__(CGL_JH_NT, 2) k_cgl_jhv(CGLArgs L)
 
 void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd* par, cudaStream_t s)
 {
-    const int threads = 256, warps = threads / 32;
-    CRT_CG_DISPATCH(k_cg_setup, (a.M + warps - 1) / warps, threads, s, a, dat, sigmaa, par);
+    const int cols_per_block = (SU_NT / 32) * SU_COLS;
+    CRT_CG_DISPATCH(k_cg_setup, (a.M + cols_per_block - 1) / cols_per_block, SU_NT, s, a, dat, sigmaa, par);
 }
 
 void launch_cg_init(const CGArgs& a, cudaStream_t s) { k_cg_init<<<1, VEC_NT, 0, s>>>(a); }
+
+bool cg_fused_fits(const CGArgs& a, int grid, size_t smem_max)
+{
+    if (a.jprec != 1 || a.jmode == 1 || grid < 1) return false;
+    const int per = (a.M + grid - 1) / grid;
+    return per <= CGF_NT && cg_fused_smem(per) <= smem_max;
+}
+
+namespace {
+void launch_cg_fused(const CGArgs& a, cudaStream_t s)
+{
+    const int grid = (a.M + a.fper - 1) / a.fper;
+    const size_t smem = cg_fused_smem(a.fper);
+    void* args[] = {const_cast<CGArgs*>(&a)};
+    if (a.jmode == 2) {
+        cudaFuncSetAttribute(k_cg_fused<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaLaunchCooperativeKernel((const void*)k_cg_fused<2>, grid, CGF_NT, args, smem, s);
+    } else {
+        cudaFuncSetAttribute(k_cg_fused<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaLaunchCooperativeKernel((const void*)k_cg_fused<0>, grid, CGF_NT, args, smem, s);
+    }
+}
+}  // namespace
 
 void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* gnn, cd* zb, cudaStream_t s)
 {
     const int nt = 256;
     dim3 gjv((a.N + JV_NT - 1) / JV_NT, a.nsplit);
-    const int warps = nt / 32;
     for (int it = 0; it < iters; ++it) {
         if (a.pc) {
             if (spc && gnn) {
@@ -815,10 +1115,14 @@ void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* g
         } else {
             k_cg_begin<<<1, VEC_NT, 0, s>>>(a);
         }
-        CRT_CG_DISPATCH(k_cg_jv, gjv, JV_NT, s, a);
-        k_cg_jv_reduce<<<(a.N + nt - 1) / nt, nt, 0, s>>>(a);
-        const int cols_per_block = warps * JH_COLS;
-        CRT_CG_DISPATCH(k_cg_jhv, (a.M + cols_per_block - 1) / cols_per_block, nt, s, a);
+        if (a.fused) {
+            launch_cg_fused(a, s);
+        } else {
+            CRT_CG_DISPATCH(k_cg_jv, gjv, JV_NT, s, a);
+            k_cg_jv_reduce<<<(a.N + nt - 1) / nt, nt, 0, s>>>(a);
+            const int cols_per_block = (JH_NT / 32) * JH_COLS;
+            CRT_CG_DISPATCH(k_cg_jhv, (a.M + cols_per_block - 1) / cols_per_block, JH_NT, s, a);
+        }
         k_cg_end<<<1, VEC_NT, 0, s>>>(a);
     }
 }

@@ -41,7 +41,29 @@ struct CGArgs {
     // zb holds the base's output (nullptr: the identity, i.e. r)
     int pc_gnn;
     const cd* zb;
+    // fused matvec (fused = 1, launch_cg_iterations): J p and J^H (w o J p)
+    // from one read of J, see k_cg_fused
+    int fused;
+    int fper;                     // columns per CTA
+    cd* fpart;                    // [CGF_Q][grid][CGF_R] per-CTA partial sums of a row block
+    cd* fv;                       // [CGF_Q][CGF_R] w o (J p) of a row block
+    int* fcnt;                    // [CGF_Q] arrivals at a ring slot
+    unsigned long long* fflag;    // [CGF_Q] ticket of the block whose w o (J p) a slot holds
+    unsigned long long* fepoch;   // [1] advanced by every iteration tail (tickets stay unique)
+    int* ferr;                    // [1] set when a wait gave up
+    int flag_lag;                 // row blocks between a block's two uses (CGF_S .. CGF_Q - 1)
 };
+
+// Fused matvec geometry: row blocks of CGF_R readings, a ring of CGF_Q
+// reduction slots, CGF_S shared-memory stages of a CTA's J tile for each of
+// the two uses of a block.
+constexpr int CGF_R = 16, CGF_Q = 32, CGF_S = 2, CGF_NT = 512;
+// dynamic shared memory of k_cg_fused for `per` columns per CTA
+inline size_t cg_fused_smem(int per)
+{
+    return (size_t)2 * CGF_S * per * CGF_R * 8 + (size_t)per * 16 + (size_t)(CGF_NT / CGF_R) * CGF_R * 16 +
+           CGF_R * 16;
+}
 
 // The learned correction is switched off for the rest of a solve when it
 // yields a non-descent direction (Re r^H z <= 0) or when |r|^2 has not
@@ -61,6 +83,10 @@ void launch_cg_init(const CGArgs& a, cudaStream_t s);
 // `spc` (crt_spc.h), the learned correction `gnn` (crt_gnn.h) on top of it
 // (zb holds the block result) or on top of the identity; either may be null.
 void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* gnn, cd* zb, cudaStream_t s);
+// Whether the fused matvec can run for these arguments on `grid` CTAs of
+// at most `smem_max` bytes of shared memory: complex64 J (jprec 1, jmode 0
+// or 2) and the CTA's tile stages fitting.
+bool cg_fused_fits(const CGArgs& a, int grid, size_t smem_max);
 // update.f90:300-351: dpar *= cgfac (lfpi: (0, Re dpar) first), par += step
 // dpar, bdpar = step * sum |dpar|^2.
 void launch_cg_finish(const CGArgs& a, int lfpi, double step, cd* par, double* bdpar, cudaStream_t s);

@@ -653,9 +653,9 @@ def test_crmod_driver_writes_sensitivity_and_potential_files(tmp_path):
         np.testing.assert_allclose(pv[:, 2] + 1j * pv[:, 3], ref, rtol=1e-6, atol=1e-6 * np.abs(ref).max())
 
 
-def _five_point_cg_case(nx, nz, ldc=False, weight=1.0):
+def _five_point_cg_case(nx, nz, ldc=False, weight=1.0, precision=None):
     from crtomo_stable_b200 import regularization, synth
-    from crtomo_stable_b200.lib import Context
+    from crtomo_stable_b200.lib import PREC_FP64, Context
     xs = np.arange(nx + 1, dtype=np.float64) - 10.0
     depths = synth.graded_depths(nz, 0.4, 1.04)
     mesh = synth.structured_mesh(xs, depths, triangles=False)
@@ -664,7 +664,7 @@ def _five_point_cg_case(nx, nz, ldc=False, weight=1.0):
     strnr, vnr = synth.encode(synth.dipole_dipole(nel, (1, 2), 6))
     rng = np.random.default_rng(11)
     sig = synth.sigma_from(np.exp(rng.uniform(np.log(20), np.log(200), mesh.elanz)), -rng.uniform(1, 20, mesh.elanz))
-    ctx = Context(mesh, enr, strnr, vnr)
+    ctx = Context(mesh, enr, strnr, vnr, precision=PREC_FP64 if precision is None else precision)
     _, sa = ctx.forward(sig, ldc=ldc)
     dat = sa + 0.02 * rng.standard_normal(len(sa))
     wmatd = np.full(len(sa), weight / 0.02 ** 2)
@@ -700,3 +700,26 @@ def test_segmented_block_preconditioner_matches_single_chain(nx, nz, monkeypatch
         a, b = out["segmented", f], out["single", f]
         assert abs(a["ncg"] - b["ncg"]) <= 1, (f, a["ncg"], b["ncg"])
         np.testing.assert_allclose(a["dpar"], b["dpar"], rtol=1e-5, atol=1e-5 * np.abs(b["dpar"]).max())
+
+
+def test_fused_cg_matvec_matches_two_pass(monkeypatch):
+    """The fused matvec (one read of J per iteration: per-CTA column
+    ranges, row blocks reduced across the grid) computes the same operator
+    as the two-pass kernels with other summation orders: the complex64-J
+    CG takes the same iterations (+-1) and gives the same update, in the
+    Jacobi form (hundreds of iterations), the block form and the final
+    phase improvement's real-part form."""
+    from crtomo_stable_b200.lib import PREC_MIXED, PRECOND_BLOCK
+    out = {}
+    for form in ("fused", "two-pass"):
+        monkeypatch.setenv("CRT_B200_CG_FUSED", "1" if form == "fused" else "0")
+        ctx, par, sa0, lam, Context = _five_point_cg_case(60, 40, precision=PREC_MIXED)
+        for name, prm in (("jacobi", Context.params(lam, eps=1e-12, ncgmax=3000)),
+                          ("block", Context.params(lam, eps=1e-12, ncgmax=3000, precond=PRECOND_BLOCK)),
+                          ("fpi", Context.params(lam, eps=1e-12, ncgmax=3000, lfpi=True))):
+            out[form, name] = ctx.update(prm, par, sigmaa=sa0)
+        ctx.close()
+    for name in ("jacobi", "block", "fpi"):
+        a, b = out["fused", name], out["two-pass", name]
+        assert abs(a["ncg"] - b["ncg"]) <= 1, (name, a["ncg"], b["ncg"])
+        np.testing.assert_allclose(a["dpar"], b["dpar"], rtol=1e-6, atol=1e-6 * np.abs(b["dpar"]).max())
