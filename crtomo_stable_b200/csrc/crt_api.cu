@@ -108,6 +108,7 @@ struct crt_ctx {
     std::string spc_why;
     cd *d_z = nullptr, *d_rold = nullptr, *d_zb = nullptr;
     CGState* d_live = nullptr;   // a never-done CG state for preconditioner applications outside the CG
+    double* d_vred = nullptr;    // partial sums of the CG head and tail
     // fused matvec of the CG (k_cg_fused): reduction ring, tickets, error word
     unsigned char* d_cgf = nullptr;
     size_t cgf_bytes = 0;
@@ -410,7 +411,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega, ctx->d_cgf,
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega, ctx->d_cgf, ctx->d_vred,
                     ctx->d_dc_rows, ctx->d_dc_ptr, ctx->d_dc_ent, ctx->d_dc_node, ctx->d_bdir};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1558,7 +1559,7 @@ int ensure_cg_buffers(crt_ctx* ctx, int ncgmax)
                   dalloc(ctx, &ctx->d_cgst, (size_t)1) && dalloc(ctx, &ctx->d_bdpar, (size_t)1) &&
                   dalloc(ctx, &ctx->d_par, (size_t)M) && dalloc(ctx, &ctx->d_z, (size_t)M) &&
                   dalloc(ctx, &ctx->d_rold, (size_t)M) && dalloc(ctx, &ctx->d_zb, (size_t)M) &&
-                  dalloc(ctx, &ctx->d_live, (size_t)1);
+                  dalloc(ctx, &ctx->d_live, (size_t)1) && dalloc(ctx, &ctx->d_vred, (size_t)32 * 8);
         if (!ok) return CRT_ERR_ALLOC;
         if (cudaMemset(ctx->d_live, 0, sizeof(CGState)) != cudaSuccess) return CRT_ERR_CUDA;
     }
@@ -1602,6 +1603,7 @@ CGArgs make_cg_args(crt_ctx* ctx, const crt_cg_params* prm)
     a.rold = ctx->d_rold;
     a.pc_gnn = 0;
     a.zb = nullptr;
+    a.vred = ctx->d_vred;
     return a;
 }
 
@@ -1708,7 +1710,7 @@ int update_device(crt_ctx* ctx, const crt_cg_params* prm, const cd* d_sigmaa, in
         int it = std::min(batch, prm->ncgmax - done_iters);
         launch_cg_iterations(a, it, use_block ? &ctx->spc : nullptr, use_gnn ? &ctx->gnn : nullptr, ctx->d_zb,
                              ctx->st);
-        ctx->launches += ((a.fused ? 3 : 5) + (a.pc ? 1 : 0) + (use_block ? 2 : 0) + (use_gnn ? 7 : 0)) * it;
+        ctx->launches += ((a.fused ? 5 : 7) + (a.pc ? 1 : 0) + (use_block ? 2 : 0) + (use_gnn ? 7 : 0)) * it;
         done_iters += it;
         CK(cudaMemcpyAsync(&hs, ctx->d_cgst, sizeof(CGState), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));

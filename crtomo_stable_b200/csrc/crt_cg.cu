@@ -11,9 +11,12 @@
 //   k_cg_jv  : ap_i = sum_e p_e J_ie cgfac_e     (threads over i, coalesced,
 //              columns split into nsplit ranges, deterministic reduction)
 //   k_cg_jhv : b_e  = (sum_i conj(J_ie) w_i ap_i + lam (R (cgfac o p))_e) cgfac_e
-//              (one warp per column)
-// The O(M) vector work and the FP64 dot products run in one CTA each; the
-// stop rule is evaluated on the device, so a batch of iterations can be
+//              (one warp per 4 columns, w o ap staged per CTA)
+// The FP64 dot products of an iteration's head and tail are formed by 32
+// one-warp CTAs in the order of one 1024-thread CTA (the last to arrive adds
+// the partials and takes the scalar step), the O(M) vector updates by
+// grid-wide kernels; the lambda-batched solve keeps one CTA per candidate.
+// The stop rule is evaluated on the device, so a batch of iterations can be
 // queued without host round trips.  Real systems (DC, final phase
 // improvement) use the same kernels with zero imaginary parts, which keeps
 // the real arithmetic of cjggdc exact.
@@ -257,6 +260,77 @@ __device__ void cg_init_body(const CGArgs& A)
 
 __global__ void __launch_bounds__(VEC_NT) k_cg_init(CGArgs A) { cg_init_body(A); }
 
+// The head's scalar step (one thread): stop rule on dr = |r|^2 and
+// beta = dr / dr1; returns 1 when the solve stops.
+__device__ int head_decide(const CGArgs& A, double dr)
+{
+    CGState* st = A.st;
+    const int k = st->k;
+    int stop = 0;
+    if (k == 1) {
+        st->dr0 = dr * A.eps;
+        // the real solver (cjggdc) tests the stop rule at k = 1 as well
+        if (A.jmode != 0 && dr <= st->dr0) stop = 1;
+    } else {
+        if (dr <= st->dr0) stop = 1;
+        st->beta = dr / st->dr1;
+    }
+    if (stop) {
+        st->done = 1;
+        st->ncg = k - 1;
+    }
+    st->dr = dr;
+    st->num = dr;
+    return stop;
+}
+
+// The preconditioned head's scalar step (one thread), see cg_begin_pc_body;
+// returns 1 when the solve stops, *use_base whether the direction comes
+// from the base preconditioner.
+__device__ int head_pc_decide(const CGArgs& A, double dr, double gam_z, double gold_z, double gam_b, double gold_b,
+                              int* use_base_out)
+{
+    CGState* st = A.st;
+    const bool guard = A.pc_gnn != 0;
+    const bool off0 = guard && st->no_gnn;
+    const int k = st->k;
+    int stop = 0;
+    int use_base = off0 ? 1 : 0, restart = 0;
+    if (guard && !off0) {
+        bool bad = !(gam_z > 0.0);
+        if (k == 1) st->dr_chk = dr;
+        else if ((k - 1) % GNN_GUARD_WINDOW == 0) {
+            if (dr > 0.5 * st->dr_chk) bad = true;
+            st->dr_chk = dr;
+        }
+        if (bad) {
+            st->no_gnn = 1;
+            use_base = 1;
+            restart = 1;
+        }
+    }
+    const double gam = use_base ? gam_b : gam_z;
+    const double gold = use_base ? gold_b : gold_z;
+    double beta = 0.0;
+    if (k == 1) {
+        st->dr0 = dr * A.eps;
+        if (A.jmode != 0 && dr <= st->dr0) stop = 1;
+    } else {
+        if (dr <= st->dr0) stop = 1;
+        if (!restart) beta = (gam - gold) / st->gam;
+    }
+    if (stop) {
+        st->done = 1;
+        st->ncg = k - 1;
+    }
+    st->dr = dr;
+    st->beta = beta;
+    st->gam = gam;
+    st->num = gam;
+    *use_base_out = use_base;
+    return stop;
+}
+
 // Iteration head: dr = |r|^2, stop rule, beta, p = r + beta p.
 __device__ void cg_begin_body(const CGArgs& A)
 {
@@ -269,30 +343,12 @@ __device__ void cg_begin_body(const CGArgs& A)
     const double dr = block_sum<VEC_NT>(v, red);
     const int k = st->k;
     double beta = 0.0;
-    if (threadIdx.x == 0) {
-        s_stop = 0;
-        if (k == 1) {
-            st->dr0 = dr * A.eps;
-            // the real solver (cjggdc) tests the stop rule at k = 1 as well
-            if (A.jmode != 0 && dr <= st->dr0) s_stop = 1;
-        } else {
-            if (dr <= st->dr0) s_stop = 1;
-            st->beta = dr / st->dr1;
-        }
-        if (s_stop) {
-            st->done = 1;
-            st->ncg = k - 1;
-        }
-        st->dr = dr;
-        st->num = dr;
-    }
+    if (threadIdx.x == 0) s_stop = head_decide(A, dr);
     __syncthreads();
     if (s_stop) return;
     beta = (k == 1) ? 0.0 : st->beta;
     for (int e = threadIdx.x; e < A.M; e += VEC_NT) A.p[e] = A.r[e] + A.p[e] * beta;
 }
-
-__global__ void __launch_bounds__(VEC_NT) k_cg_begin(CGArgs A) { cg_begin_body(A); }
 
 // Preconditioned head: z (the preconditioner's output) is in A.z.  The stop
 // rule is the reference's (|r|^2 against eps |r0|^2); beta is the flexible
@@ -329,42 +385,10 @@ __device__ void cg_begin_pc_body(const CGArgs& A)
     const double gold_z = block_sum<VEC_NT>(go, red);
     const double gam_b = guard ? block_sum<VEC_NT>(gb, red) : 0.0;
     const double gold_b = guard ? block_sum<VEC_NT>(gob, red) : 0.0;
-    const int k = st->k;
     if (threadIdx.x == 0) {
-        s_stop = 0;
-        int use_base = off0 ? 1 : 0, restart = 0;
-        if (guard && !off0) {
-            bool bad = !(gam_z > 0.0);
-            if (k == 1) st->dr_chk = dr;
-            else if ((k - 1) % GNN_GUARD_WINDOW == 0) {
-                if (dr > 0.5 * st->dr_chk) bad = true;
-                st->dr_chk = dr;
-            }
-            if (bad) {
-                st->no_gnn = 1;
-                use_base = 1;
-                restart = 1;
-            }
-        }
-        const double gam = use_base ? gam_b : gam_z;
-        const double gold = use_base ? gold_b : gold_z;
-        double beta = 0.0;
-        if (k == 1) {
-            st->dr0 = dr * A.eps;
-            if (A.jmode != 0 && dr <= st->dr0) s_stop = 1;
-        } else {
-            if (dr <= st->dr0) s_stop = 1;
-            if (!restart) beta = (gam - gold) / st->gam;
-        }
-        if (s_stop) {
-            st->done = 1;
-            st->ncg = k - 1;
-        }
-        st->dr = dr;
-        st->beta = beta;
-        st->gam = gam;
-        st->num = gam;
-        s_beta = beta;
+        int use_base = 0;
+        s_stop = head_pc_decide(A, dr, gam_z, gold_z, gam_b, gold_b, &use_base);
+        s_beta = st->beta;
         s_base = use_base;
     }
     __syncthreads();
@@ -378,8 +402,6 @@ __device__ void cg_begin_pc_body(const CGArgs& A)
         A.rold[e] = r;
     }
 }
-
-__global__ void __launch_bounds__(VEC_NT) k_cg_begin_pc(CGArgs A) { cg_begin_pc_body(A); }
 
 // ap partial sums over a column range: thread per reading.  The block stages
 // p o cgfac for JV_CHUNK columns in shared memory and keeps JV_UNROLL
@@ -727,6 +749,22 @@ __global__ void __launch_bounds__(CGF_NT, 1) k_cg_fused(CGArgs A)
     }
 }
 
+// The tail's scalar step (one thread) once alpha is known.
+__device__ void tail_decide(const CGArgs& A, double alpha)
+{
+    CGState* st = A.st;
+    const int k = st->k;
+    st->alpha = alpha;
+    st->dr1 = st->dr;
+    A.cgres[k] = (double)(float)(A.eps * st->dr / st->dr0);
+    st->k = k + 1;
+    if (A.fused) *A.fepoch += 1;
+    if (k + 1 > A.ncgmax) {
+        st->done = 1;
+        st->ncg = A.ncgmax;
+    }
+}
+
 // Iteration tail: alpha = dr / Re(p^H b), dpar += alpha p, r -= alpha b.
 __device__ void cg_end_body(const CGArgs& A)
 {
@@ -744,21 +782,142 @@ __device__ void cg_end_body(const CGArgs& A)
         A.dpar[e] = A.dpar[e] + A.p[e] * alpha;
         A.r[e] = A.r[e] - A.bvec[e] * alpha;
     }
-    if (threadIdx.x == 0) {
-        const int k = st->k;
-        st->alpha = alpha;
-        st->dr1 = st->dr;
-        A.cgres[k] = (double)(float)(A.eps * st->dr / st->dr0);
-        st->k = k + 1;
-        if (A.fused) *A.fepoch += 1;
-        if (k + 1 > A.ncgmax) {
-            st->done = 1;
-            st->ncg = A.ncgmax;
+    if (threadIdx.x == 0) tail_decide(A, alpha);
+}
+
+// ---------------------------------------------------------------------------
+// Head and tail of one solve across the grid.  CTA w (VEC_NT / 32 CTAs of one
+// warp) forms the partial sums of warp w of the one-CTA form, element by
+// element in the same order; the CTA that arrives last adds the partials as
+// that form's final warp does and takes the scalar step, so every sum and
+// every scalar is bit for bit the one-CTA form's.  The vector updates then
+// run as grid-wide kernels.
+constexpr int VS_CTAS = VEC_NT / 32, VS_UPD_NT = 256;
+
+// Lane 0 publishes q[0 .. n) of this CTA; true (in every lane) for the CTA
+// that arrives last, which then finds the totals in tot[].
+template <int n>
+__device__ bool vs_gather(const CGArgs& A, const double (&q)[n], double (&tot)[n])
+{
+    const int lane = threadIdx.x;
+    int last = 0;
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < n; ++j) __stcg(A.vred + blockIdx.x * 8 + j, q[j]);
+        __threadfence();
+        last = atomicAdd(&A.st->vcnt, 1) == VS_CTAS - 1;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return false;
+    __threadfence();
+#pragma unroll
+    for (int j = 0; j < n; ++j) tot[j] = warp_sum(__ldcg(A.vred + lane * 8 + j));
+    if (lane == 0) A.st->vcnt = 0;
+    return true;
+}
+
+__global__ void __launch_bounds__(32) k_cg_head_sums(CGArgs A)
+{
+    if (A.st->done) return;
+    double v = 0.0;
+    for (int e = blockIdx.x * 32 + threadIdx.x; e < A.M; e += VEC_NT) v += cabs2(A.r[e]);
+    const double q[1] = {warp_sum(v)};
+    double tot[1];
+    if (vs_gather<1>(A, q, tot) && threadIdx.x == 0) head_decide(A, tot[0]);
+}
+
+__global__ void __launch_bounds__(VS_UPD_NT) k_cg_head_update(CGArgs A)
+{
+    const CGState* st = A.st;
+    if (st->done) return;
+    const int e = blockIdx.x * VS_UPD_NT + threadIdx.x;
+    if (e >= A.M) return;
+    const double beta = (st->k == 1) ? 0.0 : st->beta;
+    A.p[e] = A.r[e] + A.p[e] * beta;
+}
+
+__global__ void __launch_bounds__(32) k_cg_head_pc_sums(CGArgs A)
+{
+    CGState* st = A.st;
+    if (st->done) return;
+    const bool guard = A.pc_gnn != 0;
+    const bool off0 = guard && st->no_gnn;
+    double v = 0.0, g = 0.0, go = 0.0, gb = 0.0, gob = 0.0;
+    for (int e = blockIdx.x * 32 + threadIdx.x; e < A.M; e += VEC_NT) {
+        const cd r = A.r[e], ro = A.rold[e];
+        v += cabs2(r);
+        if (!off0) {
+            const cd z = A.z[e];
+            g += r.x * z.x + r.y * z.y;
+            go += ro.x * z.x + ro.y * z.y;
         }
+        if (guard) {
+            const cd b = A.zb ? A.zb[e] : r;
+            gb += r.x * b.x + r.y * b.y;
+            gob += ro.x * b.x + ro.y * b.y;
+        }
+    }
+    const double q[5] = {warp_sum(v), warp_sum(g), warp_sum(go), warp_sum(gb), warp_sum(gob)};
+    double tot[5];
+    if (vs_gather<5>(A, q, tot) && threadIdx.x == 0) {
+        int use_base = 0;
+        head_pc_decide(A, tot[0], tot[1], tot[2], guard ? tot[3] : 0.0, guard ? tot[4] : 0.0, &use_base);
+        st->use_base = use_base;
     }
 }
 
-__global__ void __launch_bounds__(VEC_NT) k_cg_end(CGArgs A) { cg_end_body(A); }
+__global__ void __launch_bounds__(VS_UPD_NT) k_cg_head_pc_update(CGArgs A)
+{
+    const CGState* st = A.st;
+    if (st->done) return;
+    const int e = blockIdx.x * VS_UPD_NT + threadIdx.x;
+    if (e >= A.M) return;
+    const double beta = st->beta;
+    const cd r = A.r[e];
+    const cd z = st->use_base ? (A.zb ? A.zb[e] : r) : A.z[e];
+    A.p[e] = z + A.p[e] * beta;
+    A.rold[e] = r;
+}
+
+__global__ void __launch_bounds__(32) k_cg_tail_sums(CGArgs A)
+{
+    CGState* st = A.st;
+    if (st->done) return;
+    double v = 0.0;
+    for (int e = blockIdx.x * 32 + threadIdx.x; e < A.M; e += VEC_NT) {
+        const cd pp = A.p[e], bb = A.bvec[e];
+        v += pp.x * bb.x + pp.y * bb.y;
+    }
+    const double q[1] = {warp_sum(v)};
+    double tot[1];
+    if (vs_gather<1>(A, q, tot) && threadIdx.x == 0) {
+        tail_decide(A, st->num / tot[0]);
+        st->pending = 1;
+    }
+}
+
+// dpar += alpha p, r -= alpha b when the tail sums of this iteration ran
+// (they may also have ended the solve at ncgmax); the last CTA to finish
+// clears the flag.
+__global__ void __launch_bounds__(VS_UPD_NT) k_cg_tail_update(CGArgs A)
+{
+    __shared__ int s_go;
+    CGState* st = A.st;
+    if (threadIdx.x == 0) s_go = st->pending;
+    __syncthreads();
+    if (!s_go) return;
+    const double alpha = st->alpha;
+    const int e = blockIdx.x * VS_UPD_NT + threadIdx.x;
+    if (e < A.M) {
+        A.dpar[e] = A.dpar[e] + A.p[e] * alpha;
+        A.r[e] = A.r[e] - A.bvec[e] * alpha;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && atomicAdd(&st->ucnt, 1) == (int)gridDim.x - 1) {
+        st->ucnt = 0;
+        st->pending = 0;
+    }
+}
 
 __device__ void cg_finish_body(const CGArgs& A, int lfpi, double step, const cd* par_in, cd* par,
                                double* bdpar)
@@ -1101,6 +1260,7 @@ void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* g
 {
     const int nt = 256;
     dim3 gjv((a.N + JV_NT - 1) / JV_NT, a.nsplit);
+    const int gvec = (a.M + VS_UPD_NT - 1) / VS_UPD_NT;
     for (int it = 0; it < iters; ++it) {
         if (a.pc) {
             if (spc && gnn) {
@@ -1111,9 +1271,11 @@ void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* g
             } else {
                 launch_gnn_apply(*gnn, a.r, nullptr, a.z, a.st, s);
             }
-            k_cg_begin_pc<<<1, VEC_NT, 0, s>>>(a);
+            k_cg_head_pc_sums<<<VS_CTAS, 32, 0, s>>>(a);
+            k_cg_head_pc_update<<<gvec, VS_UPD_NT, 0, s>>>(a);
         } else {
-            k_cg_begin<<<1, VEC_NT, 0, s>>>(a);
+            k_cg_head_sums<<<VS_CTAS, 32, 0, s>>>(a);
+            k_cg_head_update<<<gvec, VS_UPD_NT, 0, s>>>(a);
         }
         if (a.fused) {
             launch_cg_fused(a, s);
@@ -1123,7 +1285,8 @@ void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* g
             const int cols_per_block = (JH_NT / 32) * JH_COLS;
             CRT_CG_DISPATCH(k_cg_jhv, (a.M + cols_per_block - 1) / cols_per_block, JH_NT, s, a);
         }
-        k_cg_end<<<1, VEC_NT, 0, s>>>(a);
+        k_cg_tail_sums<<<VS_CTAS, 32, 0, s>>>(a);
+        k_cg_tail_update<<<gvec, VS_UPD_NT, 0, s>>>(a);
     }
 }
 

@@ -13,6 +13,10 @@ struct CGState {
     int done;     // 1 once the stop rule fired or ncgmax was reached
     int ncg;      // completed iterations
     int no_gnn;   // 1 once the learned correction has been switched off for this solve
+    // the grid-wide form of the head and tail (one solve): arrivals at the
+    // sums, the tail update being due, arrivals at the tail update, and the
+    // head's choice of the base preconditioner's output
+    int vcnt, pending, ucnt, use_base;
 };
 
 struct CGArgs {
@@ -52,6 +56,7 @@ struct CGArgs {
     unsigned long long* fepoch;   // [1] advanced by every iteration tail (tickets stay unique)
     int* ferr;                    // [1] set when a wait gave up
     int flag_lag;                 // row blocks between a block's two uses (CGF_S .. CGF_Q - 1)
+    double* vred;                 // [32][8] per-CTA partial sums of the grid-wide head and tail
 };
 
 // Fused matvec geometry: row blocks of CGF_R readings, a ring of CGF_Q
