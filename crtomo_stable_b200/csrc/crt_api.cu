@@ -109,6 +109,7 @@ struct crt_ctx {
     cd *d_z = nullptr, *d_rold = nullptr, *d_zb = nullptr;
     CGState* d_live = nullptr;   // a never-done CG state for preconditioner applications outside the CG
     double* d_vred = nullptr;    // partial sums of the CG head and tail
+    cd* d_sfac = nullptr;        // per-reading factors of the Gram-form Jacobian
     // fused matvec of the CG (k_cg_fused): reduction ring, tickets, error word
     unsigned char* d_cgf = nullptr;
     size_t cgf_bytes = 0;
@@ -411,7 +412,7 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega, ctx->d_cgf, ctx->d_vred,
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega, ctx->d_cgf, ctx->d_vred, ctx->d_sfac,
                     ctx->d_dc_rows, ctx->d_dc_ptr, ctx->d_dc_ent, ctx->d_dc_node, ctx->d_bdir};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -1376,15 +1377,19 @@ int jacobian_device(crt_ctx* ctx, int mode, const double* strom_h)
         if (!ctx->d_part_sens && !dalloc(ctx, &ctx->d_part_sens, ne)) return CRT_ERR_ALLOC;
     }
     S.part = ctx->d_part_sens;
+    if (!ctx->d_sfac && !dalloc(ctx, &ctx->d_sfac, (size_t)ctx->N)) return CRT_ERR_ALLOC;
+    S.rfac = ctx->d_sfac;
     int LP = 0, gkc = 0, gnt = 0;
     size_t gsmem = 0;
     const char* sv = std::getenv("CRT_B200_SENS");
     const bool force_direct = sv && std::strcmp(sv, "direct") == 0;
-    if (!force_direct && sens_gram_plan(ctx->L, ctx->K, ctx->nkmax, real, &LP, &gkc, &gsmem, &gnt))
+    if (!force_direct && sens_gram_plan(ctx->L, ctx->K, ctx->nkmax, real, &LP, &gkc, &gsmem, &gnt)) {
         launch_sens_gram(S, LP, gkc, gsmem, gnt, real, ctx->st);
-    else
+        ctx->launches += S.out_prec ? 2 : 1;
+    } else {
         launch_sens(S, smem, real, ctx->st);
-    ctx->launches++;
+        ctx->launches++;
+    }
     if (!ev_rec(ctx, 6)) return CRT_ERR_CUDA;
     if (int e = kernel_check(ctx, "sensitivities")) return e;
     if (!ev_sync(ctx, 6)) return CRT_ERR_CUDA;

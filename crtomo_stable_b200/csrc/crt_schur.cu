@@ -265,7 +265,9 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
     __shared__ __align__(8) unsigned long long bar[2];
     __shared__ int s_err;
     const int tid = threadIdx.x;
-    const int blk = blockIdx.x, k = s.k0 + blockIdx.y;
+    // wavenumbers along x: the CTAs start in the order of their blocks'
+    // first rows, longest passes first over all wavenumbers
+    const int blk = blockIdx.y, k = s.k0 + blockIdx.x;
     const int start = back ? 0 : s.blk_start[blk];
     if (start >= n) return;   // every column of the block is zero, and so is its solution
     const T* Lk = Lws + (size_t)k * n * W;
@@ -1032,7 +1034,7 @@ template <typename T>
 void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t st)
 {
     const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, s.R);
-    dim3 grid(s.nblk, s.nk);
+    dim3 grid(s.nk, s.nblk);
     if (s.R == 16) {   // the back sweep's tiling: 4 x 4 tiles of a 129-row band at R = 16
         auto kern = k_schur_sweep<T, 160, 16, SCHUR_MS_BB>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1137,7 +1139,7 @@ void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, c
     const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_BK_R);
     auto kern = k_schur_sweep<T, NT, SCHUR_BK_R, SCHUR_MS_BB>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((s.L + SCHUR_BK_R - 1) / SCHUR_BK_R, s.nk);
+    dim3 grid(s.nk, (s.L + SCHUR_BK_R - 1) / SCHUR_BK_R);
     kern<<<grid, NT, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);
     const long long tot = (long long)s.nk * s.L * s.m;
     k_schur_out_gam<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, xg, n, kpot);

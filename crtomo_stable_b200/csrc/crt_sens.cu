@@ -178,26 +178,54 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
     // on an index load each
     __shared__ int s_node[4];
     if (tid < nk) s_node[tid] = A.nrel0[e * A.maxnodes + tid];
+    // flat index t = (kk nk + m) LP + a of the staging loops, stepped by the
+    // block size without divisions: a += da, q = kk nk + m += dq (+ carry)
+    const int da = blockDim.x % LP, dq = blockDim.x / LP;
+    const int a_0 = tid % LP, q_0 = tid / LP;
     for (int k0 = 0; k0 < K; k0 += kc) {
         const int kn = min(kc, K - k0);
+        const int tot = kn * nk * LP;
         __syncthreads();
+        {
+            int a = a_0, m = q_0 % nk, kk = q_0 / nk;
 #pragma unroll 4
-        for (int t = tid; t < kn * nk * LP; t += blockDim.x) {
-            const int a = t % LP, m = (t / LP) % nk, kk = t / (LP * nk);
-            const int node = s_node[m];
-            phi[t] = a < L ? ld_phi<T>(A.kpt[((size_t)(k0 + kk) * A.n + node) * L + a]) : Sc<T>::zero();
+            for (int t = tid; t < tot; t += blockDim.x) {
+                phi[t] = a < L ? ld_phi<T>(A.kpt[((size_t)(k0 + kk) * A.n + s_node[m]) * L + a]) : Sc<T>::zero();
+                a += da;
+                m += dq;
+                if (a >= LP) {
+                    a -= LP;
+                    ++m;
+                }
+                while (m >= nk) {
+                    m -= nk;
+                    ++kk;
+                }
+            }
         }
         __syncthreads();
-        for (int t = tid; t < kn * nk * LP; t += blockDim.x) {
-            const int b = t % LP, m = (t / LP) % nk, kk = t / (LP * nk);
-            const double* km = A.elbg + ((size_t)(k0 + kk) * A.E + e) * A.nmn;
-            const double w = A.swrtr ? A.kwnwi[k0 + kk] : 1.0;
-            T v = Sc<T>::zero();
-            for (int m2 = 0; m2 < nk; ++m2) {
-                const int ix = max(m, m2), in = min(m, m2);
-                v += scale(phi[((size_t)kk * nk + m2) * LP + b], km[ix * (ix + 1) / 2 + in]);
+        {
+            int b = a_0, m = q_0 % nk, kk = q_0 / nk;
+            for (int t = tid; t < tot; t += blockDim.x) {
+                const double* km = A.elbg + ((size_t)(k0 + kk) * A.E + e) * A.nmn;
+                const double w = A.swrtr ? A.kwnwi[k0 + kk] : 1.0;
+                T v = Sc<T>::zero();
+                for (int m2 = 0; m2 < nk; ++m2) {
+                    const int ix = max(m, m2), in = min(m, m2);
+                    v += scale(phi[((size_t)kk * nk + m2) * LP + b], km[ix * (ix + 1) / 2 + in]);
+                }
+                wu[t - b + (b % GR_TB) * LQ + b / GR_TB] = scale(v, w);
+                b += da;
+                m += dq;
+                if (b >= LP) {
+                    b -= LP;
+                    ++m;
+                }
+                while (m >= nk) {
+                    m -= nk;
+                    ++kk;
+                }
             }
-            wu[t - b + (b % GR_TB) * LQ + b / GR_TB] = scale(v, w);
         }
         __syncthreads();
         if (has_tile) {
@@ -234,7 +262,16 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
         auto g = [&](int a, int b) { return (a < 0 || b < 0) ? Sc<T>::zero() : G[gram_idx(a, b)]; };
         const T acc_i = ((g(el.w, el.y) - g(el.w, el.x)) - g(el.z, el.y)) + g(el.z, el.x);
         cd res;
-        if (A.mode == 0) {
+        if (A.out_prec) {
+            // stored in FP32: each reading's divisions are done once
+            // (k_sens_factors), which changes the FP64 value only by
+            // rounding far below the stored precision
+            const cd f = A.rfac[i];
+            if (A.mode == 0) res = (Sc<T>::to_cd(acc_i) * f) * sig;
+            else if (A.mode == 1) res = cd{Sc<T>::to_cd(acc_i).x * (sig * f).x, 0.0};
+            else res = Sc<T>::to_cd(acc_i) * f.x;
+        } else if (A.mode == 0) {
+            // stored in FP64: the reference's operations in its order
             cd d = Sc<T>::to_cd(acc_i);
             if (A.swrtr != 0) d = d / A.pi;
             res = (d * sig) / A.volt[i];
@@ -261,6 +298,25 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
     }
 }
 
+// Each reading's factor of the Gram form's output for FP32 storage, so that
+// the per-element loop multiplies where the reference divides: 1 / (V_i pi) for bsensi and
+// bsendc (sigma / V_i scales the Gram sum; pi only with swrtr), -I_i / pi
+// (or -I_i without swrtr) for bsens.
+__global__ void k_sens_factors(SensArgs A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= A.N) return;
+    const double sp = A.swrtr != 0 ? 1.0 / A.pi : 1.0;
+    cd f;
+    if (A.mode == 0 || A.mode == 1) {
+        f = (cd{1.0, 0.0} / A.volt[i]) * sp;
+    } else {
+        const double st = A.strom ? A.strom[i] : 1.0;
+        f = cd{-st * sp, 0.0};
+    }
+    A.rfac[i] = f;
+}
+
 bool sens_gram_plan(int L, int K, int nkmax, bool real, int* LP_out, int* kc_out, size_t* smem_out, int* nt_out)
 {
     const size_t tsz = real ? sizeof(double) : sizeof(cd);
@@ -282,6 +338,7 @@ bool sens_gram_plan(int L, int K, int nkmax, bool real, int* LP_out, int* kc_out
 void launch_sens_gram(const SensArgs& a, int LP, int kc, size_t smem, int nt, bool real, cudaStream_t st)
 {
     // one thread per tile: 320 threads up to 76 electrodes, 576 up to 132
+    if (a.out_prec) k_sens_factors<<<(a.N + 255) / 256, 256, 0, st>>>(a);
     auto go = [&](auto kern) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<a.E, nt, smem, st>>>(a, LP, kc);

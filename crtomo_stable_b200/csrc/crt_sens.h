@@ -20,6 +20,7 @@ struct SensArgs {
     const double* strom;   // [N] or NULL
     void* sens;            // [E][N]: complex for modes 0/2, real for mode 1 (precision out_prec)
     cd* part;              // [E][N] partial sums when K is split (kchunk < K)
+    cd* rfac;              // [N] scratch of the Gram form: each reading's factor, the divisions done once
 };
 
 void launch_transpose_kpot(const cd* kpot, cd* kpt, int n, int L, int K, cudaStream_t st);
