@@ -110,6 +110,12 @@ struct crt_ctx {
     CGState* d_live = nullptr;   // a never-done CG state for preconditioner applications outside the CG
     double* d_vred = nullptr;    // partial sums of the CG head and tail
     cd* d_sfac = nullptr;        // per-reading factors of the Gram-form Jacobian
+    // the forward sweep concurrent with the interior factor: the factor's
+    // progress per wavenumber and its count of started CTAs, the stream and
+    // the fork / join events
+    int* d_fprog = nullptr;
+    cudaStream_t ovl_st = nullptr;
+    cudaEvent_t ovl_ev[2] = {};
     // fused matvec of the CG (k_cg_fused): reduction ring, tickets, error word
     unsigned char* d_cgf = nullptr;
     size_t cgf_bytes = 0;
@@ -412,12 +418,15 @@ extern "C" void crt_destroy(crt_ctx* ctx)
                     ctx->d_fakws, ctx->d_scratch, ctx->d_sens, ctx->d_part_sens, ctx->d_strom, ctx->d_smatm,
                     ctx->d_nachbar, ctx->d_dat, ctx->d_wd, ctx->d_cgfac, ctx->d_cgres, ctx->d_bdpar,
                     ctx->d_rhs, ctx->d_p, ctx->d_r, ctx->d_bvec, ctx->d_dpar, ctx->d_ap, ctx->d_cgpart,
-                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega, ctx->d_cgf, ctx->d_vred, ctx->d_sfac,
+                    ctx->d_par, ctx->d_par_backup, ctx->d_cgst, ctx->d_z, ctx->d_rold, ctx->d_zb, ctx->d_live, ctx->d_cgl, ctx->d_omega, ctx->d_cgf, ctx->d_vred, ctx->d_sfac, ctx->d_fprog,
                     ctx->d_dc_rows, ctx->d_dc_ptr, ctx->d_dc_ent, ctx->d_dc_node, ctx->d_bdir};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (SpcPlan& c : ctx->spc_c) spc_plan_free_clone(c);
     spc_plan_free(ctx->spc);
+    if (ctx->ovl_st) cudaStreamDestroy(ctx->ovl_st);
+    for (cudaEvent_t e : ctx->ovl_ev)
+        if (e) cudaEventDestroy(e);
     for (int b = 0; b < CGL_MAX; ++b) {
         if (ctx->cstr[b]) cudaStreamDestroy(ctx->cstr[b]);
         if (ctx->cev_join[b]) cudaEventDestroy(ctx->cev_join[b]);
@@ -1110,19 +1119,49 @@ int run_forward_schur(crt_ctx* ctx)
         launch_band_prep<T>(AI, ctx->st);   // the scaling factors for the right-hand sides
     }
     CK(cudaMemsetAsync(X, 0, sizeof(T) * (size_t)K * ncol * nI, ctx->st));
+    // The forward sweep follows the interior factor column block by column
+    // block on a second stream (the factor occupies K SMs for its whole
+    // run); CRT_B200_SCHUR_OVERLAP=0, graph capture and the streamed
+    // factor keep the two in sequence.
+    const char* ov = std::getenv("CRT_B200_SCHUR_OVERLAP");
+    const bool overlap = blk && !ctx->capture && !(ov && std::strcmp(ov, "0") == 0);
+    if (overlap) {
+        if (!ctx->d_fprog && !dalloc(ctx, &ctx->d_fprog, (size_t)K + 1)) return CRT_ERR_ALLOC;
+        CK(cudaMemsetAsync(ctx->d_fprog, 0, sizeof(int) * ((size_t)K + 1), ctx->st));
+        if (!ctx->ovl_st) CK(cudaStreamCreateWithFlags(&ctx->ovl_st, cudaStreamNonBlocking));
+        if (!ctx->ovl_ev[0]) {
+            CK(cudaEventCreateWithFlags(&ctx->ovl_ev[0], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->ovl_ev[1], cudaEventDisableTiming));
+        }
+    }
     mk.e8 = tev_rec(ctx);
     if (blk) {
         launch_schur_rhs<T>(S, Af, ctx->d_sfak, X, cval, ctx->st);
+        if (overlap) {
+            AI.progress = ctx->d_fprog;
+            AI.started = ctx->d_fprog + K;
+            CK(cudaEventRecord(ctx->ovl_ev[0], ctx->st));
+        }
         launch_band_factor_blk<T>(AI, pb, ctx->st);
     } else {
         launch_band_factor<T>(AI, ctx->st);   // forms fak as it goes
         launch_schur_rhs<T>(S, Af, ctx->d_sfak, X, cval, ctx->st);
     }
+    if (overlap) {
+        SchurArgs So = S;
+        So.progress = ctx->d_fprog;
+        CK(cudaStreamWaitEvent(ctx->ovl_st, ctx->ovl_ev[0], 0));
+        launch_wait_started(ctx->d_fprog + K, K, S.status, ctx->ovl_st);
+        launch_schur_forward<T>(So, LI, X, ctx->ovl_st);
+        CK(cudaEventRecord(ctx->ovl_ev[1], ctx->ovl_st));
+        ctx->launches += 2;
+    }
     if (int e = kernel_check(ctx, "interior factor")) return e;
     mk.e1 = tev_rec(ctx);
     mk.blk = blk;
     launch_schur_transpose<T>(S, LI, Lrev, ctx->st);
-    launch_schur_forward<T>(S, LI, X, ctx->st);
+    if (overlap) CK(cudaStreamWaitEvent(ctx->st, ctx->ovl_ev[1], 0));
+    else launch_schur_forward<T>(S, LI, X, ctx->st);
     ctx->sev[0] = tev_rec(ctx);
     launch_schur_gram<T>(S, X, Cg, ctx->st);
     ctx->sev[1] = tev_rec(ctx);

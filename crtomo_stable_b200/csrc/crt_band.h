@@ -29,6 +29,11 @@ struct BandArgs {
     int* status;             // [total systems] errnr per system
     cd* aval;                // [b][row_ptr[n]] the prepared (scaled, edited) entries in FP64, or NULL
     size_t aval_stride;
+    // k_band_factor_blk publishes its progress for a concurrent consumer:
+    // progress[b] = c once columns [0, c) of system b are final (n at the
+    // end, also after a failure); started counts the CTAs that have begun
+    int* progress = nullptr;
+    int* started = nullptr;
 };
 
 // One assembled band entry of system (k, l): kompab's sum over the entry's

@@ -354,7 +354,19 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int b = blockIdx.x, sys = A.sys0 + b;
-    if (A.status[sys] != 0) return;    // zero diagonal found by the preparation pass
+    // progress for a consumer that sweeps the finished columns while this
+    // CTA goes on: published by the last thread after a barrier
+    auto publish = [&](int c) {
+        if (A.progress && tid == NT - 1) {
+            __threadfence();
+            asm volatile("st.release.gpu.global.s32 [%0], %1;\n" ::"l"(A.progress + b), "r"(c) : "memory");
+        }
+    };
+    if (A.started && tid == 0) atomicAdd(A.started, 1);
+    if (A.status[sys] != 0) {   // zero diagonal found by the preparation pass
+        publish(A.n);
+        return;
+    }
     int k, l;
     sys_kl(A, sys, k, l);
     T* Lc = A.Lws + (size_t)b * A.lstride;
@@ -547,6 +559,9 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
             if (fuse) bsl[x] = bx;
         }
         __syncthreads();
+        // columns [0, i0 + PB) are final (the diagonal blocks were written
+        // by earlier phases); published every 16 panels
+        if (((i0 / PB) & 15) == 15) publish(i0 + PB);
         // ---- phase 3a: the trailing update of the next panel's diagonal
         // tiles, one entry per thread, so that its block can be factored
         // while the rest of the window is updated.
@@ -637,6 +652,7 @@ __global__ void __launch_bounds__(NT, MINB) k_band_factor_blk(BandArgs<T> A, int
         __syncthreads();
     }
     if (tid == 0 && s_err) A.status[sys] = s_err;
+    publish(n);
 }
 
 }  // namespace

@@ -285,6 +285,27 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
     auto colp = [&](int j) { return X + ((size_t)k * s.ncol + colid[j]) * n; };
     auto fetch = [&](int c0, int buf) {
         if (tid == 0) {
+            if (s.progress && !s_err) {
+                // the factor's columns [c0, c0 + BB) are final once its
+                // progress passes them.  The wait gives up after about 4 s,
+                // or at once when another CTA of this wavenumber gave up
+                // (status set); the result is then flagged as failed.
+                const int want = min(n, c0 + BB);
+                long polls = 0;
+                int got;
+                while (true) {
+                    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(got) : "l"(s.progress + k) : "memory");
+                    if (got >= want) break;
+                    if (*(volatile const int*)(s.status + k) != 0 || ++polls > (1L << 22)) {
+                        s_err = 1;
+                        atomicMax(&s.status[k], (int)CRT_ERR_CUDA);
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                // the copy below reads them through the async proxy
+                asm volatile("fence.proxy.async.global;\n" ::: "memory");
+            }
             const int bytes = min(BB, n - c0) * W * (int)sizeof(T);
             mbar_expect_tx(&bar[buf], bytes);
             bulk_g2s(Lb + (size_t)buf * BB * W, Lk + (size_t)c0 * W, bytes, &bar[buf]);
@@ -420,8 +441,10 @@ __global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __rest
     __shared__ T As[TI][TG + 1];
     __shared__ T Bs[TI][TC + 1];
     __shared__ int s_i0;
-    const int tid = threadIdx.x, k = s.k0 + blockIdx.z;
-    const int g0 = blockIdx.x * TG, c0 = blockIdx.y * TC;
+    // wavenumbers along x, so the long tiles (early first rows) of every
+    // wavenumber start first
+    const int tid = threadIdx.x, k = s.k0 + blockIdx.x;
+    const int g0 = blockIdx.y * TG, c0 = blockIdx.z * TC;
     const int m = s.m, L = s.L, nI = s.nI, ncol = s.ncol;
     if (c0 >= L && c0 - L > g0 + TG - 1) return;
     if (tid == 0) {
@@ -941,7 +964,9 @@ __global__ void __launch_bounds__(128) k_schur_zrebuild(SchurArgs s, T* X, const
     __shared__ T As[TG][TI + 1];
     __shared__ T Bs[TG][TL + 1];
     const int tid = threadIdx.x;
-    const int k = s.k0 + blockIdx.z, i0 = blockIdx.x * TI, l0 = blockIdx.y * TL;
+    // wavenumbers along x and the row blocks from the last: a late row block
+    // meets the most boundary columns, so the longest tiles start first
+    const int k = s.k0 + blockIdx.x, i0 = (gridDim.y - 1 - blockIdx.y) * TI, l0 = blockIdx.z * TL;
     const int ti = tid % 16, tl = tid / 16;
     const int m = s.m, nI = s.nI, L = s.L;
     T* Xk = X + (size_t)k * s.ncol * nI;
@@ -1046,10 +1071,30 @@ void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t s
     }
 }
 
+// One thread: returns once `want` CTAs of the concurrent factor have begun
+// (bounded: about 2 s), so that the sweep's CTAs, which wait on that
+// factor's progress, never take SMs the factor still needs.
+__global__ void k_wait_started(const int* started, int want, int* status)
+{
+    long polls = 0;
+    while (*(volatile const int*)started < want) {
+        if (++polls > (1L << 21)) {
+            atomicMax(status, (int)CRT_ERR_CUDA);
+            return;
+        }
+        __nanosleep(1000);
+    }
+}
+
+void launch_wait_started(const int* started, int want, int* status, cudaStream_t st)
+{
+    k_wait_started<<<1, 1, 0, st>>>(started, want, status);
+}
+
 template <typename T>
 void launch_schur_gram(const SchurArgs& s, const T* X, T* C, cudaStream_t st)
 {
-    dim3 grid((s.m + 63) / 64, (s.ncol + 31) / 32, s.nk);
+    dim3 grid(s.nk, (s.m + 63) / 64, (s.ncol + 31) / 32);
     k_schur_gram<T><<<grid, 128, 0, st>>>(s, X, C);
 }
 
@@ -1127,7 +1172,7 @@ void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, 
 template <typename T>
 void launch_schur_zrebuild(const SchurArgs& s, T* X, const T* xg, cudaStream_t st)
 {
-    dim3 grid((s.nI + 63) / 64, (s.L + 31) / 32, s.nk);
+    dim3 grid(s.nk, (s.nI + 63) / 64, (s.L + 31) / 32);
     k_schur_zrebuild<T><<<grid, 128, 0, st>>>(s, X, xg);
 }
 

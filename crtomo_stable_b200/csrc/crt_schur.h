@@ -91,6 +91,9 @@ struct SchurArgs {
     const int* gsort;        // [m] boundary positions ordered by their column's first row
     const int* gfirst;       // [m] first row of gsort[q]'s column
     int* status;             // [K * L] errnr per (k, l); the interior factor uses [0, K)
+    // forward sweep concurrent with the interior factor: progress[k] as
+    // published by k_band_factor_blk (columns [0, progress[k]) final), or null
+    const int* progress = nullptr;
 };
 
 // Right-hand sides of the interior solves, X[k][c][i] (zeroed by the
@@ -110,6 +113,8 @@ void launch_schur_transpose(const SchurArgs& s, const T* Lws, T* Lrev, cudaStrea
 // V^ = L^-1 F A_IG), each column block from its first non-zero row.
 template <typename T>
 void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t st);
+// waits (one thread, bounded) until `want` CTAs of a concurrent factor have begun
+void launch_wait_started(const int* started, int want, int* status, cudaStream_t st);
 // Gram products C[k][c][g] = sum_i V^[i][g] X[i][c] (c < L: A_GI w_l;
 // c >= L: the lower triangle of A_GI Y = -S0), column-major with m rows.
 template <typename T>

@@ -404,6 +404,31 @@ def test_schur_iteration_matches_schur_cholesky(name, ldc, monkeypatch):
     assert np.abs(out["iter"][0] - out["direct"][0]).max() <= 1e-11 * scale
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,ldc", [("mixed_surf", False), ("TestModInv", True)])
+def test_schur_sweep_beside_the_factor_is_the_sequential_sweep(name, ldc, monkeypatch):
+    """The forward sweep run on a second stream, each column block waiting
+    for the interior factor's published progress, does the arithmetic of
+    the sweep run after the factor: potentials bit for bit equal, and no
+    wait gave up (the forward reports no error)."""
+    from fixtures import load_forward_case
+    from crtomo_stable_b200.lib import FORWARD_SCHUR, Context
+    case = load_forward_case(name)
+    c = case["cfg"]
+    out = {}
+    for ov in ("1", "0"):
+        monkeypatch.setenv("CRT_B200_SCHUR_OVERLAP", ov)
+        ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=c.swrtr,
+                      lsink=c.lsink, nsink=c.nsink)
+        ctx.set_forward_form(FORWARD_SCHUR)
+        for _ in range(2):
+            _, sa, kp = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+        out[ov] = (kp, sa)
+        ctx.close()
+    assert np.array_equal(out["1"][0], out["0"][0])
+    assert np.array_equal(out["1"][1], out["0"][1])
+
+
 def test_schur_form_is_refused_where_it_does_not_apply():
     """No mixed boundary (the 2D decoupling grid): the Schur form does not
     apply, the setter says so (errnr 201) and the direct form runs."""
