@@ -250,12 +250,13 @@ __global__ void k_schur_transpose(SchurArgs s, const T* __restrict__ Lws, T* Lre
 //   back == 1: the back sweep L^T x^ = z^ of the source columns: Lws holds
 //     the reversed row-packed factor and the rows are read reversed; the
 //     solution goes out as kpot = fak x^ at the interior rows' nodes.
-template <typename T, int NT, int R, int BB>
+template <typename T, int NT, int R, int BB, int TC = 4>
 __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __restrict__ Lws,
                                                        const double* __restrict__ fakws, T* X, cd* kpot, int n_kpot,
                                                        int WZ, int back)
 {
-    static_assert(BB == 16 && R % 4 == 0 && R <= 32 && NT % 32 == 0 && NT >= R, "sweep layout");
+    static_assert(BB == 16 && R % 4 == 0 && R <= 32 && NT % 32 == 0 && NT >= R && (TC == 4 || TC == 2),
+                  "sweep layout");
     extern __shared__ __align__(16) unsigned char sw_dyn[];
     const int W = s.WI, n = s.nI, mb = s.mbI;
     T* Lb = reinterpret_cast<T*>(sw_dyn);   // [2][BB * W]
@@ -378,29 +379,30 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
             }
         }
         {   // rows [c0 + nb, c0 + nb + mb) take the block's columns: a thread
-            // owns rows rq + NQ a and columns jq + (R/4) c, so a warp's loads
-            // fall on consecutive words
+            // owns rows rq + NQ a (4 of them) and columns jq + (R/TC) c (TC of
+            // them), so a warp's loads fall on consecutive words; every entry
+            // takes the block's columns u = 0 .. nb-1 in order, whatever TC
             const int rlo = c0 + nb, rhi = min(n, c0 + nb + mb);
             const int NQ = (rhi - rlo + 3) >> 2;
-            constexpr int RJ = R / 4;
+            constexpr int RJ = R / TC;
             for (int tile = tid; tile < NQ * RJ; tile += NT) {
                 const int rq = tile / RJ, jq = tile % RJ;
-                T acc[4][4];
+                T acc[4][TC];
                 int sl[4];
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     const int r = rlo + rq + NQ * a;
                     sl[a] = r < rhi ? r % WZ : -1;
 #pragma unroll
-                    for (int c = 0; c < 4; ++c)
+                    for (int c = 0; c < TC; ++c)
                         acc[a][c] = sl[a] >= 0 ? Z[(size_t)sl[a] * R + jq + RJ * c] : Sc<T>::zero();
                 }
 #pragma unroll
                 for (int u = 0; u < BB; ++u) {
                     if (u < nb) {
-                        T zc[4], lv[4];
+                        T zc[TC], lv[4];
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) zc[c] = Z[(size_t)(sb + u) * R + jq + RJ * c];
+                        for (int c = 0; c < TC; ++c) zc[c] = Z[(size_t)(sb + u) * R + jq + RJ * c];
 #pragma unroll
                         for (int a = 0; a < 4; ++a) {
                             const int d = rlo + rq + NQ * a - (c0 + u);
@@ -409,14 +411,14 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
 #pragma unroll
                         for (int a = 0; a < 4; ++a)
 #pragma unroll
-                            for (int c = 0; c < 4; ++c) fms_acc(acc[a][c], lv[a], zc[c]);
+                            for (int c = 0; c < TC; ++c) fms_acc(acc[a][c], lv[a], zc[c]);
                     }
                 }
 #pragma unroll
                 for (int a = 0; a < 4; ++a)
                     if (sl[a] >= 0)
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) Z[(size_t)sl[a] * R + jq + RJ * c] = acc[a][c];
+                        for (int c = 0; c < TC; ++c) Z[(size_t)sl[a] * R + jq + RJ * c] = acc[a][c];
             }
         }
         // the buffer just read is the destination of the bulk copy after next
@@ -1030,6 +1032,18 @@ int sweep_wz(int mbI) { return (mbI + 4 * SCHUR_MS_BB - 1) / SCHUR_MS_BB * SCHUR
 
 constexpr int SWEEP_NT = 288;   // 4 x 4 update tiles of a 129-row band at R = 32 in one round
 
+// Columns per update tile of the sweeps: 2 (twice the threads, each with
+// half the accumulators) or 4.  Measured on the 60k-triangle mesh: the back
+// sweep 22.7 ms with 2 against 23.7 with 4, the forward sweep's part after
+// the factor 13.0 against 11.7; CRT_B200_SCHUR_TILE=2 / 4 sets both.
+static int sweep_tc(bool back)
+{
+    const char* v = std::getenv("CRT_B200_SCHUR_TILE");
+    if (v && std::strcmp(v, "4") == 0) return 4;
+    if (v && std::strcmp(v, "2") == 0) return 2;
+    return back ? 2 : 4;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -1060,14 +1074,18 @@ void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t s
 {
     const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, s.R);
     dim3 grid(s.nk, s.nblk);
-    if (s.R == 16) {   // the back sweep's tiling: 4 x 4 tiles of a 129-row band at R = 16
-        auto kern = k_schur_sweep<T, 160, 16, SCHUR_MS_BB>;
+    auto go = [&](auto kern, int nt) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, 160, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+        kern<<<grid, nt, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+    };
+    // update tiles of 4 rows x TC columns: one round of a 129-row band
+    const bool narrow = sweep_tc(false) == 2;
+    if (s.R == 16) {
+        if (narrow) go(k_schur_sweep<T, 288, 16, SCHUR_MS_BB, 2>, 288);
+        else go(k_schur_sweep<T, 160, 16, SCHUR_MS_BB, 4>, 160);
     } else {
-        auto kern = k_schur_sweep<T, SWEEP_NT, SCHUR_MS_R, SCHUR_MS_BB>;
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, SWEEP_NT, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+        if (narrow) go(k_schur_sweep<T, 544, SCHUR_MS_R, SCHUR_MS_BB, 2>, 544);
+        else go(k_schur_sweep<T, SWEEP_NT, SCHUR_MS_R, SCHUR_MS_BB, 4>, SWEEP_NT);
     }
 }
 
@@ -1180,12 +1198,16 @@ template <typename T>
 void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, const T* X, const T* xg, int n,
                        cd* kpot, cudaStream_t st)
 {
-    constexpr int NT = 160;   // 4 x 4 update tiles of a 129-row band at R = 16 in one round
     const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_BK_R);
-    auto kern = k_schur_sweep<T, NT, SCHUR_BK_R, SCHUR_MS_BB>;
-    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid(s.nk, (s.L + SCHUR_BK_R - 1) / SCHUR_BK_R);
-    kern<<<grid, NT, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);
+    auto go = [&](auto kern, int nt) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<grid, nt, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);
+    };
+    // 4 x 2 update tiles of a 129-row band at R = 16 in one round (288
+    // threads), or 4 x 4 (160)
+    if (sweep_tc(true) == 2) go(k_schur_sweep<T, 288, SCHUR_BK_R, SCHUR_MS_BB, 2>, 288);
+    else go(k_schur_sweep<T, 160, SCHUR_BK_R, SCHUR_MS_BB, 4>, 160);
     const long long tot = (long long)s.nk * s.L * s.m;
     k_schur_out_gam<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, xg, n, kpot);
 }
