@@ -440,8 +440,9 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __restrict__ X, T* C)
 {
     constexpr int TG = 64, TC = 32, TI = 16;
-    __shared__ T As[TI][TG + 1];
-    __shared__ T Bs[TI][TC + 1];
+    extern __shared__ __align__(16) unsigned char gram_dyn[];   // both stages of both tiles
+    auto As = reinterpret_cast<T(*)[TI][TG + 1]>(gram_dyn);                                  // [2][TI][TG + 1]
+    auto Bs = reinterpret_cast<T(*)[TI][TC + 1]>(gram_dyn + 2 * TI * (TG + 1) * sizeof(T));  // [2][TI][TC + 1]
     __shared__ int s_i0;
     // wavenumbers along x, so the long tiles (early first rows) of every
     // wavenumber start first
@@ -463,14 +464,29 @@ __global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __rest
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[a][c] = Sc<T>::zero();
     const T* Xk = X + (size_t)k * ncol * nI;
-    for (int i0 = s_i0; i0 < nI; i0 += TI) {
+    // the tiles of rows [i0, i0 + TI) into buffer `buf` (cp.async, the
+    // next block's copies in flight while this one is multiplied)
+    auto stage = [&](int buf, int i0) {
         for (int idx = tid; idx < TI * TG; idx += 128) {
             const int gg = idx / TI, ii = idx % TI;
-            As[ii][gg] = (g0 + gg < m && i0 + ii < nI) ? Xk[(size_t)(L + g0 + gg) * nI + i0 + ii] : Sc<T>::zero();
+            if (g0 + gg < m && i0 + ii < nI) cp_async_elem<T>(&As[buf][ii][gg], Xk + (size_t)(L + g0 + gg) * nI + i0 + ii);
+            else As[buf][ii][gg] = Sc<T>::zero();
         }
         for (int idx = tid; idx < TI * TC; idx += 128) {
             const int cc = idx / TI, ii = idx % TI;
-            Bs[ii][cc] = (c0 + cc < ncol && i0 + ii < nI) ? Xk[(size_t)(c0 + cc) * nI + i0 + ii] : Sc<T>::zero();
+            if (c0 + cc < ncol && i0 + ii < nI) cp_async_elem<T>(&Bs[buf][ii][cc], Xk + (size_t)(c0 + cc) * nI + i0 + ii);
+            else Bs[buf][ii][cc] = Sc<T>::zero();
+        }
+        cp_async_commit();
+    };
+    int buf = 0;
+    if (s_i0 < nI) stage(0, s_i0);
+    for (int i0 = s_i0; i0 < nI; i0 += TI, buf ^= 1) {
+        if (i0 + TI < nI) {
+            stage(buf ^ 1, i0 + TI);   // its last readers finished before the trailing barrier
+            cp_async_wait_group<1>();
+        } else {
+            cp_async_wait_group<0>();
         }
         __syncthreads();
 #pragma unroll 4
@@ -478,9 +494,9 @@ __global__ void __launch_bounds__(128) k_schur_gram(SchurArgs s, const T* __rest
             T a4[4], b4[4];
             // rows ti + 16 a, columns tc + 8 c: a warp reads consecutive words
 #pragma unroll
-            for (int a = 0; a < 4; ++a) a4[a] = As[ii][ti + 16 * a];
+            for (int a = 0; a < 4; ++a) a4[a] = As[buf][ii][ti + 16 * a];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) b4[c] = Bs[ii][tc + 8 * c];
+            for (int c = 0; c < 4; ++c) b4[c] = Bs[buf][ii][tc + 8 * c];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -963,8 +979,9 @@ template <typename T>
 __global__ void __launch_bounds__(128) k_schur_zrebuild(SchurArgs s, T* X, const T* __restrict__ xg)
 {
     constexpr int TI = 64, TL = 32, TG = 16;
-    __shared__ T As[TG][TI + 1];
-    __shared__ T Bs[TG][TL + 1];
+    extern __shared__ __align__(16) unsigned char zr_dyn[];   // both stages of both tiles
+    auto As = reinterpret_cast<T(*)[TG][TI + 1]>(zr_dyn);                                  // [2][TG][TI + 1]
+    auto Bs = reinterpret_cast<T(*)[TG][TL + 1]>(zr_dyn + 2 * TG * (TI + 1) * sizeof(T));  // [2][TG][TL + 1]
     const int tid = threadIdx.x;
     // wavenumbers along x and the row blocks from the last: a late row block
     // meets the most boundary columns, so the longest tiles start first
@@ -977,26 +994,43 @@ __global__ void __launch_bounds__(128) k_schur_zrebuild(SchurArgs s, T* X, const
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int c = 0; c < 4; ++c) acc[a][c] = Sc<T>::zero();
-    for (int q0 = 0; q0 < m; q0 += TG) {
-        if (s.gfirst[q0] >= i0 + TI) break;
+    // boundary columns [q0, q0 + TG) of both operands into buffer `buf`
+    // (cp.async, the next block's copies in flight during this one)
+    auto stage = [&](int buf, int q0) {
         for (int idx = tid; idx < TG * TI; idx += 128) {
             const int gg = idx / TI, ii = idx % TI;
             const int g = q0 + gg < m ? s.gsort[q0 + gg] : -1;
-            As[gg][ii] = (g >= 0 && i0 + ii < nI) ? Xk[(size_t)(L + g) * nI + i0 + ii] : Sc<T>::zero();
+            if (g >= 0 && i0 + ii < nI) cp_async_elem<T>(&As[buf][gg][ii], Xk + (size_t)(L + g) * nI + i0 + ii);
+            else As[buf][gg][ii] = Sc<T>::zero();
         }
         for (int idx = tid; idx < TG * TL; idx += 128) {
             const int ll = idx / TG, gg = idx % TG;
             const int g = q0 + gg < m ? s.gsort[q0 + gg] : -1;
-            Bs[gg][ll] = (g >= 0 && l0 + ll < L) ? xg[((size_t)k * L + l0 + ll) * m + g] : Sc<T>::zero();
+            if (g >= 0 && l0 + ll < L) cp_async_elem<T>(&Bs[buf][gg][ll], xg + ((size_t)k * L + l0 + ll) * m + g);
+            else Bs[buf][gg][ll] = Sc<T>::zero();
+        }
+        cp_async_commit();
+    };
+    // the boundary columns in the order of their first rows: a block whose
+    // first column starts below this tile ends the loop
+    auto live = [&](int q0) { return q0 < m && s.gfirst[q0] < i0 + TI; };
+    int buf = 0;
+    if (live(0)) stage(0, 0);
+    for (int q0 = 0; live(q0); q0 += TG, buf ^= 1) {
+        if (live(q0 + TG)) {
+            stage(buf ^ 1, q0 + TG);   // its last readers finished before the trailing barrier
+            cp_async_wait_group<1>();
+        } else {
+            cp_async_wait_group<0>();
         }
         __syncthreads();
 #pragma unroll 4
         for (int gg = 0; gg < TG; ++gg) {
             T a4[4], b4[4];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) a4[a] = As[gg][ti + 16 * a];
+            for (int a = 0; a < 4; ++a) a4[a] = As[buf][gg][ti + 16 * a];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) b4[c] = Bs[gg][tl + 8 * c];
+            for (int c = 0; c < 4; ++c) b4[c] = Bs[buf][gg][tl + 8 * c];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
@@ -1113,7 +1147,9 @@ template <typename T>
 void launch_schur_gram(const SchurArgs& s, const T* X, T* C, cudaStream_t st)
 {
     dim3 grid(s.nk, (s.m + 63) / 64, (s.ncol + 31) / 32);
-    k_schur_gram<T><<<grid, 128, 0, st>>>(s, X, C);
+    const int smem = 2 * 16 * (64 + 1 + 32 + 1) * (int)sizeof(T);   // the two stages of both tiles
+    cudaFuncSetAttribute(k_schur_gram<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_schur_gram<T><<<grid, 128, smem, st>>>(s, X, C);
 }
 
 template <typename T>
@@ -1191,7 +1227,9 @@ template <typename T>
 void launch_schur_zrebuild(const SchurArgs& s, T* X, const T* xg, cudaStream_t st)
 {
     dim3 grid(s.nk, (s.nI + 63) / 64, (s.L + 31) / 32);
-    k_schur_zrebuild<T><<<grid, 128, 0, st>>>(s, X, xg);
+    const int smem = 2 * 16 * (64 + 1 + 32 + 1) * (int)sizeof(T);   // the two stages of both tiles
+    cudaFuncSetAttribute(k_schur_zrebuild<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_schur_zrebuild<T><<<grid, 128, smem, st>>>(s, X, xg);
 }
 
 template <typename T>
