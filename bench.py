@@ -692,17 +692,33 @@ def main():
                       "(preconditioned iteration per electrode, %.1f iterations)" % it_mean)
         if it_mean > 0:
             w["chol"] = w["chol_ref"] + it_mean * w["chol_it"]
+        # the forward sweep runs beside the factor (second stream) unless
+        # CRT_B200_SCHUR_OVERLAP=0: its span is the factor's time plus the
+        # part after the factor (the `schur_forward` phase)
+        overlap = os.environ.get("CRT_B200_SCHUR_OVERLAP", "1") != "0"
+        fwd_label = ("k_schur_sweep (forward sweep of [F r_I | F A_IG], beside the factor: span from the factor's "
+                     "start) + factor transpose" if overlap else
+                     "k_schur_sweep (forward sweep of [F r_I | F A_IG]) + factor transpose")
         for name, key, label in (("factor", "factor_kernel", "k_band_factor_blk<cd> (interior band Cholesky, one system per wavenumber)"),
-                                 ("forward", "schur_forward", "k_schur_sweep (forward sweep of [F r_I | F A_IG]) + factor transpose"),
+                                 ("forward", "schur_forward", fwd_label),
                                  ("gram", "schur_gram", "k_schur_gram (V^T [u^ | V^])"),
                                  ("chol", "schur_chol", chol_label),
                                  ("back", "schur_back", "k_schur_zrebuild + k_schur_sweep back + k_schur_out_gam")):
             t_ms = ph.get(key, 0.0)
+            if name == "forward" and overlap:
+                t_ms += ph.get("factor_kernel", 0.0)
             fl = 8.0 * w[name]
             ach = fl / (t_ms / 1e3) / 1e12 if t_ms > 0 else 0.0
-            kernels.append({"kernel": label, "ms": t_ms, "flops": fl, "achieved": ach, "peak": fp64_peak,
-                            "unit": "TFLOP/s", "frac": ach / fp64_peak})
-    dom = max(kernels, key=lambda k_: k_["ms"]) if kernels else None
+            ent = {"kernel": label, "ms": t_ms, "flops": fl, "achieved": ach, "peak": fp64_peak,
+                   "unit": "TFLOP/s", "frac": ach / fp64_peak}
+            if name == "factor":
+                # one CTA of 512 threads per wavenumber: K of the 148 SMs
+                ent["sms_used"] = K
+                ent["frac_of_used_sms"] = ach / (fp64_peak * K / 148.0)
+            kernels.append(ent)
+    # the dominant kernel: the longest phase whose time is its own (the
+    # overlapped sweep's span contains the factor)
+    dom = max((k_ for k_ in kernels if "span" not in k_["kernel"]), key=lambda k_: k_["ms"]) if kernels else None
     roof = None
     if dom is not None:
         roof = {"kernel": dom["kernel"], "bound": "fp64", "achieved": dom["achieved"], "peak": fp64_peak,
@@ -711,6 +727,9 @@ def main():
                 "peak_source": ("FP64 FMA pipe, 64 FMA/clk/SM x 148 SMs at the max SM clock (the Schur kernels run "
                                 "in FP64 on the CUDA cores; MEASURED_PEAKS.json holds HBM and bf16 tensor figures only)"),
                 "algorithmic_flops_per_launch": dom["flops"], "launch_ms": dom["ms"], "launches": 1.0}
+        for key in ("sms_used", "frac_of_used_sms"):
+            if key in dom:
+                roof[key] = dom[key]
     roof_cg = None
     if ncg > 0:
         bytes_it = 2.0 * N * E * 8 + 6.0 * E * 16 + 3.0 * N * 16   # J (complex64) read twice + vectors

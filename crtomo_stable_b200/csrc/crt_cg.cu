@@ -21,6 +21,8 @@
 // improvement) use the same kernels with zero imaginary parts, which keeps
 // the real arithmetic of cjggdc exact.
 #include "crt_cg.h"
+
+#include <cstdlib>
 #include "crt_spc.h"
 #include "crt_gnn.h"
 
@@ -458,39 +460,39 @@ __global__ void k_cg_jv_reduce(CGArgs A)
 // single rows past the last pair: the same order for every chunk size.
 constexpr int JH_COLS = 4, JH_NT = 256, JH_CHUNK = 1024;
 
-template <int JP, int JM>
+template <int JP, int JM, int NC = JH_COLS>
 __global__ void __launch_bounds__(JH_NT) k_cg_jhv(CGArgs A)
 {
     using RT = typename JRaw<JP, JM>::T;
     __shared__ __align__(16) cd s_ap[2][JH_CHUNK];
     if (A.st->done) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int ebase = (blockIdx.x * (JH_NT / 32) + warp) * JH_COLS;
+    const int ebase = (blockIdx.x * (JH_NT / 32) + warp) * NC;
     // warps past the last column still take part in the staging barriers
-    const int nc = max(0, min(JH_COLS, A.M - ebase));
+    const int nc = max(0, min(NC, A.M - ebase));
     const int N = A.N;
     auto stage = [&](int buf, int r0) {
         const int nr = min(JH_CHUNK, N - r0);
         for (int t = threadIdx.x; t < nr; t += JH_NT) cp_async16(&s_ap[buf][t], A.ap + r0 + t);
         cp_async_commit();
     };
-    double ax[JH_COLS], ay[JH_COLS];
+    double ax[NC], ay[NC];
 #pragma unroll
-    for (int c = 0; c < JH_COLS; ++c) {
+    for (int c = 0; c < NC; ++c) {
         ax[c] = 0.0;
         ay[c] = 0.0;
     }
-    auto pair = [&](const RT (&j0)[JH_COLS], const RT (&j1)[JH_COLS], cd w0, cd w1) {
+    auto pair = [&](const RT (&j0)[NC], const RT (&j1)[NC], cd w0, cd w1) {
 #pragma unroll
-        for (int c = 0; c < JH_COLS; ++c) {
+        for (int c = 0; c < NC; ++c) {
             const cd t0 = conj(jcvt<JM>(j0[c])) * w0, t1 = conj(jcvt<JM>(j1[c])) * w1;
             ax[c] += t0.x + t1.x;
             ay[c] += t0.y + t1.y;
         }
     };
-    auto ld = [&](RT (&dst)[JH_COLS], int i) {
+    auto ld = [&](RT (&dst)[NC], int i) {
 #pragma unroll
-        for (int c = 0; c < JH_COLS; ++c) dst[c] = c < nc ? jraw<JP, JM>(A, ebase + c, i) : RT{};
+        for (int c = 0; c < NC; ++c) dst[c] = c < nc ? jraw<JP, JM>(A, ebase + c, i) : RT{};
     };
     stage(0, 0);
     int buf = 0;
@@ -507,7 +509,7 @@ __global__ void __launch_bounds__(JH_NT) k_cg_jhv(CGArgs A)
         int i = r0 + lane;
         if (nc > 0) {
             for (; i + 96 < r1; i += 128) {
-                RT j0[JH_COLS], j1[JH_COLS], j2[JH_COLS], j3[JH_COLS];
+                RT j0[NC], j1[NC], j2[NC], j3[NC];
                 ld(j0, i);
                 ld(j1, i + 32);
                 ld(j2, i + 64);
@@ -516,16 +518,16 @@ __global__ void __launch_bounds__(JH_NT) k_cg_jhv(CGArgs A)
                 pair(j2, j3, w[i + 64], w[i + 96]);
             }
             for (; i + 32 < r1; i += 64) {
-                RT j0[JH_COLS], j1[JH_COLS];
+                RT j0[NC], j1[NC];
                 ld(j0, i);
                 ld(j1, i + 32);
                 pair(j0, j1, w[i], w[i + 32]);
             }
             for (; i < r1; i += 32) {
-                RT j0[JH_COLS];
+                RT j0[NC];
                 ld(j0, i);
 #pragma unroll
-                for (int c = 0; c < JH_COLS; ++c) {
+                for (int c = 0; c < NC; ++c) {
                     const cd t = conj(jcvt<JM>(j0[c])) * w[i];
                     ax[c] += t.x;
                     ay[c] += t.y;
@@ -536,14 +538,14 @@ __global__ void __launch_bounds__(JH_NT) k_cg_jhv(CGArgs A)
     }
     if (nc == 0) return;
 #pragma unroll
-    for (int c = 0; c < JH_COLS; ++c) {
+    for (int c = 0; c < NC; ++c) {
         ax[c] = warp_allsum(ax[c]);
         ay[c] = warp_allsum(ay[c]);
     }
     if (lane < nc) {
         double bx = 0.0, by = 0.0;
 #pragma unroll
-        for (int c = 0; c < JH_COLS; ++c)
+        for (int c = 0; c < NC; ++c)
             if (c == lane) {
                 bx = ax[c];
                 by = ay[c];
@@ -1233,6 +1235,34 @@ void launch_cg_setup(const CGArgs& a, const cd* dat, const cd* sigmaa, const cd*
 
 void launch_cg_init(const CGArgs& a, cudaStream_t s) { k_cg_init<<<1, VEC_NT, 0, s>>>(a); }
 
+namespace {
+// J^H pass with NC cells per warp (4; CRT_B200_JH_COLS=2 / 8 for the others)
+template <int NC>
+void launch_cg_jhv_nc(const CGArgs& a, cudaStream_t s)
+{
+    const int cols_per_block = (JH_NT / 32) * NC;
+    const int grid = (a.M + cols_per_block - 1) / cols_per_block;
+    switch (a.jprec * 3 + a.jmode) {
+    case 0: k_cg_jhv<0, 0, NC><<<grid, JH_NT, 0, s>>>(a); break;
+    case 1: k_cg_jhv<0, 1, NC><<<grid, JH_NT, 0, s>>>(a); break;
+    case 2: k_cg_jhv<0, 2, NC><<<grid, JH_NT, 0, s>>>(a); break;
+    case 3: k_cg_jhv<1, 0, NC><<<grid, JH_NT, 0, s>>>(a); break;
+    case 4: k_cg_jhv<1, 1, NC><<<grid, JH_NT, 0, s>>>(a); break;
+    default: k_cg_jhv<1, 2, NC><<<grid, JH_NT, 0, s>>>(a); break;
+    }
+}
+void launch_cg_jhv(const CGArgs& a, cudaStream_t s)
+{
+    static const int nc = [] {
+        const char* v = std::getenv("CRT_B200_JH_COLS");
+        return v ? std::atoi(v) : JH_COLS;
+    }();
+    if (nc == 2) launch_cg_jhv_nc<2>(a, s);
+    else if (nc == 8) launch_cg_jhv_nc<8>(a, s);
+    else launch_cg_jhv_nc<4>(a, s);
+}
+}  // namespace
+
 bool cg_fused_fits(const CGArgs& a, int grid, size_t smem_max)
 {
     if (a.jprec != 1 || a.jmode == 1 || grid < 1) return false;
@@ -1282,8 +1312,7 @@ void launch_cg_iterations(const CGArgs& a, int iters, const SpcPlan* spc, Gnn* g
         } else {
             CRT_CG_DISPATCH(k_cg_jv, gjv, JV_NT, s, a);
             k_cg_jv_reduce<<<(a.N + nt - 1) / nt, nt, 0, s>>>(a);
-            const int cols_per_block = (JH_NT / 32) * JH_COLS;
-            CRT_CG_DISPATCH(k_cg_jhv, (a.M + cols_per_block - 1) / cols_per_block, JH_NT, s, a);
+            launch_cg_jhv(a, s);
         }
         k_cg_tail_sums<<<VS_CTAS, 32, 0, s>>>(a);
         k_cg_tail_update<<<gvec, VS_UPD_NT, 0, s>>>(a);
