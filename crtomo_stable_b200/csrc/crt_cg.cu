@@ -791,9 +791,9 @@ __device__ void cg_end_body(const CGArgs& A)
 // Head and tail of one solve across the grid.  CTA w (VEC_NT / 32 CTAs of one
 // warp) forms the partial sums of warp w of the one-CTA form, element by
 // element in the same order; the CTA that arrives last adds the partials as
-// that form's final warp does and takes the scalar step, so every sum and
-// every scalar is bit for bit the one-CTA form's.  The vector updates then
-// run as grid-wide kernels.
+// that form's final warp does and takes the scalar step, so every sum is
+// formed in the one-CTA form's order (the lambda-batched solve still runs
+// that form).  The vector updates then run as grid-wide kernels.
 constexpr int VS_CTAS = VEC_NT / 32, VS_UPD_NT = 256;
 
 // Lane 0 publishes q[0 .. n) of this CTA; true (in every lane) for the CTA
