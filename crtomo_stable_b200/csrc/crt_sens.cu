@@ -41,6 +41,19 @@ __device__ __forceinline__ double ld_phi<double>(const cd& v) { return v.x; }
 template <>
 __device__ __forceinline__ cd ld_phi<cd>(const cd& v) { return v; }
 
+// ld_phi as an asynchronous copy into shared memory (cp.async): the whole
+// complex value, or its real part (the first 8 bytes)
+template <typename T>
+__device__ __forceinline__ void phi_async(T* dst, const cd* src);
+template <>
+__device__ __forceinline__ void phi_async<cd>(cd* dst, const cd* src) { cp_async16(dst, src); }
+template <>
+__device__ __forceinline__ void phi_async<double>(double* dst, const cd* src)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(&src->x) : "memory");
+}
+
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT) k_sens(SensArgs A)
 {
@@ -187,10 +200,12 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
         const int tot = kn * nk * LP;
         __syncthreads();
         {
+            // the potentials by cp.async (every copy of the thread in flight
+            // at once; the real form takes the real parts, 8 bytes each)
             int a = a_0, m = q_0 % nk, kk = q_0 / nk;
-#pragma unroll 4
             for (int t = tid; t < tot; t += blockDim.x) {
-                phi[t] = a < L ? ld_phi<T>(A.kpt[((size_t)(k0 + kk) * A.n + s_node[m]) * L + a]) : Sc<T>::zero();
+                if (a < L) phi_async<T>(phi + t, A.kpt + ((size_t)(k0 + kk) * A.n + s_node[m]) * L + a);
+                else phi[t] = Sc<T>::zero();
                 a += da;
                 m += dq;
                 if (a >= LP) {
@@ -202,6 +217,8 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
                     ++kk;
                 }
             }
+            cp_async_commit();
+            cp_async_wait_all();
         }
         __syncthreads();
         {

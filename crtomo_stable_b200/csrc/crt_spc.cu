@@ -1032,18 +1032,25 @@ __global__ void __launch_bounds__(32 * NB) k_spc_correct(const float* __restrict
         xr[t] = rightc ? hc[(size_t)sp * B + t] : cf{0.0f, 0.0f};
         __syncthreads();
         x = h[(size_t)q * B + t];
-        const float* Vq = V + (size_t)q * BB + (size_t)t * B;
-        const float* Wq = W + (size_t)q * BB + (size_t)t * B;
-        if (left)
-            for (int k = 0; k < B; ++k) {
-                x.x -= Vq[k] * xl[k].x;
-                x.y -= Vq[k] * xl[k].y;
+        // thread t's row of V and W by 16-byte loads (a row is 16-byte
+        // aligned: B floats from a 16-byte aligned base), its entries taken
+        // in order
+        const float4* Vq = reinterpret_cast<const float4*>(V + (size_t)q * BB + (size_t)t * B);
+        const float4* Wq = reinterpret_cast<const float4*>(W + (size_t)q * BB + (size_t)t * B);
+        auto row = [&](const float4* Rq, const cf* xv) {
+#pragma unroll 4
+            for (int k4 = 0; k4 < B / 4; ++k4) {
+                const float4 v = Rq[k4];
+                const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    x.x -= e[u] * xv[4 * k4 + u].x;
+                    x.y -= e[u] * xv[4 * k4 + u].y;
+                }
             }
-        if (rightc)
-            for (int k = 0; k < B; ++k) {
-                x.x -= Wq[k] * xr[k].x;
-                x.y -= Wq[k] * xr[k].y;
-            }
+        };
+        if (left) row(Vq, xl);
+        if (rightc) row(Wq, xr);
     }
     const int el = perm[(size_t)q * B + t];
     if (el >= 0) z[el] = cd{(double)x.x, (double)x.y};
