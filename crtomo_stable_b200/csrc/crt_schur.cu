@@ -243,8 +243,8 @@ __global__ void k_schur_transpose(SchurArgs s, const T* __restrict__ Lws, T* Lre
 // right-hand sides live in a window Z[WZ][R] (row r at slot r mod WZ,
 // WZ >= mb + 3 BB), their rows arriving by cp.async two blocks ahead of
 // use.  Per block: the BB x BB triangle (one half-warp per column, shuffle
-// broadcasts), the finished rows out, and the (mb x BB) x (BB x R) update
-// of the rows below (4 x 4 register tiles).
+// broadcasts, lane t holding row t), the finished rows out, and the
+// (mb x BB) x (BB x R) update of the rows below (4 x TC register tiles).
 //   back == 0: forward sweep of X's columns (col_order, from each block's
 //     first non-zero row), in place;
 //   back == 1: the back sweep L^T x^ = z^ of the source columns: Lws holds
@@ -345,23 +345,30 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
         __syncthreads();
         // the block's rows sit in consecutive slots (WZ is a multiple of BB)
         const int sb = c0 % WZ;
-        if (tid < R) {   // the block's triangle: a lane per column, its 16 rows in registers
-            const int j = tid;
-            T z[BB];
+        {   // the block's triangle: a half-warp per column, lane t holds row t
+            // and its row of the block's L in registers; at step u lane u
+            // finishes its row and hands it to the half-warp by a shuffle, so
+            // every row takes z_t -= L_tu z_u for u = 0 .. t-1, then z_t *= 1/L_tt
+            constexpr int HW = NT / 16;   // half-warps of the CTA (NT is a multiple of 32)
+            const int hw = tid >> 4, lt = tid & 15;
+            for (int j0 = 0; j0 < R; j0 += HW) {
+                const int j = j0 + hw;
+                const bool act = j < R && lt < nb;
+                T zt = Sc<T>::zero(), lrow[BB];
 #pragma unroll
-            for (int t = 0; t < BB; ++t) z[t] = t < nb ? Z[(size_t)(sb + t) * R + j] : Sc<T>::zero();
+                for (int u = 0; u < BB; ++u)
+                    lrow[u] = (act && u < lt && lt - u <= mb) ? Lc[u * W + (lt - u)] : Sc<T>::zero();
+                if (act) zt = Z[(size_t)(sb + lt) * R + j];
 #pragma unroll
-            for (int u = 0; u < BB; ++u) {
-                if (u < nb) {
-                    z[u] = Sc<T>::mul(z[u], dinv[u]);
-#pragma unroll
-                    for (int t = u + 1; t < BB; ++t)
-                        if (t < nb && t - u <= mb) fms_acc(z[t], Lc[u * W + (t - u)], z[u]);
+                for (int u = 0; u < BB; ++u) {
+                    if (u < nb) {
+                        if (lt == u) zt = Sc<T>::mul(zt, dinv[u]);
+                        const T zu = shfl_w<T>(zt, u, 16);
+                        if (lt > u && lt < nb && lt - u <= mb) fms_acc(zt, lrow[u], zu);
+                    }
                 }
+                if (act) Z[(size_t)(sb + lt) * R + j] = zt;
             }
-#pragma unroll
-            for (int t = 0; t < BB; ++t)
-                if (t < nb) Z[(size_t)(sb + t) * R + j] = z[t];
         }
         __syncthreads();
         // the block's rows are final: out
@@ -1067,15 +1074,14 @@ int sweep_wz(int mbI) { return (mbI + 4 * SCHUR_MS_BB - 1) / SCHUR_MS_BB * SCHUR
 constexpr int SWEEP_NT = 288;   // 4 x 4 update tiles of a 129-row band at R = 32 in one round
 
 // Columns per update tile of the sweeps: 2 (twice the threads, each with
-// half the accumulators) or 4.  Measured on the 60k-triangle mesh: the back
-// sweep 22.7 ms with 2 against 23.7 with 4, the forward sweep's part after
-// the factor 13.0 against 11.7; CRT_B200_SCHUR_TILE=2 / 4 sets both.
-static int sweep_tc(bool back)
+// half the accumulators) or 4.  Measured on the 60k-triangle mesh with the
+// half-warp triangles: back sweep and rebuild 20.6 ms with 2 against 24.0
+// with 4, the forward sweep's part after the factor 11.7 against 12.5;
+// CRT_B200_SCHUR_TILE=4 selects the wider tiles.
+static int sweep_tc(bool)
 {
     const char* v = std::getenv("CRT_B200_SCHUR_TILE");
-    if (v && std::strcmp(v, "4") == 0) return 4;
-    if (v && std::strcmp(v, "2") == 0) return 2;
-    return back ? 2 : 4;
+    return (v && std::strcmp(v, "4") == 0) ? 4 : 2;
 }
 
 }  // namespace
