@@ -640,9 +640,16 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
         SchurHost& H = ctx->schur_h;
         // forward-sweep column blocks: 32 columns (one CTA per SM) or 16
         // (two CTAs per SM; CRT_B200_SCHUR_R=16)
+        // (16 also where the 32-column block's buffers exceed shared memory)
         const char* rv = std::getenv("CRT_B200_SCHUR_R");
-        const int sweep_r = (rv && std::strcmp(rv, "16") == 0) ? 16 : SCHUR_MS_R;
-        if (schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H, sweep_r) == CRT_OK &&
+        int sweep_r = (rv && std::strcmp(rv, "16") == 0) ? 16 : SCHUR_MS_R;
+        int plan_e = schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H, sweep_r);
+        if (plan_e == CRT_OK && sweep_r != 16 && schur_sweep_smem<cd>(H.mbI, H.mbI + 1, sweep_r) > 227 * 1024) {
+            sweep_r = 16;
+            H = SchurHost{};
+            plan_e = schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H, sweep_r);
+        }
+        if (plan_e == CRT_OK &&
             schur_sweep_smem<cd>(H.mbI, H.mbI + 1, sweep_r) <= 227 * 1024 &&
             (size_t)(16 + 1) * H.m * sizeof(cd) <= 227 * 1024 && band_factor_smem<cd>(H.mbI + 1) <= 227 * 1024) {
             auto up = [&](int** d, const std::vector<int>& v) {
