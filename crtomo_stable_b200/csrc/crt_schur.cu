@@ -439,6 +439,187 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
 }
 
 // ---------------------------------------------------------------------------
+// The back sweep of the source columns (R = 16 per CTA, 512 threads) with the
+// triangle beside the update: per block b (rows c0 .. c0 + 16), between
+// barriers,
+//   A. warps 0-7 solve block b's triangle (a half-warp per column, lane t
+//      holding row t; the finished row handed on by a shuffle) while warps
+//      8-15 take block b-1's columns into the rows past block b (those of
+//      block b took them in phase B of block b-1);
+//   B. threads 0-255 take block b's columns into block b+1's rows (an entry
+//      each) while warps 8-15 write block b's rows out.
+// Every row takes the blocks' columns in block order and each block's
+// columns in order, with the operations of k_schur_sweep; the factor's
+// column blocks b-1, b, b+1 sit in three buffers.
+template <typename T>
+__global__ void __launch_bounds__(512, 1) k_schur_back_pp(SchurArgs s, const T* __restrict__ Lws,
+                                                        const double* __restrict__ fakws, const T* X, cd* kpot,
+                                                        int n_kpot, int WZ)
+{
+    constexpr int R = 16, BB = 16, NT = 512, TC = 2;
+    extern __shared__ __align__(16) unsigned char bp_dyn[];
+    const int W = s.WI, n = s.nI, mb = s.mbI;
+    T* Lb = reinterpret_cast<T*>(bp_dyn);   // [3][BB * W]
+    T* Z = Lb + 3 * BB * W;                 // [WZ][R]
+    __shared__ T dinv[BB];
+    __shared__ int colid[R];
+    __shared__ __align__(8) unsigned long long bar[3];
+    __shared__ int s_err;
+    const int tid = threadIdx.x;
+    const int blk = blockIdx.y, k = s.k0 + blockIdx.x;
+    const T* Lk = Lws + (size_t)k * n * W;
+    if (tid < R) {
+        const int c = blk * R + tid;
+        colid[tid] = c < s.L ? c : -1;
+    }
+    if (tid == 0) {
+        s_err = 0;
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init(&bar[2], 1);
+    }
+    __syncthreads();
+    int phs = 0;
+    auto fetch = [&](int c0, int buf) {
+        if (tid == 0) {
+            const int bytes = min(BB, n - c0) * W * (int)sizeof(T);
+            mbar_expect_tx(&bar[buf], bytes);
+            bulk_g2s(Lb + (size_t)buf * BB * W, Lk + (size_t)c0 * W, bytes, &bar[buf]);
+        }
+    };
+    auto wait = [&](int buf) {
+        if (!mbar_wait(&bar[buf], (phs >> buf) & 1)) s_err = 1;
+        phs ^= 1 << buf;
+    };
+    auto colp = [&](int j) { return X + ((size_t)k * s.ncol + colid[j]) * n; };
+    auto issue_rows = [&](int r0, int r1) {
+        const int nr = r1 - r0;
+        for (int idx = tid; idx < nr * R; idx += NT) {
+            const int j = idx / nr, r = r0 + idx % nr;
+            T* dst = Z + (size_t)(r % WZ) * R + j;
+            if (colid[j] >= 0) cp_async_elem<T>(dst, colp(j) + (n - 1 - r));
+            else *dst = Sc<T>::zero();
+        }
+        cp_async_commit();
+    };
+    // rows [rlo, rhi) take the columns of the block at cb (nbb rows, factor
+    // block Lq), threads [t0, t0 + nt): 4 rows x TC columns per thread
+    auto update_rows = [&](const T* Lq, int cb, int nbb, int rlo, int rhi, int t0, int nt) {
+        if (rlo >= rhi) return;
+        const int NQ = (rhi - rlo + 3) >> 2;
+        constexpr int RJ = R / TC;
+        const int sbb = cb % WZ;
+        for (int tile = tid - t0; tile < NQ * RJ; tile += nt) {
+            const int rq = tile / RJ, jq = tile % RJ;
+            T acc[4][TC];
+            int sl[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const int r = rlo + rq + NQ * a;
+                sl[a] = r < rhi ? r % WZ : -1;
+#pragma unroll
+                for (int c = 0; c < TC; ++c)
+                    acc[a][c] = sl[a] >= 0 ? Z[(size_t)sl[a] * R + jq + RJ * c] : Sc<T>::zero();
+            }
+#pragma unroll
+            for (int u = 0; u < BB; ++u) {
+                if (u < nbb) {
+                    T zc[TC], lv[4];
+#pragma unroll
+                    for (int c = 0; c < TC; ++c) zc[c] = Z[(size_t)(sbb + u) * R + jq + RJ * c];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        const int d = rlo + rq + NQ * a - (cb + u);
+                        lv[a] = (sl[a] >= 0 && d <= mb) ? Lq[u * W + d] : Sc<T>::zero();
+                    }
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int c = 0; c < TC; ++c) fms_acc(acc[a][c], lv[a], zc[c]);
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+                if (sl[a] >= 0)
+#pragma unroll
+                    for (int c = 0; c < TC; ++c) Z[(size_t)sl[a] * R + jq + RJ * c] = acc[a][c];
+        }
+    };
+    const int start = 0;
+    issue_rows(start, min(n, start + BB + mb));
+    issue_rows(min(n, start + BB + mb), min(n, start + 2 * BB + mb));
+    fetch(start, 0);
+    if (start + BB < n) fetch(start + BB, 1);
+    cp_async_wait_group<1>();
+    __syncthreads();
+    int bi = 0;
+    for (int c0 = start; c0 < n; c0 += BB, ++bi) {
+        const int nb = min(BB, n - c0);
+        const int cur = bi % 3, prv = (bi + 2) % 3;
+        wait(cur);
+        const T* Lc = Lb + (size_t)cur * BB * W;
+        const T* Lp = Lb + (size_t)prv * BB * W;
+        if (tid < nb) dinv[tid] = Sc<T>::recip(Lc[tid * W]);
+        __syncthreads();
+        const int sb = c0 % WZ;
+        if (tid < 256) {
+            // A. block b's triangle: half-warp hw = column, lane lt = row
+            const int j = tid >> 4, lt = tid & 15;
+            const bool act = lt < nb;
+            T zt = Sc<T>::zero(), lrow[BB];
+#pragma unroll
+            for (int u = 0; u < BB; ++u)
+                lrow[u] = (act && u < lt && lt - u <= mb) ? Lc[u * W + (lt - u)] : Sc<T>::zero();
+            if (act) zt = Z[(size_t)(sb + lt) * R + j];
+#pragma unroll
+            for (int u = 0; u < BB; ++u) {
+                if (u < nb) {
+                    if (lt == u) zt = Sc<T>::mul(zt, dinv[u]);
+                    const T zu = shfl_w<T>(zt, u, 16);
+                    if (lt > u && lt < nb && lt - u <= mb) fms_acc(zt, lrow[u], zu);
+                }
+            }
+            if (act) Z[(size_t)(sb + lt) * R + j] = zt;
+        } else if (c0 > start) {
+            // A. block b-1 (BB rows) into rows [c0 + BB, c0 + mb)
+            update_rows(Lp, c0 - BB, BB, min(n, c0 + BB), min(n, c0 + mb), 256, 256);
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid < 256) {
+            // B. block b's columns into block b+1's rows, an entry (row, column) per thread
+            const int j = tid & 15, t = tid >> 4, r = c0 + nb + t;
+            if (r < n && t < BB) {
+                T z = Z[(size_t)(r % WZ) * R + j];
+#pragma unroll
+                for (int u = 0; u < BB; ++u) {
+                    const int d = r - (c0 + u);
+                    if (u < nb && d <= mb) fms_acc(z, Lc[u * W + d], Z[(size_t)(sb + u) * R + j]);
+                }
+                Z[(size_t)(r % WZ) * R + j] = z;
+            }
+        } else {
+            // B. block b's rows out
+            for (int idx = tid - 256; idx < nb * R; idx += 256) {
+                const int jj = idx / nb, t = idx % nb;
+                if (colid[jj] < 0) continue;
+                const int r = c0 + t;
+                const T v = Z[(size_t)(sb + t) * R + jj];
+                const int i = n - 1 - r;
+                kpot[((size_t)k * s.L + colid[jj]) * n_kpot + s.permI[i]] =
+                    Sc<T>::to_cd(scale(v, fakws[(size_t)k * n + i]));
+            }
+        }
+        if (c0 + 2 * BB < n) fetch(c0 + 2 * BB, prv);
+        issue_rows(min(n, c0 + 2 * BB + mb), min(n, c0 + 3 * BB + mb));
+        cp_async_wait_group<1>();
+        __syncthreads();
+    }
+    cp_async_wait_group<0>();
+    if (tid == 0 && s_err) atomicMax(&s.status[k], (int)CRT_ERR_CUDA);
+}
+
+// ---------------------------------------------------------------------------
 // C[k][c][g] = sum_i V^[i][g] X[i][c] over the rows where both columns can
 // be non-zero; tiles 64 (g) x 32 (c), 128 threads of 4 x 4.  The tiles of
 // the V^T V^ block above its diagonal are skipped (the Cholesky reads the
@@ -1242,8 +1423,20 @@ template <typename T>
 void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, const T* X, const T* xg, int n,
                        cd* kpot, cudaStream_t st)
 {
-    const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_BK_R);
     dim3 grid(s.nk, (s.L + SCHUR_BK_R - 1) / SCHUR_BK_R);
+    // the triangle beside the update (three factor buffers; 16.4 against
+    // 20.5 ms for back sweep and rebuild on the 60k-triangle mesh), unless
+    // CRT_B200_SCHUR_BACK_PP=0 or its buffers do not fit
+    const char* pv = std::getenv("CRT_B200_SCHUR_BACK_PP");
+    const size_t smem_pp = (size_t)3 * SCHUR_MS_BB * s.WI * sizeof(T) + (size_t)sweep_wz(s.mbI) * 16 * sizeof(T);
+    if (!(pv && std::strcmp(pv, "0") == 0) && smem_pp <= 227 * 1024) {
+        cudaFuncSetAttribute(k_schur_back_pp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pp);
+        k_schur_back_pp<T><<<grid, 512, smem_pp, st>>>(s, Lrev, fakws, X, kpot, n, sweep_wz(s.mbI));
+        const long long tot = (long long)s.nk * s.L * s.m;
+        k_schur_out_gam<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, xg, n, kpot);
+        return;
+    }
+    const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_BK_R);
     auto go = [&](auto kern, int nt) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         kern<<<grid, nt, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);

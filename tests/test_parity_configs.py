@@ -429,6 +429,30 @@ def test_schur_sweep_beside_the_factor_is_the_sequential_sweep(name, ldc, monkey
     assert np.array_equal(out["1"][1], out["0"][1])
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,ldc", [("mixed_surf", False), ("TestModInv", True)])
+def test_schur_back_sweep_pipelined_is_the_sequential_sweep(name, ldc, monkeypatch):
+    """The back sweep with the block triangles beside the update of the
+    rows below (warp groups in two phases, three factor buffers) applies
+    every row's contributions in the sequential sweep's order: potentials
+    and voltages bit for bit equal."""
+    from fixtures import load_forward_case
+    from crtomo_stable_b200.lib import FORWARD_SCHUR, Context
+    case = load_forward_case(name)
+    c = case["cfg"]
+    out = {}
+    for pp in ("1", "0"):
+        monkeypatch.setenv("CRT_B200_SCHUR_BACK_PP", pp)
+        ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=c.swrtr,
+                      lsink=c.lsink, nsink=c.nsink)
+        ctx.set_forward_form(FORWARD_SCHUR)
+        _, sa, kp = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+        out[pp] = (kp, sa)
+        ctx.close()
+    assert np.array_equal(out["1"][0], out["0"][0])
+    assert np.array_equal(out["1"][1], out["0"][1])
+
+
 def test_schur_form_is_refused_where_it_does_not_apply():
     """No mixed boundary (the 2D decoupling grid): the Schur form does not
     apply, the setter says so (errnr 201) and the direct form runs."""
