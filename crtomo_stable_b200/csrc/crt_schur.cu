@@ -439,8 +439,9 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
 }
 
 // ---------------------------------------------------------------------------
-// The back sweep of the source columns (R = 16 per CTA, 512 threads) with the
-// triangle beside the update: per block b (rows c0 .. c0 + 16), between
+// The sweeps with R = 16 columns per CTA (512 threads) and the triangle
+// beside the update (back: the source columns of the back sweep; forward:
+// the 16-column blocks of the forward sweep, CRT_B200_SCHUR_R=16): per block b (rows c0 .. c0 + 16), between
 // barriers,
 //   A. warps 0-7 solve block b's triangle (a half-warp per column, lane t
 //      holding row t; the finished row handed on by a shuffle) while warps
@@ -452,9 +453,9 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
 // columns in order, with the operations of k_schur_sweep; the factor's
 // column blocks b-1, b, b+1 sit in three buffers.
 template <typename T>
-__global__ void __launch_bounds__(512, 1) k_schur_back_pp(SchurArgs s, const T* __restrict__ Lws,
-                                                        const double* __restrict__ fakws, const T* X, cd* kpot,
-                                                        int n_kpot, int WZ)
+__global__ void __launch_bounds__(512, 1) k_schur_sweep_pp(SchurArgs s, const T* __restrict__ Lws,
+                                                         const double* __restrict__ fakws, T* X, cd* kpot,
+                                                         int n_kpot, int WZ, int back)
 {
     constexpr int R = 16, BB = 16, NT = 512, TC = 2;
     extern __shared__ __align__(16) unsigned char bp_dyn[];
@@ -467,10 +468,12 @@ __global__ void __launch_bounds__(512, 1) k_schur_back_pp(SchurArgs s, const T* 
     __shared__ int s_err;
     const int tid = threadIdx.x;
     const int blk = blockIdx.y, k = s.k0 + blockIdx.x;
+    const int start = back ? 0 : s.blk_start[blk];
+    if (start >= n) return;   // every column of the block is zero, and so is its solution
     const T* Lk = Lws + (size_t)k * n * W;
     if (tid < R) {
         const int c = blk * R + tid;
-        colid[tid] = c < s.L ? c : -1;
+        colid[tid] = back ? (c < s.L ? c : -1) : (c < s.ncol ? s.col_order[c] : -1);
     }
     if (tid == 0) {
         s_err = 0;
@@ -482,6 +485,24 @@ __global__ void __launch_bounds__(512, 1) k_schur_back_pp(SchurArgs s, const T* 
     int phs = 0;
     auto fetch = [&](int c0, int buf) {
         if (tid == 0) {
+            if (s.progress && !s_err) {
+                // beside the factor: its columns [c0, c0 + BB) are final once
+                // its progress passes them (bounded wait, as k_schur_sweep)
+                const int want = min(n, c0 + BB);
+                long polls = 0;
+                int got;
+                while (true) {
+                    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(got) : "l"(s.progress + k) : "memory");
+                    if (got >= want) break;
+                    if (*(volatile const int*)(s.status + k) != 0 || ++polls > (1L << 22)) {
+                        s_err = 1;
+                        atomicMax(&s.status[k], (int)CRT_ERR_CUDA);
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+                asm volatile("fence.proxy.async.global;\n" ::: "memory");
+            }
             const int bytes = min(BB, n - c0) * W * (int)sizeof(T);
             mbar_expect_tx(&bar[buf], bytes);
             bulk_g2s(Lb + (size_t)buf * BB * W, Lk + (size_t)c0 * W, bytes, &bar[buf]);
@@ -491,13 +512,13 @@ __global__ void __launch_bounds__(512, 1) k_schur_back_pp(SchurArgs s, const T* 
         if (!mbar_wait(&bar[buf], (phs >> buf) & 1)) s_err = 1;
         phs ^= 1 << buf;
     };
-    auto colp = [&](int j) { return X + ((size_t)k * s.ncol + colid[j]) * n; };
+    auto colp = [&](int j) { return X + ((size_t)k * s.ncol + colid[j]) * n; };   // the column's rows in X
     auto issue_rows = [&](int r0, int r1) {
         const int nr = r1 - r0;
         for (int idx = tid; idx < nr * R; idx += NT) {
             const int j = idx / nr, r = r0 + idx % nr;
             T* dst = Z + (size_t)(r % WZ) * R + j;
-            if (colid[j] >= 0) cp_async_elem<T>(dst, colp(j) + (n - 1 - r));
+            if (colid[j] >= 0) cp_async_elem<T>(dst, colp(j) + (back ? n - 1 - r : r));
             else *dst = Sc<T>::zero();
         }
         cp_async_commit();
@@ -545,7 +566,6 @@ __global__ void __launch_bounds__(512, 1) k_schur_back_pp(SchurArgs s, const T* 
                     for (int c = 0; c < TC; ++c) Z[(size_t)sl[a] * R + jq + RJ * c] = acc[a][c];
         }
     };
-    const int start = 0;
     issue_rows(start, min(n, start + BB + mb));
     issue_rows(min(n, start + BB + mb), min(n, start + 2 * BB + mb));
     fetch(start, 0);
@@ -605,9 +625,13 @@ __global__ void __launch_bounds__(512, 1) k_schur_back_pp(SchurArgs s, const T* 
                 if (colid[jj] < 0) continue;
                 const int r = c0 + t;
                 const T v = Z[(size_t)(sb + t) * R + jj];
-                const int i = n - 1 - r;
-                kpot[((size_t)k * s.L + colid[jj]) * n_kpot + s.permI[i]] =
-                    Sc<T>::to_cd(scale(v, fakws[(size_t)k * n + i]));
+                if (!back) {
+                    colp(jj)[r] = v;
+                } else {
+                    const int i = n - 1 - r;
+                    kpot[((size_t)k * s.L + colid[jj]) * n_kpot + s.permI[i]] =
+                        Sc<T>::to_cd(scale(v, fakws[(size_t)k * n + i]));
+                }
             }
         }
         if (c0 + 2 * BB < n) fetch(c0 + 2 * BB, prv);
@@ -1301,6 +1325,14 @@ void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t s
     };
     // update tiles of 4 rows x TC columns: one round of a 129-row band
     const bool narrow = sweep_tc(false) == 2;
+    const size_t smem_pp = (size_t)3 * SCHUR_MS_BB * s.WI * sizeof(T) + (size_t)sweep_wz(s.mbI) * 16 * sizeof(T);
+    const char* pv = std::getenv("CRT_B200_SCHUR_BACK_PP");
+    if (s.R == 16 && !(pv && std::strcmp(pv, "0") == 0) && smem_pp <= 227 * 1024) {
+        // 16-column blocks: the triangle beside the update (as the back sweep)
+        cudaFuncSetAttribute(k_schur_sweep_pp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pp);
+        k_schur_sweep_pp<T><<<grid, 512, smem_pp, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+        return;
+    }
     if (s.R == 16) {
         if (narrow) go(k_schur_sweep<T, 288, 16, SCHUR_MS_BB, 2>, 288);
         else go(k_schur_sweep<T, 160, 16, SCHUR_MS_BB, 4>, 160);
@@ -1430,8 +1462,8 @@ void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, c
     const char* pv = std::getenv("CRT_B200_SCHUR_BACK_PP");
     const size_t smem_pp = (size_t)3 * SCHUR_MS_BB * s.WI * sizeof(T) + (size_t)sweep_wz(s.mbI) * 16 * sizeof(T);
     if (!(pv && std::strcmp(pv, "0") == 0) && smem_pp <= 227 * 1024) {
-        cudaFuncSetAttribute(k_schur_back_pp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pp);
-        k_schur_back_pp<T><<<grid, 512, smem_pp, st>>>(s, Lrev, fakws, X, kpot, n, sweep_wz(s.mbI));
+        cudaFuncSetAttribute(k_schur_sweep_pp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pp);
+        k_schur_sweep_pp<T><<<grid, 512, smem_pp, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);
         const long long tot = (long long)s.nk * s.L * s.m;
         k_schur_out_gam<T><<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(s, xg, n, kpot);
         return;
