@@ -952,8 +952,8 @@ __global__ void k_schur_s0_area(SchurArgs s, BandArgs<T> A, T* S0)
     if (g != h) Sk[(size_t)g * m + h] += a;
 }
 
-// The preconditioned iteration for SCHUR_IT_NS systems of one electrode
-// group (one CTA): x_0 = 0, r = b - S_l x, z = S_ref^-1 r, x += z, until
+// The preconditioned iteration for NS systems of one electrode group (one
+// CTA): x_0 = 0, r = b - S_l x, z = S_ref^-1 r, x += z, until
 // max |z| <= tol max |x| for every system.  X and R/Z live in shared memory,
 // a system's column contiguous ([NS][m], so that threads over rows touch
 // consecutive words); S0 and the reference factor stream from L2.  The
@@ -976,13 +976,15 @@ __global__ void k_schur_dvals(SchurArgs s, BandArgs<T> A, T* Dv)
     Dv[idx] = band_assemble_part<T>(A, s.bd_ent[q], k, l, 1, 1);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(SCHUR_IT_NT, 1) k_schur_iter(SchurArgs s, BandArgs<T> A, const T* __restrict__ C,
-                                                              const T* __restrict__ S0, const T* __restrict__ Lref,
-                                                              const T* __restrict__ Dv, T* xg, int maxit,
-                                                              double tol, int* nonconv)
+// NS systems per CTA (8, or 4 at two CTAs per SM: MINB); each system's
+// arithmetic does not depend on NS.
+template <typename T, int NS = SCHUR_IT_NS, int MINB = 1>
+__global__ void __launch_bounds__(SCHUR_IT_NT, MINB) k_schur_iter(SchurArgs s, BandArgs<T> A, const T* __restrict__ C,
+                                                                 const T* __restrict__ S0, const T* __restrict__ Lref,
+                                                                 const T* __restrict__ Dv, T* xg, int maxit,
+                                                                 double tol, int* nonconv)
 {
-    constexpr int NS = SCHUR_IT_NS, NT = SCHUR_IT_NT, PB = SCHUR_IT_PB;
+    constexpr int NT = SCHUR_IT_NT, PB = SCHUR_IT_PB;
     extern __shared__ __align__(16) unsigned char it_dyn[];
     const int m = s.m, L = s.L;
     T* X = reinterpret_cast<T*>(it_dyn);   // [NS][m]: system j's column at j m
@@ -1435,6 +1437,19 @@ template <typename T>
 void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, const T* S0, const T* Lref,
                        const T* Dv, T* xg, int maxit, double tol, int* nonconv, cudaStream_t st)
 {
+    // four systems per CTA at two CTAs per SM (electrode solves 13.6 against
+    // 15.9 ms with eight at one on the 60k-triangle mesh: the panel solves
+    // are chains of dependent steps, and two CTAs hide each other's
+    // latency); CRT_B200_SCHUR_IT_NS=8 keeps eight
+    const char* nv = std::getenv("CRT_B200_SCHUR_IT_NS");
+    if (!(nv && std::strcmp(nv, "8") == 0) && 2 * (2 * (size_t)s.m * 4 * sizeof(T)) <= 227 * 1024) {
+        const size_t smem = 2 * (size_t)s.m * 4 * sizeof(T);
+        const int cpg = (s.grp + 3) / 4;
+        auto kern = k_schur_iter<T, 4, 2>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        kern<<<s.K * s.ngrp * cpg, SCHUR_IT_NT, smem, st>>>(s, full, C, S0, Lref, Dv, xg, maxit, tol, nonconv);
+        return;
+    }
     const size_t smem = schur_iter_smem<T>(s.m);
     const int cpg = (s.grp + SCHUR_IT_NS - 1) / SCHUR_IT_NS;
     auto kern = k_schur_iter<T>;

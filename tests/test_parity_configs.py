@@ -453,6 +453,33 @@ def test_schur_back_sweep_pipelined_is_the_sequential_sweep(name, ldc, monkeypat
     assert np.array_equal(out["1"][1], out["0"][1])
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,ldc", [("mixed_surf", False), ("TestModInv", True)])
+def test_schur_iteration_four_systems_per_cta_is_eight(name, ldc, monkeypatch):
+    """The electrode iteration with 4 systems per CTA (two CTAs per SM)
+    against 8: each system's steps are the same, but a CTA iterates until
+    all its systems have converged, so the other grouping may add a step to
+    some systems; the potentials agree to the iteration's tolerance."""
+    from fixtures import load_forward_case
+    from crtomo_stable_b200.lib import FORWARD_SCHUR, Context
+    case = load_forward_case(name)
+    c = case["cfg"]
+    monkeypatch.setenv("CRT_B200_SCHUR_SOLVE", "iter")
+    out = {}
+    for ns in ("4", "8"):
+        monkeypatch.setenv("CRT_B200_SCHUR_IT_NS", ns)
+        ctx = Context(case["mesh"], case["enr"], case["volt"].strnr, case["volt"].vnr, swrtr=c.swrtr,
+                      lsink=c.lsink, nsink=c.nsink)
+        ctx.set_forward_form(FORWARD_SCHUR)
+        _, sa, kp = ctx.forward(case["sigma"], ldc=ldc, want_kpot=True)
+        out[ns] = (kp, sa, ctx.timings()["schur_iter"])
+        ctx.close()
+    assert out["4"][2] >= 1.0
+    scale = np.abs(out["8"][0]).max()
+    assert np.abs(out["4"][0] - out["8"][0]).max() <= 1e-12 * scale
+    np.testing.assert_allclose(out["4"][1], out["8"][1], rtol=1e-11, atol=0)
+
+
 def test_schur_form_is_refused_where_it_does_not_apply():
     """No mixed boundary (the 2D decoupling grid): the Schur form does not
     apply, the setter says so (errnr 201) and the direct form runs."""
