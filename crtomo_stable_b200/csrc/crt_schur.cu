@@ -1440,7 +1440,8 @@ void launch_schur_iter(const SchurArgs& s, const BandArgs<T>& full, const T* C, 
     // four systems per CTA at two CTAs per SM (electrode solves 13.6 against
     // 15.9 ms with eight at one on the 60k-triangle mesh: the panel solves
     // are chains of dependent steps, and two CTAs hide each other's
-    // latency); CRT_B200_SCHUR_IT_NS=8 keeps eight
+    // latency; two systems at three CTAs per SM measured 14.8 ms);
+    // CRT_B200_SCHUR_IT_NS=8 keeps eight
     const char* nv = std::getenv("CRT_B200_SCHUR_IT_NS");
     if (!(nv && std::strcmp(nv, "8") == 0) && 2 * (2 * (size_t)s.m * 4 * sizeof(T)) <= 227 * 1024) {
         const size_t smem = 2 * (size_t)s.m * 4 * sizeof(T);
