@@ -638,11 +638,12 @@ extern "C" crt_ctx* crt_create(int32_t device, const crt_mesh* mesh, const crt_s
         for (int rel : mixed_rel)
             for (int q = 0; q < 2; ++q) gnodes.push_back(nrel0[(size_t)(m.elanz + rel) * m.maxnodes + q]);
         SchurHost& H = ctx->schur_h;
-        // forward-sweep column blocks: 32 columns (one CTA per SM) or 16
-        // (two CTAs per SM; CRT_B200_SCHUR_R=16)
+        // forward-sweep column blocks: 16 columns (two CTAs per SM with the
+        // rows one block ahead: 11.0 ms after the factor on the 60k-triangle
+        // mesh) or 32 (one CTA per SM, 11.7 ms; CRT_B200_SCHUR_R=32)
         // (16 also where the 32-column block's buffers exceed shared memory)
         const char* rv = std::getenv("CRT_B200_SCHUR_R");
-        int sweep_r = (rv && std::strcmp(rv, "16") == 0) ? 16 : SCHUR_MS_R;
+        int sweep_r = (rv && std::strcmp(rv, "32") == 0) ? SCHUR_MS_R : 16;
         int plan_e = schur_plan_host(lists, ctx->n, gnodes, enr0, ctx->lsink, ctx->nsink - 1, H, sweep_r);
         if (plan_e == CRT_OK && sweep_r != 16 && schur_sweep_smem<cd>(H.mbI, H.mbI + 1, sweep_r) > 227 * 1024) {
             sweep_r = 16;

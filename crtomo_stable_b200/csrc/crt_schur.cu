@@ -250,10 +250,10 @@ __global__ void k_schur_transpose(SchurArgs s, const T* __restrict__ Lws, T* Lre
 //   back == 1: the back sweep L^T x^ = z^ of the source columns: Lws holds
 //     the reversed row-packed factor and the rows are read reversed; the
 //     solution goes out as kpot = fak x^ at the interior rows' nodes.
-template <typename T, int NT, int R, int BB, int TC = 4>
-__global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __restrict__ Lws,
-                                                       const double* __restrict__ fakws, T* X, cd* kpot, int n_kpot,
-                                                       int WZ, int back)
+template <typename T, int NT, int R, int BB, int TC = 4, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) k_schur_sweep(SchurArgs s, const T* __restrict__ Lws,
+                                                          const double* __restrict__ fakws, T* X, cd* kpot, int n_kpot,
+                                                          int WZ, int back, int ahead = 2)
 {
     static_assert(BB == 16 && R % 4 == 0 && R <= 32 && NT % 32 == 0 && NT >= R && (TC == 4 || TC == 2),
                   "sweep layout");
@@ -328,18 +328,23 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
         }
         cp_async_commit();
     };
+    // rows arrive `ahead` blocks before use: 2 (WZ >= mb + 3 BB, the wait at
+    // the end of a block leaves one group in flight) or 1 (WZ >= mb + 2 BB,
+    // the rows issued at the start of a block awaited at its end: the
+    // smaller window lets two CTAs share an SM)
     issue_rows(start, min(n, start + BB + mb));
-    issue_rows(min(n, start + BB + mb), min(n, start + 2 * BB + mb));
+    if (ahead == 2) issue_rows(min(n, start + BB + mb), min(n, start + 2 * BB + mb));
     fetch(start, 0);
-    cp_async_wait_group<1>();
+    if (ahead == 2) cp_async_wait_group<1>();
+    else cp_async_wait_group<0>();
     __syncthreads();
     int buf = 0;
     for (int c0 = start; c0 < n; c0 += BB) {
         const int nb = min(BB, n - c0);
         wait(buf);
         if (c0 + BB < n) fetch(c0 + BB, buf ^ 1);
-        // the rows two blocks ahead (their slots held rows finished a block ago)
-        issue_rows(min(n, c0 + 2 * BB + mb), min(n, c0 + 3 * BB + mb));
+        // the rows `ahead` blocks ahead (their slots held rows finished a block ago)
+        issue_rows(min(n, c0 + (ahead + 1) * BB + mb - BB), min(n, c0 + (ahead + 1) * BB + mb));
         const T* Lc = Lb + (size_t)buf * BB * W;
         if (tid < nb) dinv[tid] = Sc<T>::recip(Lc[tid * W]);
         __syncthreads();
@@ -430,7 +435,8 @@ __global__ void __launch_bounds__(NT, 1) k_schur_sweep(SchurArgs s, const T* __r
         }
         // the buffer just read is the destination of the bulk copy after next
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        cp_async_wait_group<1>();   // the rows of the next block have landed
+        if (ahead == 2) cp_async_wait_group<1>();   // the rows of the next block have landed
+        else cp_async_wait_group<0>();
         __syncthreads();
         buf ^= 1;
     }
@@ -1323,16 +1329,26 @@ void launch_schur_forward(const SchurArgs& s, const T* Lws, T* X, cudaStream_t s
     dim3 grid(s.nk, s.nblk);
     auto go = [&](auto kern, int nt) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, nt, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+        kern<<<grid, nt, smem, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0, 2);
     };
     // update tiles of 4 rows x TC columns: one round of a 129-row band
     const bool narrow = sweep_tc(false) == 2;
     const size_t smem_pp = (size_t)3 * SCHUR_MS_BB * s.WI * sizeof(T) + (size_t)sweep_wz(s.mbI) * 16 * sizeof(T);
-    const char* pv = std::getenv("CRT_B200_SCHUR_BACK_PP");
-    if (s.R == 16 && !(pv && std::strcmp(pv, "0") == 0) && smem_pp <= 227 * 1024) {
+    const char* fv = std::getenv("CRT_B200_SCHUR_FWD");
+    if (s.R == 16 && fv && std::strcmp(fv, "pp") == 0 && smem_pp <= 227 * 1024) {
         // 16-column blocks: the triangle beside the update (as the back sweep)
         cudaFuncSetAttribute(k_schur_sweep_pp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_pp);
         k_schur_sweep_pp<T><<<grid, 512, smem_pp, st>>>(s, Lws, nullptr, X, nullptr, 0, sweep_wz(s.mbI), 0);
+        return;
+    }
+    // 16-column blocks, rows one block ahead: the window of mb + 2 BB rows
+    // lets two CTAs share an SM (2 x 113 KB with the driver's reserve)
+    const int wz1 = (s.mbI + 2 * SCHUR_MS_BB + SCHUR_MS_BB - 1) / SCHUR_MS_BB * SCHUR_MS_BB;
+    const size_t smem1 = (size_t)2 * SCHUR_MS_BB * s.WI * sizeof(T) + (size_t)wz1 * 16 * sizeof(T);
+    if (s.R == 16 && !(fv && std::strcmp(fv, "wide") == 0) && 2 * (smem1 + 2048) <= 228 * 1024) {
+        auto kern = k_schur_sweep<T, 288, 16, SCHUR_MS_BB, 2, 2>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
+        kern<<<grid, 288, smem1, st>>>(s, Lws, nullptr, X, nullptr, 0, wz1, 0, 1);
         return;
     }
     if (s.R == 16) {
@@ -1487,7 +1503,7 @@ void launch_schur_back(const SchurArgs& s, const T* Lrev, const double* fakws, c
     const size_t smem = schur_sweep_smem<T>(s.mbI, s.WI, SCHUR_BK_R);
     auto go = [&](auto kern, int nt) {
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        kern<<<grid, nt, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1);
+        kern<<<grid, nt, smem, st>>>(s, Lrev, fakws, const_cast<T*>(X), kpot, n, sweep_wz(s.mbI), 1, 2);
     };
     // 4 x 2 update tiles of a 129-row band at R = 16 in one round (288
     // threads), or 4 x 4 (160)
