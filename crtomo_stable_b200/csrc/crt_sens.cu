@@ -274,8 +274,8 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
     }
     __syncthreads();
     const cd sig = A.sigma[e];
-    for (int i = tid; i < A.N; i += blockDim.x) {
-        const int4 el = A.elec[i];    // 0-based C1, C2, P1, P2; -1 when absent
+    // reading i: its four Gram entries, the reference's scaling, the store
+    auto value = [&](int4 el, int i) {
         auto g = [&](int a, int b) { return (a < 0 || b < 0) ? Sc<T>::zero() : G[gram_idx(a, b)]; };
         const T acc_i = ((g(el.w, el.y) - g(el.w, el.x)) - g(el.z, el.y)) + g(el.z, el.x);
         cd res;
@@ -304,6 +304,9 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
             else d = d * (st / A.pi);
             res = -d;
         }
+        return res;
+    };
+    auto store = [&](cd res, int i) {
         const size_t o = (size_t)e * A.N + i;
         if (A.mode == 1) {
             if (A.out_prec) reinterpret_cast<float*>(A.sens)[o] = (float)res.x;
@@ -312,6 +315,25 @@ __global__ void __launch_bounds__(MAXT) k_sens_gram(SensArgs A, int LP, int kc)
             if (A.out_prec) reinterpret_cast<cf*>(A.sens)[o] = cf{(float)res.x, (float)res.y};
             else reinterpret_cast<cd*>(A.sens)[o] = res;
         }
+    };
+    // four readings per thread at a time: their (dependent) chains overlap
+    const int nt = blockDim.x;
+    for (int i0 = tid; i0 < A.N; i0 += 4 * nt) {
+        int4 el[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int i = i0 + q * nt;
+            el[q] = i < A.N ? A.elec[i] : make_int4(-1, -1, -1, -1);
+        }
+        cd res[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int i = i0 + q * nt;
+            res[q] = i < A.N ? value(el[q], i) : cd{0.0, 0.0};
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (i0 + q * nt < A.N) store(res[q], i0 + q * nt);
     }
 }
 
