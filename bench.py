@@ -715,6 +715,9 @@ def main():
                 # one CTA of 512 threads per wavenumber: K of the 148 SMs
                 ent["sms_used"] = K
                 ent["frac_of_used_sms"] = ach / (fp64_peak * K / 148.0)
+                ent["note"] = ("a system per CTA: every row's pivot (complex square root and reciprocal, then the "
+                               "update of the next diagonal entry) is a chain of dependent FP64 operations, about "
+                               "1 us per row; the forward sweep runs beside it on the other SMs")
             kernels.append(ent)
     # the dominant kernel: the longest phase whose time is its own (the
     # overlapped sweep's span contains the factor)
@@ -727,7 +730,7 @@ def main():
                 "peak_source": ("FP64 FMA pipe, 64 FMA/clk/SM x 148 SMs at the max SM clock (the Schur kernels run "
                                 "in FP64 on the CUDA cores; MEASURED_PEAKS.json holds HBM and bf16 tensor figures only)"),
                 "algorithmic_flops_per_launch": dom["flops"], "launch_ms": dom["ms"], "launches": 1.0}
-        for key in ("sms_used", "frac_of_used_sms"):
+        for key in ("sms_used", "frac_of_used_sms", "note"):
             if key in dom:
                 roof[key] = dom[key]
     roof_cg = None
